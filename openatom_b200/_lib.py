@@ -1,0 +1,98 @@
+"""ctypes binding of libcpstep.so (the C ABI declared in include/cpstep.h).
+
+The library is built in-tree (``python -m openatom_b200.build``).  Loading
+fails loudly when it is missing: there is no CPU fallback for any entry point.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcpstep.so")
+
+CPSTEP_OK = 0
+CPSTEP_ERR_ARG = 1
+CPSTEP_ERR_CUDA = 2
+CPSTEP_ERR_LAYOUT = 3
+CPSTEP_ERR_NOCONV = 4
+CPSTEP_ERR_STATE = 5
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_dbl_p = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+# name -> (restype, argtypes); every exported entry point of include/cpstep.h
+SIGNATURES = {
+    "cpstep_version": (ctypes.c_int, []),
+    "cpstep_last_error": (ctypes.c_char_p, []),
+    "cpstep_layout_sizes": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, _c_int_p, _c_int_p,
+                                           _c_int_p, _c_int_p]),
+    "cpstep_layout_build": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, _c_int_p, _c_int_p,
+                                           _c_int_p, _c_int_p, ctypes.c_int, _c_int_p,
+                                           _c_int_p]),
+    "cpstep_ctx_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, ctypes.c_int,
+                                         _c_int_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         _c_dbl_p, ctypes.c_double]),
+    "cpstep_ctx_destroy": (ctypes.c_int, [_vp]),
+    "cpstep_ctx_set_stream": (ctypes.c_int, [_vp, _vp]),
+    "cpstep_ctx_info": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
+    "cpstep_ctx_sync": (ctypes.c_int, [_vp]),
+    "cpstep_expand_gspace": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
+    "cpstep_pack_gspace": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
+    "cpstep_stp_fft_gtor": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
+    "cpstep_stp_fft_rtog": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int]),
+    "cpstep_density": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "cpstep_vks_psi": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "cpstep_eke": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+}
+
+
+class CpstepError(RuntimeError):
+    def __init__(self, fn, code, msg):
+        super().__init__("%s failed (code %d): %s" % (fn, code, msg))
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libcpstep.so once; raise if it is absent (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libcpstep.so is not built (run `python -m openatom_b200.build`); "
+                              "openatom_b200 has no CPU fallback")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(name, code):
+    if code != CPSTEP_OK:
+        msg = lib().cpstep_last_error()
+        raise CpstepError(name, code, msg.decode() if msg else "")
+
+
+def call(name, *args):
+    check(name, getattr(lib(), name)(*args))
+
+
+def ptr(t):
+    """Device pointer of a torch tensor as c_void_p (None for None)."""
+    if t is None:
+        return None
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def int_array(a):
+    import numpy as np
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(_c_int_p)

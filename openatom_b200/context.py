@@ -1,0 +1,130 @@
+"""Python host mirror of the libcpstep context (device memory via torch).
+
+Each method is a thin call through the C ABI of ``include/cpstep.h``; the
+docstrings name the OpenAtom routine the call replaces.  Arrays are torch CUDA
+tensors: coefficients complex128 [nstates, npts] in the reference's packed
+order, real-space grids float64 [nz, ny, nx].
+"""
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import ptr
+
+
+class StepContext:
+    def __init__(self, layout, nstates, precision="fp64", ecut_ry=None, device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("StepContext needs a CUDA device (no CPU fallback)")
+        self.layout = layout
+        self.nstates = int(nstates)
+        self.precision = precision
+        prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[precision]
+        self.device = torch.device(device or "cuda")
+        self.n = layout.n
+        kx, pkx = _lib.int_array(layout.kx)
+        ky, pky = _lib.int_array(layout.ky)
+        kz, pkz = _lib.int_array(layout.kz)
+        runs, pruns = _lib.int_array(layout.runs.reshape(-1))
+        hm = layout.hmat.astype("float64")
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.call("cpstep_ctx_create", ctypes.byref(h), prec, self.nstates, layout.npts,
+                      pkx, pky, pkz, len(layout.runs), pruns, self.n, self.n, self.n,
+                      hm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                      float(ecut_ry if ecut_ry is not None else layout.ecut_ry))
+        self._h = h
+        self._stream = None
+        self._sync_stream()
+
+    # -- plumbing ----------------------------------------------------------
+    def _sync_stream(self):
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        if s != self._stream:
+            _lib.call("cpstep_ctx_set_stream", self._h, ctypes.c_void_p(s))
+            self._stream = s
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.lib().cpstep_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk_psi(self, psi, nstates=None):
+        S = self.nstates if nstates is None else nstates
+        if psi.dtype != torch.complex128 or not psi.is_cuda or not psi.is_contiguous():
+            raise ValueError("psi must be a contiguous complex128 CUDA tensor")
+        if psi.shape != (S, self.layout.npts):
+            raise ValueError("psi shape %s != (%d, %d)" % (tuple(psi.shape), S, self.layout.npts))
+
+    def info(self):
+        nl, npx = ctypes.c_int(), ctypes.c_int()
+        _lib.call("cpstep_ctx_info", self._h, ctypes.byref(nl), ctypes.byref(npx))
+        return nl.value, npx.value
+
+    # -- FFTcache mirrors ----------------------------------------------------
+    def expand_gspace(self, psi):
+        """FFTcache::expandGSpace (fftCache.C:460-507): packed -> [S, nlines, nz]."""
+        self._sync_stream()
+        S = psi.shape[0]
+        out = torch.empty((S, self.layout.nlines, self.n), dtype=torch.complex128,
+                          device=self.device)
+        _lib.call("cpstep_expand_gspace", self._h, ptr(psi), ptr(out), S)
+        return out
+
+    def pack_gspace(self, lines):
+        """FFTcache::packGSpace (fftCache.C:517-553): [S, nlines, nz] -> packed."""
+        self._sync_stream()
+        S = lines.shape[0]
+        out = torch.zeros((S, self.layout.npts), dtype=torch.complex128, device=self.device)
+        _lib.call("cpstep_pack_gspace", self._h, ptr(lines), ptr(out), S)
+        return out
+
+    def fft_g_to_r(self, psi):
+        """doStpFFTGtoR_Gchare + transpose + doStpFFTGtoR_Rchare: psi(r) [S, n, n, n]."""
+        self._sync_stream()
+        S = psi.shape[0]
+        self._chk_psi(psi, S)
+        out = torch.empty((S, self.n, self.n, self.n), dtype=torch.float64, device=self.device)
+        _lib.call("cpstep_stp_fft_gtor", self._h, ptr(psi), ptr(out), S)
+        return out
+
+    def fft_r_to_g(self, f):
+        """doStpFFTRtoG_Rchare + transpose + doStpFFTRtoG_Gchare (unscaled)."""
+        self._sync_stream()
+        S = f.shape[0]
+        f = f.contiguous()
+        out = torch.empty((S, self.layout.npts), dtype=torch.complex128, device=self.device)
+        _lib.call("cpstep_stp_fft_rtog", self._h, ptr(f), ptr(out), S)
+        return out
+
+    def density(self, psi, occ):
+        """rho(r) = sum occ psi^2 / vol (CP_State_RealSpacePlane.C:349-355 + reduction)."""
+        self._sync_stream()
+        self._chk_psi(psi)
+        rho = torch.empty((self.n, self.n, self.n), dtype=torch.float64, device=self.device)
+        _lib.call("cpstep_density", self._h, ptr(psi), ptr(occ), ptr(rho))
+        return rho
+
+    def vks_psi(self, psi, vks, occ, kinetic=True):
+        """F = addForces(-2/N FFT^-1[occ V psi]) (+ CP_eke_calc when kinetic)."""
+        self._sync_stream()
+        self._chk_psi(psi)
+        force = torch.empty_like(psi)
+        eke = torch.empty(self.nstates, dtype=torch.float64, device=self.device) if kinetic else None
+        _lib.call("cpstep_vks_psi", self._h, ptr(psi), ptr(vks.contiguous()), ptr(occ),
+                  ptr(force), ptr(eke))
+        return force, eke
+
+    def eke(self, force, psi, occ):
+        """CPNONLOCAL::CP_eke_calc on all states; updates force in place."""
+        self._sync_stream()
+        e = torch.empty(self.nstates, dtype=torch.float64, device=self.device)
+        _lib.call("cpstep_eke", self._h, ptr(force), ptr(psi), ptr(occ), ptr(e))
+        return e

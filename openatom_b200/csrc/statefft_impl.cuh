@@ -1,0 +1,548 @@
+// State FFT pipeline for a cubic grid of compile-time size N:
+//   packed psi(G) -> z-pencils -> xy planes -> rho(r)
+//   V_KS(r).psi(r) -> xy planes -> z-pencils -> packed F(G) (+ kinetic term)
+//
+// Reference steps (OpenAtom, src_charm_driver/):
+//   expandGSpace / z-FFT           fft_slab_ctrl/fftCache.C:460-507, :1133-1159
+//   transpose to planes            cp_state_ctrl/CP_State_GSpacePlane.C:1473-1498,
+//                                  cp_state_ctrl/CP_State_RealSpacePlane.C:248-268
+//   y-FFT, imag flip, x C2R        fft_slab_ctrl/fftCache.C:1167-1243
+//   occ*psi^2 and the reduction    cp_state_ctrl/CP_State_RealSpacePlane.C:349-355, :484-500
+//   psi*V_KS*occ                   cp_state_ctrl/CP_State_RealSpacePlane.C:580-587
+//   x R2C, imag flip, y-FFT        fft_slab_ctrl/fftCache.C:1252-1319
+//   z-FFT, packGSpace, -2/N scale  fft_slab_ctrl/fftCache.C:1099-1123, :517-553,
+//                                  cp_state_ctrl/CP_State_GSpacePlane.C:1605-1612
+//   addForces (x2 off Gx=0)        fft_slab_ctrl/stateSlab.C:240-272
+//   CP_eke_calc                    src_piny_physics_v1.0/abinito_physics/cp_nonlocal/cp_eke.C:30-140
+//
+// On one GPU the Charm++ transposes become the [state][z][line] pencil layout:
+// the z-pass writes, for every z, the contiguous run of its lines, and the
+// plane pass reads one contiguous row of nlines values per (state, z).  psi(r)
+// is never stored: the V.psi pass recomputes it from the pencils, which hold
+// 2*nlines*N reals per state against N^3 for psi(r).
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <vector>
+#include "ctx.cuh"
+
+namespace sfft {
+
+constexpr int ZTHREADS = 256;
+constexpr int ZEPT = 16;
+constexpr int PTHREADS = 512;
+constexpr int PEPT = 8;
+
+template <typename T>
+struct Kmax;
+template <>
+struct Kmax<float> { static constexpr int v = 16; };
+template <>
+struct Kmax<double> { static constexpr int v = 8; };
+
+// packed point p -> (line index within the batch, z) by binary search over the
+// batch's line offsets held in shared memory.
+__device__ __forceinline__ void locate(int p, const int* soff, int nl, const int* snneg,
+                                       const int* szneg, const int* szpos, int& li, int& z) {
+  int lo = 0, hi = nl - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (soff[mid] <= p) lo = mid; else hi = mid - 1;
+  }
+  li = lo;
+  int q = p - soff[lo];
+  z = (q < snneg[lo]) ? szneg[lo] + q : szpos[lo] + (q - snneg[lo]);
+}
+
+template <int N>
+struct ZShape {
+  static constexpr int LB = std::min(64, (ZEPT * ZTHREADS) / N);  // lines per block
+  static constexpr int LD = N + 1;
+  template <typename T>
+  static constexpr size_t bytes() {
+    return sizeof(cplx<T>) * (size_t)(N + LB * LD) + sizeof(int) * (4 * LB + 1);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// K1: expand packed psi into z-lines, forward z-FFT, write [s][z][line] pencils
+template <typename T, int N>
+__global__ void __launch_bounds__(ZTHREADS)
+k_zfft_fwd(const double2* __restrict__ psi, cplx<T>* __restrict__ pen, StateGeom g,
+           const cplx<T>* __restrict__ twz) {
+  constexpr int LB = ZShape<N>::LB, LD = ZShape<N>::LD;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* buf = tw + N;
+  int* soff = reinterpret_cast<int*>(buf + LB * LD);
+  int* snneg = soff + LB + 1;
+  int* szneg = snneg + LB;
+  int* szpos = szneg + LB;
+  const int s = blockIdx.y;
+  const int l0 = blockIdx.x * LB;
+  const int nl = min(LB, g.nlines - l0);
+  for (int i = threadIdx.x; i < N; i += ZTHREADS) tw[i] = twz[i];
+  for (int i = threadIdx.x; i < LB * LD; i += ZTHREADS) buf[i] = mk<T>(0, 0);
+  for (int i = threadIdx.x; i < nl; i += ZTHREADS) {
+    soff[i] = g.line_off[l0 + i];
+    snneg[i] = g.line_nneg[l0 + i];
+    szneg[i] = g.line_zneg[l0 + i];
+    szpos[i] = g.line_zpos[l0 + i];
+  }
+  if (threadIdx.x == 0) soff[nl] = (l0 + nl < g.nlines) ? g.line_off[l0 + nl] : g.npts;
+  __syncthreads();
+  const int p0 = soff[0], p1 = soff[nl];
+  const double2* ps = psi + (size_t)s * g.npts;
+  for (int p = p0 + threadIdx.x; p < p1; p += ZTHREADS) {
+    int li, z;
+    locate(p, soff, nl, snneg, szneg, szpos, li, z);
+    double2 v = ps[p];
+    buf[li * LD + z] = mk<T>((T)v.x, (T)v.y);
+  }
+  __syncthreads();
+  fft_lines<T, N, ZEPT, ZTHREADS, false>(buf, LD, nl, tw);  // FFTW_FORWARD along z
+  cplx<T>* po = pen + (size_t)s * N * g.nlpad + l0;
+  for (int i = threadIdx.x; i < nl * N; i += ZTHREADS) {
+    int z = i / nl, li = i - z * nl;
+    po[(size_t)z * g.nlpad + li] = buf[li * LD + z];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// shared plane helpers.  plane is [nplane_x][N+1] (column kx holds y contiguous)
+
+template <typename T, int N>
+__device__ __forceinline__ void scatter_plane(const cplx<T>* __restrict__ prow, cplx<T>* plane,
+                                              const StateGeom& g) {
+  constexpr int LDY = N + 1;
+  for (int i = threadIdx.x; i < g.nplane_x * LDY; i += PTHREADS) plane[i] = mk<T>(0, 0);
+  __syncthreads();
+  for (int l = threadIdx.x; l < g.nlines; l += PTHREADS) {
+    int xy = __ldg(g.line_xy + l);
+    plane[(xy & 0xffff) * LDY + (xy >> 16)] = prow[l];
+  }
+  __syncthreads();
+}
+
+// Build npair complex rows Z = Xa + i Xb for the C2R of rows (ya, ya+1) from the
+// y-transformed plane, with the reference's imag flip (conj) applied, the
+// Hermitian extension to kx > N/2 and zero outside the nplane_x columns.
+template <typename T, int N>
+__device__ __forceinline__ void build_c2r_rows(const cplx<T>* plane, cplx<T>* rows, int nplx,
+                                               int ybase, int npair) {
+  constexpr int LDY = N + 1, LDX = N + 1;
+  for (int i = threadIdx.x; i < npair * N; i += PTHREADS) {
+    int pp = i / N, k = i - pp * N;
+    int ya = ybase + 2 * pp;
+    cplx<T> z;
+    if (k == 0) {
+      z = mk<T>(plane[ya].x, plane[ya + 1].x);
+    } else if (k < nplx) {
+      cplx<T> a = plane[k * LDY + ya], b = plane[k * LDY + ya + 1];
+      z = mk<T>(a.x + b.y, b.x - a.y);  // conj(a) + i conj(b)
+    } else if (N - k < nplx) {
+      int m = N - k;
+      cplx<T> a = plane[m * LDY + ya], b = plane[m * LDY + ya + 1];
+      z = mk<T>(a.x - b.y, a.y + b.x);  // a + i b
+    } else {
+      z = mk<T>(0, 0);
+    }
+    rows[pp * LDX + k] = z;
+  }
+}
+
+template <typename T, int N>
+struct PShape {
+  static constexpr int LDY = N + 1, LDX = N + 1;
+  static constexpr size_t LIMIT = 227 * 1024;
+  static constexpr size_t TW = sizeof(cplx<T>) * 2 * N;
+  // rows per chunk (pairs): register budget of the FFT and shared memory
+  static constexpr int rc_for(int nplx, bool with_v) {
+    int rc = std::min(N / 2, (PEPT * PTHREADS) / N);
+    while (rc > 1 && bytes(nplx, rc, with_v) > LIMIT) --rc;
+    return rc;
+  }
+  static constexpr size_t bytes(int nplx, int rc, bool with_v) {
+    return TW + sizeof(cplx<T>) * ((size_t)nplx * LDY + (size_t)rc * LDX) +
+           (with_v ? sizeof(T) * (size_t)N * N : 0);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// K2: planes -> psi(r); MODE 0 accumulates occ*psi^2 into per-group FP64
+// partial densities held in registers, MODE 1 writes psi(r) (FP64).
+template <typename T, int N, int MODE>
+__global__ void __launch_bounds__(PTHREADS, 1)
+k_xy_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict__ twx_g,
+         const double* __restrict__ occ, int nstates, int spg, int ysplit_rows, int RC,
+         double* __restrict__ out) {
+  constexpr int KM = Kmax<T>::v;
+  constexpr int LDY = N + 1, LDX = N + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* plane = tw + 2 * N;
+  cplx<T>* rows = plane + g.nplane_x * LDY;
+  const int z = blockIdx.x;
+  const int grp = blockIdx.y;
+  const int y0 = blockIdx.z * ysplit_rows;
+  const int nrows = min(ysplit_rows, N - y0);
+  const int s0 = grp * spg, s1 = min(nstates, s0 + spg);
+  for (int i = threadIdx.x; i < N; i += PTHREADS) tw[i] = twx_g[i];
+  double acc[KM];
+#pragma unroll
+  for (int k = 0; k < KM; ++k) acc[k] = 0.0;
+  __syncthreads();
+  for (int s = s0; s < s1; ++s) {
+    scatter_plane<T, N>(pen + ((size_t)s * N + z) * g.nlpad, plane, g);
+    fft_lines<T, N, PEPT, PTHREADS, false>(plane, LDY, g.nplane_x, tw);  // FFTW_FORWARD y
+    const double w = (MODE == 0) ? occ[s] : 1.0;
+    for (int r0 = 0; r0 < nrows; r0 += 2 * RC) {
+      const int npair = min(RC, (nrows - r0) / 2);
+      build_c2r_rows<T, N>(plane, rows, g.nplane_x, y0 + r0, npair);
+      __syncthreads();
+      fft_lines<T, N, PEPT, PTHREADS, true>(rows, LDX, npair, tw);  // C2R, +i sign
+      if (MODE == 0) {
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+          int pl = threadIdx.x + k * PTHREADS;
+          int r = pl / N;
+          if (r >= r0 && r < r0 + 2 * npair) {
+            int x = pl - r * N;
+            int rr = r - r0;
+            cplx<T> v = rows[(rr >> 1) * LDX + x];
+            double ps = (double)((rr & 1) ? v.y : v.x);
+            acc[k] += w * ps * ps;
+          }
+        }
+      } else {
+        for (int i = threadIdx.x; i < 2 * npair * N; i += PTHREADS) {
+          int rr = i / N, x = i - rr * N;
+          cplx<T> v = rows[(rr >> 1) * LDX + x];
+          out[(((size_t)s * N + z) * N + y0 + r0 + rr) * N + x] = (double)((rr & 1) ? v.y : v.x);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (MODE == 0) {
+    double* o = out + ((size_t)grp * N + z) * N * N + (size_t)y0 * N;
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+      int pl = threadIdx.x + k * PTHREADS;
+      if (pl < nrows * N) o[pl] = acc[k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K3: MODE 0: pencils -> psi(r) -> psi*V*occ -> planes -> pencils_out
+//     MODE 1: real f(r) (FP64, [s][z][y][x]) -> planes -> pencils_out
+template <typename T, int N, int MODE>
+__global__ void __launch_bounds__(PTHREADS, 1)
+k_xy_bwd(const cplx<T>* __restrict__ pen, const double* __restrict__ freal,
+         const T* __restrict__ vks, cplx<T>* __restrict__ pen_out, StateGeom g,
+         const cplx<T>* __restrict__ twx_g, const double* __restrict__ occ, int nstates, int spg,
+         int RC, int v_in_smem) {
+  constexpr int LDY = N + 1, LDX = N + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* plane = tw + 2 * N;
+  cplx<T>* rows = plane + g.nplane_x * LDY;
+  T* vs = reinterpret_cast<T*>(rows + RC * LDX);
+  const int z = blockIdx.x;
+  const int s0 = blockIdx.y * spg, s1 = min(nstates, s0 + spg);
+  for (int i = threadIdx.x; i < N; i += PTHREADS) tw[i] = twx_g[i];
+  const T* vplane = nullptr;
+  if (MODE == 0) {
+    vplane = vks + (size_t)z * N * N;
+    if (v_in_smem) {
+      for (int i = threadIdx.x; i < N * N; i += PTHREADS) vs[i] = vplane[i];
+      vplane = vs;
+    }
+  }
+  __syncthreads();
+  for (int s = s0; s < s1; ++s) {
+    if (MODE == 0) {
+      scatter_plane<T, N>(pen + ((size_t)s * N + z) * g.nlpad, plane, g);
+      fft_lines<T, N, PEPT, PTHREADS, false>(plane, LDY, g.nplane_x, tw);
+    }
+    const T w = (MODE == 0) ? (T)occ[s] : (T)1;
+    for (int r0 = 0; r0 < N; r0 += 2 * RC) {
+      const int npair = min(RC, (N - r0) / 2);
+      if (MODE == 0) {
+        build_c2r_rows<T, N>(plane, rows, g.nplane_x, r0, npair);
+        __syncthreads();
+        fft_lines<T, N, PEPT, PTHREADS, true>(rows, LDX, npair, tw);
+        for (int i = threadIdx.x; i < npair * N; i += PTHREADS) {
+          int pp = i / N, x = i - pp * N;
+          int ya = r0 + 2 * pp;
+          cplx<T> v = rows[pp * LDX + x];
+          v.x *= vplane[ya * N + x] * w;
+          v.y *= vplane[(ya + 1) * N + x] * w;
+          rows[pp * LDX + x] = v;
+        }
+      } else {
+        const double* fs = freal + ((size_t)s * N + z) * N * N;
+        for (int i = threadIdx.x; i < npair * N; i += PTHREADS) {
+          int pp = i / N, x = i - pp * N;
+          int ya = r0 + 2 * pp;
+          rows[pp * LDX + x] = mk<T>((T)fs[ya * N + x], (T)fs[(ya + 1) * N + x]);
+        }
+      }
+      __syncthreads();
+      fft_lines<T, N, PEPT, PTHREADS, false>(rows, LDX, npair, tw);  // R2C, -i sign
+      // split the two real rows' spectra, imag flip, keep kx < nplane_x
+      for (int i = threadIdx.x; i < npair * g.nplane_x; i += PTHREADS) {
+        int pp = i / g.nplane_x, k = i - pp * g.nplane_x;
+        int ya = r0 + 2 * pp;
+        cplx<T> zk = rows[pp * LDX + k];
+        cplx<T> zm = rows[pp * LDX + (k == 0 ? 0 : N - k)];
+        // A = (zk + conj zm)/2 ; B = (zk - conj zm)/(2i); stored conjugated
+        plane[k * LDY + ya] = mk<T>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zm.y - zk.y));
+        plane[k * LDY + ya + 1] = mk<T>((T)0.5 * (zk.y + zm.y), (T)0.5 * (zk.x - zm.x));
+      }
+      __syncthreads();
+    }
+    fft_lines<T, N, PEPT, PTHREADS, true>(plane, LDY, g.nplane_x, tw);  // FFTW_BACKWARD y
+    cplx<T>* po = pen_out + ((size_t)s * N + z) * g.nlpad;
+    for (int l = threadIdx.x; l < g.nlines; l += PTHREADS) {
+      int xy = __ldg(g.line_xy + l);
+      po[l] = plane[(xy & 0xffff) * LDY + (xy >> 16)];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K4: pencils -> backward z-FFT -> pack -> scale.
+//   MODE 0: F = scale * wpt * val (then, if occ != null, the kinetic term)
+//   MODE 1: plain pack with scale (adjoint transform)
+template <typename T, int N, int MODE>
+__global__ void __launch_bounds__(ZTHREADS)
+k_zfft_bwd(const cplx<T>* __restrict__ pen, double2* __restrict__ fout,
+           const double2* __restrict__ psi, const double* __restrict__ occ, StateGeom g,
+           const cplx<T>* __restrict__ twz, double scale, double ecut,
+           double* __restrict__ eke_part) {
+  constexpr int LB = ZShape<N>::LB, LD = ZShape<N>::LD;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[32];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* buf = tw + N;
+  int* soff = reinterpret_cast<int*>(buf + LB * LD);
+  int* snneg = soff + LB + 1;
+  int* szneg = snneg + LB;
+  int* szpos = szneg + LB;
+  const int s = blockIdx.y;
+  const int l0 = blockIdx.x * LB;
+  const int nl = min(LB, g.nlines - l0);
+  for (int i = threadIdx.x; i < N; i += ZTHREADS) tw[i] = twz[i];
+  for (int i = threadIdx.x; i < nl; i += ZTHREADS) {
+    soff[i] = g.line_off[l0 + i];
+    snneg[i] = g.line_nneg[l0 + i];
+    szneg[i] = g.line_zneg[l0 + i];
+    szpos[i] = g.line_zpos[l0 + i];
+  }
+  if (threadIdx.x == 0) soff[nl] = (l0 + nl < g.nlines) ? g.line_off[l0 + nl] : g.npts;
+  const cplx<T>* pi = pen + (size_t)s * N * g.nlpad + l0;
+  for (int i = threadIdx.x; i < nl * N; i += ZTHREADS) {
+    int z = i / nl, li = i - z * nl;
+    buf[li * LD + z] = pi[(size_t)z * g.nlpad + li];
+  }
+  __syncthreads();
+  fft_lines<T, N, ZEPT, ZTHREADS, true>(buf, LD, nl, tw);  // FFTW_BACKWARD along z
+  const int p0 = soff[0], p1 = soff[nl];
+  double e = 0.0;
+  const double wocc = (MODE == 0 && occ) ? occ[s] : 0.0;
+  for (int p = p0 + threadIdx.x; p < p1; p += ZTHREADS) {
+    int li, z;
+    locate(p, soff, nl, snneg, szneg, szpos, li, z);
+    cplx<T> v = buf[li * LD + z];
+    double fx = (double)v.x * scale, fy = (double)v.y * scale;
+    if (MODE == 0) {
+      double wp = g.wpt[p];
+      fx *= wp;
+      fy *= wp;
+      if (occ) {
+        double g2 = g.g2[p];
+        double2 ps = psi[(size_t)s * g.npts + p];
+        if (g2 <= ecut) {
+          double wt = wocc * wp * g2;
+          fx -= wt * ps.x;
+          fy -= wt * ps.y;
+          e += wt * (ps.x * ps.x + ps.y * ps.y);
+        } else {
+          fx = 0.0;
+          fy = 0.0;
+        }
+      }
+    }
+    fout[(size_t)s * g.npts + p] = make_double2(fx, fy);
+  }
+  if (MODE == 0 && occ) {
+    double t = block_sum(e, red);
+    if (threadIdx.x == 0) eke_part[(size_t)s * gridDim.x + blockIdx.x] = 0.5 * t;
+  }
+}
+
+// sum rho partials over groups, scale by 1/vol
+__global__ void k_rho_reduce(const double* __restrict__ part, int ngroups, size_t nr,
+                             double scale, double* __restrict__ rho);
+__global__ void k_rowsum(const double* __restrict__ part, int ncol, int nrow,
+                         double* __restrict__ out);
+__global__ void k_to_float(const double* __restrict__ in, float* __restrict__ out, size_t n);
+
+// ---------------------------------------------------------------------------
+// host side
+
+template <typename T>
+const Twiddles<T>& tws(const cpstep_ctx* c);
+template <>
+inline const Twiddles<double>& tws<double>(const cpstep_ctx* c) { return c->tw64; }
+template <>
+inline const Twiddles<float>& tws<float>(const cpstep_ctx* c) { return c->tw32; }
+
+template <typename K>
+int set_smem(K kernel, size_t smem) {
+  CPSTEP_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+  return CPSTEP_OK;
+}
+
+// state groups for the plane passes: aim at >= 3 waves of CTAs
+inline int plane_groups(const cpstep_ctx* c, int nstates, int other) {
+  int target = 3 * c->num_sms;
+  int per = c->nz * other;
+  int g = cdiv(target, per);
+  return std::max(1, std::min(nstates, g));
+}
+
+template <typename T, int N>
+struct StateFft {
+  static int zfft_fwd(cpstep_ctx* c, const double* psi, int nstates) {
+    dim3 grid(cdiv(c->nlines, ZShape<N>::LB), nstates);
+    const size_t smem = ZShape<N>::template bytes<T>();
+    if (int rc = set_smem(k_zfft_fwd<T, N>, smem)) return rc;
+    k_zfft_fwd<T, N><<<grid, ZTHREADS, smem, c->stream>>>(
+        reinterpret_cast<const double2*>(psi), reinterpret_cast<cplx<T>*>(c->d_pen_a), c->geom(),
+        tws<T>(c).z);
+    CPSTEP_LAUNCH_CHECK();
+    return CPSTEP_OK;
+  }
+
+  static int density(cpstep_ctx* c, const double* psi, const double* occ, double* rho) {
+    if (int rc = zfft_fwd(c, psi, c->nstates)) return rc;
+    const int RC = PShape<T, N>::rc_for(c->nplane_x, false);
+    const size_t smem = PShape<T, N>::bytes(c->nplane_x, RC, false);
+    int rows = std::min(N, (Kmax<T>::v * PTHREADS) / N) & ~1;
+    int ysplit = cdiv(N, rows);
+    int ng = std::min(c->ngroups_rho, plane_groups(c, c->nstates, ysplit));
+    int spg = cdiv(c->nstates, ng);
+    ng = cdiv(c->nstates, spg);
+    if (int rc = set_smem(k_xy_fwd<T, N, 0>, smem)) return rc;
+    k_xy_fwd<T, N, 0><<<dim3(N, ng, ysplit), PTHREADS, smem, c->stream>>>(
+        reinterpret_cast<const cplx<T>*>(c->d_pen_a), c->geom(), tws<T>(c).x, occ, c->nstates,
+        spg, rows, RC, c->d_rho_part);
+    CPSTEP_LAUNCH_CHECK();
+    size_t nr = (size_t)N * N * N;
+    k_rho_reduce<<<2 * c->num_sms, 256, 0, c->stream>>>(c->d_rho_part, ng, nr, 1.0 / c->vol, rho);
+    CPSTEP_LAUNCH_CHECK();
+    return CPSTEP_OK;
+  }
+
+  static int gtor(cpstep_ctx* c, const double* psi, double* psi_r, int nstates) {
+    if (int rc = zfft_fwd(c, psi, nstates)) return rc;
+    const int RC = PShape<T, N>::rc_for(c->nplane_x, false);
+    const size_t smem = PShape<T, N>::bytes(c->nplane_x, RC, false);
+    if (int rc = set_smem(k_xy_fwd<T, N, 1>, smem)) return rc;
+    k_xy_fwd<T, N, 1><<<dim3(N, nstates, 1), PTHREADS, smem, c->stream>>>(
+        reinterpret_cast<const cplx<T>*>(c->d_pen_a), c->geom(), tws<T>(c).x, nullptr, nstates,
+        1, N, RC, psi_r);
+    CPSTEP_LAUNCH_CHECK();
+    return CPSTEP_OK;
+  }
+
+  static int zfft_bwd(cpstep_ctx* c, double* out, const double* psi, const double* occ,
+                      int nstates, double scale, int mode) {
+    dim3 grid(cdiv(c->nlines, ZShape<N>::LB), nstates);
+    const size_t smem = ZShape<N>::template bytes<T>();
+    if (mode == 0) {
+      if (int rc = set_smem(k_zfft_bwd<T, N, 0>, smem)) return rc;
+      k_zfft_bwd<T, N, 0><<<grid, ZTHREADS, smem, c->stream>>>(
+          reinterpret_cast<const cplx<T>*>(c->d_pen_b), reinterpret_cast<double2*>(out),
+          reinterpret_cast<const double2*>(psi), occ, c->geom(), tws<T>(c).z, scale, c->ecut_ry,
+          c->d_eke_part);
+    } else {
+      if (int rc = set_smem(k_zfft_bwd<T, N, 1>, smem)) return rc;
+      k_zfft_bwd<T, N, 1><<<grid, ZTHREADS, smem, c->stream>>>(
+          reinterpret_cast<const cplx<T>*>(c->d_pen_b), reinterpret_cast<double2*>(out), nullptr,
+          nullptr, c->geom(), tws<T>(c).z, scale, 0.0, nullptr);
+    }
+    CPSTEP_LAUNCH_CHECK();
+    return CPSTEP_OK;
+  }
+
+  static int vpsi(cpstep_ctx* c, const double* psi, const double* vks, const double* occ,
+                  double* force, double* eke, int pencils_ready) {
+    size_t nr = (size_t)N * N * N;
+    if (!pencils_ready) {
+      if (int rc = zfft_fwd(c, psi, c->nstates)) return rc;
+    }
+    const T* vt;
+    if (sizeof(T) == sizeof(double)) {
+      vt = reinterpret_cast<const T*>(vks);
+    } else {
+      k_to_float<<<2 * c->num_sms, 256, 0, c->stream>>>(vks, reinterpret_cast<float*>(c->d_vks_t), nr);
+      CPSTEP_LAUNCH_CHECK();
+      vt = reinterpret_cast<const T*>(c->d_vks_t);
+    }
+    bool want_v = PShape<T, N>::bytes(c->nplane_x, 1, true) <= PShape<T, N>::LIMIT;
+    int RC = PShape<T, N>::rc_for(c->nplane_x, want_v);
+    size_t smem = PShape<T, N>::bytes(c->nplane_x, RC, want_v);
+    int ng = plane_groups(c, c->nstates, 1);
+    int spg = cdiv(c->nstates, ng);
+    ng = cdiv(c->nstates, spg);
+    if (int rc = set_smem(k_xy_bwd<T, N, 0>, smem)) return rc;
+    k_xy_bwd<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
+        reinterpret_cast<const cplx<T>*>(c->d_pen_a), nullptr, vt,
+        reinterpret_cast<cplx<T>*>(c->d_pen_b), c->geom(), tws<T>(c).x, occ, c->nstates, spg, RC,
+        want_v ? 1 : 0);
+    CPSTEP_LAUNCH_CHECK();
+    double scale = -2.0 / ((double)N * N * N);
+    if (int rc = zfft_bwd(c, force, psi, eke ? occ : nullptr, c->nstates, scale, 0)) return rc;
+    if (eke) {
+      int nblk = cdiv(c->nlines, ZShape<N>::LB);
+      k_rowsum<<<cdiv(c->nstates, 128), 128, 0, c->stream>>>(c->d_eke_part, nblk, c->nstates, eke);
+      CPSTEP_LAUNCH_CHECK();
+    }
+    return CPSTEP_OK;
+  }
+
+  static int rtog(cpstep_ctx* c, const double* f_r, double* fg, int nstates) {
+    const int RC = PShape<T, N>::rc_for(c->nplane_x, false);
+    const size_t smem = PShape<T, N>::bytes(c->nplane_x, RC, false);
+    if (int rc = set_smem(k_xy_bwd<T, N, 1>, smem)) return rc;
+    k_xy_bwd<T, N, 1><<<dim3(N, nstates), PTHREADS, smem, c->stream>>>(
+        nullptr, f_r, nullptr, reinterpret_cast<cplx<T>*>(c->d_pen_b), c->geom(), tws<T>(c).x,
+        nullptr, nstates, 1, RC, 0);
+    CPSTEP_LAUNCH_CHECK();
+    return zfft_bwd(c, fg, nullptr, nullptr, nstates, 1.0, 1);
+  }
+
+  static StateFftOps ops() {
+    StateFftOps o;
+    o.density = &density;
+    o.vpsi = &vpsi;
+    o.gtor = &gtor;
+    o.rtog = &rtog;
+    o.lb = ZShape<N>::LB;
+    return o;
+  }
+};
+
+}  // namespace sfft
+
+#define CPSTEP_INSTANTIATE_STATEFFT(N)                                         \
+  template <>                                                                  \
+  StateFftOps statefft_ops<double, N>() { return sfft::StateFft<double, N>::ops(); } \
+  template <>                                                                  \
+  StateFftOps statefft_ops<float, N>() { return sfft::StateFft<float, N>::ops(); }

@@ -1,0 +1,26 @@
+#!/bin/sh
+# Compile the reference leaves the oracle is pinned to, from their own
+# sources, into oracle/_ref/libref.so (git-ignored; it travels with the tree).
+#   src_charm_driver/utility/para_grp_parse.C   flip_data_set, get_chareG_line_prms
+#   src_mathlib/lst_sort_clean.C                sort_commence
+#   src_piny_physics_v1.0/abinito_physics/cp_orthog/cp_lowdin.C   get_iter_Tmat
+# The shims in oracle/ref_shim stand in for the Charm++/PINY headers, and
+# oracle/ref_mathlib.c for the Fortran GENMATMUL.  Test infrastructure only.
+set -e
+HERE=$(cd "$(dirname "$0")" && pwd)
+REF=${OPENATOM_REF:-/root/reference}
+OUT="$HERE/_ref"
+mkdir -p "$OUT"
+if [ ! -d "$REF/src_charm_driver" ]; then
+  echo "reference tree not found at $REF; keeping any prebuilt $OUT/libref.so" >&2
+  exit 0
+fi
+gcc -O2 -fPIC -c "$HERE/ref_mathlib.c" -o "$OUT/ref_mathlib.o"
+g++ -O2 -fPIC -shared -w -o "$OUT/libref.so" \
+  -I "$HERE/ref_shim" -I "$HERE/ref_shim/sub" -I "$REF" \
+  -I "$REF/src_charm_driver/utility" -I "$REF/src_piny_physics_v1.0/include/class_defs" \
+  "$REF/src_charm_driver/utility/para_grp_parse.C" \
+  "$REF/src_mathlib/lst_sort_clean.C" \
+  "$REF/src_piny_physics_v1.0/abinito_physics/cp_orthog/cp_lowdin.C" \
+  "$HERE/ref_driver.cpp" "$OUT/ref_mathlib.o"
+echo "$OUT/libref.so"

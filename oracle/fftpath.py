@@ -1,0 +1,115 @@
+"""Oracle: state FFTs, density and V_KS.psi in FP64, following the reference steps.
+
+TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).
+
+FFTW-2 sign conventions (``fftCache.C:252-255`` plans): FFTW_FORWARD is
+exp(-2 pi i jk/n), FFTW_BACKWARD exp(+2 pi i jk/n), both unnormalised;
+``rfftwnd`` COMPLEX_TO_REAL uses the +i sign and REAL_TO_COMPLEX the -i sign.
+
+* expand / pack            fftCache.C:460-553
+* G->R, G-chare (z)        doStpFFTGtoR_Gchare fftCache.C:1133-1159
+* transpose                CP_State_GSpacePlane.C:1473-1498 + CP_State_RealSpacePlane.C:248-268
+                           (line (x,y) goes to x + y*(nx/2+1) of plane z)
+* G->R, R-chare (y, x)     doStpFFTGtoR_Rchare fftCache.C:1167-1243 (imag flip :1209-1213)
+* density                  CP_State_RealSpacePlane.C:349-355 (occ*wkpt*psi^2),
+                           CP_Rho_RealSpacePlane.C:630-650 (x 1/vol)
+* V.psi                    CP_State_RealSpacePlane.C:580-587
+* R->G, R-chare (x, y)     doStpFFTRtoG_Rchare fftCache.C:1252-1319 (imag flip :1272-1274)
+* R->G, G-chare (z), pack  doStpFFTRtoG_Gchare fftCache.C:1099-1123
+* force scale              CP_State_GSpacePlane.C:1605-1612 (-2/(nx ny nz))
+* addForces                stateSlab.C:240-272 (x2 off the Gx=0 plane)
+* kinetic energy           CP_eke_calc cp_eke.C:30-140
+"""
+import numpy as np
+
+
+def expand(psi, lay):
+    """[S, npts] complex -> [S, nlines, n] complex z-lines (expandGSpace)."""
+    t = lay.line_tables()
+    S = psi.shape[0]
+    n = lay.n
+    out = np.zeros((S, lay.nlines, n), dtype=np.complex128)
+    for l in range(lay.nlines):
+        o, nn, npo = int(t['off'][l]), int(t['nneg'][l]), int(t['npos'][l])
+        zn, zp = int(t['zneg'][l]), int(t['zpos'][l])
+        out[:, l, zn:zn + nn] = psi[:, o:o + nn]
+        out[:, l, zp:zp + npo] = psi[:, o + nn:o + nn + npo]
+    return out
+
+
+def pack(lines, lay):
+    """[S, nlines, n] -> [S, npts] (packGSpace)."""
+    t = lay.line_tables()
+    S = lines.shape[0]
+    out = np.zeros((S, lay.npts), dtype=np.complex128)
+    for l in range(lay.nlines):
+        o, nn, npo = int(t['off'][l]), int(t['nneg'][l]), int(t['npos'][l])
+        zn, zp = int(t['zneg'][l]), int(t['zpos'][l])
+        out[:, o:o + nn] = lines[:, l, zn:zn + nn]
+        out[:, o + nn:o + nn + npo] = lines[:, l, zp:zp + npo]
+    return out
+
+
+def state_g_to_r(psi, lay):
+    """Packed psi(G) [S, npts] -> real psi(r) [S, nz, ny, nx] (FP64)."""
+    n = lay.n
+    t = lay.line_tables()
+    z = np.fft.fft(expand(psi, lay), axis=2)               # FFTW_FORWARD along z
+    S = psi.shape[0]
+    plane = np.zeros((S, n, n, n // 2 + 1), dtype=np.complex128)   # [s, z, y, x]
+    plane[:, :, t['y'], t['x']] = np.transpose(z, (0, 2, 1))
+    plane = np.fft.fft(plane, axis=2)                      # FFTW_FORWARD along y
+    plane = np.conj(plane)                                 # imag flip
+    return np.fft.irfft(plane, n=n, axis=3) * n            # rfftw C2R (+i, unnormalised)
+
+
+def state_r_to_g(f, lay):
+    """Real f(r) [S, nz, ny, nx] -> packed F(G) [S, npts], unscaled (FP64)."""
+    n = lay.n
+    t = lay.line_tables()
+    X = np.conj(np.fft.rfft(f, axis=3))                    # rfftw R2C (-i), imag flip
+    X = np.fft.ifft(X, axis=2) * n                         # FFTW_BACKWARD along y
+    lines = np.transpose(X[:, :, t['y'], t['x']], (0, 2, 1))   # [s, line, z]
+    lines = np.fft.ifft(lines, axis=2) * n                 # FFTW_BACKWARD along z
+    return pack(lines, lay)
+
+
+def density(psi, lay, occ, vol, chunk=16):
+    """rho(r) = sum_s occ_s psi_s(r)^2 / vol, [nz, ny, nx] FP64."""
+    n = lay.n
+    rho = np.zeros((n, n, n))
+    for s0 in range(0, psi.shape[0], chunk):
+        pr = state_g_to_r(psi[s0:s0 + chunk], lay)
+        rho += np.einsum('s,szyx->zyx', occ[s0:s0 + chunk], pr * pr)
+    return rho / vol
+
+
+def vpsi_force(psi, vks, lay, occ, chunk=16):
+    """F(G) = -2/N * FFT^-1[occ * V_KS * psi(r)]  (before addForces)."""
+    n = lay.n
+    out = np.zeros(psi.shape, dtype=np.complex128)
+    for s0 in range(0, psi.shape[0], chunk):
+        pr = state_g_to_r(psi[s0:s0 + chunk], lay)
+        f = pr * vks[None] * occ[s0:s0 + chunk, None, None, None]
+        out[s0:s0 + chunk] = state_r_to_g(f, lay) * (-2.0 / float(n * n * n))
+    return out
+
+
+def add_forces(force_vks, force_nl, lay):
+    """GStateSlab::addForces: x2 off the Gx=0 plane, then + non-local force."""
+    w = np.where(lay.kx == 0, 1.0, 2.0)
+    out = force_vks * w[None]
+    if force_nl is not None:
+        out = out + force_nl
+    return out
+
+
+def eke(force, psi, lay, occ, ecut_ry):
+    """CP_eke_calc: F -= w g^2 psi, E_kin = sum w g^2 |psi|^2 / 2 (cp_eke.C:77-125)."""
+    g2 = lay.g2
+    w = np.where(lay.kx == 0, 1.0, 2.0)
+    inside = g2 <= ecut_ry
+    wt = occ[:, None] * (w * g2)[None]
+    f = np.where(inside[None], force - psi * wt, 0.0)
+    e = 0.5 * np.sum(np.where(inside[None], wt * np.abs(psi) ** 2, 0.0), axis=1)
+    return f, e

@@ -1,0 +1,12 @@
+/* Minimal complex type with the members and operators the compiled reference
+ * leaves use (.re/.im, *, *=, +=, getMagSqr).  Test infrastructure only. */
+#pragma once
+struct complex {
+  double re, im;
+  complex() : re(0), im(0) {}
+  complex(double r, double i = 0.0) : re(r), im(i) {}
+  double getMagSqr() const { return re * re + im * im; }
+  complex& operator*=(double s) { re *= s; im *= s; return *this; }
+  complex& operator+=(const complex& o) { re += o.re; im += o.im; return *this; }
+  complex operator*(double s) const { return complex(re * s, im * s); }
+};
