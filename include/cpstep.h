@@ -39,6 +39,18 @@ extern "C" {
 #define CPSTEP_ERR_NOCONV 4   /* Ortho S->T iteration did not converge (ortho.C:129-133) */
 #define CPSTEP_ERR_STATE 5    /* call out of order */
 
+/* slots of the energies array (Hartree): the reference's Iter [n] names */
+#define CPSTEP_E_EXC 0     /* EEXC       (CP_exc_calc exc_ret)                */
+#define CPSTEP_E_MUXC 1    /* muxc       (CP_exc_calc muxc_ret)               */
+#define CPSTEP_E_HART 2    /* EHART      (CP_hart_eext_calc ehart_ret)        */
+#define CPSTEP_E_EXT 3     /* EExt       (CP_hart_eext_calc eext_ret)         */
+#define CPSTEP_E_EWD 4     /* reciprocal Ewald (CP_hart_eext_calc ewd_ret)    */
+#define CPSTEP_E_EXT_G0 5  /* reserved                                        */
+#define CPSTEP_E_KE 6      /* EKE        (sum of CP_eke_calc)                 */
+#define CPSTEP_E_NL 7      /* ENL        (EES non-local)                      */
+#define CPSTEP_E_TOT 8     /* ELEC_ENERGY_TOT = EKE+ENL+EHART+EExt+EEXC       */
+#define CPSTEP_NENERGY 12
+
 #define CPSTEP_PREC_FP64 0    /* plain FP64 path: the drop-in */
 #define CPSTEP_PREC_MIXED 1   /* FP32 FFT/density/V.psi, FP64 accumulation, split GEMMs */
 
@@ -151,6 +163,92 @@ CPSTEP_API int cpstep_vks_psi(cpstep_ctx* ctx, const double* d_psi, const double
  */
 CPSTEP_API int cpstep_eke(cpstep_ctx* ctx, double* d_force, const double* d_psi,
                const double* d_occ, double* d_eke);
+
+/* ---------------------------------------------------------------------------
+ * PairCalculator and Ortho.
+ *
+ * cpstep_pc_overlap: d_c(i,j) = alpha * sum_p wpt_p Re(conj a_i(p) b_j(p))
+ *   + beta * d_c(i,j), column-major with leading dimension ldc; a: [na][npts],
+ *   b: [nb][npts] packed complex, wpt = 1 on Gx=0 and 2 elsewhere.  With
+ *   alpha = 1 this is the reference's forward product: S = 2 psi_r^T psi_r
+ *   (symmetric) or lambda = 2 psi_r^T F_r (asymmetric) over the real view with
+ *   the Gx=0 rows scaled by 1/sqrt(2) (psi) and sqrt(2) (F)
+ *   (PairCalculator::multiplyForward, paircalc/ckPairCalculator.C:682-802;
+ *   scaling cp_state_ctrl/CP_State_GSpacePlane.C:1933-1954, :3120-3123).
+ *   Split over G with a fixed-order reduction: deterministic.
+ * cpstep_pc_backmultiply: out_i(p) = alpha * sum_{j<nin} M(j,i) in_j(p)
+ *   + beta * out_i(p) for i < nout, M column-major (ldm): the backward
+ *   products psi.T, F.T and psi.gamma (bwMultiplyHelper :1189-1425,
+ *   bwMultiplyDynOrthoT :1444-1510).  in/out: [n][npts] packed complex.
+ * cpstep_dgemm: column-major BLAS DGEMM semantics on device pointers, the
+ *   myGEMM wrapper (ckPairCalculator.C:57-66).
+ */
+CPSTEP_API int cpstep_pc_overlap(cpstep_ctx* ctx, const double* d_a, const double* d_b,
+                                 int na, int nb, double alpha, double beta, double* d_c,
+                                 int ldc);
+CPSTEP_API int cpstep_pc_backmultiply(cpstep_ctx* ctx, const double* d_m, int ldm,
+                                      const double* d_in, int nin, double* d_out, int nout,
+                                      double alpha, double beta);
+CPSTEP_API int cpstep_dgemm(cpstep_ctx* ctx, char transa, char transb, int m, int n, int k,
+                            double alpha, const double* d_a, int lda, const double* d_b,
+                            int ldb, double beta, double* d_c, int ldc);
+
+/*
+ * cpstep_ortho_tmat: T = (S/2)^(-1/2) for a symmetric n x n S (device FP64),
+ * CPORTHOG::get_iter_Tmat (src_piny_physics_v1.0/abinito_physics/cp_orthog/
+ * cp_lowdin.C:180-265) and the Ortho chare iteration (orthog_ctrl/ortho.C:
+ * 153-269, :862-985): A = I, B = S/2, C = 3I - A B, B <- B C / 2,
+ * A <- C A / 2 until rms(dA) <= tol or max_iter (reference: 1e-15, 10;
+ * ortho.h:86-87).  mode bit 0: FP32 iteration followed by an FP64
+ * correction that restores T^T (S/2) T = I to FP64 rounding; bit 1: scale
+ * by a Gershgorin bound of the spectrum first (converges for eig(S/2) >= 2,
+ * where the reference's iteration diverges).  Blocks the host until done.
+ * Returns CPSTEP_ERR_NOCONV (T still written) where the reference aborts.
+ * iters / rms (may be NULL) receive the iteration count and final rms.
+ */
+CPSTEP_API int cpstep_ortho_tmat(cpstep_ctx* ctx, const double* d_s, double* d_t, int n,
+                                 int mode, double tol, int max_iter, int* iters, double* rms);
+
+/* ---------------------------------------------------------------------------
+ * Density side: XC, density FFT, Hartree + local pseudopotential + Ewald.
+ *
+ * cpstep_set_atoms: atoms and local pseudopotential tables, the data
+ *   CP_hart_eext_calc reads from PINY (cp_local/cp_hart_ext.C:72-110):
+ *   typ[natm] (0-based type), pos[natm][3] (bohr), q[ntyp] (ionic charges),
+ *   spline tables vps[ntyp][4][nspl] = vps0..vps3 on g = gmin_spl + i*dg_spl
+ *   (cppseudo->vps0..3, CP_get_vpsnow :433-475), gzvps[ntyp] (the G=0 term)
+ *   and the Ewald alpha (genewald->alp_ewd).  Host pointers, copied.
+ * cpstep_rho_layout: the density sphere's packed order (|G|^2/2 <= 4 Ecut,
+ *   countkvec3d/setkvec3d set_cp_ewald.C:230-500, flip_data_set order):
+ *   npts, and kx/ky/kz (host, room for cap) when given.
+ * cpstep_exc_calc: CPXCFNCTS::CP_exc_calc (cp_xc_fnctl/cp_pz_lda.C:23-170) on
+ *   the dense [nz][ny][nx] grid: d_vxc = v_xc(r); d_energies[EXC], [MUXC].
+ * cpstep_rho_fft_r2g: rho(G) = (vol/N) sum_r rho(r) e^{-iG.r} on the packed
+ *   density sphere (CP_Rho_RealSpacePlane::fftRhoRtoRhoG, CP_Rho_RealSpacePlane.C:831-864).
+ * cpstep_hart_eext: CPLOCAL::CP_hart_eext_calc (cp_local/cp_hart_ext.C:56-405):
+ *   d_vksg = vks(G) (Hartree + local), d_energies[HART], [EXT], [EWD], and
+ *   when d_force is not NULL the local + Ewald atom forces [natm][3].
+ * cpstep_vks_fft_g2r: V(r) = sum_G vks(G) e^{+iG.r} (CP_Rho_GHartExt::FFTVks,
+ *   CP_Rho_GHartExt.C:532-540).
+ * cpstep_vks_from_rho: the chain CP_exc_calc -> fftRhoRtoRhoG -> CP_hart_eext_calc
+ *   -> FFTVks -> acceptHartVks (CP_Rho_RealSpacePlane.C:1365-1415):
+ *   d_vks_r = v_xc + V_H + V_loc on the grid, the five energies, forces.
+ * d_energies: device array of CPSTEP_NENERGY doubles; only the named slots are written.
+ */
+CPSTEP_API int cpstep_set_atoms(cpstep_ctx* ctx, int natm, int ntyp, const int* typ,
+                                const double* pos, const double* q, int nspl, double gmin_spl,
+                                double dg_spl, const double* vps, const double* gzvps,
+                                double alp_ewd);
+CPSTEP_API int cpstep_rho_layout(const cpstep_ctx* ctx, int cap, int* npts, int* kx, int* ky,
+                                 int* kz);
+CPSTEP_API int cpstep_exc_calc(cpstep_ctx* ctx, const double* d_rho, double* d_vxc,
+                               double* d_energies);
+CPSTEP_API int cpstep_rho_fft_r2g(cpstep_ctx* ctx, const double* d_rho_r, double* d_rhog);
+CPSTEP_API int cpstep_hart_eext(cpstep_ctx* ctx, const double* d_rhog, double* d_vksg,
+                                double* d_energies, double* d_force);
+CPSTEP_API int cpstep_vks_fft_g2r(cpstep_ctx* ctx, const double* d_vksg, double* d_v_r);
+CPSTEP_API int cpstep_vks_from_rho(cpstep_ctx* ctx, const double* d_rho_r, double* d_vks_r,
+                                   double* d_energies, double* d_force);
 
 #ifdef __cplusplus
 }

@@ -47,7 +47,29 @@ SIGNATURES = {
     "cpstep_density": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "cpstep_vks_psi": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "cpstep_eke": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cpstep_pc_overlap": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int]),
+    "cpstep_pc_backmultiply": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                              ctypes.c_int, ctypes.c_double, ctypes.c_double]),
+    "cpstep_dgemm": (ctypes.c_int, [_vp, ctypes.c_char, ctypes.c_char, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp,
+                                    ctypes.c_int, _vp, ctypes.c_int, ctypes.c_double, _vp,
+                                    ctypes.c_int]),
+    "cpstep_ortho_tmat": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_double, ctypes.c_int, _c_int_p, _c_dbl_p]),
+    "cpstep_set_atoms": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _c_int_p, _c_dbl_p,
+                                        _c_dbl_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        _c_dbl_p, _c_dbl_p, ctypes.c_double]),
+    "cpstep_rho_layout": (ctypes.c_int, [_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p,
+                                         _c_int_p]),
+    "cpstep_exc_calc": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "cpstep_rho_fft_r2g": (ctypes.c_int, [_vp, _vp, _vp]),
+    "cpstep_hart_eext": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cpstep_vks_fft_g2r": (ctypes.c_int, [_vp, _vp, _vp]),
+    "cpstep_vks_from_rho": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
 }
+NENERGY = 12
+E_EXC, E_MUXC, E_HART, E_EXT, E_EWD, E_EXT_G0, E_KE, E_NL, E_TOT = range(9)
 
 
 class CpstepError(RuntimeError):

@@ -128,3 +128,114 @@ class StepContext:
         e = torch.empty(self.nstates, dtype=torch.float64, device=self.device)
         _lib.call("cpstep_eke", self._h, ptr(force), ptr(psi), ptr(occ), ptr(e))
         return e
+
+    # -- PairCalculator / Ortho ---------------------------------------------
+    def pc_overlap(self, a, b, alpha=1.0, beta=0.0, out=None):
+        """S or lambda: out(i,j) = alpha sum_p wpt Re(conj a_i b_j) + beta out (col-major)."""
+        self._sync_stream()
+        na, nb = a.shape[0], b.shape[0]
+        if out is None:
+            out = torch.zeros((nb, na), dtype=torch.float64, device=self.device)  # col-major (na x nb)
+        _lib.call("cpstep_pc_overlap", self._h, ptr(a), ptr(b), na, nb, float(alpha), float(beta),
+                  ptr(out), na)
+        return out
+
+    def pc_backmultiply(self, m_colmajor, x, nout=None, alpha=1.0, beta=0.0, out=None):
+        """out_i = alpha sum_j M(j,i) x_j + beta out_i  (psi.T, psi.gamma, F.T)."""
+        self._sync_stream()
+        nin = x.shape[0]
+        nout = nin if nout is None else nout
+        if out is None:
+            out = torch.zeros((nout, self.layout.npts), dtype=torch.complex128, device=self.device)
+        ldm = m_colmajor.shape[1]  # tensor [ncols][ld] holds a column-major matrix
+        _lib.call("cpstep_pc_backmultiply", self._h, ptr(m_colmajor), ldm, ptr(x), nin, ptr(out),
+                  nout, float(alpha), float(beta))
+        return out
+
+    def ortho_tmat(self, S, mixed=False, scale=False, tol=1e-15, max_iter=10):
+        """T = (S/2)^(-1/2) (CPORTHOG::get_iter_Tmat); returns (T, iterations, rms)."""
+        self._sync_stream()
+        n = S.shape[0]
+        T = torch.empty_like(S)
+        it, rms = ctypes.c_int(), ctypes.c_double()
+        mode = (1 if mixed else 0) | (2 if scale else 0)
+        _lib.call("cpstep_ortho_tmat", self._h, ptr(S.contiguous()), ptr(T), n, mode, float(tol),
+                  int(max_iter), ctypes.byref(it), ctypes.byref(rms))
+        return T, it.value, rms.value
+
+    def dgemm(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+        """Column-major DGEMM on device tensors (the myGEMM wrapper)."""
+        self._sync_stream()
+        _lib.call("cpstep_dgemm", self._h, transa.encode(), transb.encode(), m, n, k,
+                  float(alpha), ptr(A), lda, ptr(B), ldb, float(beta), ptr(C), ldc)
+        return C
+
+    # -- density side --------------------------------------------------------
+    def set_atoms(self, system):
+        """Atoms + local pseudopotential tables (the PINY data CP_hart_eext_calc reads)."""
+        import numpy as np
+        tab = system.tab
+        typ, ptyp = _lib.int_array(system.typ)
+        pos = np.ascontiguousarray(system.pos, dtype=np.float64)
+        q = np.ascontiguousarray(tab["q"], dtype=np.float64)
+        vps = np.ascontiguousarray(tab["vps"], dtype=np.float64)
+        gz = np.ascontiguousarray(tab["gzvps"], dtype=np.float64)
+        dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        self._sync_stream()
+        _lib.call("cpstep_set_atoms", self._h, len(system.typ), len(tab["q"]), ptyp, dp(pos),
+                  dp(q), int(tab["nspl"]), float(tab["gmin"]), float(tab["dg"]), dp(vps), dp(gz),
+                  float(system.alp_ewd))
+        self.natm = len(system.typ)
+
+    def rho_layout(self):
+        import numpy as np
+        n = ctypes.c_int()
+        _lib.call("cpstep_rho_layout", self._h, 0, ctypes.byref(n), None, None, None)
+        kx = np.zeros(n.value, np.int32)
+        ky = np.zeros(n.value, np.int32)
+        kz = np.zeros(n.value, np.int32)
+        ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        _lib.call("cpstep_rho_layout", self._h, n.value, ctypes.byref(n), ip(kx), ip(ky), ip(kz))
+        return kx, ky, kz
+
+    def _energies(self):
+        return torch.zeros(_lib.NENERGY, dtype=torch.float64, device=self.device)
+
+    def exc(self, rho):
+        """CP_exc_calc: (v_xc(r), energies with EXC/MUXC)."""
+        self._sync_stream()
+        v = torch.empty_like(rho)
+        e = self._energies()
+        _lib.call("cpstep_exc_calc", self._h, ptr(rho), ptr(v), ptr(e))
+        return v, e
+
+    def rho_r2g(self, rho):
+        self._sync_stream()
+        n = self.rho_layout()[0].shape[0]
+        out = torch.empty(n, dtype=torch.complex128, device=self.device)
+        _lib.call("cpstep_rho_fft_r2g", self._h, ptr(rho), ptr(out))
+        return out
+
+    def hart_eext(self, rhog, forces=True):
+        """CP_hart_eext_calc: (vks(G), energies HART/EXT/EWD, forces [natm,3])."""
+        self._sync_stream()
+        v = torch.empty_like(rhog)
+        e = self._energies()
+        f = torch.zeros((self.natm, 3), dtype=torch.float64, device=self.device) if forces else None
+        _lib.call("cpstep_hart_eext", self._h, ptr(rhog), ptr(v), ptr(e), ptr(f))
+        return v, e, f
+
+    def vks_g2r(self, vksg):
+        self._sync_stream()
+        out = torch.empty((self.n, self.n, self.n), dtype=torch.float64, device=self.device)
+        _lib.call("cpstep_vks_fft_g2r", self._h, ptr(vksg), ptr(out))
+        return out
+
+    def vks_from_rho(self, rho, forces=True):
+        """XC -> rho(G) -> Hartree/local/Ewald -> V_KS(r); returns (vks, energies, forces)."""
+        self._sync_stream()
+        v = torch.empty_like(rho)
+        e = self._energies()
+        f = torch.zeros((self.natm, 3), dtype=torch.float64, device=self.device) if forces else None
+        _lib.call("cpstep_vks_from_rho", self._h, ptr(rho), ptr(v), ptr(e), ptr(f))
+        return v, e, f

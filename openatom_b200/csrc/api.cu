@@ -17,12 +17,6 @@ void cpstep_set_error(const char* fmt, ...) {
   va_end(ap);
 }
 
-// defined in statefft.cu
-int statefft_density(cpstep_ctx* c, const double* psi, const double* occ, double* rho);
-int statefft_vpsi(cpstep_ctx* c, const double* psi, const double* vks, const double* occ,
-                  double* force, double* eke, int pencils_ready);
-int statefft_gtor(cpstep_ctx* c, const double* psi, double* psi_r, int nstates);
-int statefft_rtog(cpstep_ctx* c, const double* f_r, double* fg, int nstates);
 
 namespace {
 
@@ -211,6 +205,7 @@ int cpstep_ctx_create(cpstep_ctx** out, int precision, int nstates, int npts, co
   if (!rc) rc = upload(&c->d_g2, g2.data(), npts);
   if (!rc) rc = upload(&c->d_wpt, wpt.data(), npts);
   if (!rc) rc = statefft_init(c);
+  if (!rc) rc = rho_init(c, std::fabs(hmat[0]), ecut_ry);
   if (rc) {
     cpstep_ctx_destroy(c);
     return rc;
@@ -225,6 +220,8 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
   cudaFree(c->d_line_zneg); cudaFree(c->d_line_zpos); cudaFree(c->d_line_xy);
   cudaFree(c->d_kx); cudaFree(c->d_ky); cudaFree(c->d_kz);
   cudaFree(c->d_g2); cudaFree(c->d_wpt);
+  cudaFree(c->d_pc_part); cudaFree(c->d_ortho_ws); cudaFree(c->d_hmati);
+  rho_free(c);
   statefft_free(c);
   delete c;
   return CPSTEP_OK;
@@ -300,6 +297,92 @@ int cpstep_eke(cpstep_ctx* c, double* d_force, const double* d_psi, const double
   k_rowsum2<<<cdiv(c->nstates, 128), 128, 0, c->stream>>>(c->d_eke_part, nb, c->nstates, d_eke);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
+}
+
+int cpstep_pc_overlap(cpstep_ctx* c, const double* d_a, const double* d_b, int na, int nb,
+                      double alpha, double beta, double* d_c, int ldc) {
+  if (!c || !d_a || !d_b || !d_c || na <= 0 || nb <= 0 || ldc < na) return CPSTEP_ERR_ARG;
+  return pc_overlap_launch(c, d_a, d_b, na, nb, 2 * c->npts, c->d_wpt, alpha, beta, d_c, ldc);
+}
+
+int cpstep_pc_backmultiply(cpstep_ctx* c, const double* d_m, int ldm, const double* d_in,
+                           int nin, double* d_out, int nout, double alpha, double beta) {
+  if (!c || !d_m || !d_in || !d_out || nin <= 0 || nout <= 0 || ldm < nin) return CPSTEP_ERR_ARG;
+  const int K = 2 * c->npts;
+  return pc_backmul_launch(c, d_m, ldm, d_in, K, d_out, K, nout, nin, K, alpha, beta);
+}
+
+int cpstep_dgemm(cpstep_ctx* c, char transa, char transb, int m, int n, int k, double alpha,
+                 const double* d_a, int lda, const double* d_b, int ldb, double beta, double* d_c,
+                 int ldc) {
+  if (!c || !d_a || !d_b || !d_c || m < 0 || n < 0 || k < 0) return CPSTEP_ERR_ARG;
+  int ta = (transa == 'T' || transa == 't' || transa == 'C' || transa == 'c');
+  int tb = (transb == 'T' || transb == 't' || transb == 'C' || transb == 'c');
+  if (lda < (ta ? k : m) || ldb < (tb ? n : k) || ldc < m) return CPSTEP_ERR_ARG;
+  if (m == 0 || n == 0) return CPSTEP_OK;
+  return dgemm_launch(c->stream, ta, tb, m, n, k, alpha, d_a, lda, d_b, ldb, beta, d_c, ldc);
+}
+
+int cpstep_ortho_tmat(cpstep_ctx* c, const double* d_s, double* d_t, int n, int mode,
+                      double tol, int max_iter, int* iters, double* rms) {
+  if (!c || !d_s || !d_t || n <= 0 || max_iter <= 0 || mode < 0 || mode > 3) return CPSTEP_ERR_ARG;
+  return ortho_tmat(c, d_s, d_t, n, mode & 1, (mode >> 1) & 1, tol, max_iter, iters, rms, 1);
+}
+
+int cpstep_set_atoms(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* pos,
+                     const double* q, int nspl, double gmin_spl, double dg_spl,
+                     const double* vps, const double* gzvps, double alp_ewd) {
+  if (!c || natm <= 0 || ntyp <= 0 || !typ || !pos || !q || nspl <= 1 || !(dg_spl > 0) || !vps ||
+      !gzvps || !(alp_ewd > 0))
+    return CPSTEP_ERR_ARG;
+  return atoms_set(c, natm, ntyp, typ, pos, q, nspl, gmin_spl, dg_spl, vps, gzvps, alp_ewd);
+}
+
+int cpstep_rho_layout(const cpstep_ctx* c, int cap, int* npts, int* kx, int* ky, int* kz) {
+  if (!c || !npts) return CPSTEP_ERR_ARG;
+  *npts = c->rg.npts;
+  if (!kx || !ky || !kz) return CPSTEP_OK;
+  if (cap < c->rg.npts) return CPSTEP_ERR_ARG;
+  CPSTEP_CUDA_TRY(cudaMemcpy(kx, c->rg.kx, sizeof(int) * c->rg.npts, cudaMemcpyDeviceToHost));
+  CPSTEP_CUDA_TRY(cudaMemcpy(ky, c->rg.ky, sizeof(int) * c->rg.npts, cudaMemcpyDeviceToHost));
+  CPSTEP_CUDA_TRY(cudaMemcpy(kz, c->rg.kz, sizeof(int) * c->rg.npts, cudaMemcpyDeviceToHost));
+  return CPSTEP_OK;
+}
+
+int cpstep_exc_calc(cpstep_ctx* c, const double* d_rho, double* d_vxc, double* d_energies) {
+  if (!c || !d_rho || !d_vxc || !d_energies) return CPSTEP_ERR_ARG;
+  return rho_xc(c, d_rho, d_vxc, d_energies);
+}
+
+int cpstep_rho_fft_r2g(cpstep_ctx* c, const double* d_rho_r, double* d_rhog) {
+  if (!c || !d_rho_r || !d_rhog) return CPSTEP_ERR_ARG;
+  if (int rc = rho_r2g(c, d_rho_r)) return rc;
+  return rho_conj_scale(c, reinterpret_cast<const double*>(c->rg.rhog), d_rhog, c->rg.npts, 1.0);
+}
+
+int cpstep_hart_eext(cpstep_ctx* c, const double* d_rhog, double* d_vksg, double* d_energies,
+                     double* d_force) {
+  if (!c || !d_rhog || !d_vksg || !d_energies) return CPSTEP_ERR_ARG;
+  if (int rc = rho_conj_scale(c, d_rhog, reinterpret_cast<double*>(c->rg.rhog), c->rg.npts, 1.0))
+    return rc;
+  if (int rc = rho_hart(c, d_energies, d_force)) return rc;
+  return rho_conj_scale(c, reinterpret_cast<const double*>(c->rg.vg), d_vksg, c->rg.npts, 1.0);
+}
+
+int cpstep_vks_fft_g2r(cpstep_ctx* c, const double* d_vksg, double* d_v_r) {
+  if (!c || !d_vksg || !d_v_r) return CPSTEP_ERR_ARG;
+  if (int rc = rho_conj_scale(c, d_vksg, reinterpret_cast<double*>(c->rg.vg), c->rg.npts, 1.0))
+    return rc;
+  return c->ops64.g2r(c, rho_job(c), reinterpret_cast<const double*>(c->rg.vg), d_v_r, 1);
+}
+
+int cpstep_vks_from_rho(cpstep_ctx* c, const double* d_rho_r, double* d_vks_r,
+                        double* d_energies, double* d_force) {
+  if (!c || !d_rho_r || !d_vks_r || !d_energies) return CPSTEP_ERR_ARG;
+  if (int rc = rho_xc(c, d_rho_r, d_vks_r, d_energies)) return rc;
+  if (int rc = rho_r2g(c, d_rho_r)) return rc;
+  if (int rc = rho_hart(c, d_energies, d_force)) return rc;
+  return rho_vks_r(c, d_vks_r);
 }
 
 }  // extern "C"

@@ -20,16 +20,52 @@ struct StateGeom {
 
 struct cpstep_ctx;
 
-// Per-grid-size state FFT entry points (compile-time N inside).
+// One FFT geometry with its pencil buffers (state sphere or density sphere).
+struct FftJob {
+  StateGeom g;
+  void* pen_a;  // [nstates][nz][nlpad] pencils of the G->R pass
+  void* pen_b;  // [nstates][nz][nlpad] pencils of the R->G pass
+};
+
+// Per-grid-size FFT entry points (compile-time N inside).
 struct StateFftOps {
   int (*density)(cpstep_ctx*, const double*, const double*, double*);
   int (*vpsi)(cpstep_ctx*, const double*, const double*, const double*, double*, double*, int);
   int (*gtor)(cpstep_ctx*, const double*, double*, int);
   int (*rtog)(cpstep_ctx*, const double*, double*, int);
+  int (*g2r)(cpstep_ctx*, const FftJob&, const double*, double*, int);
+  int (*r2g)(cpstep_ctx*, const FftJob&, const double*, double*, int, double);
   int lb;  // z-lines per block of the z-passes
 };
 template <typename T, int N>
 StateFftOps statefft_ops();
+
+// Density sphere geometry and buffers (FP64 in both precision modes).
+struct RhoGeom {
+  int npts = 0, nlines = 0, nlpad = 0, nplane_x = 0;
+  int *line_off = nullptr, *line_nneg = nullptr, *line_npos = nullptr;
+  int *line_zneg = nullptr, *line_zpos = nullptr, *line_xy = nullptr;
+  int *kx = nullptr, *ky = nullptr, *kz = nullptr;
+  double *g2 = nullptr, *wpt = nullptr;
+  void *pen_a = nullptr, *pen_b = nullptr;
+  double2* rhog = nullptr;   // transformed density (conj of the reference rho(G))
+  double2* vg = nullptr;     // conj of the reference vks(G)
+  double4* fterm = nullptr;  // per-point force terms of CP_hart_eext_calc
+  double* vhl = nullptr;     // Hartree + local potential on the grid
+  double* part = nullptr;    // reduction partials
+  int nblk_xc = 0, nblk_h = 0;
+};
+
+// Atoms, pseudopotential spline tables and structure-factor phase tables.
+struct AtomData {
+  int natm = 0, ntyp = 0, nspl = 0;
+  double gmin = 0, dg = 0, alp_ewd = 0;
+  int* typ = nullptr;
+  double *frac = nullptr, *q = nullptr, *vps = nullptr, *gzvps = nullptr;
+  int kxm = 0, kym = 0, kzm = 0;
+  double2 *ex = nullptr, *ey = nullptr, *ez = nullptr;
+  double* fpart = nullptr;
+};
 
 template <typename T>
 struct Twiddles {
@@ -59,7 +95,13 @@ struct cpstep_ctx {
   std::vector<int> h_kx, h_ky, h_kz;
   std::vector<int> h_line_xy, h_line_off;
 
-  StateFftOps ops;
+  StateFftOps ops;    // working precision
+  StateFftOps ops64;  // FP64 (density path)
+  RhoGeom rg;
+  AtomData atoms;
+  int rho_izero = -1;
+  double* d_energies = nullptr;  // [CPSTEP_NENERGY]
+  double* d_hmati = nullptr;
   Twiddles<double> tw64;
   Twiddles<float> tw32;
 
@@ -72,6 +114,21 @@ struct cpstep_ctx {
   double* d_eke_part;    // [nstates][nblk_z]
   int nblk_z;
   double* d_red;         // small reduction scratch
+
+  // PairCalculator / Ortho scratch (grown on demand)
+  double* d_pc_part = nullptr;
+  size_t pc_part_elems = 0;
+  double* d_ortho_ws = nullptr;
+  size_t ortho_ws_elems = 0;
+  int* d_ortho_status = nullptr;  // [iterations, converged] of the last Ortho launch
+
+  FftJob state_job() const {
+    FftJob j;
+    j.g = geom();
+    j.pen_a = d_pen_a;
+    j.pen_b = d_pen_b;
+    return j;
+  }
 
   StateGeom geom() const {
     StateGeom g;
@@ -87,3 +144,34 @@ struct cpstep_ctx {
 // statefft.cu
 int statefft_init(cpstep_ctx* c);
 void statefft_free(cpstep_ctx* c);
+int statefft_density(cpstep_ctx* c, const double* psi, const double* occ, double* rho);
+int statefft_vpsi(cpstep_ctx* c, const double* psi, const double* vks, const double* occ,
+                  double* force, double* eke, int pencils_ready);
+int statefft_gtor(cpstep_ctx* c, const double* psi, double* psi_r, int nstates);
+int statefft_rtog(cpstep_ctx* c, const double* f_r, double* fg, int nstates);
+
+// rhopath.cu
+int rho_init(cpstep_ctx* c, double box_len, double ecut_ry);
+void rho_free(cpstep_ctx* c);
+FftJob rho_job(const cpstep_ctx* c);
+int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* pos,
+              const double* q, int nspl, double gmin, double dg, const double* vps,
+              const double* gzvps, double alp_ewd);
+int rho_xc(cpstep_ctx* c, const double* rho_r, double* vxc, double* energies);
+int rho_r2g(cpstep_ctx* c, const double* rho_r);
+int rho_hart(cpstep_ctx* c, double* energies, double* force);
+int rho_vks_r(cpstep_ctx* c, double* vks_r);
+int rho_conj_scale(cpstep_ctx* c, const double* in, double* out, int n, double s);
+
+// paircalc.cu
+int pc_overlap_launch(cpstep_ctx* c, const double* a, const double* b, int M, int N, int K,
+                      const double* w, double alpha, double beta, double* C, int ldc);
+int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
+                      double* out, int ldo, int nout, int nin, int K, double alpha, double beta);
+int dgemm_launch(cudaStream_t s, int ta, int tb, int m, int n, int k, double alpha,
+                 const double* A, int lda, const double* B, int ldb, double beta, double* C,
+                 int ldc);
+
+// ortho.cu
+int ortho_tmat(cpstep_ctx* c, const double* S, double* T, int n, int mixed, int scale,
+               double tol, int max_iter, int* iters_out, double* rms_out, int check_host);

@@ -298,3 +298,29 @@ extern "C" int cpstep_layout_build(double box_len, double ecut_ry, int nchareG, 
   }
   return CPSTEP_OK;
 }
+
+// Density sphere |G|^2/2 <= 4 ecut_Ha (countkvec3d/setkvec3d, set_cp_ewald.C:230-500,
+// with the kmaxv = 2 kmax_cp loop bounds of calc_cutoff :205-207), in flip_data_set
+// order as one chunk: its z-lines are already contiguous and (kx, ky)-sorted.
+int cpstep_density_layout(double box_len, double ecut_ry, int nfft, std::vector<int>& kx,
+                          std::vector<int>& ky, std::vector<int>& kz, std::vector<int>& runs) {
+  int km = kmax_of(box_len, ecut_ry);
+  std::vector<K3> hs = half_sphere(box_len, 2.0 * ecut_ry, 2 * km), fl;
+  if (!flip(hs, fl)) return CPSTEP_ERR_LAYOUT;
+  int kxmax = 0, kymax = 0, kzmax = 0;
+  for (const K3& k : fl) {
+    kxmax = std::max(kxmax, std::abs(k.a));
+    kymax = std::max(kymax, std::abs(k.b));
+    kzmax = std::max(kzmax, std::abs(k.c));
+  }
+  if (2 * kxmax + 2 > nfft || 2 * kymax + 1 > nfft || 2 * kzmax + 1 > nfft) return CPSTEP_ERR_ARG;
+  kx.resize(fl.size());
+  ky.resize(fl.size());
+  kz.resize(fl.size());
+  for (size_t i = 0; i < fl.size(); ++i) {
+    kx[i] = fl[i].a;
+    ky[i] = fl[i].b;
+    kz[i] = fl[i].c;
+  }
+  return make_runs(fl, nfft, nfft, nfft, runs) ? CPSTEP_OK : CPSTEP_ERR_LAYOUT;
+}

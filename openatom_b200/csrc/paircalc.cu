@@ -1,0 +1,238 @@
+// PairCalculator products (SIMT path).
+//
+//   overlap:      C(i,j) = alpha * sum_p wpt_p Re(conj a_i(p) b_j(p)) (+ beta C)
+//                 = the reference's 2 * psi_r^T psi_r with Gx=0 rows scaled by
+//                 1/sqrt(2) (ckPairCalculator.C:682-751, multiplyForward 'T','N'
+//                 with alpha = 2 for double pack; scaling CP_State_GSpacePlane.C:
+//                 1933-1954, :3120-3123).  C is column-major (ld = ldc).
+//   backmultiply: out_i(p) = alpha * sum_j M(j,i) in_j(p) + beta * out_i(p),
+//                 M column-major: psi.T ('N','N', ckPairCalculator.C:1314) and
+//                 the gamma / lambda products (:1358, :1408, :1497).
+//   dgemm:        column-major BLAS semantics, the myGEMM wrapper
+//                 (ckPairCalculator.C:57-66).
+//
+// All three run on FP64 SIMT tiles; the overlap is split over K (the
+// reference's numChunks K-split, pcCommManager.C:165-172) with a fixed-order
+// reduction of the partial tiles, so results are deterministic.
+#include <algorithm>
+#include "ctx.cuh"
+
+namespace pcalc {
+
+constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
+
+// C_part[ks] (BM x BN tiles, column-major, ld = M) for the K-slab of split ks.
+// A: [M][K] row-major (lda), B: [N][K] row-major (ldb), K counted in reals;
+// w (per complex point) multiplies column k by w[k/2] when non-null.
+__global__ void __launch_bounds__(NT)
+k_overlap_part(const double* __restrict__ A, int lda, const double* __restrict__ B, int ldb,
+               const double* __restrict__ w, int M, int N, int K, int kslab,
+               double* __restrict__ part) {
+  __shared__ double As[BK][BM + 1];
+  __shared__ double Bs[BK][BN + 1];
+  const int i0 = blockIdx.x * BM, j0 = blockIdx.y * BN, ks = blockIdx.z;
+  const int kbeg = ks * kslab, kend = min(K, kbeg + kslab);
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4] = {};
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    for (int e = threadIdx.x; e < BM * BK; e += NT) {
+      int r = e / BK, c = e % BK;
+      int k = k0 + c;
+      double av = 0.0, bv = 0.0;
+      if (k < kend) {
+        if (i0 + r < M) {
+          av = A[(size_t)(i0 + r) * lda + k];
+          if (w) av *= w[k >> 1];
+        }
+        if (j0 + r < N) bv = B[(size_t)(j0 + r) * ldb + k];
+      }
+      As[c][r] = av;
+      Bs[c][r] = bv;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = As[kk][ty + 16 * q];
+        b[q] = Bs[kk][tx + 16 * q];
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[q][r] += a[q] * b[r];
+    }
+    __syncthreads();
+  }
+  double* P = part + (size_t)ks * M * N;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      int i = i0 + ty + 16 * q, j = j0 + tx + 16 * r;
+      if (i < M && j < N) P[(size_t)j * M + i] = acc[q][r];
+    }
+}
+
+__global__ void k_splitk_reduce(const double* __restrict__ part, int nsplit, int M, int N,
+                                double alpha, double beta, double* __restrict__ C, int ldc) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= M * N) return;
+  int j = e / M, i = e - j * M;
+  double s = 0.0;
+  for (int k = 0; k < nsplit; ++k) s += part[(size_t)k * M * N + e];
+  double* c = C + (size_t)j * ldc + i;
+  *c = alpha * s + (beta == 0.0 ? 0.0 : beta * (*c));
+}
+
+// out[i][p] = alpha * sum_j Mcm[j + i*ldm] * in[j][p] + beta * out[i][p]
+// (i < nout, j < nin, p < K; in/out row-major with ld = ldi / ldo)
+__global__ void __launch_bounds__(NT)
+k_backmul(const double* __restrict__ Mcm, int ldm, const double* __restrict__ in, int ldi,
+          double* __restrict__ out, int ldo, int nout, int nin, int K, double alpha,
+          double beta) {
+  __shared__ double Ms[BK][BM + 1];
+  __shared__ double Is[BK][BN + 1];
+  const int p0 = blockIdx.x * BN, i0 = blockIdx.y * BM;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4] = {};
+  for (int j0 = 0; j0 < nin; j0 += BK) {
+    for (int e = threadIdx.x; e < BM * BK; e += NT) {
+      int r = e / BK, c = e % BK;  // M tile: row i0+r, col j0+c -> Mcm[j + i ldm]
+      int i = i0 + r, j = j0 + c;
+      Ms[c][r] = (i < nout && j < nin) ? Mcm[(size_t)i * ldm + j] : 0.0;
+    }
+    for (int e = threadIdx.x; e < BK * BN; e += NT) {
+      int c = e / BN, q = e % BN;
+      int j = j0 + c, p = p0 + q;
+      Is[c][q] = (j < nin && p < K) ? in[(size_t)j * ldi + p] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      double m[4], v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        m[q] = Ms[kk][ty + 16 * q];
+        v[q] = Is[kk][tx + 16 * q];
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[q][r] += m[q] * v[r];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      int i = i0 + ty + 16 * q, p = p0 + tx + 16 * r;
+      if (i < nout && p < K) {
+        double* o = out + (size_t)i * ldo + p;
+        *o = alpha * acc[q][r] + (beta == 0.0 ? 0.0 : beta * (*o));
+      }
+    }
+}
+
+// column-major C = alpha op(A) op(B) + beta C (reference DGEMM semantics)
+__global__ void __launch_bounds__(NT)
+k_dgemm(int ta, int tb, int m, int n, int k, double alpha, const double* __restrict__ A, int lda,
+        const double* __restrict__ B, int ldb, double beta, double* __restrict__ C, int ldc) {
+  __shared__ double As[BK][BM + 1];
+  __shared__ double Bs[BK][BN + 1];
+  const int i0 = blockIdx.x * BM, j0 = blockIdx.y * BN;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4] = {};
+  for (int l0 = 0; l0 < k; l0 += BK) {
+    for (int e = threadIdx.x; e < BM * BK; e += NT) {
+      int r, c;
+      if (ta) { r = e / BK; c = e % BK; } else { c = e / BM; r = e % BM; }
+      int i = i0 + r, l = l0 + c;
+      double v = 0.0;
+      if (i < m && l < k) v = ta ? A[(size_t)i * lda + l] : A[(size_t)l * lda + i];
+      As[c][r] = v;
+    }
+    for (int e = threadIdx.x; e < BN * BK; e += NT) {
+      int r, c;
+      if (tb) { c = e / BN; r = e % BN; } else { r = e / BK; c = e % BK; }
+      int j = j0 + r, l = l0 + c;
+      double v = 0.0;
+      if (j < n && l < k) v = tb ? B[(size_t)l * ldb + j] : B[(size_t)j * ldb + l];
+      Bs[c][r] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = As[kk][ty + 16 * q];
+        b[q] = Bs[kk][tx + 16 * q];
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[q][r] += a[q] * b[r];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      int i = i0 + ty + 16 * q, j = j0 + tx + 16 * r;
+      if (i < m && j < n) {
+        double* c = C + (size_t)j * ldc + i;
+        *c = alpha * acc[q][r] + (beta == 0.0 ? 0.0 : beta * (*c));
+      }
+    }
+}
+
+}  // namespace pcalc
+
+// ---------------------------------------------------------------------------
+// host side
+
+int pc_overlap_launch(cpstep_ctx* c, const double* a, const double* b, int M, int N, int K,
+                      const double* w, double alpha, double beta, double* C, int ldc) {
+  using namespace pcalc;
+  int tm = cdiv(M, BM), tn = cdiv(N, BN);
+  int want = std::max(1, (2 * c->num_sms) / (tm * tn));
+  int kslab = cdiv(cdiv(K, want), BK) * BK;
+  int nsplit = cdiv(K, kslab);
+  size_t need = (size_t)nsplit * M * N;
+  if (need > c->pc_part_elems) {
+    cudaFree(c->d_pc_part);
+    c->d_pc_part = nullptr;
+    CPSTEP_CUDA_TRY(cudaMalloc(&c->d_pc_part, need * sizeof(double)));
+    c->pc_part_elems = need;
+  }
+  k_overlap_part<<<dim3(tm, tn, nsplit), NT, 0, c->stream>>>(a, K, b, K, w, M, N, K, kslab,
+                                                             c->d_pc_part);
+  CPSTEP_LAUNCH_CHECK();
+  k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, c->stream>>>(c->d_pc_part, nsplit, M, N, alpha,
+                                                            beta, C, ldc);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
+int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
+                      double* out, int ldo, int nout, int nin, int K, double alpha, double beta) {
+  using namespace pcalc;
+  dim3 grid(cdiv(K, BN), cdiv(nout, BM));
+  k_backmul<<<grid, NT, 0, c->stream>>>(Mcm, ldm, in, ldi, out, ldo, nout, nin, K, alpha, beta);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
+int dgemm_launch(cudaStream_t s, int ta, int tb, int m, int n, int k, double alpha,
+                 const double* A, int lda, const double* B, int ldb, double beta, double* C,
+                 int ldc) {
+  using namespace pcalc;
+  dim3 grid(cdiv(m, BM), cdiv(n, BN));
+  k_dgemm<<<grid, NT, 0, s>>>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}

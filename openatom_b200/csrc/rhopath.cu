@@ -1,0 +1,493 @@
+// Density side of the step: PZ-LDA exchange-correlation, the density FFT on
+// the density sphere, Hartree + local pseudopotential + reciprocal Ewald in G
+// space with the atom forces, and V_KS(r).
+//
+//   CPXCFNCTS::CP_exc_calc       src_piny_physics_v1.0/abinito_physics/cp_xc_fnctl/cp_pz_lda.C:23-170
+//   CPLOCAL::CP_hart_eext_calc   src_piny_physics_v1.0/abinito_physics/cp_local/cp_hart_ext.C:56-405
+//   CP_get_vpsnow (spline)       cp_hart_ext.C:433-475
+//   density FFTs                 CP_Rho_RealSpacePlane::fftRhoRtoRhoG (cp_density_ctrl/
+//                                CP_Rho_RealSpacePlane.C:831-864), CP_Rho_GHartExt::FFTVks
+//                                (CP_Rho_GHartExt.C:532-540), acceptHartVks (:1365-1415)
+//
+// The density sphere (|G|^2/2 <= 4 Ecut) is held in the same packed line
+// layout as the states, so the state FFT kernels (FP64) transform it.  Those
+// compute sum_r f e^{+iG.r} and sum_G c e^{-iG.r}; the reference's rho(G) uses
+// e^{-iG.r} and V(r) = sum vks(G) e^{+iG.r}, so the kernels below read conj of
+// the transformed density and store conj of vks: the arithmetic on rho(G),
+// vks(G), the energies and forces is the reference's.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+#include "ctx.cuh"
+
+int cpstep_density_layout(double box_len, double ecut_ry, int nfft, std::vector<int>& kx,
+                          std::vector<int>& ky, std::vector<int>& kz, std::vector<int>& runs);
+
+namespace rho {
+
+// PZ-LDA constants (cp_pz_lda.C:47-53)
+__constant__ double kPZ[7] = {-0.14230, 1.05290, 0.33340, 0.03110, -0.0480, 0.00200, -0.01160};
+
+__global__ void k_xc(const double* __restrict__ rho, double* __restrict__ vxc, size_t n,
+                     double* __restrict__ part) {
+  __shared__ double red[32];
+  const double gamma = kPZ[0], beta1 = kPZ[1], beta2 = kPZ[2], au = kPZ[3], bu = kPZ[4],
+               cu = kPZ[5], du = kPZ[6];
+  const double rat1 = (7.0 / 6.0) * beta1, rat2 = (4.0 / 3.0) * beta2, third = 1.0 / 3.0;
+  double ex = 0.0, ec = 0.0, mu = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double r = rho[i];
+    double v = 0.0;
+    if (r > 0.0) {
+      double rs = cbrt(3.0 / (4.0 * M_PI * r));
+      double sq = sqrt(rs);
+      double xfact = -cbrt(3.0 * r / M_PI);
+      double cfact, mufact;
+      if (rs >= 1.0) {
+        double cf1 = 1.0 + beta1 * sq + beta2 * rs;
+        double cf2 = 1.0 + rat1 * sq + rat2 * rs;
+        cfact = gamma / cf1;
+        mufact = cfact * (cf2 / cf1);
+      } else {
+        double lnrs = log(rs);
+        cfact = au * lnrs + bu + cu * rs * lnrs + du * rs;
+        mufact = au * lnrs + (bu - third * au) + 2.0 * third * cu * rs * lnrs +
+                 third * (2.0 * du - cu) * rs;
+      }
+      ex += xfact * r;
+      ec += cfact * r;
+      v = xfact + mufact;
+      mu += v * r;
+    }
+    vxc[i] = v;
+  }
+  double a = block_sum(0.75 * ex + ec, red);
+  double b = block_sum(mu, red);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = a;
+    part[2 * blockIdx.x + 1] = b;
+  }
+}
+
+struct Atoms {
+  int natm, ntyp;
+  const int* typ;      // [natm]
+  const double* frac;  // [natm][3] fractional coordinates (hmati R)
+  const double* q;     // [ntyp]
+  const double* vps;   // [ntyp][4][nspl]
+  const double* gzvps; // [ntyp]
+  int nspl;
+  double gmin, dg;
+  int kxm, kym, kzm;   // phase-table extents
+  const double2* ex;   // [kxm+1][natm]      e^{i 2pi kx s_x}
+  const double2* ey;   // [2kym+1][natm]     ky in [-kym, kym]
+  const double2* ez;   // [2kzm+1][natm]
+};
+
+__global__ void k_phase(const double* __restrict__ frac, int natm, int kxm, int kym, int kzm,
+                        double2* __restrict__ ex, double2* __restrict__ ey,
+                        double2* __restrict__ ez) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natm) return;
+  const double tpi = 2.0 * M_PI;
+  for (int k = 0; k <= kxm; ++k) {
+    double s, c;
+    sincos(tpi * k * frac[3 * a], &s, &c);
+    ex[(size_t)k * natm + a] = make_double2(c, s);
+  }
+  for (int k = -kym; k <= kym; ++k) {
+    double s, c;
+    sincos(tpi * k * frac[3 * a + 1], &s, &c);
+    ey[(size_t)(k + kym) * natm + a] = make_double2(c, s);
+  }
+  for (int k = -kzm; k <= kzm; ++k) {
+    double s, c;
+    sincos(tpi * k * frac[3 * a + 2], &s, &c);
+    ez[(size_t)(k + kzm) * natm + a] = make_double2(c, s);
+  }
+}
+
+__device__ __forceinline__ double2 phase(const Atoms& A, int a, int kx, int ky, int kz) {
+  double2 x = A.ex[(size_t)kx * A.natm + a];
+  double2 y = A.ey[(size_t)(ky + A.kym) * A.natm + a];
+  double2 z = A.ez[(size_t)(kz + A.kzm) * A.natm + a];
+  double2 xy = make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
+  return make_double2(xy.x * z.x - xy.y * z.y, xy.x * z.y + xy.y * z.x);
+}
+
+// spline value / vol of type t at g (CP_get_vpsnow, cp_hart_ext.C:459-471)
+__device__ __forceinline__ double vps_at(const Atoms& A, int t, double g, double rvol) {
+  int iii = (int)((g - A.gmin) / A.dg + 1.0);
+  iii = min(iii, A.nspl);
+  iii = max(iii, 1);
+  double h = g - ((double)(iii - 1) * A.dg + A.gmin);
+  const double* v = A.vps + (size_t)t * 4 * A.nspl + (iii - 1);
+  return (((v[3 * A.nspl] * h + v[2 * A.nspl]) * h + v[A.nspl]) * h + v[0]) * rvol;
+}
+
+// One thread per density-sphere point.  rhog_t: transformed density
+// (sum rho e^{+iGr} * vol/N = conj of the reference rho(G)); writes conj(vks)
+// for the G->R kernels, the force kernel's per-point terms and energy partials.
+__global__ void k_hart(const double2* __restrict__ rhog_t, const int* __restrict__ kx,
+                       const int* __restrict__ ky, const int* __restrict__ kz, int npts,
+                       const double* __restrict__ hmati, double vol, double ecut4, double alp,
+                       Atoms A, double2* __restrict__ vg_t, double4* __restrict__ fterm,
+                       double* __restrict__ part) {
+  __shared__ double red[32];
+  const double tpi = 2.0 * M_PI, rvol = 1.0 / vol, fpi = 4.0 * M_PI;
+  const double falp2 = 4.0 * alp * alp;
+  double eh = 0.0, ee = 0.0, ew = 0.0;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npts; p += gridDim.x * blockDim.x) {
+    int a = kx[p], b = ky[p], c = kz[p];
+    double gx = tpi * (a * hmati[0] + b * hmati[1] + c * hmati[2]);
+    double gy = tpi * (a * hmati[3] + b * hmati[4] + c * hmati[5]);
+    double gz = tpi * (a * hmati[6] + b * hmati[7] + c * hmati[8]);
+    double g2 = gx * gx + gy * gy + gz * gz;
+    double2 out = make_double2(0.0, 0.0);
+    double4 ft = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (g2 <= ecut4 && g2 != 0.0) {
+      double w = (a == 0) ? 1.0 : 2.0;
+      double2 r = rhog_t[p];
+      r.y = -r.y;  // reference rho(G)
+      double hart = fpi / (g2 * vol);
+      eh += 0.5 * hart * (r.x * r.x + r.y * r.y) * w;
+      double g = sqrt(g2);
+      double2 vext = make_double2(0.0, 0.0), sewd = make_double2(0.0, 0.0);
+      for (int t = 0; t < A.ntyp; ++t) {
+        double vt = vps_at(A, t, g, rvol);
+        double qt = A.q[t];
+        double2 st = make_double2(0.0, 0.0);
+        for (int i = 0; i < A.natm; ++i) {
+          if (A.typ[i] != t) continue;
+          double2 h = phase(A, i, a, b, c);
+          st.x += h.x;
+          st.y += h.y;
+        }
+        vext.x += vt * st.x;
+        vext.y += vt * st.y;
+        sewd.x += qt * st.x;
+        sewd.y += qt * st.y;
+      }
+      double ewdf = fpi * exp(-g2 / falp2) / (g2 * vol);
+      ew += 0.5 * ewdf * (sewd.x * sewd.x + sewd.y * sewd.y) * w;
+      ee += (r.x * vext.x - r.y * vext.y) * w;
+      // vks = rho*hart + conj(vext); store conj(vks)
+      out = make_double2(r.x * hart + vext.x, -(r.y * hart - vext.y));
+      ft = make_double4(r.x * w, -r.y * w, sewd.x * ewdf * w, sewd.y * ewdf * w);
+    }
+    vg_t[p] = out;
+    fterm[p] = ft;
+  }
+  double s1 = block_sum(eh, red);
+  double s2 = block_sum(ee, red);
+  double s3 = block_sum(ew, red);
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x] = s1;
+    part[3 * blockIdx.x + 1] = s2;
+    part[3 * blockIdx.x + 2] = s3;
+  }
+}
+
+// G = 0 (cp_hart_ext.C:345-368); single thread
+__global__ void k_hart_g0(const double2* __restrict__ rhog_t, int izero, double vol, Atoms A,
+                          double2* __restrict__ vg_t, double* __restrict__ eext) {
+  double v = 0.0;
+  for (int i = 0; i < A.natm; ++i) v += A.gzvps[A.typ[i]];
+  v /= vol;
+  vg_t[izero] = make_double2(v, 0.0);
+  *eext += v * rhog_t[izero].x;
+}
+
+// Forces: block b handles a chunk of points for all atoms (thread <-> atom).
+constexpr int FCHUNK = 256;
+__global__ void k_local_forces(const double4* __restrict__ fterm, const int* __restrict__ kx,
+                               const int* __restrict__ ky, const int* __restrict__ kz, int npts,
+                               const double* __restrict__ hmati, double vol, Atoms A,
+                               double* __restrict__ fpart) {
+  __shared__ double4 sft[FCHUNK];
+  __shared__ int sk[FCHUNK][3];
+  __shared__ double sg[FCHUNK][4];  // gx, gy, gz, g
+  const double tpi = 2.0 * M_PI, rvol = 1.0 / vol;
+  const int p0 = blockIdx.x * FCHUNK;
+  const int np = min(FCHUNK, npts - p0);
+  for (int i = threadIdx.x; i < np; i += blockDim.x) {
+    int p = p0 + i;
+    int a = kx[p], b = ky[p], c = kz[p];
+    sft[i] = fterm[p];
+    sk[i][0] = a; sk[i][1] = b; sk[i][2] = c;
+    double gx = tpi * (a * hmati[0] + b * hmati[1] + c * hmati[2]);
+    double gy = tpi * (a * hmati[3] + b * hmati[4] + c * hmati[5]);
+    double gz = tpi * (a * hmati[6] + b * hmati[7] + c * hmati[8]);
+    sg[i][0] = gx; sg[i][1] = gy; sg[i][2] = gz;
+    sg[i][3] = sqrt(gx * gx + gy * gy + gz * gz);
+  }
+  __syncthreads();
+  for (int at = threadIdx.x; at < A.natm; at += blockDim.x) {
+    const int t = A.typ[at];
+    const double qa = A.q[t];
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int i = 0; i < np; ++i) {
+      double4 f = sft[i];
+      if (f.x == 0.0 && f.y == 0.0 && f.z == 0.0 && f.w == 0.0) continue;
+      double vt = vps_at(A, t, sg[i][3], rvol);
+      double2 h = phase(A, at, sk[i][0], sk[i][1], sk[i][2]);
+      double tr = f.x * vt + f.z * qa;
+      double ti = f.y * vt + f.w * qa;
+      double s = tr * h.y - ti * h.x;
+      fx += sg[i][0] * s;
+      fy += sg[i][1] * s;
+      fz += sg[i][2] * s;
+    }
+    double* o = fpart + ((size_t)blockIdx.x * A.natm + at) * 3;
+    o[0] = fx; o[1] = fy; o[2] = fz;
+  }
+}
+
+__global__ void k_sum_cols(const double* __restrict__ part, int nrow, int ncol,
+                           double* __restrict__ out, double scale) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  double s = 0.0;
+  for (int r = 0; r < nrow; ++r) s += part[(size_t)r * ncol + c];
+  out[c] = s * scale;
+}
+
+__global__ void k_add(double* __restrict__ a, const double* __restrict__ b, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    a[i] += b[i];
+}
+
+__global__ void k_conj_scale(const double2* __restrict__ in, double2* __restrict__ out, int n,
+                             double s) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_double2(in[i].x * s, -in[i].y * s);
+}
+
+}  // namespace rho
+
+// ===========================================================================
+
+static int upload_i(int** d, const std::vector<int>& h) {
+  CPSTEP_CUDA_TRY(cudaMalloc(d, sizeof(int) * std::max<size_t>(1, h.size())));
+  CPSTEP_CUDA_TRY(cudaMemcpy(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
+  return CPSTEP_OK;
+}
+static int upload_d(double** d, const std::vector<double>& h) {
+  CPSTEP_CUDA_TRY(cudaMalloc(d, sizeof(double) * std::max<size_t>(1, h.size())));
+  CPSTEP_CUDA_TRY(cudaMemcpy(*d, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  return CPSTEP_OK;
+}
+
+int rho_init(cpstep_ctx* c, double box_len, double ecut_ry) {
+  std::vector<int> kx, ky, kz, runs;
+  int rc = cpstep_density_layout(box_len, ecut_ry, c->nx, kx, ky, kz, runs);
+  if (rc) {
+    cpstep_set_error("density sphere does not fit the %d grid", c->nx);
+    return rc;
+  }
+  int nl = (int)runs.size() / 14;
+  std::vector<int> off(nl), nneg(nl), npos(nl), zneg(nl), zpos(nl), xy(nl);
+  int kxmax = 0;
+  for (int l = 0; l < nl; ++l) {
+    const int* rn = runs.data() + 14 * l;
+    const int* rp = rn + 7;
+    off[l] = rn[3]; nneg[l] = rn[4]; npos[l] = rp[4];
+    zneg[l] = rn[2] + (c->nz - rn[6]);
+    zpos[l] = rp[2];
+    xy[l] = rp[0] | (rp[1] << 16);
+    kxmax = std::max(kxmax, rp[0]);
+  }
+  int np = (int)kx.size();
+  std::vector<double> g2(np), wpt(np);
+  const double* hi = c->hmati;
+  for (int i = 0; i < np; ++i) {
+    double a = kx[i], b = ky[i], cc = kz[i];
+    double gx = (a * hi[0] + b * hi[1] + cc * hi[2]) * 2.0 * M_PI;
+    double gy = (a * hi[3] + b * hi[4] + cc * hi[5]) * 2.0 * M_PI;
+    double gz = (a * hi[6] + b * hi[7] + cc * hi[8]) * 2.0 * M_PI;
+    g2[i] = gx * gx + gy * gy + gz * gz;
+    wpt[i] = kx[i] == 0 ? 1.0 : 2.0;
+    if (kx[i] == 0 && ky[i] == 0 && kz[i] == 0) c->rho_izero = i;
+  }
+  RhoGeom& r = c->rg;
+  r.npts = np;
+  r.nlines = nl;
+  r.nlpad = (nl + 3) & ~3;
+  r.nplane_x = kxmax + 1;
+  if ((rc = upload_i(&r.line_off, off)) || (rc = upload_i(&r.line_nneg, nneg)) ||
+      (rc = upload_i(&r.line_npos, npos)) || (rc = upload_i(&r.line_zneg, zneg)) ||
+      (rc = upload_i(&r.line_zpos, zpos)) || (rc = upload_i(&r.line_xy, xy)) ||
+      (rc = upload_i(&r.kx, kx)) || (rc = upload_i(&r.ky, ky)) || (rc = upload_i(&r.kz, kz)) ||
+      (rc = upload_d(&r.g2, g2)) || (rc = upload_d(&r.wpt, wpt)))
+    return rc;
+  size_t pen = (size_t)c->nz * r.nlpad * sizeof(double2);
+  CPSTEP_CUDA_TRY(cudaMalloc(&r.pen_a, pen));
+  CPSTEP_CUDA_TRY(cudaMalloc(&r.pen_b, pen));
+  CPSTEP_CUDA_TRY(cudaMalloc(&r.rhog, sizeof(double2) * np));
+  CPSTEP_CUDA_TRY(cudaMalloc(&r.vg, sizeof(double2) * np));
+  CPSTEP_CUDA_TRY(cudaMalloc(&r.fterm, sizeof(double4) * np));
+  size_t nr = (size_t)c->nx * c->ny * c->nz;
+  CPSTEP_CUDA_TRY(cudaMalloc(&r.vhl, sizeof(double) * nr));
+  r.nblk_xc = 4 * c->num_sms;
+  r.nblk_h = 2 * c->num_sms;
+  CPSTEP_CUDA_TRY(cudaMalloc(&r.part, sizeof(double) * (2 * r.nblk_xc + 3 * r.nblk_h + 8)));
+  CPSTEP_CUDA_TRY(cudaMalloc(&c->d_energies, sizeof(double) * CPSTEP_NENERGY));
+  CPSTEP_CUDA_TRY(cudaMemset(c->d_energies, 0, sizeof(double) * CPSTEP_NENERGY));
+  return CPSTEP_OK;
+}
+
+void rho_free(cpstep_ctx* c) {
+  RhoGeom& r = c->rg;
+  cudaFree(r.line_off); cudaFree(r.line_nneg); cudaFree(r.line_npos); cudaFree(r.line_zneg);
+  cudaFree(r.line_zpos); cudaFree(r.line_xy); cudaFree(r.kx); cudaFree(r.ky); cudaFree(r.kz);
+  cudaFree(r.g2); cudaFree(r.wpt); cudaFree(r.pen_a); cudaFree(r.pen_b); cudaFree(r.rhog);
+  cudaFree(r.vg); cudaFree(r.fterm); cudaFree(r.vhl); cudaFree(r.part);
+  cudaFree(c->d_energies);
+  AtomData& a = c->atoms;
+  cudaFree(a.typ); cudaFree(a.frac); cudaFree(a.q); cudaFree(a.vps); cudaFree(a.gzvps);
+  cudaFree(a.ex); cudaFree(a.ey); cudaFree(a.ez); cudaFree(a.fpart);
+}
+
+FftJob rho_job(const cpstep_ctx* c) {
+  FftJob j;
+  const RhoGeom& r = c->rg;
+  j.g.nx = c->nx; j.g.ny = c->ny; j.g.nz = c->nz;
+  j.g.nlines = r.nlines; j.g.nlpad = r.nlpad; j.g.nplane_x = r.nplane_x; j.g.npts = r.npts;
+  j.g.line_off = r.line_off; j.g.line_nneg = r.line_nneg; j.g.line_npos = r.line_npos;
+  j.g.line_zneg = r.line_zneg; j.g.line_zpos = r.line_zpos; j.g.line_xy = r.line_xy;
+  j.g.g2 = r.g2; j.g.wpt = r.wpt;
+  j.pen_a = r.pen_a;
+  j.pen_b = r.pen_b;
+  return j;
+}
+
+int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* pos,
+              const double* q, int nspl, double gmin, double dg, const double* vps,
+              const double* gzvps, double alp_ewd) {
+  AtomData& a = c->atoms;
+  cudaFree(a.typ); cudaFree(a.frac); cudaFree(a.q); cudaFree(a.vps); cudaFree(a.gzvps);
+  cudaFree(a.ex); cudaFree(a.ey); cudaFree(a.ez); cudaFree(a.fpart);
+  a = AtomData();
+  std::vector<int> t(typ, typ + natm);
+  for (int v : t)
+    if (v < 0 || v >= ntyp) {
+      cpstep_set_error("atoms: type index out of range");
+      return CPSTEP_ERR_ARG;
+    }
+  std::vector<double> frac(3 * (size_t)natm);
+  const double* hi = c->hmati;  // s = hmati R (column-major hmati)
+  for (int i = 0; i < natm; ++i) {
+    const double* R = pos + 3 * i;
+    for (int d = 0; d < 3; ++d)
+      frac[3 * i + d] = hi[d] * R[0] + hi[d + 3] * R[1] + hi[d + 6] * R[2];
+  }
+  int rc;
+  if ((rc = upload_i(&a.typ, t)) || (rc = upload_d(&a.frac, frac)) ||
+      (rc = upload_d(&a.q, std::vector<double>(q, q + ntyp))) ||
+      (rc = upload_d(&a.vps, std::vector<double>(vps, vps + (size_t)ntyp * 4 * nspl))) ||
+      (rc = upload_d(&a.gzvps, std::vector<double>(gzvps, gzvps + ntyp))))
+    return rc;
+  a.natm = natm;
+  a.ntyp = ntyp;
+  a.nspl = nspl;
+  a.gmin = gmin;
+  a.dg = dg;
+  a.alp_ewd = alp_ewd;
+  a.kxm = c->nx / 2;
+  a.kym = c->ny / 2;
+  a.kzm = c->nz / 2;
+  CPSTEP_CUDA_TRY(cudaMalloc(&a.ex, sizeof(double2) * (a.kxm + 1) * natm));
+  CPSTEP_CUDA_TRY(cudaMalloc(&a.ey, sizeof(double2) * (2 * a.kym + 1) * natm));
+  CPSTEP_CUDA_TRY(cudaMalloc(&a.ez, sizeof(double2) * (2 * a.kzm + 1) * natm));
+  int nfb = cdiv(c->rg.npts, rho::FCHUNK);
+  CPSTEP_CUDA_TRY(cudaMalloc(&a.fpart, sizeof(double) * 3 * (size_t)natm * nfb));
+  rho::k_phase<<<cdiv(natm, 128), 128, 0, c->stream>>>(a.frac, natm, a.kxm, a.kym, a.kzm, a.ex,
+                                                        a.ey, a.ez);
+  CPSTEP_LAUNCH_CHECK();
+  CPSTEP_CUDA_TRY(cudaMalloc(&c->d_hmati, sizeof(double) * 9));
+  CPSTEP_CUDA_TRY(cudaMemcpy(c->d_hmati, c->hmati, sizeof(double) * 9, cudaMemcpyHostToDevice));
+  return CPSTEP_OK;
+}
+
+static rho::Atoms atoms_view(const cpstep_ctx* c) {
+  const AtomData& a = c->atoms;
+  rho::Atoms A;
+  A.natm = a.natm; A.ntyp = a.ntyp; A.typ = a.typ; A.frac = a.frac; A.q = a.q; A.vps = a.vps;
+  A.gzvps = a.gzvps; A.nspl = a.nspl; A.gmin = a.gmin; A.dg = a.dg;
+  A.kxm = a.kxm; A.kym = a.kym; A.kzm = a.kzm; A.ex = a.ex; A.ey = a.ey; A.ez = a.ez;
+  return A;
+}
+
+// E_xc, muxc -> energies[EXC], [MUXC]; vxc written to out
+int rho_xc(cpstep_ctx* c, const double* rho_r, double* vxc, double* energies) {
+  size_t nr = (size_t)c->nx * c->ny * c->nz;
+  RhoGeom& r = c->rg;
+  rho::k_xc<<<r.nblk_xc, 256, 0, c->stream>>>(rho_r, vxc, nr, r.part);
+  CPSTEP_LAUNCH_CHECK();
+  rho::k_sum_cols<<<1, 32, 0, c->stream>>>(r.part, r.nblk_xc, 2, energies + CPSTEP_E_EXC,
+                                           c->vol / (double)nr);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
+// rho(r) -> transformed density (conj of the reference rho(G)) in r.rhog
+int rho_r2g(cpstep_ctx* c, const double* rho_r) {
+  FftJob j = rho_job(c);
+  double scale = c->vol / ((double)c->nx * c->ny * c->nz);
+  return c->ops64.r2g(c, j, rho_r, reinterpret_cast<double*>(c->rg.rhog), 1, scale);
+}
+
+// Hartree + local + Ewald from r.rhog: conj(vks) in r.vg, energies, force terms
+int rho_hart(cpstep_ctx* c, double* energies, double* force) {
+  RhoGeom& r = c->rg;
+  if (c->atoms.natm <= 0) {
+    cpstep_set_error("hart_eext: no atoms set (cpstep_set_atoms)");
+    return CPSTEP_ERR_STATE;
+  }
+  rho::Atoms A = atoms_view(c);
+  double ecut4 = 8.0 * (0.5 * c->ecut_ry);
+  double* hp = r.part + 2 * r.nblk_xc;
+  rho::k_hart<<<r.nblk_h, 256, 0, c->stream>>>(r.rhog, r.kx, r.ky, r.kz, r.npts, c->d_hmati,
+                                               c->vol, ecut4, c->atoms.alp_ewd, A, r.vg,
+                                               r.fterm, hp);
+  CPSTEP_LAUNCH_CHECK();
+  rho::k_sum_cols<<<1, 32, 0, c->stream>>>(hp, r.nblk_h, 3, energies + CPSTEP_E_HART, 1.0);
+  CPSTEP_LAUNCH_CHECK();
+  if (c->rho_izero >= 0) {
+    rho::k_hart_g0<<<1, 1, 0, c->stream>>>(r.rhog, c->rho_izero, c->vol, A, r.vg,
+                                           energies + CPSTEP_E_EXT);
+    CPSTEP_LAUNCH_CHECK();
+  }
+  if (force) {
+    int nfb = cdiv(r.npts, rho::FCHUNK);
+    int nt = std::min(1024, ((c->atoms.natm + 31) / 32) * 32);
+    rho::k_local_forces<<<nfb, nt, 0, c->stream>>>(r.fterm, r.kx, r.ky, r.kz, r.npts,
+                                                   c->d_hmati, c->vol, A, c->atoms.fpart);
+    CPSTEP_LAUNCH_CHECK();
+    rho::k_sum_cols<<<cdiv(3 * c->atoms.natm, 128), 128, 0, c->stream>>>(
+        c->atoms.fpart, nfb, 3 * c->atoms.natm, force, 1.0);
+    CPSTEP_LAUNCH_CHECK();
+  }
+  return CPSTEP_OK;
+}
+
+// V_KS(r) = vxc (already in vks_r) + sum_G vks(G) e^{iGr}
+int rho_vks_r(cpstep_ctx* c, double* vks_r) {
+  FftJob j = rho_job(c);
+  size_t nr = (size_t)c->nx * c->ny * c->nz;
+  if (int rc = c->ops64.g2r(c, j, reinterpret_cast<const double*>(c->rg.vg), c->rg.vhl, 1))
+    return rc;
+  rho::k_add<<<2 * c->num_sms, 256, 0, c->stream>>>(vks_r, c->rg.vhl, nr);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
+// helpers for the ABI entries that exchange reference-convention arrays
+int rho_conj_scale(cpstep_ctx* c, const double* in, double* out, int n, double s) {
+  rho::k_conj_scale<<<cdiv(n, 256), 256, 0, c->stream>>>(
+      reinterpret_cast<const double2*>(in), reinterpret_cast<double2*>(out), n, s);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}

@@ -79,7 +79,7 @@ int statefft_init(cpstep_ctx* c) {
     cpstep_set_error("state FFT: only cubic grids are built (got %d x %d x %d)", c->nx, c->ny, c->nz);
     return CPSTEP_ERR_ARG;
   }
-  if (!lookup_ops(c->precision, c->nx, &c->ops)) {
+  if (!lookup_ops(c->precision, c->nx, &c->ops) || !lookup_ops(CPSTEP_PREC_FP64, c->nx, &c->ops64)) {
     cpstep_set_error("state FFT: grid size %d not built into libcpstep", c->nx);
     return CPSTEP_ERR_ARG;
   }

@@ -418,21 +418,22 @@ inline int plane_groups(const cpstep_ctx* c, int nstates, int other) {
 
 template <typename T, int N>
 struct StateFft {
-  static int zfft_fwd(cpstep_ctx* c, const double* psi, int nstates) {
-    dim3 grid(cdiv(c->nlines, ZShape<N>::LB), nstates);
+  static int zfft_fwd(cpstep_ctx* c, const FftJob& j, const double* psi, int nstates) {
+    dim3 grid(cdiv(j.g.nlines, ZShape<N>::LB), nstates);
     const size_t smem = ZShape<N>::template bytes<T>();
     if (int rc = set_smem(k_zfft_fwd<T, N>, smem)) return rc;
     k_zfft_fwd<T, N><<<grid, ZTHREADS, smem, c->stream>>>(
-        reinterpret_cast<const double2*>(psi), reinterpret_cast<cplx<T>*>(c->d_pen_a), c->geom(),
+        reinterpret_cast<const double2*>(psi), reinterpret_cast<cplx<T>*>(j.pen_a), j.g,
         tws<T>(c).z);
     CPSTEP_LAUNCH_CHECK();
     return CPSTEP_OK;
   }
 
   static int density(cpstep_ctx* c, const double* psi, const double* occ, double* rho) {
-    if (int rc = zfft_fwd(c, psi, c->nstates)) return rc;
-    const int RC = PShape<T, N>::rc_for(c->nplane_x, false);
-    const size_t smem = PShape<T, N>::bytes(c->nplane_x, RC, false);
+    const FftJob j = c->state_job();
+    if (int rc = zfft_fwd(c, j, psi, c->nstates)) return rc;
+    const int RC = PShape<T, N>::rc_for(j.g.nplane_x, false);
+    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x, RC, false);
     int rows = std::min(N, (Kmax<T>::v * PTHREADS) / N) & ~1;
     int ysplit = cdiv(N, rows);
     int ng = std::min(c->ngroups_rho, plane_groups(c, c->nstates, ysplit));
@@ -440,8 +441,8 @@ struct StateFft {
     ng = cdiv(c->nstates, spg);
     if (int rc = set_smem(k_xy_fwd<T, N, 0>, smem)) return rc;
     k_xy_fwd<T, N, 0><<<dim3(N, ng, ysplit), PTHREADS, smem, c->stream>>>(
-        reinterpret_cast<const cplx<T>*>(c->d_pen_a), c->geom(), tws<T>(c).x, occ, c->nstates,
-        spg, rows, RC, c->d_rho_part);
+        reinterpret_cast<const cplx<T>*>(j.pen_a), j.g, tws<T>(c).x, occ, c->nstates, spg, rows,
+        RC, c->d_rho_part);
     CPSTEP_LAUNCH_CHECK();
     size_t nr = (size_t)N * N * N;
     k_rho_reduce<<<2 * c->num_sms, 256, 0, c->stream>>>(c->d_rho_part, ng, nr, 1.0 / c->vol, rho);
@@ -449,33 +450,34 @@ struct StateFft {
     return CPSTEP_OK;
   }
 
-  static int gtor(cpstep_ctx* c, const double* psi, double* psi_r, int nstates) {
-    if (int rc = zfft_fwd(c, psi, nstates)) return rc;
-    const int RC = PShape<T, N>::rc_for(c->nplane_x, false);
-    const size_t smem = PShape<T, N>::bytes(c->nplane_x, RC, false);
+  // packed G -> real r for nstates arrays of the job's geometry
+  static int g2r(cpstep_ctx* c, const FftJob& j, const double* packed, double* real, int nstates) {
+    if (int rc = zfft_fwd(c, j, packed, nstates)) return rc;
+    const int RC = PShape<T, N>::rc_for(j.g.nplane_x, false);
+    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x, RC, false);
     if (int rc = set_smem(k_xy_fwd<T, N, 1>, smem)) return rc;
     k_xy_fwd<T, N, 1><<<dim3(N, nstates, 1), PTHREADS, smem, c->stream>>>(
-        reinterpret_cast<const cplx<T>*>(c->d_pen_a), c->geom(), tws<T>(c).x, nullptr, nstates,
-        1, N, RC, psi_r);
+        reinterpret_cast<const cplx<T>*>(j.pen_a), j.g, tws<T>(c).x, nullptr, nstates, 1, N, RC,
+        real);
     CPSTEP_LAUNCH_CHECK();
     return CPSTEP_OK;
   }
 
-  static int zfft_bwd(cpstep_ctx* c, double* out, const double* psi, const double* occ,
-                      int nstates, double scale, int mode) {
-    dim3 grid(cdiv(c->nlines, ZShape<N>::LB), nstates);
+  static int zfft_bwd(cpstep_ctx* c, const FftJob& j, double* out, const double* psi,
+                      const double* occ, int nstates, double scale, int mode) {
+    dim3 grid(cdiv(j.g.nlines, ZShape<N>::LB), nstates);
     const size_t smem = ZShape<N>::template bytes<T>();
     if (mode == 0) {
       if (int rc = set_smem(k_zfft_bwd<T, N, 0>, smem)) return rc;
       k_zfft_bwd<T, N, 0><<<grid, ZTHREADS, smem, c->stream>>>(
-          reinterpret_cast<const cplx<T>*>(c->d_pen_b), reinterpret_cast<double2*>(out),
-          reinterpret_cast<const double2*>(psi), occ, c->geom(), tws<T>(c).z, scale, c->ecut_ry,
+          reinterpret_cast<const cplx<T>*>(j.pen_b), reinterpret_cast<double2*>(out),
+          reinterpret_cast<const double2*>(psi), occ, j.g, tws<T>(c).z, scale, c->ecut_ry,
           c->d_eke_part);
     } else {
       if (int rc = set_smem(k_zfft_bwd<T, N, 1>, smem)) return rc;
       k_zfft_bwd<T, N, 1><<<grid, ZTHREADS, smem, c->stream>>>(
-          reinterpret_cast<const cplx<T>*>(c->d_pen_b), reinterpret_cast<double2*>(out), nullptr,
-          nullptr, c->geom(), tws<T>(c).z, scale, 0.0, nullptr);
+          reinterpret_cast<const cplx<T>*>(j.pen_b), reinterpret_cast<double2*>(out), nullptr,
+          nullptr, j.g, tws<T>(c).z, scale, 0.0, nullptr);
     }
     CPSTEP_LAUNCH_CHECK();
     return CPSTEP_OK;
@@ -483,9 +485,10 @@ struct StateFft {
 
   static int vpsi(cpstep_ctx* c, const double* psi, const double* vks, const double* occ,
                   double* force, double* eke, int pencils_ready) {
+    const FftJob j = c->state_job();
     size_t nr = (size_t)N * N * N;
     if (!pencils_ready) {
-      if (int rc = zfft_fwd(c, psi, c->nstates)) return rc;
+      if (int rc = zfft_fwd(c, j, psi, c->nstates)) return rc;
     }
     const T* vt;
     if (sizeof(T) == sizeof(double)) {
@@ -495,37 +498,46 @@ struct StateFft {
       CPSTEP_LAUNCH_CHECK();
       vt = reinterpret_cast<const T*>(c->d_vks_t);
     }
-    bool want_v = PShape<T, N>::bytes(c->nplane_x, 1, true) <= PShape<T, N>::LIMIT;
-    int RC = PShape<T, N>::rc_for(c->nplane_x, want_v);
-    size_t smem = PShape<T, N>::bytes(c->nplane_x, RC, want_v);
+    bool want_v = PShape<T, N>::bytes(j.g.nplane_x, 1, true) <= PShape<T, N>::LIMIT;
+    int RC = PShape<T, N>::rc_for(j.g.nplane_x, want_v);
+    size_t smem = PShape<T, N>::bytes(j.g.nplane_x, RC, want_v);
     int ng = plane_groups(c, c->nstates, 1);
     int spg = cdiv(c->nstates, ng);
     ng = cdiv(c->nstates, spg);
     if (int rc = set_smem(k_xy_bwd<T, N, 0>, smem)) return rc;
     k_xy_bwd<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
-        reinterpret_cast<const cplx<T>*>(c->d_pen_a), nullptr, vt,
-        reinterpret_cast<cplx<T>*>(c->d_pen_b), c->geom(), tws<T>(c).x, occ, c->nstates, spg, RC,
+        reinterpret_cast<const cplx<T>*>(j.pen_a), nullptr, vt,
+        reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, occ, c->nstates, spg, RC,
         want_v ? 1 : 0);
     CPSTEP_LAUNCH_CHECK();
     double scale = -2.0 / ((double)N * N * N);
-    if (int rc = zfft_bwd(c, force, psi, eke ? occ : nullptr, c->nstates, scale, 0)) return rc;
+    if (int rc = zfft_bwd(c, j, force, psi, eke ? occ : nullptr, c->nstates, scale, 0)) return rc;
     if (eke) {
-      int nblk = cdiv(c->nlines, ZShape<N>::LB);
+      int nblk = cdiv(j.g.nlines, ZShape<N>::LB);
       k_rowsum<<<cdiv(c->nstates, 128), 128, 0, c->stream>>>(c->d_eke_part, nblk, c->nstates, eke);
       CPSTEP_LAUNCH_CHECK();
     }
     return CPSTEP_OK;
   }
 
-  static int rtog(cpstep_ctx* c, const double* f_r, double* fg, int nstates) {
-    const int RC = PShape<T, N>::rc_for(c->nplane_x, false);
-    const size_t smem = PShape<T, N>::bytes(c->nplane_x, RC, false);
+  // real r -> packed G (sum_r f(r) e^{+iG.r}) times scale, for the job's geometry
+  static int r2g(cpstep_ctx* c, const FftJob& j, const double* f_r, double* fg, int nstates,
+                 double scale) {
+    const int RC = PShape<T, N>::rc_for(j.g.nplane_x, false);
+    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x, RC, false);
     if (int rc = set_smem(k_xy_bwd<T, N, 1>, smem)) return rc;
     k_xy_bwd<T, N, 1><<<dim3(N, nstates), PTHREADS, smem, c->stream>>>(
-        nullptr, f_r, nullptr, reinterpret_cast<cplx<T>*>(c->d_pen_b), c->geom(), tws<T>(c).x,
-        nullptr, nstates, 1, RC, 0);
+        nullptr, f_r, nullptr, reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, nullptr,
+        nstates, 1, RC, 0);
     CPSTEP_LAUNCH_CHECK();
-    return zfft_bwd(c, fg, nullptr, nullptr, nstates, 1.0, 1);
+    return zfft_bwd(c, j, fg, nullptr, nullptr, nstates, scale, 1);
+  }
+
+  static int gtor(cpstep_ctx* c, const double* psi, double* psi_r, int nstates) {
+    return g2r(c, c->state_job(), psi, psi_r, nstates);
+  }
+  static int rtog(cpstep_ctx* c, const double* f_r, double* fg, int nstates) {
+    return r2g(c, c->state_job(), f_r, fg, nstates, 1.0);
   }
 
   static StateFftOps ops() {
@@ -534,6 +546,8 @@ struct StateFft {
     o.vpsi = &vpsi;
     o.gtor = &gtor;
     o.rtog = &rtog;
+    o.g2r = &g2r;
+    o.r2g = &r2g;
     o.lb = ZShape<N>::LB;
     return o;
   }

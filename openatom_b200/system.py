@@ -64,3 +64,102 @@ def loewdin(psi, w):
     evals, evecs = torch.linalg.eigh(S / 2.0)
     T = evecs @ torch.diag(evals.rsqrt()) @ evecs.T
     return (T.to(psi.dtype) @ psi).contiguous()
+
+
+# ---------------------------------------------------------------------------
+# atoms and local pseudopotentials
+
+# Synthetic Gaussian pseudopotentials (Hartree atomic units):
+#   v_loc(g) = -4 pi Z exp(-g^2 rc^2/4)/g^2 + c pi^1.5 b^3 exp(-g^2 b^2/4)
+# i.e. the potential of a Gaussian ionic charge of width rc plus a short-range
+# Gaussian c exp(-r^2/b^2).  The G=0 limit without the Coulomb term is
+# gzvps = pi Z rc^2 + c pi^1.5 b^3.
+SPECIES = {
+    "O": dict(Z=6.0, rc=0.45, c=-2.5, b=0.55),
+    "H": dict(Z=1.0, rc=0.25, c=-0.6, b=0.35),
+}
+
+
+def v_loc(sp, g):
+    p = SPECIES[sp]
+    g = np.asarray(g, dtype=np.float64)
+    g2 = g * g
+    with np.errstate(divide="ignore", invalid="ignore"):
+        coul = np.where(g2 > 0, -4.0 * np.pi * p["Z"] * np.exp(-g2 * p["rc"] ** 2 / 4.0) / g2, 0.0)
+    return coul + p["c"] * np.pi ** 1.5 * p["b"] ** 3 * np.exp(-g2 * p["b"] ** 2 / 4.0)
+
+
+def gzvps(sp):
+    p = SPECIES[sp]
+    return np.pi * p["Z"] * p["rc"] ** 2 + p["c"] * np.pi ** 1.5 * p["b"] ** 3
+
+
+def spline_tables(species, gmin, gmax, nspl=4000):
+    """vps0..vps3 [ntyp, 4, nspl]: cubic coefficients of v_loc on g_i = gmin + i dg,
+    the layout CP_get_vpsnow evaluates (cp_hart_ext.C:459-471)."""
+    from scipy.interpolate import CubicSpline
+    dg = (gmax - gmin) / (nspl - 1)
+    g = gmin + dg * np.arange(nspl + 1)
+    tab = np.zeros((len(species), 4, nspl))
+    for t, sp in enumerate(species):
+        cs = CubicSpline(g, v_loc(sp, g), bc_type="natural")
+        # cs.c[k, i]: coefficient of (x - g_i)^(3-k) on interval i
+        tab[t, 0] = cs.c[3, :nspl]
+        tab[t, 1] = cs.c[2, :nspl]
+        tab[t, 2] = cs.c[1, :nspl]
+        tab[t, 3] = cs.c[0, :nspl]
+    return dict(vps=tab, gmin=gmin, dg=dg, nspl=nspl,
+                gzvps=np.array([gzvps(sp) for sp in species]),
+                q=np.array([SPECIES[sp]["Z"] for sp in species]))
+
+
+def place_atoms(counts, box_len, seed=7, dmin=1.8, max_tries=200000):
+    """Seeded uniform positions with a minimum (periodic) distance; returns
+    (pos [natm, 3], typ [natm], species list)."""
+    rng = np.random.default_rng(seed)
+    species = list(counts.keys())
+    pos, typ = [], []
+    for t, sp in enumerate(species):
+        for _ in range(counts[sp]):
+            for _try in range(max_tries):
+                x = rng.uniform(0.0, box_len, 3)
+                ok = True
+                for y in pos:
+                    d = x - y
+                    d -= box_len * np.round(d / box_len)
+                    if d @ d < dmin * dmin:
+                        ok = False
+                        break
+                if ok:
+                    pos.append(x)
+                    typ.append(t)
+                    break
+            else:
+                raise RuntimeError("could not place atoms at the minimum distance")
+    return np.array(pos), np.array(typ, dtype=np.int32), species
+
+
+class System:
+    """A synthetic water-like CP system of the benchmark shapes."""
+
+    def __init__(self, box_len, ecut_ry, nstates, counts, nfft=None, seed=1234,
+                 alp_ewd=3.5, nspl=4000):
+        from .layout import StateLayout
+        self.layout = StateLayout(box_len, ecut_ry, nfft=nfft)
+        self.box_len = float(box_len)
+        self.ecut_ry = float(ecut_ry)
+        self.nstates = int(nstates)
+        self.seed = seed
+        self.pos, self.typ, self.species = place_atoms(counts, box_len, seed=seed + 1)
+        self.natm = len(self.typ)
+        tpi = 2.0 * np.pi / box_len
+        gmax = np.sqrt(8.0 * 0.5 * ecut_ry) * 4.0 / 3.0 + tpi
+        self.tab = spline_tables(self.species, 0.75 * tpi, gmax, nspl)
+        self.alp_ewd = alp_ewd / box_len  # PINY divides the input alpha by the box side
+        self.occ = np.ones(self.nstates)
+
+    def psi(self, device="cuda"):
+        return make_psi(self.layout, self.nstates, seed=self.seed, device=device)
+
+    def atoms_dict(self):
+        return dict(pos=self.pos, typ=self.typ, q=self.tab["q"])
