@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""Benchmark: CP electronic steps per second on one B200, mixed precision vs the
+plain FP64 path, on the 192-atom water-like system (64 O + 128 H, L = 23.5 bohr,
+128 states, Ecut 70 Ry, 128^3 grid).  Synthetic seeded inputs of that shape.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm prints one JSON line: value = mixed-precision steps/s (whole job, all
+ranks; ranks are independent replicas), the FP64 path's steps/s beside it,
+e2e through the C-ABI host-buffer call (positions in, energies and atom forces
+out every step), the roofline of the state FFT / density / V.psi kernels, the
+CPU baseline (the FP64 oracle on the host cores, bounded sample), clocks and
+the number of library kernel launches in the timed region.
+The reference arm (--impl reference) times the FP64 CPU oracle of the same
+step on the host cores (the reference itself cannot be built here: no
+Charm++, FFTW-2, BLAS or Fortran in the image).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CP steps/sec, mixed vs FP64-plain on one GPU, at <=1e-6 Ha/atom energy error"
+CONFIGS = {
+    # name: box (bohr), Ecut (Ry), states, atoms, grid
+    "water192": dict(box=23.5, ecut=70.0, nstates=128, atoms={"O": 64, "H": 128}, grid=128),
+    "water24": dict(box=12.0, ecut=30.0, nstates=32, atoms={"O": 8, "H": 16}, grid=48),
+    "water768": dict(box=37.2, ecut=70.0, nstates=1024, atoms={"O": 256, "H": 512}, grid=200),
+}
+DT = 5.0          # a.u.
+TAU_FS = 25.0     # CP mass parameter
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def workload_name(name, cfg):
+    return ("CP electronic step, %d atoms (%d O, %d H), L=%g bohr, %d states, Ecut=%g Ry, grid %d^3"
+            % (sum(cfg["atoms"].values()), cfg["atoms"]["O"], cfg["atoms"]["H"], cfg["box"],
+               cfg["nstates"], cfg["ecut"], cfg["grid"]))
+
+
+def peaks():
+    try:
+        with open(PEAKS) as f:
+            p = json.load(f)
+        return p.get("hbm_gbs", 6650.0), "measured", p
+    except Exception:
+        return 6650.0, "fallback", {}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas: each rank runs its own system)
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, ws, dist
+
+
+def max_over_ranks(x, dist):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class Clocks:
+    def __init__(self):
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + q, "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", os.environ.get("LOCAL_RANK", "0")],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax = max(smax, float(f[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        except Exception:
+            pass
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# traffic / flop models of one step (per launch of each phase group)
+
+def models(cfg, lay, nlines, nlines_d, npts_d, c_bytes):
+    S, n = cfg["nstates"], cfg["grid"]
+    npw, nl, nr = lay.npts, nlines, n ** 3
+    # what this design must move for density (phase 0) + V.psi/kinetic (phase 2):
+    # psi read (G->R pass) and re-read (kinetic term), F written: 3 x 16 B per point;
+    # z-pencils written, read by the density pass, read again and written by the
+    # V.psi pass, read by the inverse z pass: 5 x c per pencil element; rho partials,
+    # rho, V in working precision.
+    ours = S * (3 * 16 * npw + 5 * nl * n * c_bytes) + nr * (8 * 5 + c_bytes)
+    # the survey's model of the reference algorithm (psi(r) stored and re-read)
+    survey = S * (2 * npw * c_bytes + 4 * nl * n * c_bytes + 2 * nr * c_bytes // 2) + 2 * nr * 8
+    K = 2 * npw
+    gemm_flops = 4 * 2.0 * S * S * K  # lambda, psi.lambda, S, psi.T
+    return ours, survey, gemm_flops
+
+
+# ---------------------------------------------------------------------------
+
+def run_ours(args, cfg, name, rank, ws, dist):
+    import numpy as np
+    import torch
+    from openatom_b200 import _lib
+    from openatom_b200.context import StepContext
+    from openatom_b200.system import System
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    sysm = System(cfg["box"], cfg["ecut"], cfg["nstates"], cfg["atoms"], nfft=cfg["grid"],
+                  seed=1234 + rank)
+    psi0 = sysm.psi(device=dev)
+    occ = torch.ones(sysm.nstates, dtype=torch.float64, device=dev)
+    L = _lib.lib()
+
+    def make(prec):
+        ctx = StepContext(sysm.layout, sysm.nstates, precision=prec, device=dev)
+        ctx.set_atoms(sysm)
+        ctx.set_cp_mass(TAU_FS, cfg["ecut"])
+        return ctx
+
+    out = {}
+    e_ref = f_ref = None
+    for prec in ("fp64", "mixed"):
+        ctx = make(prec)
+        psi = psi0.clone()
+        v = torch.zeros_like(psi)
+        energies = torch.zeros(_lib.NENERGY, dtype=torch.float64, device=dev)
+        forces = torch.zeros((sysm.natm, 3), dtype=torch.float64, device=dev)
+        # accuracy: first step from the same input, mixed vs FP64
+        ctx.cp_step(psi, v, occ, DT, 1, energies, forces)
+        it, ok = ctx.step_status()
+        first = (energies.cpu().numpy().copy(), forces.cpu().numpy().copy(), ok, it)
+        if prec == "fp64":
+            e_ref, f_ref = first[0], first[1]
+        for w in range(args.warmup):
+            ctx.cp_step(psi, v, occ, DT, 2 + w, energies, forces)
+        torch.cuda.synchronize()
+        ctx_prof = prec == "mixed"
+        if ctx_prof:
+            _lib.call("cpstep_ctx_profile", ctx._h, 1)
+        barrier(dist)
+        clk = Clocks()
+        if prec == "mixed":
+            clk.start()
+        torch.cuda.synchronize()
+        n0 = L.cpstep_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(args.steps):
+            ctx.cp_step(psi, v, occ, DT, 2 + args.warmup + k, energies, forces)
+        e1.record()
+        torch.cuda.synchronize()
+        launches = L.cpstep_launch_count() - n0
+        clocks = clk.stop() if prec == "mixed" else None
+        ms = e0.elapsed_time(e1)
+        ms = max_over_ranks(ms, dist)
+        barrier(dist)
+        phase = None
+        if ctx_prof:
+            import ctypes
+            arr = (ctypes.c_double * 6)()
+            nst = ctypes.c_int()
+            _lib.call("cpstep_phase_times", ctx._h, arr, ctypes.byref(nst))
+            phase = [arr[i] / max(1, nst.value) for i in range(6)]
+            _lib.call("cpstep_ctx_profile", ctx._h, 0)
+        it2, ok2 = ctx.step_status()
+        out[prec] = dict(ms=ms, launches=launches, clocks=clocks, phase=phase, first=first,
+                         ortho_ok=ok2, ortho_iters=it2)
+        if prec == "mixed":
+            # e2e: the reference-facing host-buffer call (positions in, energies/forces out)
+            import ctypes
+            pos = torch.from_numpy(np.ascontiguousarray(sysm.pos)).pin_memory()
+            he = torch.zeros(_lib.NENERGY, dtype=torch.float64).pin_memory()
+            hf = torch.zeros((sysm.natm, 3), dtype=torch.float64).pin_memory()
+            barrier(dist)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for k in range(args.steps):
+                _lib.call("cpstep_cp_step_host", ctx._h, _lib.ptr(psi), _lib.ptr(v), _lib.ptr(occ),
+                          DT, 2 + args.warmup + args.steps + k, ctypes.c_void_p(pos.data_ptr()),
+                          ctypes.c_void_p(he.data_ptr()), ctypes.c_void_p(hf.data_ptr()))
+            t1 = time.perf_counter()
+            e2e_ms = max_over_ranks((t1 - t0) * 1e3, dist)
+            out["e2e"] = dict(ms=e2e_ms, h2d=pos.numel() * 8,
+                              d2h=he.numel() * 8 + hf.numel() * 8)
+        nl, _ = ctx.info()
+        out.setdefault("nlines", nl)
+        out.setdefault("npts_d", ctx.rho_layout()[0].shape[0])
+        ctx.close()
+    return sysm, out, e_ref, f_ref
+
+
+def cpu_baseline(cfg, sample_states=4):
+    """FP64 oracle step time on the host cores, bounded sample, extrapolated.
+
+    FFT/density/V.psi cost is linear in the states (timed on `sample_states`);
+    the density side once; the four PairCalc products and the Ortho iteration
+    at full size (numpy BLAS)."""
+    import numpy as np
+    from oracle import density as OD
+    from oracle import fftpath as OF
+    from oracle import layout as OL
+    from oracle import ortho as OO
+    from openatom_b200.system import System
+    OF.set_workers(os.cpu_count() or 1)
+    sysm = System(cfg["box"], cfg["ecut"], cfg["nstates"], cfg["atoms"], nfft=cfg["grid"])
+    lay = OL.Layout(cfg["box"], cfg["ecut"], grid=cfg["grid"])
+    dlay = OD.density_layout(cfg["box"], cfg["ecut"], cfg["grid"])
+    rng = np.random.default_rng(0)
+    S = cfg["nstates"]
+    sub = (rng.standard_normal((sample_states, lay.npts)) + 1j * rng.standard_normal((sample_states, lay.npts))) * 1e-2
+    vol = cfg["box"] ** 3
+    occ = np.ones(sample_states)
+    t0 = time.perf_counter()
+    rho = OF.density(sub, lay, occ, vol, chunk=sample_states)
+    vks = rho * 0.1
+    fv = OF.vpsi_force(sub, vks, lay, occ, chunk=sample_states)
+    t_fft = (time.perf_counter() - t0) / sample_states
+    t0 = time.perf_counter()
+    vxc, exc, mu = OD.pz_lda(np.abs(rho) + 1e-8, vol)
+    rg = OD.rho_to_g(rho, dlay, vol)
+    natm_s = min(16, sysm.natm)
+    a = sysm.atoms_dict()
+    a_s = dict(pos=a["pos"][:natm_s], typ=a["typ"][:natm_s], q=a["q"])
+    OD.hart_eext(rg, dlay.kx, dlay.ky, dlay.kz, cfg["box"], 0.5 * cfg["ecut"], a_s, sysm.tab,
+                 sysm.alp_ewd)
+    t_dens = (time.perf_counter() - t0)
+    t_dens *= 1.0  # the atom loop part is extrapolated below
+    t_atom = t_dens * (sysm.natm / natm_s - 1.0) * 0.5
+    K = 2 * lay.npts
+    A = rng.standard_normal((S, K))
+    t0 = time.perf_counter()
+    C = A @ A.T
+    A2 = C.T @ A
+    t_gemm = (time.perf_counter() - t0) / 2.0
+    Sm = np.eye(S) * 2.0 + 1e-3 * (C / np.max(np.abs(C)))
+    Sm = 0.5 * (Sm + Sm.T)
+    t0 = time.perf_counter()
+    OO.schulz_tmat(Sm, tol=1e-15, max_iter=10)
+    t_ortho = time.perf_counter() - t0
+    t_step = t_fft * S + t_dens + t_atom + 4 * t_gemm + t_ortho
+    sample = ("%d of %d states through the FFT/density/V.psi path, the density side with %d of %d "
+              "atoms (atom loop extrapolated), full-size PairCalc products and Ortho; "
+              "per-step time = sum, extrapolated linearly in states/atoms"
+              % (sample_states, S, natm_s, sysm.natm))
+    del A2
+    return t_step, sample
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="water192", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    cfg = CONFIGS[args.config]
+    wname = workload_name(args.config, cfg)
+    rank, ws, dist = dist_init()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        ncpu = os.cpu_count() or 1
+        times = []
+        for k in range(args.warmup + args.steps):
+            t, sample = cpu_baseline(cfg)
+            if k >= args.warmup:
+                times.append(t)
+        t = statistics.mean(times)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": 1.0 / t, "unit": "steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wname, "precision": "FP64 CPU oracle",
+                       "parallelism": "host cores"},
+            "cpu_baseline": {"value": 1.0 / t, "unit": "steps/s", "cores": ncpu, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": 1.0 / t, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
+
+    sysm, out, e_ref, f_ref = run_ours(args, cfg, args.config, rank, ws, dist)
+    import numpy as np
+    mixed, fp64 = out["mixed"], out["fp64"]
+    sps_mixed = ws * args.steps / (mixed["ms"] / 1e3)
+    sps_fp64 = ws * args.steps / (fp64["ms"] / 1e3)
+    e_mix, f_mix = mixed["first"][0], mixed["first"][1]
+    err_e = abs(e_mix[8] - e_ref[8]) / sysm.natm
+    err_f = float(np.max(np.abs(f_mix - f_ref)))
+    hbm, peak_kind, pk = peaks()
+    c_bytes = 8  # FP32 complex in the mixed path
+    ours_b, survey_b, gflops = models(cfg, sysm.layout, out["nlines"], None, out["npts_d"], c_bytes)
+    ph = mixed["phase"] or [0.0] * 6
+    fft_ms = ph[0] + ph[2]
+    achieved = ours_b / (fft_ms * 1e-3) / 1e9 if fft_ms > 0 else None
+    gemm_ms = ph[3] + ph[5]
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC,
+        "value": sps_mixed,
+        "unit": "steps/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": mixed["ms"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 FFT/density/V.psi, f64 accumulation, f64 GEMM/Ortho correction",
+        "data": "synthetic",
+        "config": {"workload": wname, "parallelism": "replicas" if ws > 1 else "1 GPU",
+                   "inputs_vs_L2": "inputs larger than L2: psi %.1f MB FP64 per replica"
+                   % (sysm.nstates * sysm.layout.npts * 16 / 1e6),
+                   "precision": "mixed", "dt_au": DT},
+        "fp64_steps_per_sec": sps_fp64,
+        "fp64_ms_per_step": fp64["ms"] / args.steps,
+        "mixed_over_fp64": sps_mixed / sps_fp64,
+        "accuracy_vs_fp64": {"energy_Ha_per_atom": err_e, "local_force_Ha_per_bohr": err_f,
+                             "ortho_converged": bool(mixed["ortho_ok"])},
+        "phase_ms_mixed": {"density": ph[0], "vks": ph[1], "vpsi_kinetic": ph[2],
+                           "lambda": ph[3], "integrate": ph[4], "ortho_psiT": ph[5]},
+        "roofline": {"bound": "hbm", "kernel": "state FFT + density + V.psi (phases 0+2)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                     "algorithmic_bytes": ours_b, "survey_model_bytes": survey_b,
+                     "peak_kind": peak_kind},
+        "roofline_paircalc": {"bound": "fp64", "flops": gflops,
+                              "achieved_tflops": gflops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None},
+        "gpu_launches": int(mixed["launches"]),
+        "clocks": mixed["clocks"],
+        "e2e": {"value": ws * args.steps / (out["e2e"]["ms"] / 1e3), "unit": "steps/s",
+                "h2d_bytes_per_step": out["e2e"]["h2d"], "d2h_bytes_per_step": out["e2e"]["d2h"]},
+    }
+    if ws == 1 and not args.no_cpu_baseline:
+        t, sample = cpu_baseline(cfg)
+        line["cpu_baseline"] = {"value": 1.0 / t, "unit": "steps/s", "cores": os.cpu_count() or 1,
+                                "kind": "port", "sample": sample}
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -49,6 +49,7 @@ extern "C" {
 #define CPSTEP_E_KE 6      /* EKE        (sum of CP_eke_calc)                 */
 #define CPSTEP_E_NL 7      /* ENL        (EES non-local)                      */
 #define CPSTEP_E_TOT 8     /* ELEC_ENERGY_TOT = EKE+ENL+EHART+EExt+EEXC       */
+#define CPSTEP_E_FICT 9    /* fictitious kinetic energy (get_fictKE)          */
 #define CPSTEP_NENERGY 12
 
 #define CPSTEP_PREC_FP64 0    /* plain FP64 path: the drop-in */
@@ -61,6 +62,22 @@ CPSTEP_API int cpstep_version(void);
 
 /* Text of the last error on this thread ("" if none). */
 CPSTEP_API const char* cpstep_last_error(void);
+
+/* Kernels the library has launched since it was loaded (all contexts). */
+CPSTEP_API unsigned long long cpstep_launch_count(void);
+
+/* Phases of cpstep_cp_step timed with CUDA events on the context's stream when
+ * profiling is on (cpstep_ctx_profile(ctx, 1) resets the sums):
+ *   0 density (state FFTs G->R, rho)   1 V_KS (XC, rho FFT, Hartree/local/Ewald)
+ *   2 V.psi + kinetic (state FFTs R->G) 3 lambda + constraint (PairCalc)
+ *   4 integrate                         5 S + Ortho + psi.T (PairCalc, Ortho)
+ * cpstep_phase_times returns the summed milliseconds per phase and the number
+ * of profiled steps (synchronises the stream).  The Ortho S->T iteration has
+ * no counterpart timer in the reference beyond TimeKeeper's substeps
+ * (main/TimeKeeper.h:1-181). */
+#define CPSTEP_NPHASE 6
+CPSTEP_API int cpstep_ctx_profile(cpstep_ctx* ctx, int enable);
+CPSTEP_API int cpstep_phase_times(cpstep_ctx* ctx, double* ms, int* steps);
 
 /* ---------------------------------------------------------------------------
  * G-vector layout (host, no GPU needed).
@@ -249,6 +266,52 @@ CPSTEP_API int cpstep_hart_eext(cpstep_ctx* ctx, const double* d_rhog, double* d
 CPSTEP_API int cpstep_vks_fft_g2r(cpstep_ctx* ctx, const double* d_vksg, double* d_v_r);
 CPSTEP_API int cpstep_vks_from_rho(cpstep_ctx* ctx, const double* d_rho_r, double* d_vks_r,
                                    double* d_energies, double* d_force);
+
+/* ---------------------------------------------------------------------------
+ * Integrator and the fused electronic step.
+ *
+ * cpstep_set_cp_mass: CP coefficient masses of set_cpmass (src_piny_physics_v1.0/
+ *   interface/cp_ewald/set_cp_ewald.C:32-74): cmass0 = 4 tau^2 CP_EMAGIC with
+ *   tau = tau_fs / TIME_CONV, scaled by (g^2/2)/(cut/2) above cut (Ry), G=0 halved.
+ * cpstep_cp_integrate: velocity Verlet of CPINTEGRATE::CP_integrate_dyn /
+ *   cp_evolve_vel / get_fictKE (cp_integrate/cp_dynamics.C:29-258) on all
+ *   states, without the isokinetic Nose-Hoover chains: second half kick of the
+ *   previous step when iteration > 1, fictitious KE (d_fict_ke, may be NULL),
+ *   first half kick, psi += v dt, then the redundant lower Gx=0 half is
+ *   overwritten by the conjugate of its partner (sendRedPsi/unpackRedPsi,
+ *   CP_State_GSpacePlane.C:2862-3061).  d_force: the constrained force.
+ * cpstep_cp_step: one electronic step on orthonormal psi (S = 2 I):
+ *   rho -> V_KS (XC, Hartree, local, Ewald) -> F = V.psi + kinetic force ->
+ *   lambda = <psi|F>, F <- F - wpt/2 psi.lambda -> Verlet -> S -> T = (S/2)^-1/2
+ *   -> psi <- psi.T.  d_energies (CPSTEP_NENERGY doubles, device) receives
+ *   every slot; d_atom_force (may be NULL) the local + Ewald atom forces.
+ *   Asynchronous: the Ortho convergence of the step is read by cpstep_step_status.
+ * cpstep_step_status: iterations and convergence flag of the last Ortho launch
+ *   (synchronises the context's stream).
+ */
+CPSTEP_API int cpstep_set_cp_mass(cpstep_ctx* ctx, double tau_fs, double cut_ry);
+CPSTEP_API int cpstep_cp_integrate(cpstep_ctx* ctx, const double* d_force, double* d_psi,
+                                   double* d_vpsi, double dt, int iteration, double* d_fict_ke);
+CPSTEP_API int cpstep_cp_step(cpstep_ctx* ctx, double* d_psi, double* d_vpsi,
+                              const double* d_occ, double dt, int iteration,
+                              double* d_energies, double* d_atom_force);
+CPSTEP_API int cpstep_step_status(cpstep_ctx* ctx, int* ortho_iters, int* converged);
+
+/*
+ * cpstep_set_positions: new atom positions from host memory (natm x 3, bohr),
+ *   copied on the context's stream (pinned memory makes it asynchronous); the
+ *   structure-factor tables follow on the device.
+ * cpstep_cp_step_host: the step as the reference's driver calls it, with host
+ *   buffers for what crosses the boundary every MD step: positions in (h_pos,
+ *   may be NULL to keep the current ones), energies (CPSTEP_NENERGY doubles)
+ *   and atom forces (natm x 3, may be NULL) out.  The coefficients stay on the
+ *   device between steps.  Synchronous.
+ */
+CPSTEP_API int cpstep_set_positions(cpstep_ctx* ctx, const double* h_pos);
+CPSTEP_API int cpstep_cp_step_host(cpstep_ctx* ctx, double* d_psi, double* d_vpsi,
+                                   const double* d_occ, double dt, int iteration,
+                                   const double* h_pos, double* h_energies,
+                                   double* h_atom_force);
 
 #ifdef __cplusplus
 }

@@ -26,6 +26,9 @@ _vp = ctypes.c_void_p
 SIGNATURES = {
     "cpstep_version": (ctypes.c_int, []),
     "cpstep_last_error": (ctypes.c_char_p, []),
+    "cpstep_launch_count": (ctypes.c_ulonglong, []),
+    "cpstep_ctx_profile": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "cpstep_phase_times": (ctypes.c_int, [_vp, _c_dbl_p, _c_int_p]),
     "cpstep_layout_sizes": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, _c_int_p, _c_int_p,
                                            _c_int_p, _c_int_p]),
     "cpstep_layout_build": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_int,
@@ -67,9 +70,18 @@ SIGNATURES = {
     "cpstep_hart_eext": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "cpstep_vks_fft_g2r": (ctypes.c_int, [_vp, _vp, _vp]),
     "cpstep_vks_from_rho": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cpstep_set_cp_mass": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
+    "cpstep_cp_integrate": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int,
+                                           _vp]),
+    "cpstep_cp_step": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int, _vp,
+                                      _vp]),
+    "cpstep_step_status": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
+    "cpstep_set_positions": (ctypes.c_int, [_vp, _vp]),
+    "cpstep_cp_step_host": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int,
+                                           _vp, _vp, _vp]),
 }
 NENERGY = 12
-E_EXC, E_MUXC, E_HART, E_EXT, E_EWD, E_EXT_G0, E_KE, E_NL, E_TOT = range(9)
+E_EXC, E_MUXC, E_HART, E_EXT, E_EWD, E_EXT_G0, E_KE, E_NL, E_TOT, E_FICT = range(10)
 
 
 class CpstepError(RuntimeError):

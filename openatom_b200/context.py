@@ -239,3 +239,33 @@ class StepContext:
         f = torch.zeros((self.natm, 3), dtype=torch.float64, device=self.device) if forces else None
         _lib.call("cpstep_vks_from_rho", self._h, ptr(rho), ptr(v), ptr(e), ptr(f))
         return v, e, f
+
+    # -- electronic step -----------------------------------------------------
+    def set_cp_mass(self, tau_fs=25.0, cut_ry=None):
+        """set_cpmass: CP coefficient masses (cut defaults to the state cutoff)."""
+        cut = self.layout.ecut_ry if cut_ry is None else cut_ry
+        _lib.call("cpstep_set_cp_mass", self._h, float(tau_fs), float(cut))
+
+    def cp_integrate(self, force, psi, vpsi, dt, iteration):
+        self._sync_stream()
+        ke = torch.zeros(1, dtype=torch.float64, device=self.device)
+        _lib.call("cpstep_cp_integrate", self._h, ptr(force), ptr(psi), ptr(vpsi), float(dt),
+                  int(iteration), ptr(ke))
+        return ke
+
+    def cp_step(self, psi, vpsi, occ, dt, iteration, energies=None, atom_force=None):
+        """One electronic step in place on psi / vpsi; returns (energies, atom forces)."""
+        self._sync_stream()
+        self._chk_psi(psi)
+        e = self._energies() if energies is None else energies
+        f = atom_force
+        if f is None:
+            f = torch.zeros((self.natm, 3), dtype=torch.float64, device=self.device)
+        _lib.call("cpstep_cp_step", self._h, ptr(psi), ptr(vpsi), ptr(occ), float(dt),
+                  int(iteration), ptr(e), ptr(f))
+        return e, f
+
+    def step_status(self):
+        it, ok = ctypes.c_int(), ctypes.c_int()
+        _lib.call("cpstep_step_status", self._h, ctypes.byref(it), ctypes.byref(ok))
+        return it.value, bool(ok.value)

@@ -9,6 +9,7 @@
 #include "ctx.cuh"
 
 static thread_local char g_err[1024] = {0};
+unsigned long long g_cpstep_launches = 0;
 
 void cpstep_set_error(const char* fmt, ...) {
   va_list ap;
@@ -104,9 +105,50 @@ __global__ void k_rowsum2(const double* __restrict__ part, int ncol, int nrow,
 
 }  // namespace
 
+int prof_fold(cpstep_ctx* c) {
+  if (c->prof_pending == 0) return CPSTEP_OK;
+  const int W = CPSTEP_NPHASE + 1;
+  CPSTEP_CUDA_TRY(cudaEventSynchronize(c->prof_ev[(size_t)(c->prof_pending - 1) * W + CPSTEP_NPHASE]));
+  for (int s = 0; s < c->prof_pending; ++s)
+    for (int k = 0; k < CPSTEP_NPHASE; ++k) {
+      float ms = 0.f;
+      CPSTEP_CUDA_TRY(cudaEventElapsedTime(&ms, c->prof_ev[(size_t)s * W + k],
+                                           c->prof_ev[(size_t)s * W + k + 1]));
+      c->prof_ms[k] += ms;
+    }
+  c->prof_steps += c->prof_pending;
+  c->prof_pending = 0;
+  return CPSTEP_OK;
+}
+
 extern "C" {
 
 int cpstep_version(void) { return 100; }
+
+unsigned long long cpstep_launch_count(void) {
+  return __atomic_load_n(&g_cpstep_launches, __ATOMIC_RELAXED);
+}
+
+int cpstep_ctx_profile(cpstep_ctx* c, int enable) {
+  if (!c) return CPSTEP_ERR_ARG;
+  if (enable && c->prof_ev.empty()) {
+    c->prof_ev.resize((size_t)cpstep_ctx::PROF_RING * (CPSTEP_NPHASE + 1));
+    for (auto& e : c->prof_ev) CPSTEP_CUDA_TRY(cudaEventCreate(&e));
+  }
+  c->profile = enable ? 1 : 0;
+  for (int i = 0; i < CPSTEP_NPHASE; ++i) c->prof_ms[i] = 0.0;
+  c->prof_steps = 0;
+  c->prof_pending = 0;
+  return CPSTEP_OK;
+}
+
+int cpstep_phase_times(cpstep_ctx* c, double* ms, int* steps) {
+  if (!c || !ms) return CPSTEP_ERR_ARG;
+  if (int rc = prof_fold(c)) return rc;
+  for (int i = 0; i < CPSTEP_NPHASE; ++i) ms[i] = c->prof_ms[i];
+  if (steps) *steps = c->prof_steps;
+  return CPSTEP_OK;
+}
 
 const char* cpstep_last_error(void) { return g_err; }
 
@@ -206,6 +248,7 @@ int cpstep_ctx_create(cpstep_ctx** out, int precision, int nstates, int npts, co
   if (!rc) rc = upload(&c->d_wpt, wpt.data(), npts);
   if (!rc) rc = statefft_init(c);
   if (!rc) rc = rho_init(c, std::fabs(hmat[0]), ecut_ry);
+  if (!rc) rc = step_init_classes(c);
   if (rc) {
     cpstep_ctx_destroy(c);
     return rc;
@@ -221,7 +264,10 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
   cudaFree(c->d_kx); cudaFree(c->d_ky); cudaFree(c->d_kz);
   cudaFree(c->d_g2); cudaFree(c->d_wpt);
   cudaFree(c->d_pc_part); cudaFree(c->d_ortho_ws); cudaFree(c->d_hmati);
+  cudaFree(c->d_force_atoms);
+  for (auto& e : c->prof_ev) cudaEventDestroy(e);
   rho_free(c);
+  step_free(c);
   statefft_free(c);
   delete c;
   return CPSTEP_OK;
@@ -383,6 +429,68 @@ int cpstep_vks_from_rho(cpstep_ctx* c, const double* d_rho_r, double* d_vks_r,
   if (int rc = rho_r2g(c, d_rho_r)) return rc;
   if (int rc = rho_hart(c, d_energies, d_force)) return rc;
   return rho_vks_r(c, d_vks_r);
+}
+
+int cpstep_set_cp_mass(cpstep_ctx* c, double tau_fs, double cut_ry) {
+  if (!c || !(tau_fs > 0) || !(cut_ry > 0)) return CPSTEP_ERR_ARG;
+  return step_set_mass(c, tau_fs, cut_ry);
+}
+
+int cpstep_cp_integrate(cpstep_ctx* c, const double* d_force, double* d_psi, double* d_vpsi,
+                        double dt, int iteration, double* d_fict_ke) {
+  if (!c || !d_force || !d_psi || !d_vpsi || iteration < 1) return CPSTEP_ERR_ARG;
+  return step_integrate(c, d_force, d_psi, d_vpsi, dt, iteration, d_fict_ke);
+}
+
+int cpstep_cp_step(cpstep_ctx* c, double* d_psi, double* d_vpsi, const double* d_occ, double dt,
+                   int iteration, double* d_energies, double* d_atom_force) {
+  if (!c || !d_psi || !d_vpsi || !d_occ || !d_energies || iteration < 1) return CPSTEP_ERR_ARG;
+  if (c->atoms.natm <= 0 || !c->d_cmass) {
+    cpstep_set_error("cp_step: atoms and CP masses must be set first");
+    return CPSTEP_ERR_STATE;
+  }
+  return step_run(c, d_psi, d_vpsi, d_occ, dt, iteration, d_energies, d_atom_force, 0);
+}
+
+int cpstep_set_positions(cpstep_ctx* c, const double* h_pos) {
+  if (!c || !h_pos) return CPSTEP_ERR_ARG;
+  return atoms_set_positions(c, h_pos);
+}
+
+int cpstep_cp_step_host(cpstep_ctx* c, double* d_psi, double* d_vpsi, const double* d_occ,
+                        double dt, int iteration, const double* h_pos, double* h_energies,
+                        double* h_atom_force) {
+  if (!c || !d_psi || !d_vpsi || !d_occ || !h_energies || iteration < 1) return CPSTEP_ERR_ARG;
+  if (h_pos) {
+    if (int rc = atoms_set_positions(c, h_pos)) return rc;
+  }
+  if (!c->d_force_atoms) {
+    CPSTEP_CUDA_TRY(cudaMalloc(&c->d_force_atoms, sizeof(double) * 3 * std::max(1, c->atoms.natm)));
+  }
+  if (int rc = cpstep_cp_step(c, d_psi, d_vpsi, d_occ, dt, iteration, c->d_energies,
+                              h_atom_force ? c->d_force_atoms : nullptr))
+    return rc;
+  CPSTEP_CUDA_TRY(cudaMemcpyAsync(h_energies, c->d_energies, sizeof(double) * CPSTEP_NENERGY,
+                                  cudaMemcpyDeviceToHost, c->stream));
+  if (h_atom_force)
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(h_atom_force, c->d_force_atoms,
+                                    sizeof(double) * 3 * c->atoms.natm, cudaMemcpyDeviceToHost,
+                                    c->stream));
+  CPSTEP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CPSTEP_OK;
+}
+
+int cpstep_step_status(cpstep_ctx* c, int* iters, int* converged) {
+  if (!c) return CPSTEP_ERR_ARG;
+  int st[2] = {0, 0};
+  if (c->d_ortho_status) {
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(st, c->d_ortho_status, sizeof(st), cudaMemcpyDeviceToHost,
+                                    c->stream));
+  }
+  CPSTEP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (iters) *iters = st[0];
+  if (converged) *converged = st[1];
+  return CPSTEP_OK;
 }
 
 }  // extern "C"

@@ -15,8 +15,11 @@
     }                                                                           \
   } while (0)
 
+extern unsigned long long g_cpstep_launches;  // kernels launched by the library
+
 #define CPSTEP_LAUNCH_CHECK()                                                   \
   do {                                                                          \
+    __atomic_add_fetch(&g_cpstep_launches, 1ull, __ATOMIC_RELAXED);             \
     cudaError_t _e = cudaGetLastError();                                        \
     if (_e != cudaSuccess) {                                                    \
       cpstep_set_error("%s:%d: launch: %s", __FILE__, __LINE__,                 \

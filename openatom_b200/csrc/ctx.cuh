@@ -65,6 +65,7 @@ struct AtomData {
   int kxm = 0, kym = 0, kzm = 0;
   double2 *ex = nullptr, *ey = nullptr, *ez = nullptr;
   double* fpart = nullptr;
+  double* pos = nullptr;  // staging for cpstep_set_positions
 };
 
 template <typename T>
@@ -101,6 +102,27 @@ struct cpstep_ctx {
   AtomData atoms;
   int rho_izero = -1;
   double* d_energies = nullptr;  // [CPSTEP_NENERGY]
+  // electronic step
+  int* d_cls = nullptr;      // point class (0 redundant Gx=0, 1 G=0, 2 unique Gx=0, 3 Gx>0)
+  int* d_red_idx = nullptr;  // redundant points and their stored partners
+  int* d_red_src = nullptr;
+  int nred = 0;
+  double* d_cmass = nullptr;
+  int nblk_ke = 0;
+  double* d_step_part = nullptr;
+  double *d_lambda = nullptr, *d_smat = nullptr, *d_tmat = nullptr;
+  double *d_psi_tmp = nullptr, *d_rho = nullptr, *d_vks = nullptr, *d_eke = nullptr;
+  double* d_force = nullptr;
+  double* d_force_atoms = nullptr;  // staging of cpstep_cp_step_host
+  // phase timing (cpstep_ctx_profile): events recorded on the context's stream
+  // (a ring of PROF_RING steps' events, folded into prof_ms when it fills or
+  // when cpstep_phase_times is called, so profiling adds no per-step sync)
+  static constexpr int PROF_RING = 64;
+  int profile = 0;
+  std::vector<cudaEvent_t> prof_ev;  // [PROF_RING][CPSTEP_NPHASE + 1]
+  int prof_pending = 0;
+  double prof_ms[CPSTEP_NPHASE] = {};
+  int prof_steps = 0;
   double* d_hmati = nullptr;
   Twiddles<double> tw64;
   Twiddles<float> tw32;
@@ -157,6 +179,7 @@ FftJob rho_job(const cpstep_ctx* c);
 int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* pos,
               const double* q, int nspl, double gmin, double dg, const double* vps,
               const double* gzvps, double alp_ewd);
+int atoms_set_positions(cpstep_ctx* c, const double* h_pos);
 int rho_xc(cpstep_ctx* c, const double* rho_r, double* vxc, double* energies);
 int rho_r2g(cpstep_ctx* c, const double* rho_r);
 int rho_hart(cpstep_ctx* c, double* energies, double* force);
@@ -171,6 +194,22 @@ int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
 int dgemm_launch(cudaStream_t s, int ta, int tb, int m, int n, int k, double alpha,
                  const double* A, int lda, const double* B, int ldb, double beta, double* C,
                  int ldc);
+
+int pc_backmul_w_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
+                        double* out, int ldo, int nout, int nin, int K, double alpha, double beta,
+                        const double* w);
+
+// api.cu
+int prof_fold(cpstep_ctx* c);
+
+// step.cu
+int step_init_classes(cpstep_ctx* c);
+void step_free(cpstep_ctx* c);
+int step_set_mass(cpstep_ctx* c, double tau_fs, double cut_ry);
+int step_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi, double dt,
+                   int iteration, double* d_fict_ke);
+int step_run(cpstep_ctx* c, double* psi, double* vpsi, const double* occ, double dt,
+             int iteration, double* energies, double* atom_force, int ortho_check);
 
 // ortho.cu
 int ortho_tmat(cpstep_ctx* c, const double* S, double* T, int n, int mixed, int scale,

@@ -86,12 +86,12 @@ __global__ void k_splitk_reduce(const double* __restrict__ part, int nsplit, int
   *c = alpha * s + (beta == 0.0 ? 0.0 : beta * (*c));
 }
 
-// out[i][p] = alpha * sum_j Mcm[j + i*ldm] * in[j][p] + beta * out[i][p]
-// (i < nout, j < nin, p < K; in/out row-major with ld = ldi / ldo)
+// out[i][p] = alpha * w[p/2] * sum_j Mcm[j + i*ldm] * in[j][p] + beta * out[i][p]
+// (i < nout, j < nin, p < K; in/out row-major with ld = ldi / ldo; w optional)
 __global__ void __launch_bounds__(NT)
 k_backmul(const double* __restrict__ Mcm, int ldm, const double* __restrict__ in, int ldi,
           double* __restrict__ out, int ldo, int nout, int nin, int K, double alpha,
-          double beta) {
+          double beta, const double* __restrict__ w) {
   __shared__ double Ms[BK][BM + 1];
   __shared__ double Is[BK][BN + 1];
   const int p0 = blockIdx.x * BN, i0 = blockIdx.y * BM;
@@ -131,7 +131,8 @@ k_backmul(const double* __restrict__ Mcm, int ldm, const double* __restrict__ in
       int i = i0 + ty + 16 * q, p = p0 + tx + 16 * r;
       if (i < nout && p < K) {
         double* o = out + (size_t)i * ldo + p;
-        *o = alpha * acc[q][r] + (beta == 0.0 ? 0.0 : beta * (*o));
+        double a = w ? alpha * w[p >> 1] : alpha;
+        *o = a * acc[q][r] + (beta == 0.0 ? 0.0 : beta * (*o));
       }
     }
 }
@@ -222,7 +223,18 @@ int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
                       double* out, int ldo, int nout, int nin, int K, double alpha, double beta) {
   using namespace pcalc;
   dim3 grid(cdiv(K, BN), cdiv(nout, BM));
-  k_backmul<<<grid, NT, 0, c->stream>>>(Mcm, ldm, in, ldi, out, ldo, nout, nin, K, alpha, beta);
+  k_backmul<<<grid, NT, 0, c->stream>>>(Mcm, ldm, in, ldi, out, ldo, nout, nin, K, alpha, beta,
+                                        nullptr);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
+int pc_backmul_w_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
+                        double* out, int ldo, int nout, int nin, int K, double alpha, double beta,
+                        const double* w) {
+  using namespace pcalc;
+  dim3 grid(cdiv(K, BN), cdiv(nout, BM));
+  k_backmul<<<grid, NT, 0, c->stream>>>(Mcm, ldm, in, ldi, out, ldo, nout, nin, K, alpha, beta, w);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }

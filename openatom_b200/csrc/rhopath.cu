@@ -108,6 +108,16 @@ __global__ void k_phase(const double* __restrict__ frac, int natm, int kxm, int 
   }
 }
 
+// fractional coordinates s = hmati R from Cartesian positions
+__global__ void k_frac(const double* __restrict__ pos, const double* __restrict__ hmati, int natm,
+                       double* __restrict__ frac) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natm) return;
+  const double* R = pos + 3 * a;
+  for (int d = 0; d < 3; ++d)
+    frac[3 * a + d] = hmati[d] * R[0] + hmati[d + 3] * R[1] + hmati[d + 6] * R[2];
+}
+
 __device__ __forceinline__ double2 phase(const Atoms& A, int a, int kx, int ky, int kz) {
   double2 x = A.ex[(size_t)kx * A.natm + a];
   double2 y = A.ey[(size_t)(ky + A.kym) * A.natm + a];
@@ -347,7 +357,7 @@ void rho_free(cpstep_ctx* c) {
   cudaFree(c->d_energies);
   AtomData& a = c->atoms;
   cudaFree(a.typ); cudaFree(a.frac); cudaFree(a.q); cudaFree(a.vps); cudaFree(a.gzvps);
-  cudaFree(a.ex); cudaFree(a.ey); cudaFree(a.ez); cudaFree(a.fpart);
+  cudaFree(a.ex); cudaFree(a.ey); cudaFree(a.ez); cudaFree(a.fpart); cudaFree(a.pos);
 }
 
 FftJob rho_job(const cpstep_ctx* c) {
@@ -368,7 +378,7 @@ int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* p
               const double* gzvps, double alp_ewd) {
   AtomData& a = c->atoms;
   cudaFree(a.typ); cudaFree(a.frac); cudaFree(a.q); cudaFree(a.vps); cudaFree(a.gzvps);
-  cudaFree(a.ex); cudaFree(a.ey); cudaFree(a.ez); cudaFree(a.fpart);
+  cudaFree(a.ex); cudaFree(a.ey); cudaFree(a.ez); cudaFree(a.fpart); cudaFree(a.pos);
   a = AtomData();
   std::vector<int> t(typ, typ + natm);
   for (int v : t)
@@ -406,7 +416,7 @@ int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* p
   rho::k_phase<<<cdiv(natm, 128), 128, 0, c->stream>>>(a.frac, natm, a.kxm, a.kym, a.kzm, a.ex,
                                                         a.ey, a.ez);
   CPSTEP_LAUNCH_CHECK();
-  CPSTEP_CUDA_TRY(cudaMalloc(&c->d_hmati, sizeof(double) * 9));
+  if (!c->d_hmati) CPSTEP_CUDA_TRY(cudaMalloc(&c->d_hmati, sizeof(double) * 9));
   CPSTEP_CUDA_TRY(cudaMemcpy(c->d_hmati, c->hmati, sizeof(double) * 9, cudaMemcpyHostToDevice));
   return CPSTEP_OK;
 }
@@ -418,6 +428,25 @@ static rho::Atoms atoms_view(const cpstep_ctx* c) {
   A.gzvps = a.gzvps; A.nspl = a.nspl; A.gmin = a.gmin; A.dg = a.dg;
   A.kxm = a.kxm; A.kym = a.kym; A.kzm = a.kzm; A.ex = a.ex; A.ey = a.ey; A.ez = a.ez;
   return A;
+}
+
+// New atom positions (host, natm x 3): queued H2D copy, fractional
+// coordinates and phase tables on the context's stream.
+int atoms_set_positions(cpstep_ctx* c, const double* h_pos) {
+  AtomData& a = c->atoms;
+  if (a.natm <= 0) {
+    cpstep_set_error("set_positions: no atoms set");
+    return CPSTEP_ERR_STATE;
+  }
+  if (!a.pos) CPSTEP_CUDA_TRY(cudaMalloc(&a.pos, sizeof(double) * 3 * a.natm));
+  CPSTEP_CUDA_TRY(cudaMemcpyAsync(a.pos, h_pos, sizeof(double) * 3 * a.natm,
+                                  cudaMemcpyHostToDevice, c->stream));
+  rho::k_frac<<<cdiv(a.natm, 128), 128, 0, c->stream>>>(a.pos, c->d_hmati, a.natm, a.frac);
+  CPSTEP_LAUNCH_CHECK();
+  rho::k_phase<<<cdiv(a.natm, 128), 128, 0, c->stream>>>(a.frac, a.natm, a.kxm, a.kym, a.kzm,
+                                                          a.ex, a.ey, a.ez);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
 }
 
 // E_xc, muxc -> energies[EXC], [MUXC]; vxc written to out

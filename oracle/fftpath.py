@@ -21,6 +21,15 @@ exp(-2 pi i jk/n), FFTW_BACKWARD exp(+2 pi i jk/n), both unnormalised;
 * kinetic energy           CP_eke_calc cp_eke.C:30-140
 """
 import numpy as np
+import scipy.fft as sfft
+
+_WORKERS = 1
+
+
+def set_workers(n):
+    """Threads the oracle's FFTs may use (pocketfft via scipy.fft)."""
+    global _WORKERS
+    _WORKERS = max(1, int(n))
 
 
 def expand(psi, lay):
@@ -54,23 +63,23 @@ def state_g_to_r(psi, lay):
     """Packed psi(G) [S, npts] -> real psi(r) [S, nz, ny, nx] (FP64)."""
     n = lay.n
     t = lay.line_tables()
-    z = np.fft.fft(expand(psi, lay), axis=2)               # FFTW_FORWARD along z
+    z = sfft.fft(expand(psi, lay), axis=2, workers=_WORKERS)               # FFTW_FORWARD along z
     S = psi.shape[0]
     plane = np.zeros((S, n, n, n // 2 + 1), dtype=np.complex128)   # [s, z, y, x]
     plane[:, :, t['y'], t['x']] = np.transpose(z, (0, 2, 1))
-    plane = np.fft.fft(plane, axis=2)                      # FFTW_FORWARD along y
+    plane = sfft.fft(plane, axis=2, workers=_WORKERS)      # FFTW_FORWARD along y
     plane = np.conj(plane)                                 # imag flip
-    return np.fft.irfft(plane, n=n, axis=3) * n            # rfftw C2R (+i, unnormalised)
+    return sfft.irfft(plane, n=n, axis=3, workers=_WORKERS) * n  # rfftw C2R (+i, unnormalised)
 
 
 def state_r_to_g(f, lay):
     """Real f(r) [S, nz, ny, nx] -> packed F(G) [S, npts], unscaled (FP64)."""
     n = lay.n
     t = lay.line_tables()
-    X = np.conj(np.fft.rfft(f, axis=3))                    # rfftw R2C (-i), imag flip
-    X = np.fft.ifft(X, axis=2) * n                         # FFTW_BACKWARD along y
+    X = np.conj(sfft.rfft(f, axis=3, workers=_WORKERS))    # rfftw R2C (-i), imag flip
+    X = sfft.ifft(X, axis=2, workers=_WORKERS) * n         # FFTW_BACKWARD along y
     lines = np.transpose(X[:, :, t['y'], t['x']], (0, 2, 1))   # [s, line, z]
-    lines = np.fft.ifft(lines, axis=2) * n                 # FFTW_BACKWARD along z
+    lines = sfft.ifft(lines, axis=2, workers=_WORKERS) * n  # FFTW_BACKWARD along z
     return pack(lines, lay)
 
 

@@ -9,7 +9,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     txt = open(os.path.join(ROOT, "include", "cpstep.h")).read()
-    return sorted(set(re.findall(r"CPSTEP_API\s+(?:const\s+)?\w+\*?\s+\**(cpstep_\w+)\s*\(", txt)))
+    return sorted(set(re.findall(r"CPSTEP_API\s+[\w\s\*]*?\b(cpstep_\w+)\s*\(", txt)))
 
 
 def test_header_declares_entry_points():

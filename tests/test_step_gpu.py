@@ -1,0 +1,82 @@
+"""The fused CP electronic step on the GPU vs the FP64 oracle step.
+
+FP64 path: energies to 1e-10 relative, coefficients to 1e-9.
+Mixed path vs the FP64 oracle: energy per atom <= 1e-6 Ha, local atom force
+<= 1e-5 Ha/bohr, |psi^T psi - 2I| <= 1e-10 (FP64 Ortho correction).
+"""
+import numpy as np
+import pytest
+
+from conftest import cuda_ok
+
+pytestmark = pytest.mark.gpu
+
+DT = 5.0
+
+
+@pytest.fixture(scope="module")
+def stepsys():
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    import torch
+    from oracle import density as OD
+    from oracle import layout as OL
+    from oracle import step as OS
+    from openatom_b200.system import System
+    sysm = System(12.0, 30.0, 16, {"O": 4, "H": 8}, nfft=48)
+    lay = OL.Layout(12.0, 30.0, grid=48)
+    dlay = OD.density_layout(12.0, 30.0, 48)
+    psi = sysm.psi()
+    occ = torch.ones(sysm.nstates, dtype=torch.float64, device="cuda")
+    cmass = OS.cp_mass(lay, 25.0, 30.0)
+    pn = psi.cpu().numpy()
+    v0 = np.zeros_like(pn)
+    p1, v1, en1, f1, aux1 = OS.cp_step(pn, v0, np.ones(sysm.nstates), sysm, lay, dlay, cmass, DT, 1)
+    p2, v2, en2, f2, aux2 = OS.cp_step(p1, v1, np.ones(sysm.nstates), sysm, lay, dlay, cmass, DT, 2)
+    return dict(sys=sysm, psi=psi, occ=occ, ref=[(p1, v1, en1, f1), (p2, v2, en2, f2)])
+
+
+def run(stepsys, precision):
+    import torch
+    from openatom_b200.context import StepContext
+    s = stepsys["sys"]
+    ctx = StepContext(s.layout, s.nstates, precision=precision)
+    ctx.set_atoms(s)
+    ctx.set_cp_mass(25.0, 30.0)
+    psi = stepsys["psi"].clone()
+    v = torch.zeros_like(psi)
+    out = []
+    for it in (1, 2):
+        e, f = ctx.cp_step(psi, v, stepsys["occ"], DT, it)
+        iters, ok = ctx.step_status()
+        out.append((psi.cpu().numpy().copy(), v.cpu().numpy().copy(), e.cpu().numpy().copy(),
+                    f.cpu().numpy().copy(), ok))
+    ctx.close()
+    return out
+
+
+NAMES = [("EXC", 0), ("EHART", 2), ("EEXT", 3), ("EKE", 6), ("ETOT", 8), ("FICT", 9)]
+
+
+def test_fp64_step_matches_oracle(stepsys):
+    out = run(stepsys, "fp64")
+    for (p, v, e, f, ok), (pr, vr, er, fr) in zip(out, stepsys["ref"]):
+        assert ok
+        for name, slot in NAMES:
+            assert abs(e[slot] - er[name]) <= 1e-10 * max(1.0, abs(er[name])), name
+        assert np.max(np.abs(p - pr)) < 1e-9
+        assert np.max(np.abs(v - vr)) < 1e-9 * max(1.0, np.max(np.abs(vr)))
+        assert np.max(np.abs(f - fr)) < 1e-9 * max(1.0, np.max(np.abs(fr)))
+
+
+def test_mixed_step_within_budget(stepsys):
+    from oracle import ortho as OO
+    out = run(stepsys, "mixed")
+    natm = stepsys["sys"].natm
+    lay = stepsys["sys"].layout
+    for (p, v, e, f, ok), (pr, vr, er, fr) in zip(out, stepsys["ref"]):
+        assert ok
+        assert abs(e[8] - er["ETOT"]) / natm <= 1e-6
+        assert np.max(np.abs(f - fr)) <= 1e-5
+        S = OO.pc_overlap(p, p, lay.kx)
+        assert np.max(np.abs(S - 2.0 * np.eye(S.shape[0]))) < 1e-10
