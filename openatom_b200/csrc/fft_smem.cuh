@@ -202,6 +202,82 @@ struct FftStages<T, N, N, EPT, NT, INV> {
   static __device__ __forceinline__ void run(cplx<T>*, int, int, const cplx<T>*) {}
 };
 
+// ---------------------------------------------------------------------------
+// Warp-per-line variant: a warp runs every stage of its own lines with only
+// __syncwarp between stages (no block barriers).  Radix 4 first for powers of
+// two so that a 128-point stage has 32 butterflies, one per lane.
+
+__host__ __device__ constexpr int next_radix_w(int m) {
+  return (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : (m % 3 == 0) ? 3 : (m % 5 == 0) ? 5
+         : (m % 7 == 0) ? 7 : (m % 11 == 0) ? 11 : 0;
+}
+
+template <typename T, int N, int R, int NS, bool INV>
+__device__ __forceinline__ void warp_stage(cplx<T>* line, const cplx<T>* tw, int lane) {
+  constexpr int NBL = N / R;
+  constexpr int PER = (NBL + 31) / 32;
+  constexpr int TSTRIDE = N / (NS * R);
+  cplx<T> v[PER][R];
+  int dst[PER];
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    const int j = lane + 32 * b;
+    dst[b] = -1;
+    if (j < NBL) {
+      const int k = j % NS;
+      const int ts = k * TSTRIDE;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        cplx<T> a = line[j + r * NBL];
+        if (NS > 1 && r > 0) {
+          cplx<T> w = tw[r * ts];
+          a = INV ? cmulc(a, w) : cmul(a, w);
+        }
+        v[b][r] = a;
+      }
+      Dft<T, R, INV>::template run<N>(v[b], tw);
+      dst[b] = (j - k) * R + k;
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    if (dst[b] >= 0) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) line[dst[b] + r * NS] = v[b][r];
+    }
+  }
+  __syncwarp();
+}
+
+template <typename T, int N, int NS, bool INV>
+struct WarpStages {
+  static __device__ __forceinline__ void run(cplx<T>* line, const cplx<T>* tw, int lane) {
+    constexpr int R = next_radix_w(N / NS);
+    static_assert(R > 0, "FFT length has an unsupported prime factor");
+    warp_stage<T, N, R, NS, INV>(line, tw, lane);
+    WarpStages<T, N, NS * R, INV>::run(line, tw, lane);
+  }
+};
+template <typename T, int N, bool INV>
+struct WarpStages<T, N, N, INV> {
+  static __device__ __forceinline__ void run(cplx<T>*, const cplx<T>*, int) {}
+};
+
+// One line of length N in smem by the calling warp (all 32 lanes).
+template <typename T, int N, bool INV>
+__device__ __forceinline__ void fft_line_warp(cplx<T>* line, const cplx<T>* tw) {
+  WarpStages<T, N, 1, INV>::run(line, tw, threadIdx.x & 31);
+}
+
+// Lines l = warp, warp + nwarps, ... of `nlines` (stride ldl), warp-local only.
+template <typename T, int N, bool INV>
+__device__ __forceinline__ void fft_lines_warp(cplx<T>* buf, int ldl, int nlines,
+                                               const cplx<T>* tw) {
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int l = warp; l < nlines; l += nw) fft_line_warp<T, N, INV>(buf + l * ldl, tw);
+}
+
 // Full FFT of `nlines` lines of length N in smem (line stride ldl), in batches
 // that respect the EPT register budget.  Called by all NT threads of the block.
 template <typename T, int N, int EPT, int NT, bool INV>

@@ -132,10 +132,18 @@ __global__ void __launch_bounds__(NT) k_schulz(Work w) {
     T* t2 = B; B = B2; B2 = t2;
     grid.sync();  // partials are rewritten next iteration
   }
-  // T = A * (sigma/2)^(-1/2)
+  // T = A * (sigma/2)^(-1/2); before the FP64 correction the FP32 result is
+  // symmetrised, so that W = X (S/2) X below is the matrix T^T (S/2) T tests
   const double post = sqrt(2.0 / w.sigma);
   double* X = w.newton ? w.X : w.T;
-  for (size_t e = gtid; e < (size_t)nn; e += gstride) X[e] = (double)A[e] * post;
+  for (size_t e = gtid; e < (size_t)nn; e += gstride) {
+    if (w.newton) {
+      int i = e / n, j = e % n;
+      X[e] = 0.5 * ((double)A[e] + (double)A[(size_t)j * n + i]) * post;
+    } else {
+      X[e] = (double)A[e] * post;
+    }
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     w.status[0] = it;
     w.status[1] = (tol_now <= w.tol) ? 1 : 0;

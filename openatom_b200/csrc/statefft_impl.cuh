@@ -28,17 +28,9 @@
 
 namespace sfft {
 
-constexpr int ZTHREADS = 256;
-constexpr int ZEPT = 16;
-constexpr int PTHREADS = 512;
-constexpr int PEPT = 8;
-
-template <typename T>
-struct Kmax;
-template <>
-struct Kmax<float> { static constexpr int v = 16; };
-template <>
-struct Kmax<double> { static constexpr int v = 8; };
+constexpr int ZTHREADS = 256;  // z passes: 8 warps, each owns whole z-lines
+constexpr int PTHREADS = 512;  // plane passes: 16 warps
+constexpr int PWARPS = PTHREADS / 32;
 
 // packed point p -> (line index within the batch, z) by binary search over the
 // batch's line offsets held in shared memory.
@@ -56,7 +48,7 @@ __device__ __forceinline__ void locate(int p, const int* soff, int nl, const int
 
 template <int N>
 struct ZShape {
-  static constexpr int LB = std::min(64, (ZEPT * ZTHREADS) / N);  // lines per block
+  static constexpr int LB = std::min(64, std::max(8, 4096 / N));  // lines per block
   static constexpr int LD = N + 1;
   template <typename T>
   static constexpr size_t bytes() {
@@ -100,7 +92,8 @@ k_zfft_fwd(const double2* __restrict__ psi, cplx<T>* __restrict__ pen, StateGeom
     buf[li * LD + z] = mk<T>((T)v.x, (T)v.y);
   }
   __syncthreads();
-  fft_lines<T, N, ZEPT, ZTHREADS, false>(buf, LD, nl, tw);  // FFTW_FORWARD along z
+  fft_lines_warp<T, N, false>(buf, LD, nl, tw);  // FFTW_FORWARD along z
+  __syncthreads();
   cplx<T>* po = pen + (size_t)s * N * g.nlpad + l0;
   for (int i = threadIdx.x; i < nl * N; i += ZTHREADS) {
     int z = i / nl, li = i - z * nl;
@@ -124,16 +117,14 @@ __device__ __forceinline__ void scatter_plane(const cplx<T>* __restrict__ prow, 
   __syncthreads();
 }
 
-// Build npair complex rows Z = Xa + i Xb for the C2R of rows (ya, ya+1) from the
-// y-transformed plane, with the reference's imag flip (conj) applied, the
-// Hermitian extension to kx > N/2 and zero outside the nplane_x columns.
+// The calling warp builds Z = Xa + i Xb for the C2R of rows (ya, ya+1) from the
+// y-transformed plane: the reference's imag flip (conj), the Hermitian
+// extension to kx > N/2, zero outside the nplane_x columns.
 template <typename T, int N>
-__device__ __forceinline__ void build_c2r_rows(const cplx<T>* plane, cplx<T>* rows, int nplx,
-                                               int ybase, int npair) {
-  constexpr int LDY = N + 1, LDX = N + 1;
-  for (int i = threadIdx.x; i < npair * N; i += PTHREADS) {
-    int pp = i / N, k = i - pp * N;
-    int ya = ybase + 2 * pp;
+__device__ __forceinline__ void build_c2r_row(const cplx<T>* plane, cplx<T>* row, int nplx,
+                                              int ya) {
+  constexpr int LDY = N + 1;
+  for (int k = threadIdx.x & 31; k < N; k += 32) {
     cplx<T> z;
     if (k == 0) {
       z = mk<T>(plane[ya].x, plane[ya + 1].x);
@@ -147,89 +138,122 @@ __device__ __forceinline__ void build_c2r_rows(const cplx<T>* plane, cplx<T>* ro
     } else {
       z = mk<T>(0, 0);
     }
-    rows[pp * LDX + k] = z;
+    row[k] = z;
   }
+  __syncwarp();
+}
+
+// The calling warp splits the spectra of the two real rows held in `row`
+// (after the forward x-FFT), applies the imag flip and stores kx < nplane_x
+// into plane rows (ya, ya+1).
+template <typename T, int N>
+__device__ __forceinline__ void extract_r2c_row(const cplx<T>* row, cplx<T>* plane, int nplx,
+                                                int ya) {
+  constexpr int LDY = N + 1;
+  for (int k = threadIdx.x & 31; k < nplx; k += 32) {
+    cplx<T> zk = row[k];
+    cplx<T> zm = row[k == 0 ? 0 : N - k];
+    // A = (zk + conj zm)/2 ; B = (zk - conj zm)/(2i); stored conjugated
+    plane[k * LDY + ya] = mk<T>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zm.y - zk.y));
+    plane[k * LDY + ya + 1] = mk<T>((T)0.5 * (zk.y + zm.y), (T)0.5 * (zk.x - zm.x));
+  }
+  __syncwarp();
 }
 
 template <typename T, int N>
 struct PShape {
   static constexpr int LDY = N + 1, LDX = N + 1;
+  static constexpr int E = (N + 31) / 32;               // row elements per lane
+  static constexpr int QMAX = std::max(1, 32 / (2 * E));  // row pairs a warp accumulates
+  static constexpr int ROWS = std::min(N, 2 * QMAX * PWARPS) & ~1;  // rows per y-split
   static constexpr size_t LIMIT = 227 * 1024;
-  static constexpr size_t TW = sizeof(cplx<T>) * 2 * N;
-  // rows per chunk (pairs): register budget of the FFT and shared memory
-  static constexpr int rc_for(int nplx, bool with_v) {
-    int rc = std::min(N / 2, (PEPT * PTHREADS) / N);
-    while (rc > 1 && bytes(nplx, rc, with_v) > LIMIT) --rc;
-    return rc;
-  }
-  static constexpr size_t bytes(int nplx, int rc, bool with_v) {
-    return TW + sizeof(cplx<T>) * ((size_t)nplx * LDY + (size_t)rc * LDX) +
-           (with_v ? sizeof(T) * (size_t)N * N : 0);
+  static constexpr size_t bytes(int nplx) {
+    return sizeof(cplx<T>) * ((size_t)N + (size_t)nplx * LDY + (size_t)PWARPS * LDX);
   }
 };
 
 // ---------------------------------------------------------------------------
-// K2: planes -> psi(r); MODE 0 accumulates occ*psi^2 into per-group FP64
-// partial densities held in registers, MODE 1 writes psi(r) (FP64).
+// K2: planes -> psi(r).  MODE 0 accumulates occ*psi^2 into per-group FP64
+// partial densities held in registers (each warp owns row pairs
+// warp, warp+16, ... of the block's y range); MODE 1 writes psi(r) (FP64).
 template <typename T, int N, int MODE>
 __global__ void __launch_bounds__(PTHREADS, 1)
 k_xy_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict__ twx_g,
-         const double* __restrict__ occ, int nstates, int spg, int ysplit_rows, int RC,
+         const double* __restrict__ occ, int nstates, int spg, int ysplit_rows,
          double* __restrict__ out) {
-  constexpr int KM = Kmax<T>::v;
   constexpr int LDY = N + 1, LDX = N + 1;
+  constexpr int E = PShape<T, N>::E, QMAX = PShape<T, N>::QMAX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
-  cplx<T>* plane = tw + 2 * N;
+  cplx<T>* plane = tw + N;
   cplx<T>* rows = plane + g.nplane_x * LDY;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  cplx<T>* row = rows + warp * LDX;
   const int z = blockIdx.x;
   const int grp = blockIdx.y;
   const int y0 = blockIdx.z * ysplit_rows;
   const int nrows = min(ysplit_rows, N - y0);
+  const int npair = nrows / 2;
   const int s0 = grp * spg, s1 = min(nstates, s0 + spg);
   for (int i = threadIdx.x; i < N; i += PTHREADS) tw[i] = twx_g[i];
-  double acc[KM];
+  double acc[QMAX][2][E];
 #pragma unroll
-  for (int k = 0; k < KM; ++k) acc[k] = 0.0;
+  for (int q = 0; q < QMAX; ++q)
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int e = 0; e < E; ++e) acc[q][h][e] = 0.0;
   __syncthreads();
   for (int s = s0; s < s1; ++s) {
     scatter_plane<T, N>(pen + ((size_t)s * N + z) * g.nlpad, plane, g);
-    fft_lines<T, N, PEPT, PTHREADS, false>(plane, LDY, g.nplane_x, tw);  // FFTW_FORWARD y
+    fft_lines_warp<T, N, false>(plane, LDY, g.nplane_x, tw);  // FFTW_FORWARD y
+    __syncthreads();
     const double w = (MODE == 0) ? occ[s] : 1.0;
-    for (int r0 = 0; r0 < nrows; r0 += 2 * RC) {
-      const int npair = min(RC, (nrows - r0) / 2);
-      build_c2r_rows<T, N>(plane, rows, g.nplane_x, y0 + r0, npair);
-      __syncthreads();
-      fft_lines<T, N, PEPT, PTHREADS, true>(rows, LDX, npair, tw);  // C2R, +i sign
-      if (MODE == 0) {
 #pragma unroll
-        for (int k = 0; k < KM; ++k) {
-          int pl = threadIdx.x + k * PTHREADS;
-          int r = pl / N;
-          if (r >= r0 && r < r0 + 2 * npair) {
-            int x = pl - r * N;
-            int rr = r - r0;
-            cplx<T> v = rows[(rr >> 1) * LDX + x];
-            double ps = (double)((rr & 1) ? v.y : v.x);
-            acc[k] += w * ps * ps;
+    for (int q = 0; q < (MODE == 0 ? QMAX : 1); ++q) {
+      for (int pp = warp + PWARPS * q; pp < npair; pp += (MODE == 0 ? npair : PWARPS)) {
+        const int ya = y0 + 2 * pp;
+        build_c2r_row<T, N>(plane, row, g.nplane_x, ya);
+        fft_line_warp<T, N, true>(row, tw);  // C2R, +i sign
+        if (MODE == 0) {
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            int x = lane + 32 * e;
+            if (x < N) {
+              cplx<T> v = row[x];
+              acc[q][0][e] += w * (double)v.x * (double)v.x;
+              acc[q][1][e] += w * (double)v.y * (double)v.y;
+            }
+          }
+        } else {
+          double* o = out + (((size_t)s * N + z) * N + ya) * N;
+          for (int x = lane; x < N; x += 32) {
+            cplx<T> v = row[x];
+            o[x] = (double)v.x;
+            o[N + x] = (double)v.y;
           }
         }
-      } else {
-        for (int i = threadIdx.x; i < 2 * npair * N; i += PTHREADS) {
-          int rr = i / N, x = i - rr * N;
-          cplx<T> v = rows[(rr >> 1) * LDX + x];
-          out[(((size_t)s * N + z) * N + y0 + r0 + rr) * N + x] = (double)((rr & 1) ? v.y : v.x);
-        }
+        __syncwarp();
       }
-      __syncthreads();
     }
+    __syncthreads();
   }
   if (MODE == 0) {
-    double* o = out + ((size_t)grp * N + z) * N * N + (size_t)y0 * N;
+    double* o = out + ((size_t)grp * N + z) * N * N;
 #pragma unroll
-    for (int k = 0; k < KM; ++k) {
-      int pl = threadIdx.x + k * PTHREADS;
-      if (pl < nrows * N) o[pl] = acc[k];
+    for (int q = 0; q < QMAX; ++q) {
+      int pp = warp + PWARPS * q;
+      if (pp < npair) {
+        int ya = y0 + 2 * pp;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          int x = lane + 32 * e;
+          if (x < N) {
+            o[(size_t)ya * N + x] = acc[q][0][e];
+            o[(size_t)(ya + 1) * N + x] = acc[q][1][e];
+          }
+        }
+      }
     }
   }
 }
@@ -237,73 +261,56 @@ k_xy_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict
 // ---------------------------------------------------------------------------
 // K3: MODE 0: pencils -> psi(r) -> psi*V*occ -> planes -> pencils_out
 //     MODE 1: real f(r) (FP64, [s][z][y][x]) -> planes -> pencils_out
+// Each warp takes row pairs warp, warp+16, ... through C2R, the product and
+// R2C in its own row buffer.
 template <typename T, int N, int MODE>
 __global__ void __launch_bounds__(PTHREADS, 1)
 k_xy_bwd(const cplx<T>* __restrict__ pen, const double* __restrict__ freal,
          const T* __restrict__ vks, cplx<T>* __restrict__ pen_out, StateGeom g,
-         const cplx<T>* __restrict__ twx_g, const double* __restrict__ occ, int nstates, int spg,
-         int RC, int v_in_smem) {
+         const cplx<T>* __restrict__ twx_g, const double* __restrict__ occ, int nstates,
+         int spg) {
   constexpr int LDY = N + 1, LDX = N + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
-  cplx<T>* plane = tw + 2 * N;
+  cplx<T>* plane = tw + N;
   cplx<T>* rows = plane + g.nplane_x * LDY;
-  T* vs = reinterpret_cast<T*>(rows + RC * LDX);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  cplx<T>* row = rows + warp * LDX;
   const int z = blockIdx.x;
   const int s0 = blockIdx.y * spg, s1 = min(nstates, s0 + spg);
   for (int i = threadIdx.x; i < N; i += PTHREADS) tw[i] = twx_g[i];
-  const T* vplane = nullptr;
-  if (MODE == 0) {
-    vplane = vks + (size_t)z * N * N;
-    if (v_in_smem) {
-      for (int i = threadIdx.x; i < N * N; i += PTHREADS) vs[i] = vplane[i];
-      vplane = vs;
-    }
-  }
+  const T* vplane = (MODE == 0) ? vks + (size_t)z * N * N : nullptr;
   __syncthreads();
   for (int s = s0; s < s1; ++s) {
     if (MODE == 0) {
       scatter_plane<T, N>(pen + ((size_t)s * N + z) * g.nlpad, plane, g);
-      fft_lines<T, N, PEPT, PTHREADS, false>(plane, LDY, g.nplane_x, tw);
+      fft_lines_warp<T, N, false>(plane, LDY, g.nplane_x, tw);
+      __syncthreads();
     }
     const T w = (MODE == 0) ? (T)occ[s] : (T)1;
-    for (int r0 = 0; r0 < N; r0 += 2 * RC) {
-      const int npair = min(RC, (N - r0) / 2);
+    for (int pp = warp; pp < N / 2; pp += PWARPS) {
+      const int ya = 2 * pp;
       if (MODE == 0) {
-        build_c2r_rows<T, N>(plane, rows, g.nplane_x, r0, npair);
-        __syncthreads();
-        fft_lines<T, N, PEPT, PTHREADS, true>(rows, LDX, npair, tw);
-        for (int i = threadIdx.x; i < npair * N; i += PTHREADS) {
-          int pp = i / N, x = i - pp * N;
-          int ya = r0 + 2 * pp;
-          cplx<T> v = rows[pp * LDX + x];
-          v.x *= vplane[ya * N + x] * w;
-          v.y *= vplane[(ya + 1) * N + x] * w;
-          rows[pp * LDX + x] = v;
+        build_c2r_row<T, N>(plane, row, g.nplane_x, ya);
+        fft_line_warp<T, N, true>(row, tw);
+        for (int x = lane; x < N; x += 32) {
+          cplx<T> v = row[x];
+          v.x *= __ldg(vplane + ya * N + x) * w;
+          v.y *= __ldg(vplane + (ya + 1) * N + x) * w;
+          row[x] = v;
         }
       } else {
         const double* fs = freal + ((size_t)s * N + z) * N * N;
-        for (int i = threadIdx.x; i < npair * N; i += PTHREADS) {
-          int pp = i / N, x = i - pp * N;
-          int ya = r0 + 2 * pp;
-          rows[pp * LDX + x] = mk<T>((T)fs[ya * N + x], (T)fs[(ya + 1) * N + x]);
-        }
+        for (int x = lane; x < N; x += 32)
+          row[x] = mk<T>((T)fs[ya * N + x], (T)fs[(ya + 1) * N + x]);
       }
-      __syncthreads();
-      fft_lines<T, N, PEPT, PTHREADS, false>(rows, LDX, npair, tw);  // R2C, -i sign
-      // split the two real rows' spectra, imag flip, keep kx < nplane_x
-      for (int i = threadIdx.x; i < npair * g.nplane_x; i += PTHREADS) {
-        int pp = i / g.nplane_x, k = i - pp * g.nplane_x;
-        int ya = r0 + 2 * pp;
-        cplx<T> zk = rows[pp * LDX + k];
-        cplx<T> zm = rows[pp * LDX + (k == 0 ? 0 : N - k)];
-        // A = (zk + conj zm)/2 ; B = (zk - conj zm)/(2i); stored conjugated
-        plane[k * LDY + ya] = mk<T>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zm.y - zk.y));
-        plane[k * LDY + ya + 1] = mk<T>((T)0.5 * (zk.y + zm.y), (T)0.5 * (zk.x - zm.x));
-      }
-      __syncthreads();
+      __syncwarp();
+      fft_line_warp<T, N, false>(row, tw);  // R2C, -i sign
+      extract_r2c_row<T, N>(row, plane, g.nplane_x, ya);
     }
-    fft_lines<T, N, PEPT, PTHREADS, true>(plane, LDY, g.nplane_x, tw);  // FFTW_BACKWARD y
+    __syncthreads();
+    fft_lines_warp<T, N, true>(plane, LDY, g.nplane_x, tw);  // FFTW_BACKWARD along y
+    __syncthreads();
     cplx<T>* po = pen_out + ((size_t)s * N + z) * g.nlpad;
     for (int l = threadIdx.x; l < g.nlines; l += PTHREADS) {
       int xy = __ldg(g.line_xy + l);
@@ -349,7 +356,8 @@ k_zfft_bwd(const cplx<T>* __restrict__ pen, double2* __restrict__ fout,
     buf[li * LD + z] = pi[(size_t)z * g.nlpad + li];
   }
   __syncthreads();
-  fft_lines<T, N, ZEPT, ZTHREADS, true>(buf, LD, nl, tw);  // FFTW_BACKWARD along z
+  fft_lines_warp<T, N, true>(buf, LD, nl, tw);  // FFTW_BACKWARD along z
+  __syncthreads();
   const int p0 = soff[0], p1 = soff[nl];
   double e = 0.0;
   const double wocc = (MODE == 0 && occ) ? occ[s] : 0.0;
@@ -432,9 +440,8 @@ struct StateFft {
   static int density(cpstep_ctx* c, const double* psi, const double* occ, double* rho) {
     const FftJob j = c->state_job();
     if (int rc = zfft_fwd(c, j, psi, c->nstates)) return rc;
-    const int RC = PShape<T, N>::rc_for(j.g.nplane_x, false);
-    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x, RC, false);
-    int rows = std::min(N, (Kmax<T>::v * PTHREADS) / N) & ~1;
+    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
+    const int rows = PShape<T, N>::ROWS;
     int ysplit = cdiv(N, rows);
     int ng = std::min(c->ngroups_rho, plane_groups(c, c->nstates, ysplit));
     int spg = cdiv(c->nstates, ng);
@@ -442,7 +449,7 @@ struct StateFft {
     if (int rc = set_smem(k_xy_fwd<T, N, 0>, smem)) return rc;
     k_xy_fwd<T, N, 0><<<dim3(N, ng, ysplit), PTHREADS, smem, c->stream>>>(
         reinterpret_cast<const cplx<T>*>(j.pen_a), j.g, tws<T>(c).x, occ, c->nstates, spg, rows,
-        RC, c->d_rho_part);
+        c->d_rho_part);
     CPSTEP_LAUNCH_CHECK();
     size_t nr = (size_t)N * N * N;
     k_rho_reduce<<<2 * c->num_sms, 256, 0, c->stream>>>(c->d_rho_part, ng, nr, 1.0 / c->vol, rho);
@@ -453,11 +460,10 @@ struct StateFft {
   // packed G -> real r for nstates arrays of the job's geometry
   static int g2r(cpstep_ctx* c, const FftJob& j, const double* packed, double* real, int nstates) {
     if (int rc = zfft_fwd(c, j, packed, nstates)) return rc;
-    const int RC = PShape<T, N>::rc_for(j.g.nplane_x, false);
-    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x, RC, false);
+    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
     if (int rc = set_smem(k_xy_fwd<T, N, 1>, smem)) return rc;
     k_xy_fwd<T, N, 1><<<dim3(N, nstates, 1), PTHREADS, smem, c->stream>>>(
-        reinterpret_cast<const cplx<T>*>(j.pen_a), j.g, tws<T>(c).x, nullptr, nstates, 1, N, RC,
+        reinterpret_cast<const cplx<T>*>(j.pen_a), j.g, tws<T>(c).x, nullptr, nstates, 1, N,
         real);
     CPSTEP_LAUNCH_CHECK();
     return CPSTEP_OK;
@@ -498,17 +504,14 @@ struct StateFft {
       CPSTEP_LAUNCH_CHECK();
       vt = reinterpret_cast<const T*>(c->d_vks_t);
     }
-    bool want_v = PShape<T, N>::bytes(j.g.nplane_x, 1, true) <= PShape<T, N>::LIMIT;
-    int RC = PShape<T, N>::rc_for(j.g.nplane_x, want_v);
-    size_t smem = PShape<T, N>::bytes(j.g.nplane_x, RC, want_v);
+    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
     int ng = plane_groups(c, c->nstates, 1);
     int spg = cdiv(c->nstates, ng);
     ng = cdiv(c->nstates, spg);
     if (int rc = set_smem(k_xy_bwd<T, N, 0>, smem)) return rc;
     k_xy_bwd<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
         reinterpret_cast<const cplx<T>*>(j.pen_a), nullptr, vt,
-        reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, occ, c->nstates, spg, RC,
-        want_v ? 1 : 0);
+        reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, occ, c->nstates, spg);
     CPSTEP_LAUNCH_CHECK();
     double scale = -2.0 / ((double)N * N * N);
     if (int rc = zfft_bwd(c, j, force, psi, eke ? occ : nullptr, c->nstates, scale, 0)) return rc;
@@ -523,12 +526,11 @@ struct StateFft {
   // real r -> packed G (sum_r f(r) e^{+iG.r}) times scale, for the job's geometry
   static int r2g(cpstep_ctx* c, const FftJob& j, const double* f_r, double* fg, int nstates,
                  double scale) {
-    const int RC = PShape<T, N>::rc_for(j.g.nplane_x, false);
-    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x, RC, false);
+    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
     if (int rc = set_smem(k_xy_bwd<T, N, 1>, smem)) return rc;
     k_xy_bwd<T, N, 1><<<dim3(N, nstates), PTHREADS, smem, c->stream>>>(
         nullptr, f_r, nullptr, reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, nullptr,
-        nstates, 1, RC, 0);
+        nstates, 1);
     CPSTEP_LAUNCH_CHECK();
     return zfft_bwd(c, j, fg, nullptr, nullptr, nstates, scale, 1);
   }
