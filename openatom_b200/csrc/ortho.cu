@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(NT) k_schulz(Work w) {
   }
   grid.sync();
   int it = 0;
-  double tol_now = 1.0;
+  double tol_now = 1.0, prev = 1e300;
   while (tol_now > w.tol && it < w.max_iter) {
     ++it;
     // C = 3I - A B^T
@@ -127,7 +127,17 @@ __global__ void __launch_bounds__(NT) k_schulz(Work w) {
     grid.sync();
     double tot = 0.0;
     for (int b = 0; b < (int)gridDim.x; ++b) tot += w.partial[b];  // same order everywhere
-    tol_now = sqrt(tot / (double)nn);
+    const double r = sqrt(tot / (double)nn);
+    // FP32 iteration (mixed path): the coupled iteration loses stability once it
+    // has converged to working precision on an ill-conditioned S; stop at the
+    // first rise of the update and keep the previous iterate (the FP64
+    // correction polishes it).  The FP64 path keeps the reference's rule.
+    if (w.newton && prev < 1e-3 && !(r < prev)) {
+      grid.sync();
+      break;
+    }
+    prev = r;
+    tol_now = r;
     T* t1 = A; A = A2; A2 = t1;
     T* t2 = B; B = B2; B2 = t2;
     grid.sync();  // partials are rewritten next iteration
@@ -146,7 +156,9 @@ __global__ void __launch_bounds__(NT) k_schulz(Work w) {
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     w.status[0] = it;
-    w.status[1] = (tol_now <= w.tol) ? 1 : 0;
+    // mixed: converged once the FP32 iteration has stagnated below 1e-3 (the
+    // FP64 correction takes it from there)
+    w.status[1] = (tol_now <= w.tol || (w.newton && tol_now < 1e-3)) ? 1 : 0;
     *w.rms = tol_now;
   }
 }
