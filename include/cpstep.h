@@ -313,6 +313,32 @@ CPSTEP_API int cpstep_cp_step_host(cpstep_ctx* ctx, double* d_psi, double* d_vps
                                    const double* h_pos, double* h_energies,
                                    double* h_atom_force);
 
+/*
+ * cpstep_pc_overlap_noalloc: the overlap product of cpstep_pc_overlap,
+ * d_c(i,j) = alpha * sum_p w_p Re(conj a_i(p) b_j(p)) + beta * d_c(i,j)
+ * (column-major, ldc), for callers that must not allocate device memory: a
+ * host application whose device memory is owned by its own pool or has a
+ * fixed budget, or code running where cudaMalloc is not allowed (a host
+ * callback, a library that promises its user no allocations).  It has no
+ * counterpart in the reference, which always multiplies into memory its
+ * chares own.  It needs no context and allocates nothing: the split-K
+ * partial tiles go to a fixed 8 MiB device array inside libcpstep
+ * (2^20 doubles), which every GPU that loads the library keeps until the
+ * process exits.  Limit: na * nb <= 2^20 (e.g. 1024 x 1024 states); larger
+ * sizes return CPSTEP_ERR_ARG.  d_a: [na][npts], d_b: [nb][npts] packed
+ * complex128; d_w: per-point weights [npts] (1 on the Gx=0 plane and 2
+ * elsewhere give the reference's S and lambda) or NULL for all 1;
+ * stream: a cudaStream_t or NULL.
+ * The first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress) with that device current: make it before any stream
+ * capture.  Every call uses the same array: two calls that can run at the
+ * same time on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller.
+ */
+CPSTEP_API int cpstep_pc_overlap_noalloc(const double* d_a, const double* d_b, int na, int nb,
+                                         int npts, const double* d_w, double alpha,
+                                         double beta, double* d_c, int ldc, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

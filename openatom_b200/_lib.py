@@ -77,6 +77,9 @@ SIGNATURES = {
                                       _vp]),
     "cpstep_step_status": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
     "cpstep_set_positions": (ctypes.c_int, [_vp, _vp]),
+    "cpstep_pc_overlap_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_int, _vp, ctypes.c_double,
+                                                 ctypes.c_double, _vp, ctypes.c_int, _vp]),
     "cpstep_cp_step_host": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int,
                                            _vp, _vp, _vp]),
 }

@@ -15,6 +15,7 @@
 // reference's numChunks K-split, pcCommManager.C:165-172) with a fixed-order
 // reduction of the partial tiles, so results are deterministic.
 #include <algorithm>
+#include <mutex>
 #include "ctx.cuh"
 
 namespace pcalc {
@@ -245,6 +246,80 @@ int dgemm_launch(cudaStream_t s, int ta, int tb, int m, int n, int k, double alp
   using namespace pcalc;
   dim3 grid(cdiv(m, BM), cdiv(n, BN));
   k_dgemm<<<grid, NT, 0, s>>>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the overlap product (cpstep_pc_overlap_noalloc).
+//
+// For callers that cannot allocate device memory: the split-K partial tiles go
+// to a fixed array compiled into the library instead of context scratch.  The
+// array exists on every GPU that loads the library, for the life of the
+// process.  In host code `g_noalloc_part` names a host-side shadow, not device
+// memory, so the kernels get the device address looked up below.
+
+#define CPSTEP_NOALLOC_PART_DOUBLES (1 << 20)  // 8 MiB of partial tiles
+static __device__ __align__(256) double g_noalloc_part[CPSTEP_NOALLOC_PART_DOUBLES];
+
+namespace {
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[64] = {};  // device address of the array, per device
+int g_noalloc_sms[64] = {};
+}  // namespace
+
+extern "C" int cpstep_pc_overlap_noalloc(const double* d_a, const double* d_b, int na, int nb,
+                                         int npts, const double* d_w, double alpha,
+                                         double beta, double* d_c, int ldc, void* stream) {
+  using namespace pcalc;
+  if (!d_a || !d_b || !d_c || na <= 0 || nb <= 0 || npts <= 0 || ldc < na) {
+    cpstep_set_error("pc_overlap_noalloc: bad argument");
+    return CPSTEP_ERR_ARG;
+  }
+  if ((size_t)na * nb > CPSTEP_NOALLOC_PART_DOUBLES) {
+    cpstep_set_error("pc_overlap_noalloc: na*nb = %zu exceeds the fixed scratch of %d doubles "
+                     "(at most %d x %d); use cpstep_pc_overlap",
+                     (size_t)na * nb, CPSTEP_NOALLOC_PART_DOUBLES, 1024, 1024);
+    return CPSTEP_ERR_ARG;
+  }
+  int dev = 0;
+  CPSTEP_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    cpstep_set_error("pc_overlap_noalloc: device index %d out of range", dev);
+    return CPSTEP_ERR_ARG;
+  }
+  double* part = nullptr;
+  int nsm = 0;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      // once per device, with that device current
+      void* addr = nullptr;
+      CPSTEP_CUDA_TRY(cudaGetSymbolAddress(&addr, g_noalloc_part));
+      int sms = 0;
+      CPSTEP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      g_noalloc_addr[dev] = static_cast<double*>(addr);
+      g_noalloc_sms[dev] = sms > 0 ? sms : 148;
+    }
+    part = g_noalloc_addr[dev];
+    nsm = g_noalloc_sms[dev];
+  }
+  const int M = na, N = nb, K = 2 * npts;
+  const int tm = cdiv(M, BM), tn = cdiv(N, BN);
+  int want = std::max(1, (2 * nsm) / (tm * tn));
+  const int fit = (int)std::max<size_t>(1, CPSTEP_NOALLOC_PART_DOUBLES / ((size_t)M * N));
+  want = std::min(want, fit);
+  int kslab = cdiv(cdiv(K, want), BK) * BK;
+  int nsplit = cdiv(K, kslab);
+  while ((size_t)nsplit * M * N > CPSTEP_NOALLOC_PART_DOUBLES) {  // rounding of kslab
+    kslab += BK;
+    nsplit = cdiv(K, kslab);
+  }
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  // every partial the reduction reads is written by this call: nothing to clear
+  k_overlap_part<<<dim3(tm, tn, nsplit), NT, 0, s>>>(d_a, K, d_b, K, d_w, M, N, K, kslab, part);
+  CPSTEP_LAUNCH_CHECK();
+  k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, s>>>(part, nsplit, M, N, alpha, beta, d_c, ldc);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }
