@@ -310,6 +310,43 @@ def cpu_baseline(cfg, sample_states=4):
     return t_step, sample
 
 
+def kernel_case(args):
+    """Small single-GPU case of one kernel group, for profiler captures.
+
+    statefft: density + 2 x (V.psi, density) of `--states` states of the
+    water192 layout (128^3 grid) in the chosen precision.
+    rhoside:  the density-side pass (XC, rho FFT, Hartree/local/Ewald and
+    atom forces, V_KS) of the water192 system, run 3 times.
+    """
+    import torch
+    from openatom_b200.context import StepContext
+    from openatom_b200.system import System
+    cfg = CONFIGS["water192"]
+    S = args.states
+    sysm = System(cfg["box"], cfg["ecut"], S, cfg["atoms"], nfft=cfg["grid"])
+    occ = torch.ones(S, dtype=torch.float64, device="cuda")
+    ctx = StepContext(sysm.layout, S, precision=args.precision)
+    psi = sysm.psi()
+    rho = ctx.density(psi, occ)
+    if args.kernel_case == "statefft":
+        v = torch.randn(cfg["grid"], cfg["grid"], cfg["grid"], dtype=torch.float64,
+                        device="cuda") * 0.1
+        for _ in range(2):
+            f, e = ctx.vks_psi(psi, v, occ)
+            rho = ctx.density(psi, occ)
+        chk = float(e.sum())
+    else:
+        ctx.set_atoms(sysm)
+        for _ in range(3):
+            vks, _, _ = ctx.vks_from_rho(rho)
+        chk = float(vks.sum())
+    torch.cuda.synchronize()
+    ctx.close()
+    print(json.dumps({"kernel_case": args.kernel_case, "states": S,
+                      "precision": args.precision, "rho_sum": float(rho.sum()),
+                      "check": chk}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -318,7 +355,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="water192", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-case", choices=["statefft", "rhoside"], default=None,
+                    help="run a small profiling case instead of the benchmark")
+    ap.add_argument("--states", type=int, default=8)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     args = ap.parse_args()
+    if args.kernel_case:
+        kernel_case(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     cfg = CONFIGS[args.config]

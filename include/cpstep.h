@@ -52,6 +52,8 @@ extern "C" {
 #define CPSTEP_E_FICT 9    /* fictitious kinetic energy (get_fictKE)          */
 #define CPSTEP_NENERGY 12
 
+#define CPSTEP_MAX_TYPES 16   /* atom types a context accepts (cpstep_set_atoms) */
+
 #define CPSTEP_PREC_FP64 0    /* plain FP64 path: the drop-in */
 #define CPSTEP_PREC_MIXED 1   /* FP32 FFT/density/V.psi, FP64 accumulation, split GEMMs */
 
@@ -235,6 +237,7 @@ CPSTEP_API int cpstep_ortho_tmat(cpstep_ctx* ctx, const double* d_s, double* d_t
  *   spline tables vps[ntyp][4][nspl] = vps0..vps3 on g = gmin_spl + i*dg_spl
  *   (cppseudo->vps0..3, CP_get_vpsnow :433-475), gzvps[ntyp] (the G=0 term)
  *   and the Ewald alpha (genewald->alp_ewd).  Host pointers, copied.
+ *   At most CPSTEP_MAX_TYPES types.
  * cpstep_rho_layout: the density sphere's packed order (|G|^2/2 <= 4 Ecut,
  *   countkvec3d/setkvec3d set_cp_ewald.C:230-500, flip_data_set order):
  *   npts, and kx/ky/kz (host, room for cap) when given.

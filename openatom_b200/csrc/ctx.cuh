@@ -64,6 +64,10 @@ struct AtomData {
   double *frac = nullptr, *q = nullptr, *vps = nullptr, *gzvps = nullptr;
   int kxm = 0, kym = 0, kzm = 0;
   double2 *ex = nullptr, *ey = nullptr, *ez = nullptr;
+  double2* ezt = nullptr;  // [natm][2 kzm + 1], atoms in type order
+  int* rank = nullptr;     // atom -> position in type order
+  int tstart[CPSTEP_MAX_TYPES + 1] = {};  // type t holds ranks [tstart[t], tstart[t+1])
+  int nfblk = 0;           // blocks (rows of fpart) of the force pass
   double* fpart = nullptr;
   double* pos = nullptr;  // staging for cpstep_set_positions
 };

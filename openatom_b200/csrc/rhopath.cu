@@ -83,11 +83,15 @@ struct Atoms {
   const double2* ex;   // [kxm+1][natm]      e^{i 2pi kx s_x}
   const double2* ey;   // [2kym+1][natm]     ky in [-kym, kym]
   const double2* ez;   // [2kzm+1][natm]
+  const double2* ezt;  // [natm][2kzm+1], atoms in type order
+  const int* rank;     // atom -> type-ordered position
+  int tstart[CPSTEP_MAX_TYPES + 1];
 };
 
 __global__ void k_phase(const double* __restrict__ frac, int natm, int kxm, int kym, int kzm,
-                        double2* __restrict__ ex, double2* __restrict__ ey,
-                        double2* __restrict__ ez) {
+                        const int* __restrict__ rank, double2* __restrict__ ex,
+                        double2* __restrict__ ey, double2* __restrict__ ez,
+                        double2* __restrict__ ezt) {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= natm) return;
   const double tpi = 2.0 * M_PI;
@@ -101,10 +105,12 @@ __global__ void k_phase(const double* __restrict__ frac, int natm, int kxm, int 
     sincos(tpi * k * frac[3 * a + 1], &s, &c);
     ey[(size_t)(k + kym) * natm + a] = make_double2(c, s);
   }
+  double2* zt = ezt + (size_t)rank[a] * (2 * kzm + 1);
   for (int k = -kzm; k <= kzm; ++k) {
     double s, c;
     sincos(tpi * k * frac[3 * a + 2], &s, &c);
     ez[(size_t)(k + kzm) * natm + a] = make_double2(c, s);
+    zt[k + kzm] = make_double2(c, s);
   }
 }
 
@@ -136,23 +142,48 @@ __device__ __forceinline__ double vps_at(const Atoms& A, int t, double g, double
   return (((v[3 * A.nspl] * h + v[2 * A.nspl]) * h + v[A.nspl]) * h + v[0]) * rvol;
 }
 
-// One thread per density-sphere point.  rhog_t: transformed density
-// (sum rho e^{+iGr} * vol/N = conj of the reference rho(G)); writes conj(vks)
-// for the G->R kernels, the force kernel's per-point terms and energy partials.
-__global__ void k_hart(const double2* __restrict__ rhog_t, const int* __restrict__ kx,
-                       const int* __restrict__ ky, const int* __restrict__ kz, int npts,
-                       const double* __restrict__ hmati, double vol, double ecut4, double alp,
-                       Atoms A, double2* __restrict__ vg_t, double4* __restrict__ fterm,
-                       double* __restrict__ part) {
+// Structure factors along z-lines.  The density sphere is packed line by line
+// (all kz of one (kx, ky) contiguous), and e^{iG.R} = [e^{i2pi kx sx} e^{i2pi ky sy}]
+// e^{i2pi kz sz}: the bracket is formed once per line and atom (in shared
+// memory, type order) and each point of the line multiplies it by the atom's
+// z phase.  The reference advances the structure factor along kz the same way
+// (ei_inc recursion, cp_hart_ext.C:150-210); the tables keep every phase exact.
+//
+// One block per line, one thread per point (lines longer than the block loop).
+// rhog_t: transformed density (sum rho e^{+iGr} vol/N = conj of the reference
+// rho(G)); writes conj(vks) for the G->R kernels, the per-point force terms
+// and per-line energy partials [nlines][3].
+constexpr int HT = 128;
+constexpr int kMaxAtoms = 1024;  // the force pass holds at most 4 atoms per thread of 256
+__global__ void __launch_bounds__(HT)
+k_hart_lines(const double2* __restrict__ rhog_t, const int* __restrict__ line_off, int nlines,
+             const int* __restrict__ kx, const int* __restrict__ ky, const int* __restrict__ kz,
+             int npts, const double* __restrict__ hmati, double vol, double ecut4, double alp,
+             Atoms A, double2* __restrict__ vg_t, double4* __restrict__ fterm,
+             double* __restrict__ part) {
+  extern __shared__ double2 su[];  // [natm] line phases, type order
   __shared__ double red[32];
   const double tpi = 2.0 * M_PI, rvol = 1.0 / vol, fpi = 4.0 * M_PI;
   const double falp2 = 4.0 * alp * alp;
+  const int l = blockIdx.x;
+  const int off = line_off[l], end = (l + 1 < nlines) ? line_off[l + 1] : npts;
+  const int a = kx[off], b = ky[off];
+  const int nz = 2 * A.kzm + 1;
+  for (int i = threadIdx.x; i < A.natm; i += HT) {
+    double2 x = A.ex[(size_t)a * A.natm + i];
+    double2 y = A.ey[(size_t)(b + A.kym) * A.natm + i];
+    su[A.rank[i]] = make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
+  }
+  __syncthreads();
   double eh = 0.0, ee = 0.0, ew = 0.0;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npts; p += gridDim.x * blockDim.x) {
-    int a = kx[p], b = ky[p], c = kz[p];
-    double gx = tpi * (a * hmati[0] + b * hmati[1] + c * hmati[2]);
-    double gy = tpi * (a * hmati[3] + b * hmati[4] + c * hmati[5]);
-    double gz = tpi * (a * hmati[6] + b * hmati[7] + c * hmati[8]);
+  const double gx0 = tpi * (a * hmati[0] + b * hmati[1]);
+  const double gy0 = tpi * (a * hmati[3] + b * hmati[4]);
+  const double gz0 = tpi * (a * hmati[6] + b * hmati[7]);
+  for (int p = off + threadIdx.x; p < end; p += HT) {
+    const int c = kz[p];
+    double gx = gx0 + tpi * c * hmati[2];
+    double gy = gy0 + tpi * c * hmati[5];
+    double gz = gz0 + tpi * c * hmati[8];
     double g2 = gx * gx + gy * gy + gz * gz;
     double2 out = make_double2(0.0, 0.0);
     double4 ft = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -164,16 +195,17 @@ __global__ void k_hart(const double2* __restrict__ rhog_t, const int* __restrict
       eh += 0.5 * hart * (r.x * r.x + r.y * r.y) * w;
       double g = sqrt(g2);
       double2 vext = make_double2(0.0, 0.0), sewd = make_double2(0.0, 0.0);
+      const double2* zc = A.ezt + (c + A.kzm);
       for (int t = 0; t < A.ntyp; ++t) {
+        double2 st = make_double2(0.0, 0.0);
+        for (int i = A.tstart[t]; i < A.tstart[t + 1]; ++i) {
+          double2 u = su[i];
+          double2 z = zc[(size_t)i * nz];
+          st.x += u.x * z.x - u.y * z.y;
+          st.y += u.x * z.y + u.y * z.x;
+        }
         double vt = vps_at(A, t, g, rvol);
         double qt = A.q[t];
-        double2 st = make_double2(0.0, 0.0);
-        for (int i = 0; i < A.natm; ++i) {
-          if (A.typ[i] != t) continue;
-          double2 h = phase(A, i, a, b, c);
-          st.x += h.x;
-          st.y += h.y;
-        }
         vext.x += vt * st.x;
         vext.y += vt * st.y;
         sewd.x += qt * st.x;
@@ -193,9 +225,9 @@ __global__ void k_hart(const double2* __restrict__ rhog_t, const int* __restrict
   double s2 = block_sum(ee, red);
   double s3 = block_sum(ew, red);
   if (threadIdx.x == 0) {
-    part[3 * blockIdx.x] = s1;
-    part[3 * blockIdx.x + 1] = s2;
-    part[3 * blockIdx.x + 2] = s3;
+    part[3 * l] = s1;
+    part[3 * l + 1] = s2;
+    part[3 * l + 2] = s3;
   }
 }
 
@@ -209,58 +241,99 @@ __global__ void k_hart_g0(const double2* __restrict__ rhog_t, int izero, double 
   *eext += v * rhog_t[izero].x;
 }
 
-// Forces: block b handles a chunk of points for all atoms (thread <-> atom).
-constexpr int FCHUNK = 256;
-__global__ void k_local_forces(const double4* __restrict__ fterm, const int* __restrict__ kx,
-                               const int* __restrict__ ky, const int* __restrict__ kz, int npts,
-                               const double* __restrict__ hmati, double vol, Atoms A,
-                               double* __restrict__ fpart) {
-  __shared__ double4 sft[FCHUNK];
-  __shared__ int sk[FCHUNK][3];
-  __shared__ double sg[FCHUNK][4];  // gx, gy, gz, g
+// Local + Ewald forces on the atoms, line by line: for line (kx, ky) and atom
+// a with type t, with T_t(G) the per-point term and u_a the line phase,
+//   F_a += sum_kz g(G) Im(u_a e^{i2pi kz sz_a} conj T_t(G))
+//        = g0 Im(u_a P_a) + (2pi hmati col z) Im(u_a Q_a),
+//   P_a = sum_kz e^{i2pi kz sz_a} conj T_t,  Q_a = sum_kz kz e^{i2pi kz sz_a} conj T_t,
+// g = g0 + kz (2pi hmati col z) being linear along the line.  A block (one
+// thread per atom) walks lines blockIdx.x, +gridDim.x, ...; T_t of the line's
+// points is staged in shared memory [ntyp][lmax] with kz beside it.
+// Writes fpart[block][natm][3].
+__global__ void k_local_forces_lines(const double4* __restrict__ fterm,
+                                     const int* __restrict__ line_off, int nlines,
+                                     const int* __restrict__ kx, const int* __restrict__ ky,
+                                     const int* __restrict__ kz, int npts,
+                                     const double* __restrict__ hmati, double vol, Atoms A,
+                                     int lmax, double* __restrict__ fpart) {
+  extern __shared__ double2 sT[];  // [ntyp][lmax] conj T, then int kz[lmax]
+  int* skz = reinterpret_cast<int*>(sT + (size_t)A.ntyp * lmax);
   const double tpi = 2.0 * M_PI, rvol = 1.0 / vol;
-  const int p0 = blockIdx.x * FCHUNK;
-  const int np = min(FCHUNK, npts - p0);
-  for (int i = threadIdx.x; i < np; i += blockDim.x) {
-    int p = p0 + i;
-    int a = kx[p], b = ky[p], c = kz[p];
-    sft[i] = fterm[p];
-    sk[i][0] = a; sk[i][1] = b; sk[i][2] = c;
-    double gx = tpi * (a * hmati[0] + b * hmati[1] + c * hmati[2]);
-    double gy = tpi * (a * hmati[3] + b * hmati[4] + c * hmati[5]);
-    double gz = tpi * (a * hmati[6] + b * hmati[7] + c * hmati[8]);
-    sg[i][0] = gx; sg[i][1] = gy; sg[i][2] = gz;
-    sg[i][3] = sqrt(gx * gx + gy * gy + gz * gz);
-  }
-  __syncthreads();
-  for (int at = threadIdx.x; at < A.natm; at += blockDim.x) {
-    const int t = A.typ[at];
-    const double qa = A.q[t];
-    double fx = 0.0, fy = 0.0, fz = 0.0;
-    for (int i = 0; i < np; ++i) {
-      double4 f = sft[i];
-      if (f.x == 0.0 && f.y == 0.0 && f.z == 0.0 && f.w == 0.0) continue;
-      double vt = vps_at(A, t, sg[i][3], rvol);
-      double2 h = phase(A, at, sk[i][0], sk[i][1], sk[i][2]);
-      double tr = f.x * vt + f.z * qa;
-      double ti = f.y * vt + f.w * qa;
-      double s = tr * h.y - ti * h.x;
-      fx += sg[i][0] * s;
-      fy += sg[i][1] * s;
-      fz += sg[i][2] * s;
+  const double cx = tpi * hmati[2], cy = tpi * hmati[5], cz = tpi * hmati[8];
+  double f[4][3] = {};  // up to 4 atoms per thread
+  const int nper = (A.natm + blockDim.x - 1) / blockDim.x;
+  for (int l = blockIdx.x; l < nlines; l += gridDim.x) {
+    const int off = line_off[l], end = (l + 1 < nlines) ? line_off[l + 1] : npts;
+    const int a = kx[off], b = ky[off];
+    const double g0x = tpi * (a * hmati[0] + b * hmati[1]);
+    const double g0y = tpi * (a * hmati[3] + b * hmati[4]);
+    const double g0z = tpi * (a * hmati[6] + b * hmati[7]);
+    for (int c0 = off; c0 < end; c0 += lmax) {
+      const int len = min(lmax, end - c0);
+      __syncthreads();
+      for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        const int p = c0 + i;
+        const int c = kz[p];
+        skz[i] = c;
+        double4 ft = fterm[p];
+        double gx = g0x + c * cx, gy = g0y + c * cy, gz = g0z + c * cz;
+        double g = sqrt(gx * gx + gy * gy + gz * gz);
+        for (int t = 0; t < A.ntyp; ++t) {
+          double vt = (ft.x != 0.0 || ft.y != 0.0) ? vps_at(A, t, g, rvol) : 0.0;
+          double qt = A.q[t];
+          sT[(size_t)t * lmax + i] = make_double2(ft.x * vt + ft.z * qt, -(ft.y * vt + ft.w * qt));
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int at = threadIdx.x + k * blockDim.x;
+        if (k < nper && at < A.natm) {
+          const int t = A.typ[at];
+          double2 x = A.ex[(size_t)a * A.natm + at];
+          double2 y = A.ey[(size_t)(b + A.kym) * A.natm + at];
+          double2 u = make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
+          const double2* T = sT + (size_t)t * lmax;
+          double px = 0.0, py = 0.0, qx = 0.0, qy = 0.0;
+          for (int i = 0; i < len; ++i) {
+            const int c = skz[i];
+            double2 e = A.ez[(size_t)(c + A.kzm) * A.natm + at];
+            double2 tt = T[i];
+            double rx = e.x * tt.x - e.y * tt.y;
+            double ry = e.x * tt.y + e.y * tt.x;
+            px += rx;
+            py += ry;
+            qx += c * rx;
+            qy += c * ry;
+          }
+          double ip = u.x * py + u.y * px;  // Im(u P)
+          double iq = u.x * qy + u.y * qx;  // Im(u Q)
+          f[k][0] += g0x * ip + cx * iq;
+          f[k][1] += g0y * ip + cy * iq;
+          f[k][2] += g0z * ip + cz * iq;
+        }
+      }
     }
-    double* o = fpart + ((size_t)blockIdx.x * A.natm + at) * 3;
-    o[0] = fx; o[1] = fy; o[2] = fz;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int at = threadIdx.x + k * blockDim.x;
+    if (k < nper && at < A.natm) {
+      double* o = fpart + ((size_t)blockIdx.x * A.natm + at) * 3;
+      o[0] = f[k][0]; o[1] = f[k][1]; o[2] = f[k][2];
+    }
   }
 }
 
+// out[c] = scale * sum_r part[r][c]; one block per column, fixed order.
 __global__ void k_sum_cols(const double* __restrict__ part, int nrow, int ncol,
                            double* __restrict__ out, double scale) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncol) return;
+  __shared__ double red[32];
+  const int c = blockIdx.x;
   double s = 0.0;
-  for (int r = 0; r < nrow; ++r) s += part[(size_t)r * ncol + c];
-  out[c] = s * scale;
+  for (int r = threadIdx.x; r < nrow; r += blockDim.x) s += part[(size_t)r * ncol + c];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) out[c] = s * scale;
 }
 
 __global__ void k_add(double* __restrict__ a, const double* __restrict__ b, size_t n) {
@@ -341,7 +414,7 @@ int rho_init(cpstep_ctx* c, double box_len, double ecut_ry) {
   size_t nr = (size_t)c->nx * c->ny * c->nz;
   CPSTEP_CUDA_TRY(cudaMalloc(&r.vhl, sizeof(double) * nr));
   r.nblk_xc = 4 * c->num_sms;
-  r.nblk_h = 2 * c->num_sms;
+  r.nblk_h = nl;  // k_hart_lines: one block per line
   CPSTEP_CUDA_TRY(cudaMalloc(&r.part, sizeof(double) * (2 * r.nblk_xc + 3 * r.nblk_h + 8)));
   CPSTEP_CUDA_TRY(cudaMalloc(&c->d_energies, sizeof(double) * CPSTEP_NENERGY));
   CPSTEP_CUDA_TRY(cudaMemset(c->d_energies, 0, sizeof(double) * CPSTEP_NENERGY));
@@ -357,7 +430,8 @@ void rho_free(cpstep_ctx* c) {
   cudaFree(c->d_energies);
   AtomData& a = c->atoms;
   cudaFree(a.typ); cudaFree(a.frac); cudaFree(a.q); cudaFree(a.vps); cudaFree(a.gzvps);
-  cudaFree(a.ex); cudaFree(a.ey); cudaFree(a.ez); cudaFree(a.fpart); cudaFree(a.pos);
+  cudaFree(a.ex); cudaFree(a.ey); cudaFree(a.ez); cudaFree(a.ezt); cudaFree(a.rank);
+  cudaFree(a.fpart); cudaFree(a.pos);
 }
 
 FftJob rho_job(const cpstep_ctx* c) {
@@ -378,14 +452,29 @@ int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* p
               const double* gzvps, double alp_ewd) {
   AtomData& a = c->atoms;
   cudaFree(a.typ); cudaFree(a.frac); cudaFree(a.q); cudaFree(a.vps); cudaFree(a.gzvps);
-  cudaFree(a.ex); cudaFree(a.ey); cudaFree(a.ez); cudaFree(a.fpart); cudaFree(a.pos);
+  cudaFree(a.ex); cudaFree(a.ey); cudaFree(a.ez); cudaFree(a.ezt); cudaFree(a.rank);
+  cudaFree(a.fpart); cudaFree(a.pos);
   a = AtomData();
+  if (ntyp > CPSTEP_MAX_TYPES || natm > rho::kMaxAtoms) {
+    cpstep_set_error("atoms: %d types / %d atoms exceed the limits %d / %d", ntyp, natm,
+                     CPSTEP_MAX_TYPES, rho::kMaxAtoms);
+    return CPSTEP_ERR_ARG;
+  }
   std::vector<int> t(typ, typ + natm);
   for (int v : t)
     if (v < 0 || v >= ntyp) {
       cpstep_set_error("atoms: type index out of range");
       return CPSTEP_ERR_ARG;
     }
+  // type order (stable): rank[atom], tstart[type]
+  std::vector<int> cnt(ntyp + 1, 0), rank(natm);
+  for (int v : t) ++cnt[v + 1];
+  for (int k = 0; k < ntyp; ++k) cnt[k + 1] += cnt[k];
+  for (int k = 0; k <= ntyp; ++k) a.tstart[k] = cnt[k];
+  {
+    std::vector<int> next(cnt.begin(), cnt.end() - 1);
+    for (int i = 0; i < natm; ++i) rank[i] = next[t[i]]++;
+  }
   std::vector<double> frac(3 * (size_t)natm);
   const double* hi = c->hmati;  // s = hmati R (column-major hmati)
   for (int i = 0; i < natm; ++i) {
@@ -394,7 +483,8 @@ int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* p
       frac[3 * i + d] = hi[d] * R[0] + hi[d + 3] * R[1] + hi[d + 6] * R[2];
   }
   int rc;
-  if ((rc = upload_i(&a.typ, t)) || (rc = upload_d(&a.frac, frac)) ||
+  if ((rc = upload_i(&a.typ, t)) || (rc = upload_i(&a.rank, rank)) ||
+      (rc = upload_d(&a.frac, frac)) ||
       (rc = upload_d(&a.q, std::vector<double>(q, q + ntyp))) ||
       (rc = upload_d(&a.vps, std::vector<double>(vps, vps + (size_t)ntyp * 4 * nspl))) ||
       (rc = upload_d(&a.gzvps, std::vector<double>(gzvps, gzvps + ntyp))))
@@ -411,10 +501,11 @@ int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* p
   CPSTEP_CUDA_TRY(cudaMalloc(&a.ex, sizeof(double2) * (a.kxm + 1) * natm));
   CPSTEP_CUDA_TRY(cudaMalloc(&a.ey, sizeof(double2) * (2 * a.kym + 1) * natm));
   CPSTEP_CUDA_TRY(cudaMalloc(&a.ez, sizeof(double2) * (2 * a.kzm + 1) * natm));
-  int nfb = cdiv(c->rg.npts, rho::FCHUNK);
-  CPSTEP_CUDA_TRY(cudaMalloc(&a.fpart, sizeof(double) * 3 * (size_t)natm * nfb));
-  rho::k_phase<<<cdiv(natm, 128), 128, 0, c->stream>>>(a.frac, natm, a.kxm, a.kym, a.kzm, a.ex,
-                                                        a.ey, a.ez);
+  CPSTEP_CUDA_TRY(cudaMalloc(&a.ezt, sizeof(double2) * (2 * a.kzm + 1) * natm));
+  a.nfblk = std::max(1, std::min(c->rg.nlines, 2 * c->num_sms));
+  CPSTEP_CUDA_TRY(cudaMalloc(&a.fpart, sizeof(double) * 3 * (size_t)natm * a.nfblk));
+  rho::k_phase<<<cdiv(natm, 128), 128, 0, c->stream>>>(a.frac, natm, a.kxm, a.kym, a.kzm, a.rank,
+                                                        a.ex, a.ey, a.ez, a.ezt);
   CPSTEP_LAUNCH_CHECK();
   if (!c->d_hmati) CPSTEP_CUDA_TRY(cudaMalloc(&c->d_hmati, sizeof(double) * 9));
   CPSTEP_CUDA_TRY(cudaMemcpy(c->d_hmati, c->hmati, sizeof(double) * 9, cudaMemcpyHostToDevice));
@@ -427,6 +518,8 @@ static rho::Atoms atoms_view(const cpstep_ctx* c) {
   A.natm = a.natm; A.ntyp = a.ntyp; A.typ = a.typ; A.frac = a.frac; A.q = a.q; A.vps = a.vps;
   A.gzvps = a.gzvps; A.nspl = a.nspl; A.gmin = a.gmin; A.dg = a.dg;
   A.kxm = a.kxm; A.kym = a.kym; A.kzm = a.kzm; A.ex = a.ex; A.ey = a.ey; A.ez = a.ez;
+  A.ezt = a.ezt; A.rank = a.rank;
+  for (int k = 0; k <= CPSTEP_MAX_TYPES; ++k) A.tstart[k] = a.tstart[k];
   return A;
 }
 
@@ -444,7 +537,7 @@ int atoms_set_positions(cpstep_ctx* c, const double* h_pos) {
   rho::k_frac<<<cdiv(a.natm, 128), 128, 0, c->stream>>>(a.pos, c->d_hmati, a.natm, a.frac);
   CPSTEP_LAUNCH_CHECK();
   rho::k_phase<<<cdiv(a.natm, 128), 128, 0, c->stream>>>(a.frac, a.natm, a.kxm, a.kym, a.kzm,
-                                                          a.ex, a.ey, a.ez);
+                                                          a.rank, a.ex, a.ey, a.ez, a.ezt);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }
@@ -455,8 +548,8 @@ int rho_xc(cpstep_ctx* c, const double* rho_r, double* vxc, double* energies) {
   RhoGeom& r = c->rg;
   rho::k_xc<<<r.nblk_xc, 256, 0, c->stream>>>(rho_r, vxc, nr, r.part);
   CPSTEP_LAUNCH_CHECK();
-  rho::k_sum_cols<<<1, 32, 0, c->stream>>>(r.part, r.nblk_xc, 2, energies + CPSTEP_E_EXC,
-                                           c->vol / (double)nr);
+  rho::k_sum_cols<<<2, 256, 0, c->stream>>>(r.part, r.nblk_xc, 2, energies + CPSTEP_E_EXC,
+                                            c->vol / (double)nr);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }
@@ -478,11 +571,15 @@ int rho_hart(cpstep_ctx* c, double* energies, double* force) {
   rho::Atoms A = atoms_view(c);
   double ecut4 = 8.0 * (0.5 * c->ecut_ry);
   double* hp = r.part + 2 * r.nblk_xc;
-  rho::k_hart<<<r.nblk_h, 256, 0, c->stream>>>(r.rhog, r.kx, r.ky, r.kz, r.npts, c->d_hmati,
-                                               c->vol, ecut4, c->atoms.alp_ewd, A, r.vg,
-                                               r.fterm, hp);
+  const size_t hsm = sizeof(double2) * (size_t)c->atoms.natm;
+  if (hsm > 48 * 1024)
+    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(rho::k_hart_lines,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
+  rho::k_hart_lines<<<r.nlines, rho::HT, hsm, c->stream>>>(
+      r.rhog, r.line_off, r.nlines, r.kx, r.ky, r.kz, r.npts, c->d_hmati, c->vol, ecut4,
+      c->atoms.alp_ewd, A, r.vg, r.fterm, hp);
   CPSTEP_LAUNCH_CHECK();
-  rho::k_sum_cols<<<1, 32, 0, c->stream>>>(hp, r.nblk_h, 3, energies + CPSTEP_E_HART, 1.0);
+  rho::k_sum_cols<<<3, 256, 0, c->stream>>>(hp, r.nlines, 3, energies + CPSTEP_E_HART, 1.0);
   CPSTEP_LAUNCH_CHECK();
   if (c->rho_izero >= 0) {
     rho::k_hart_g0<<<1, 1, 0, c->stream>>>(r.rhog, c->rho_izero, c->vol, A, r.vg,
@@ -490,13 +587,21 @@ int rho_hart(cpstep_ctx* c, double* energies, double* force) {
     CPSTEP_LAUNCH_CHECK();
   }
   if (force) {
-    int nfb = cdiv(r.npts, rho::FCHUNK);
-    int nt = std::min(1024, ((c->atoms.natm + 31) / 32) * 32);
-    rho::k_local_forces<<<nfb, nt, 0, c->stream>>>(r.fterm, r.kx, r.ky, r.kz, r.npts,
-                                                   c->d_hmati, c->vol, A, c->atoms.fpart);
+    const int natm = c->atoms.natm;
+    const int per = cdiv(natm, 256);  // atoms per thread, <= 4 (kMaxAtoms)
+    const int nt = std::max(32, cdiv(cdiv(natm, per), 32) * 32);
+    const int lmax = c->nz + 1;
+    const size_t fsm = (sizeof(double2) * c->atoms.ntyp + sizeof(int)) * (size_t)lmax;
+    if (fsm > 48 * 1024)
+      CPSTEP_CUDA_TRY(cudaFuncSetAttribute(rho::k_local_forces_lines,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)fsm));
+    rho::k_local_forces_lines<<<c->atoms.nfblk, nt, fsm, c->stream>>>(
+        r.fterm, r.line_off, r.nlines, r.kx, r.ky, r.kz, r.npts, c->d_hmati, c->vol, A, lmax,
+        c->atoms.fpart);
     CPSTEP_LAUNCH_CHECK();
-    rho::k_sum_cols<<<cdiv(3 * c->atoms.natm, 128), 128, 0, c->stream>>>(
-        c->atoms.fpart, nfb, 3 * c->atoms.natm, force, 1.0);
+    rho::k_sum_cols<<<3 * natm, 256, 0, c->stream>>>(c->atoms.fpart, c->atoms.nfblk, 3 * natm,
+                                                     force, 1.0);
     CPSTEP_LAUNCH_CHECK();
   }
   return CPSTEP_OK;
