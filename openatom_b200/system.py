@@ -113,6 +113,42 @@ def spline_tables(species, gmin, gmax, nspl=4000):
                 q=np.array([SPECIES[sp]["Z"] for sp in species]))
 
 
+# Synthetic Kleinman-Bylander projectors, s and p, with Gaussian radials in g:
+#   v_0(g) = A0 exp(-g^2 r0^2/4),   v_1(g) = A1 (g r1) exp(-g^2 r1^2/4)
+# tabulated on the local tables' g grid; vnorm are the KB energies
+# (cppseudo->vpsnorm) and gzvps0 = v_0(0), the G = 0 value of the s channel
+# (eesProjGchare, cp_ees_nonlocal.C:663-673).
+KB = {
+    "O": dict(A0=6.0, r0=0.55, A1=3.0, r1=0.60, vn0=1.2, vn1=0.6),
+    "H": dict(A0=1.5, r0=0.40, A1=0.6, r1=0.45, vn0=0.4, vn1=0.15),
+}
+
+
+def v_kb(sp, l, g):
+    p = KB[sp]
+    g = np.asarray(g, dtype=np.float64)
+    if l == 0:
+        return p["A0"] * np.exp(-g * g * p["r0"] ** 2 / 4.0)
+    return p["A1"] * (g * p["r1"]) * np.exp(-g * g * p["r1"] ** 2 / 4.0)
+
+
+def nonlocal_channels(species, gmin, dg, nspl):
+    """EES channels (type, l, m) of every species, s then p (m = 0, 1, -1), each
+    with its spline table [4][nspl] on g_i = gmin + i dg, vnorm and gzvps0."""
+    from scipy.interpolate import CubicSpline
+    g = gmin + dg * np.arange(nspl + 1)
+    chans = []
+    for t, sp in enumerate(species):
+        for l, ms in ((0, (0,)), (1, (0, 1, -1))):
+            cs = CubicSpline(g, v_kb(sp, l, g), bc_type="natural")
+            tab = np.stack([cs.c[3, :nspl], cs.c[2, :nspl], cs.c[1, :nspl], cs.c[0, :nspl]])
+            for m in ms:
+                chans.append(dict(type=t, l=l, m=m, vnl=tab,
+                                  gzvps0=float(v_kb(sp, 0, 0.0)) if l == 0 else 0.0,
+                                  vnorm=KB[sp]["vn%d" % l]))
+    return chans
+
+
 def place_atoms(counts, box_len, seed=7, dmin=1.8, max_tries=200000):
     """Seeded uniform positions with a minimum (periodic) distance; returns
     (pos [natm, 3], typ [natm], species list)."""
@@ -157,6 +193,12 @@ class System:
         self.tab = spline_tables(self.species, 0.75 * tpi, gmax, nspl)
         self.alp_ewd = alp_ewd / box_len  # PINY divides the input alpha by the box side
         self.occ = np.ones(self.nstates)
+        self.channels = nonlocal_channels(self.species, self.tab["gmin"], self.tab["dg"],
+                                          self.tab["nspl"])
+
+    def hmati(self):
+        """Inverse cell matrix, column-major 3x3 flattened (cubic box)."""
+        return (np.eye(3) / self.box_len).reshape(-1)
 
     def psi(self, device="cuda"):
         return make_psi(self.layout, self.nstates, seed=self.seed, device=device)

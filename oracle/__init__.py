@@ -14,7 +14,12 @@ and cites the reference ``file:line`` it follows.  Parity pins:
   against the committed fixtures in ``tests/golden``;
 * the Ortho Schulz iteration (``ortho.py``) is checked against the reference's
   ``CPORTHOG::get_iter_Tmat`` compiled from ``cp_lowdin.C`` under ``oracle/_ref``;
-* FFT, density, V.psi, EES, XC, Hartree and integrator arithmetic have no
+* the EES non-local pass (``ees.py``: b(G) weights, spline look-up, atom
+  B-splines, projector, Z matrix, energy, atom and psi forces, NL grid size)
+  is checked against the reference's ``cp_ees_nonlocal.C`` and
+  ``set_cp_ewald.C`` routines compiled from their sources under ``oracle/_ref``
+  (``ref_ees.cpp`` fills the PINY singletons they read);
+* FFT, density, V.psi, XC, Hartree and integrator arithmetic have no
   golden vectors in the reference (its regression datasets are external and
   absent), so they are pinned by mathematical identities (Parseval, electron
   count, adjointness of the forward/backward transforms, finite differences

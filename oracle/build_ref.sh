@@ -4,6 +4,9 @@
 #   src_charm_driver/utility/para_grp_parse.C   flip_data_set, get_chareG_line_prms
 #   src_mathlib/lst_sort_clean.C                sort_commence
 #   src_piny_physics_v1.0/abinito_physics/cp_orthog/cp_lowdin.C   get_iter_Tmat
+#   src_piny_physics_v1.0/abinito_physics/cp_nonlocal/cp_ees_nonlocal.C  EES non-local
+#   src_piny_physics_v1.0/interface/cp_ewald/set_cp_ewald.C  get_bspline_wght1d,
+#                                                           init_nonlocal_ees
 # The shims in oracle/ref_shim stand in for the Charm++/PINY headers, and
 # oracle/ref_mathlib.c for the Fortran GENMATMUL.  Test infrastructure only.
 set -e
@@ -16,11 +19,22 @@ if [ ! -d "$REF/src_charm_driver" ]; then
   exit 0
 fi
 gcc -O2 -fPIC -c "$HERE/ref_mathlib.c" -o "$OUT/ref_mathlib.o"
+# the EES sources read the PINY singletons (CP::get() under CHARM_ON) and the
+# PINY constants/macros (SIMP_NINT as every platform standard_include.h sets)
+PINY="$REF/src_piny_physics_v1.0"
+EESFLAGS="-O2 -fPIC -w -DCHARM_ON -DSIMP_NINT -include $HERE/ref_shim/ees_shim.h \
+  -include $PINY/include/class_defs/piny_constants.h -I $HERE/ref_shim -I $HERE/ref_shim/sub \
+  -I $REF -I $REF/src_charm_driver/utility -I $PINY/include/class_defs -I $REF/include"
+for f in "$PINY/abinito_physics/cp_nonlocal/cp_ees_nonlocal.C" \
+         "$PINY/interface/cp_ewald/set_cp_ewald.C" "$HERE/ref_ees.cpp"; do
+  g++ $EESFLAGS -c "$f" -o "$OUT/$(basename "$f" | sed 's/\.[Cc]p*$//').o"
+done
 g++ -O2 -fPIC -shared -w -o "$OUT/libref.so" \
   -I "$HERE/ref_shim" -I "$HERE/ref_shim/sub" -I "$REF" \
   -I "$REF/src_charm_driver/utility" -I "$REF/src_piny_physics_v1.0/include/class_defs" \
   "$REF/src_charm_driver/utility/para_grp_parse.C" \
   "$REF/src_mathlib/lst_sort_clean.C" \
   "$REF/src_piny_physics_v1.0/abinito_physics/cp_orthog/cp_lowdin.C" \
-  "$HERE/ref_driver.cpp" "$OUT/ref_mathlib.o"
+  "$HERE/ref_driver.cpp" "$OUT/ref_mathlib.o" \
+  "$OUT/cp_ees_nonlocal.o" "$OUT/set_cp_ewald.o" "$OUT/ref_ees.o"
 echo "$OUT/libref.so"
