@@ -102,11 +102,30 @@ class Clocks:
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "--query-gpu=" + q, "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", "--query-gpu=" + q, "--format=csv,noheader,nounits", "-lms", "50",
                  "-i", os.environ.get("LOCAL_RANK", "0")],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+
+    def mark(self):
+        """Samples from here on belong to the timed region."""
+        try:
+            with open(self.path) as f:
+                self.skip = max(0, sum(1 for _ in f) - 1)  # keep the latest sample before
+        except Exception:
+            self.skip = 0
+
+    def ready(self, timeout=5.0):
+        """Wait until the sampler has written its first line (it starts slowly)."""
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < timeout:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    return
+            except OSError:
+                return
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -119,7 +138,9 @@ class Clocks:
         sm, smax, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         try:
-            for line in open(self.path):
+            for k, line in enumerate(open(self.path)):
+                if k < getattr(self, "skip", 0):
+                    continue
                 f = [x.strip() for x in line.split(",")]
                 if len(f) < 9:
                     continue
@@ -178,6 +199,7 @@ def run_ours(args, cfg, name, rank, ws, dist):
     def make(prec):
         ctx = StepContext(sysm.layout, sysm.nstates, precision=prec, device=dev)
         ctx.set_atoms(sysm)
+        ctx.set_nonlocal(sysm)
         ctx.set_cp_mass(TAU_FS, cfg["ecut"])
         return ctx
 
@@ -195,17 +217,19 @@ def run_ours(args, cfg, name, rank, ws, dist):
         first = (energies.cpu().numpy().copy(), forces.cpu().numpy().copy(), ok, it)
         if prec == "fp64":
             e_ref, f_ref = first[0], first[1]
+        clk = Clocks()
+        if prec == "mixed":
+            clk.start()
         for w in range(args.warmup):
             ctx.cp_step(psi, v, occ, DT, 2 + w, energies, forces)
         torch.cuda.synchronize()
         ctx_prof = prec == "mixed"
         if ctx_prof:
             _lib.call("cpstep_ctx_profile", ctx._h, 1)
+        clk.ready()
         barrier(dist)
-        clk = Clocks()
-        if prec == "mixed":
-            clk.start()
         torch.cuda.synchronize()
+        clk.mark()
         n0 = L.cpstep_launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -221,10 +245,10 @@ def run_ours(args, cfg, name, rank, ws, dist):
         phase = None
         if ctx_prof:
             import ctypes
-            arr = (ctypes.c_double * 6)()
+            arr = (ctypes.c_double * 7)()
             nst = ctypes.c_int()
             _lib.call("cpstep_phase_times", ctx._h, arr, ctypes.byref(nst))
-            phase = [arr[i] / max(1, nst.value) for i in range(6)]
+            phase = [arr[i] / max(1, nst.value) for i in range(7)]
             _lib.call("cpstep_ctx_profile", ctx._h, 0)
         it2, ok2 = ctx.step_status()
         out[prec] = dict(ms=ms, launches=launches, clocks=clocks, phase=phase, first=first,
@@ -261,6 +285,7 @@ def cpu_baseline(cfg, sample_states=4):
     at full size (numpy BLAS)."""
     import numpy as np
     from oracle import density as OD
+    from oracle import ees as OE
     from oracle import fftpath as OF
     from oracle import layout as OL
     from oracle import ortho as OO
@@ -278,6 +303,8 @@ def cpu_baseline(cfg, sample_states=4):
     rho = OF.density(sub, lay, occ, vol, chunk=sample_states)
     vks = rho * 0.1
     fv = OF.vpsi_force(sub, vks, lay, occ, chunk=sample_states)
+    OE.nonlocal_ees(sub, lay, occ, vol, sysm.hmati(), dict(pos=sysm.pos, typ=sysm.typ),
+                    sysm.channels, sysm.tab)
     t_fft = (time.perf_counter() - t0) / sample_states
     t0 = time.perf_counter()
     vxc, exc, mu = OD.pz_lda(np.abs(rho) + 1e-8, vol)
@@ -302,7 +329,7 @@ def cpu_baseline(cfg, sample_states=4):
     OO.schulz_tmat(Sm, tol=1e-15, max_iter=10)
     t_ortho = time.perf_counter() - t0
     t_step = t_fft * S + t_dens + t_atom + 4 * t_gemm + t_ortho
-    sample = ("%d of %d states through the FFT/density/V.psi path, the density side with %d of %d "
+    sample = ("%d of %d states through the FFT/density/V.psi/EES non-local path, the density side with %d of %d "
               "atoms (atom loop extrapolated), full-size PairCalc products and Ortho; "
               "per-step time = sum, extrapolated linearly in states/atoms"
               % (sample_states, S, natm_s, sysm.natm))
@@ -317,6 +344,8 @@ def kernel_case(args):
     water192 layout (128^3 grid) in the chosen precision.
     rhoside:  the density-side pass (XC, rho FFT, Hartree/local/Ewald and
     atom forces, V_KS) of the water192 system, run 3 times.
+    ees:      the EES non-local pass of `--states` states of the water192
+    system (8 s+p channels, 80^3 NL grid), run 2 times.
     """
     import torch
     from openatom_b200.context import StepContext
@@ -335,11 +364,17 @@ def kernel_case(args):
             f, e = ctx.vks_psi(psi, v, occ)
             rho = ctx.density(psi, occ)
         chk = float(e.sum())
-    else:
+    elif args.kernel_case == "rhoside":
         ctx.set_atoms(sysm)
         for _ in range(3):
             vks, _, _ = ctx.vks_from_rho(rho)
         chk = float(vks.sum())
+    else:
+        ctx.set_atoms(sysm)
+        ctx.set_nonlocal(sysm)
+        for _ in range(2):
+            fpsi, e, f = ctx.ees_nonlocal(psi, occ)
+        chk = float(e[7])
     torch.cuda.synchronize()
     ctx.close()
     print(json.dumps({"kernel_case": args.kernel_case, "states": S,
@@ -355,7 +390,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="water192", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel-case", choices=["statefft", "rhoside"], default=None,
+    ap.add_argument("--kernel-case", choices=["statefft", "rhoside", "ees"], default=None,
                     help="run a small profiling case instead of the benchmark")
     ap.add_argument("--states", type=int, default=8)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
@@ -405,7 +440,7 @@ def main():
     hbm, peak_kind, pk = peaks()
     c_bytes = 8  # FP32 complex in the mixed path
     ours_b, survey_b, gflops = models(cfg, sysm.layout, out["nlines"], None, out["npts_d"], c_bytes)
-    ph = mixed["phase"] or [0.0] * 6
+    ph = mixed["phase"] or [0.0] * 7
     fft_ms = ph[0] + ph[2]
     achieved = ours_b / (fft_ms * 1e-3) / 1e9 if fft_ms > 0 else None
     gemm_ms = ph[3] + ph[5]
@@ -434,7 +469,8 @@ def main():
         "accuracy_vs_fp64": {"energy_Ha_per_atom": err_e, "local_force_Ha_per_bohr": err_f,
                              "ortho_converged": bool(mixed["ortho_ok"])},
         "phase_ms_mixed": {"density": ph[0], "vks": ph[1], "vpsi_kinetic": ph[2],
-                           "lambda": ph[3], "integrate": ph[4], "ortho_psiT": ph[5]},
+                           "lambda": ph[3], "integrate": ph[4], "ortho_psiT": ph[5],
+                           "ees_nonlocal": ph[6]},
         "roofline": {"bound": "hbm", "kernel": "state FFT + density + V.psi (phases 0+2)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": None,

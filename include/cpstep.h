@@ -73,11 +73,12 @@ CPSTEP_API unsigned long long cpstep_launch_count(void);
  *   0 density (state FFTs G->R, rho)   1 V_KS (XC, rho FFT, Hartree/local/Ewald)
  *   2 V.psi + kinetic (state FFTs R->G) 3 lambda + constraint (PairCalc)
  *   4 integrate                         5 S + Ortho + psi.T (PairCalc, Ortho)
+ *   6 EES non-local (runs between phases 2 and 3)
  * cpstep_phase_times returns the summed milliseconds per phase and the number
  * of profiled steps (synchronises the stream).  The Ortho S->T iteration has
  * no counterpart timer in the reference beyond TimeKeeper's substeps
  * (main/TimeKeeper.h:1-181). */
-#define CPSTEP_NPHASE 6
+#define CPSTEP_NPHASE 7
 CPSTEP_API int cpstep_ctx_profile(cpstep_ctx* ctx, int enable);
 CPSTEP_API int cpstep_phase_times(cpstep_ctx* ctx, double* ms, int* steps);
 
@@ -271,6 +272,39 @@ CPSTEP_API int cpstep_vks_from_rho(cpstep_ctx* ctx, const double* d_rho_r, doubl
                                    double* d_energies, double* d_force);
 
 /* ---------------------------------------------------------------------------
+ * EES non-local pseudopotential (Kleinman-Bylander s and p channels,
+ * src_piny_physics_v1.0/abinito_physics/cp_nonlocal/cp_ees_nonlocal.C).
+ *
+ * cpstep_nl_grid_size: the NL FFT grid of init_nonlocal_ees
+ *   (interface/cp_ewald/set_cp_ewald.C:1329-1400) for a cubic box: the first
+ *   set_fftsizes entry >= int(2 scale (kmax+1)) (+1 if below 2 (kmax+1)).
+ *   Returns the size, or -1 if the table has none.
+ * cpstep_set_nonlocal: channels of the reference's iter_nl loop (lang_v,
+ *   mang_v, ityp_v): ch_type (0-based type of cpstep_set_atoms), ch_l in
+ *   {0, 1}, ch_m in [-l, l]; vnl[nchan][4][nspl] the channel's radial spline
+ *   (vps0..vps3 of its type and l) on the g grid of cpstep_set_atoms; gz0[nchan]
+ *   the G = 0 value of an s channel (gzvps0); vnorm[nchan] (vpsnorm).  nkf the
+ *   NL grid (cpstep_nl_grid_size), n_interp the B-spline order (8).  Forms the
+ *   projector dyp = Ylm b(G) v_l(|G|) of eesSetEesWghtGgrp / eesYlmOnD /
+ *   eesProjGchare (:60-240, :594-1236) once.  Host pointers, copied.  Call
+ *   after cpstep_set_atoms.  cpstep_cp_step includes the non-local pass once
+ *   this is set.
+ * cpstep_ees_nonlocal: for every state and channel, projPsiG = conj(dyp psi)
+ *   -> NL grid (doNlFFTGtoR) -> Z = sum projPsiR Mn over each atom's
+ *   8x8x8 B-spline stencil (eesAtmBsplineRgrp, eesZmatRchare) -> E_NL +=
+ *   Z^2 vnorm/vol occ, F_atom -= Z' sum projPsiR dMn, scatter Z' Mn with
+ *   Z' = 2 vnorm/vol occ Z (eesEnergyAtmForcRchare) -> NL R->G -> d_fpsi +=
+ *   -w conj(dyp projPsiG') (eesPsiForcGspace).  d_energies[E_NL] is written,
+ *   d_fatm[natm][3] (may be NULL) accumulated, d_fpsi accumulated.
+ */
+CPSTEP_API int cpstep_nl_grid_size(int kmax, double scale, int n_interp);
+CPSTEP_API int cpstep_set_nonlocal(cpstep_ctx* ctx, int nkf, int n_interp, int nchan,
+                                   const int* ch_type, const int* ch_l, const int* ch_m,
+                                   const double* vnl, const double* gz0, const double* vnorm);
+CPSTEP_API int cpstep_ees_nonlocal(cpstep_ctx* ctx, const double* d_psi, const double* d_occ,
+                                   double* d_fpsi, double* d_energies, double* d_fatm);
+
+/* ---------------------------------------------------------------------------
  * Integrator and the fused electronic step.
  *
  * cpstep_set_cp_mass: CP coefficient masses of set_cpmass (src_piny_physics_v1.0/
@@ -284,10 +318,12 @@ CPSTEP_API int cpstep_vks_from_rho(cpstep_ctx* ctx, const double* d_rho_r, doubl
  *   overwritten by the conjugate of its partner (sendRedPsi/unpackRedPsi,
  *   CP_State_GSpacePlane.C:2862-3061).  d_force: the constrained force.
  * cpstep_cp_step: one electronic step on orthonormal psi (S = 2 I):
- *   rho -> V_KS (XC, Hartree, local, Ewald) -> F = V.psi + kinetic force ->
+ *   rho -> V_KS (XC, Hartree, local, Ewald) -> F = V.psi + kinetic force
+ *   (+ the EES non-local force when cpstep_set_nonlocal was called) ->
  *   lambda = <psi|F>, F <- F - wpt/2 psi.lambda -> Verlet -> S -> T = (S/2)^-1/2
  *   -> psi <- psi.T.  d_energies (CPSTEP_NENERGY doubles, device) receives
- *   every slot; d_atom_force (may be NULL) the local + Ewald atom forces.
+ *   every slot; d_atom_force (may be NULL) the local + Ewald (+ non-local)
+ *   atom forces.
  *   Asynchronous: the Ortho convergence of the step is read by cpstep_step_status.
  * cpstep_step_status: iterations and convergence flag of the last Ortho launch
  *   (synchronises the context's stream).

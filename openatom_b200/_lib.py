@@ -70,6 +70,11 @@ SIGNATURES = {
     "cpstep_hart_eext": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "cpstep_vks_fft_g2r": (ctypes.c_int, [_vp, _vp, _vp]),
     "cpstep_vks_from_rho": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cpstep_nl_grid_size": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+    "cpstep_set_nonlocal": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           _c_int_p, _c_int_p, _c_int_p, _c_dbl_p, _c_dbl_p,
+                                           _c_dbl_p]),
+    "cpstep_ees_nonlocal": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "cpstep_set_cp_mass": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
     "cpstep_cp_integrate": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int,
                                            _vp]),

@@ -187,6 +187,36 @@ class StepContext:
                   float(system.alp_ewd))
         self.natm = len(system.typ)
 
+    def set_nonlocal(self, system, nkf=None):
+        """EES non-local channels of `system` (cpstep_set_nonlocal); nkf defaults
+        to the reference's NL grid rule for the layout's kmax."""
+        import numpy as np
+        chans = system.channels
+        if nkf is None:
+            nkf = _lib.lib().cpstep_nl_grid_size(int(self.layout.kmax), 1.2, 8)
+        ct, pct = _lib.int_array([c["type"] for c in chans])
+        cl, pcl = _lib.int_array([c["l"] for c in chans])
+        cm, pcm = _lib.int_array([c["m"] for c in chans])
+        vnl = np.ascontiguousarray(np.stack([c["vnl"] for c in chans]), dtype=np.float64)
+        gz = np.ascontiguousarray([c["gzvps0"] for c in chans], dtype=np.float64)
+        vn = np.ascontiguousarray([c["vnorm"] for c in chans], dtype=np.float64)
+        dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        self._sync_stream()
+        _lib.call("cpstep_set_nonlocal", self._h, int(nkf), 8, len(chans), pct, pcl, pcm,
+                  dp(vnl), dp(gz), dp(vn))
+        self.nkf = int(nkf)
+        return self.nkf
+
+    def ees_nonlocal(self, psi, occ, fpsi=None, forces=True):
+        """EES non-local pass: returns (fpsi accumulated, energies, atom forces)."""
+        self._sync_stream()
+        if fpsi is None:
+            fpsi = torch.zeros_like(psi)
+        e = self._energies()
+        f = torch.zeros((self.natm, 3), dtype=torch.float64, device=self.device) if forces else None
+        _lib.call("cpstep_ees_nonlocal", self._h, ptr(psi), ptr(occ), ptr(fpsi), ptr(e), ptr(f))
+        return fpsi, e, f
+
     def rho_layout(self):
         import numpy as np
         n = ctypes.c_int()

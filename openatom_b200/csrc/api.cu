@@ -105,6 +105,9 @@ __global__ void k_rowsum2(const double* __restrict__ part, int ncol, int nrow,
 
 }  // namespace
 
+// step intervals in time order -> phase numbers of the header (EES runs third)
+static const int kPhaseOfInterval[CPSTEP_NPHASE] = {0, 1, 2, 6, 3, 4, 5};
+
 int prof_fold(cpstep_ctx* c) {
   if (c->prof_pending == 0) return CPSTEP_OK;
   const int W = CPSTEP_NPHASE + 1;
@@ -114,7 +117,7 @@ int prof_fold(cpstep_ctx* c) {
       float ms = 0.f;
       CPSTEP_CUDA_TRY(cudaEventElapsedTime(&ms, c->prof_ev[(size_t)s * W + k],
                                            c->prof_ev[(size_t)s * W + k + 1]));
-      c->prof_ms[k] += ms;
+      c->prof_ms[kPhaseOfInterval[k]] += ms;
     }
   c->prof_steps += c->prof_pending;
   c->prof_pending = 0;
@@ -266,6 +269,7 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
   cudaFree(c->d_pc_part); cudaFree(c->d_ortho_ws); cudaFree(c->d_hmati);
   cudaFree(c->d_force_atoms);
   for (auto& e : c->prof_ev) cudaEventDestroy(e);
+  nl_free(c);
   rho_free(c);
   step_free(c);
   statefft_free(c);
@@ -429,6 +433,29 @@ int cpstep_vks_from_rho(cpstep_ctx* c, const double* d_rho_r, double* d_vks_r,
   if (int rc = rho_r2g(c, d_rho_r)) return rc;
   if (int rc = rho_hart(c, d_energies, d_force)) return rc;
   return rho_vks_r(c, d_vks_r);
+}
+
+int cpstep_nl_grid_size(int kmax, double scale, int n_interp) {
+  return nl_grid_size(kmax, scale, n_interp);
+}
+
+int cpstep_set_nonlocal(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type,
+                        const int* ch_l, const int* ch_m, const double* vnl, const double* gz0,
+                        const double* vnorm) {
+  if (!c || nchan <= 0 || !ch_type || !ch_l || !ch_m || !vnl || !gz0 || !vnorm) {
+    cpstep_set_error("set_nonlocal: bad argument");
+    return CPSTEP_ERR_ARG;
+  }
+  return nl_set(c, nkf, n_interp, nchan, ch_type, ch_l, ch_m, vnl, gz0, vnorm);
+}
+
+int cpstep_ees_nonlocal(cpstep_ctx* c, const double* d_psi, const double* d_occ, double* d_fpsi,
+                        double* d_energies, double* d_fatm) {
+  if (!c || !d_psi || !d_occ || !d_fpsi || !d_energies) {
+    cpstep_set_error("ees_nonlocal: bad argument");
+    return CPSTEP_ERR_ARG;
+  }
+  return nl_run(c, d_psi, d_occ, d_fpsi, d_energies, d_fatm);
 }
 
 int cpstep_set_cp_mass(cpstep_ctx* c, double tau_fs, double cut_ry) {

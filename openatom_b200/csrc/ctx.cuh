@@ -27,6 +27,32 @@ struct FftJob {
   void* pen_b;  // [nstates][nz][nlpad] pencils of the R->G pass
 };
 
+// EES non-local: the atoms' B-spline factors on the NL grid (per atom a, axis
+// d = a, b, c and interpolation point j < 8; eesAtmBsplineRgrp,
+// cp_ees_nonlocal.C:256-580) as the NL plane kernels read them.
+constexpr int kNlInterp = 8;
+struct NlAtoms {
+  int natm;
+  const int* typ;      // [natm]
+  const int* ig;       // [natm][3][8] 0-based grid index along a, b, c
+  const double* mn;    // [natm][3][8] M_n factors
+  const double* dmn;   // [natm][3][8] their derivatives
+  double hmati[9];
+  double grid;         // NL grid size (cubic)
+  // per (type, plane): the atoms of the type with an interpolation plane there,
+  // atom | (jc << 16) in atom order, and their count
+  const int* plist;    // [ntyp][nkf][natm]
+  const int* pcount;   // [ntyp][nkf]
+};
+
+// One channel's NL pass on the NL grid: geometry, pencils, twiddles, atoms.
+struct NlJob {
+  FftJob f;
+  const void* tw;      // [nkf] twiddles in working precision
+  NlAtoms A;
+  int ctype;           // atom type of the channel
+};
+
 // Per-grid-size FFT entry points (compile-time N inside).
 struct StateFftOps {
   int (*density)(cpstep_ctx*, const double*, const double*, double*);
@@ -35,6 +61,11 @@ struct StateFftOps {
   int (*rtog)(cpstep_ctx*, const double*, double*, int);
   int (*g2r)(cpstep_ctx*, const FftJob&, const double*, double*, int);
   int (*r2g)(cpstep_ctx*, const FftJob&, const double*, double*, int, double);
+  // EES on this grid size: conj(dyp psi) -> NL grid -> per-plane atom sums
+  // zpart[s][atom][8][4]; scatter of zs[s][atom] -> NL grid -> fpsi +=
+  int (*nl_proj)(cpstep_ctx*, const NlJob&, const double*, const double2*, int, double*);
+  int (*nl_force)(cpstep_ctx*, const NlJob&, const double*, const double2*, int, double*);
+  size_t (*nl_smem)(int nplane_x);
   int lb;  // z-lines per block of the z-passes
 };
 template <typename T, int N>
@@ -72,6 +103,26 @@ struct AtomData {
   double* pos = nullptr;  // staging for cpstep_set_positions
 };
 
+// EES non-local state of a context (cpstep_set_nonlocal).
+struct NlData {
+  int on = 0, nkf = 0, nchan = 0;
+  std::vector<int> ch_type;
+  std::vector<double> ch_vn;        // vnorm / vol per channel
+  double2* dyp = nullptr;           // [nchan][npts] projector b(G) Ylm v_l(g)
+  int *line_zneg = nullptr, *line_zpos = nullptr, *line_xy = nullptr;  // NL-grid lines
+  void *pen_a = nullptr, *pen_b = nullptr;  // [nstates][nkf][nlpad]
+  void* tw = nullptr;               // [nkf] twiddles, working precision
+  StateFftOps ops;
+  int* ig = nullptr;                // [natm][3][8]
+  int *plist = nullptr, *pcount = nullptr;  // per-plane atom lists (NlAtoms)
+  double *mn = nullptr, *dmn = nullptr;
+  double* zpart = nullptr;          // [nstates][natm][8][4]
+  double* zs = nullptr;             // [nstates][natm]
+  double* enl_s = nullptr;          // [nstates]
+  double* fnl = nullptr;            // [nstates][natm][3]
+  int natm = 0;
+};
+
 template <typename T>
 struct Twiddles {
   cplx<T>* x = nullptr;
@@ -104,6 +155,7 @@ struct cpstep_ctx {
   StateFftOps ops64;  // FP64 (density path)
   RhoGeom rg;
   AtomData atoms;
+  NlData nl;
   int rho_izero = -1;
   double* d_energies = nullptr;  // [CPSTEP_NENERGY]
   // electronic step
@@ -175,6 +227,16 @@ int statefft_vpsi(cpstep_ctx* c, const double* psi, const double* vks, const dou
                   double* force, double* eke, int pencils_ready);
 int statefft_gtor(cpstep_ctx* c, const double* psi, double* psi_r, int nstates);
 int statefft_rtog(cpstep_ctx* c, const double* f_r, double* fg, int nstates);
+
+int statefft_lookup(int precision, int n, StateFftOps* o);
+
+// ees.cu
+int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, const int* ch_l,
+           const int* ch_m, const double* vnl, const double* gz0, const double* vnorm);
+void nl_free(cpstep_ctx* c);
+int nl_run(cpstep_ctx* c, const double* psi, const double* occ, double* fpsi, double* energies,
+           double* fatm);
+int nl_grid_size(int kmax, double scale, int n_interp);
 
 // rhopath.cu
 int rho_init(cpstep_ctx* c, double box_len, double ecut_ry);

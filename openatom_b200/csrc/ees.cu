@@ -1,0 +1,428 @@
+// EES non-local pseudopotential (Euler exponential spline, Kleinman-Bylander
+// s and p channels) for every state on one GPU.
+//
+//   set-up                       eesSetEesWghtGgrp / get_bspline_wght1d / eesSplProjectorGgrp
+//                                (src_piny_physics_v1.0/abinito_physics/cp_nonlocal/
+//                                cp_ees_nonlocal.C:60-240, interface/cp_ewald/set_cp_ewald.C:1237-1322)
+//   atom B-splines               eesAtmBsplineRgrp  cp_ees_nonlocal.C:256-580
+//   projector x psi, NL G->R     eesProjGchare / eesYlmOnD :594-1236, doNlFFTGtoR (fftCache.C)
+//   Z matrix, energy, forces     eesZmatRchare :1238-1346, eesEnergyAtmForcRchare :1480-1700
+//   scatter, NL R->G, psi force  eesEnergyAtmForcRchare, doNlFFTRtoG, eesPsiForcGspace :2000-2064
+//
+// The reference runs one (state, channel) per chare pair with the NL grid
+// split into planes; here one channel at a time runs for all states: K1 with
+// the projector (conj(dyp psi)), a plane kernel that finishes the G->R
+// transform in shared memory and forms each atom's per-plane sums, a small
+// kernel for Z, E_NL, the atom forces and the scaled Z, a plane kernel that
+// scatters Z Mn and starts the R->G transform, and K4 adding the psi force.
+// The projector dyp depends on the cell only and is formed once at set-up.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+#include "ctx.cuh"
+
+namespace ees {
+
+// eesAtmBsplineRgrp I-III for one atom and axis: grid indices, M_n and dM_n.
+__global__ void k_nl_bspline(const double* __restrict__ frac, int natm, int nkf,
+                             int* __restrict__ ig, double* __restrict__ mn,
+                             double* __restrict__ dmn) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natm) return;
+  constexpr int n_interp = kNlInterp;
+  const double grid = (double)nkf;
+  for (int d = 0; d < 3; ++d) {
+    double t = frac[3 * a + d];
+    const double xm = t - 0.5;
+    t -= (double)(int)(xm >= 0.0 ? xm + 0.5 : xm - 0.5);  // NINT, SIMP_NINT form
+    t = (t == 1.0) ? 0.0 : t;
+    t = t * grid;
+    const int it = (int)t;
+    const double fr = t - (double)it;
+    double u[n_interp], m[n_interp], dm[n_interp];
+    int* igo = ig + ((size_t)a * 3 + d) * n_interp;
+#pragma unroll
+    for (int j = 1; j <= n_interp; ++j) {
+      u[j - 1] = fr + (double)(j - 1);
+      int idx = it - (j - 2);
+      idx = (idx > 0) ? idx : nkf + idx;
+      idx = (idx <= nkf) ? idx : idx - nkf;
+      igo[j - 1] = min(max(idx, 1), nkf) - 1;  // in [1, nkf] already; kept as a bound
+      m[j - 1] = 0.0;
+      dm[j - 1] = 0.0;
+    }
+    m[0] = 1.0 - fabs(u[0] - 1.0);
+    m[1] = 1.0 - fabs(u[1] - 1.0);
+#pragma unroll
+    for (int n = 3; n <= n_interp; ++n) {
+      const double rn = (double)n, rn1 = 1.0 / (double)(n - 1);
+#pragma unroll
+      for (int j = n; j >= 2; --j) m[j - 1] = (u[j - 1] * m[j - 1] + (rn - u[j - 1]) * m[j - 2]) * rn1;
+      m[0] = u[0] * m[0] * rn1;
+      if (n == n_interp - 1) {
+        dm[0] = m[0];
+#pragma unroll
+        for (int j = 2; j <= n_interp; ++j) dm[j - 1] = m[j - 1] - m[j - 2];
+      }
+    }
+    double* mo = mn + ((size_t)a * 3 + d) * n_interp;
+    double* dmo = dmn + ((size_t)a * 3 + d) * n_interp;
+#pragma unroll
+    for (int j = 0; j < n_interp; ++j) {
+      mo[j] = m[j];
+      dmo[j] = dm[j];
+    }
+  }
+}
+
+// Per (type, plane) lists of the atoms with an interpolation plane there, in
+// atom order (so the scatter of the R->G kernel adds in a fixed order).
+// One warp per (type, plane): 32 atoms per step, ballot + prefix count keep
+// the atom order.
+__global__ void k_nl_planes(const int* __restrict__ typ, const int* __restrict__ ig, int natm,
+                            int ntyp, int nkf, int* __restrict__ plist,
+                            int* __restrict__ pcount) {
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= ntyp * nkf) return;
+  const int t = i / nkf, z = i - t * nkf;
+  int* out = plist + (size_t)i * natm;
+  int n = 0;
+  for (int a0 = 0; a0 < natm; a0 += 32) {
+    const int a = a0 + lane;
+    int jc = -1;
+    if (a < natm && typ[a] == t) {
+      const int* c = ig + ((size_t)a * 3 + 2) * kNlInterp;
+#pragma unroll
+      for (int k = 0; k < kNlInterp; ++k)
+        if (c[k] == z) jc = k;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, jc >= 0);
+    if (jc >= 0) out[n + __popc(m & ((1u << lane) - 1u))] = a | (jc << 16);
+    n += __popc(m);
+  }
+  if (lane == 0) pcount[i] = n;
+}
+
+// Z_a = sum over the atom's planes, E_NL += Z^2 vn occ, Z <- 2 vn occ Z,
+// F_a -= Z sum P dMn (eesEnergyAtmForcRchare :1545-1560, :1596-1600).
+// One block per state; atoms of the channel's type.
+__global__ void k_nl_zmat(const double* __restrict__ zpart, NlAtoms A, int ctype, double vn,
+                          const double* __restrict__ occ, double* __restrict__ zs,
+                          double* __restrict__ enl_s, double* __restrict__ fnl) {
+  __shared__ double red[32];
+  const int s = blockIdx.x;
+  const double w = occ[s];
+  double e = 0.0;
+  for (int a = threadIdx.x; a < A.natm; a += blockDim.x) {
+    if (A.typ[a] != ctype) continue;
+    const double* zp = zpart + ((size_t)s * A.natm + a) * kNlInterp * 4;
+    double z = 0.0, dx = 0.0, dy = 0.0, dz = 0.0;
+#pragma unroll
+    for (int jc = 0; jc < kNlInterp; ++jc) {
+      z += zp[4 * jc];
+      dx += zp[4 * jc + 1];
+      dy += zp[4 * jc + 2];
+      dz += zp[4 * jc + 3];
+    }
+    e += z * z * vn * w;
+    const double zsc = z * (2.0 * vn * w);
+    zs[(size_t)s * A.natm + a] = zsc;
+    double* f = fnl + ((size_t)s * A.natm + a) * 3;
+    f[0] -= dx * zsc;
+    f[1] -= dy * zsc;
+    f[2] -= dz * zsc;
+  }
+  e = block_sum(e, red);
+  if (threadIdx.x == 0) enl_s[s] += e;
+}
+
+// energies[E_NL] = sum_s enl_s[s]; fatm[a][k] += sum_s fnl[s][a][k] (fixed order)
+__global__ void k_nl_finish(const double* __restrict__ enl_s, const double* __restrict__ fnl,
+                            int nstates, int natm, double* __restrict__ energies,
+                            double* __restrict__ fatm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0 && energies) {
+    double e = 0.0;
+    for (int s = 0; s < nstates; ++s) e += enl_s[s];
+    energies[CPSTEP_E_NL] = e;
+  }
+  if (fatm && i < 3 * natm) {
+    double f = 0.0;
+    for (int s = 0; s < nstates; ++s) f += fnl[(size_t)s * 3 * natm + i];
+    fatm[i] += f;
+  }
+}
+
+}  // namespace ees
+
+// ===========================================================================
+// host side
+
+namespace {
+
+// get_bspline_wght1d (set_cp_ewald.C:1237-1322): the complex 1/b(m) factors
+// for m = 0 .. ngrid-1 of the order-n_interp cardinal B-spline.
+void bspline_wght1d(int n_interp, int ngrid, std::vector<double>& br, std::vector<double>& bi) {
+  std::vector<double> mnk(n_interp + 1, 0.0), uk(n_interp + 1, 0.0);
+  mnk[1] = 1.0;
+  uk[1] = 1.0;
+  for (int k = 2; k <= n_interp; ++k) uk[k] = (double)k;
+  for (int n = 3; n <= n_interp; ++n) {
+    const double rn = (double)n, rn1 = 1.0 / (double)(n - 1);
+    for (int k = n; k >= 2; --k) mnk[k] = (uk[k] * mnk[k] + (rn - uk[k]) * mnk[k - 1]) * rn1;
+    mnk[1] = uk[1] * mnk[1] * rn1;
+  }
+  const double grid = (double)ngrid;
+  const double tpi_n = 2.0 * M_PI / grid;
+  br.assign(ngrid, 0.0);
+  bi.assign(ngrid, 0.0);
+  for (int m = 0; m < ngrid; ++m) {
+    double r = 0.0, i = 0.0;
+    for (int k = 1; k <= n_interp - 1; ++k) {
+      const double arg = tpi_n * (double)((k - 1) * m);
+      r += cos(arg) * mnk[k];
+      i += sin(arg) * mnk[k];
+    }
+    const double arg = 2.0 * M_PI * (double)(n_interp - 1) / grid * (double)m;
+    const double nr = cos(arg), ni = sin(arg);
+    const double den = r * r + i * i;
+    br[m] = (nr * r + ni * i) / den;
+    bi[m] = (ni * r - nr * i) / den;
+  }
+}
+
+template <typename T>
+int upload_tw_n(int n, void** dst) {
+  std::vector<cplx<T>> h(n);
+  for (int m = 0; m < n; ++m) {
+    double a = -2.0 * M_PI * (double)m / (double)n;
+    h[m] = mk<T>((T)cos(a), (T)sin(a));
+  }
+  CPSTEP_CUDA_TRY(cudaMalloc(dst, sizeof(cplx<T>) * n));
+  CPSTEP_CUDA_TRY(cudaMemcpy(*dst, h.data(), sizeof(cplx<T>) * n, cudaMemcpyHostToDevice));
+  return CPSTEP_OK;
+}
+
+int wrap(int v, int n) { return v < 0 ? v + n : v; }
+
+}  // namespace
+
+void nl_free(cpstep_ctx* c) {
+  NlData& n = c->nl;
+  cudaFree(n.dyp); cudaFree(n.line_zneg); cudaFree(n.line_zpos); cudaFree(n.line_xy);
+  cudaFree(n.pen_a); cudaFree(n.pen_b); cudaFree(n.tw); cudaFree(n.ig); cudaFree(n.mn);
+  cudaFree(n.dmn); cudaFree(n.zpart); cudaFree(n.zs); cudaFree(n.enl_s); cudaFree(n.fnl);
+  cudaFree(n.plist); cudaFree(n.pcount);
+  n = NlData();
+}
+
+int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, const int* ch_l,
+           const int* ch_m, const double* vnl, const double* gz0, const double* vnorm) {
+  const AtomData& at = c->atoms;
+  if (at.natm <= 0) {
+    cpstep_set_error("set_nonlocal: call cpstep_set_atoms first");
+    return CPSTEP_ERR_STATE;
+  }
+  if (n_interp != kNlInterp || nkf < n_interp || nchan <= 0) {
+    cpstep_set_error("set_nonlocal: n_interp must be %d, nkf >= n_interp, nchan > 0", kNlInterp);
+    return CPSTEP_ERR_ARG;
+  }
+  for (int k = 0; k < nchan; ++k) {
+    if (ch_type[k] < 0 || ch_type[k] >= at.ntyp || ch_l[k] < 0 || ch_l[k] > 1 ||
+        ch_m[k] < -ch_l[k] || ch_m[k] > ch_l[k]) {
+      cpstep_set_error("set_nonlocal: channel %d (type %d, l %d, m %d) not supported (s, p)", k,
+                       ch_type[k], ch_l[k], ch_m[k]);
+      return CPSTEP_ERR_ARG;
+    }
+  }
+  // the state sphere must fit the NL grid: |k| < nkf / 2 on every axis
+  int km = 0;
+  for (int p = 0; p < c->npts; ++p)
+    km = std::max(km, std::max(std::abs(c->h_kx[p]), std::max(std::abs(c->h_ky[p]),
+                                                               std::abs(c->h_kz[p]))));
+  if (2 * km >= nkf) {
+    cpstep_set_error("set_nonlocal: NL grid %d too small for |k| <= %d", nkf, km);
+    return CPSTEP_ERR_ARG;
+  }
+  StateFftOps ops;
+  if (!statefft_lookup(c->precision, nkf, &ops)) {
+    cpstep_set_error("set_nonlocal: NL grid size %d not built into libcpstep", nkf);
+    return CPSTEP_ERR_ARG;
+  }
+  if (ops.nl_smem(c->nplane_x) > 227 * 1024) {
+    cpstep_set_error("set_nonlocal: NL plane of %d x %d does not fit shared memory in this "
+                     "precision", nkf, nkf);
+    return CPSTEP_ERR_ARG;
+  }
+  nl_free(c);
+  NlData& n = c->nl;
+  n.nkf = nkf;
+  n.nchan = nchan;
+  n.ops = ops;
+  n.natm = at.natm;
+  n.ch_type.assign(ch_type, ch_type + nchan);
+  n.ch_vn.resize(nchan);
+  for (int k = 0; k < nchan; ++k) n.ch_vn[k] = vnorm[k] / c->vol;
+  // NL-grid line tables from the state lines
+  const int nl = c->nlines;
+  std::vector<int> zneg(nl), zpos(nl), xy(nl);
+  for (int l = 0; l < nl; ++l) {
+    const int off = c->h_line_off[l];
+    const int end = (l + 1 < nl) ? c->h_line_off[l + 1] : c->npts;
+    int nneg = 0;
+    while (off + nneg < end && c->h_kz[off + nneg] < 0) ++nneg;
+    zneg[l] = nneg > 0 ? wrap(c->h_kz[off], nkf) : 0;
+    zpos[l] = (off + nneg < end) ? wrap(c->h_kz[off + nneg], nkf) : 0;
+    xy[l] = wrap(c->h_kx[off], nkf) | (wrap(c->h_ky[off], nkf) << 16);
+  }
+  auto up = [&](int** d, const std::vector<int>& h) -> int {
+    CPSTEP_CUDA_TRY(cudaMalloc(d, sizeof(int) * h.size()));
+    CPSTEP_CUDA_TRY(cudaMemcpy(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
+    return CPSTEP_OK;
+  };
+  int rc;
+  if ((rc = up(&n.line_zneg, zneg)) || (rc = up(&n.line_zpos, zpos)) || (rc = up(&n.line_xy, xy)))
+    return rc;
+  // projector dyp per channel and point (eesSetEesWghtGgrp, eesYlmOnD, eesProjGchare)
+  std::vector<double> br, bi;
+  bspline_wght1d(n_interp, nkf, br, bi);
+  const double fpi = 4.0 * M_PI;
+  const double y00 = 1.0 / sqrt(fpi), y10 = sqrt(3.0 / fpi), y11 = sqrt(1.5 / fpi) * sqrt(2.0);
+  const double* h = c->hmati;
+  const double tpi = 2.0 * M_PI;
+  std::vector<double2> dyp((size_t)nchan * c->npts);
+  for (int p = 0; p < c->npts; ++p) {
+    const int ka = c->h_kx[p], kb = c->h_ky[p], kc = c->h_kz[p];
+    const int ia = wrap(ka, nkf), ib = wrap(kb, nkf), ic = wrap(kc, nkf);
+    double abr = br[ia] * br[ib] - bi[ia] * bi[ib];
+    double abi = bi[ia] * br[ib] + br[ia] * bi[ib];
+    double dre = abr * br[ic] - abi * bi[ic];
+    double dim = abi * br[ic] + abr * bi[ic];
+    const bool g0 = (ka == 0 && kb == 0 && kc == 0);
+    if (g0) {
+      dre = br[0] * br[0] * br[0];
+      dim = 0.0;
+    }
+    const double xk = (ka * h[0] + kb * h[1] + kc * h[2]) * tpi;
+    const double yk = (ka * h[3] + kb * h[4] + kc * h[5]) * tpi;
+    const double zk = (ka * h[6] + kb * h[7] + kc * h[8]) * tpi;
+    const double g = sqrt(xk * xk + yk * yk + zk * zk);
+    int iii = (int)((g - at.gmin) / at.dg + 1.0);
+    iii = std::min(iii, at.nspl);
+    iii = std::max(iii, 1);
+    double hh = g - ((double)(iii - 1) * at.dg + at.gmin);
+    if (g < 1.0e-12) {
+      hh = 0.0;
+      iii = 1;
+    }
+    for (int k = 0; k < nchan; ++k) {
+      double yr, yi;
+      if (ch_l[k] == 0) {
+        yr = dre * y00;
+        yi = dim * y00;
+      } else if (g != 0.0) {
+        double y;
+        if (ch_m[k] == 0) {
+          y = y10 * (zk / g);
+        } else {
+          const double gs = sqrt(xk * xk + yk * yk);
+          const double ph = (ch_m[k] == 1) ? (gs == 0.0 ? 1.0 : xk / gs)
+                                           : (gs == 0.0 ? 0.0 : yk / gs);
+          y = y11 * (gs / g) * ph;
+        }
+        yr = -dim * y;
+        yi = dre * y;
+      } else {
+        yr = yi = 0.0;
+      }
+      double2 v;
+      if (g0) {
+        v = (ch_l[k] == 0) ? make_double2(yr * gz0[k], 0.0) : make_double2(0.0, 0.0);
+      } else {
+        const double* t = vnl + (size_t)k * 4 * at.nspl + (iii - 1);
+        const double vnow =
+            ((t[3 * at.nspl] * hh + t[2 * at.nspl]) * hh + t[at.nspl]) * hh + t[0];
+        v = make_double2(yr * vnow, yi * vnow);
+      }
+      dyp[(size_t)k * c->npts + p] = v;
+    }
+  }
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.dyp, sizeof(double2) * dyp.size()));
+  CPSTEP_CUDA_TRY(cudaMemcpy(n.dyp, dyp.data(), sizeof(double2) * dyp.size(),
+                             cudaMemcpyHostToDevice));
+  const bool fp64 = c->precision == CPSTEP_PREC_FP64;
+  if ((rc = fp64 ? upload_tw_n<double>(nkf, &n.tw) : upload_tw_n<float>(nkf, &n.tw))) return rc;
+  const size_t csz = fp64 ? sizeof(cplx<double>) : sizeof(cplx<float>);
+  const size_t pen = (size_t)c->nstates * nkf * c->nlpad * csz;
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.pen_a, pen));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.pen_b, pen));
+  const size_t na = (size_t)at.natm;
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.ig, sizeof(int) * na * 3 * kNlInterp));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.mn, sizeof(double) * na * 3 * kNlInterp));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.dmn, sizeof(double) * na * 3 * kNlInterp));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.plist, sizeof(int) * (size_t)at.ntyp * nkf * na));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.pcount, sizeof(int) * (size_t)at.ntyp * nkf));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.zpart, sizeof(double) * c->nstates * na * kNlInterp * 4));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.zs, sizeof(double) * c->nstates * na));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.enl_s, sizeof(double) * c->nstates));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.fnl, sizeof(double) * c->nstates * na * 3));
+  n.on = 1;
+  return CPSTEP_OK;
+}
+
+int nl_run(cpstep_ctx* c, const double* psi, const double* occ, double* fpsi, double* energies,
+           double* fatm) {
+  NlData& n = c->nl;
+  if (!n.on) {
+    cpstep_set_error("ees_nonlocal: call cpstep_set_nonlocal first");
+    return CPSTEP_ERR_STATE;
+  }
+  if (n.natm != c->atoms.natm) {
+    cpstep_set_error("ees_nonlocal: atoms changed since cpstep_set_nonlocal");
+    return CPSTEP_ERR_STATE;
+  }
+  const int S = c->nstates, natm = n.natm;
+  ees::k_nl_bspline<<<cdiv(natm, 128), 128, 0, c->stream>>>(c->atoms.frac, natm, n.nkf, n.ig,
+                                                            n.mn, n.dmn);
+  CPSTEP_LAUNCH_CHECK();
+  const int ntyp = c->atoms.ntyp;
+  ees::k_nl_planes<<<cdiv(ntyp * n.nkf, 8), 256, 0, c->stream>>>(c->atoms.typ, n.ig, natm, ntyp,
+                                                                  n.nkf, n.plist, n.pcount);
+  CPSTEP_LAUNCH_CHECK();
+  CPSTEP_CUDA_TRY(cudaMemsetAsync(n.enl_s, 0, sizeof(double) * S, c->stream));
+  CPSTEP_CUDA_TRY(cudaMemsetAsync(n.fnl, 0, sizeof(double) * S * natm * 3, c->stream));
+  NlJob j;
+  j.f.g = c->geom();
+  j.f.g.nx = j.f.g.ny = j.f.g.nz = n.nkf;
+  j.f.g.line_zneg = n.line_zneg;
+  j.f.g.line_zpos = n.line_zpos;
+  j.f.g.line_xy = n.line_xy;
+  j.f.pen_a = n.pen_a;
+  j.f.pen_b = n.pen_b;
+  j.tw = n.tw;
+  j.A.natm = natm;
+  j.A.typ = c->atoms.typ;
+  j.A.ig = n.ig;
+  j.A.mn = n.mn;
+  j.A.dmn = n.dmn;
+  for (int k = 0; k < 9; ++k) j.A.hmati[k] = c->hmati[k];
+  j.A.grid = (double)n.nkf;
+  j.A.plist = n.plist;
+  j.A.pcount = n.pcount;
+  const int zt = std::min(1024, std::max(32, cdiv(natm, 32) * 32));
+  for (int k = 0; k < n.nchan; ++k) {
+    j.ctype = n.ch_type[k];
+    const double2* dyp = n.dyp + (size_t)k * c->npts;
+    int rc;
+    if ((rc = n.ops.nl_proj(c, j, psi, dyp, S, n.zpart))) return rc;
+    ees::k_nl_zmat<<<S, zt, 0, c->stream>>>(n.zpart, j.A, j.ctype, n.ch_vn[k], occ, n.zs,
+                                            n.enl_s, n.fnl);
+    CPSTEP_LAUNCH_CHECK();
+    if ((rc = n.ops.nl_force(c, j, n.zs, dyp, S, fpsi))) return rc;
+  }
+  ees::k_nl_finish<<<cdiv(std::max(1, 3 * natm), 128), 128, 0, c->stream>>>(
+      n.enl_s, n.fnl, S, natm, energies, fatm);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}

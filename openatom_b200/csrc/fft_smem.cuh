@@ -136,6 +136,53 @@ struct Dft<T, 8, INV> {
   }
 };
 
+// 16-point DFT as 4 x 4: X[k1 + 4 k2] = sum_n2 W16^(n2 k1) W4^(n2 k2) [DFT4 over n1
+// of x[4 n1 + n2]](k1).  W16 constants: cos(pi/8) = sqrt(2 + sqrt2)/2,
+// sin(pi/8) = sqrt(2 - sqrt2)/2.
+#define K_C8 0.92387953251128675613   /* cos(pi/8) */
+#define K_S8 0.38268343236508977173   /* sin(pi/8) */
+template <typename T, bool INV>
+struct Dft<T, 16, INV> {
+  // multiply by W16^e (forward e^{-2 pi i e/16}; INV: conjugate), e in 0..9
+  static __device__ __forceinline__ cplx<T> w16(cplx<T> a, int e) {
+    const T c = (T)K_C8, s = (T)K_S8, r = (T)K_R2;
+    cplx<T> w;
+    switch (e) {
+      case 1: w = mk<T>(c, -s); break;
+      case 2: w = mk<T>(r, -r); break;
+      case 3: w = mk<T>(s, -c); break;
+      case 4: return mul_i(a, INV);
+      case 6: w = mk<T>(-r, -r); break;
+      case 9: w = mk<T>(-c, s); break;
+      default: return a;
+    }
+    return INV ? cmulc(a, w) : cmul(a, w);
+  }
+  template <int N>
+  static __device__ __forceinline__ void run(cplx<T>* v, const cplx<T>* tw) {
+    // DFT4 over n1 in place: element k1 of column n2 lands in v[4 k1 + n2]
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+      cplx<T> a[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+      Dft<T, 4, INV>::template run<N>(a, tw);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; ++k1) v[4 * k1 + n2] = w16(a[k1], n2 * k1);
+    }
+    // DFT4 over n2 in place: X[k1 + 4 k2] lands in v[4 k1 + k2]
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) Dft<T, 4, INV>::template run<N>(v + 4 * k1, tw);
+    // transpose 4 x 4 (register renaming)
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = i + 1; j < 4; ++j) {
+        cplx<T> t = v[4 * i + j];
+        v[4 * i + j] = v[4 * j + i];
+        v[4 * j + i] = t;
+      }
+  }
+};
+
 // One Stockham stage (radix R, product of earlier radices NS) over `nlines`
 // lines of length N (line stride ldl) in smem.  EPT bounds the elements a
 // thread holds: nlines*N <= EPT*NT.
@@ -287,5 +334,78 @@ __device__ __forceinline__ void fft_lines(cplx<T>* buf, int ldl, int nlines, con
   for (int l0 = 0; l0 < nlines; l0 += CAP) {
     const int nl = min(CAP, nlines - l0);
     FftStages<T, N, 1, EPT, NT, INV>::run(buf + l0 * ldl, ldl, nl, tw);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Two-stage warp FFT for N = 16 * M2: a radix-16 stage, then a radix-M2 stage,
+// on up to L = 32 / M2 lines at a time per warp (lines base + i*ld).  The
+// stage-1 output goes to the line buffer padded by one element every 16
+// (index i -> i + i/16), so ld must be >= N + N/16; with ld = 8 (mod 16)
+// complex elements neither stage has shared-memory bank conflicts for the
+// FP32 and FP64 access widths.  Input and output are in natural order.
+template <int N>
+struct Fft16Shape {
+  // Not selected by the plane kernels for now: with the density accumulators
+  // the 512-thread plane kernels run out of their 128 registers and spill, and
+  // the one-line-at-a-time Stockham path measured as fast.
+  static constexpr bool ok = false && (N % 16 == 0) && (N / 16 >= 2) && (N / 16 <= 8);
+  static constexpr int M2 = ok ? N / 16 : 1;
+  static constexpr int L = ok ? 32 / M2 : 1;           // lines per warp pass
+  static constexpr int PER2 = ok ? (L * 16 + 31) / 32 : 1;  // stage-2 butterflies per lane
+  static constexpr int LD = ((N + N / 16 + 7) / 16) * 16 + 8;  // >= N + N/16, = 8 mod 16
+};
+
+template <typename T, int N, bool INV>
+__device__ __forceinline__ void fft16_lines(cplx<T>* base, int ld, int nl, const cplx<T>* tw,
+                                            int lane) {
+  using S = Fft16Shape<N>;
+  constexpr int M2 = S::M2;
+  // stage 1: radix 16, butterfly j < M2 of line li = lane / M2
+  {
+    const int li = lane / M2, j = lane - li * M2;
+    const bool act = (li < S::L) && (li < nl);
+    cplx<T> v[16];
+    cplx<T>* line = base + (size_t)li * ld;
+    if (act) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = line[j + M2 * r];
+      Dft<T, 16, INV>::template run<N>(v, tw);
+    }
+    __syncwarp();
+    if (act) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) line[j * 17 + r] = v[r];  // padded j*16 + r
+    }
+    __syncwarp();
+  }
+  // stage 2: radix M2, butterfly j < 16 (twiddle W_N^(r j)), natural-order output.
+  // Butterflies t = 0, 1, .. of a lane lie on different lines (b = lane + 32 t,
+  // line b / 16), so each t is read, transformed and written on its own.
+#pragma unroll 1
+  for (int t = 0; t < S::PER2; ++t) {
+    const int b = lane + 32 * t;
+    const int li = b >> 4, j = b & 15;
+    const bool act = (li < nl) && (li < S::L);
+    cplx<T>* line = base + (size_t)li * ld;
+    cplx<T> v[M2];
+    if (act) {
+#pragma unroll
+      for (int r = 0; r < M2; ++r) {
+        cplx<T> a = line[j + 17 * r];
+        if (r > 0) {
+          cplx<T> w = tw[r * j];
+          a = INV ? cmulc(a, w) : cmul(a, w);
+        }
+        v[r] = a;
+      }
+      Dft<T, M2, INV>::template run<N>(v, tw);
+    }
+    __syncwarp();
+    if (act) {
+#pragma unroll
+      for (int r = 0; r < M2; ++r) line[j + 16 * r] = v[r];
+    }
+    __syncwarp();
   }
 }

@@ -26,6 +26,16 @@ const int kFftSizes[] = {
     308, 320, 330, 336, 352, 360, 384, 396, 420, 440, 448, 462, 480, 504, 512, 528, 560, 576,
     616, 630, 640, 660, 672, 704, 720, 768, 770, 792, 840, 880, 896, 924, 960, 990, 1008, 1024};
 
+// init_nonlocal_ees (set_cp_ewald.C:1329-1400), one axis
+int nl_grid_size_of(int kmax, double scale, int n_interp) {
+  const int nk = kmax + 1;
+  int nkf = (int)(2.0 * scale * (double)nk);
+  if (nkf < 2 * nk) ++nkf;
+  for (int k : kFftSizes)
+    if (k >= nkf) return k >= n_interp ? k : -1;
+  return -1;
+}
+
 int kmax_of(double L, double ecut_ry) {
   double ecut_ha = 0.5 * ecut_ry;
   double temp = std::sqrt(ecut_ha * 0.5) / (M_PI * (1.0 / L));
@@ -228,6 +238,10 @@ bool make_runs(const std::vector<K3>& k, int nx, int ny, int nz, std::vector<int
 }
 
 }  // namespace
+
+int nl_grid_size(int kmax, double scale, int n_interp) {
+  return nl_grid_size_of(kmax, scale, n_interp);
+}
 
 extern "C" int cpstep_layout_sizes(double box_len, double ecut_ry, int* kmax, int* nfft,
                                    int* nktot_half, int* npts) {

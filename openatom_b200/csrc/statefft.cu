@@ -57,6 +57,8 @@ static bool lookup_ops(int precision, int n, StateFftOps* o) {
 #undef CPSTEP_CASE
 }
 
+int statefft_lookup(int precision, int n, StateFftOps* o) { return lookup_ops(precision, n, o) ? 1 : 0; }
+
 int statefft_supported(int n) {
   StateFftOps o;
   return lookup_ops(CPSTEP_PREC_FP64, n, &o) ? 1 : 0;

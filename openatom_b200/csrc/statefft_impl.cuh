@@ -47,21 +47,59 @@ __device__ __forceinline__ void locate(int p, const int* soff, int nl, const int
 }
 
 template <int N>
+struct PlaneLd;
+
+template <int N>
 struct ZShape {
   static constexpr int LB = std::min(64, std::max(8, 4096 / N));  // lines per block
-  static constexpr int LD = N + 1;
+  static constexpr int LD = PlaneLd<N>::value;
   template <typename T>
   static constexpr size_t bytes() {
     return sizeof(cplx<T>) * (size_t)(N + LB * LD) + sizeof(int) * (4 * LB + 1);
   }
 };
 
+// Line stride of the plane columns and row buffers: room for the padded
+// stage-1 output of the two-stage warp FFT where N = 16 * M2, else N + 1.
+template <int N>
+struct PlaneLd {
+  static constexpr int value = Fft16Shape<N>::ok ? Fft16Shape<N>::LD : N + 1;
+  static constexpr int lines = Fft16Shape<N>::ok ? Fft16Shape<N>::L : 1;  // per warp pass
+};
+
+// nl lines of length N at base (stride ld) by the calling warp, up to
+// PlaneLd<N>::lines at a time.
+// (FP64 keeps the one-line-at-a-time Stockham FFT: the two-stage form needs
+// more than the 128 registers a thread of the 512-thread plane kernels has.)
+template <typename T, int N, bool INV>
+__device__ __forceinline__ void warp_lines(cplx<T>* base, int ld, int nl, const cplx<T>* tw) {
+  if constexpr (Fft16Shape<N>::ok && sizeof(T) == 4) {
+    constexpr int L = Fft16Shape<N>::L;
+    const int lane = threadIdx.x & 31;
+    for (int l0 = 0; l0 < nl; l0 += L)
+      fft16_lines<T, N, INV>(base + (size_t)l0 * ld, ld, min(L, nl - l0), tw, lane);
+  } else {
+    for (int l = 0; l < nl; ++l) fft_line_warp<T, N, INV>(base + (size_t)l * ld, tw);
+  }
+}
+
+// nl lines (stride ld) shared out to all warps of the block in groups.
+template <typename T, int N, bool INV>
+__device__ __forceinline__ void block_lines(cplx<T>* buf, int ld, int nl, const cplx<T>* tw) {
+  constexpr int L = PlaneLd<N>::lines;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int l0 = warp * L; l0 < nl; l0 += nw * L)
+    warp_lines<T, N, INV>(buf + (size_t)l0 * ld, ld, min(L, nl - l0), tw);
+}
+
 // ---------------------------------------------------------------------------
 // K1: expand packed psi into z-lines, forward z-FFT, write [s][z][line] pencils
+// With mul (EES projector dyp), the line holds conj(mul * psi) instead of psi
+// (eesProjGchare, cp_ees_nonlocal.C:705-709).
 template <typename T, int N>
 __global__ void __launch_bounds__(ZTHREADS)
 k_zfft_fwd(const double2* __restrict__ psi, cplx<T>* __restrict__ pen, StateGeom g,
-           const cplx<T>* __restrict__ twz) {
+           const cplx<T>* __restrict__ twz, const double2* __restrict__ mul) {
   constexpr int LB = ZShape<N>::LB, LD = ZShape<N>::LD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
@@ -89,10 +127,14 @@ k_zfft_fwd(const double2* __restrict__ psi, cplx<T>* __restrict__ pen, StateGeom
     int li, z;
     locate(p, soff, nl, snneg, szneg, szpos, li, z);
     double2 v = ps[p];
+    if (mul) {
+      double2 d = mul[p];
+      v = make_double2(d.x * v.x - d.y * v.y, -(d.y * v.x + d.x * v.y));
+    }
     buf[li * LD + z] = mk<T>((T)v.x, (T)v.y);
   }
   __syncthreads();
-  fft_lines_warp<T, N, false>(buf, LD, nl, tw);  // FFTW_FORWARD along z
+  block_lines<T, N, false>(buf, LD, nl, tw);  // FFTW_FORWARD along z
   __syncthreads();
   cplx<T>* po = pen + (size_t)s * N * g.nlpad + l0;
   for (int i = threadIdx.x; i < nl * N; i += ZTHREADS) {
@@ -102,15 +144,21 @@ k_zfft_fwd(const double2* __restrict__ psi, cplx<T>* __restrict__ pen, StateGeom
 }
 
 // ---------------------------------------------------------------------------
-// shared plane helpers.  plane is [nplane_x][N+1] (column kx holds y contiguous)
+// shared plane helpers.  plane is [nplane_x][LDY] (column kx holds y contiguous)
+
+// The nplx plane columns, shared out to the block's warps in groups.
+template <typename T, int N, bool INV>
+__device__ __forceinline__ void plane_columns(cplx<T>* plane, int nplx, const cplx<T>* tw) {
+  block_lines<T, N, INV>(plane, PlaneLd<N>::value, nplx, tw);
+}
 
 template <typename T, int N>
 __device__ __forceinline__ void scatter_plane(const cplx<T>* __restrict__ prow, cplx<T>* plane,
                                               const StateGeom& g) {
-  constexpr int LDY = N + 1;
-  for (int i = threadIdx.x; i < g.nplane_x * LDY; i += PTHREADS) plane[i] = mk<T>(0, 0);
+  constexpr int LDY = PlaneLd<N>::value;
+  for (int i = threadIdx.x; i < g.nplane_x * LDY; i += blockDim.x) plane[i] = mk<T>(0, 0);
   __syncthreads();
-  for (int l = threadIdx.x; l < g.nlines; l += PTHREADS) {
+  for (int l = threadIdx.x; l < g.nlines; l += blockDim.x) {
     int xy = __ldg(g.line_xy + l);
     plane[(xy & 0xffff) * LDY + (xy >> 16)] = prow[l];
   }
@@ -123,7 +171,7 @@ __device__ __forceinline__ void scatter_plane(const cplx<T>* __restrict__ prow, 
 template <typename T, int N>
 __device__ __forceinline__ void build_c2r_row(const cplx<T>* plane, cplx<T>* row, int nplx,
                                               int ya) {
-  constexpr int LDY = N + 1;
+  constexpr int LDY = PlaneLd<N>::value;
   for (int k = threadIdx.x & 31; k < N; k += 32) {
     cplx<T> z;
     if (k == 0) {
@@ -149,7 +197,7 @@ __device__ __forceinline__ void build_c2r_row(const cplx<T>* plane, cplx<T>* row
 template <typename T, int N>
 __device__ __forceinline__ void extract_r2c_row(const cplx<T>* row, cplx<T>* plane, int nplx,
                                                 int ya) {
-  constexpr int LDY = N + 1;
+  constexpr int LDY = PlaneLd<N>::value;
   for (int k = threadIdx.x & 31; k < nplx; k += 32) {
     cplx<T> zk = row[k];
     cplx<T> zm = row[k == 0 ? 0 : N - k];
@@ -162,13 +210,15 @@ __device__ __forceinline__ void extract_r2c_row(const cplx<T>* row, cplx<T>* pla
 
 template <typename T, int N>
 struct PShape {
-  static constexpr int LDY = N + 1, LDX = N + 1;
+  static constexpr int LDY = PlaneLd<N>::value, LDX = PlaneLd<N>::value;
   static constexpr int E = (N + 31) / 32;               // row elements per lane
   static constexpr int QMAX = std::max(1, 32 / (2 * E));  // row pairs a warp accumulates
   static constexpr int ROWS = std::min(N, 2 * QMAX * PWARPS) & ~1;  // rows per y-split
+  static constexpr int RPW = PlaneLd<N>::lines;         // row buffers per warp
   static constexpr size_t LIMIT = 227 * 1024;
   static constexpr size_t bytes(int nplx) {
-    return sizeof(cplx<T>) * ((size_t)N + (size_t)nplx * LDY + (size_t)PWARPS * LDX);
+    return sizeof(cplx<T>) *
+           ((size_t)N + (size_t)nplx * LDY + (size_t)PWARPS * RPW * LDX);
   }
 };
 
@@ -176,19 +226,20 @@ struct PShape {
 // K2: planes -> psi(r).  MODE 0 accumulates occ*psi^2 into per-group FP64
 // partial densities held in registers (each warp owns row pairs
 // warp, warp+16, ... of the block's y range); MODE 1 writes psi(r) (FP64).
+// A warp builds and transforms up to RPW row pairs together.
 template <typename T, int N, int MODE>
 __global__ void __launch_bounds__(PTHREADS, 1)
 k_xy_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict__ twx_g,
          const double* __restrict__ occ, int nstates, int spg, int ysplit_rows,
          double* __restrict__ out) {
-  constexpr int LDY = N + 1, LDX = N + 1;
-  constexpr int E = PShape<T, N>::E, QMAX = PShape<T, N>::QMAX;
+  constexpr int LDY = PShape<T, N>::LDY, LDX = PShape<T, N>::LDX;
+  constexpr int E = PShape<T, N>::E, QMAX = PShape<T, N>::QMAX, RPW = PShape<T, N>::RPW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* plane = tw + N;
   cplx<T>* rows = plane + g.nplane_x * LDY;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  cplx<T>* row = rows + warp * LDX;
+  cplx<T>* wrows = rows + (size_t)warp * RPW * LDX;
   const int z = blockIdx.x;
   const int grp = blockIdx.y;
   const int y0 = blockIdx.z * ysplit_rows;
@@ -206,29 +257,52 @@ k_xy_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict
   __syncthreads();
   for (int s = s0; s < s1; ++s) {
     scatter_plane<T, N>(pen + ((size_t)s * N + z) * g.nlpad, plane, g);
-    fft_lines_warp<T, N, false>(plane, LDY, g.nplane_x, tw);  // FFTW_FORWARD y
+    plane_columns<T, N, false>(plane, g.nplane_x, tw);  // FFTW_FORWARD y
     __syncthreads();
     const double w = (MODE == 0) ? occ[s] : 1.0;
+    if (MODE == 0) {
 #pragma unroll
-    for (int q = 0; q < (MODE == 0 ? QMAX : 1); ++q) {
-      for (int pp = warp + PWARPS * q; pp < npair; pp += (MODE == 0 ? npair : PWARPS)) {
-        const int ya = y0 + 2 * pp;
-        build_c2r_row<T, N>(plane, row, g.nplane_x, ya);
-        fft_line_warp<T, N, true>(row, tw);  // C2R, +i sign
-        if (MODE == 0) {
+      for (int q0 = 0; q0 < QMAX; q0 += RPW) {
+        int nb = 0;
 #pragma unroll
-          for (int e = 0; e < E; ++e) {
-            int x = lane + 32 * e;
-            if (x < N) {
-              cplx<T> v = row[x];
-              acc[q][0][e] += w * (double)v.x * (double)v.x;
-              acc[q][1][e] += w * (double)v.y * (double)v.y;
+        for (int i = 0; i < RPW; ++i) {
+          const int pp = warp + PWARPS * (q0 + i);
+          if (q0 + i < QMAX && pp < npair) {
+            build_c2r_row<T, N>(plane, wrows + i * LDX, g.nplane_x, y0 + 2 * pp);
+            nb = i + 1;
+          }
+        }
+        warp_lines<T, N, true>(wrows, LDX, nb, tw);  // C2R, +i sign
+#pragma unroll
+        for (int i = 0; i < RPW; ++i) {
+          const int q = q0 + i;
+          if (q < QMAX && i < nb) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+              int x = lane + 32 * e;
+              if (x < N) {
+                cplx<T> v = wrows[i * LDX + x];
+                acc[q][0][e] += w * (double)v.x * (double)v.x;
+                acc[q][1][e] += w * (double)v.y * (double)v.y;
+              }
             }
           }
-        } else {
+        }
+        __syncwarp();
+      }
+    } else {
+      for (int p0 = warp * RPW; p0 < npair; p0 += PWARPS * RPW) {
+        const int nb = min(RPW, npair - p0);
+#pragma unroll 1
+        for (int i = 0; i < nb; ++i)
+          build_c2r_row<T, N>(plane, wrows + i * LDX, g.nplane_x, y0 + 2 * (p0 + i));
+        warp_lines<T, N, true>(wrows, LDX, nb, tw);  // C2R, +i sign
+#pragma unroll 1
+        for (int i = 0; i < nb; ++i) {
+          const int ya = y0 + 2 * (p0 + i);
           double* o = out + (((size_t)s * N + z) * N + ya) * N;
           for (int x = lane; x < N; x += 32) {
-            cplx<T> v = row[x];
+            cplx<T> v = wrows[i * LDX + x];
             o[x] = (double)v.x;
             o[N + x] = (double)v.y;
           }
@@ -261,21 +335,21 @@ k_xy_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict
 // ---------------------------------------------------------------------------
 // K3: MODE 0: pencils -> psi(r) -> psi*V*occ -> planes -> pencils_out
 //     MODE 1: real f(r) (FP64, [s][z][y][x]) -> planes -> pencils_out
-// Each warp takes row pairs warp, warp+16, ... through C2R, the product and
-// R2C in its own row buffer.
+// Each warp takes up to RPW row pairs at a time (pairs warp*RPW + i, then
+// + PWARPS*RPW) through C2R, the product and R2C in its own row buffers.
 template <typename T, int N, int MODE>
 __global__ void __launch_bounds__(PTHREADS, 1)
 k_xy_bwd(const cplx<T>* __restrict__ pen, const double* __restrict__ freal,
          const T* __restrict__ vks, cplx<T>* __restrict__ pen_out, StateGeom g,
          const cplx<T>* __restrict__ twx_g, const double* __restrict__ occ, int nstates,
          int spg) {
-  constexpr int LDY = N + 1, LDX = N + 1;
+  constexpr int LDY = PShape<T, N>::LDY, LDX = PShape<T, N>::LDX, RPW = PShape<T, N>::RPW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* plane = tw + N;
   cplx<T>* rows = plane + g.nplane_x * LDY;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  cplx<T>* row = rows + warp * LDX;
+  cplx<T>* wrows = rows + (size_t)warp * RPW * LDX;
   const int z = blockIdx.x;
   const int s0 = blockIdx.y * spg, s1 = min(nstates, s0 + spg);
   for (int i = threadIdx.x; i < N; i += PTHREADS) tw[i] = twx_g[i];
@@ -284,32 +358,46 @@ k_xy_bwd(const cplx<T>* __restrict__ pen, const double* __restrict__ freal,
   for (int s = s0; s < s1; ++s) {
     if (MODE == 0) {
       scatter_plane<T, N>(pen + ((size_t)s * N + z) * g.nlpad, plane, g);
-      fft_lines_warp<T, N, false>(plane, LDY, g.nplane_x, tw);
+      plane_columns<T, N, false>(plane, g.nplane_x, tw);
       __syncthreads();
     }
     const T w = (MODE == 0) ? (T)occ[s] : (T)1;
-    for (int pp = warp; pp < N / 2; pp += PWARPS) {
-      const int ya = 2 * pp;
+    for (int p0 = warp * RPW; p0 < N / 2; p0 += PWARPS * RPW) {
+      const int nb = min(RPW, N / 2 - p0);
       if (MODE == 0) {
-        build_c2r_row<T, N>(plane, row, g.nplane_x, ya);
-        fft_line_warp<T, N, true>(row, tw);
-        for (int x = lane; x < N; x += 32) {
-          cplx<T> v = row[x];
-          v.x *= __ldg(vplane + ya * N + x) * w;
-          v.y *= __ldg(vplane + (ya + 1) * N + x) * w;
-          row[x] = v;
+#pragma unroll 1
+        for (int i = 0; i < nb; ++i)
+          build_c2r_row<T, N>(plane, wrows + i * LDX, g.nplane_x, 2 * (p0 + i));
+        warp_lines<T, N, true>(wrows, LDX, nb, tw);
+#pragma unroll 1
+        for (int i = 0; i < nb; ++i) {
+          const int ya = 2 * (p0 + i);
+          cplx<T>* row = wrows + i * LDX;
+          for (int x = lane; x < N; x += 32) {
+            cplx<T> v = row[x];
+            v.x *= __ldg(vplane + ya * N + x) * w;
+            v.y *= __ldg(vplane + (ya + 1) * N + x) * w;
+            row[x] = v;
+          }
         }
       } else {
         const double* fs = freal + ((size_t)s * N + z) * N * N;
-        for (int x = lane; x < N; x += 32)
-          row[x] = mk<T>((T)fs[ya * N + x], (T)fs[(ya + 1) * N + x]);
+#pragma unroll 1
+        for (int i = 0; i < nb; ++i) {
+          const int ya = 2 * (p0 + i);
+          cplx<T>* row = wrows + i * LDX;
+          for (int x = lane; x < N; x += 32)
+            row[x] = mk<T>((T)fs[ya * N + x], (T)fs[(ya + 1) * N + x]);
+        }
       }
       __syncwarp();
-      fft_line_warp<T, N, false>(row, tw);  // R2C, -i sign
-      extract_r2c_row<T, N>(row, plane, g.nplane_x, ya);
+      warp_lines<T, N, false>(wrows, LDX, nb, tw);  // R2C, -i sign
+#pragma unroll 1
+      for (int i = 0; i < nb; ++i)
+        extract_r2c_row<T, N>(wrows + i * LDX, plane, g.nplane_x, 2 * (p0 + i));
     }
     __syncthreads();
-    fft_lines_warp<T, N, true>(plane, LDY, g.nplane_x, tw);  // FFTW_BACKWARD along y
+    plane_columns<T, N, true>(plane, g.nplane_x, tw);  // FFTW_BACKWARD along y
     __syncthreads();
     cplx<T>* po = pen_out + ((size_t)s * N + z) * g.nlpad;
     for (int l = threadIdx.x; l < g.nlines; l += PTHREADS) {
@@ -324,12 +412,15 @@ k_xy_bwd(const cplx<T>* __restrict__ pen, const double* __restrict__ freal,
 // K4: pencils -> backward z-FFT -> pack -> scale.
 //   MODE 0: F = scale * wpt * val (then, if occ != null, the kinetic term)
 //   MODE 1: plain pack with scale (adjoint transform)
+//   MODE 2: EES psi force, F += -wpt conj(mul * val) with the imaginary parts
+//           of val and mul dropped at G = 0 (eesPsiForcGspace,
+//           cp_ees_nonlocal.C:2000-2064)
 template <typename T, int N, int MODE>
 __global__ void __launch_bounds__(ZTHREADS)
 k_zfft_bwd(const cplx<T>* __restrict__ pen, double2* __restrict__ fout,
            const double2* __restrict__ psi, const double* __restrict__ occ, StateGeom g,
            const cplx<T>* __restrict__ twz, double scale, double ecut,
-           double* __restrict__ eke_part) {
+           double* __restrict__ eke_part, const double2* __restrict__ mul) {
   constexpr int LB = ZShape<N>::LB, LD = ZShape<N>::LD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
@@ -356,7 +447,7 @@ k_zfft_bwd(const cplx<T>* __restrict__ pen, double2* __restrict__ fout,
     buf[li * LD + z] = pi[(size_t)z * g.nlpad + li];
   }
   __syncthreads();
-  fft_lines_warp<T, N, true>(buf, LD, nl, tw);  // FFTW_BACKWARD along z
+  block_lines<T, N, true>(buf, LD, nl, tw);  // FFTW_BACKWARD along z
   __syncthreads();
   const int p0 = soff[0], p1 = soff[nl];
   double e = 0.0;
@@ -365,6 +456,20 @@ k_zfft_bwd(const cplx<T>* __restrict__ pen, double2* __restrict__ fout,
     int li, z;
     locate(p, soff, nl, snneg, szneg, szpos, li, z);
     cplx<T> v = buf[li * LD + z];
+    if (MODE == 2) {
+      double vx = (double)v.x, vy = (double)v.y;
+      double2 d = mul[p];
+      if (g.g2[p] == 0.0) {
+        vy = 0.0;
+        d.y = 0.0;
+      }
+      const double wp = g.wpt[p];
+      double2 f = fout[(size_t)s * g.npts + p];
+      f.x -= wp * (d.x * vx - d.y * vy);
+      f.y += wp * (d.y * vx + d.x * vy);
+      fout[(size_t)s * g.npts + p] = f;
+      continue;
+    }
     double fx = (double)v.x * scale, fy = (double)v.y * scale;
     if (MODE == 0) {
       double wp = g.wpt[p];
@@ -389,6 +494,196 @@ k_zfft_bwd(const cplx<T>* __restrict__ pen, double2* __restrict__ fout,
   if (MODE == 0 && occ) {
     double t = block_sum(e, red);
     if (threadIdx.x == 0) eke_part[(size_t)s * gridDim.x + blockIdx.x] = 0.5 * t;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// EES non-local plane kernels (N is the NL grid).  The real plane [N][N] lives
+// in shared memory and doubles as the row-pair buffers of the x transforms: a
+// complex row of N elements occupies exactly the two real rows it produces.
+
+// Per-plane shared memory of the NL kernels: twiddles, the complex plane, the
+// real plane.
+template <typename T, int N>
+struct NlShape {
+  static constexpr int LDY = PlaneLd<N>::value;
+  static size_t bytes(int nplx) {
+    return sizeof(cplx<T>) * ((size_t)N + (size_t)nplx * LDY) + sizeof(T) * (size_t)N * N;
+  }
+};
+
+// The B-spline product of one stencil point, in the reference's order
+// (eesAtmBsplineRgrp IV, cp_ees_nonlocal.C:523-532): mn and dmn_{x,y,z}.
+__device__ __forceinline__ void nl_point(const NlAtoms& A, int a, int ja, int jb, int jc,
+                                         double& mn, double& dx, double& dy, double& dz) {
+  const double* m = A.mn + (size_t)a * 3 * kNlInterp;
+  const double* d = A.dmn + (size_t)a * 3 * kNlInterp;
+  const double ma = m[ja], mb = m[kNlInterp + jb], mc = m[2 * kNlInterp + jc];
+  const double at = d[ja] * mb * mc * A.grid;
+  const double bt = ma * d[kNlInterp + jb] * mc * A.grid;
+  const double ct = ma * mb * d[2 * kNlInterp + jc] * A.grid;
+  mn = ma * mb * mc;
+  const double* h = A.hmati;
+  dx = at * h[0] + bt * h[1] + ct * h[2];
+  dy = at * h[3] + bt * h[4] + ct * h[5];
+  dz = at * h[6] + bt * h[7] + ct * h[8];
+}
+
+// NL G->R (doNlFFTGtoR_Gchare/Rchare, fftCache.C:589-809) of plane z for the
+// block's states s0..s1, then for every atom of type ctype with an
+// interpolation plane jc on z: zpart[s][atom][jc] = (sum P mn, sum P dmn_x,
+// sum P dmn_y, sum P dmn_z) over its 8x8 points (eesZmatRchare :1238-1346 and
+// the force sums of eesEnergyAtmForcRchare :1480-1700, before the Z factor).
+constexpr int NLTHREADS = 256;  // NL plane kernels: 8 warps, two blocks per SM
+template <typename T, int N>
+__global__ void __launch_bounds__(NLTHREADS, 2)
+k_nl_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict__ twx_g,
+         NlAtoms A, int ctype, int nstates, int spg, double* __restrict__ zpart) {
+  constexpr int LDY = PlaneLd<N>::value;
+  constexpr int E = (N + 31) / 32;
+  constexpr int NW = NLTHREADS / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* plane = tw + N;
+  T* R = reinterpret_cast<T*>(plane + g.nplane_x * LDY);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int z = blockIdx.x;
+  const int s0 = blockIdx.y * spg, s1 = min(nstates, s0 + spg);
+  for (int i = threadIdx.x; i < N; i += NLTHREADS) tw[i] = twx_g[i];
+  const int* pl = A.plist + ((size_t)ctype * (int)A.grid + z) * A.natm;
+  const int npl = A.pcount[ctype * (int)A.grid + z];
+  const int ja = lane & 7, jb0 = lane >> 3;
+  __syncthreads();
+  for (int s = s0; s < s1; ++s) {
+    scatter_plane<T, N>(pen + ((size_t)s * N + z) * g.nlpad, plane, g);
+    plane_columns<T, N, false>(plane, g.nplane_x, tw);  // FFTW_FORWARD y
+    __syncthreads();
+    for (int pp = warp; pp < N / 2; pp += NW) {
+      const int ya = 2 * pp;
+      cplx<T>* row = reinterpret_cast<cplx<T>*>(R + (size_t)ya * N);
+      build_c2r_row<T, N>(plane, row, g.nplane_x, ya);
+      fft_line_warp<T, N, true>(row, tw);  // C2R, +i sign
+      cplx<T> v[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int x = lane + 32 * e;
+        if (x < N) v[e] = row[x];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int x = lane + 32 * e;
+        if (x < N) {
+          R[(size_t)ya * N + x] = v[e].x;
+          R[(size_t)(ya + 1) * N + x] = v[e].y;
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    // atoms on this plane: lane -> (jb, ja) = (lane / 8 + 4 h, lane % 8), h = 0, 1
+    for (int e = warp; e < npl; e += NW) {
+      const int a = pl[e] & 0xffff, jc = pl[e] >> 16;
+      const int* ig = A.ig + (size_t)a * 3 * kNlInterp;
+      double sz = 0.0, sx = 0.0, sy = 0.0, sw = 0.0;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int jb = jb0 + 4 * h;
+        const double pz = (double)R[(size_t)ig[kNlInterp + jb] * N + ig[ja]];
+        double mn, dx, dy, dz;
+        nl_point(A, a, ja, jb, jc, mn, dx, dy, dz);
+        sz += pz * mn;
+        sx += pz * dx;
+        sy += pz * dy;
+        sw += pz * dz;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sz += __shfl_xor_sync(0xffffffffu, sz, o);
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        sw += __shfl_xor_sync(0xffffffffu, sw, o);
+      }
+      if (lane == 0) {
+        double* o = zpart + (((size_t)s * A.natm + a) * kNlInterp + jc) * 4;
+        o[0] = sz; o[1] = sx; o[2] = sy; o[3] = sw;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// NL R->G of plane z for the block's states: the plane holds sum_atoms
+// zs[s][atom] Mn over the atoms of type ctype (the projPsiRScr scatter of
+// eesEnergyAtmForcRchare, applied by one warp atom after atom so the sum order
+// is fixed), then x R2C, imag flip, y-FFT (doNlFFTRtoG_Rchare,
+// fftCache.C:634-699) into pencils.
+template <typename T, int N>
+__global__ void __launch_bounds__(NLTHREADS, 2)
+k_nl_bwd(cplx<T>* __restrict__ pen_out, StateGeom g, const cplx<T>* __restrict__ twx_g,
+         NlAtoms A, int ctype, int nstates, int spg, const double* __restrict__ zs) {
+  constexpr int LDY = PlaneLd<N>::value;
+  constexpr int E = (N + 31) / 32;
+  constexpr int NW = NLTHREADS / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* plane = tw + N;
+  T* R = reinterpret_cast<T*>(plane + g.nplane_x * LDY);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int z = blockIdx.x;
+  const int s0 = blockIdx.y * spg, s1 = min(nstates, s0 + spg);
+  for (int i = threadIdx.x; i < N; i += NLTHREADS) tw[i] = twx_g[i];
+  const int* pl = A.plist + ((size_t)ctype * (int)A.grid + z) * A.natm;
+  const int npl = A.pcount[ctype * (int)A.grid + z];
+  for (int s = s0; s < s1; ++s) {
+    for (int i = threadIdx.x; i < N * N; i += NLTHREADS) R[i] = (T)0;
+    __syncthreads();
+    if (warp == 0) {
+      const int ja = lane & 7, jb0 = lane >> 3;
+      for (int e = 0; e < npl; ++e) {
+        const int a = pl[e] & 0xffff, jc = pl[e] >> 16;
+        const int* ig = A.ig + (size_t)a * 3 * kNlInterp;
+        const double za = zs[(size_t)s * A.natm + a];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int jb = jb0 + 4 * h;
+          double mn, dx, dy, dz;
+          nl_point(A, a, ja, jb, jc, mn, dx, dy, dz);
+          T* r = R + (size_t)ig[kNlInterp + jb] * N + ig[ja];
+          *r = (T)((double)*r + za * mn);
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int pp = warp; pp < N / 2; pp += NW) {
+      const int ya = 2 * pp;
+      cplx<T>* row = reinterpret_cast<cplx<T>*>(R + (size_t)ya * N);
+      cplx<T> v[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int x = lane + 32 * e;
+        if (x < N) v[e] = mk<T>(R[(size_t)ya * N + x], R[(size_t)(ya + 1) * N + x]);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int x = lane + 32 * e;
+        if (x < N) row[x] = v[e];
+      }
+      __syncwarp();
+      fft_line_warp<T, N, false>(row, tw);  // R2C, -i sign
+      extract_r2c_row<T, N>(row, plane, g.nplane_x, ya);
+    }
+    __syncthreads();
+    plane_columns<T, N, true>(plane, g.nplane_x, tw);  // FFTW_BACKWARD along y
+    __syncthreads();
+    cplx<T>* po = pen_out + ((size_t)s * N + z) * g.nlpad;
+    for (int l = threadIdx.x; l < g.nlines; l += NLTHREADS) {
+      int xy = __ldg(g.line_xy + l);
+      po[l] = plane[(xy & 0xffff) * LDY + (xy >> 16)];
+    }
+    __syncthreads();
   }
 }
 
@@ -426,13 +721,14 @@ inline int plane_groups(const cpstep_ctx* c, int nstates, int other) {
 
 template <typename T, int N>
 struct StateFft {
-  static int zfft_fwd(cpstep_ctx* c, const FftJob& j, const double* psi, int nstates) {
+  static int zfft_fwd(cpstep_ctx* c, const FftJob& j, const double* psi, int nstates,
+                      const cplx<T>* twz = nullptr, const double2* mul = nullptr) {
     dim3 grid(cdiv(j.g.nlines, ZShape<N>::LB), nstates);
     const size_t smem = ZShape<N>::template bytes<T>();
     if (int rc = set_smem(k_zfft_fwd<T, N>, smem)) return rc;
     k_zfft_fwd<T, N><<<grid, ZTHREADS, smem, c->stream>>>(
         reinterpret_cast<const double2*>(psi), reinterpret_cast<cplx<T>*>(j.pen_a), j.g,
-        tws<T>(c).z);
+        twz ? twz : tws<T>(c).z, mul);
     CPSTEP_LAUNCH_CHECK();
     return CPSTEP_OK;
   }
@@ -478,12 +774,12 @@ struct StateFft {
       k_zfft_bwd<T, N, 0><<<grid, ZTHREADS, smem, c->stream>>>(
           reinterpret_cast<const cplx<T>*>(j.pen_b), reinterpret_cast<double2*>(out),
           reinterpret_cast<const double2*>(psi), occ, j.g, tws<T>(c).z, scale, c->ecut_ry,
-          c->d_eke_part);
+          c->d_eke_part, nullptr);
     } else {
       if (int rc = set_smem(k_zfft_bwd<T, N, 1>, smem)) return rc;
       k_zfft_bwd<T, N, 1><<<grid, ZTHREADS, smem, c->stream>>>(
           reinterpret_cast<const cplx<T>*>(j.pen_b), reinterpret_cast<double2*>(out), nullptr,
-          nullptr, j.g, tws<T>(c).z, scale, 0.0, nullptr);
+          nullptr, j.g, tws<T>(c).z, scale, 0.0, nullptr, nullptr);
     }
     CPSTEP_LAUNCH_CHECK();
     return CPSTEP_OK;
@@ -542,8 +838,57 @@ struct StateFft {
     return r2g(c, c->state_job(), f_r, fg, nstates, 1.0);
   }
 
+  // NL plane kernels: states per block so that N x groups is about six blocks
+  // per SM
+  static void nl_groups(const cpstep_ctx* c, int nstates, int& spg, int& ng) {
+    ng = std::max(1, std::min(nstates, cdiv(6 * c->num_sms, N)));
+    spg = cdiv(nstates, ng);
+    ng = cdiv(nstates, spg);
+  }
+
+  // EES: K1 with the projector, then the NL plane pass with the atom sums
+  static int nl_proj(cpstep_ctx* c, const NlJob& j, const double* psi, const double2* dyp,
+                     int nstates, double* zpart) {
+    const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(j.tw);
+    if (int rc = zfft_fwd(c, j.f, psi, nstates, tw, dyp)) return rc;
+    const size_t smem = NlShape<T, N>::bytes(j.f.g.nplane_x);
+    int spg, ng;
+    nl_groups(c, nstates, spg, ng);
+    if (int rc = set_smem(k_nl_fwd<T, N>, smem)) return rc;
+    k_nl_fwd<T, N><<<dim3(N, ng), NLTHREADS, smem, c->stream>>>(
+        reinterpret_cast<const cplx<T>*>(j.f.pen_a), j.f.g, tw, j.A, j.ctype, nstates, spg, zpart);
+    CPSTEP_LAUNCH_CHECK();
+    return CPSTEP_OK;
+  }
+
+  // EES: scatter of the scaled Z, NL plane pass back, K4 into the psi force
+  static int nl_force(cpstep_ctx* c, const NlJob& j, const double* zs, const double2* dyp,
+                      int nstates, double* fpsi) {
+    const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(j.tw);
+    const size_t smem = NlShape<T, N>::bytes(j.f.g.nplane_x);
+    int spg, ng;
+    nl_groups(c, nstates, spg, ng);
+    if (int rc = set_smem(k_nl_bwd<T, N>, smem)) return rc;
+    k_nl_bwd<T, N><<<dim3(N, ng), NLTHREADS, smem, c->stream>>>(
+        reinterpret_cast<cplx<T>*>(j.f.pen_b), j.f.g, tw, j.A, j.ctype, nstates, spg, zs);
+    CPSTEP_LAUNCH_CHECK();
+    dim3 grid(cdiv(j.f.g.nlines, ZShape<N>::LB), nstates);
+    const size_t zsm = ZShape<N>::template bytes<T>();
+    if (int rc = set_smem(k_zfft_bwd<T, N, 2>, zsm)) return rc;
+    k_zfft_bwd<T, N, 2><<<grid, ZTHREADS, zsm, c->stream>>>(
+        reinterpret_cast<const cplx<T>*>(j.f.pen_b), reinterpret_cast<double2*>(fpsi), nullptr,
+        nullptr, j.f.g, tw, 1.0, 0.0, nullptr, dyp);
+    CPSTEP_LAUNCH_CHECK();
+    return CPSTEP_OK;
+  }
+
+  static size_t nl_smem(int nplx) { return NlShape<T, N>::bytes(nplx); }
+
   static StateFftOps ops() {
     StateFftOps o;
+    o.nl_proj = &nl_proj;
+    o.nl_force = &nl_force;
+    o.nl_smem = &nl_smem;
     o.density = &density;
     o.vpsi = &vpsi;
     o.gtor = &gtor;

@@ -255,20 +255,27 @@ int step_run(cpstep_ctx* c, double* psi, double* vpsi, const double* occ, double
   mark(2);
   // 2. V.psi force with the kinetic term (z-pencils of psi are still valid)
   if ((rc = statefft_vpsi(c, psi, c->d_vks, occ, c->d_force, c->d_eke, 1))) return rc;
+  mark(3);
+  // 2b. EES non-local energy, psi force and atom forces
+  if (c->nl.on) {
+    if ((rc = nl_run(c, psi, occ, c->d_force, energies, atom_force))) return rc;
+  } else {
+    CPSTEP_CUDA_TRY(cudaMemsetAsync(energies + CPSTEP_E_NL, 0, sizeof(double), c->stream));
+  }
   stp::k_energy_tot<<<1, 32, 0, c->stream>>>(c->d_eke, S, energies);
   CPSTEP_LAUNCH_CHECK();
-  mark(3);
+  mark(4);
   // 3. lambda_ji = sum_p Re(conj psi_j F_i); F <- F - (wpt/2) psi.lambda
   const int K = 2 * c->npts;
   if ((rc = pc_overlap_launch(c, psi, c->d_force, S, S, K, nullptr, 1.0, 0.0, c->d_lambda, S))) return rc;
   if ((rc = pc_backmul_w_launch(c, c->d_lambda, S, psi, K, c->d_force, K, S, S, K, -0.5, 1.0,
                                 c->d_wpt)))
     return rc;
-  mark(4);
+  mark(5);
   // 4. Verlet update
   if ((rc = step_integrate(c, c->d_force, psi, vpsi, dt, iteration, energies + CPSTEP_E_FICT)))
     return rc;
-  mark(5);
+  mark(6);
   // 5. S = overlap, T = (S/2)^(-1/2), psi <- psi.T
   if ((rc = pc_overlap_launch(c, psi, psi, S, S, K, c->d_wpt, 1.0, 0.0, c->d_smat, S))) return rc;
   const int mixed = c->precision == CPSTEP_PREC_MIXED;
@@ -278,7 +285,7 @@ int step_run(cpstep_ctx* c, double* psi, double* vpsi, const double* occ, double
   if ((rc = pc_backmul_launch(c, c->d_tmat, S, psi, K, c->d_psi_tmp, K, S, S, K, 1.0, 0.0))) return rc;
   CPSTEP_CUDA_TRY(cudaMemcpyAsync(psi, c->d_psi_tmp, sizeof(double2) * ncoef,
                                   cudaMemcpyDeviceToDevice, c->stream));
-  mark(6);
+  mark(7);
   if (c->profile) c->prof_pending += 1;
   return CPSTEP_OK;
 }

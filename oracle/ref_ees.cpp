@@ -32,7 +32,7 @@ double getdeth(double* h) {
 void init_nonlocal_ees(int* kmax, double ecut, PSNONLOCAL* psnonlocal, int fft_opt);
 
 namespace {
-std::vector<double> g_vps[4], g_gz, g_norm, g_occ, g_wk, g_kp, g_hmati;
+std::vector<double> g_vps[4], g_gz, g_norm, g_occ, g_wk, g_kp;
 std::vector<int> g_map, g_natm_lang, g_str, g_lang, g_mang, g_ityp;
 std::vector<int*> g_typ_lang_rows;
 std::vector<std::vector<int>> g_typ_lang;
@@ -120,8 +120,8 @@ void ref_ees_setup(int nkf, int n_interp, const double* hmati, double vol, int n
   g_natm = natm;
   g_ntyp = ntyp;
   g_nchan = nchan;
-  g_hmati.assign(hmati, hmati + 9);
-  gd->gencell.hmati = one_based(g_hmati);
+  // GENCELL owns its hmati array (constructor/destructor): fill it in place
+  for (int k = 0; k < 9; ++k) gd->gencell.hmati[k + 1] = hmati[k];
   gd->gencell.vol = vol;
   ps->nsplin_g = nspl;
   ps->gmin_spl = gmin;

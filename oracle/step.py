@@ -79,8 +79,10 @@ def constrain(F, psi, lay):
     return F - 0.5 * w[None] * (lam.T @ psi), lam
 
 
-def forces(psi, occ, sysm, lay, dlay, chunk=16):
-    """Energies, V_KS, constrained-force input F and local atom forces."""
+def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None):
+    """Energies, V_KS, constrained-force input F and atom forces (local + Ewald,
+    plus the EES non-local pass when nonlocal_on: addForces adds its psi force,
+    stateSlab.C:240-272)."""
     vol = sysm.box_len ** 3
     rho = OF.density(psi, lay, occ, vol, chunk=chunk)
     vxc, exc, muxc = OD.pz_lda(rho, vol)
@@ -90,15 +92,22 @@ def forces(psi, occ, sysm, lay, dlay, chunk=16):
                                        sysm.alp_ewd)
     vks = vxc + OD.vg_to_r(vg, dlay)
     fv = OF.vpsi_force(psi, vks, lay, occ, chunk=chunk)
-    F = OF.add_forces(fv, None, lay)
+    enl, fnl, fatm = 0.0, None, None
+    if nonlocal_on:
+        from . import ees as OE
+        enl, fnl, fatm = OE.nonlocal_ees(psi, lay, occ, vol, sysm.hmati(),
+                                         dict(pos=sysm.pos, typ=sysm.typ), sysm.channels,
+                                         sysm.tab, nkf)
+        floc = floc + fatm
+    F = OF.add_forces(fv, fnl, lay)
     F, eke = OF.eke(F, psi, lay, occ, sysm.ecut_ry)
-    en = dict(EXC=exc, MUXC=muxc, EHART=eh, EEXT=ee, EWD=ew, EKE=float(np.sum(eke)))
-    en["ETOT"] = en["EKE"] + eh + ee + exc
+    en = dict(EXC=exc, MUXC=muxc, EHART=eh, EEXT=ee, EWD=ew, EKE=float(np.sum(eke)), ENL=enl)
+    en["ETOT"] = en["EKE"] + enl + eh + ee + exc
     return en, F, floc, rho, vks
 
 
-def cp_step(psi, v, occ, sysm, lay, dlay, cmass, dt, iteration):
-    en, F, floc, rho, vks = forces(psi, occ, sysm, lay, dlay)
+def cp_step(psi, v, occ, sysm, lay, dlay, cmass, dt, iteration, nonlocal_on=False, nkf=None):
+    en, F, floc, rho, vks = forces(psi, occ, sysm, lay, dlay, nonlocal_on=nonlocal_on, nkf=nkf)
     Fc, lam = constrain(F, psi, lay)
     psi2, v2, ke = integrate(Fc, psi, v, cmass, lay, dt, iteration)
     en["FICT"] = ke
