@@ -346,6 +346,8 @@ def kernel_case(args):
     atom forces, V_KS) of the water192 system, run 3 times.
     ees:      the EES non-local pass of `--states` states of the water192
     system (8 s+p channels, 80^3 NL grid), run 2 times.
+    paircalc: S = overlap(psi, psi) and psi.T of `--states` states of the
+    water192 layout (K = 131,472 reals), run 2 times.
     """
     import torch
     from openatom_b200.context import StepContext
@@ -369,12 +371,17 @@ def kernel_case(args):
         for _ in range(3):
             vks, _, _ = ctx.vks_from_rho(rho)
         chk = float(vks.sum())
-    else:
+    elif args.kernel_case == "ees":
         ctx.set_atoms(sysm)
         ctx.set_nonlocal(sysm)
         for _ in range(2):
             fpsi, e, f = ctx.ees_nonlocal(psi, occ)
         chk = float(e[7])
+    else:
+        for _ in range(2):
+            smat = ctx.pc_overlap(psi, psi)
+            out = ctx.pc_backmultiply(smat, psi)
+        chk = float(smat.sum()) + float(out.real.sum())
     torch.cuda.synchronize()
     ctx.close()
     print(json.dumps({"kernel_case": args.kernel_case, "states": S,
@@ -390,7 +397,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="water192", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel-case", choices=["statefft", "rhoside", "ees"], default=None,
+    ap.add_argument("--kernel-case", choices=["statefft", "rhoside", "ees", "paircalc"], default=None,
                     help="run a small profiling case instead of the benchmark")
     ap.add_argument("--states", type=int, default=8)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")

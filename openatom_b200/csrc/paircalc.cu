@@ -87,57 +87,6 @@ __global__ void k_splitk_reduce(const double* __restrict__ part, int nsplit, int
   *c = alpha * s + (beta == 0.0 ? 0.0 : beta * (*c));
 }
 
-// out[i][p] = alpha * w[p/2] * sum_j Mcm[j + i*ldm] * in[j][p] + beta * out[i][p]
-// (i < nout, j < nin, p < K; in/out row-major with ld = ldi / ldo; w optional)
-__global__ void __launch_bounds__(NT)
-k_backmul(const double* __restrict__ Mcm, int ldm, const double* __restrict__ in, int ldi,
-          double* __restrict__ out, int ldo, int nout, int nin, int K, double alpha,
-          double beta, const double* __restrict__ w) {
-  __shared__ double Ms[BK][BM + 1];
-  __shared__ double Is[BK][BN + 1];
-  const int p0 = blockIdx.x * BN, i0 = blockIdx.y * BM;
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  double acc[4][4] = {};
-  for (int j0 = 0; j0 < nin; j0 += BK) {
-    for (int e = threadIdx.x; e < BM * BK; e += NT) {
-      int r = e / BK, c = e % BK;  // M tile: row i0+r, col j0+c -> Mcm[j + i ldm]
-      int i = i0 + r, j = j0 + c;
-      Ms[c][r] = (i < nout && j < nin) ? Mcm[(size_t)i * ldm + j] : 0.0;
-    }
-    for (int e = threadIdx.x; e < BK * BN; e += NT) {
-      int c = e / BN, q = e % BN;
-      int j = j0 + c, p = p0 + q;
-      Is[c][q] = (j < nin && p < K) ? in[(size_t)j * ldi + p] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < BK; ++kk) {
-      double m[4], v[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        m[q] = Ms[kk][ty + 16 * q];
-        v[q] = Is[kk][tx + 16 * q];
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) acc[q][r] += m[q] * v[r];
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      int i = i0 + ty + 16 * q, p = p0 + tx + 16 * r;
-      if (i < nout && p < K) {
-        double* o = out + (size_t)i * ldo + p;
-        double a = w ? alpha * w[p >> 1] : alpha;
-        *o = a * acc[q][r] + (beta == 0.0 ? 0.0 : beta * (*o));
-      }
-    }
-}
-
 // column-major C = alpha op(A) op(B) + beta C (reference DGEMM semantics)
 __global__ void __launch_bounds__(NT)
 k_dgemm(int ta, int tb, int m, int n, int k, double alpha, const double* __restrict__ A, int lda,
@@ -192,17 +141,217 @@ k_dgemm(int ta, int tb, int m, int n, int k, double alpha, const double* __restr
     }
 }
 
+// ---------------------------------------------------------------------------
+// 128 x 128 block tiles: 256 threads, 8 x 8 outputs each (rows ty + 16 i,
+// columns tx + 16 j), K chunks of 16 staged through registers into two
+// shared buffers so the global loads of chunk k+1 overlap the FMAs of chunk k.
+constexpr int TB = 128, TK = 16, TLD = TB + 1;
+constexpr size_t T128_SMEM = sizeof(double) * 4 * TK * TLD;  // two operands, two buffers
+
+// C_part[ks] = A[i0:i0+128, kslab] B[j0:j0+128, kslab]^T (A, B row-major [rows][K],
+// K in reals; w per complex point scales A).  Column-major partial tiles, ld = M.
+__global__ void __launch_bounds__(256, 1)
+k_overlap_t128(const double* __restrict__ A, int lda, const double* __restrict__ B, int ldb,
+               const double* __restrict__ w, int M, int N, int K, int kslab,
+               double* __restrict__ part) {
+  extern __shared__ __align__(16) double t128_smem[];
+  double (*As)[TK][TLD] = reinterpret_cast<double (*)[TK][TLD]>(t128_smem);
+  double (*Bs)[TK][TLD] = reinterpret_cast<double (*)[TK][TLD]>(t128_smem + 2 * TK * TLD);
+  const int i0 = blockIdx.x * TB, j0 = blockIdx.y * TB, ks = blockIdx.z;
+  const int kbeg = ks * kslab, kend = min(K, kbeg + kslab);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  // loader: 4 double2 of A and of B per thread (row = idx / 8, k pair = idx % 8)
+  double2 ra[4], rb[4];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = threadIdx.x + 256 * q;
+      const int row = idx >> 3, kp = idx & 7;
+      const int k = k0 + 2 * kp;
+      double2 va = make_double2(0.0, 0.0), vb = make_double2(0.0, 0.0);
+      if (k < kend) {  // kend and k are even: the pair is inside
+        if (i0 + row < M) {
+          va = *reinterpret_cast<const double2*>(A + (size_t)(i0 + row) * lda + k);
+          if (w) {
+            const double sw = w[k >> 1];
+            va.x *= sw;
+            va.y *= sw;
+          }
+        }
+        if (j0 + row < N) vb = *reinterpret_cast<const double2*>(B + (size_t)(j0 + row) * ldb + k);
+      }
+      ra[q] = va;
+      rb[q] = vb;
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = threadIdx.x + 256 * q;
+      const int row = idx >> 3, kp = idx & 7;
+      As[buf][2 * kp][row] = ra[q].x;
+      As[buf][2 * kp + 1][row] = ra[q].y;
+      Bs[buf][2 * kp][row] = rb[q].x;
+      Bs[buf][2 * kp + 1][row] = rb[q].y;
+    }
+  };
+  int buf = 0;
+  if (kbeg < kend) {
+    load(kbeg);
+    store(0);
+  }
+  __syncthreads();
+  for (int k0 = kbeg; k0 < kend; k0 += TK) {
+    const bool more = k0 + TK < kend;
+    if (more) load(k0 + TK);
+#pragma unroll
+    for (int kk = 0; kk < TK; ++kk) {
+      double a[8], b[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = As[buf][kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = Bs[buf][kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    if (more) store(buf ^ 1);
+    __syncthreads();
+    buf ^= 1;
+  }
+  double* P = part + (size_t)ks * M * N;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int r = i0 + ty + 16 * i, c = j0 + tx + 16 * j;
+      if (r < M && c < N) P[(size_t)c * M + r] = acc[i][j];
+    }
+}
+
+// out[i][p] = alpha w[p/2] sum_j Mcm[j + i ldm] in[j][p] + beta out[i][p] on
+// 128 (i) x 128 (p) tiles; the inner dimension j runs in chunks of 16.
+__global__ void __launch_bounds__(256, 1)
+k_backmul_t128(const double* __restrict__ Mcm, int ldm, const double* __restrict__ in, int ldi,
+               double* __restrict__ out, int ldo, int nout, int nin, int K, double alpha,
+               double beta, const double* __restrict__ w) {
+  extern __shared__ __align__(16) double t128_smem[];
+  double (*Ms)[TK][TLD] = reinterpret_cast<double (*)[TK][TLD]>(t128_smem);  // [j][i]
+  double (*Is)[TK][TLD] = reinterpret_cast<double (*)[TK][TLD]>(t128_smem + 2 * TK * TLD);
+  const int p0 = blockIdx.x * TB, i0 = blockIdx.y * TB;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  double2 rm[4], ri[4];
+  // M tile: row i (128) x 16 j: idx -> i = idx / 8, j pair = idx % 8 (contiguous j)
+  // in tile: 16 j x 128 p: idx -> j = idx / 64, p pair = idx % 64
+  auto load = [&](int j0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = threadIdx.x + 256 * q;
+      const int i = idx >> 3, jp = idx & 7;
+      const int j = j0 + 2 * jp;
+      double2 vm = make_double2(0.0, 0.0);
+      if (i0 + i < nout) {
+        const double* mrow = Mcm + (size_t)(i0 + i) * ldm;
+        if (j + 1 < nin) vm = make_double2(mrow[j], mrow[j + 1]);
+        else if (j < nin) vm.x = mrow[j];
+      }
+      rm[q] = vm;
+      const int jj = idx >> 6, pp = idx & 63;
+      const int jr = j0 + jj, p = p0 + 2 * pp;
+      double2 vi = make_double2(0.0, 0.0);
+      if (jr < nin && p < K)  // K even, p even: the pair is inside
+        vi = *reinterpret_cast<const double2*>(in + (size_t)jr * ldi + p);
+      ri[q] = vi;
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = threadIdx.x + 256 * q;
+      const int i = idx >> 3, jp = idx & 7;
+      Ms[buf][2 * jp][i] = rm[q].x;
+      Ms[buf][2 * jp + 1][i] = rm[q].y;
+      const int jj = idx >> 6, pp = idx & 63;
+      Is[buf][jj][2 * pp] = ri[q].x;
+      Is[buf][jj][2 * pp + 1] = ri[q].y;
+    }
+  };
+  int buf = 0;
+  load(0);
+  store(0);
+  __syncthreads();
+  for (int j0 = 0; j0 < nin; j0 += TK) {
+    const bool more = j0 + TK < nin;
+    if (more) load(j0 + TK);
+#pragma unroll
+    for (int kk = 0; kk < TK; ++kk) {
+      double a[8], b[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = Ms[buf][kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = Is[buf][kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    if (more) store(buf ^ 1);
+    __syncthreads();
+    buf ^= 1;
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int r = i0 + ty + 16 * i, p = p0 + tx + 16 * j;
+      if (r < nout && p < K) {
+        double* o = out + (size_t)r * ldo + p;
+        const double a = w ? alpha * w[p >> 1] : alpha;
+        *o = a * acc[i][j] + (beta == 0.0 ? 0.0 : beta * (*o));
+      }
+    }
+}
+
 }  // namespace pcalc
 
 // ---------------------------------------------------------------------------
 // host side
 
+static int t128_attr() {
+  static unsigned long long done = 0;  // one bit per device (the attribute is per device)
+  int dev = 0;
+  CPSTEP_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(__atomic_load_n(&done, __ATOMIC_ACQUIRE) & bit)) {
+    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(pcalc::k_overlap_t128,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pcalc::T128_SMEM));
+    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(pcalc::k_backmul_t128,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pcalc::T128_SMEM));
+    __atomic_or_fetch(&done, bit, __ATOMIC_RELEASE);
+  }
+  return CPSTEP_OK;
+}
+
 int pc_overlap_launch(cpstep_ctx* c, const double* a, const double* b, int M, int N, int K,
                       const double* w, double alpha, double beta, double* C, int ldc) {
   using namespace pcalc;
-  int tm = cdiv(M, BM), tn = cdiv(N, BN);
-  int want = std::max(1, (2 * c->num_sms) / (tm * tn));
-  int kslab = cdiv(cdiv(K, want), BK) * BK;
+  if (int rc = t128_attr()) return rc;
+  int tm = cdiv(M, TB), tn = cdiv(N, TB);
+  int want = std::max(1, c->num_sms / (tm * tn));
+  int kslab = cdiv(cdiv(K, want), TK) * TK;
   int nsplit = cdiv(K, kslab);
   size_t need = (size_t)nsplit * M * N;
   if (need > c->pc_part_elems) {
@@ -211,8 +360,8 @@ int pc_overlap_launch(cpstep_ctx* c, const double* a, const double* b, int M, in
     CPSTEP_CUDA_TRY(cudaMalloc(&c->d_pc_part, need * sizeof(double)));
     c->pc_part_elems = need;
   }
-  k_overlap_part<<<dim3(tm, tn, nsplit), NT, 0, c->stream>>>(a, K, b, K, w, M, N, K, kslab,
-                                                             c->d_pc_part);
+  k_overlap_t128<<<dim3(tm, tn, nsplit), 256, T128_SMEM, c->stream>>>(a, K, b, K, w, M, N, K,
+                                                                     kslab, c->d_pc_part);
   CPSTEP_LAUNCH_CHECK();
   k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, c->stream>>>(c->d_pc_part, nsplit, M, N, alpha,
                                                             beta, C, ldc);
@@ -223,9 +372,10 @@ int pc_overlap_launch(cpstep_ctx* c, const double* a, const double* b, int M, in
 int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
                       double* out, int ldo, int nout, int nin, int K, double alpha, double beta) {
   using namespace pcalc;
-  dim3 grid(cdiv(K, BN), cdiv(nout, BM));
-  k_backmul<<<grid, NT, 0, c->stream>>>(Mcm, ldm, in, ldi, out, ldo, nout, nin, K, alpha, beta,
-                                        nullptr);
+  if (int rc = t128_attr()) return rc;
+  dim3 grid(cdiv(K, TB), cdiv(nout, TB));
+  k_backmul_t128<<<grid, 256, T128_SMEM, c->stream>>>(Mcm, ldm, in, ldi, out, ldo, nout, nin, K,
+                                                      alpha, beta, nullptr);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }
@@ -234,8 +384,10 @@ int pc_backmul_w_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double*
                         double* out, int ldo, int nout, int nin, int K, double alpha, double beta,
                         const double* w) {
   using namespace pcalc;
-  dim3 grid(cdiv(K, BN), cdiv(nout, BM));
-  k_backmul<<<grid, NT, 0, c->stream>>>(Mcm, ldm, in, ldi, out, ldo, nout, nin, K, alpha, beta, w);
+  if (int rc = t128_attr()) return rc;
+  dim3 grid(cdiv(K, TB), cdiv(nout, TB));
+  k_backmul_t128<<<grid, 256, T128_SMEM, c->stream>>>(Mcm, ldm, in, ldi, out, ldo, nout, nin, K,
+                                                      alpha, beta, w);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }
