@@ -25,6 +25,7 @@
 #include <cmath>
 #include <vector>
 #include "ctx.cuh"
+#include "fft_shfl.cuh"
 
 namespace sfft {
 
@@ -92,6 +93,28 @@ __device__ __forceinline__ void block_lines(cplx<T>* buf, int ld, int nl, const 
     warp_lines<T, N, INV>(buf + (size_t)l0 * ld, ld, min(L, nl - l0), tw);
 }
 
+// Lines c = grp, grp + ngrp, ... (stride ldy) through dif (DIF: natural in,
+// permuted out, see shfl_perm) or dit (permuted in, natural out), in place.
+template <typename T, int N, bool INV, bool DIF>
+__device__ __forceinline__ void shfl_columns(cplx<T>* plane, int ldy, int nplx,
+                                             const ShflFft<T, N>& F, const cplx<T>* tw,
+                                             int grp, int ngrp) {
+  constexpr int NL = ShflCfg<N>::NL, M = ShflCfg<N>::M;
+  for (int c0 = 0; c0 < nplx; c0 += ngrp) {
+    const int c = c0 + grp;
+    const bool act = c < nplx;
+    cplx<T> v[M];
+    cplx<T>* col = plane + (size_t)(act ? c : 0) * ldy;
+#pragma unroll
+    for (int k = 0; k < M; ++k) v[k] = act ? col[F.l + NL * k] : mk<T>(0, 0);
+    if (DIF) F.template dif<INV>(v, tw); else F.template dit<INV>(v, tw);
+    if (act) {
+#pragma unroll
+      for (int k = 0; k < M; ++k) col[F.l + NL * k] = v[k];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // K1: expand packed psi into z-lines, forward z-FFT, write [s][z][line] pencils
 // With mul (EES projector dyp), the line holds conj(mul * psi) instead of psi
@@ -134,12 +157,19 @@ k_zfft_fwd(const double2* __restrict__ psi, cplx<T>* __restrict__ pen, StateGeom
     buf[li * LD + z] = mk<T>((T)v.x, (T)v.y);
   }
   __syncthreads();
-  block_lines<T, N, false>(buf, LD, nl, tw);  // FFTW_FORWARD along z
+  if constexpr (ShflCfg<N>::ok) {
+    ShflFft<T, N> F;
+    F.init(tw);
+    shfl_columns<T, N, false, true>(buf, LD, nl, F, tw, threadIdx.x / ShflCfg<N>::NL,
+                                    ZTHREADS / ShflCfg<N>::NL);  // FFTW_FORWARD along z
+  } else {
+    block_lines<T, N, false>(buf, LD, nl, tw);  // FFTW_FORWARD along z
+  }
   __syncthreads();
   cplx<T>* po = pen + (size_t)s * N * g.nlpad + l0;
   for (int i = threadIdx.x; i < nl * N; i += ZTHREADS) {
     int z = i / nl, li = i - z * nl;
-    po[(size_t)z * g.nlpad + li] = buf[li * LD + z];
+    po[(size_t)z * g.nlpad + li] = buf[li * LD + (ShflCfg<N>::ok ? shfl_perm<N>(z) : z)];
   }
 }
 
@@ -409,6 +439,222 @@ k_xy_bwd(const cplx<T>* __restrict__ pen, const double* __restrict__ freal,
 }
 
 // ---------------------------------------------------------------------------
+// Plane passes with register-resident line FFTs (ShflFft) for the sizes
+// ShflCfg<N> lists.  A group of NL lanes owns one column (y) or one row pair
+// (x) at a time; only the plane itself is in shared memory.  Columns are
+// transformed in place by dif (natural -> the permuted storage shfl_perm) or
+// dit (permuted -> natural); rows are built from the plane straight into
+// registers and written back to the permuted positions they came from.
+
+template <typename T, int N>
+struct SShape {
+  static constexpr int LDY = N + 1;
+  static constexpr int NL = ShflCfg<N>::NL, M = ShflCfg<N>::M;
+  static constexpr int NG = PTHREADS / NL;                 // lane groups per block
+  static constexpr int QMAX = (N / 2 + NG - 1) / NG;       // row pairs per group
+  static constexpr size_t bytes(int nplx) {
+    return sizeof(cplx<T>) * ((size_t)N + (size_t)nplx * LDY);
+  }
+};
+
+// Row pair (ya, ya+1) of the y-transformed (permuted) plane as the C2R input
+// Z = Xa + i Xb in dif order (element x = l + NL k in slot k): the imag flip,
+// the Hermitian extension to kx > N/2, zero outside the nplane_x columns.
+template <typename T, int N>
+__device__ __forceinline__ void shfl_build_row(const cplx<T>* plane, int ldy, int nplx, int ya,
+                                               const ShflFft<T, N>& F,
+                                               cplx<T> (&v)[ShflCfg<N>::M]) {
+  constexpr int NL = ShflCfg<N>::NL, M = ShflCfg<N>::M;
+  const int pa = shfl_perm<N>(ya), pb = shfl_perm<N>(ya + 1);
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    const int x = F.l + NL * k;
+    cplx<T> z = mk<T>(0, 0);
+    if (x == 0) {
+      z = mk<T>(plane[pa].x, plane[pb].x);
+    } else if (x < nplx) {
+      const cplx<T> a = plane[x * ldy + pa], b = plane[x * ldy + pb];
+      z = mk<T>(a.x + b.y, b.x - a.y);  // conj(a) + i conj(b)
+    } else if (N - x < nplx) {
+      const int m = N - x;
+      const cplx<T> a = plane[m * ldy + pa], b = plane[m * ldy + pb];
+      z = mk<T>(a.x - b.y, a.y + b.x);  // a + i b
+    }
+    v[k] = z;
+  }
+}
+
+// After dit (forward, R2C) of a row pair: natural Zf[l + NL k] in slot k.
+// Split the two real rows' spectra, apply the imag flip and store kx <
+// nplane_x at the permuted positions of rows ya, ya+1.
+template <typename T, int N>
+__device__ __forceinline__ void shfl_extract_row(const cplx<T> (&v)[ShflCfg<N>::M],
+                                                 cplx<T>* plane, int ldy, int nplx, int ya,
+                                                 const ShflFft<T, N>& F, bool act) {
+  constexpr int NL = ShflCfg<N>::NL, M = ShflCfg<N>::M;
+  const int pa = shfl_perm<N>(ya), pb = shfl_perm<N>(ya + 1);
+  const int src = (NL - F.l) & (NL - 1);
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    // Zf[N - kx] with kx = l + NL k: lane NL - l, slot M - 1 - k (l > 0); own slot (M - k) % M (l = 0)
+    cplx<T> zm;
+    zm.x = __shfl_sync(0xffffffffu, v[M - 1 - k].x, src, NL);
+    zm.y = __shfl_sync(0xffffffffu, v[M - 1 - k].y, src, NL);
+    if (F.l == 0) zm = v[(M - k) % M];
+    const int kx = F.l + NL * k;
+    if (act && kx < nplx) {
+      const cplx<T> zk = v[k];
+      plane[kx * ldy + pa] = mk<T>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zm.y - zk.y));
+      plane[kx * ldy + pb] = mk<T>((T)0.5 * (zk.y + zm.y), (T)0.5 * (zk.x - zm.x));
+    }
+  }
+}
+
+// K2 (shuffle form): planes -> psi(r).  MODE 0 accumulates occ psi^2 into the
+// group's FP64 registers (row pairs grp, grp + NG, ...), MODE 1 writes psi(r).
+template <typename T, int N, int MODE>
+__global__ void __launch_bounds__(PTHREADS, 1)
+k_xy_fwd_s(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict__ twx_g,
+           const double* __restrict__ occ, int nstates, int spg, double* __restrict__ out) {
+  using S = SShape<T, N>;
+  constexpr int LDY = S::LDY, NL = S::NL, M = S::M, NG = S::NG, QMAX = S::QMAX;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* plane = tw + N;
+  const int grp = threadIdx.x / NL;
+  const int z = blockIdx.x;
+  const int s0 = blockIdx.y * spg, s1 = min(nstates, s0 + spg);
+  for (int i = threadIdx.x; i < N; i += PTHREADS) tw[i] = twx_g[i];
+  __syncthreads();
+  ShflFft<T, N> F;
+  F.init(tw);
+  double acc[QMAX][2][M];
+#pragma unroll
+  for (int q = 0; q < QMAX; ++q)
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int k = 0; k < M; ++k) acc[q][h][k] = 0.0;
+  for (int s = s0; s < s1; ++s) {
+    scatter_plane<T, N>(pen + ((size_t)s * N + z) * g.nlpad, plane, g);
+    shfl_columns<T, N, false, true>(plane, LDY, g.nplane_x, F, tw, grp, NG);  // FFTW_FORWARD y
+    __syncthreads();
+    const double w = (MODE == 0) ? occ[s] : 1.0;
+    // every lane of a warp runs the shuffles: groups past the last pair
+    // transform row 0 and drop the result
+#pragma unroll
+    for (int q = 0; q < QMAX; ++q) {
+      const int pp = grp + NG * q;
+      const bool act = pp < N / 2;
+      const int ya = act ? 2 * pp : 0;
+      cplx<T> v[M];
+      shfl_build_row<T, N>(plane, LDY, g.nplane_x, ya, F, v);
+      F.template dif<true>(v, tw);  // C2R, +i sign
+      if (act) {
+        if (MODE == 0) {
+#pragma unroll
+          for (int k = 0; k < M; ++k) {
+            acc[q][0][k] += w * (double)v[k].x * (double)v[k].x;
+            acc[q][1][k] += w * (double)v[k].y * (double)v[k].y;
+          }
+        } else {
+          double* o = out + (((size_t)s * N + z) * N + ya) * N;
+#pragma unroll
+          for (int k = 0; k < M; ++k) {
+            const int x = F.pos(k);
+            o[x] = (double)v[k].x;
+            o[N + x] = (double)v[k].y;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (MODE == 0) {
+    double* o = out + ((size_t)blockIdx.y * N + z) * N * N;
+#pragma unroll
+    for (int q = 0; q < QMAX; ++q) {
+      const int pp = grp + NG * q;
+      if (pp < N / 2) {
+        const int ya = 2 * pp;
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+          const int x = F.pos(k);
+          o[(size_t)ya * N + x] = acc[q][0][k];
+          o[(size_t)(ya + 1) * N + x] = acc[q][1][k];
+        }
+      }
+    }
+  }
+}
+
+// K3 (shuffle form): MODE 0 pencils -> psi(r) -> psi V occ -> pencils_out;
+// MODE 1 real f(r) (FP64, [s][z][y][x]) -> pencils_out.
+template <typename T, int N, int MODE>
+__global__ void __launch_bounds__(PTHREADS, 1)
+k_xy_bwd_s(const cplx<T>* __restrict__ pen, const double* __restrict__ freal,
+           const T* __restrict__ vks, cplx<T>* __restrict__ pen_out, StateGeom g,
+           const cplx<T>* __restrict__ twx_g, const double* __restrict__ occ, int nstates,
+           int spg) {
+  using S = SShape<T, N>;
+  constexpr int LDY = S::LDY, M = S::M, NG = S::NG, NL = S::NL;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* plane = tw + N;
+  const int grp = threadIdx.x / NL;
+  const int z = blockIdx.x;
+  const int s0 = blockIdx.y * spg, s1 = min(nstates, s0 + spg);
+  for (int i = threadIdx.x; i < N; i += PTHREADS) tw[i] = twx_g[i];
+  const T* vplane = (MODE == 0) ? vks + (size_t)z * N * N : nullptr;
+  __syncthreads();
+  ShflFft<T, N> F;
+  F.init(tw);
+  for (int s = s0; s < s1; ++s) {
+    if (MODE == 0) {
+      scatter_plane<T, N>(pen + ((size_t)s * N + z) * g.nlpad, plane, g);
+      shfl_columns<T, N, false, true>(plane, LDY, g.nplane_x, F, tw, grp, NG);
+      __syncthreads();
+    }
+    const T w = (MODE == 0) ? (T)occ[s] : (T)1;
+    // same trip count for every group of a warp (the shuffles need all lanes)
+    for (int p0 = 0; p0 < N / 2; p0 += NG) {
+      const int pp = p0 + grp;
+      const bool act = pp < N / 2;
+      const int ya = act ? 2 * pp : 0;
+      cplx<T> v[M];
+      if (MODE == 0) {
+        shfl_build_row<T, N>(plane, LDY, g.nplane_x, ya, F, v);
+        F.template dif<true>(v, tw);  // C2R, +i sign
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+          const int x = F.pos(k);
+          v[k].x *= __ldg(vplane + ya * N + x) * w;
+          v[k].y *= __ldg(vplane + (ya + 1) * N + x) * w;
+        }
+      } else {
+        const double* fs = freal + ((size_t)s * N + z) * N * N;
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+          const int x = F.pos(k);
+          v[k] = mk<T>((T)fs[ya * N + x], (T)fs[(ya + 1) * N + x]);
+        }
+      }
+      F.template dit<false>(v, tw);  // R2C, -i sign
+      shfl_extract_row<T, N>(v, plane, LDY, g.nplane_x, ya, F, act);
+    }
+    __syncthreads();
+    shfl_columns<T, N, true, false>(plane, LDY, g.nplane_x, F, tw, grp, NG);  // BACKWARD y
+    __syncthreads();
+    cplx<T>* po = pen_out + ((size_t)s * N + z) * g.nlpad;
+    for (int l = threadIdx.x; l < g.nlines; l += PTHREADS) {
+      int xy = __ldg(g.line_xy + l);
+      po[l] = plane[(xy & 0xffff) * LDY + (xy >> 16)];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // K4: pencils -> backward z-FFT -> pack -> scale.
 //   MODE 0: F = scale * wpt * val (then, if occ != null, the kinetic term)
 //   MODE 1: plain pack with scale (adjoint transform)
@@ -447,7 +693,14 @@ k_zfft_bwd(const cplx<T>* __restrict__ pen, double2* __restrict__ fout,
     buf[li * LD + z] = pi[(size_t)z * g.nlpad + li];
   }
   __syncthreads();
-  block_lines<T, N, true>(buf, LD, nl, tw);  // FFTW_BACKWARD along z
+  if constexpr (ShflCfg<N>::ok) {
+    ShflFft<T, N> F;
+    F.init(tw);
+    shfl_columns<T, N, true, true>(buf, LD, nl, F, tw, threadIdx.x / ShflCfg<N>::NL,
+                                   ZTHREADS / ShflCfg<N>::NL);  // FFTW_BACKWARD along z
+  } else {
+    block_lines<T, N, true>(buf, LD, nl, tw);  // FFTW_BACKWARD along z
+  }
   __syncthreads();
   const int p0 = soff[0], p1 = soff[nl];
   double e = 0.0;
@@ -455,7 +708,7 @@ k_zfft_bwd(const cplx<T>* __restrict__ pen, double2* __restrict__ fout,
   for (int p = p0 + threadIdx.x; p < p1; p += ZTHREADS) {
     int li, z;
     locate(p, soff, nl, snneg, szneg, szpos, li, z);
-    cplx<T> v = buf[li * LD + z];
+    cplx<T> v = buf[li * LD + (ShflCfg<N>::ok ? shfl_perm<N>(z) : z)];
     if (MODE == 2) {
       double vx = (double)v.x, vy = (double)v.y;
       double2 d = mul[p];
@@ -553,12 +806,47 @@ k_nl_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict
   const int* pl = A.plist + ((size_t)ctype * (int)A.grid + z) * A.natm;
   const int npl = A.pcount[ctype * (int)A.grid + z];
   const int ja = lane & 7, jb0 = lane >> 3;
+  // row pairs that some atom's stencil reads (the others are not transformed)
+  __shared__ int pairs[N / 2];
+  for (int i = threadIdx.x; i < N / 2; i += NLTHREADS) pairs[i] = 0;
   __syncthreads();
+  for (int i = threadIdx.x; i < npl * kNlInterp; i += NLTHREADS) {
+    const int e = i / kNlInterp, jb = i - e * kNlInterp;
+    pairs[A.ig[(size_t)(pl[e] & 0xffff) * 3 * kNlInterp + kNlInterp + jb] >> 1] = 1;
+  }
+  __syncthreads();
+  ShflFft<T, N> F;
+  if constexpr (ShflCfg<N>::ok) F.init(tw);
   for (int s = s0; s < s1; ++s) {
     scatter_plane<T, N>(pen + ((size_t)s * N + z) * g.nlpad, plane, g);
+    if constexpr (ShflCfg<N>::ok) {
+      constexpr int NL = ShflCfg<N>::NL, M = ShflCfg<N>::M, NG = NLTHREADS / NL;
+      const int grp = threadIdx.x / NL;
+      shfl_columns<T, N, false, true>(plane, LDY, g.nplane_x, F, tw, grp, NG);  // FORWARD y
+      __syncthreads();
+      for (int p0 = 0; p0 < N / 2; p0 += NG) {
+        const int pp = p0 + grp;
+        const bool act = pp < N / 2 && pairs[pp];
+        if (!__any_sync(0xffffffffu, act)) continue;  // warp-uniform: the shuffles need all lanes
+        const int ya = act ? 2 * pp : 0;
+        cplx<T> v[M];
+        shfl_build_row<T, N>(plane, LDY, g.nplane_x, ya, F, v);
+        F.template dif<true>(v, tw);  // C2R, +i sign
+        if (act) {
+#pragma unroll
+          for (int k = 0; k < M; ++k) {
+            const int x = F.pos(k);
+            R[(size_t)ya * N + x] = v[k].x;
+            R[(size_t)(ya + 1) * N + x] = v[k].y;
+          }
+        }
+      }
+      __syncthreads();
+    } else {
     plane_columns<T, N, false>(plane, g.nplane_x, tw);  // FFTW_FORWARD y
     __syncthreads();
     for (int pp = warp; pp < N / 2; pp += NW) {
+      if (!pairs[pp]) continue;
       const int ya = 2 * pp;
       cplx<T>* row = reinterpret_cast<cplx<T>*>(R + (size_t)ya * N);
       build_c2r_row<T, N>(plane, row, g.nplane_x, ya);
@@ -581,6 +869,7 @@ k_nl_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict
       __syncwarp();
     }
     __syncthreads();
+    }
     // atoms on this plane: lane -> (jb, ja) = (lane / 8 + 4 h, lane % 8), h = 0, 1
     for (int e = warp; e < npl; e += NW) {
       const int a = pl[e] & 0xffff, jc = pl[e] >> 16;
@@ -635,8 +924,20 @@ k_nl_bwd(cplx<T>* __restrict__ pen_out, StateGeom g, const cplx<T>* __restrict__
   for (int i = threadIdx.x; i < N; i += NLTHREADS) tw[i] = twx_g[i];
   const int* pl = A.plist + ((size_t)ctype * (int)A.grid + z) * A.natm;
   const int npl = A.pcount[ctype * (int)A.grid + z];
+  // row pairs the scatter writes (the others transform to zero)
+  __shared__ int pairs[N / 2];
+  for (int i = threadIdx.x; i < N / 2; i += NLTHREADS) pairs[i] = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < npl * kNlInterp; i += NLTHREADS) {
+    const int e = i / kNlInterp, jb = i - e * kNlInterp;
+    pairs[A.ig[(size_t)(pl[e] & 0xffff) * 3 * kNlInterp + kNlInterp + jb] >> 1] = 1;
+  }
+  __syncthreads();
+  ShflFft<T, N> F;
+  if constexpr (ShflCfg<N>::ok) F.init(tw);
   for (int s = s0; s < s1; ++s) {
     for (int i = threadIdx.x; i < N * N; i += NLTHREADS) R[i] = (T)0;
+    for (int i = threadIdx.x; i < g.nplane_x * LDY; i += NLTHREADS) plane[i] = mk<T>(0, 0);
     __syncthreads();
     if (warp == 0) {
       const int ja = lane & 7, jb0 = lane >> 3;
@@ -656,7 +957,29 @@ k_nl_bwd(cplx<T>* __restrict__ pen_out, StateGeom g, const cplx<T>* __restrict__
       }
     }
     __syncthreads();
+    if constexpr (ShflCfg<N>::ok) {
+      constexpr int NL = ShflCfg<N>::NL, M = ShflCfg<N>::M, NG = NLTHREADS / NL;
+      const int grp = threadIdx.x / NL;
+      for (int p0 = 0; p0 < N / 2; p0 += NG) {
+        const int pp = p0 + grp;
+        const bool act = pp < N / 2 && pairs[pp];
+        if (!__any_sync(0xffffffffu, act)) continue;  // warp-uniform: the shuffles need all lanes
+        const int ya = act ? 2 * pp : 0;
+        cplx<T> v[M];
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+          const int x = F.pos(k);
+          v[k] = mk<T>(R[(size_t)ya * N + x], R[(size_t)(ya + 1) * N + x]);
+        }
+        F.template dit<false>(v, tw);  // R2C, -i sign
+        shfl_extract_row<T, N>(v, plane, LDY, g.nplane_x, ya, F, act);
+      }
+      __syncthreads();
+      shfl_columns<T, N, true, false>(plane, LDY, g.nplane_x, F, tw, grp, NG);  // BACKWARD y
+      __syncthreads();
+    } else {
     for (int pp = warp; pp < N / 2; pp += NW) {
+      if (!pairs[pp]) continue;
       const int ya = 2 * pp;
       cplx<T>* row = reinterpret_cast<cplx<T>*>(R + (size_t)ya * N);
       cplx<T> v[E];
@@ -678,6 +1001,7 @@ k_nl_bwd(cplx<T>* __restrict__ pen_out, StateGeom g, const cplx<T>* __restrict__
     __syncthreads();
     plane_columns<T, N, true>(plane, g.nplane_x, tw);  // FFTW_BACKWARD along y
     __syncthreads();
+    }
     cplx<T>* po = pen_out + ((size_t)s * N + z) * g.nlpad;
     for (int l = threadIdx.x; l < g.nlines; l += NLTHREADS) {
       int xy = __ldg(g.line_xy + l);
@@ -736,6 +1060,22 @@ struct StateFft {
   static int density(cpstep_ctx* c, const double* psi, const double* occ, double* rho) {
     const FftJob j = c->state_job();
     if (int rc = zfft_fwd(c, j, psi, c->nstates)) return rc;
+    if constexpr (ShflCfg<N>::ok) {
+      const size_t smem = SShape<T, N>::bytes(j.g.nplane_x);
+      int ng = std::min(c->ngroups_rho, plane_groups(c, c->nstates, 1));
+      int spg = cdiv(c->nstates, ng);
+      ng = cdiv(c->nstates, spg);
+      if (int rc = set_smem(k_xy_fwd_s<T, N, 0>, smem)) return rc;
+      k_xy_fwd_s<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
+          reinterpret_cast<const cplx<T>*>(j.pen_a), j.g, tws<T>(c).x, occ, c->nstates, spg,
+          c->d_rho_part);
+      CPSTEP_LAUNCH_CHECK();
+      size_t nr = (size_t)N * N * N;
+      k_rho_reduce<<<2 * c->num_sms, 256, 0, c->stream>>>(c->d_rho_part, ng, nr, 1.0 / c->vol,
+                                                          rho);
+      CPSTEP_LAUNCH_CHECK();
+      return CPSTEP_OK;
+    }
     const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
     const int rows = PShape<T, N>::ROWS;
     int ysplit = cdiv(N, rows);
@@ -756,6 +1096,14 @@ struct StateFft {
   // packed G -> real r for nstates arrays of the job's geometry
   static int g2r(cpstep_ctx* c, const FftJob& j, const double* packed, double* real, int nstates) {
     if (int rc = zfft_fwd(c, j, packed, nstates)) return rc;
+    if constexpr (ShflCfg<N>::ok) {
+      const size_t smem = SShape<T, N>::bytes(j.g.nplane_x);
+      if (int rc = set_smem(k_xy_fwd_s<T, N, 1>, smem)) return rc;
+      k_xy_fwd_s<T, N, 1><<<dim3(N, nstates), PTHREADS, smem, c->stream>>>(
+          reinterpret_cast<const cplx<T>*>(j.pen_a), j.g, tws<T>(c).x, nullptr, nstates, 1, real);
+      CPSTEP_LAUNCH_CHECK();
+      return CPSTEP_OK;
+    }
     const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
     if (int rc = set_smem(k_xy_fwd<T, N, 1>, smem)) return rc;
     k_xy_fwd<T, N, 1><<<dim3(N, nstates, 1), PTHREADS, smem, c->stream>>>(
@@ -800,14 +1148,22 @@ struct StateFft {
       CPSTEP_LAUNCH_CHECK();
       vt = reinterpret_cast<const T*>(c->d_vks_t);
     }
-    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
     int ng = plane_groups(c, c->nstates, 1);
     int spg = cdiv(c->nstates, ng);
     ng = cdiv(c->nstates, spg);
-    if (int rc = set_smem(k_xy_bwd<T, N, 0>, smem)) return rc;
-    k_xy_bwd<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
-        reinterpret_cast<const cplx<T>*>(j.pen_a), nullptr, vt,
-        reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, occ, c->nstates, spg);
+    if constexpr (ShflCfg<N>::ok) {
+      const size_t smem = SShape<T, N>::bytes(j.g.nplane_x);
+      if (int rc = set_smem(k_xy_bwd_s<T, N, 0>, smem)) return rc;
+      k_xy_bwd_s<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
+          reinterpret_cast<const cplx<T>*>(j.pen_a), nullptr, vt,
+          reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, occ, c->nstates, spg);
+    } else {
+      const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
+      if (int rc = set_smem(k_xy_bwd<T, N, 0>, smem)) return rc;
+      k_xy_bwd<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
+          reinterpret_cast<const cplx<T>*>(j.pen_a), nullptr, vt,
+          reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, occ, c->nstates, spg);
+    }
     CPSTEP_LAUNCH_CHECK();
     double scale = -2.0 / ((double)N * N * N);
     if (int rc = zfft_bwd(c, j, force, psi, eke ? occ : nullptr, c->nstates, scale, 0)) return rc;
@@ -822,11 +1178,19 @@ struct StateFft {
   // real r -> packed G (sum_r f(r) e^{+iG.r}) times scale, for the job's geometry
   static int r2g(cpstep_ctx* c, const FftJob& j, const double* f_r, double* fg, int nstates,
                  double scale) {
-    const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
-    if (int rc = set_smem(k_xy_bwd<T, N, 1>, smem)) return rc;
-    k_xy_bwd<T, N, 1><<<dim3(N, nstates), PTHREADS, smem, c->stream>>>(
-        nullptr, f_r, nullptr, reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, nullptr,
-        nstates, 1);
+    if constexpr (ShflCfg<N>::ok) {
+      const size_t smem = SShape<T, N>::bytes(j.g.nplane_x);
+      if (int rc = set_smem(k_xy_bwd_s<T, N, 1>, smem)) return rc;
+      k_xy_bwd_s<T, N, 1><<<dim3(N, nstates), PTHREADS, smem, c->stream>>>(
+          nullptr, f_r, nullptr, reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, nullptr,
+          nstates, 1);
+    } else {
+      const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
+      if (int rc = set_smem(k_xy_bwd<T, N, 1>, smem)) return rc;
+      k_xy_bwd<T, N, 1><<<dim3(N, nstates), PTHREADS, smem, c->stream>>>(
+          nullptr, f_r, nullptr, reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, nullptr,
+          nstates, 1);
+    }
     CPSTEP_LAUNCH_CHECK();
     return zfft_bwd(c, j, fg, nullptr, nullptr, nstates, scale, 1);
   }

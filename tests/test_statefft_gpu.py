@@ -11,8 +11,10 @@ from conftest import cuda_ok
 pytestmark = pytest.mark.gpu
 
 TOL = {"fp64": 1e-11, "mixed": 2e-5}
-# (box bohr, ecut Ry, grid) -> grids 28, 42 (reference radixme), 48 (grid override)
-CASES = [(9.0, 20.0, None), (12.0, 30.0, None), (12.0, 30.0, 48)]
+# (box bohr, ecut Ry, grid) -> grids 28, 42 (reference radixme), 48 (grid override);
+# 32, 64, 80, 96 and 128 run the register (shuffle) plane FFTs
+CASES = [(9.0, 20.0, None), (12.0, 30.0, None), (12.0, 30.0, 48), (9.0, 20.0, 32),
+         (12.0, 30.0, 64), (12.0, 30.0, 80), (12.0, 30.0, 96), (12.0, 30.0, 128)]
 
 
 def relerr(a, b):
