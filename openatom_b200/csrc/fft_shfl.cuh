@@ -36,7 +36,11 @@ struct ShflFft {
   using C = ShflCfg<N>;
   static constexpr int NL = C::NL, M = C::M, LOG = C::LOG;
   cplx<T> twl[M];    // W_N^{l k'}, k' < M
-  cplx<T> twd[LOG];  // per stage d = 2^s: W_{2d}^{l mod d} = W_N^{(l mod d) N / (2d)}
+  // per stage d = 2^s: W_{2d}^{l mod d} = W_N^{(l mod d) N / (2d)} on the upper
+  // lane of each pair (l & d), 1 on the lower one; sgn = -1 upper, +1 lower.
+  // With them a butterfly is the same straight-line code on both lanes.
+  cplx<T> twd[LOG];
+  T sgn[LOG];
   int l;             // lane within the group
 
   __device__ __forceinline__ void init(const cplx<T>* tw) {
@@ -46,7 +50,9 @@ struct ShflFft {
 #pragma unroll
     for (int s = 0; s < LOG; ++s) {
       const int d = 1 << s;
-      twd[s] = tw[(l & (d - 1)) * (N / (2 * d))];
+      const bool up = (l & d) != 0;
+      twd[s] = up ? tw[(l & (d - 1)) * (N / (2 * d))] : mk<T>((T)1, (T)0);
+      sgn[s] = up ? (T)-1 : (T)1;
     }
   }
 
@@ -63,29 +69,31 @@ struct ShflFft {
     Dft<T, M, INV>::template run<N>(v, tw);
 #pragma unroll
     for (int k = 1; k < M; ++k) v[k] = mulw<INV>(v[k], twl[k]);
+    // lower lane: a + b; upper lane: (a - b) W  (a lower value, b upper value)
 #pragma unroll
     for (int s = LOG - 1; s >= 0; --s) {
       const int d = 1 << s;
-      const bool up = (l & d) != 0;
 #pragma unroll
       for (int k = 0; k < M; ++k) {
         const cplx<T> p = shfl(v[k], d);
-        v[k] = up ? mulw<INV>(p - v[k], twd[s]) : v[k] + p;
+        const cplx<T> t = mk<T>(p.x + sgn[s] * v[k].x, p.y + sgn[s] * v[k].y);
+        v[k] = mulw<INV>(t, twd[s]);
       }
     }
   }
 
   template <bool INV>
   __device__ __forceinline__ void dit(cplx<T> (&v)[M], const cplx<T>* tw) const {
+    // lower lane: a + W b; upper lane: a - W b.  The upper lane applies W to
+    // its own value before the exchange.
 #pragma unroll
     for (int s = 0; s < LOG; ++s) {
       const int d = 1 << s;
-      const bool up = (l & d) != 0;
 #pragma unroll
       for (int k = 0; k < M; ++k) {
-        const cplx<T> p = shfl(v[k], d);
-        const cplx<T> t = mulw<INV>(up ? v[k] : p, twd[s]);
-        v[k] = up ? p - t : v[k] + t;
+        const cplx<T> u = mulw<INV>(v[k], twd[s]);
+        const cplx<T> p = shfl(u, d);
+        v[k] = mk<T>(p.x + sgn[s] * u.x, p.y + sgn[s] * u.y);
       }
     }
 #pragma unroll
