@@ -45,18 +45,6 @@ struct NlAtoms {
   const int* pcount;   // [ntyp][nkf]
 };
 
-// The B-spline factors of one (atom, plane) entry of a plane's atom list,
-// staged in shared memory once per NL plane block (they do not depend on the
-// state): the a and b factors and their derivatives, the c factor of this
-// plane, the grid columns and rows.
-struct NlStage {
-  double ma[kNlInterp], mb[kNlInterp], da[kNlInterp], db[kNlInterp];
-  double mc, dc;
-  int ia[kNlInterp], ib[kNlInterp];
-  int atom, jc;
-};
-constexpr int kNlStageCap = 64;  // entries staged per plane; the rest read global memory
-
 // One channel's NL pass on the NL grid: geometry, pencils, twiddles, atoms.
 struct NlJob {
   FftJob f;

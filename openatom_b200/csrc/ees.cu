@@ -250,9 +250,7 @@ int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, 
     cpstep_set_error("set_nonlocal: NL grid size %d not built into libcpstep", nkf);
     return CPSTEP_ERR_ARG;
   }
-  // dynamic plane buffers plus the kernels' static stencil stage and row flags
-  const size_t nl_static = sizeof(NlStage) * kNlStageCap + sizeof(int) * nkf;
-  if (ops.nl_smem(c->nplane_x) + nl_static > 227 * 1024) {
+  if (ops.nl_smem(c->nplane_x) > 227 * 1024) {
     cpstep_set_error("set_nonlocal: NL plane of %d x %d does not fit shared memory in this "
                      "precision", nkf, nkf);
     return CPSTEP_ERR_ARG;

@@ -782,46 +782,6 @@ __device__ __forceinline__ void nl_point(const NlAtoms& A, int a, int ja, int jb
   dz = at * h[6] + bt * h[7] + ct * h[8];
 }
 
-// Staging of a plane's atom entries (NlStage) and the products from them;
-// nl_point_s forms the same products as nl_point.
-
-__device__ __forceinline__ void nl_stage_fill(const NlAtoms& A, const int* pl, int n,
-                                              NlStage* st) {
-  for (int i = threadIdx.x; i < n * kNlInterp; i += blockDim.x) {
-    const int e = i / kNlInterp, j = i - e * kNlInterp;
-    const int a = pl[e] & 0xffff, jc = pl[e] >> 16;
-    const double* m = A.mn + (size_t)a * 3 * kNlInterp;
-    const double* d = A.dmn + (size_t)a * 3 * kNlInterp;
-    const int* ig = A.ig + (size_t)a * 3 * kNlInterp;
-    NlStage& t = st[e];
-    t.ma[j] = m[j];
-    t.mb[j] = m[kNlInterp + j];
-    t.da[j] = d[j];
-    t.db[j] = d[kNlInterp + j];
-    t.ia[j] = ig[j];
-    t.ib[j] = ig[kNlInterp + j];
-    if (j == 0) {
-      t.mc = m[2 * kNlInterp + jc];
-      t.dc = d[2 * kNlInterp + jc];
-      t.atom = a;
-      t.jc = jc;
-    }
-  }
-}
-
-__device__ __forceinline__ void nl_point_s(const NlStage& t, const NlAtoms& A, int ja, int jb,
-                                           double& mn, double& dx, double& dy, double& dz) {
-  const double ma = t.ma[ja], mb = t.mb[jb], mc = t.mc;
-  const double at = t.da[ja] * mb * mc * A.grid;
-  const double bt = ma * t.db[jb] * mc * A.grid;
-  const double ct = ma * mb * t.dc * A.grid;
-  mn = ma * mb * mc;
-  const double* h = A.hmati;
-  dx = at * h[0] + bt * h[1] + ct * h[2];
-  dy = at * h[3] + bt * h[4] + ct * h[5];
-  dz = at * h[6] + bt * h[7] + ct * h[8];
-}
-
 // NL G->R (doNlFFTGtoR_Gchare/Rchare, fftCache.C:589-809) of plane z for the
 // block's states s0..s1, then for every atom of type ctype with an
 // interpolation plane jc on z: zpart[s][atom][jc] = (sum P mn, sum P dmn_x,
@@ -854,9 +814,6 @@ k_nl_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict
     const int e = i / kNlInterp, jb = i - e * kNlInterp;
     pairs[A.ig[(size_t)(pl[e] & 0xffff) * 3 * kNlInterp + kNlInterp + jb] >> 1] = 1;
   }
-  __shared__ NlStage st[kNlStageCap];
-  const int nst = min(npl, kNlStageCap);
-  nl_stage_fill(A, pl, nst, st);
   __syncthreads();
   ShflFft<T, N> F;
   if constexpr (ShflCfg<N>::ok) F.init(tw);
@@ -921,14 +878,9 @@ k_nl_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int jb = jb0 + 4 * h;
-        double mn, dx, dy, dz, pz;
-        if (e < nst) {
-          pz = (double)R[(size_t)st[e].ib[jb] * N + st[e].ia[ja]];
-          nl_point_s(st[e], A, ja, jb, mn, dx, dy, dz);
-        } else {
-          pz = (double)R[(size_t)ig[kNlInterp + jb] * N + ig[ja]];
-          nl_point(A, a, ja, jb, jc, mn, dx, dy, dz);
-        }
+        const double pz = (double)R[(size_t)ig[kNlInterp + jb] * N + ig[ja]];
+        double mn, dx, dy, dz;
+        nl_point(A, a, ja, jb, jc, mn, dx, dy, dz);
         sz += pz * mn;
         sx += pz * dx;
         sy += pz * dy;
@@ -980,9 +932,6 @@ k_nl_bwd(cplx<T>* __restrict__ pen_out, StateGeom g, const cplx<T>* __restrict__
     const int e = i / kNlInterp, jb = i - e * kNlInterp;
     pairs[A.ig[(size_t)(pl[e] & 0xffff) * 3 * kNlInterp + kNlInterp + jb] >> 1] = 1;
   }
-  __shared__ NlStage st[kNlStageCap];
-  const int nst = min(npl, kNlStageCap);
-  nl_stage_fill(A, pl, nst, st);
   __syncthreads();
   ShflFft<T, N> F;
   if constexpr (ShflCfg<N>::ok) F.init(tw);
@@ -990,28 +939,18 @@ k_nl_bwd(cplx<T>* __restrict__ pen_out, StateGeom g, const cplx<T>* __restrict__
     for (int i = threadIdx.x; i < N * N; i += NLTHREADS) R[i] = (T)0;
     for (int i = threadIdx.x; i < g.nplane_x * LDY; i += NLTHREADS) plane[i] = mk<T>(0, 0);
     __syncthreads();
-    // scatter: warp w owns the rows y with y % NW == w, lanes 0..7 the eight
-    // columns of a stencil row; every cell adds its atoms in list order
-    for (int e = 0; e < npl; ++e) {
-      const bool staged = e < nst;
-      const int a = staged ? st[e].atom : (pl[e] & 0xffff);
-      const int jc = staged ? st[e].jc : (pl[e] >> 16);
-      const int* ig = A.ig + (size_t)a * 3 * kNlInterp;
-      const double za = zs[(size_t)s * A.natm + a];
-      for (int jb = 0; jb < kNlInterp; ++jb) {
-        const int y = staged ? st[e].ib[jb] : ig[kNlInterp + jb];
-        if (y % NW != warp) continue;  // uniform in the warp
-        if (lane < kNlInterp) {
+    if (warp == 0) {
+      const int ja = lane & 7, jb0 = lane >> 3;
+      for (int e = 0; e < npl; ++e) {
+        const int a = pl[e] & 0xffff, jc = pl[e] >> 16;
+        const int* ig = A.ig + (size_t)a * 3 * kNlInterp;
+        const double za = zs[(size_t)s * A.natm + a];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int jb = jb0 + 4 * h;
           double mn, dx, dy, dz;
-          int x;
-          if (staged) {
-            nl_point_s(st[e], A, lane, jb, mn, dx, dy, dz);
-            x = st[e].ia[lane];
-          } else {
-            nl_point(A, a, lane, jb, jc, mn, dx, dy, dz);
-            x = ig[lane];
-          }
-          T* r = R + (size_t)y * N + x;
+          nl_point(A, a, ja, jb, jc, mn, dx, dy, dz);
+          T* r = R + (size_t)ig[kNlInterp + jb] * N + ig[ja];
           *r = (T)((double)*r + za * mn);
         }
         __syncwarp();
