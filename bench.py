@@ -214,7 +214,8 @@ def run_ours(args, cfg, name, rank, ws, dist):
         # accuracy: first step from the same input, mixed vs FP64
         ctx.cp_step(psi, v, occ, DT, 1, energies, forces)
         it, ok = ctx.step_status()
-        first = (energies.cpu().numpy().copy(), forces.cpu().numpy().copy(), ok, it)
+        first = (energies.cpu().numpy().copy(), forces.cpu().numpy().copy(), ok, it,
+                 orthonormality(psi, sysm.layout))
         if prec == "fp64":
             e_ref, f_ref = first[0], first[1]
         clk = Clocks()
@@ -270,11 +271,47 @@ def run_ours(args, cfg, name, rank, ws, dist):
             e2e_ms = max_over_ranks((t1 - t0) * 1e3, dist)
             out["e2e"] = dict(ms=e2e_ms, h2d=pos.numel() * 8,
                               d2h=he.numel() * 8 + hf.numel() * 8)
+        if prec == "mixed":
+            out["pc_us"] = pc_kernel_times(ctx, psi, v)
         nl, _ = ctx.info()
         out.setdefault("nlines", nl)
         out.setdefault("npts_d", ctx.rho_layout()[0].shape[0])
         ctx.close()
     return sysm, out, e_ref, f_ref
+
+
+def orthonormality(psi, lay):
+    """max |psi^T psi / 2 - I| (the S of the packed half sphere, FP64)."""
+    import torch
+    w = torch.where(torch.from_numpy(lay.kx).to(psi.device) == 0, 1.0, 2.0).to(torch.float64)
+    re, im = psi.real.contiguous(), psi.imag.contiguous()
+    S = (re * w) @ re.T + (im * w) @ im.T
+    eye = torch.eye(S.shape[0], dtype=torch.float64, device=psi.device)
+    return float((S / 2 - eye).abs().max())
+
+
+def pc_kernel_times(ctx, psi, f, reps=5):
+    """Device time (us) of the PairCalc products of the context alone, outside
+    the timed step: S = psi^T psi, lambda = psi^T F, psi.T."""
+    import torch
+    S = psi.shape[0]
+    cS = torch.zeros((S, S), dtype=torch.float64, device=psi.device)
+    out = torch.empty_like(psi)
+    T = torch.eye(S, dtype=torch.float64, device=psi.device) * 1.0001
+    res = {}
+    for name, fn in (("S", lambda: ctx.pc_overlap(psi, psi, out=cS)),
+                     ("lambda", lambda: ctx.pc_overlap(psi, f, out=cS)),
+                     ("psiT", lambda: ctx.pc_backmultiply(T, psi, out=out))):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        res[name] = e0.elapsed_time(e1) / reps * 1e3
+    return res
 
 
 def cpu_baseline(cfg, sample_states=4):
@@ -335,6 +372,22 @@ def cpu_baseline(cfg, sample_states=4):
               % (sample_states, S, natm_s, sysm.natm))
     del A2
     return t_step, sample
+
+
+def pc_roofline(us, sysm, hbm, pk, gflops, gemm_ms):
+    """S = psi^T psi on the tensor cores: it must read psi once (16 B per
+    coefficient); the split products issue 6 BF16 MMAs per FP64 product."""
+    S, npw = sysm.nstates, sysm.layout.npts
+    t = us["S"] * 1e-6
+    byt = 16.0 * S * npw
+    bf16 = 6 * 2.0 * S * S * 2 * npw
+    peak_tc = pk.get("bf16_tflops") if pk else None
+    return {"bound": "hbm", "kernel": "k_pc_tc overlap S = psi^T psi (split BF16, tcgen05)",
+            "achieved": byt / t / 1e9, "peak": hbm, "unit": "GB/s", "frac": byt / t / 1e9 / hbm,
+            "algorithmic_bytes": byt, "bf16_tflops": bf16 / t / 1e12,
+            "bf16_frac": (bf16 / t / 1e12 / peak_tc) if peak_tc else None,
+            "kernel_us": us, "phases_tflops_fp64_equiv": gflops / (gemm_ms * 1e-3) / 1e12
+            if gemm_ms > 0 else None}
 
 
 def kernel_case(args):
@@ -464,7 +517,8 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 FFT/density/V.psi, f64 accumulation, f64 GEMM/Ortho correction",
+        "dtype": "f32 FFT/density/V.psi with f64 rho/energy accumulation; PairCalc split-BF16 "
+                 "tensor-core products (FP32 accumulate, FP64 sums); Ortho f32 + f64 correction",
         "data": "synthetic",
         "config": {"workload": wname, "parallelism": "replicas" if ws > 1 else "1 GPU",
                    "inputs_vs_L2": "inputs larger than L2: psi %.1f MB FP64 per replica"
@@ -474,6 +528,8 @@ def main():
         "fp64_ms_per_step": fp64["ms"] / args.steps,
         "mixed_over_fp64": sps_mixed / sps_fp64,
         "accuracy_vs_fp64": {"energy_Ha_per_atom": err_e, "local_force_Ha_per_bohr": err_f,
+                             "orthonormality_mixed": mixed["first"][4],
+                             "orthonormality_fp64": fp64["first"][4],
                              "ortho_converged": bool(mixed["ortho_ok"])},
         "phase_ms_mixed": {"density": ph[0], "vks": ph[1], "vpsi_kinetic": ph[2],
                            "lambda": ph[3], "integrate": ph[4], "ortho_psiT": ph[5],
@@ -483,8 +539,7 @@ def main():
                      "frac": (achieved / hbm) if achieved else None, "traffic": None,
                      "algorithmic_bytes": ours_b, "survey_model_bytes": survey_b,
                      "peak_kind": peak_kind},
-        "roofline_paircalc": {"bound": "fp64", "flops": gflops,
-                              "achieved_tflops": gflops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None},
+        "roofline_paircalc": pc_roofline(out["pc_us"], sysm, hbm, pk, gflops, gemm_ms),
         "gpu_launches": int(mixed["launches"]),
         "clocks": mixed["clocks"],
         "e2e": {"value": ws * args.steps / (out["e2e"]["ms"] / 1e3), "unit": "steps/s",

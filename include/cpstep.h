@@ -203,6 +203,21 @@ CPSTEP_API int cpstep_eke(cpstep_ctx* ctx, double* d_force, const double* d_psi,
  * cpstep_dgemm: column-major BLAS DGEMM semantics on device pointers, the
  *   myGEMM wrapper (ckPairCalculator.C:57-66).
  */
+/*
+ * cpstep_set_gemm_path: on a CPSTEP_PREC_MIXED context the overlap and
+ *   back-multiply products run on the tensor cores (tensor_cores = 1, the
+ *   default on compute capability 10.x) as split-BF16 compensated products:
+ *   each FP64 element split into BF16 hi + lo, the three products
+ *   lo*hi + hi*lo + hi*hi accumulated in FP32 over chunks of 32 reals, the
+ *   chunks summed in FP64; the back-multiply adds the diagonal of M in FP64.
+ *   tensor_cores = 0 selects the FP64 products.  FP64 contexts always use
+ *   FP64.  No counterpart in the reference (its products are DGEMM calls).
+ * cpstep_device_errors: error bits recorded by kernels since the last call
+ *   (1: a bounded wait of a tensor-core product timed out and its tile was not
+ *   written); clears them.  Synchronises the context's stream.
+ */
+CPSTEP_API int cpstep_set_gemm_path(cpstep_ctx* ctx, int tensor_cores);
+CPSTEP_API int cpstep_device_errors(cpstep_ctx* ctx, int* flags);
 CPSTEP_API int cpstep_pc_overlap(cpstep_ctx* ctx, const double* d_a, const double* d_b,
                                  int na, int nb, double alpha, double beta, double* d_c,
                                  int ldc);

@@ -295,6 +295,16 @@ class StepContext:
                   int(iteration), ptr(e), ptr(f))
         return e, f
 
+    def set_gemm_path(self, tensor_cores):
+        """Mixed contexts: overlap / back-multiply on the tensor cores (split BF16) or in FP64."""
+        _lib.call("cpstep_set_gemm_path", self._h, 1 if tensor_cores else 0)
+
+    def device_errors(self):
+        """Error bits recorded by kernels since the last call (0: none); clears them."""
+        f = ctypes.c_int()
+        _lib.call("cpstep_device_errors", self._h, ctypes.byref(f))
+        return f.value
+
     def step_status(self):
         it, ok = ctypes.c_int(), ctypes.c_int()
         _lib.call("cpstep_step_status", self._h, ctypes.byref(it), ctypes.byref(ok))

@@ -237,6 +237,12 @@ int cpstep_ctx_create(cpstep_ctx** out, int precision, int nstates, int npts, co
   if (!rc) {
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
     if (c->num_sms <= 0) c->num_sms = 148;
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, c->device);
+    c->tc_ok = major == 10;
+    if (cudaMalloc(&c->d_dev_err, sizeof(int)) != cudaSuccess ||
+        cudaMemset(c->d_dev_err, 0, sizeof(int)) != cudaSuccess)
+      rc = CPSTEP_ERR_CUDA;
   }
   if (!rc) rc = upload(&c->d_line_off, off.data(), nl);
   if (!rc) rc = upload(&c->d_line_nneg, nneg.data(), nl);
@@ -267,6 +273,7 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
   cudaFree(c->d_kx); cudaFree(c->d_ky); cudaFree(c->d_kz);
   cudaFree(c->d_g2); cudaFree(c->d_wpt);
   cudaFree(c->d_pc_part); cudaFree(c->d_ortho_ws); cudaFree(c->d_hmati);
+  cudaFree(c->d_dev_err);
   cudaFree(c->d_force_atoms);
   for (auto& e : c->prof_ev) cudaEventDestroy(e);
   nl_free(c);
@@ -503,6 +510,30 @@ int cpstep_cp_step_host(cpstep_ctx* c, double* d_psi, double* d_vpsi, const doub
     CPSTEP_CUDA_TRY(cudaMemcpyAsync(h_atom_force, c->d_force_atoms,
                                     sizeof(double) * 3 * c->atoms.natm, cudaMemcpyDeviceToHost,
                                     c->stream));
+  CPSTEP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CPSTEP_OK;
+}
+
+int cpstep_set_gemm_path(cpstep_ctx* c, int tensor_cores) {
+  if (!c || (tensor_cores != 0 && tensor_cores != 1)) return CPSTEP_ERR_ARG;
+  if (tensor_cores) {
+    int major = 0;
+    CPSTEP_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, c->device));
+    if (major != 10) {
+      cpstep_set_error("set_gemm_path: tensor-core products need compute capability 10.x");
+      return CPSTEP_ERR_ARG;
+    }
+  }
+  c->tc_ok = tensor_cores;
+  return CPSTEP_OK;
+}
+
+int cpstep_device_errors(cpstep_ctx* c, int* flags) {
+  if (!c || !flags) return CPSTEP_ERR_ARG;
+  *flags = 0;
+  CPSTEP_CUDA_TRY(cudaMemcpyAsync(flags, c->d_dev_err, sizeof(int), cudaMemcpyDeviceToHost,
+                                  c->stream));
+  CPSTEP_CUDA_TRY(cudaMemsetAsync(c->d_dev_err, 0, sizeof(int), c->stream));
   CPSTEP_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return CPSTEP_OK;
 }

@@ -199,6 +199,10 @@ struct cpstep_ctx {
   double* d_ortho_ws = nullptr;
   size_t ortho_ws_elems = 0;
   int* d_ortho_status = nullptr;  // [iterations, converged] of the last Ortho launch
+  // tensor-core PairCalc products (mixed precision on sm_100): on by default
+  // where the device is compute capability 10.x; cpstep_set_gemm_path
+  int tc_ok = 0;
+  int* d_dev_err = nullptr;  // error bits set by kernels (bounded waits that timed out)
 
   FftJob state_job() const {
     FftJob j;
@@ -257,6 +261,17 @@ int pc_overlap_launch(cpstep_ctx* c, const double* a, const double* b, int M, in
                       const double* w, double alpha, double beta, double* C, int ldc);
 int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
                       double* out, int ldo, int nout, int nin, int K, double alpha, double beta);
+int pc_part_reserve(cpstep_ctx* c, size_t elems);
+int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
+                            double* C, int ldc, int sym);
+// paircalc_tc.cu (tensor-core products; *used = false when the SIMT path must run)
+bool pc_tc_usable(const cpstep_ctx* c);
+int pc_overlap_tc_launch(cpstep_ctx* c, const double* a, const double* b, int M, int N, int K,
+                         const double* w, double alpha, double beta, double* C, int ldc,
+                         bool* used);
+int pc_backmul_tc_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
+                         double* out, int ldo, int nout, int nin, int K, double alpha,
+                         double beta, const double* w, bool* used);
 int dgemm_launch(cudaStream_t s, int ta, int tb, int m, int n, int k, double alpha,
                  const double* A, int lda, const double* B, int ldb, double beta, double* C,
                  int ldc);

@@ -1,4 +1,5 @@
-// PairCalculator products (SIMT path).
+// PairCalculator products (FP64 SIMT path; the mixed-precision context sends
+// them to the tensor-core kernels of paircalc_tc.cu where those apply).
 //
 //   overlap:      C(i,j) = alpha * sum_p wpt_p Re(conj a_i(p) b_j(p)) (+ beta C)
 //                 = the reference's 2 * psi_r^T psi_r with Gx=0 rows scaled by
@@ -76,13 +77,26 @@ k_overlap_part(const double* __restrict__ A, int lda, const double* __restrict__
     }
 }
 
+// sym (M == N): C = alpha (P + P^T) / 2 + beta C, summed in the same order for
+// (i,j) and (j,i) so the result is exactly symmetric.
 __global__ void k_splitk_reduce(const double* __restrict__ part, int nsplit, int M, int N,
-                                double alpha, double beta, double* __restrict__ C, int ldc) {
+                                double alpha, double beta, double* __restrict__ C, int ldc,
+                                int sym) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= M * N) return;
   int j = e / M, i = e - j * M;
   double s = 0.0;
-  for (int k = 0; k < nsplit; ++k) s += part[(size_t)k * M * N + e];
+  if (sym) {
+    const size_t e1 = (size_t)min(i, j) * M + max(i, j), e2 = (size_t)max(i, j) * M + min(i, j);
+    double s1 = 0.0, s2 = 0.0;
+    for (int k = 0; k < nsplit; ++k) {
+      s1 += part[(size_t)k * M * N + e1];
+      s2 += part[(size_t)k * M * N + e2];
+    }
+    s = 0.5 * (s1 + s2);
+  } else {
+    for (int k = 0; k < nsplit; ++k) s += part[(size_t)k * M * N + e];
+  }
   double* c = C + (size_t)j * ldc + i;
   *c = alpha * s + (beta == 0.0 ? 0.0 : beta * (*c));
 }
@@ -345,33 +359,51 @@ static int t128_attr() {
   return CPSTEP_OK;
 }
 
+int pc_part_reserve(cpstep_ctx* c, size_t need) {
+  if (need > c->pc_part_elems) {
+    cudaFree(c->d_pc_part);
+    c->d_pc_part = nullptr;
+    c->pc_part_elems = 0;
+    CPSTEP_CUDA_TRY(cudaMalloc(&c->d_pc_part, need * sizeof(double)));
+    c->pc_part_elems = need;
+  }
+  return CPSTEP_OK;
+}
+
+int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
+                            double* C, int ldc, int sym) {
+  pcalc::k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, c->stream>>>(c->d_pc_part, nsplit, M, N,
+                                                                   alpha, beta, C, ldc, sym);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
 int pc_overlap_launch(cpstep_ctx* c, const double* a, const double* b, int M, int N, int K,
                       const double* w, double alpha, double beta, double* C, int ldc) {
   using namespace pcalc;
+  bool used = false;
+  if (int rc = pc_overlap_tc_launch(c, a, b, M, N, K, w, alpha, beta, C, ldc, &used)) return rc;
+  if (used) return CPSTEP_OK;
   if (int rc = t128_attr()) return rc;
   int tm = cdiv(M, TB), tn = cdiv(N, TB);
   int want = std::max(1, c->num_sms / (tm * tn));
   int kslab = cdiv(cdiv(K, want), TK) * TK;
   int nsplit = cdiv(K, kslab);
-  size_t need = (size_t)nsplit * M * N;
-  if (need > c->pc_part_elems) {
-    cudaFree(c->d_pc_part);
-    c->d_pc_part = nullptr;
-    CPSTEP_CUDA_TRY(cudaMalloc(&c->d_pc_part, need * sizeof(double)));
-    c->pc_part_elems = need;
-  }
+  if (int rc = pc_part_reserve(c, (size_t)nsplit * M * N)) return rc;
   k_overlap_t128<<<dim3(tm, tn, nsplit), 256, T128_SMEM, c->stream>>>(a, K, b, K, w, M, N, K,
                                                                      kslab, c->d_pc_part);
   CPSTEP_LAUNCH_CHECK();
-  k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, c->stream>>>(c->d_pc_part, nsplit, M, N, alpha,
-                                                            beta, C, ldc);
-  CPSTEP_LAUNCH_CHECK();
-  return CPSTEP_OK;
+  return pc_splitk_reduce_launch(c, nsplit, M, N, alpha, beta, C, ldc, 0);
 }
 
 int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
                       double* out, int ldo, int nout, int nin, int K, double alpha, double beta) {
   using namespace pcalc;
+  bool used = false;
+  if (int rc = pc_backmul_tc_launch(c, Mcm, ldm, in, ldi, out, ldo, nout, nin, K, alpha, beta,
+                                    nullptr, &used))
+    return rc;
+  if (used) return CPSTEP_OK;
   if (int rc = t128_attr()) return rc;
   dim3 grid(cdiv(K, TB), cdiv(nout, TB));
   k_backmul_t128<<<grid, 256, T128_SMEM, c->stream>>>(Mcm, ldm, in, ldi, out, ldo, nout, nin, K,
@@ -384,6 +416,11 @@ int pc_backmul_w_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double*
                         double* out, int ldo, int nout, int nin, int K, double alpha, double beta,
                         const double* w) {
   using namespace pcalc;
+  bool used = false;
+  if (int rc = pc_backmul_tc_launch(c, Mcm, ldm, in, ldi, out, ldo, nout, nin, K, alpha, beta, w,
+                                    &used))
+    return rc;
+  if (used) return CPSTEP_OK;
   if (int rc = t128_attr()) return rc;
   dim3 grid(cdiv(K, TB), cdiv(nout, TB));
   k_backmul_t128<<<grid, 256, T128_SMEM, c->stream>>>(Mcm, ldm, in, ldi, out, ldo, nout, nin, K,
@@ -471,7 +508,7 @@ extern "C" int cpstep_pc_overlap_noalloc(const double* d_a, const double* d_b, i
   // every partial the reduction reads is written by this call: nothing to clear
   k_overlap_part<<<dim3(tm, tn, nsplit), NT, 0, s>>>(d_a, K, d_b, K, d_w, M, N, K, kslab, part);
   CPSTEP_LAUNCH_CHECK();
-  k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, s>>>(part, nsplit, M, N, alpha, beta, d_c, ldc);
+  k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, s>>>(part, nsplit, M, N, alpha, beta, d_c, ldc, 0);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }

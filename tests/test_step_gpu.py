@@ -36,11 +36,13 @@ def stepsys():
     return dict(sys=sysm, psi=psi, occ=occ, ref=[(p1, v1, en1, f1), (p2, v2, en2, f2)])
 
 
-def run(stepsys, precision):
+def run(stepsys, precision, tensor_cores=True):
     import torch
     from openatom_b200.context import StepContext
     s = stepsys["sys"]
     ctx = StepContext(s.layout, s.nstates, precision=precision)
+    if precision == "mixed" and not tensor_cores:
+        ctx.set_gemm_path(False)
     ctx.set_atoms(s)
     ctx.set_cp_mass(25.0, 30.0)
     psi = stepsys["psi"].clone()
@@ -78,5 +80,19 @@ def test_mixed_step_within_budget(stepsys):
         assert ok
         assert abs(e[8] - er["ETOT"]) / natm <= 1e-6
         assert np.max(np.abs(f - fr)) <= 1e-5
+        # the mixed step's S is a split-BF16 tensor-core product (FP32-level
+        # accuracy): the orthonormality it leaves is at that level, not FP64's
+        S = OO.pc_overlap(p, p, lay.kx)
+        assert np.max(np.abs(S - 2.0 * np.eye(S.shape[0]))) < 1e-6
+
+
+def test_mixed_step_fp64_products_orthonormal_to_fp64(stepsys):
+    """With the FP64 PairCalc products selected, the mixed step keeps S = 2 I
+    to FP64 rounding (the FP64 Ortho correction)."""
+    from oracle import ortho as OO
+    out = run(stepsys, "mixed", tensor_cores=False)
+    lay = stepsys["sys"].layout
+    for (p, v, e, f, ok), _ in zip(out, stepsys["ref"]):
+        assert ok
         S = OO.pc_overlap(p, p, lay.kx)
         assert np.max(np.abs(S - 2.0 * np.eye(S.shape[0]))) < 1e-10
