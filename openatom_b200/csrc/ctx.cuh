@@ -31,6 +31,11 @@ struct FftJob {
 // d = a, b, c and interpolation point j < 8; eesAtmBsplineRgrp,
 // cp_ees_nonlocal.C:256-580) as the NL plane kernels read them.
 constexpr int kNlInterp = 8;
+// Mn and its gradient at one stencil point of one atom (see nl_point).
+struct __align__(16) NlVal {
+  double mn, dx, dy, dz;
+};
+
 struct NlAtoms {
   int natm;
   const int* typ;      // [natm]
@@ -43,7 +48,36 @@ struct NlAtoms {
   // atom | (jc << 16) in atom order, and their count
   const int* plist;    // [ntyp][nkf][natm]
   const int* pcount;   // [ntyp][nkf]
+  // per-plane stencil tables of the channel's type (k_nl_table), tcap entries
+  // per plane: entry e*64 + q is point q = jb*8 + ja of atom slot e of plist:
+  // its plane cell tcell (y*N + x) and tval (Mn, dMn/dx, dMn/dy, dMn/dz as in
+  // nl_point); the gather list: the gcount touched cells gcell in increasing
+  // order, their entries gent[goff[c] .. goff[c+1]) in atom-slot order
+  int tcap;
+  const int* tcell;          // [nkf][tcap]
+  const NlVal* tval;         // [nkf][tcap]
+  const int* gcell;          // [nkf][tcap]
+  const int* goff;           // [nkf][tcap + 1]
+  const int* gent;           // [nkf][tcap]
+  const int* gcount;         // [nkf]
 };
+
+// The B-spline product of one stencil point, in the reference's order
+// (eesAtmBsplineRgrp IV, cp_ees_nonlocal.C:523-532): mn and dmn_{x,y,z}.
+__device__ __forceinline__ void nl_point(const NlAtoms& A, int a, int ja, int jb, int jc,
+                                         double& mn, double& dx, double& dy, double& dz) {
+  const double* m = A.mn + (size_t)a * 3 * kNlInterp;
+  const double* d = A.dmn + (size_t)a * 3 * kNlInterp;
+  const double ma = m[ja], mb = m[kNlInterp + jb], mc = m[2 * kNlInterp + jc];
+  const double at = d[ja] * mb * mc * A.grid;
+  const double bt = ma * d[kNlInterp + jb] * mc * A.grid;
+  const double ct = ma * mb * d[2 * kNlInterp + jc] * A.grid;
+  mn = ma * mb * mc;
+  const double* h = A.hmati;
+  dx = at * h[0] + bt * h[1] + ct * h[2];
+  dy = at * h[3] + bt * h[4] + ct * h[5];
+  dz = at * h[6] + bt * h[7] + ct * h[8];
+}
 
 // One channel's NL pass on the NL grid: geometry, pencils, twiddles, atoms.
 struct NlJob {
@@ -121,6 +155,12 @@ struct NlData {
   double* enl_s = nullptr;          // [nstates]
   double* fnl = nullptr;            // [nstates][natm][3]
   int natm = 0;
+  // stencil tables (NlAtoms), one block per type: type t starts at entry
+  // tab_off[t] (nkf * tab_cap[t] entries), tab_cap[t] = 64 * atoms of type t
+  int *tcell = nullptr, *gcell = nullptr, *goff = nullptr, *gent = nullptr, *gcount = nullptr;
+  NlVal* tval = nullptr;
+  std::vector<size_t> tab_off;
+  std::vector<int> tab_cap;
 };
 
 template <typename T>

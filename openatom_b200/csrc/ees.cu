@@ -104,6 +104,105 @@ __global__ void k_nl_planes(const int* __restrict__ typ, const int* __restrict__
   if (lane == 0) pcount[i] = n;
 }
 
+// Stencil tables of one (type, plane) (NlAtoms): for every atom slot e of the
+// plane's list and point q = jb*8 + ja, its cell and nl_point's products;
+// then the gather list that lets the R->G kernel form each touched cell's
+// sum of Z Mn with one thread per cell, adding the atoms in list order as a
+// serial scatter would.  One block per (plane, type); shared memory: two ints
+// per plane cell (counts, then fill cursors).
+constexpr int TABTHREADS = 256;
+}  // namespace ees
+constexpr int kNlGridMax = 160;
+namespace ees {
+struct TabDims {
+  int cap[CPSTEP_MAX_TYPES];
+  long long off[CPSTEP_MAX_TYPES];
+};
+__global__ void __launch_bounds__(TABTHREADS)
+k_nl_table(NlAtoms A, int nkf, TabDims d, int* __restrict__ tcell, NlVal* __restrict__ tval,
+           int* __restrict__ gcell, int* __restrict__ goff, int* __restrict__ gent,
+           int* __restrict__ gcount) {
+  extern __shared__ int tab_smem[];
+  const int z = blockIdx.x, t = blockIdx.y;
+  const int ncell = nkf * nkf;
+  int* cnt = tab_smem;           // [ncell]
+  int* cur = tab_smem + ncell;   // [ncell]
+  const int cap = d.cap[t];
+  const size_t base = (size_t)d.off[t] + (size_t)z * cap;
+  const size_t gbase = (size_t)d.off[t] + (size_t)t * nkf + (size_t)z * (cap + 1);
+  const int* pl = A.plist + ((size_t)t * nkf + z) * A.natm;
+  const int npl = A.pcount[t * nkf + z];
+  for (int i = threadIdx.x; i < ncell; i += TABTHREADS) cnt[i] = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < npl * 64; i += TABTHREADS) {
+    const int e = i >> 6, q = i & 63, ja = q & 7, jb = q >> 3;
+    const int a = pl[e] & 0xffff, jc = pl[e] >> 16;
+    const int* ig = A.ig + (size_t)a * 3 * kNlInterp;
+    const int cell = ig[kNlInterp + jb] * nkf + ig[ja];
+    NlVal v;
+    nl_point(A, a, ja, jb, jc, v.mn, v.dx, v.dy, v.dz);
+    tcell[base + i] = cell;
+    tval[base + i] = v;
+    atomicAdd(&cnt[cell], 1);
+  }
+  __syncthreads();
+  // compact the touched cells in increasing order: each thread a contiguous
+  // range of cells, then a block scan of (touched cells, entries)
+  __shared__ int wsum_c[TABTHREADS / 32], wsum_e[TABTHREADS / 32];
+  const int per = (ncell + TABTHREADS - 1) / TABTHREADS;
+  const int c0 = threadIdx.x * per, c1 = min(ncell, c0 + per);
+  int nc = 0, ne = 0;
+  for (int c = c0; c < c1; ++c) {
+    nc += cnt[c] > 0;
+    ne += cnt[c];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int ic = nc, ie = ne;  // inclusive warp scans
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int uc = __shfl_up_sync(0xffffffffu, ic, o), ue = __shfl_up_sync(0xffffffffu, ie, o);
+    if (lane >= o) {
+      ic += uc;
+      ie += ue;
+    }
+  }
+  if (lane == 31) {
+    wsum_c[warp] = ic;
+    wsum_e[warp] = ie;
+  }
+  __syncthreads();
+  int pc = ic - nc, pe = ie - ne;  // exclusive within the warp
+  for (int w = 0; w < warp; ++w) {
+    pc += wsum_c[w];
+    pe += wsum_e[w];
+  }
+  for (int c = c0; c < c1; ++c) {
+    const int k = cnt[c];
+    if (k > 0) {
+      gcell[base + pc] = c;
+      goff[gbase + pc] = pe;
+      cur[c] = pe;
+      ++pc;
+      pe += k;
+    }
+  }
+  if (threadIdx.x == TABTHREADS - 1) {
+    gcount[t * nkf + z] = pc;
+    goff[gbase + pc] = pe;  // = npl * 64
+  }
+  __syncthreads();
+  // entries in atom-slot order: an atom's 64 cells are distinct
+  for (int e = 0; e < npl; ++e) {
+    if (threadIdx.x < 64) {
+      const int i = e * 64 + threadIdx.x;
+      const int cell = tcell[base + i];
+      gent[base + cur[cell]] = i;
+      cur[cell] += 1;
+    }
+    __syncthreads();
+  }
+}
+
 // Z_a = sum over the atom's planes, E_NL += Z^2 vn occ, Z <- 2 vn occ Z,
 // F_a -= Z sum P dMn (eesEnergyAtmForcRchare :1545-1560, :1596-1600).
 // One block per state; atoms of the channel's type.
@@ -213,6 +312,8 @@ void nl_free(cpstep_ctx* c) {
   cudaFree(n.dyp); cudaFree(n.line_zneg); cudaFree(n.line_zpos); cudaFree(n.line_xy);
   cudaFree(n.pen_a); cudaFree(n.pen_b); cudaFree(n.tw); cudaFree(n.ig); cudaFree(n.mn);
   cudaFree(n.dmn); cudaFree(n.zpart); cudaFree(n.zs); cudaFree(n.enl_s); cudaFree(n.fnl);
+  cudaFree(n.tcell); cudaFree(n.tval); cudaFree(n.gcell); cudaFree(n.goff); cudaFree(n.gent);
+  cudaFree(n.gcount);
   cudaFree(n.plist); cudaFree(n.pcount);
   n = NlData();
 }
@@ -226,6 +327,10 @@ int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, 
   }
   if (n_interp != kNlInterp || nkf < n_interp || nchan <= 0) {
     cpstep_set_error("set_nonlocal: n_interp must be %d, nkf >= n_interp, nchan > 0", kNlInterp);
+    return CPSTEP_ERR_ARG;
+  }
+  if (nkf > kNlGridMax) {  // the stencil-table kernel keeps two ints per plane cell in shared memory
+    cpstep_set_error("set_nonlocal: NL grid %d above %d", nkf, kNlGridMax);
     return CPSTEP_ERR_ARG;
   }
   for (int k = 0; k < nchan; ++k) {
@@ -367,6 +472,22 @@ int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, 
   CPSTEP_CUDA_TRY(cudaMalloc(&n.zs, sizeof(double) * c->nstates * na));
   CPSTEP_CUDA_TRY(cudaMalloc(&n.enl_s, sizeof(double) * c->nstates));
   CPSTEP_CUDA_TRY(cudaMalloc(&n.fnl, sizeof(double) * c->nstates * na * 3));
+  // stencil tables: 64 entries per atom of the type on each plane at most
+  n.tab_cap.assign(at.ntyp, 0);
+  n.tab_off.assign(at.ntyp, 0);
+  size_t tot = 0;
+  for (int t = 0; t < at.ntyp; ++t) {
+    n.tab_off[t] = tot;
+    n.tab_cap[t] = 64 * (at.tstart[t + 1] - at.tstart[t]);
+    tot += (size_t)nkf * n.tab_cap[t];
+  }
+  const size_t tot1 = std::max<size_t>(tot, 1);
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.tcell, sizeof(int) * tot1));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.tval, sizeof(NlVal) * tot1));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.gcell, sizeof(int) * tot1));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.gent, sizeof(int) * tot1));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.goff, sizeof(int) * (tot + (size_t)at.ntyp * nkf)));
+  CPSTEP_CUDA_TRY(cudaMalloc(&n.gcount, sizeof(int) * (size_t)at.ntyp * nkf));
   n.on = 1;
   return CPSTEP_OK;
 }
@@ -410,9 +531,30 @@ int nl_run(cpstep_ctx* c, const double* psi, const double* occ, double* fpsi, do
   j.A.grid = (double)n.nkf;
   j.A.plist = n.plist;
   j.A.pcount = n.pcount;
+  {
+    ees::TabDims d{};
+    for (int t = 0; t < ntyp; ++t) {
+      d.cap[t] = n.tab_cap[t];
+      d.off[t] = (long long)n.tab_off[t];
+    }
+    const int tsm = (int)(2 * sizeof(int) * (size_t)n.nkf * n.nkf);
+    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(ees::k_nl_table,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, tsm));
+    ees::k_nl_table<<<dim3(n.nkf, ntyp), ees::TABTHREADS, tsm, c->stream>>>(
+        j.A, n.nkf, d, n.tcell, n.tval, n.gcell, n.goff, n.gent, n.gcount);
+    CPSTEP_LAUNCH_CHECK();
+  }
   const int zt = std::min(1024, std::max(32, cdiv(natm, 32) * 32));
   for (int k = 0; k < n.nchan; ++k) {
     j.ctype = n.ch_type[k];
+    const int t = j.ctype;
+    j.A.tcap = n.tab_cap[t];
+    j.A.tcell = n.tcell + n.tab_off[t];
+    j.A.tval = n.tval + n.tab_off[t];
+    j.A.gcell = n.gcell + n.tab_off[t];
+    j.A.gent = n.gent + n.tab_off[t];
+    j.A.goff = n.goff + n.tab_off[t] + (size_t)t * n.nkf;
+    j.A.gcount = n.gcount + (size_t)t * n.nkf;
     const double2* dyp = n.dyp + (size_t)k * c->npts;
     int rc;
     if ((rc = n.ops.nl_proj(c, j, psi, dyp, S, n.zpart))) return rc;

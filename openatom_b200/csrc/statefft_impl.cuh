@@ -765,23 +765,6 @@ struct NlShape {
   }
 };
 
-// The B-spline product of one stencil point, in the reference's order
-// (eesAtmBsplineRgrp IV, cp_ees_nonlocal.C:523-532): mn and dmn_{x,y,z}.
-__device__ __forceinline__ void nl_point(const NlAtoms& A, int a, int ja, int jb, int jc,
-                                         double& mn, double& dx, double& dy, double& dz) {
-  const double* m = A.mn + (size_t)a * 3 * kNlInterp;
-  const double* d = A.dmn + (size_t)a * 3 * kNlInterp;
-  const double ma = m[ja], mb = m[kNlInterp + jb], mc = m[2 * kNlInterp + jc];
-  const double at = d[ja] * mb * mc * A.grid;
-  const double bt = ma * d[kNlInterp + jb] * mc * A.grid;
-  const double ct = ma * mb * d[2 * kNlInterp + jc] * A.grid;
-  mn = ma * mb * mc;
-  const double* h = A.hmati;
-  dx = at * h[0] + bt * h[1] + ct * h[2];
-  dy = at * h[3] + bt * h[4] + ct * h[5];
-  dz = at * h[6] + bt * h[7] + ct * h[8];
-}
-
 // NL G->R (doNlFFTGtoR_Gchare/Rchare, fftCache.C:589-809) of plane z for the
 // block's states s0..s1, then for every atom of type ctype with an
 // interpolation plane jc on z: zpart[s][atom][jc] = (sum P mn, sum P dmn_x,
@@ -805,7 +788,8 @@ k_nl_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict
   for (int i = threadIdx.x; i < N; i += NLTHREADS) tw[i] = twx_g[i];
   const int* pl = A.plist + ((size_t)ctype * (int)A.grid + z) * A.natm;
   const int npl = A.pcount[ctype * (int)A.grid + z];
-  const int ja = lane & 7, jb0 = lane >> 3;
+  const int* tcell = A.tcell + (size_t)z * A.tcap;
+  const NlVal* tval = A.tval + (size_t)z * A.tcap;
   // row pairs that some atom's stencil reads (the others are not transformed)
   __shared__ int pairs[N / 2];
   for (int i = threadIdx.x; i < N / 2; i += NLTHREADS) pairs[i] = 0;
@@ -870,21 +854,20 @@ k_nl_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict
     }
     __syncthreads();
     }
-    // atoms on this plane: lane -> (jb, ja) = (lane / 8 + 4 h, lane % 8), h = 0, 1
+    // atoms on this plane: lane -> point q = lane + 32 h, (jb, ja) = (q / 8, q % 8),
+    // cells and Mn products from the plane's stencil table
     for (int e = warp; e < npl; e += NW) {
       const int a = pl[e] & 0xffff, jc = pl[e] >> 16;
-      const int* ig = A.ig + (size_t)a * 3 * kNlInterp;
       double sz = 0.0, sx = 0.0, sy = 0.0, sw = 0.0;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int jb = jb0 + 4 * h;
-        const double pz = (double)R[(size_t)ig[kNlInterp + jb] * N + ig[ja]];
-        double mn, dx, dy, dz;
-        nl_point(A, a, ja, jb, jc, mn, dx, dy, dz);
-        sz += pz * mn;
-        sx += pz * dx;
-        sy += pz * dy;
-        sw += pz * dz;
+        const int i = e * 64 + lane + 32 * h;
+        const double pz = (double)R[tcell[i]];
+        const NlVal v = tval[i];
+        sz += pz * v.mn;
+        sx += pz * v.dx;
+        sy += pz * v.dy;
+        sw += pz * v.dz;
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
@@ -904,9 +887,9 @@ k_nl_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict
 
 // NL R->G of plane z for the block's states: the plane holds sum_atoms
 // zs[s][atom] Mn over the atoms of type ctype (the projPsiRScr scatter of
-// eesEnergyAtmForcRchare, applied by one warp atom after atom so the sum order
-// is fixed), then x R2C, imag flip, y-FFT (doNlFFTRtoG_Rchare,
-// fftCache.C:634-699) into pencils.
+// eesEnergyAtmForcRchare, formed per touched cell from the plane's gather
+// list, atoms in list order, so the sum order is fixed), then x R2C, imag
+// flip, y-FFT (doNlFFTRtoG_Rchare, fftCache.C:634-699) into pencils.
 template <typename T, int N>
 __global__ void __launch_bounds__(NLTHREADS, 2)
 k_nl_bwd(cplx<T>* __restrict__ pen_out, StateGeom g, const cplx<T>* __restrict__ twx_g,
@@ -935,26 +918,33 @@ k_nl_bwd(cplx<T>* __restrict__ pen_out, StateGeom g, const cplx<T>* __restrict__
   __syncthreads();
   ShflFft<T, N> F;
   if constexpr (ShflCfg<N>::ok) F.init(tw);
-  for (int s = s0; s < s1; ++s) {
+  const int ncell = A.gcount[z];
+  const int* gcell = A.gcell + (size_t)z * A.tcap;
+  const int* goff = A.goff + (size_t)z * (A.tcap + 1);
+  const int* gent = A.gent + (size_t)z * A.tcap;
+  const NlVal* tval = A.tval + (size_t)z * A.tcap;
+  // the shuffle row transforms only read R, so the untouched cells stay zero
+  // for every state; the shared-memory line FFT works in place in R
+  constexpr bool RKEEP = ShflCfg<N>::ok;
+  if (RKEEP) {
     for (int i = threadIdx.x; i < N * N; i += NLTHREADS) R[i] = (T)0;
+  }
+  for (int s = s0; s < s1; ++s) {
+    if (!RKEEP) {
+      for (int i = threadIdx.x; i < N * N; i += NLTHREADS) R[i] = (T)0;
+    }
     for (int i = threadIdx.x; i < g.nplane_x * LDY; i += NLTHREADS) plane[i] = mk<T>(0, 0);
     __syncthreads();
-    if (warp == 0) {
-      const int ja = lane & 7, jb0 = lane >> 3;
-      for (int e = 0; e < npl; ++e) {
-        const int a = pl[e] & 0xffff, jc = pl[e] >> 16;
-        const int* ig = A.ig + (size_t)a * 3 * kNlInterp;
-        const double za = zs[(size_t)s * A.natm + a];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int jb = jb0 + 4 * h;
-          double mn, dx, dy, dz;
-          nl_point(A, a, ja, jb, jc, mn, dx, dy, dz);
-          T* r = R + (size_t)ig[kNlInterp + jb] * N + ig[ja];
-          *r = (T)((double)*r + za * mn);
-        }
-        __syncwarp();
+    // each touched cell: sum over its atoms in list order of Z Mn (the order a
+    // serial scatter atom after atom would add them)
+    const double* zss = zs + (size_t)s * A.natm;
+    for (int c = threadIdx.x; c < ncell; c += NLTHREADS) {
+      double v = 0.0;
+      for (int k = goff[c]; k < goff[c + 1]; ++k) {
+        const int i = gent[k];
+        v += zss[pl[i >> 6] & 0xffff] * tval[i].mn;
       }
+      R[gcell[c]] = (T)v;
     }
     __syncthreads();
     if constexpr (ShflCfg<N>::ok) {
