@@ -225,8 +225,6 @@ def run_ours(args, cfg, name, rank, ws, dist):
             ctx.cp_step(psi, v, occ, DT, 2 + w, energies, forces)
         torch.cuda.synchronize()
         ctx_prof = prec == "mixed"
-        if ctx_prof:
-            _lib.call("cpstep_ctx_profile", ctx._h, 1)
         clk.ready()
         barrier(dist)
         torch.cuda.synchronize()
@@ -243,9 +241,14 @@ def run_ours(args, cfg, name, rank, ws, dist):
         ms = e0.elapsed_time(e1)
         ms = max_over_ranks(ms, dist)
         barrier(dist)
+        graph = ctx.graph_status()
         phase = None
         if ctx_prof:
+            # phase breakdown: a separate profiled run (profiled steps run without the graph)
             import ctypes
+            _lib.call("cpstep_ctx_profile", ctx._h, 1)
+            for k in range(max(3, args.steps // 2)):
+                ctx.cp_step(psi, v, occ, DT, 2 + args.warmup + args.steps + k, energies, forces)
             arr = (ctypes.c_double * 7)()
             nst = ctypes.c_int()
             _lib.call("cpstep_phase_times", ctx._h, arr, ctypes.byref(nst))
@@ -253,19 +256,25 @@ def run_ours(args, cfg, name, rank, ws, dist):
             _lib.call("cpstep_ctx_profile", ctx._h, 0)
         it2, ok2 = ctx.step_status()
         out[prec] = dict(ms=ms, launches=launches, clocks=clocks, phase=phase, first=first,
-                         ortho_ok=ok2, ortho_iters=it2)
+                         ortho_ok=ok2, ortho_iters=it2, graph=graph)
         if prec == "mixed":
             # e2e: the reference-facing host-buffer call (positions in, energies/forces out)
             import ctypes
             pos = torch.from_numpy(np.ascontiguousarray(sysm.pos)).pin_memory()
             he = torch.zeros(_lib.NENERGY, dtype=torch.float64).pin_memory()
             hf = torch.zeros((sysm.natm, 3), dtype=torch.float64).pin_memory()
+            it0 = 2 + args.warmup + 2 * args.steps + 3
+            for k in range(3):  # the host-buffer call's own direct step and graph capture
+                _lib.call("cpstep_cp_step_host", ctx._h, _lib.ptr(psi), _lib.ptr(v), _lib.ptr(occ),
+                          DT, it0 + k, ctypes.c_void_p(pos.data_ptr()),
+                          ctypes.c_void_p(he.data_ptr()), ctypes.c_void_p(hf.data_ptr()))
+            it0 += 3
             barrier(dist)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             for k in range(args.steps):
                 _lib.call("cpstep_cp_step_host", ctx._h, _lib.ptr(psi), _lib.ptr(v), _lib.ptr(occ),
-                          DT, 2 + args.warmup + args.steps + k, ctypes.c_void_p(pos.data_ptr()),
+                          DT, it0 + k, ctypes.c_void_p(pos.data_ptr()),
                           ctypes.c_void_p(he.data_ptr()), ctypes.c_void_p(hf.data_ptr()))
             t1 = time.perf_counter()
             e2e_ms = max_over_ranks((t1 - t0) * 1e3, dist)
@@ -541,6 +550,8 @@ def main():
                      "peak_kind": peak_kind},
         "roofline_paircalc": pc_roofline(out["pc_us"], sysm, hbm, pk, gflops, gemm_ms),
         "gpu_launches": int(mixed["launches"]),
+        "cuda_graph": {"mixed": mixed["graph"], "fp64": fp64["graph"],
+                       "fields": ["enabled", "captured", "kernels_per_step"]},
         "clocks": mixed["clocks"],
         "e2e": {"value": ws * args.steps / (out["e2e"]["ms"] / 1e3), "unit": "steps/s",
                 "h2d_bytes_per_step": out["e2e"]["h2d"], "d2h_bytes_per_step": out["e2e"]["d2h"]},

@@ -352,6 +352,22 @@ CPSTEP_API int cpstep_cp_step(cpstep_ctx* ctx, double* d_psi, double* d_vpsi,
 CPSTEP_API int cpstep_step_status(cpstep_ctx* ctx, int* ortho_iters, int* converged);
 
 /*
+ * CUDA graph of the step (no reference counterpart; the reference's step is a
+ * Charm++ message flow).  With graphs enabled (the default), cpstep_cp_step
+ * and cpstep_cp_step_host with iteration > 1 run one step directly for a new
+ * set of (psi, vpsi, occ, dt, energies, atom_force), capture the next one
+ * into a graph and replay it while the arguments stay the same.  Setting
+ * atoms, non-local data, CP masses, the stream, profiling or the GEMM path
+ * drops the graph; profiled steps and iteration 1 always run directly.  If a
+ * capture fails the context falls back to direct launches (enabled = 0).
+ * cpstep_ctx_graph_status: enabled flag, whether a graph is held, and its
+ * kernel count (cpstep_launch_count adds it per replay).
+ */
+CPSTEP_API int cpstep_ctx_set_graph(cpstep_ctx* ctx, int enable);
+CPSTEP_API int cpstep_ctx_graph_status(cpstep_ctx* ctx, int* enabled, int* captured,
+                                       unsigned long long* kernels);
+
+/*
  * cpstep_set_positions: new atom positions from host memory (natm x 3, bohr),
  *   copied on the context's stream (pinned memory makes it asynchronous); the
  *   structure-factor tables follow on the device.

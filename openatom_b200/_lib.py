@@ -82,6 +82,9 @@ SIGNATURES = {
                                       _vp]),
     "cpstep_step_status": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
     "cpstep_set_gemm_path": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "cpstep_ctx_set_graph": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "cpstep_ctx_graph_status": (ctypes.c_int, [_vp, _c_int_p, _c_int_p,
+                                               ctypes.POINTER(ctypes.c_ulonglong)]),
     "cpstep_device_errors": (ctypes.c_int, [_vp, _c_int_p]),
     "cpstep_set_positions": (ctypes.c_int, [_vp, _vp]),
     "cpstep_pc_overlap_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int,

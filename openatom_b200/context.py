@@ -299,6 +299,17 @@ class StepContext:
         """Mixed contexts: overlap / back-multiply on the tensor cores (split BF16) or in FP64."""
         _lib.call("cpstep_set_gemm_path", self._h, 1 if tensor_cores else 0)
 
+    def set_graph(self, enable):
+        """Capture / replay cp_step as a CUDA graph (iteration > 1; default on)."""
+        _lib.call("cpstep_ctx_set_graph", self._h, 1 if enable else 0)
+
+    def graph_status(self):
+        """(enabled, captured, kernels per replay)."""
+        en, cap, k = ctypes.c_int(), ctypes.c_int(), ctypes.c_ulonglong()
+        _lib.call("cpstep_ctx_graph_status", self._h, ctypes.byref(en), ctypes.byref(cap),
+                  ctypes.byref(k))
+        return bool(en.value), bool(cap.value), int(k.value)
+
     def device_errors(self):
         """Error bits recorded by kernels since the last call (0: none); clears them."""
         f = ctypes.c_int()

@@ -124,6 +124,12 @@ int prof_fold(cpstep_ctx* c) {
   return CPSTEP_OK;
 }
 
+void graph_drop(cpstep_ctx* c) {
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  c->gexec = nullptr;
+  c->graph_warm = 0;
+}
+
 extern "C" {
 
 int cpstep_version(void) { return 100; }
@@ -134,6 +140,7 @@ unsigned long long cpstep_launch_count(void) {
 
 int cpstep_ctx_profile(cpstep_ctx* c, int enable) {
   if (!c) return CPSTEP_ERR_ARG;
+  graph_drop(c);
   if (enable && c->prof_ev.empty()) {
     c->prof_ev.resize((size_t)cpstep_ctx::PROF_RING * (CPSTEP_NPHASE + 1));
     for (auto& e : c->prof_ev) CPSTEP_CUDA_TRY(cudaEventCreate(&e));
@@ -275,6 +282,8 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
   cudaFree(c->d_pc_part); cudaFree(c->d_ortho_ws); cudaFree(c->d_hmati);
   cudaFree(c->d_dev_err);
   cudaFree(c->d_force_atoms);
+  graph_drop(c);
+  if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   for (auto& e : c->prof_ev) cudaEventDestroy(e);
   nl_free(c);
   rho_free(c);
@@ -286,6 +295,7 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
 
 int cpstep_ctx_set_stream(cpstep_ctx* c, void* stream) {
   if (!c) return CPSTEP_ERR_ARG;
+  graph_drop(c);
   c->stream = reinterpret_cast<cudaStream_t>(stream);
   return CPSTEP_OK;
 }
@@ -389,6 +399,7 @@ int cpstep_ortho_tmat(cpstep_ctx* c, const double* d_s, double* d_t, int n, int 
 int cpstep_set_atoms(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* pos,
                      const double* q, int nspl, double gmin_spl, double dg_spl,
                      const double* vps, const double* gzvps, double alp_ewd) {
+  if (c) graph_drop(c);
   if (!c || natm <= 0 || ntyp <= 0 || !typ || !pos || !q || nspl <= 1 || !(dg_spl > 0) || !vps ||
       !gzvps || !(alp_ewd > 0))
     return CPSTEP_ERR_ARG;
@@ -449,6 +460,7 @@ int cpstep_nl_grid_size(int kmax, double scale, int n_interp) {
 int cpstep_set_nonlocal(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type,
                         const int* ch_l, const int* ch_m, const double* vnl, const double* gz0,
                         const double* vnorm) {
+  if (c) graph_drop(c);
   if (!c || nchan <= 0 || !ch_type || !ch_l || !ch_m || !vnl || !gz0 || !vnorm) {
     cpstep_set_error("set_nonlocal: bad argument");
     return CPSTEP_ERR_ARG;
@@ -467,6 +479,7 @@ int cpstep_ees_nonlocal(cpstep_ctx* c, const double* d_psi, const double* d_occ,
 
 int cpstep_set_cp_mass(cpstep_ctx* c, double tau_fs, double cut_ry) {
   if (!c || !(tau_fs > 0) || !(cut_ry > 0)) return CPSTEP_ERR_ARG;
+  graph_drop(c);
   return step_set_mass(c, tau_fs, cut_ry);
 }
 
@@ -483,7 +496,68 @@ int cpstep_cp_step(cpstep_ctx* c, double* d_psi, double* d_vpsi, const double* d
     cpstep_set_error("cp_step: atoms and CP masses must be set first");
     return CPSTEP_ERR_STATE;
   }
-  return step_run(c, d_psi, d_vpsi, d_occ, dt, iteration, d_energies, d_atom_force, 0);
+  // the first step (no second half kick) and profiled steps run directly
+  if (!c->use_graph || iteration <= 1 || c->profile)
+    return step_run(c, d_psi, d_vpsi, d_occ, dt, iteration, d_energies, d_atom_force, 0);
+  const cpstep_ctx::StepKey key{d_psi, d_vpsi, d_occ, dt, d_energies, d_atom_force};
+  if (c->gexec && key == c->gkey) {
+    CPSTEP_CUDA_TRY(cudaGraphLaunch(c->gexec, c->stream));
+    __atomic_add_fetch(&g_cpstep_launches, c->gkernels, __ATOMIC_RELAXED);
+    return CPSTEP_OK;
+  }
+  if (!c->graph_warm || !(key == c->gkey)) {  // one direct step: buffers allocated, sizes set
+    graph_drop(c);
+    int rc = step_run(c, d_psi, d_vpsi, d_occ, dt, iteration, d_energies, d_atom_force, 0);
+    if (!rc) {
+      c->graph_warm = 1;
+      c->gkey = key;
+    }
+    return rc;
+  }
+  // capture on a private stream (the legacy default stream cannot be captured)
+  if (!c->cap_stream) CPSTEP_CUDA_TRY(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+  const cudaStream_t user = c->stream;
+  const unsigned long long n0 = cpstep_launch_count();
+  c->stream = c->cap_stream;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeRelaxed);
+  int rc = e == cudaSuccess ? step_run(c, d_psi, d_vpsi, d_occ, dt, iteration, d_energies,
+                                       d_atom_force, 0)
+                            : CPSTEP_ERR_CUDA;
+  if (e == cudaSuccess) e = cudaStreamEndCapture(c->cap_stream, &g);
+  c->stream = user;
+  const unsigned long long nk = cpstep_launch_count() - n0;
+  __atomic_sub_fetch(&g_cpstep_launches, nk, __ATOMIC_RELAXED);  // captured, not run
+  cudaGraphExec_t x = nullptr;
+  if (!rc && e == cudaSuccess && g) e = cudaGraphInstantiate(&x, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (rc || e != cudaSuccess || !x) {  // not capturable here: direct launches from now on
+    cudaGetLastError();
+    if (x) cudaGraphExecDestroy(x);
+    c->use_graph = 0;
+    return step_run(c, d_psi, d_vpsi, d_occ, dt, iteration, d_energies, d_atom_force, 0);
+  }
+  c->gexec = x;
+  c->gkernels = nk;
+  CPSTEP_CUDA_TRY(cudaGraphLaunch(c->gexec, c->stream));
+  __atomic_add_fetch(&g_cpstep_launches, c->gkernels, __ATOMIC_RELAXED);
+  return CPSTEP_OK;
+}
+
+int cpstep_ctx_set_graph(cpstep_ctx* c, int enable) {
+  if (!c || (enable != 0 && enable != 1)) return CPSTEP_ERR_ARG;
+  graph_drop(c);
+  c->use_graph = enable;
+  return CPSTEP_OK;
+}
+
+int cpstep_ctx_graph_status(cpstep_ctx* c, int* enabled, int* captured,
+                            unsigned long long* kernels) {
+  if (!c) return CPSTEP_ERR_ARG;
+  if (enabled) *enabled = c->use_graph;
+  if (captured) *captured = c->gexec != nullptr;
+  if (kernels) *kernels = c->gkernels;
+  return CPSTEP_OK;
 }
 
 int cpstep_set_positions(cpstep_ctx* c, const double* h_pos) {
@@ -516,6 +590,7 @@ int cpstep_cp_step_host(cpstep_ctx* c, double* d_psi, double* d_vpsi, const doub
 
 int cpstep_set_gemm_path(cpstep_ctx* c, int tensor_cores) {
   if (!c || (tensor_cores != 0 && tensor_cores != 1)) return CPSTEP_ERR_ARG;
+  graph_drop(c);
   if (tensor_cores) {
     int major = 0;
     CPSTEP_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, c->device));

@@ -244,6 +244,26 @@ struct cpstep_ctx {
   int tc_ok = 0;
   int* d_dev_err = nullptr;  // error bits set by kernels (bounded waits that timed out)
 
+  // CUDA graph of cpstep_cp_step (iteration > 1): captured after one direct
+  // step with the same arguments, replayed while they stay the same; dropped
+  // by every call that changes what it holds (graph_drop)
+  struct StepKey {
+    double *psi, *vpsi;
+    const double* occ;
+    double dt;
+    double *energies, *atom_force;
+    bool operator==(const StepKey& o) const {
+      return psi == o.psi && vpsi == o.vpsi && occ == o.occ && dt == o.dt &&
+             energies == o.energies && atom_force == o.atom_force;
+    }
+  };
+  int use_graph = 1;
+  int graph_warm = 0;              // a direct step with gkey ran
+  StepKey gkey{};
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  unsigned long long gkernels = 0;  // kernels in the graph
+
   FftJob state_job() const {
     FftJob j;
     j.g = geom();
@@ -301,6 +321,7 @@ int pc_overlap_launch(cpstep_ctx* c, const double* a, const double* b, int M, in
                       const double* w, double alpha, double beta, double* C, int ldc);
 int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
                       double* out, int ldo, int nout, int nin, int K, double alpha, double beta);
+void graph_drop(cpstep_ctx* c);
 int pc_part_reserve(cpstep_ctx* c, size_t elems);
 int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
                             double* C, int ldc, int sym);

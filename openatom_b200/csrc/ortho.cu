@@ -216,8 +216,9 @@ __global__ void k_gershgorin(const double* __restrict__ S, int n, double* __rest
 
 // ---------------------------------------------------------------------------
 
-static int ensure(double** p, size_t* have, size_t need) {
+static int ensure(cpstep_ctx* c, double** p, size_t* have, size_t need) {
   if (*have >= need) return CPSTEP_OK;
+  graph_drop(c);  // a captured step may hold the old buffer
   cudaFree(*p);
   *p = nullptr;
   CPSTEP_CUDA_TRY(cudaMalloc(p, need * sizeof(double)));
@@ -233,7 +234,7 @@ int ortho_tmat(cpstep_ctx* c, const double* S, double* T, int n, int mixed, int 
   size_t nn = (size_t)n * n;
   // workspace: 5 working matrices (as doubles: enough for either precision), 3 FP64, misc
   size_t need = 9 * nn + 4096 + 8;
-  if (int rc = ensure(&c->d_ortho_ws, &c->ortho_ws_elems, need)) return rc;
+  if (int rc = ensure(c, &c->d_ortho_ws, &c->ortho_ws_elems, need)) return rc;
   double* ws = c->d_ortho_ws;
   Work w;
   w.n = n;

@@ -361,6 +361,7 @@ static int t128_attr() {
 
 int pc_part_reserve(cpstep_ctx* c, size_t need) {
   if (need > c->pc_part_elems) {
+    graph_drop(c);  // a captured step may hold the old buffer
     cudaFree(c->d_pc_part);
     c->d_pc_part = nullptr;
     c->pc_part_elems = 0;

@@ -1,0 +1,98 @@
+"""cpstep_cp_step as a CUDA graph: capture after one direct step, replay while
+the arguments stay the same, recapture when they change, identical results to
+direct launches (every kernel of the step is deterministic)."""
+import numpy as np
+import pytest
+
+from conftest import cuda_ok
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gsys():
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    import torch
+    from openatom_b200.system import System
+    sysm = System(9.0, 20.0, 6, {"O": 1, "H": 2}, seed=5, nfft=28)
+    occ = torch.ones(sysm.nstates, dtype=torch.float64, device="cuda")
+    return dict(sys=sysm, psi=sysm.psi(), occ=occ)
+
+
+def _ctx(gsys, precision, graph):
+    from openatom_b200.context import StepContext
+    s = gsys["sys"]
+    ctx = StepContext(s.layout, s.nstates, precision=precision)
+    ctx.set_atoms(s)
+    ctx.set_nonlocal(s)
+    ctx.set_cp_mass(25.0, 20.0)
+    ctx.set_graph(graph)
+    return ctx
+
+
+def _run(ctx, gsys, nsteps, it0=1, psi=None, v=None):
+    import torch
+    psi = gsys["psi"].clone() if psi is None else psi
+    v = torch.zeros_like(psi) if v is None else v
+    e = torch.zeros(16, dtype=torch.float64, device="cuda")
+    f = torch.zeros((gsys["sys"].natm, 3), dtype=torch.float64, device="cuda")
+    status = []
+    for k in range(nsteps):
+        ctx.cp_step(psi, v, gsys["occ"], 5.0, it0 + k, e, f)
+        status.append(ctx.graph_status())
+    torch.cuda.synchronize()
+    return psi, v, e, f, status
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_replay_matches_direct_launches(gsys, precision):
+    from openatom_b200 import _lib
+    cg, cd = _ctx(gsys, precision, True), _ctx(gsys, precision, False)
+    try:
+        n0 = _lib.lib().cpstep_launch_count()
+        pg, vg, eg, fg, st = _run(cg, gsys, 6)
+        ng = _lib.lib().cpstep_launch_count() - n0
+        n0 = _lib.lib().cpstep_launch_count()
+        pd, vd, ed, fd, _ = _run(cd, gsys, 6)
+        nd = _lib.lib().cpstep_launch_count() - n0
+        # iteration 1 and 2 direct, capture on 3, replays after
+        assert [s[1] for s in st] == [False, False, True, True, True, True]
+        assert st[-1][2] > 0
+        # replays count their kernels: the same total as direct launches
+        assert ng == nd
+        for a, b in ((pg, pd), (vg, vd), (eg, ed), (fg, fd)):
+            assert bool((a == b).all())
+        ok, _ = cg.step_status()
+        assert ok
+    finally:
+        cg.close()
+        cd.close()
+
+
+def test_graph_recaptures_on_new_arguments_and_setters(gsys):
+    import torch
+    c = _ctx(gsys, "mixed", True)
+    try:
+        psi, v, e, f, st = _run(c, gsys, 4)
+        assert st[-1][1]
+        # new psi buffer: one direct step, then a new capture
+        psi2, v2 = psi.clone(), v.clone()
+        _, _, _, _, st2 = _run(c, gsys, 3, it0=5, psi=psi2, v=v2)
+        assert [s[1] for s in st2] == [False, True, True]
+        # a setter drops the graph
+        c.set_gemm_path(False)
+        assert not c.graph_status()[1]
+        _, _, _, _, st3 = _run(c, gsys, 3, it0=8, psi=psi2, v=v2)
+        assert [s[1] for s in st3] == [False, True, True]
+        # and the replayed steps still agree with a direct context fed the same input
+        d = _ctx(gsys, "mixed", False)
+        d.set_gemm_path(False)
+        p3, v3 = psi2.clone(), v2.clone()
+        _run(c, gsys, 2, it0=11, psi=psi2, v=v2)
+        _run(d, gsys, 2, it0=11, psi=p3, v=v3)
+        assert bool((psi2 == p3).all()) and bool((v2 == v3).all())
+        d.close()
+        torch.cuda.synchronize()
+    finally:
+        c.close()
