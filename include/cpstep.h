@@ -109,6 +109,36 @@ CPSTEP_API int cpstep_layout_build(double box_len, double ecut_ry, int nchareG, 
                         int runs_cap, int* runs, int* nruns);
 
 /* ---------------------------------------------------------------------------
+ * State files (host, no GPU), one state per file as the reference writes them.
+ *
+ * cpstep_state_write: writeStateFile (src_charm_driver/utility/util.C:1955-
+ *   2180) for one state: the packed points sorted as sort_psi_output
+ *   (:2180-2220) orders them, the stored half sphere after G=0 and G=0 last;
+ *   header "npts nx ny nz".  format: CPSTEP_STATE_TEXT ("%g %g %d %d %d"
+ *   lines, as lossy as the reference's), CPSTEP_STATE_BINARY (int header,
+ *   records double re, double im, int kx, ky, kz), and the _GZ variants
+ *   (zlib, ".gz" appended to path).  The reference's TimeStamp side file is
+ *   not written.
+ * cpstep_state_read: readState (util.C:1107-1330) into the caller's packed
+ *   layout (kx/ky/kz of npts points, as cpstep_layout_build or the reference
+ *   produces it): every point takes the record with its (kx,ky,kz), the
+ *   redundant Gx=0 half the conjugate of its partner (flip_data_set,
+ *   para_grp_parse.C:178-286).  coef: npts complex (interleaved doubles).
+ *   nx/ny/nz (may be NULL) receive the header's grid.  A layout point missing
+ *   from the file returns CPSTEP_ERR_LAYOUT (the reference exits).
+ */
+#define CPSTEP_STATE_TEXT 0
+#define CPSTEP_STATE_BINARY 1
+#define CPSTEP_STATE_TEXT_GZ 2
+#define CPSTEP_STATE_BINARY_GZ 3
+CPSTEP_API int cpstep_state_write(const char* path, int format, int npts, const double* coef,
+                                  const int* kx, const int* ky, const int* kz, int nx, int ny,
+                                  int nz);
+CPSTEP_API int cpstep_state_read(const char* path, int format, int npts, const int* kx,
+                                 const int* ky, const int* kz, double* coef, int* nx, int* ny,
+                                 int* nz);
+
+/* ---------------------------------------------------------------------------
  * Context: the layout tables on the device plus the step's scratch.
  *
  * kx/ky/kz/runs: as produced by the reference (or cpstep_layout_build), copied.

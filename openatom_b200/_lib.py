@@ -82,6 +82,11 @@ SIGNATURES = {
                                       _vp]),
     "cpstep_step_status": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
     "cpstep_set_gemm_path": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "cpstep_state_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _vp,
+                                          _vp, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int]),
+    "cpstep_state_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _vp, _vp,
+                                         _vp, _vp, _c_int_p, _c_int_p, _c_int_p]),
     "cpstep_ctx_set_graph": (ctypes.c_int, [_vp, ctypes.c_int]),
     "cpstep_ctx_graph_status": (ctypes.c_int, [_vp, _c_int_p, _c_int_p,
                                                ctypes.POINTER(ctypes.c_ulonglong)]),

@@ -14,7 +14,8 @@ BUILD = os.path.join(HERE, "_build")
 import glob
 from concurrent.futures import ThreadPoolExecutor
 
-SOURCES = sorted(os.path.basename(p) for p in glob.glob(os.path.join(CSRC, "*.cu"))) + ["layout.cpp"]
+SOURCES = sorted(os.path.basename(p) for p in glob.glob(os.path.join(CSRC, "*.cu"))) + [
+    "layout.cpp", "statefile.cpp"]
 HEADERS = sorted(os.path.basename(p) for p in glob.glob(os.path.join(CSRC, "*.cuh")))
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -63,7 +64,7 @@ def build(force=False, verbose=False):
                 sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
             if r.returncode:
                 raise RuntimeError("nvcc failed: " + cmd[-3])
-    cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"]
+    cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart", "-lz"]
     subprocess.run(cmd, check=True)
     return OUT
 
