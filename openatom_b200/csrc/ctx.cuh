@@ -236,6 +236,8 @@ struct cpstep_ctx {
   // PairCalculator / Ortho scratch (grown on demand)
   double* d_pc_part = nullptr;
   size_t pc_part_elems = 0;
+  void* d_split = nullptr;  // plane buffer of the split plane passes (k_split_*)
+  size_t split_bytes = 0;
   double* d_ortho_ws = nullptr;
   size_t ortho_ws_elems = 0;
   int* d_ortho_status = nullptr;  // [iterations, converged] of the last Ortho launch
@@ -323,6 +325,7 @@ int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
                       double* out, int ldo, int nout, int nin, int K, double alpha, double beta);
 void graph_drop(cpstep_ctx* c);
 int pc_part_reserve(cpstep_ctx* c, size_t elems);
+int split_reserve(cpstep_ctx* c, size_t bytes);
 int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
                             double* C, int ldc, int sym);
 // paircalc_tc.cu (tensor-core products; *used = false when the SIMT path must run)

@@ -371,6 +371,18 @@ int pc_part_reserve(cpstep_ctx* c, size_t need) {
   return CPSTEP_OK;
 }
 
+int split_reserve(cpstep_ctx* c, size_t bytes) {
+  if (bytes > c->split_bytes) {
+    graph_drop(c);  // a captured step may hold the old buffer
+    cudaFree(c->d_split);
+    c->d_split = nullptr;
+    c->split_bytes = 0;
+    CPSTEP_CUDA_TRY(cudaMalloc(&c->d_split, bytes));
+    c->split_bytes = bytes;
+  }
+  return CPSTEP_OK;
+}
+
 int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
                             double* C, int ldc, int sym) {
   pcalc::k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, c->stream>>>(c->d_pc_part, nsplit, M, N,

@@ -439,6 +439,120 @@ k_xy_bwd(const cplx<T>* __restrict__ pen, const double* __restrict__ freal,
 }
 
 // ---------------------------------------------------------------------------
+// Plane passes for planes that do not fit in a block's shared memory (the
+// density sphere at n = 200 in FP64: 99 columns of 201 complex): the columns
+// (y) and the row pairs (x) of K2/K3 MODE 1 in separate launches, the
+// y-transformed plane in global memory as [state][z][y][nplane_x].  Same
+// transforms, signs and imag flips as k_xy_fwd / k_xy_bwd.
+constexpr int SPLIT_THREADS = 256;
+constexpr int SPLIT_CW = 8;  // columns per block (one per warp)
+
+// FWD: lines of the plane with x in [x0, x0 + CW) -> forward y-FFT -> tbuf.
+// !FWD: tbuf columns -> backward y-FFT -> the lines of those columns.
+template <typename T, int N, bool FWD>
+__global__ void __launch_bounds__(SPLIT_THREADS)
+k_split_cols(const cplx<T>* __restrict__ pen, cplx<T>* __restrict__ pen_out, StateGeom g,
+             const cplx<T>* __restrict__ twx_g, cplx<T>* __restrict__ tbuf) {
+  constexpr int LDY = PlaneLd<N>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* cols = tw + N;  // [SPLIT_CW][LDY]
+  const int z = blockIdx.x, x0 = blockIdx.y * SPLIT_CW, s = blockIdx.z;
+  const int nplx = g.nplane_x;
+  const int ncol = min(SPLIT_CW, nplx - x0);
+  for (int i = threadIdx.x; i < N; i += SPLIT_THREADS) tw[i] = twx_g[i];
+  cplx<T>* t0 = tbuf + ((size_t)s * N + z) * N * nplx;
+  const size_t prow = ((size_t)s * N + z) * g.nlpad;
+  if (FWD) {
+    for (int i = threadIdx.x; i < SPLIT_CW * LDY; i += SPLIT_THREADS) cols[i] = mk<T>(0, 0);
+    __syncthreads();
+    for (int l = threadIdx.x; l < g.nlines; l += SPLIT_THREADS) {
+      const int xy = __ldg(g.line_xy + l), x = xy & 0xffff;
+      if (x >= x0 && x < x0 + ncol) cols[(x - x0) * LDY + (xy >> 16)] = pen[prow + l];
+    }
+  } else {
+    for (int i = threadIdx.x; i < N * ncol; i += SPLIT_THREADS) {
+      const int y = i / ncol, xi = i - y * ncol;
+      cols[xi * LDY + y] = t0[(size_t)y * nplx + x0 + xi];
+    }
+  }
+  __syncthreads();
+  block_lines<T, N, !FWD>(cols, LDY, ncol, tw);  // FFTW_FORWARD y / FFTW_BACKWARD y
+  __syncthreads();
+  if (FWD) {
+    for (int i = threadIdx.x; i < N * ncol; i += SPLIT_THREADS) {
+      const int y = i / ncol, xi = i - y * ncol;
+      t0[(size_t)y * nplx + x0 + xi] = cols[xi * LDY + y];
+    }
+  } else {
+    for (int l = threadIdx.x; l < g.nlines; l += SPLIT_THREADS) {
+      const int xy = __ldg(g.line_xy + l), x = xy & 0xffff;
+      if (x >= x0 && x < x0 + ncol) pen_out[prow + l] = cols[(x - x0) * LDY + (xy >> 16)];
+    }
+  }
+}
+
+// FWD: row pair (ya, ya + 1) from tbuf -> C2R -> real rows of out.
+// !FWD: real rows of freal -> R2C -> tbuf.  One warp per row pair.
+template <typename T, int N, bool FWD>
+__global__ void __launch_bounds__(SPLIT_THREADS)
+k_split_rows(const double* __restrict__ freal, double* __restrict__ out, StateGeom g,
+             const cplx<T>* __restrict__ twx_g, cplx<T>* __restrict__ tbuf) {
+  constexpr int LDX = PlaneLd<N>::value;
+  constexpr int NW = SPLIT_THREADS / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  cplx<T>* row = tw + N + (size_t)warp * LDX;
+  const int z = blockIdx.x, s = blockIdx.z;
+  const int nplx = g.nplane_x;
+  for (int i = threadIdx.x; i < N; i += SPLIT_THREADS) tw[i] = twx_g[i];
+  __syncthreads();
+  const int pp = blockIdx.y * NW + warp;
+  if (pp >= N / 2) return;  // no block-wide barrier follows
+  const int ya = 2 * pp;
+  cplx<T>* t0 = tbuf + ((size_t)s * N + z) * N * nplx;
+  const cplx<T>* ra = t0 + (size_t)ya * nplx;
+  const cplx<T>* rb = ra + nplx;
+  const size_t ro = (((size_t)s * N + z) * N + ya) * N;
+  if (FWD) {
+    for (int k = lane; k < N; k += 32) {  // as build_c2r_row
+      cplx<T> zz;
+      if (k == 0) {
+        zz = mk<T>(ra[0].x, rb[0].x);
+      } else if (k < nplx) {
+        const cplx<T> a = ra[k], b = rb[k];
+        zz = mk<T>(a.x + b.y, b.x - a.y);
+      } else if (N - k < nplx) {
+        const cplx<T> a = ra[N - k], b = rb[N - k];
+        zz = mk<T>(a.x - b.y, a.y + b.x);
+      } else {
+        zz = mk<T>(0, 0);
+      }
+      row[k] = zz;
+    }
+    __syncwarp();
+    fft_line_warp<T, N, true>(row, tw);  // C2R, +i sign
+    for (int x = lane; x < N; x += 32) {
+      const cplx<T> v = row[x];
+      out[ro + x] = (double)v.x;
+      out[ro + N + x] = (double)v.y;
+    }
+  } else {
+    for (int x = lane; x < N; x += 32) row[x] = mk<T>((T)freal[ro + x], (T)freal[ro + N + x]);
+    __syncwarp();
+    fft_line_warp<T, N, false>(row, tw);  // R2C, -i sign
+    cplx<T>* wa = t0 + (size_t)ya * nplx;
+    cplx<T>* wb = wa + nplx;
+    for (int k = lane; k < nplx; k += 32) {  // as extract_r2c_row
+      const cplx<T> zk = row[k], zm = row[k == 0 ? 0 : N - k];
+      wa[k] = mk<T>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zm.y - zk.y));
+      wb[k] = mk<T>((T)0.5 * (zk.y + zm.y), (T)0.5 * (zk.x - zm.x));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Plane passes with register-resident line FFTs (ShflFft) for the sizes
 // ShflCfg<N> lists.  A group of NL lanes owns one column (y) or one row pair
 // (x) at a time; only the plane itself is in shared memory.  Columns are
@@ -1095,10 +1209,50 @@ struct StateFft {
       return CPSTEP_OK;
     }
     const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
+    if (smem > PShape<T, N>::LIMIT) return split_g2r(c, j, real, nstates);
     if (int rc = set_smem(k_xy_fwd<T, N, 1>, smem)) return rc;
     k_xy_fwd<T, N, 1><<<dim3(N, nstates, 1), PTHREADS, smem, c->stream>>>(
         reinterpret_cast<const cplx<T>*>(j.pen_a), j.g, tws<T>(c).x, nullptr, nstates, 1, N,
         real);
+    CPSTEP_LAUNCH_CHECK();
+    return CPSTEP_OK;
+  }
+
+  // the split plane passes (k_split_cols / k_split_rows) with their buffer
+  static int split_buf(cpstep_ctx* c, const FftJob& j, int nstates, cplx<T>** buf) {
+    const size_t need = sizeof(cplx<T>) * (size_t)nstates * N * N * j.g.nplane_x;
+    if (int rc = split_reserve(c, need)) return rc;
+    *buf = reinterpret_cast<cplx<T>*>(c->d_split);
+    return CPSTEP_OK;
+  }
+  static size_t split_smem() { return sizeof(cplx<T>) * (N + (size_t)SPLIT_CW * PlaneLd<N>::value); }
+  static int split_g2r(cpstep_ctx* c, const FftJob& j, double* real, int nstates) {
+    cplx<T>* tb;
+    if (int rc = split_buf(c, j, nstates, &tb)) return rc;
+    const size_t sm = split_smem();
+    if (int rc = set_smem(k_split_cols<T, N, true>, sm)) return rc;
+    k_split_cols<T, N, true><<<dim3(N, cdiv(j.g.nplane_x, SPLIT_CW), nstates), SPLIT_THREADS, sm,
+                               c->stream>>>(reinterpret_cast<const cplx<T>*>(j.pen_a), nullptr,
+                                            j.g, tws<T>(c).x, tb);
+    CPSTEP_LAUNCH_CHECK();
+    if (int rc = set_smem(k_split_rows<T, N, true>, sm)) return rc;
+    k_split_rows<T, N, true><<<dim3(N, cdiv(N / 2, SPLIT_THREADS / 32), nstates), SPLIT_THREADS,
+                               sm, c->stream>>>(nullptr, real, j.g, tws<T>(c).x, tb);
+    CPSTEP_LAUNCH_CHECK();
+    return CPSTEP_OK;
+  }
+  static int split_r2g(cpstep_ctx* c, const FftJob& j, const double* f_r, int nstates) {
+    cplx<T>* tb;
+    if (int rc = split_buf(c, j, nstates, &tb)) return rc;
+    const size_t sm = split_smem();
+    if (int rc = set_smem(k_split_rows<T, N, false>, sm)) return rc;
+    k_split_rows<T, N, false><<<dim3(N, cdiv(N / 2, SPLIT_THREADS / 32), nstates), SPLIT_THREADS,
+                                sm, c->stream>>>(f_r, nullptr, j.g, tws<T>(c).x, tb);
+    CPSTEP_LAUNCH_CHECK();
+    if (int rc = set_smem(k_split_cols<T, N, false>, sm)) return rc;
+    k_split_cols<T, N, false><<<dim3(N, cdiv(j.g.nplane_x, SPLIT_CW), nstates), SPLIT_THREADS,
+                                sm, c->stream>>>(nullptr, reinterpret_cast<cplx<T>*>(j.pen_b),
+                                                 j.g, tws<T>(c).x, tb);
     CPSTEP_LAUNCH_CHECK();
     return CPSTEP_OK;
   }
@@ -1176,6 +1330,10 @@ struct StateFft {
           nstates, 1);
     } else {
       const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
+      if (smem > PShape<T, N>::LIMIT) {
+        if (int rc = split_r2g(c, j, f_r, nstates)) return rc;
+        return zfft_bwd(c, j, fg, nullptr, nullptr, nstates, scale, 1);
+      }
       if (int rc = set_smem(k_xy_bwd<T, N, 1>, smem)) return rc;
       k_xy_bwd<T, N, 1><<<dim3(N, nstates), PTHREADS, smem, c->stream>>>(
           nullptr, f_r, nullptr, reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, nullptr,

@@ -107,3 +107,58 @@ def test_local_force_is_minus_energy_gradient(dsys):
             lst.append(ee + ew)
         fd = -(ep[0] - em[0]) / (2 * h)
         assert abs(fd - f[0, d]) < 1e-6 * max(1.0, abs(fd))
+
+
+@pytest.fixture(scope="module")
+def big():
+    """The 768-atom box and grid (L = 37.2 bohr, 70 Ry, 200^3) with a few states:
+    the density sphere's plane (99 columns of 201 FP64 complex) does not fit in
+    a block's shared memory, so the split plane passes run."""
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    import torch
+    from openatom_b200.context import StepContext
+    from openatom_b200.system import System
+    sysm = System(37.2, 70.0, 4, {"O": 4, "H": 8}, nfft=200, seed=3)
+    ctx = StepContext(sysm.layout, sysm.nstates, precision="fp64")
+    ctx.set_atoms(sysm)
+    occ = torch.ones(sysm.nstates, dtype=torch.float64, device="cuda")
+    rho = ctx.density(sysm.psi(), occ)
+    yield dict(sys=sysm, ctx=ctx, rho=rho, occ=occ)
+    ctx.close()
+
+
+def test_split_plane_passes_at_200(big):
+    from oracle import density as OD
+    s = big["sys"]
+    o = OD.density_layout(s.box_len, s.ecut_ry, 200)
+    assert int(o.kx.max()) + 1 == 99  # the plane that needs the split passes
+    rho = big["rho"].cpu().numpy()
+    rg = big["ctx"].rho_r2g(big["rho"]).cpu().numpy()
+    ref = OD.rho_to_g(rho, o, s.box_len ** 3)
+    assert np.max(np.abs(rg - ref)) < 1e-12 * np.max(np.abs(ref))
+    v, e, f = big["ctx"].vks_from_rho(big["rho"])
+    vxc, exc, mu = OD.pz_lda(rho, s.box_len ** 3)
+    vg, eh, ee, ew, fr = OD.hart_eext(ref, o.kx, o.ky, o.kz, s.box_len, 0.5 * s.ecut_ry,
+                                      s.atoms_dict(), s.tab, s.alp_ewd)
+    vref = vxc + OD.vg_to_r(vg, o)
+    assert np.max(np.abs(v.cpu().numpy() - vref)) < 1e-11 * np.max(np.abs(vref))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_step_runs_at_200(big, precision):
+    import torch
+    from openatom_b200.context import StepContext
+    s = big["sys"]
+    ctx = StepContext(s.layout, s.nstates, precision=precision)
+    try:
+        ctx.set_atoms(s)
+        ctx.set_nonlocal(s)
+        ctx.set_cp_mass(25.0, 70.0)
+        psi = s.psi()
+        v = torch.zeros_like(psi)
+        e, f = ctx.cp_step(psi, v, big["occ"], 5.0, 1)
+        it, ok = ctx.step_status()
+        assert ok and np.isfinite(e.cpu().numpy()).all()
+    finally:
+        ctx.close()
