@@ -451,6 +451,135 @@ def kernel_case(args):
                       "check": chk}))
 
 
+def batch16_systems(seed=4):
+    """16 water-like systems: states in [16, 256], grids from {32, 48, 64, 96},
+    Ecut in [30, 70] Ry, the box chosen so that the grid rule lands on the
+    grid (for 32, which the FFT size table skips, the largest box whose grid is
+    smaller, with the grid set to 32), water at liquid density (1 molecule per
+    200 bohr^3)."""
+    import ctypes
+    import numpy as np
+    from openatom_b200 import _lib
+    L = _lib.lib()
+
+    def nfft(box, ec):
+        k, n, nk, npts = (ctypes.c_int() for _ in range(4))
+        L.cpstep_layout_sizes(float(box), float(ec), ctypes.byref(k), ctypes.byref(n),
+                              ctypes.byref(nk), ctypes.byref(npts))
+        return n.value
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(16):
+        grid = int(rng.choice([32, 48, 64, 96]))
+        ec = float(rng.uniform(30.0, 70.0))
+        S = int(rng.integers(16, 257))
+        box = None
+        last_below = None
+        for b in np.arange(5.0, 60.0, 0.05):
+            n = nfft(b, ec)
+            if n == grid:
+                box = float(b)
+                break
+            if n < grid:
+                last_below = float(b)
+        if box is None:
+            box = last_below
+        nw = max(1, int(round(box ** 3 / 200.0)))
+        out.append(dict(box=round(box, 2), ecut=ec, nstates=S, grid=grid,
+                        atoms={"O": nw, "H": 2 * nw}))
+    return out
+
+
+def run_batch16(args):
+    import numpy as np
+    import torch
+    from openatom_b200 import _lib
+    from openatom_b200.batch import StepBatch
+    from openatom_b200.context import StepContext
+    from openatom_b200.system import System
+    specs = batch16_systems()
+    L = _lib.lib()
+    systems = []
+    for k, sp in enumerate(specs):
+        sysm = System(sp["box"], sp["ecut"], sp["nstates"], sp["atoms"], nfft=sp["grid"],
+                      seed=300 + k)
+        systems.append(sysm)
+
+    def contexts(prec, graph):
+        out = []
+        for sysm, sp in zip(systems, specs):
+            ctx = StepContext(sysm.layout, sysm.nstates, precision=prec)
+            ctx.set_atoms(sysm)
+            ctx.set_nonlocal(sysm)
+            ctx.set_cp_mass(TAU_FS, sp["ecut"])
+            ctx.set_graph(graph)
+            psi = sysm.psi()
+            out.append(dict(ctx=ctx, psi=psi, v=torch.zeros_like(psi),
+                            occ=torch.ones(sysm.nstates, dtype=torch.float64, device="cuda"),
+                            e=torch.zeros(_lib.NENERGY, dtype=torch.float64, device="cuda"),
+                            f=torch.zeros((sysm.natm, 3), dtype=torch.float64, device="cuda")))
+        return out
+
+    def timed(fn, nsteps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(nsteps):
+            fn(k)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    # batched graph, mixed
+    mix = contexts("mixed", False)
+    batch = StepBatch([d["ctx"] for d in mix])
+    arg = lambda key: [d[key] for d in mix]
+    for w in range(args.warmup):
+        batch.step(arg("psi"), arg("v"), arg("occ"), DT, 1 + w, arg("e"), arg("f"))
+    n0 = L.cpstep_launch_count()
+    ms_batch = timed(lambda k: batch.step(arg("psi"), arg("v"), arg("occ"), DT,
+                                          1 + args.warmup + k, arg("e"), arg("f")), args.steps)
+    launches = L.cpstep_launch_count() - n0
+    status = batch.status()
+    e_mix = [d["e"].cpu().numpy().copy() for d in mix]
+    batch.close()
+    for d in mix:
+        d["ctx"].close()
+    # the plain path looped over the systems (direct launches)
+    pl = contexts("fp64", False)
+
+    def loop(k):
+        for d in pl:
+            d["ctx"].cp_step(d["psi"], d["v"], d["occ"], DT, 1 + args.warmup + k, d["e"], d["f"])
+
+    for w in range(args.warmup):
+        for d in pl:
+            d["ctx"].cp_step(d["psi"], d["v"], d["occ"], DT, 1 + w, d["e"], d["f"])
+    ms_loop = timed(loop, args.steps)
+    for d in pl:
+        d["ctx"].close()
+    nsys = len(specs)
+    v_batch = nsys * args.steps / (ms_batch / 1e3)
+    v_loop = nsys * args.steps / (ms_loop / 1e3)
+    line = {
+        "metric": "aggregate CP steps/sec of 16 independent systems on one GPU",
+        "value": v_batch, "unit": "system-steps/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_batch / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "mixed (as the single-system line)",
+        "data": "synthetic",
+        "config": {"workload": "16 water-like systems, states %s, grids %s" % (
+            [sp["nstates"] for sp in specs], [sp["grid"] for sp in specs]),
+                   "systems": specs, "parallelism": "one batch graph, a branch per system"},
+        "plain_fp64_loop_value": v_loop, "batched_over_plain_loop": v_batch / v_loop,
+        "gpu_launches": int(launches), "batch_graph": {"enabled": status[0],
+                                                      "captured": status[1],
+                                                      "kernels_per_step": status[2]},
+        "energies_finite": bool(all(np.isfinite(e).all() for e in e_mix)),
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -463,9 +592,17 @@ def main():
                     help="run a small profiling case instead of the benchmark")
     ap.add_argument("--states", type=int, default=8)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--batch16", action="store_true",
+                    help="16 independent systems of uneven size stepped by one batch graph "
+                         "(mixed) against looping the plain FP64 path")
     args = ap.parse_args()
     if args.kernel_case:
         kernel_case(args)
+        return
+    if args.batch16:
+        if args.warmup < 3:
+            args.warmup = 3
+        run_batch16(args)
         return
     if args.warmup < 3:
         args.warmup = 3

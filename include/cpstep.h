@@ -394,6 +394,30 @@ CPSTEP_API int cpstep_step_status(cpstep_ctx* ctx, int* ortho_iters, int* conver
  * kernel count (cpstep_launch_count adds it per replay).
  */
 CPSTEP_API int cpstep_ctx_set_graph(cpstep_ctx* ctx, int enable);
+
+/*
+ * Batches of independent systems (no reference counterpart beyond running
+ * instances side by side): one context per system, one electronic step of
+ * every context per cpstep_batch_step, captured into a single CUDA graph with
+ * one branch per context and replayed while the arguments stay the same
+ * (iteration 1 and a new argument set run directly; a context's setters force
+ * a new capture).  Arrays are indexed by context; atom_force may be NULL (or
+ * hold NULL entries).  The graph is launched on the batch's stream
+ * (cpstep_batch_set_stream, default the legacy stream); the contexts' own
+ * streams are not used by batch steps.  cpstep_batch_status as
+ * cpstep_ctx_graph_status.
+ */
+typedef struct cpstep_batch cpstep_batch;
+CPSTEP_API int cpstep_batch_create(cpstep_batch** batch, int nctx, cpstep_ctx* const* ctxs);
+CPSTEP_API int cpstep_batch_destroy(cpstep_batch* batch);
+CPSTEP_API int cpstep_batch_set_stream(cpstep_batch* batch, void* stream);
+CPSTEP_API int cpstep_batch_set_graph(cpstep_batch* batch, int enable);
+CPSTEP_API int cpstep_batch_status(cpstep_batch* batch, int* enabled, int* captured,
+                                   unsigned long long* kernels);
+CPSTEP_API int cpstep_batch_step(cpstep_batch* batch, double* const* d_psi,
+                                 double* const* d_vpsi, const double* const* d_occ, double dt,
+                                 int iteration, double* const* d_energies,
+                                 double* const* d_atom_force);
 CPSTEP_API int cpstep_ctx_graph_status(cpstep_ctx* ctx, int* enabled, int* captured,
                                        unsigned long long* kernels);
 

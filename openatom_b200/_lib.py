@@ -88,6 +88,15 @@ SIGNATURES = {
     "cpstep_state_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                          _vp, _vp, _c_int_p, _c_int_p, _c_int_p]),
     "cpstep_ctx_set_graph": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "cpstep_batch_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]),
+    "cpstep_batch_destroy": (ctypes.c_int, [_vp]),
+    "cpstep_batch_set_stream": (ctypes.c_int, [_vp, _vp]),
+    "cpstep_batch_set_graph": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "cpstep_batch_status": (ctypes.c_int, [_vp, _c_int_p, _c_int_p,
+                                           ctypes.POINTER(ctypes.c_ulonglong)]),
+    "cpstep_batch_step": (ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                         ctypes.POINTER(_vp), ctypes.c_double, ctypes.c_int,
+                                         ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "cpstep_ctx_graph_status": (ctypes.c_int, [_vp, _c_int_p, _c_int_p,
                                                ctypes.POINTER(ctypes.c_ulonglong)]),
     "cpstep_device_errors": (ctypes.c_int, [_vp, _c_int_p]),

@@ -125,6 +125,7 @@ int prof_fold(cpstep_ctx* c) {
 }
 
 void graph_drop(cpstep_ctx* c) {
+  c->gen += 1;
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   c->gexec = nullptr;
   c->graph_warm = 0;

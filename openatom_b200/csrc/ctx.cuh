@@ -265,6 +265,11 @@ struct cpstep_ctx {
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t gexec = nullptr;
   unsigned long long gkernels = 0;  // kernels in the graph
+  unsigned gen = 0;                 // counts graph_drop calls (batch graphs recapture)
+  // batches: the Ortho launch (cooperative, grid-wide barriers) waits for
+  // ortho_wait and records ortho_signal, so no two contexts' Ortho kernels run
+  // at the same time
+  cudaEvent_t ortho_wait = nullptr, ortho_signal = nullptr;
 
   FftJob state_job() const {
     FftJob j;

@@ -267,6 +267,7 @@ int ortho_tmat(cpstep_ctx* c, const double* S, double* T, int n, int mixed, int 
   int ntiles = cdiv(n, TS) * cdiv(n, TS);
   int per_sm = 0;
   void* args[] = {&w};
+  if (c->ortho_wait) CPSTEP_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ortho_wait, 0));
   if (mixed) {
     CPSTEP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_schulz<float>, NT, 0));
     int nb = std::max(1, std::min(2 * ntiles, per_sm * c->num_sms));
@@ -280,6 +281,7 @@ int ortho_tmat(cpstep_ctx* c, const double* S, double* T, int n, int mixed, int 
     int nb = std::max(1, std::min(2 * ntiles, per_sm * c->num_sms));
     CPSTEP_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_schulz<double>, nb, NT, args, 0, c->stream));
   }
+  if (c->ortho_signal) CPSTEP_CUDA_TRY(cudaEventRecord(c->ortho_signal, c->stream));
   c->d_ortho_status = w.status;
   if (check_host) {
     int st[2] = {0, 0};
