@@ -201,6 +201,9 @@ def run_ours(args, cfg, name, rank, ws, dist):
         ctx.set_atoms(sysm)
         ctx.set_nonlocal(sysm)
         ctx.set_cp_mass(TAU_FS, cfg["ecut"])
+        # launch choices from the project's autotuner (timed on this system)
+        choice, _ = ctx.autotune(psi0, occ)
+        out.setdefault("tune", {})[prec] = choice
         return ctx
 
     out = {}
@@ -687,6 +690,7 @@ def main():
                      "peak_kind": peak_kind},
         "roofline_paircalc": pc_roofline(out["pc_us"], sysm, hbm, pk, gflops, gemm_ms),
         "gpu_launches": int(mixed["launches"]),
+        "autotune": out.get("tune"),
         "cuda_graph": {"mixed": mixed["graph"], "fp64": fp64["graph"],
                        "fields": ["enabled", "captured", "kernels_per_step"]},
         "clocks": mixed["clocks"],

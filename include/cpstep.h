@@ -396,6 +396,26 @@ CPSTEP_API int cpstep_step_status(cpstep_ctx* ctx, int* ortho_iters, int* conver
 CPSTEP_API int cpstep_ctx_set_graph(cpstep_ctx* ctx, int enable);
 
 /*
+ * Launch choices of a context (no reference counterpart; FFTW_MEASURE plans,
+ * fftCache.C:252-255, are the nearest relative).  CPSTEP_NTUNE values:
+ *   [0] state plane passes: register-shuffle line FFTs (1) or shared-memory
+ *       Stockham (0) where both exist;  [1] state plane passes: blocks about
+ *       this many times the SM count;  [2] EES plane kernels: the same;
+ *   [3] PairCalc overlap split-K: CTAs about this many times the SM count;
+ *   [4] mixed contexts: tensor-core products (1) or FP64 (0).
+ * cpstep_autotune times the candidates of each choice on the caller's psi
+ * (device, nstates x npts) and occ with CUDA events and keeps the fastest;
+ * ms (may be NULL, CPSTEP_NTUNE doubles) receives the best time (ms) per
+ * choice.  Synchronises the stream; uses scratch of about one psi.
+ * Choices change results by rounding only; get/set reproduce a tuned run.
+ */
+#define CPSTEP_NTUNE 5
+CPSTEP_API int cpstep_tune_get(const cpstep_ctx* ctx, int* vals, int n);
+CPSTEP_API int cpstep_tune_set(cpstep_ctx* ctx, const int* vals, int n);
+CPSTEP_API int cpstep_autotune(cpstep_ctx* ctx, const double* d_psi, const double* d_occ,
+                               double* ms);
+
+/*
  * Batches of independent systems (no reference counterpart beyond running
  * instances side by side): one context per system, one electronic step of
  * every context per cpstep_batch_step, captured into a single CUDA graph with

@@ -88,6 +88,9 @@ SIGNATURES = {
     "cpstep_state_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                          _vp, _vp, _c_int_p, _c_int_p, _c_int_p]),
     "cpstep_ctx_set_graph": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "cpstep_tune_get": (ctypes.c_int, [_vp, _c_int_p, ctypes.c_int]),
+    "cpstep_tune_set": (ctypes.c_int, [_vp, _c_int_p, ctypes.c_int]),
+    "cpstep_autotune": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_double)]),
     "cpstep_batch_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]),
     "cpstep_batch_destroy": (ctypes.c_int, [_vp]),
     "cpstep_batch_set_stream": (ctypes.c_int, [_vp, _vp]),

@@ -259,6 +259,15 @@ struct cpstep_ctx {
              energies == o.energies && atom_force == o.atom_force;
     }
   };
+  // launch choices (cpstep_autotune, cpstep_tune_get/set); the defaults are
+  // the fixed heuristics
+  struct Tune {
+    int shfl = 1;         // state plane passes (density, V.psi): register shuffle FFT (1) or
+                          // shared-memory Stockham (0), where both exist
+    int plane_waves = 3;  // state plane passes: blocks ~ plane_waves x SMs
+    int nl_blocks = 6;    // EES plane kernels: blocks ~ nl_blocks x SMs
+    int pc_split = 1;     // PairCalc overlap split-K: CTAs ~ pc_split x SMs
+  } tune;
   int use_graph = 1;
   int graph_warm = 0;              // a direct step with gkey ran
   StepKey gkey{};

@@ -399,7 +399,7 @@ int pc_overlap_launch(cpstep_ctx* c, const double* a, const double* b, int M, in
   if (used) return CPSTEP_OK;
   if (int rc = t128_attr()) return rc;
   int tm = cdiv(M, TB), tn = cdiv(N, TB);
-  int want = std::max(1, c->num_sms / (tm * tn));
+  int want = std::max(1, c->tune.pc_split * c->num_sms / (tm * tn));
   int kslab = cdiv(cdiv(K, want), TK) * TK;
   int nsplit = cdiv(K, kslab);
   if (int rc = pc_part_reserve(c, (size_t)nsplit * M * N)) return rc;

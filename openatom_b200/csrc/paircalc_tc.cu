@@ -446,7 +446,7 @@ int pc_overlap_tc_launch(cpstep_ctx* c, const double* a, const double* b, int M,
     return CPSTEP_OK;
   const bool one = a == b && M == N && M <= ROWS;
   const int tm = cdiv(M, ROWS), tn = cdiv(N, ROWS);
-  const int want = std::max(1, c->num_sms / (tm * tn));
+  const int want = std::max(1, c->tune.pc_split * c->num_sms / (tm * tn));
   const int kslab = cdiv(cdiv(K, want), 128) * 128;  // whole TMEM groups per slab
   const int nsplit = cdiv(K, kslab);
   if (int rc = pc_part_reserve(c, (size_t)nsplit * M * N)) return rc;

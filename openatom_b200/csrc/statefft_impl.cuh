@@ -1139,9 +1139,10 @@ int set_smem(K kernel, size_t smem) {
   return CPSTEP_OK;
 }
 
-// state groups for the plane passes: aim at >= 3 waves of CTAs
+// state groups for the plane passes: aim at tune.plane_waves (default 3)
+// waves of CTAs
 inline int plane_groups(const cpstep_ctx* c, int nstates, int other) {
-  int target = 3 * c->num_sms;
+  int target = c->tune.plane_waves * c->num_sms;
   int per = c->nz * other;
   int g = cdiv(target, per);
   return std::max(1, std::min(nstates, g));
@@ -1165,20 +1166,22 @@ struct StateFft {
     const FftJob j = c->state_job();
     if (int rc = zfft_fwd(c, j, psi, c->nstates)) return rc;
     if constexpr (ShflCfg<N>::ok) {
-      const size_t smem = SShape<T, N>::bytes(j.g.nplane_x);
-      int ng = std::min(c->ngroups_rho, plane_groups(c, c->nstates, 1));
-      int spg = cdiv(c->nstates, ng);
-      ng = cdiv(c->nstates, spg);
-      if (int rc = set_smem(k_xy_fwd_s<T, N, 0>, smem)) return rc;
-      k_xy_fwd_s<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
-          reinterpret_cast<const cplx<T>*>(j.pen_a), j.g, tws<T>(c).x, occ, c->nstates, spg,
-          c->d_rho_part);
-      CPSTEP_LAUNCH_CHECK();
-      size_t nr = (size_t)N * N * N;
-      k_rho_reduce<<<2 * c->num_sms, 256, 0, c->stream>>>(c->d_rho_part, ng, nr, 1.0 / c->vol,
-                                                          rho);
-      CPSTEP_LAUNCH_CHECK();
-      return CPSTEP_OK;
+      if (c->tune.shfl) {
+        const size_t smem = SShape<T, N>::bytes(j.g.nplane_x);
+        int ng = std::min(c->ngroups_rho, plane_groups(c, c->nstates, 1));
+        int spg = cdiv(c->nstates, ng);
+        ng = cdiv(c->nstates, spg);
+        if (int rc = set_smem(k_xy_fwd_s<T, N, 0>, smem)) return rc;
+        k_xy_fwd_s<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
+            reinterpret_cast<const cplx<T>*>(j.pen_a), j.g, tws<T>(c).x, occ, c->nstates, spg,
+            c->d_rho_part);
+        CPSTEP_LAUNCH_CHECK();
+        size_t nr = (size_t)N * N * N;
+        k_rho_reduce<<<2 * c->num_sms, 256, 0, c->stream>>>(c->d_rho_part, ng, nr, 1.0 / c->vol,
+                                                            rho);
+        CPSTEP_LAUNCH_CHECK();
+        return CPSTEP_OK;
+      }
     }
     const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
     const int rows = PShape<T, N>::ROWS;
@@ -1295,13 +1298,18 @@ struct StateFft {
     int ng = plane_groups(c, c->nstates, 1);
     int spg = cdiv(c->nstates, ng);
     ng = cdiv(c->nstates, spg);
+    bool shfl_done = false;
     if constexpr (ShflCfg<N>::ok) {
-      const size_t smem = SShape<T, N>::bytes(j.g.nplane_x);
-      if (int rc = set_smem(k_xy_bwd_s<T, N, 0>, smem)) return rc;
-      k_xy_bwd_s<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
-          reinterpret_cast<const cplx<T>*>(j.pen_a), nullptr, vt,
-          reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, occ, c->nstates, spg);
-    } else {
+      if (c->tune.shfl) {
+        const size_t smem = SShape<T, N>::bytes(j.g.nplane_x);
+        if (int rc = set_smem(k_xy_bwd_s<T, N, 0>, smem)) return rc;
+        k_xy_bwd_s<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
+            reinterpret_cast<const cplx<T>*>(j.pen_a), nullptr, vt,
+            reinterpret_cast<cplx<T>*>(j.pen_b), j.g, tws<T>(c).x, occ, c->nstates, spg);
+        shfl_done = true;
+      }
+    }
+    if (!shfl_done) {
       const size_t smem = PShape<T, N>::bytes(j.g.nplane_x);
       if (int rc = set_smem(k_xy_bwd<T, N, 0>, smem)) return rc;
       k_xy_bwd<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(
@@ -1353,7 +1361,7 @@ struct StateFft {
   // NL plane kernels: states per block so that N x groups is about six blocks
   // per SM
   static void nl_groups(const cpstep_ctx* c, int nstates, int& spg, int& ng) {
-    ng = std::max(1, std::min(nstates, cdiv(6 * c->num_sms, N)));
+    ng = std::max(1, std::min(nstates, cdiv(c->tune.nl_blocks * c->num_sms, N)));
     spg = cdiv(nstates, ng);
     ng = cdiv(nstates, spg);
   }
