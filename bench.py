@@ -201,8 +201,9 @@ def run_ours(args, cfg, name, rank, ws, dist):
         ctx.set_atoms(sysm)
         ctx.set_nonlocal(sysm)
         ctx.set_cp_mass(TAU_FS, cfg["ecut"])
-        # launch choices from the project's autotuner (timed on this system)
-        choice, _ = ctx.autotune(psi0, occ)
+        # launch choices from the project's autotuner (timed on this system);
+        # profiler runs keep the defaults (a profiler distorts the timing)
+        choice = ctx.autotune(psi0, occ)[0] if not args.no_autotune else ctx.tune_get()
         out.setdefault("tune", {})[prec] = choice
         return ctx
 
@@ -591,6 +592,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="water192", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch choices (for profiler runs)")
     ap.add_argument("--kernel-case", choices=["statefft", "rhoside", "ees", "paircalc"], default=None,
                     help="run a small profiling case instead of the benchmark")
     ap.add_argument("--states", type=int, default=8)
