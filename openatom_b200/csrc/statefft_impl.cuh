@@ -884,9 +884,9 @@ struct NlShape {
 // interpolation plane jc on z: zpart[s][atom][jc] = (sum P mn, sum P dmn_x,
 // sum P dmn_y, sum P dmn_z) over its 8x8 points (eesZmatRchare :1238-1346 and
 // the force sums of eesEnergyAtmForcRchare :1480-1700, before the Z factor).
-constexpr int NLTHREADS = 256;  // NL plane kernels: 8 warps, two blocks per SM
+constexpr int NLTHREADS = 256;  // NL plane kernels: 8 warps, three blocks per SM
 template <typename T, int N>
-__global__ void __launch_bounds__(NLTHREADS, 2)
+__global__ void __launch_bounds__(NLTHREADS, 3)
 k_nl_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict__ twx_g,
          NlAtoms A, int ctype, int nstates, int spg, double* __restrict__ zpart) {
   constexpr int LDY = PlaneLd<N>::value;
@@ -1005,7 +1005,7 @@ k_nl_fwd(const cplx<T>* __restrict__ pen, StateGeom g, const cplx<T>* __restrict
 // list, atoms in list order, so the sum order is fixed), then x R2C, imag
 // flip, y-FFT (doNlFFTRtoG_Rchare, fftCache.C:634-699) into pencils.
 template <typename T, int N>
-__global__ void __launch_bounds__(NLTHREADS, 2)
+__global__ void __launch_bounds__(NLTHREADS, 3)
 k_nl_bwd(cplx<T>* __restrict__ pen_out, StateGeom g, const cplx<T>* __restrict__ twx_g,
          NlAtoms A, int ctype, int nstates, int spg, const double* __restrict__ zs) {
   constexpr int LDY = PlaneLd<N>::value;
