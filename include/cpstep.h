@@ -402,14 +402,17 @@ CPSTEP_API int cpstep_ctx_set_graph(cpstep_ctx* ctx, int enable);
  *       Stockham (0) where both exist;  [1] state plane passes: blocks about
  *       this many times the SM count;  [2] EES plane kernels: the same;
  *   [3] PairCalc overlap split-K: CTAs about this many times the SM count;
- *   [4] mixed contexts: tensor-core products (1) or FP64 (0).
+ *   [4] mixed contexts: tensor-core products (1) or FP64 (0);
+ *   [5] mixed contexts on the tensor cores: the EES non-local pass in G space
+ *       (1: its grid sums by Parseval as tensor-core products with separable
+ *       B-spline transforms) or through the NL-grid FFTs (0).
  * cpstep_autotune times the candidates of each choice on the caller's psi
  * (device, nstates x npts) and occ with CUDA events and keeps the fastest;
  * ms (may be NULL, CPSTEP_NTUNE doubles) receives the best time (ms) per
  * choice.  Synchronises the stream; uses scratch of about one psi.
  * Choices change results by rounding only; get/set reproduce a tuned run.
  */
-#define CPSTEP_NTUNE 5
+#define CPSTEP_NTUNE 6
 CPSTEP_API int cpstep_tune_get(const cpstep_ctx* ctx, int* vals, int n);
 CPSTEP_API int cpstep_tune_set(cpstep_ctx* ctx, const int* vals, int n);
 CPSTEP_API int cpstep_autotune(cpstep_ctx* ctx, const double* d_psi, const double* d_occ,

@@ -299,24 +299,25 @@ class StepContext:
         """Mixed contexts: overlap / back-multiply on the tensor cores (split BF16) or in FP64."""
         _lib.call("cpstep_set_gemm_path", self._h, 1 if tensor_cores else 0)
 
-    TUNE_NAMES = ("plane_shfl", "plane_waves", "nl_blocks", "pc_split", "tensor_cores")
+    TUNE_NAMES = ("plane_shfl", "plane_waves", "nl_blocks", "pc_split", "tensor_cores",
+                  "ees_gspace")
 
     def tune_get(self):
-        v = (ctypes.c_int * 5)()
-        _lib.call("cpstep_tune_get", self._h, v, 5)
+        v = (ctypes.c_int * 6)()
+        _lib.call("cpstep_tune_get", self._h, v, 6)
         return dict(zip(self.TUNE_NAMES, list(v)))
 
     def tune_set(self, choices):
         cur = self.tune_get()
         cur.update(choices)
-        v = (ctypes.c_int * 5)(*[int(cur[k]) for k in self.TUNE_NAMES])
-        _lib.call("cpstep_tune_set", self._h, v, 5)
+        v = (ctypes.c_int * 6)(*[int(cur[k]) for k in self.TUNE_NAMES])
+        _lib.call("cpstep_tune_set", self._h, v, 6)
 
     def autotune(self, psi, occ):
         """Time the launch choices on psi/occ and keep the fastest; returns
         (choices, best ms per choice)."""
         self._sync_stream()
-        ms = (ctypes.c_double * 5)()
+        ms = (ctypes.c_double * 6)()
         _lib.call("cpstep_autotune", self._h, ptr(psi), ptr(occ), ms)
         return self.tune_get(), dict(zip(self.TUNE_NAMES, list(ms)))
 

@@ -161,6 +161,22 @@ struct NlData {
   NlVal* tval = nullptr;
   std::vector<size_t> tab_off;
   std::vector<int> tab_cap;
+  // G-space evaluation of the same sums (mixed contexts on the tensor cores,
+  // ees_gspace_run): per atom separable transforms, S matrices (FP32) of each
+  // type [v][atom of type][ld_s], each type's channels with contiguous dyp
+  int km = 0;                       // largest |k| of the state sphere on an axis
+  double2* sep = nullptr;           // [natm][3][2][2 km + 1]
+  float* sv = nullptr;              // per type at sv_off[t]
+  long long ld_s = 0;               // floats per S row (2 npts rounded up to 4)
+  std::vector<long long> sv_off;
+  std::vector<std::vector<int>> tch;  // channels of each type, in channel order
+  std::vector<double2*> tdyp;       // [nch_t][npts] per type
+  int* d_order = nullptr;           // atom of each type-order rank
+  int* d_tch = nullptr;             // [ntyp][4] channel indices (-1 unused)
+  double* d_vn = nullptr;           // [nchan] vnorm / vol
+  double* csum = nullptr;           // sums of one type [nch 4 natm_t][nstates]
+  double* zt = nullptr;             // scaled Z of one type [nstates][ldz]
+  int gspace_ok = 0;                // every type has at most 4 channels
 };
 
 template <typename T>
@@ -267,6 +283,8 @@ struct cpstep_ctx {
     int plane_waves = 3;  // state plane passes: blocks ~ plane_waves x SMs
     int nl_blocks = 6;    // EES plane kernels: blocks ~ nl_blocks x SMs
     int pc_split = 1;     // PairCalc overlap split-K: CTAs ~ pc_split x SMs
+    int ees_gspace = 1;   // mixed contexts on the tensor cores: EES in G space (1) or
+                          // through the NL-grid FFTs (0)
   } tune;
   int use_graph = 1;
   int graph_warm = 0;              // a direct step with gkey ran
@@ -340,6 +358,10 @@ int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
 void graph_drop(cpstep_ctx* c);
 int pc_part_reserve(cpstep_ctx* c, size_t elems);
 int split_reserve(cpstep_ctx* c, size_t bytes);
+int ees_tc_sums(cpstep_ctx* c, const double* psi, const float* sv, long long ld_s,
+                const double2* dyp, int nch, int jp, double* C, int ldc);
+int ees_tc_force(cpstep_ctx* c, const float* sv, long long ld_s, const double2* dyp, int nch,
+                 int natm_t, const double* Z, int ldz, double alpha, double* fpsi);
 int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
                             double* C, int ldc, int sym);
 // paircalc_tc.cu (tensor-core products; *used = false when the SIMT path must run)

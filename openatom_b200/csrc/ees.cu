@@ -203,6 +203,126 @@ k_nl_table(NlAtoms A, int nkf, TabDims d, int* __restrict__ tcell, NlVal* __rest
   }
 }
 
+// ---------------------------------------------------------------------------
+// G-space evaluation of the same sums (mixed contexts, tensor cores).  With
+// F(r) the C2R transform of proj = conj(dyp psi), Parseval turns the grid sums
+// of an atom's stencil into sums over the packed points:
+//   sum_r M(r) F(r) = sum_p wpt_p Re(proj(p) S(p)),   S(p) = s_a(kx) s_b(ky) s_c(kz),
+//   s_d(k) = sum_j M_d[j] exp(-2 pi i k ig_d[j] / nkf)
+// (the B-spline factors of eesAtmBsplineRgrp), and the scatter + R2C of the
+// psi force into pg(p) = sum_atoms zs conj(S(p)).  The dMn sums take the
+// derivative factors in one axis at a time, combined with hmati as nl_point
+// does.
+
+// separable transforms [atom][axis][Mn, dMn][k + km], k in [-km, km]
+__global__ void k_ees_sep(const int* __restrict__ ig, const double* __restrict__ mn,
+                          const double* __restrict__ dmn, int natm, int nkf, int km,
+                          double2* __restrict__ sep) {
+  const int nk = 2 * km + 1;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)natm * 6 * nk) return;
+  const int kk = (int)(i % nk);
+  const long long rest = i / nk;
+  const int m = (int)(rest % 2), d = (int)((rest / 2) % 3), a = (int)(rest / 6);
+  const int k = kk - km;
+  const int* g = ig + ((size_t)a * 3 + d) * kNlInterp;
+  const double* f = (m ? dmn : mn) + ((size_t)a * 3 + d) * kNlInterp;
+  double re = 0.0, im = 0.0;
+#pragma unroll
+  for (int j = 0; j < kNlInterp; ++j) {
+    long long t = ((long long)k * g[j]) % nkf;
+    if (t < 0) t += nkf;
+    double sn, cs;
+    sincospi(2.0 * (double)t / (double)nkf, &sn, &cs);
+    re += f[j] * cs;
+    im -= f[j] * sn;
+  }
+  sep[i] = make_double2(re, im);
+}
+
+struct TypeDims {
+  int tstart[CPSTEP_MAX_TYPES + 1];
+  long long svoff[CPSTEP_MAX_TYPES];
+};
+
+__device__ __forceinline__ double2 cm(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// S matrices: rows v natm_t + a (v = Mn, d/dx, d/dy, d/dz) of each type, FP32
+// complex per packed point.  One block row per atom.
+__global__ void k_ees_smat(const double2* __restrict__ sep, const int* __restrict__ kx,
+                           const int* __restrict__ ky, const int* __restrict__ kz, int npts,
+                           int km, const int* __restrict__ typ, const int* __restrict__ rank,
+                           TypeDims td, NlAtoms A, long long ld_s, float* __restrict__ sv) {
+  const int a = blockIdx.y;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const int t = typ[a];
+  const int nt = td.tstart[t + 1] - td.tstart[t], al = rank[a] - td.tstart[t];
+  const int nk = 2 * km + 1;
+  const double2* T = sep + (size_t)a * 6 * nk;
+  const int ix = kx[p] + km, iy = ky[p] + km, iz = kz[p] + km;
+  const double2 sa = T[0 * nk + ix], da = T[1 * nk + ix];
+  const double2 sb = T[2 * nk + iy], db = T[3 * nk + iy];
+  const double2 sc = T[4 * nk + iz], dc = T[5 * nk + iz];
+  const double2 sbc = cm(sb, sc);
+  const double2 S = cm(sa, sbc);
+  const double2 at = cm(da, sbc), bt = cm(sa, cm(db, sc)), ct = cm(cm(sa, sb), dc);
+  const double* h = A.hmati;
+  const double g = A.grid;
+  double2 out[4];
+  out[0] = S;
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    const double h0 = h[3 * v] * g, h1 = h[3 * v + 1] * g, h2 = h[3 * v + 2] * g;
+    out[v + 1] = make_double2(at.x * h0 + bt.x * h1 + ct.x * h2, at.y * h0 + bt.y * h1 + ct.y * h2);
+  }
+  float* base = sv + td.svoff[t];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    float2* o = reinterpret_cast<float2*>(base + (size_t)(v * nt + al) * ld_s) + p;
+    *o = make_float2((float)out[v].x, (float)out[v].y);
+  }
+}
+
+// Z, E_NL, scaled Z and atom forces of one type from its G-space sums
+// C(s, ch jp + v nt + a) (column-major, ld = nstates): as k_nl_zmat.
+__global__ void k_ees_zglue(const double* __restrict__ C, int nstates, int nt, int nch,
+                            const int* __restrict__ chan, const double* __restrict__ vnc,
+                            const int* __restrict__ order, int t0, int natm,
+                            const double* __restrict__ occ, double* __restrict__ zt, int ldz,
+                            double* __restrict__ enl_s, double* __restrict__ fnl) {
+  __shared__ double red[32];
+  const int s = blockIdx.x;
+  const double w = occ[s];
+  const int jp = 4 * nt;
+  double e = 0.0;
+  for (int al = threadIdx.x; al < nt; al += blockDim.x) {
+    const int atom = order[t0 + al];
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+    for (int ch = 0; ch < nch; ++ch) {
+      const double vn = vnc[chan[ch]];
+      const double* cc = C + ((size_t)ch * jp + al) * nstates + s;
+      const double z = cc[0];
+      const double dx = cc[(size_t)nt * nstates], dy = cc[(size_t)2 * nt * nstates];
+      const double dz = cc[(size_t)3 * nt * nstates];
+      e += z * z * vn * w;
+      const double zsc = z * (2.0 * vn * w);
+      zt[(size_t)s * ldz + ch * nt + al] = zsc;
+      f0 -= dx * zsc;
+      f1 -= dy * zsc;
+      f2 -= dz * zsc;
+    }
+    double* f = fnl + ((size_t)s * natm + atom) * 3;
+    f[0] += f0;
+    f[1] += f1;
+    f[2] += f2;
+  }
+  e = block_sum(e, red);
+  if (threadIdx.x == 0) enl_s[s] += e;
+}
+
 // Z_a = sum over the atom's planes, E_NL += Z^2 vn occ, Z <- 2 vn occ Z,
 // F_a -= Z sum P dMn (eesEnergyAtmForcRchare :1545-1560, :1596-1600).
 // One block per state; atoms of the channel's type.
@@ -314,6 +434,12 @@ void nl_free(cpstep_ctx* c) {
   cudaFree(n.dmn); cudaFree(n.zpart); cudaFree(n.zs); cudaFree(n.enl_s); cudaFree(n.fnl);
   cudaFree(n.tcell); cudaFree(n.tval); cudaFree(n.gcell); cudaFree(n.goff); cudaFree(n.gent);
   cudaFree(n.gcount);
+  cudaFree(n.sep); cudaFree(n.sv); cudaFree(n.d_order); cudaFree(n.d_tch); cudaFree(n.d_vn);
+  cudaFree(n.csum); cudaFree(n.zt);
+  for (auto d : n.tdyp) cudaFree(d);
+  n.tdyp.clear();
+  n.sep = nullptr; n.sv = nullptr; n.d_order = nullptr; n.d_tch = nullptr; n.d_vn = nullptr;
+  n.csum = nullptr; n.zt = nullptr; n.gspace_ok = 0;
   cudaFree(n.plist); cudaFree(n.pcount);
   n = NlData();
 }
@@ -488,7 +614,100 @@ int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, 
   CPSTEP_CUDA_TRY(cudaMalloc(&n.gent, sizeof(int) * tot1));
   CPSTEP_CUDA_TRY(cudaMalloc(&n.goff, sizeof(int) * (tot + (size_t)at.ntyp * nkf)));
   CPSTEP_CUDA_TRY(cudaMalloc(&n.gcount, sizeof(int) * (size_t)at.ntyp * nkf));
+  // G-space form (mixed contexts): channels per type, S matrices, scratch
+  n.km = km;
+  n.tch.assign(at.ntyp, {});
+  for (int k = 0; k < nchan; ++k) n.tch[ch_type[k]].push_back(k);
+  n.gspace_ok = c->precision == CPSTEP_PREC_MIXED;
+  for (int t = 0; t < at.ntyp; ++t) n.gspace_ok = n.gspace_ok && n.tch[t].size() <= 4;
+  if (n.gspace_ok) {
+    n.ld_s = (long long)((2 * (size_t)c->npts + 3) / 4 * 4);
+    n.sv_off.assign(at.ntyp, 0);
+    long long tot = 0;
+    size_t csz = 1, zsz = 1;
+    for (int t = 0; t < at.ntyp; ++t) {
+      const int nt = at.tstart[t + 1] - at.tstart[t];
+      n.sv_off[t] = tot;
+      tot += 4LL * nt * n.ld_s;
+      csz = std::max(csz, (size_t)n.tch[t].size() * 4 * nt * c->nstates);
+      zsz = std::max(zsz, (size_t)c->nstates * (((size_t)n.tch[t].size() * nt + 1) / 2 * 2));
+    }
+    CPSTEP_CUDA_TRY(cudaMalloc(&n.sv, sizeof(float) * (size_t)std::max(tot, 4LL)));
+    CPSTEP_CUDA_TRY(cudaMemset(n.sv, 0, sizeof(float) * (size_t)std::max(tot, 4LL)));
+    CPSTEP_CUDA_TRY(cudaMalloc(&n.sep, sizeof(double2) * na * 6 * (2 * (size_t)km + 1)));
+    CPSTEP_CUDA_TRY(cudaMalloc(&n.csum, sizeof(double) * csz));
+    CPSTEP_CUDA_TRY(cudaMalloc(&n.zt, sizeof(double) * zsz));
+    n.tdyp.assign(at.ntyp, nullptr);
+    std::vector<int> htch((size_t)at.ntyp * 4, -1);
+    for (int t = 0; t < at.ntyp; ++t) {
+      const size_t nc = n.tch[t].size();
+      if (!nc) continue;
+      CPSTEP_CUDA_TRY(cudaMalloc(&n.tdyp[t], sizeof(double2) * nc * c->npts));
+      for (size_t k = 0; k < nc; ++k) {
+        htch[(size_t)t * 4 + k] = n.tch[t][k];
+        CPSTEP_CUDA_TRY(cudaMemcpy(n.tdyp[t] + k * c->npts, n.dyp + (size_t)n.tch[t][k] * c->npts,
+                                   sizeof(double2) * c->npts, cudaMemcpyDeviceToDevice));
+      }
+    }
+    CPSTEP_CUDA_TRY(cudaMalloc(&n.d_tch, sizeof(int) * htch.size()));
+    CPSTEP_CUDA_TRY(cudaMemcpy(n.d_tch, htch.data(), sizeof(int) * htch.size(),
+                               cudaMemcpyHostToDevice));
+    CPSTEP_CUDA_TRY(cudaMalloc(&n.d_vn, sizeof(double) * nchan));
+    CPSTEP_CUDA_TRY(cudaMemcpy(n.d_vn, n.ch_vn.data(), sizeof(double) * nchan,
+                               cudaMemcpyHostToDevice));
+    std::vector<int> hrank(na), horder(na);
+    CPSTEP_CUDA_TRY(cudaMemcpy(hrank.data(), at.rank, sizeof(int) * na, cudaMemcpyDeviceToHost));
+    for (int a = 0; a < (int)na; ++a) horder[hrank[a]] = a;
+    CPSTEP_CUDA_TRY(cudaMalloc(&n.d_order, sizeof(int) * na));
+    CPSTEP_CUDA_TRY(cudaMemcpy(n.d_order, horder.data(), sizeof(int) * na,
+                               cudaMemcpyHostToDevice));
+  }
   n.on = 1;
+  return CPSTEP_OK;
+}
+
+// The EES pass in G space (see k_ees_sep): per type, the forward sums as one
+// tensor-core product of psi with conj(dyp) S, the glue, and the psi force as
+// one back-multiply with the same matrix.
+static int ees_gspace_run(cpstep_ctx* c, const double* psi, const double* occ, double* fpsi,
+                          double* energies, double* fatm) {
+  NlData& n = c->nl;
+  const int S = c->nstates, natm = n.natm, ntyp = c->atoms.ntyp;
+  ees::k_nl_bspline<<<cdiv(natm, 128), 128, 0, c->stream>>>(c->atoms.frac, natm, n.nkf, n.ig,
+                                                            n.mn, n.dmn);
+  CPSTEP_LAUNCH_CHECK();
+  const long long nsep = (long long)natm * 6 * (2 * n.km + 1);
+  ees::k_ees_sep<<<(unsigned)((nsep + 255) / 256), 256, 0, c->stream>>>(n.ig, n.mn, n.dmn, natm,
+                                                                         n.nkf, n.km, n.sep);
+  CPSTEP_LAUNCH_CHECK();
+  ees::TypeDims td{};
+  for (int t = 0; t <= ntyp; ++t) td.tstart[t] = c->atoms.tstart[t];
+  for (int t = 0; t < ntyp; ++t) td.svoff[t] = n.sv_off[t];
+  NlAtoms A{};
+  for (int k = 0; k < 9; ++k) A.hmati[k] = c->hmati[k];
+  A.grid = (double)n.nkf;
+  ees::k_ees_smat<<<dim3(cdiv(c->npts, 256), natm), 256, 0, c->stream>>>(
+      n.sep, c->d_kx, c->d_ky, c->d_kz, c->npts, n.km, c->atoms.typ, c->atoms.rank, td, A,
+      n.ld_s, n.sv);
+  CPSTEP_LAUNCH_CHECK();
+  CPSTEP_CUDA_TRY(cudaMemsetAsync(n.enl_s, 0, sizeof(double) * S, c->stream));
+  CPSTEP_CUDA_TRY(cudaMemsetAsync(n.fnl, 0, sizeof(double) * S * natm * 3, c->stream));
+  for (int t = 0; t < ntyp; ++t) {
+    const int nch = (int)n.tch[t].size();
+    const int nt = c->atoms.tstart[t + 1] - c->atoms.tstart[t];
+    if (!nch || !nt) continue;
+    const float* sv = n.sv + n.sv_off[t];
+    if (int rc = ees_tc_sums(c, psi, sv, n.ld_s, n.tdyp[t], nch, 4 * nt, n.csum, S)) return rc;
+    const int ldz = (nch * nt + 1) / 2 * 2;
+    ees::k_ees_zglue<<<S, 128, 0, c->stream>>>(n.csum, S, nt, nch, n.d_tch + 4 * t, n.d_vn,
+                                                n.d_order, c->atoms.tstart[t], natm, occ, n.zt,
+                                                ldz, n.enl_s, n.fnl);
+    CPSTEP_LAUNCH_CHECK();
+    if (int rc = ees_tc_force(c, sv, n.ld_s, n.tdyp[t], nch, nt, n.zt, ldz, -1.0, fpsi)) return rc;
+  }
+  ees::k_nl_finish<<<cdiv(std::max(1, 3 * natm), 128), 128, 0, c->stream>>>(
+      n.enl_s, n.fnl, S, natm, energies, fatm);
+  CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }
 
@@ -503,6 +722,8 @@ int nl_run(cpstep_ctx* c, const double* psi, const double* occ, double* fpsi, do
     cpstep_set_error("ees_nonlocal: atoms changed since cpstep_set_nonlocal");
     return CPSTEP_ERR_STATE;
   }
+  if (n.gspace_ok && c->precision == CPSTEP_PREC_MIXED && c->tc_ok && c->tune.ees_gspace)
+    return ees_gspace_run(c, psi, occ, fpsi, energies, fatm);
   const int S = c->nstates, natm = n.natm;
   ees::k_nl_bspline<<<cdiv(natm, 128), 128, 0, c->stream>>>(c->atoms.frac, natm, n.nkf, n.ig,
                                                             n.mn, n.dmn);

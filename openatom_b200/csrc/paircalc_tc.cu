@@ -59,10 +59,18 @@ struct Cfg {
   static constexpr int RSP = ROWS + 2;                   // row stride of a [KC][128] stage
   static constexpr int LVB = KS * TILE_B;                // one level of one operand
   static constexpr int OPB = NLV * LVB;                  // one operand of one chunk
-  static constexpr int RAW_A = MODE == 0 ? ROWS * RS * 8 : KC * RSP * 8;
-  static constexpr int RAW_B = ROWS * RS * 8;
-  static constexpr int WST = MODE == 0 ? KC / 2 * 8 : 0;     // point weights of the chunk
-  static constexpr int RAW = RAW_A + (NLD == 2 ? RAW_B : 0) + WST;  // one stage
+  // EES (MODE 2, 3): FP32 complex S rows (stride RSF / RSPF floats) and the
+  // channels' projector values dyp (double2) staged beside them
+  static constexpr int RSF = KC + 4;                     // [rows][KC] floats
+  static constexpr int RSPF = ROWS + 4;                  // [KC][128] floats
+  static constexpr int DYP2 = 4 * (KC / 2) * 16;         // MODE 2: 4 channels x KC/2 points
+  static constexpr int DYP3 = 4 * (ROWS / 2) * 16;       // MODE 3: 4 channels x 64 points
+  static constexpr int RAW_A = (MODE == 0 || MODE == 2) ? ROWS * RS * 8
+                               : MODE == 1 ? KC * RSP * 8 : KC * RSPF * 4 + DYP3;
+  static constexpr int RAW_B = MODE == 2 ? ROWS * RSF * 4 + DYP2 : ROWS * RS * 8;
+  static constexpr int WST = (MODE == 0 || MODE == 2) ? KC / 2 * 8 : 0;  // point weights
+  static constexpr int WOFF = RAW_A + (NLD == 2 ? RAW_B : 0);      // weights in a stage
+  static constexpr int RAW = WOFF + WST;                            // one stage
   static constexpr int BF = 2 * 2 * OPB;                 // two chunk buffers, A and B
   static constexpr int BYTES = 1024 + BF + NST * RAW;    // + alignment slack
   static_assert(KC % 16 == 0 && 128 % KC == 0, "chunk");
@@ -85,6 +93,19 @@ struct Args {
   double* part;      // overlap partial tiles [nsplit][N][M] (column-major, ld = M)
   double* out;       // backmul output [nout][ldo]
   int ldo;
+  // EES (MODE 2: forward sums, MODE 3: psi force), one atom type:
+  //   sv: S rows of the type, row j at sv + j ld_s (floats, complex pairs per
+  //       point); MODE 2 pairs j = v natm_t + a (v = Mn, d/dx, d/dy, d/dz),
+  //       MODE 3 rows a < natm_t (Mn)
+  //   dyp: the type's nch channel projectors, channel c at dyp + c ld_d
+  //   MODE 2: B-tile rows c jt + jj (c < nch, jj < jt) = channel c x pair
+  //           t jt + jj, jp pairs; output column c jp + j
+  //   MODE 3: inner index j = c natm_t + a (nin = nch natm_t)
+  const float* sv;
+  long long ld_s;
+  const double2* dyp;
+  int ld_d;
+  int nch, jt, jp, natm_t;
   double alpha, beta;
   int* err;
 };
@@ -110,9 +131,9 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   int r0, c0, kbeg, kend;
-  if (MODE == 0) {
+  if (MODE == 0 || MODE == 2) {
     r0 = blockIdx.x * ROWS;
-    c0 = blockIdx.y * ROWS;
+    c0 = blockIdx.y * (MODE == 2 ? p.jt : ROWS);  // MODE 2: first pair of the B tile
     kbeg = blockIdx.z * p.kslab;
     kend = min(p.K, kbeg + p.kslab);
   } else {
@@ -142,9 +163,9 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
   auto load = [&](int ch, int st) {
     const int k0 = kbeg + ch * KC;
     double* ra = raw + (size_t)st * (C::RAW / 8);
-    if (MODE == 0) {
+    if (MODE == 0 || MODE == 2) {
 #pragma unroll
-      for (int op = 0; op < NLD; ++op) {
+      for (int op = 0; op < (MODE == 2 ? 1 : NLD); ++op) {
         const double* src = op == 0 ? p.A : p.B;
         const int ld = op == 0 ? p.lda : p.ldb;
         const int rr0 = op == 0 ? r0 : c0, nr = op == 0 ? p.M : p.N;
@@ -152,7 +173,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
         if (op == 0 && p.w && tid < KC / 4) {  // weights of points k0/2 .. (k0 + KC)/2
           const int pt = (k0 >> 1) + 2 * tid;
           const int nb = 2 * pt + 2 < kend ? 16 : (2 * pt < kend ? 8 : 0);
-          tc::cp16(ra + (C::RAW - C::WST) / 8 + 2 * tid, nb ? p.w + pt : p.w, nb);
+          tc::cp16(ra + C::WOFF / 8 + 2 * tid, nb ? p.w + pt : p.w, nb);
         }
 #pragma unroll
         for (int it = 0; it < ROWS * (KC / 2) / NTHR; ++it) {
@@ -163,6 +184,58 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
           const double* g = ok ? src + (size_t)(rr0 + r) * ld + k : src;
           tc::cp16(dst + r * RS + 2 * pc, g, ok ? 16 : 0);
         }
+      }
+      if (MODE == 2) {
+        // B: S rows of pairs c0 .. c0 + jt, KC reals (FP32), and dyp of the chunk's points
+        float* fs = reinterpret_cast<float*>(ra + C::RAW_A / 8);
+        for (int q = tid; q < p.jt * (KC / 4); q += NTHR) {
+          const int jj = q / (KC / 4), pc = q % (KC / 4);
+          const int j = c0 + jj, k = k0 + 4 * pc;
+          const bool ok = j < p.jp && k < kend;  // kend even, rows padded to 4 floats
+          const float* g = ok ? p.sv + (size_t)j * p.ld_s + k : p.sv;
+          tc::cp16(fs + jj * C::RSF + 4 * pc, g, ok ? 16 : 0);
+        }
+        double2* dd = reinterpret_cast<double2*>(fs + ROWS * C::RSF);
+        for (int q = tid; q < p.nch * (KC / 2); q += NTHR) {
+          const int c = q / (KC / 2), e = q % (KC / 2);
+          const int pt = (k0 >> 1) + e;
+          const bool ok = 2 * pt < kend;
+          tc::cp16(dd + c * (KC / 2) + e, ok ? p.dyp + (size_t)c * p.ld_d + pt : p.dyp,
+                   ok ? 16 : 0);
+        }
+      }
+    } else if (MODE == 3) {
+      // A: S rows (Mn) of the chunk's inner indices j = c natm_t + a over the
+      // tile's 64 points, and the channels' dyp over the same points
+      float* fs = reinterpret_cast<float*>(ra);
+#pragma unroll
+      for (int it = 0; it < KC * (ROWS / 4) / NTHR; ++it) {
+        const int q = tid + NTHR * it;
+        const int jj = q / (ROWS / 4), pc = q % (ROWS / 4);
+        const int j = k0 + jj, pr = r0 + 4 * pc;  // reals
+        const bool ok = j < kend && pr < p.M;      // M reals, rows padded to 4 floats
+        const int a = ok ? j % p.natm_t : 0;
+        const float* g = ok ? p.sv + (size_t)a * p.ld_s + pr : p.sv;
+        tc::cp16(fs + jj * C::RSPF + 4 * pc, g, ok ? 16 : 0);
+      }
+      double2* dd = reinterpret_cast<double2*>(fs + KC * C::RSPF);
+      for (int q = tid; q < p.nch * (ROWS / 2); q += NTHR) {
+        const int c = q / (ROWS / 2), e = q % (ROWS / 2);
+        const int pt = (r0 >> 1) + e;
+        const bool ok = 2 * pt < p.M;
+        tc::cp16(dd + c * (ROWS / 2) + e, ok ? p.dyp + (size_t)c * p.ld_d + pt : p.dyp,
+                 ok ? 16 : 0);
+      }
+      // B: M(j, i) = Mcm[j + i ldm], rows i = c0 .. c0 + 128, j pairs
+      double* rb = ra + C::RAW_A / 8;
+#pragma unroll
+      for (int it = 0; it < ROWS * (KC / 2) / NTHR; ++it) {
+        const int q = tid + NTHR * it;
+        const int r = q / (KC / 2), pc = q % (KC / 2);
+        const int i = c0 + r, j = k0 + 2 * pc;
+        const int nb = (i < p.N && j < kend) ? (j + 1 < kend ? 16 : 8) : 0;
+        const double* g = nb ? p.B + (size_t)i * p.ldb + j : p.B;
+        tc::cp16(rb + r * RS + 2 * pc, g, nb);
       }
     } else {
       // A: in[j][p] rows j = k0 .. k0 + KC, 128 points from r0
@@ -229,6 +302,39 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
       put(dA, off, x, one);
       return;
     }
+    if (MODE == 3 && op == 0) {  // A[p][j] = (conj(dyp_c) S_a)(point r / 2), re or im
+      const float* fs = reinterpret_cast<const float*>(ra);
+      const double2* dd = reinterpret_cast<const double2*>(fs + KC * C::RSPF);
+      const int pl = r >> 1;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int j = k0 + 8 * u + e;
+        const int c = min(j / p.natm_t, 3);
+        const float2 sa = *reinterpret_cast<const float2*>(fs + (8 * u + e) * C::RSPF + 2 * pl);
+        const double2 d = dd[c * (ROWS / 2) + pl];
+        x[e] = (r & 1) ? d.x * (double)sa.y - d.y * (double)sa.x
+                       : d.x * (double)sa.x + d.y * (double)sa.y;
+      }
+      put(dA, off, x, one);
+      return;
+    }
+    if (MODE == 2 && op == 1) {  // B row r = channel c, pair jj: conj(dyp_c) S_pair
+      const float* fs = reinterpret_cast<const float*>(ra + C::RAW_A / 8);
+      const double2* dd = reinterpret_cast<const double2*>(fs + ROWS * C::RSF);
+      const int c = r / p.jt, jj = r - c * p.jt;
+      const bool ok = c < p.nch;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float2 sa =
+            ok ? *reinterpret_cast<const float2*>(fs + jj * C::RSF + 8 * u + 2 * e)
+               : make_float2(0.f, 0.f);
+        const double2 d = ok ? dd[c * (KC / 2) + 4 * u + e] : make_double2(0.0, 0.0);
+        x[2 * e] = d.x * (double)sa.x + d.y * (double)sa.y;
+        x[2 * e + 1] = d.x * (double)sa.y - d.y * (double)sa.x;
+      }
+      put(dB, off, x, one);
+      return;
+    }
     const double2* s2 =
         reinterpret_cast<const double2*>(ra + op * (C::RAW_A / 8) + r * RS + 8 * u);
 #pragma unroll
@@ -237,11 +343,13 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
       x[2 * e] = v.x;
       x[2 * e + 1] = v.y;
     }
-    if (MODE == 1) {  // B[i][j] = M(j, i), its diagonal left to the epilogue
-      const int d = (c0 + r) - (k0 + 8 * u);
+    if (MODE == 1 || MODE == 3) {  // B[i][j] = M(j, i); MODE 1: diagonal left to the epilogue
+      if (MODE == 1) {
+        const int d = (c0 + r) - (k0 + 8 * u);
 #pragma unroll
-      for (int e = 0; e < 8; ++e)
-        if (e == d) x[e] = 0.0;
+        for (int e = 0; e < 8; ++e)
+          if (e == d) x[e] = 0.0;
+      }
       put(dB, off, x, one);
       return;
     }
@@ -251,7 +359,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
     }
     float ws[4] = {1.f, 1.f, 1.f, 1.f};
     if (p.w) {  // staged with the chunk (zero past the end, where x is zero too)
-      const double2* w2 = reinterpret_cast<const double2*>(ra + (C::RAW - C::WST) / 8 + 4 * u);
+      const double2* w2 = reinterpret_cast<const double2*>(ra + C::WOFF / 8 + 4 * u);
       const double2 wa = w2[0], wb = w2[1];
       ws[0] = (float)wa.x;
       ws[1] = (float)wa.y;
@@ -386,6 +494,16 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
         if (c < p.N) P[(size_t)c * p.M + r] = (same && cb + e == rl) ? diag_s[rl] : acc[e];
       }
     }
+  } else if (MODE == 2) {  // tile column cb + e = channel ch, pair c0 + jj -> ch jp + pair
+    double* P = p.part + (size_t)blockIdx.z * p.M * p.N;
+    const int r = r0 + rl;
+    if (r < p.M) {
+#pragma unroll
+      for (int e = 0; e < 32; ++e) {
+        const int ch = (cb + e) / p.jt, j = c0 + (cb + e) - ch * p.jt;
+        if (ch < p.nch && j < p.jp) P[(size_t)(ch * p.jp + j) * p.M + r] = acc[e];
+      }
+    }
   } else {
     const int pt = r0 + rl;
     if (pt < p.M) {
@@ -395,7 +513,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
         const int i = c0 + cb + e;
         if (i < p.N) {
           double v = acc[e];
-          if (i < p.nin) v = fma(p.B[(size_t)i * p.ldb + i], p.A[(size_t)i * p.lda + pt], v);
+          if (MODE == 1 && i < p.nin)
+            v = fma(p.B[(size_t)i * p.ldb + i], p.A[(size_t)i * p.lda + pt], v);
           double* o = p.out + (size_t)i * p.ldo + pt;
           *o = p.beta == 0.0 ? sc * v : fma(p.beta, *o, sc * v);
         }
@@ -428,6 +547,70 @@ constexpr int KC_ONE = 32, NST_ONE = 3, KC_TWO = 16, NST_TWO = 4;
 inline bool al16(const void* q) { return ((uintptr_t)q & 15) == 0; }
 
 }  // namespace pctc
+
+// EES sums of one atom type (MODE 2): C(s, ch jp + j) = sum_p wpt Re(conj psi_s
+// conj(dyp_ch) S_j), j < jp pairs; C column-major [nch jp][ldc], alpha = 1.
+int ees_tc_sums(cpstep_ctx* c, const double* psi, const float* sv, long long ld_s,
+                const double2* dyp, int nch, int jp, double* C, int ldc) {
+  using namespace pctc;
+  const int S = c->nstates, K = 2 * c->npts;
+  if (nch < 1 || nch > 4 || (ld_s & 3) || !al16(sv) || !al16(psi)) return CPSTEP_ERR_ARG;
+  const int jt = ROWS / nch;
+  const int tm = cdiv(S, ROWS), tn = cdiv(jp, jt);
+  const int want = std::max(1, c->tune.pc_split * c->num_sms / (tm * tn));
+  const int kslab = cdiv(cdiv(K, want), 128) * 128;
+  const int nsplit = cdiv(K, kslab);
+  const int N = nch * jp;
+  if (int rc = pc_part_reserve(c, (size_t)nsplit * S * N)) return rc;
+  Args p{};
+  p.A = psi;
+  p.lda = K;
+  p.w = c->d_wpt;
+  p.M = S;
+  p.N = N;
+  p.K = K;
+  p.kslab = kslab;
+  p.part = c->d_pc_part;
+  p.err = c->d_dev_err;
+  p.sv = sv;
+  p.ld_s = ld_s;
+  p.dyp = dyp;
+  p.ld_d = c->npts;
+  p.nch = nch;
+  p.jt = jt;
+  p.jp = jp;
+  if (int rc = launch<2, 2, NST_TWO, KC_TWO>(c->stream, dim3(tm, tn, nsplit), p)) return rc;
+  return pc_splitk_reduce_launch(c, nsplit, S, N, 1.0, 0.0, C, ldc, 0);
+}
+
+// EES psi force of one atom type (MODE 3): fpsi_s(p) += alpha wpt(p) sum_j
+// Z(j, s) (conj(dyp_c) S_a)(p), j = c natm_t + a; Z column-major [S][ldz].
+int ees_tc_force(cpstep_ctx* c, const float* sv, long long ld_s, const double2* dyp, int nch,
+                 int natm_t, const double* Z, int ldz, double alpha, double* fpsi) {
+  using namespace pctc;
+  const int S = c->nstates, K = 2 * c->npts;
+  if (nch < 1 || nch > 4 || (ld_s & 3) || (ldz & 1) || !al16(sv) || !al16(Z)) return CPSTEP_ERR_ARG;
+  Args p{};
+  p.B = Z;
+  p.ldb = ldz;
+  p.w = c->d_wpt;
+  p.M = K;
+  p.N = S;
+  p.K = K;
+  p.nin = nch * natm_t;
+  p.out = fpsi;
+  p.ldo = K;
+  p.alpha = alpha;
+  p.beta = 1.0;
+  p.err = c->d_dev_err;
+  p.sv = sv;
+  p.ld_s = ld_s;
+  p.dyp = dyp;
+  p.ld_d = c->npts;
+  p.nch = nch;
+  p.natm_t = natm_t;
+  return launch<3, 2, NST_TWO, KC_TWO>(c->stream, dim3(cdiv(K, ROWS), cdiv(S, ROWS)), p);
+}
 
 // The tensor-core path takes 16-byte aligned operands with even leading
 // dimensions and even K (every row segment a whole number of 16-byte pieces),

@@ -78,13 +78,15 @@ int cpstep_tune_get(const cpstep_ctx* c, int* vals, int n) {
   vals[2] = c->tune.nl_blocks;
   vals[3] = c->tune.pc_split;
   vals[4] = c->tc_ok;
+  vals[5] = c->tune.ees_gspace;
   return CPSTEP_OK;
 }
 
 int cpstep_tune_set(cpstep_ctx* c, const int* vals, int n) {
   if (!c || !vals || n < CPSTEP_NTUNE) return CPSTEP_ERR_ARG;
   if ((vals[0] != 0 && vals[0] != 1) || vals[1] < 1 || vals[1] > 64 || vals[2] < 1 ||
-      vals[2] > 64 || vals[3] < 1 || vals[3] > 16 || (vals[4] != 0 && vals[4] != 1))
+      vals[2] > 64 || vals[3] < 1 || vals[3] > 16 || (vals[4] != 0 && vals[4] != 1) ||
+      (vals[5] != 0 && vals[5] != 1))
     return CPSTEP_ERR_ARG;
   if (vals[4] && !c->tc_ok) {
     if (int rc = cpstep_set_gemm_path(c, 1)) return rc;
@@ -95,6 +97,7 @@ int cpstep_tune_set(cpstep_ctx* c, const int* vals, int n) {
   c->tune.nl_blocks = vals[2];
   c->tune.pc_split = vals[3];
   c->tc_ok = vals[4];
+  c->tune.ees_gspace = vals[5];
   return CPSTEP_OK;
 }
 
@@ -114,7 +117,7 @@ int cpstep_autotune(cpstep_ctx* c, const double* d_psi, const double* d_occ, dou
   al(&eke, S);
   al(&smat, (size_t)S * S);
   al(&en, CPSTEP_NENERGY);
-  float ms[CPSTEP_NTUNE] = {0, 0, 0, 0, 0};
+  float ms[CPSTEP_NTUNE] = {0, 0, 0, 0, 0, 0};
   // 1, 2: the state plane passes (density, then V.psi with rho standing in for V)
   auto planes = [&]() -> int {
     if (int r = statefft_density(c, d_psi, d_occ, rho)) return r;
@@ -122,20 +125,23 @@ int cpstep_autotune(cpstep_ctx* c, const double* d_psi, const double* d_occ, dou
   };
   if (!rc) rc = pick(c, &c->tune.shfl, {1, 0}, planes, &ms[0]);
   if (!rc) rc = pick(c, &c->tune.plane_waves, {1, 2, 3, 6}, planes, &ms[1]);
-  // 3: the EES plane kernels
-  if (!rc && c->nl.on) {
-    auto ees = [&]() -> int {
-      CPSTEP_CUDA_TRY(cudaMemsetAsync(force, 0, sizeof(double) * 2 * ncoef, c->stream));
-      return nl_run(c, d_psi, d_occ, force, en, nullptr);
-    };
-    rc = pick(c, &c->tune.nl_blocks, {3, 6, 12}, ees, &ms[2]);
-  }
   // 4, 5: the overlap product S (split-K width; tensor cores or FP64 in a mixed context)
   auto ovl = [&]() -> int {
     return pc_overlap_launch(c, d_psi, d_psi, S, S, 2 * c->npts, c->d_wpt, 1.0, 0.0, smat, S);
   };
   if (!rc) rc = pick(c, &c->tune.pc_split, {1, 2}, ovl, &ms[3]);
   if (!rc && c->precision == CPSTEP_PREC_MIXED && c->tc_ok) rc = pick(c, &c->tc_ok, {1, 0}, ovl, &ms[4]);
+  // 6, 3: the EES pass: G space or NL-grid FFTs (mixed on the tensor cores), then
+  // the FFT path's blocks per SM if it runs
+  if (!rc && c->nl.on) {
+    auto ees = [&]() -> int {
+      CPSTEP_CUDA_TRY(cudaMemsetAsync(force, 0, sizeof(double) * 2 * ncoef, c->stream));
+      return nl_run(c, d_psi, d_occ, force, en, nullptr);
+    };
+    const bool gs = c->nl.gspace_ok && c->precision == CPSTEP_PREC_MIXED && c->tc_ok;
+    if (gs) rc = pick(c, &c->tune.ees_gspace, {1, 0}, ees, &ms[5]);
+    if (!rc && !(gs && c->tune.ees_gspace)) rc = pick(c, &c->tune.nl_blocks, {3, 6, 12}, ees, &ms[2]);
+  }
   if (!rc) rc = cudaStreamSynchronize(c->stream) == cudaSuccess ? CPSTEP_OK : CPSTEP_ERR_CUDA;
   cudaFree(rho);
   cudaFree(force);

@@ -4,8 +4,10 @@ cp_ees_nonlocal.C routines by tests/test_ees_oracle.py).
 
 FP64 path: E_NL to 1e-11 relative, psi force and atom forces to 1e-10 of
 their largest entry.  Mixed path (FP32 NL FFTs, FP64 sums): E_NL to 1e-5
-relative, forces to 1e-5 of their largest entry; inside the step, energy per
-atom <= 1e-6 Ha and atom forces <= 1e-5 Ha/bohr.
+relative, forces to 1e-5 of their largest entry, both for the NL-grid FFT
+form and for the G-space form (the same stencil sums by Parseval, evaluated
+as split-BF16 tensor-core products with the separable B-spline transforms);
+inside the step, energy per atom <= 1e-6 Ha and atom forces <= 1e-5 Ha/bohr.
 """
 import numpy as np
 import pytest
@@ -35,13 +37,15 @@ def nlsys():
     return dict(sys=sysm, psi=psi, occ=occ, nkf=nkf, ref=(e, fpsi, fatm))
 
 
-def _run(nlsys, precision):
+def _run(nlsys, precision, gspace=None):
     from openatom_b200.context import StepContext
     s = nlsys["sys"]
     ctx = StepContext(s.layout, s.nstates, precision=precision)
     try:
         ctx.set_atoms(s)
         nkf = ctx.set_nonlocal(s)
+        if gspace is not None:
+            ctx.tune_set({"ees_gspace": int(gspace)})
         assert nkf == nlsys["nkf"]
         fpsi, e, f = ctx.ees_nonlocal(nlsys["psi"], nlsys["occ"])
         return e.cpu().numpy()[7], fpsi.cpu().numpy(), f.cpu().numpy()
@@ -66,8 +70,11 @@ def test_fp64_ees_matches_oracle(nlsys):
     assert np.max(np.abs(f - far)) <= 1e-10 * np.max(np.abs(far))
 
 
-def test_mixed_ees_within_budget(nlsys):
-    e, fpsi, f = _run(nlsys, "mixed")
+@pytest.mark.parametrize("gspace", [True, False])
+def test_mixed_ees_within_budget(nlsys, gspace):
+    """Mixed contexts: the G-space form on the tensor cores (gspace) and the
+    NL-grid FFT form."""
+    e, fpsi, f = _run(nlsys, "mixed", gspace)
     er, fr, far = nlsys["ref"]
     assert abs(e - er) <= 1e-5 * abs(er)
     assert np.max(np.abs(fpsi - fr)) <= 1e-5 * np.max(np.abs(fr))

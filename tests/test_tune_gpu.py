@@ -36,7 +36,10 @@ def test_autotune_choices_and_step(precision):
         assert choice["plane_waves"] in (1, 2, 3, 6)
         assert choice["nl_blocks"] in (3, 6, 12)
         assert choice["pc_split"] in (1, 2)
-        assert all(v > 0 for k, v in ms.items() if k != "tensor_cores" or precision == "mixed")
+        assert ms["plane_shfl"] > 0 and ms["plane_waves"] > 0 and ms["pc_split"] > 0
+        assert choice["ees_gspace"] in (0, 1)
+        if precision == "mixed":
+            assert ms["tensor_cores"] > 0
         ctx.tune_set(default)
         assert ctx.tune_get() == default
         ctx.tune_set(choice)
