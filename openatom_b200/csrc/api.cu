@@ -283,6 +283,7 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
   cudaFree(c->d_pc_part); cudaFree(c->d_ortho_ws); cudaFree(c->d_hmati);
   cudaFree(c->d_dev_err);
   cudaFree(c->d_split);
+  cudaFree(c->d_lv);
   cudaFree(c->d_force_atoms);
   graph_drop(c);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);

@@ -254,6 +254,8 @@ struct cpstep_ctx {
   size_t pc_part_elems = 0;
   void* d_split = nullptr;  // plane buffer of the split plane passes (k_split_*)
   size_t split_bytes = 0;
+  uint8_t* d_lv = nullptr;  // BF16 levels of pre-split tensor-core operands (k_presplit)
+  size_t lv_bytes = 0;
   double* d_ortho_ws = nullptr;
   size_t ortho_ws_elems = 0;
   int* d_ortho_status = nullptr;  // [iterations, converged] of the last Ortho launch
@@ -358,8 +360,10 @@ int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
 void graph_drop(cpstep_ctx* c);
 int pc_part_reserve(cpstep_ctx* c, size_t elems);
 int split_reserve(cpstep_ctx* c, size_t bytes);
-int ees_tc_sums(cpstep_ctx* c, const double* psi, const float* sv, long long ld_s,
-                const double2* dyp, int nch, int jp, double* C, int ldc);
+int lv_reserve(cpstep_ctx* c, size_t bytes);
+int ees_tc_presplit(cpstep_ctx* c, const double* psi, int nin_max);
+int ees_tc_sums(cpstep_ctx* c, const float* sv, long long ld_s, const double2* dyp, int nch,
+                int jp, double* C, int ldc);
 int ees_tc_force(cpstep_ctx* c, const float* sv, long long ld_s, const double2* dyp, int nch,
                  int natm_t, const double* Z, int ldz, double alpha, double* fpsi);
 int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,

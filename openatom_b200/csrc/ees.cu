@@ -692,12 +692,16 @@ static int ees_gspace_run(cpstep_ctx* c, const double* psi, const double* occ, d
   CPSTEP_LAUNCH_CHECK();
   CPSTEP_CUDA_TRY(cudaMemsetAsync(n.enl_s, 0, sizeof(double) * S, c->stream));
   CPSTEP_CUDA_TRY(cudaMemsetAsync(n.fnl, 0, sizeof(double) * S * natm * 3, c->stream));
+  int nin_max = 1;  // the largest type's inner dimension of the psi force
+  for (int t = 0; t < ntyp; ++t)
+    nin_max = std::max(nin_max, (int)n.tch[t].size() * (c->atoms.tstart[t + 1] - c->atoms.tstart[t]));
+  if (int rc = ees_tc_presplit(c, psi, nin_max)) return rc;
   for (int t = 0; t < ntyp; ++t) {
     const int nch = (int)n.tch[t].size();
     const int nt = c->atoms.tstart[t + 1] - c->atoms.tstart[t];
     if (!nch || !nt) continue;
     const float* sv = n.sv + n.sv_off[t];
-    if (int rc = ees_tc_sums(c, psi, sv, n.ld_s, n.tdyp[t], nch, 4 * nt, n.csum, S)) return rc;
+    if (int rc = ees_tc_sums(c, sv, n.ld_s, n.tdyp[t], nch, 4 * nt, n.csum, S)) return rc;
     const int ldz = (nch * nt + 1) / 2 * 2;
     ees::k_ees_zglue<<<S, 128, 0, c->stream>>>(n.csum, S, nt, nch, n.d_tch + 4 * t, n.d_vn,
                                                 n.d_order, c->atoms.tstart[t], natm, occ, n.zt,

@@ -371,6 +371,18 @@ int pc_part_reserve(cpstep_ctx* c, size_t need) {
   return CPSTEP_OK;
 }
 
+int lv_reserve(cpstep_ctx* c, size_t bytes) {
+  if (bytes > c->lv_bytes) {
+    graph_drop(c);  // a captured step may hold the old buffer
+    cudaFree(c->d_lv);
+    c->d_lv = nullptr;
+    c->lv_bytes = 0;
+    CPSTEP_CUDA_TRY(cudaMalloc(&c->d_lv, bytes));
+    c->lv_bytes = bytes;
+  }
+  return CPSTEP_OK;
+}
+
 int split_reserve(cpstep_ctx* c, size_t bytes) {
   if (bytes > c->split_bytes) {
     graph_drop(c);  // a captured step may hold the old buffer
