@@ -170,7 +170,8 @@ struct NlData {
   long long ld_s = 0;               // floats per S row (2 npts rounded up to 4)
   std::vector<long long> sv_off;
   std::vector<std::vector<int>> tch;  // channels of each type, in channel order
-  std::vector<double2*> tdyp;       // [nch_t][npts] per type
+  std::vector<float2*> tdyp;        // [nch_t][ld_d32] per type, FP32 (tensor-core path)
+  int ld_d32 = 0;                   // npts rounded up to even
   int* d_order = nullptr;           // atom of each type-order rank
   int* d_tch = nullptr;             // [ntyp][4] channel indices (-1 unused)
   double* d_vn = nullptr;           // [nchan] vnorm / vol
@@ -362,10 +363,10 @@ int pc_part_reserve(cpstep_ctx* c, size_t elems);
 int split_reserve(cpstep_ctx* c, size_t bytes);
 int lv_reserve(cpstep_ctx* c, size_t bytes);
 int ees_tc_presplit(cpstep_ctx* c, const double* psi, int nin_max);
-int ees_tc_sums(cpstep_ctx* c, const float* sv, long long ld_s, const double2* dyp, int nch,
-                int jp, double* C, int ldc);
-int ees_tc_force(cpstep_ctx* c, const float* sv, long long ld_s, const double2* dyp, int nch,
-                 int natm_t, const double* Z, int ldz, double alpha, double* fpsi);
+int ees_tc_sums(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
+                int nch, int jp, double* C, int ldc);
+int ees_tc_force(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
+                 int nch, int natm_t, const double* Z, int ldz, double alpha, double* fpsi);
 int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
                             double* C, int ldc, int sym);
 // paircalc_tc.cu (tensor-core products; *used = false when the SIMT path must run)

@@ -638,16 +638,25 @@ int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, 
     CPSTEP_CUDA_TRY(cudaMalloc(&n.csum, sizeof(double) * csz));
     CPSTEP_CUDA_TRY(cudaMalloc(&n.zt, sizeof(double) * zsz));
     n.tdyp.assign(at.ntyp, nullptr);
+    n.ld_d32 = (c->npts + 1) / 2 * 2;
     std::vector<int> htch((size_t)at.ntyp * 4, -1);
     for (int t = 0; t < at.ntyp; ++t) {
       const size_t nc = n.tch[t].size();
       if (!nc) continue;
-      CPSTEP_CUDA_TRY(cudaMalloc(&n.tdyp[t], sizeof(double2) * nc * c->npts));
+      // FP32 copies, rows padded to an even number of points (16-byte rows)
+      const size_t ld = n.ld_d32;
+      CPSTEP_CUDA_TRY(cudaMalloc(&n.tdyp[t], sizeof(float2) * nc * ld));
+      std::vector<double2> hd(c->npts);
+      std::vector<float2> hf(nc * ld, make_float2(0.f, 0.f));
       for (size_t k = 0; k < nc; ++k) {
         htch[(size_t)t * 4 + k] = n.tch[t][k];
-        CPSTEP_CUDA_TRY(cudaMemcpy(n.tdyp[t] + k * c->npts, n.dyp + (size_t)n.tch[t][k] * c->npts,
-                                   sizeof(double2) * c->npts, cudaMemcpyDeviceToDevice));
+        CPSTEP_CUDA_TRY(cudaMemcpy(hd.data(), n.dyp + (size_t)n.tch[t][k] * c->npts,
+                                   sizeof(double2) * c->npts, cudaMemcpyDeviceToHost));
+        for (int q = 0; q < c->npts; ++q)
+          hf[k * ld + q] = make_float2((float)hd[q].x, (float)hd[q].y);
       }
+      CPSTEP_CUDA_TRY(cudaMemcpy(n.tdyp[t], hf.data(), sizeof(float2) * nc * ld,
+                                 cudaMemcpyHostToDevice));
     }
     CPSTEP_CUDA_TRY(cudaMalloc(&n.d_tch, sizeof(int) * htch.size()));
     CPSTEP_CUDA_TRY(cudaMemcpy(n.d_tch, htch.data(), sizeof(int) * htch.size(),
@@ -701,13 +710,13 @@ static int ees_gspace_run(cpstep_ctx* c, const double* psi, const double* occ, d
     const int nt = c->atoms.tstart[t + 1] - c->atoms.tstart[t];
     if (!nch || !nt) continue;
     const float* sv = n.sv + n.sv_off[t];
-    if (int rc = ees_tc_sums(c, sv, n.ld_s, n.tdyp[t], nch, 4 * nt, n.csum, S)) return rc;
+    if (int rc = ees_tc_sums(c, sv, n.ld_s, n.tdyp[t], n.ld_d32, nch, 4 * nt, n.csum, S)) return rc;
     const int ldz = (nch * nt + 1) / 2 * 2;
     ees::k_ees_zglue<<<S, 128, 0, c->stream>>>(n.csum, S, nt, nch, n.d_tch + 4 * t, n.d_vn,
                                                 n.d_order, c->atoms.tstart[t], natm, occ, n.zt,
                                                 ldz, n.enl_s, n.fnl);
     CPSTEP_LAUNCH_CHECK();
-    if (int rc = ees_tc_force(c, sv, n.ld_s, n.tdyp[t], nch, nt, n.zt, ldz, -1.0, fpsi)) return rc;
+    if (int rc = ees_tc_force(c, sv, n.ld_s, n.tdyp[t], n.ld_d32, nch, nt, n.zt, ldz, -1.0, fpsi)) return rc;
   }
   ees::k_nl_finish<<<cdiv(std::max(1, 3 * natm), 128), 128, 0, c->stream>>>(
       n.enl_s, n.fnl, S, natm, energies, fatm);

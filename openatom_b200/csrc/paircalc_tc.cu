@@ -88,11 +88,11 @@ struct Cfg {
   static constexpr int WOFF = RAW0 * NLD;                // MODE 0: point weights after the rows
   // one stage: MODE 0 the FP64 rows; MODE 1 in[j][p]; MODE 2 the FP32 S rows
   // and 4 channels' dyp of the chunk's points; MODE 3 the FP32 S rows of the
-  // chunk's inner indices and 4 channels' dyp of the tile's points
+  // chunk's inner indices and 4 channels' dyp of the tile's points (dyp FP32)
   static constexpr int RAW = MODE == 0   ? WOFF + KC / 2 * 8
                              : MODE == 1 ? KC * RSP * 8
-                             : MODE == 2 ? ROWS * RSF * 4 + 4 * (KC / 2) * 16
-                                         : KC * RSPF * 4 + 4 * (ROWS / 2) * 16;
+                             : MODE == 2 ? ROWS * RSF * 4 + 4 * (KC / 2) * 8
+                                         : KC * RSPF * 4 + 4 * (ROWS / 2) * 8;
   static constexpr int CONV = 2 * NCONV * OPB;           // split operands, two chunk buffers
   static constexpr int PREB = PRE ? NSTP * OPB : 0;      // pre-split operand stages
   static constexpr int BYTES = 1024 + CONV + PREB + NST * RAW;  // + alignment slack
@@ -122,13 +122,14 @@ struct Args {
   //   sv: S rows of the type, row j at sv + j ld_s (floats, complex pairs per
   //       point); MODE 2 pairs j = v natm_t + a (v = Mn, d/dx, d/dy, d/dz),
   //       MODE 3 rows a < natm_t (Mn)
-  //   dyp: the type's nch channel projectors, channel c at dyp + c ld_d
+  //   dyp: the type's nch channel projectors (FP32), channel c at dyp + c ld_d
+  //        (ld_d even: 16-byte rows)
   //   MODE 2: B-tile rows c jt + jj (c < nch, jj < jt) = channel c x pair
   //           t jt + jj, jp pairs; output column c jp + j
   //   MODE 3: inner index j = c natm_t + a (nin = nch natm_t)
   const float* sv;
   long long ld_s;
-  const double2* dyp;
+  const float2* dyp;
   int ld_d;
   int nch, jt, jp, natm_t;
   double alpha, beta;
@@ -145,25 +146,22 @@ __host__ __device__ __forceinline__ int core_off(int r, int k) {
   return (r >> 3) * 256 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
 }
 
-// 8 FP64 values of one row (8 consecutive K) -> three BF16 levels, each
-// level scaled by its point's weight, stored as 16 bytes at dst + v TILE_B
-__device__ __forceinline__ void split_store(uint8_t* dst, const double (&x)[8],
-                                            const float (&ws)[4]) {
+// 8 FP32 values of one row (8 consecutive K) -> three BF16 levels, stored as
+// 16 bytes at dst + v TILE_B
+__device__ __forceinline__ void split_store(uint8_t* dst, const float (&f)[8]) {
   uint32_t lv[NLV][4];
 #pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    uint32_t a[NLV], b[NLV];
-    tc::split3(x[2 * e], a);
-    tc::split3(x[2 * e + 1], b);
-#pragma unroll
-    for (int v = 0; v < NLV; ++v) {
-      const float fa = __uint_as_float(a[v]) * ws[e], fb = __uint_as_float(b[v]) * ws[e];
-      lv[v][e] = tc::pack_bf16x2(__float_as_uint(fa), __float_as_uint(fb));
-    }
-  }
+  for (int e = 0; e < 4; ++e) tc::split3_pair(f[2 * e], f[2 * e + 1], lv[0][e], lv[1][e], lv[2][e]);
 #pragma unroll
   for (int v = 0; v < NLV; ++v)
     *reinterpret_cast<uint4*>(dst + v * TILE_B) = make_uint4(lv[v][0], lv[v][1], lv[v][2], lv[v][3]);
+}
+
+// FP64 values rounded to FP32 and scaled by their point's weight (a power of
+// two, so the levels of the product are the weighted levels exactly)
+__device__ __forceinline__ void to_f32(const double (&x)[8], const float (&ws)[4], float (&f)[8]) {
+#pragma unroll
+  for (int e = 0; e < 8; ++e) f[e] = (float)x[e] * ws[e >> 1];
 }
 
 struct PreArgs {
@@ -220,7 +218,9 @@ __global__ void __launch_bounds__(256) k_presplit(const PreArgs a) {
       if (2 * pt < a.K) ws[e] = (float)a.w[pt];
     }
   }
-  split_store(a.dst + ((size_t)rt * a.nsp + s) * STEP_B + core_off(rl, 8 * kh), x, ws);
+  float f[8];
+  to_f32(x, ws, f);
+  split_store(a.dst + ((size_t)rt * a.nsp + s) * STEP_B + core_off(rl, 8 * kh), f);
 }
 
 template <int MODE, int NLD, int NST, int KC>
@@ -399,13 +399,12 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
           const float* g = ok ? p.sv + (size_t)j * p.ld_s + k : p.sv;
           tc::cp16(fs + jj * C::RSF + 4 * pc, g, ok ? 16 : 0);
         }
-        double2* dd = reinterpret_cast<double2*>(fs + ROWS * C::RSF);
-        for (int q = tid; q < p.nch * (KC / 2); q += NW) {
-          const int c = q / (KC / 2), e = q % (KC / 2);
+        float2* dd = reinterpret_cast<float2*>(fs + ROWS * C::RSF);
+        for (int q = tid; q < p.nch * (KC / 4); q += NW) {  // two points per copy
+          const int c = q / (KC / 4), e = 2 * (q % (KC / 4));
           const int pt = (k0 >> 1) + e;
-          const bool ok = 2 * pt < kend;
-          tc::cp16(dd + c * (KC / 2) + e, ok ? p.dyp + (size_t)c * p.ld_d + pt : p.dyp,
-                   ok ? 16 : 0);
+          const int nb = 2 * pt + 2 < kend ? 16 : (2 * pt < kend ? 8 : 0);
+          tc::cp16(dd + c * (KC / 2) + e, nb ? p.dyp + (size_t)c * p.ld_d + pt : p.dyp, nb);
         }
       } else if (MODE == 3) {
         // S rows (Mn) of the chunk's inner indices j = c natm_t + a over the
@@ -421,13 +420,12 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
           const float* g = ok ? p.sv + (size_t)a * p.ld_s + pr : p.sv;
           tc::cp16(fs + jj * C::RSPF + 4 * pc, g, ok ? 16 : 0);
         }
-        double2* dd = reinterpret_cast<double2*>(fs + KC * C::RSPF);
-        for (int q = tid; q < p.nch * (ROWS / 2); q += NW) {
-          const int c = q / (ROWS / 2), e = q % (ROWS / 2);
+        float2* dd = reinterpret_cast<float2*>(fs + KC * C::RSPF);
+        for (int q = tid; q < p.nch * (ROWS / 4); q += NW) {  // two points per copy
+          const int c = q / (ROWS / 4), e = 2 * (q % (ROWS / 4));
           const int pt = (r0 >> 1) + e;
-          const bool ok = 2 * pt < p.M;
-          tc::cp16(dd + c * (ROWS / 2) + e, ok ? p.dyp + (size_t)c * p.ld_d + pt : p.dyp,
-                   ok ? 16 : 0);
+          const int nb = 2 * pt + 2 < p.M ? 16 : (2 * pt < p.M ? 8 : 0);
+          tc::cp16(dd + c * (ROWS / 2) + e, nb ? p.dyp + (size_t)c * p.ld_d + pt : p.dyp, nb);
         }
       } else {
         // in[j][p] rows j = k0 .. k0 + KC, 128 points from r0
@@ -456,31 +454,33 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
       uint8_t* dB = base + conv_off(buf, 1) + off;
       const float one[4] = {1.f, 1.f, 1.f, 1.f};
       double x[8];
+      float f[8];
       if (MODE == 1) {  // A[p][j] = in[j][p] from the [KC][128] stage
 #pragma unroll
         for (int e = 0; e < 8; ++e) x[e] = ra[(8 * u + e) * RSP + r];
-        split_store(dA, x, one);
+        to_f32(x, one, f);
+        split_store(dA, f);
         return;
       }
+      // EES operands in FP32 (S is FP32): conj(dyp) S, one rounding per product
       if (MODE == 3) {  // A[p][j] = (conj(dyp_c) S_a)(point r / 2), re or im
         const float* fs = reinterpret_cast<const float*>(ra);
-        const double2* dd = reinterpret_cast<const double2*>(fs + KC * C::RSPF);
+        const float2* dd = reinterpret_cast<const float2*>(fs + KC * C::RSPF);
         const int pl = r >> 1;
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
           const int j = k0 + 8 * u + e;
           const int c = min(j / p.natm_t, 3);
           const float2 sa = *reinterpret_cast<const float2*>(fs + (8 * u + e) * C::RSPF + 2 * pl);
-          const double2 d = dd[c * (ROWS / 2) + pl];
-          x[e] = (r & 1) ? d.x * (double)sa.y - d.y * (double)sa.x
-                         : d.x * (double)sa.x + d.y * (double)sa.y;
+          const float2 d = dd[c * (ROWS / 2) + pl];
+          f[e] = (r & 1) ? fmaf(d.x, sa.y, -d.y * sa.x) : fmaf(d.x, sa.x, d.y * sa.y);
         }
-        split_store(dA, x, one);
+        split_store(dA, f);
         return;
       }
       if (MODE == 2) {  // B row r = channel c, pair jj: conj(dyp_c) S_pair
         const float* fs = reinterpret_cast<const float*>(ra);
-        const double2* dd = reinterpret_cast<const double2*>(fs + ROWS * C::RSF);
+        const float2* dd = reinterpret_cast<const float2*>(fs + ROWS * C::RSF);
         const int c = r / p.jt, jj = r - c * p.jt;
         const bool ok = c < p.nch;
 #pragma unroll
@@ -488,11 +488,11 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
           const float2 sa =
               ok ? *reinterpret_cast<const float2*>(fs + jj * C::RSF + 8 * u + 2 * e)
                  : make_float2(0.f, 0.f);
-          const double2 d = ok ? dd[c * (KC / 2) + 4 * u + e] : make_double2(0.0, 0.0);
-          x[2 * e] = d.x * (double)sa.x + d.y * (double)sa.y;
-          x[2 * e + 1] = d.x * (double)sa.y - d.y * (double)sa.x;
+          const float2 d = ok ? dd[c * (KC / 2) + 4 * u + e] : make_float2(0.f, 0.f);
+          f[2 * e] = fmaf(d.x, sa.x, d.y * sa.y);
+          f[2 * e + 1] = fmaf(d.x, sa.y, -d.y * sa.x);
         }
-        split_store(dB, x, one);
+        split_store(dB, f);
         return;
       }
       const double2* s2 =
@@ -504,7 +504,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
         x[2 * e + 1] = v.y;
       }
       if (op == 1) {
-        split_store(dB, x, one);
+        to_f32(x, one, f);
+        split_store(dB, f);
         return;
       }
       float ws[4] = {1.f, 1.f, 1.f, 1.f};
@@ -522,8 +523,12 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
         for (int e = 0; e < 8; ++e) d = fma((double)ws[e >> 1] * x[e], x[e], d);
         dacc += d;
       }
-      split_store(dA, x, ws);
-      if (NLD == 1) split_store(dB, x, one);
+      if (NLD == 1) {
+        to_f32(x, one, f);
+        split_store(dB, f);
+      }
+      to_f32(x, ws, f);
+      split_store(dA, f);
     };
 
     // group of chunk c (its last), once its MMAs are done: each FP32
@@ -705,11 +710,12 @@ int ees_tc_presplit(cpstep_ctx* c, const double* psi, int nin_max) {
 // EES sums of one atom type (MODE 2): C(s, ch jp + j) = sum_p wpt Re(conj psi_s
 // conj(dyp_ch) S_j), j < jp pairs; C column-major [nch jp][ldc], alpha = 1.
 // Takes psi's levels from ees_tc_presplit.
-int ees_tc_sums(cpstep_ctx* c, const float* sv, long long ld_s, const double2* dyp, int nch,
-                int jp, double* C, int ldc) {
+int ees_tc_sums(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
+                int nch, int jp, double* C, int ldc) {
   using namespace pctc;
   const int S = c->nstates, K = 2 * c->npts;
-  if (nch < 1 || nch > 4 || (ld_s & 3) || !al16(sv) || c->lv_bytes < pre_bytes(S, K))
+  if (nch < 1 || nch > 4 || (ld_s & 3) || (ld_d & 1) || !al16(sv) || !al16(dyp) ||
+      c->lv_bytes < pre_bytes(S, K))
     return CPSTEP_ERR_ARG;
   const int jt = ROWS / nch;
   const int tm = cdiv(S, ROWS), tn = cdiv(jp, jt);
@@ -729,7 +735,7 @@ int ees_tc_sums(cpstep_ctx* c, const float* sv, long long ld_s, const double2* d
   p.sv = sv;
   p.ld_s = ld_s;
   p.dyp = dyp;
-  p.ld_d = c->npts;
+  p.ld_d = ld_d;
   p.nch = nch;
   p.jt = jt;
   p.jp = jp;
@@ -742,12 +748,12 @@ int ees_tc_sums(cpstep_ctx* c, const float* sv, long long ld_s, const double2* d
 // EES psi force of one atom type (MODE 3): fpsi_s(p) += alpha wpt(p) sum_j
 // Z(j, s) (conj(dyp_c) S_a)(p), j = c natm_t + a; Z column-major [S][ldz].
 // Z's levels go after psi's (room reserved by ees_tc_presplit).
-int ees_tc_force(cpstep_ctx* c, const float* sv, long long ld_s, const double2* dyp, int nch,
-                 int natm_t, const double* Z, int ldz, double alpha, double* fpsi) {
+int ees_tc_force(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
+                 int nch, int natm_t, const double* Z, int ldz, double alpha, double* fpsi) {
   using namespace pctc;
   const int S = c->nstates, K = 2 * c->npts, nin = nch * natm_t;
-  if (nch < 1 || nch > 4 || (ld_s & 3) || (ldz & 1) || !al16(sv) || !al16(Z) ||
-      c->lv_bytes < pre_bytes(S, K) + pre_bytes(S, nin))
+  if (nch < 1 || nch > 4 || (ld_s & 3) || (ld_d & 1) || (ldz & 1) || !al16(sv) || !al16(Z) ||
+      !al16(dyp) || c->lv_bytes < pre_bytes(S, K) + pre_bytes(S, nin))
     return CPSTEP_ERR_ARG;
   uint8_t* zl = c->d_lv + pre_bytes(S, K);
   if (int rc = presplit(c, Z, ldz, S, nin, nullptr, 0, zl)) return rc;
@@ -765,7 +771,7 @@ int ees_tc_force(cpstep_ctx* c, const float* sv, long long ld_s, const double2* 
   p.sv = sv;
   p.ld_s = ld_s;
   p.dyp = dyp;
-  p.ld_d = c->npts;
+  p.ld_d = ld_d;
   p.nch = nch;
   p.natm_t = natm_t;
   p.pre = zl;

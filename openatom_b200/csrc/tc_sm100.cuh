@@ -109,28 +109,29 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
   }
 }
 
-// One test of the phase with the given parity (no spinning).
-__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+// One test of the phase with the given parity; the thread may sleep up to
+// hint_ns waiting for it (woken when the phase completes).
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
   uint32_t done;
   asm volatile(
       "{\n\t"
       ".reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t"
       "}\n"
       : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
       : "memory");
   return done != 0;
 }
 
 // Bounded wait that also gives up as soon as *stop is set (another role of
-// the CTA reported an error): false on either.
+// the CTA reported an error): false on either.  Sleeps between tests.
 __device__ __forceinline__ bool mbar_wait_or(uint64_t* bar, uint32_t parity, const volatile int* stop,
                                              uint64_t limit_ns = 1000000000ull) {
   const uint64_t t0 = globaltimer_ns();
   for (;;) {
-    if (mbar_test(bar, parity)) return true;
+    if (mbar_test(bar, parity, 20000u)) return true;
     if (*stop) return false;
     if (globaltimer_ns() - t0 > limit_ns) return false;
   }
@@ -223,21 +224,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// 8 consecutive FP32 columns of TMEM lane (warp's 32-lane slice + lane).
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
-  uint32_t r[8];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// 16 consecutive 32-bit TMEM columns (raw words), load and store; a store is
-// complete for the storing thread after tmem_wait_st.
+// 16 or 8 consecutive 32-bit TMEM columns (raw words), loads and a store; a
+// store is complete for the storing thread after tmem_wait_st.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
@@ -247,15 +235,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
         "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
-      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(taddr),
-      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
-      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
-      "r"(r[15])
-      : "memory");
 }
 __device__ __forceinline__ void tmem_ld8u(uint32_t taddr, uint32_t (&r)[8]) {
   asm volatile(
@@ -276,29 +255,24 @@ __device__ __forceinline__ void tmem_wait_st() {
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
-// Round-to-nearest-even of f to BF16, returned as FP32 bits (low 16 bits 0).
-__device__ __forceinline__ uint32_t bf16_round_bits(float f) {
-  uint32_t u = __float_as_uint(f);
-  u += 0x7FFFu + ((u >> 16) & 1u);
-  return u & 0xFFFF0000u;
+// Two FP32 values rounded to nearest even BF16, packed: a in the low half
+// (the lower address).
+__device__ __forceinline__ uint32_t cvt_bf16x2(float a, float b) {
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+  return r;
 }
+__device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
 
-// Three-level BF16 split of f = (float)x: f = hi + mid + lo exactly (each
-// remainder is exact in FP32 and has at most 8 significant bits left after
-// two levels), so x = hi + mid + lo + O(2^-24 |x|).  Levels as FP32 bit
-// patterns (low 16 bits zero).
-__device__ __forceinline__ void split3(double x, uint32_t (&v)[3]) {
-  const float f = (float)x;
-  v[0] = bf16_round_bits(f);
-  const float r = f - __uint_as_float(v[0]);
-  v[1] = bf16_round_bits(r);
-  v[2] = __float_as_uint(r - __uint_as_float(v[1]));  // already a BF16 value
-}
-
-// Two FP32 bit patterns with zero low halves -> one BF16x2 word (a in the low
-// half, the lower address).
-__device__ __forceinline__ uint32_t pack_bf16x2(uint32_t a, uint32_t b) {
-  return __byte_perm(a, b, 0x7632);
+// Three-level BF16 split of a pair of FP32 values, packed per level:
+// a = h + m + l exactly (the remainders are exact in FP32; after two levels
+// at most 8 significant bits are left, so the third rounding is exact).
+__device__ __forceinline__ void split3_pair(float a, float b, uint32_t& h, uint32_t& m, uint32_t& l) {
+  h = cvt_bf16x2(a, b);
+  const float ra = a - bf16_lo(h), rb = b - bf16_hi(h);
+  m = cvt_bf16x2(ra, rb);
+  l = cvt_bf16x2(ra - bf16_lo(m), rb - bf16_hi(m));
 }
 
 }  // namespace tc
