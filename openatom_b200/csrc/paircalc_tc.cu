@@ -8,12 +8,15 @@
 //     a b ~ l_a h_b + h_a l_b + m_a m_b + m_a h_b + h_a m_b + h_a h_b
 //
 // (the level pairs of total order <= 2; the dropped ones are O(2^-24 |ab|)) is
-// accumulated by tcgen05.mma (kind::f16, BF16 in, FP32 accumulator in TMEM),
-// smallest terms first.  The FP32 accumulator holds at most 128 reals of K:
-// it is then read back (tcgen05.ld) and added into an FP64 copy of the tile
-// kept in the other half of TMEM (two 32-bit columns per element, read and
-// written back with tcgen05.ld / tcgen05.st), so the sums over those groups,
-// over the split-K slabs and the epilogue terms are FP64.
+// accumulated by tcgen05.mma (kind::f16, BF16 in, FP32 accumulators in TMEM),
+// smallest terms first, h_a h_b in an accumulator of its own.  That one holds
+// at most 128 reals of K: it is then read back (tcgen05.ld) and added into an
+// FP64 copy of the tile kept in the other half of TMEM (two 32-bit columns
+// per element, read and written back with tcgen05.ld / tcgen05.st).  The five
+// small products (2^-7 of the total) run over the CTA's whole K range in FP32
+// and join the FP64 tile in the epilogue: their rounding stays well below the
+// hi*hi groups' own.  The sums over the groups, the split-K slabs and the
+// epilogue terms are FP64.
 //
 // One CTA = one 128 x 128 output tile (M = N = 128 MMA) and one K range,
 // one CTA per SM, 17 warps in two roles:
@@ -23,13 +26,12 @@
 //     matrix; the two 8-element K halves of a 16-wide K step 128 bytes apart,
 //     8-row groups 256 bytes apart; per K step the three levels 4 KB apart),
 //     applying the per-point weight (a power of two: exact) on the way, and
-//     after every 128 reals fold the finished FP32 accumulators into the FP64
-//     tile, releasing each accumulator as soon as it is read;
+//     after every 128 reals fold the hi*hi accumulator into the FP64 tile,
+//     releasing it to the MMA warp as soon as it is read;
 //   * warp 16 issues the 6 MMAs per K step into two FP32 TMEM accumulators
-//     (the five small products in columns 0-127, hi*hi in columns 128-255,
-//     so the FP32 rounding of the small terms' sum is relative to their own
-//     size; the FP64 tile holds columns 256-511), commits them to an
-//     mbarrier, and keeps the stages of a pre-split operand filled.
+//     (the five small products in columns 0-127, hi*hi in columns 128-255;
+//     the FP64 tile holds columns 256-511), commits them to an mbarrier, and
+//     keeps the stages of a pre-split operand filled.
 // An operand that many CTAs share (psi in the EES sums, Z in the EES force,
 // T in the back-multiply) is split once, by k_presplit, into its BF16 levels
 // in global memory in the same core-matrix image; the MMA warp brings its
@@ -37,9 +39,8 @@
 // other operand is split in the CTA.
 //
 // Handshakes (all mbarriers): full[b] (workers' chunk in split buffer b),
-// done[b] (MMAs of the chunk that used buffer b completed), tfree[h] (TMEM
-// accumulator h read back: 0 small terms, 1 hi*hi), pfull[s] (pre-split
-// stage s landed).  Every wait is
+// done[b] (MMAs of the chunk that used buffer b completed), tfree (hi*hi
+// accumulator read back), pfull[s] (pre-split stage s landed).  Every wait is
 // bounded (1 s) and also ends when the other role has raised `stop`; the CTA
 // then records an error bit in *err, drains its copies, waits (bounded) for
 // its MMAs, releases TMEM and returns without writing its tile.
@@ -229,7 +230,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
   constexpr int KS = C::KS, U = C::U, NF = C::NF, RS = C::RS, RSP = C::RSP;
   constexpr bool DIAG = MODE == 0;
   extern __shared__ uint8_t dsm[];
-  __shared__ uint64_t full[2], done[2], tfree[2], pfull[NSTP];
+  __shared__ uint64_t full[2], done[2], tfree, pfull[NSTP];
   __shared__ uint32_t tslot;
   __shared__ int stop_s, issued_s;
   __shared__ double diag_s[DIAG ? ROWS : 1];
@@ -263,8 +264,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
     for (int i = 0; i < 2; ++i) {
       tc::mbar_init(&full[i], NW);
       tc::mbar_init(&done[i], 1);
-      tc::mbar_init(&tfree[i], NW);
     }
+    tc::mbar_init(&tfree, NW);
     for (int i = 0; i < NSTP; ++i) tc::mbar_init(&pfull[i], 1);
     stop_s = 0;
     issued_s = 0;
@@ -298,8 +299,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
         tc::bulk_g2s(pre_base + (size_t)st * C::OPB, src, C::OPB, &pfull[st]);
       };
       // the MMAs of chunk ch, smallest level products first; the first chunk
-      // of a group waits for each accumulator's read-back (tfree) before it
-      // overwrites it.  The commit covers whatever was issued.
+      // of a group waits for the hi*hi accumulator's read-back (tfree) before
+      // it overwrites it.  The commit covers whatever was issued.
       auto issue = [&](int ch) -> bool {
         const int buf = ch & 1, g = ch / NF;
         const bool first = ch % NF == 0;
@@ -313,9 +314,9 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
         for (int s = 0; s < KS; ++s) {
 #pragma unroll
           for (int t = 0; t < 6; ++t) {
-            const bool zero = first && s == 0 && (t == 0 || t == 5);
-            if (zero && g >= 1 && ok) {
-              ok = tc::mbar_wait_or(&tfree[t == 5 ? 1 : 0], (g - 1) & 1, stop);
+            const bool zero = first && s == 0 && (t == 5 || (t == 0 && ch == 0));
+            if (first && s == 0 && t == 5 && g >= 1 && ok) {
+              ok = tc::mbar_wait_or(&tfree, (g - 1) & 1, stop);
               tc::fence_after_sync();
             }
             const uint64_t da = tc::smem_desc_kmajor(a0 + s * STEP_B + LA[t] * TILE_B, 128, 256);
@@ -531,41 +532,37 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
       split_store(dA, f);
     };
 
-    // group of chunk c (its last), once its MMAs are done: each FP32
-    // accumulator (small terms, then hi*hi) is read, released to the MMA warp
-    // and added into the FP64 tile, 4 columns at a time
+    // group of chunk c (its last), once its MMAs are done: the hi*hi
+    // accumulator is read, released to the MMA warp and added into the FP64
+    // tile (the first group's is stored), 4 columns at a time
     auto flush = [&](int c) -> bool {
       const int g = c / NF;
       if (!__all_sync(0xffffffffu, tc::mbar_wait_or(&done[c & 1], (c >> 1) & 1, stop)))
         return false;
       tc::fence_after_sync();
-      const uint32_t tg = tbase + tlanes + (uint32_t)(32 * (warp >> 2));
+      float v[32];
+      tc::tmem_ld32(tbase + tlanes + (uint32_t)(ROWS + 32 * (warp >> 2)), v);
+      tc::fence_before_sync();
+      tc::mbar_arrive(&tfree);
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        float v[32];
-        tc::tmem_ld32(tg + h * ROWS, v);
-        tc::fence_before_sync();
-        tc::mbar_arrive(&tfree[h]);
+      for (int pc = 0; pc < 8; ++pc) {
+        uint32_t a[8];
+        if (g > 0) {
+          tc::tmem_ld8u(tf64 + 8 * pc, a);
+        } else {
 #pragma unroll
-        for (int pc = 0; pc < 8; ++pc) {
-          uint32_t a[8];
-          if (g > 0 || h > 0) {
-            tc::tmem_ld8u(tf64 + 8 * pc, a);
-          } else {
-#pragma unroll
-            for (int e = 0; e < 8; ++e) a[e] = 0u;
-          }
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const double d =
-                __hiloint2double((int)a[2 * e + 1], (int)a[2 * e]) + (double)v[4 * pc + e];
-            a[2 * e] = (uint32_t)__double2loint(d);
-            a[2 * e + 1] = (uint32_t)__double2hiint(d);
-          }
-          tc::tmem_st8(tf64 + 8 * pc, a);
+          for (int e = 0; e < 8; ++e) a[e] = 0u;
         }
-        tc::tmem_wait_st();  // the next read of the FP64 tile sees these
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const double d =
+              __hiloint2double((int)a[2 * e + 1], (int)a[2 * e]) + (double)v[4 * pc + e];
+          a[2 * e] = (uint32_t)__double2loint(d);
+          a[2 * e + 1] = (uint32_t)__double2hiint(d);
+        }
+        tc::tmem_st8(tf64 + 8 * pc, a);
       }
+      tc::tmem_wait_st();  // the next read of the FP64 tile sees these
       return true;
     };
 
@@ -608,16 +605,21 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
       if (q < ROWS * U && ((q >> 3) % U) == 0) diag_s[(q & 7) + 8 * ((q >> 3) / U)] = d;
       tc::bar_sync(WBAR, NW);
     }
-    // ---- epilogue (workers): the FP64 tile out of TMEM, 8 columns at a time
+    // ---- epilogue (workers): the FP64 tile plus the small terms' FP32
+    // accumulator out of TMEM, 8 columns at a time
     const int rl = 32 * (warp & 3) + lane, cb = 32 * (warp >> 2);
+    const uint32_t tsm = tbase + tlanes + (uint32_t)(32 * (warp >> 2));
 #pragma unroll 1
     for (int pc = 0; pc < 4; ++pc) {
-      uint32_t a[16];
+      uint32_t a[16], sm[8];
       tc::tmem_ld16(tf64 + 16 * pc, a);
+      tc::tmem_ld8u(tsm + 8 * pc, sm);
 #pragma unroll
       for (int e8 = 0; e8 < 8; ++e8) {
         const int e = 8 * pc + e8;
-        const double acc = nch > 0 ? __hiloint2double((int)a[2 * e8 + 1], (int)a[2 * e8]) : 0.0;
+        const double acc = nch > 0 ? __hiloint2double((int)a[2 * e8 + 1], (int)a[2 * e8]) +
+                                         (double)__uint_as_float(sm[e8])
+                                   : 0.0;
         if (MODE == 0) {
           const int r = r0 + rl, c = c0 + cb + e;
           if (r < p.M && c < p.N)
