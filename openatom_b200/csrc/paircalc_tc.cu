@@ -64,7 +64,7 @@ constexpr int STEP_B = NLV * TILE_B;      // one K step, all levels: 12 KB
 constexpr int NW = 512;                   // worker threads (warps 0-15)
 constexpr int MMA_WARP = NW / 32;         // warp 16 issues the MMAs
 constexpr int NTHR = NW + 32;
-constexpr int NSTP = 3;                   // shared-memory stages of a pre-split operand
+constexpr int NSTP_MAX = 5;               // shared-memory stages of a pre-split operand (at most)
 constexpr int WBAR = 1;                   // named barrier of the workers
 constexpr uint32_t IDESC = tc::idesc_bf16_f32(ROWS, ROWS);
 constexpr uint32_t TMEM_COLS = 512;       // two FP32 accumulators + the FP64 tile
@@ -84,6 +84,9 @@ struct Cfg {
   static constexpr bool CA = MODE != 2, CB = MODE == 0 || MODE == 2;
   static constexpr bool PA = MODE == 2, PB = MODE == 1 || MODE == 3;
   static constexpr bool PRE = PA || PB;
+  // pre-split stages: as deep as shared memory allows (the back-multiply's
+  // FP64 [KC][128] stages leave room for 3)
+  static constexpr int NSTP = MODE == 1 ? 3 : NSTP_MAX;
   static constexpr int NCONV = (CA ? 1 : 0) + (CB ? 1 : 0);
   static constexpr int RAW0 = ROWS * RS * 8;             // [128][KC] FP64
   static constexpr int WOFF = RAW0 * NLD;                // MODE 0: point weights after the rows
@@ -230,6 +233,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
   constexpr int KS = C::KS, U = C::U, NF = C::NF, RS = C::RS, RSP = C::RSP;
   constexpr bool DIAG = MODE == 0;
   extern __shared__ uint8_t dsm[];
+  constexpr int NSTP = C::NSTP;
   __shared__ uint64_t full[2], done[2], tfree, pfull[NSTP];
   __shared__ uint32_t tslot;
   __shared__ int stop_s, issued_s;
@@ -262,10 +266,10 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
   if (warp == 0) tc::tmem_alloc(&tslot, TMEM_COLS);
   if (tid == 0) {
     for (int i = 0; i < 2; ++i) {
-      tc::mbar_init(&full[i], NW);
+      tc::mbar_init(&full[i], NW / 32);  // one arrival per worker warp
       tc::mbar_init(&done[i], 1);
     }
-    tc::mbar_init(&tfree, NW);
+    tc::mbar_init(&tfree, NW / 32);
     for (int i = 0; i < NSTP; ++i) tc::mbar_init(&pfull[i], 1);
     stop_s = 0;
     issued_s = 0;
@@ -534,7 +538,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
 
     // group of chunk c (its last), once its MMAs are done: the hi*hi
     // accumulator is read, released to the MMA warp and added into the FP64
-    // tile (the first group's is stored), 4 columns at a time
+    // tile (the first group's is stored), 8 columns at a time
     auto flush = [&](int c) -> bool {
       const int g = c / NF;
       if (!__all_sync(0xffffffffu, tc::mbar_wait_or(&done[c & 1], (c >> 1) & 1, stop)))
@@ -543,24 +547,25 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
       float v[32];
       tc::tmem_ld32(tbase + tlanes + (uint32_t)(ROWS + 32 * (warp >> 2)), v);
       tc::fence_before_sync();
-      tc::mbar_arrive(&tfree);
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&tfree);
 #pragma unroll
-      for (int pc = 0; pc < 8; ++pc) {
-        uint32_t a[8];
+      for (int h = 0; h < 4; ++h) {  // 8 columns (16 words) per TMEM round trip
+        uint32_t a[16];
         if (g > 0) {
-          tc::tmem_ld8u(tf64 + 8 * pc, a);
+          tc::tmem_ld16(tf64 + 16 * h, a);
         } else {
 #pragma unroll
-          for (int e = 0; e < 8; ++e) a[e] = 0u;
+          for (int e = 0; e < 16; ++e) a[e] = 0u;
         }
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
+        for (int e = 0; e < 8; ++e) {
           const double d =
-              __hiloint2double((int)a[2 * e + 1], (int)a[2 * e]) + (double)v[4 * pc + e];
+              __hiloint2double((int)a[2 * e + 1], (int)a[2 * e]) + (double)v[8 * h + e];
           a[2 * e] = (uint32_t)__double2loint(d);
           a[2 * e + 1] = (uint32_t)__double2hiint(d);
         }
-        tc::tmem_st8(tf64 + 8 * pc, a);
+        tc::tmem_st16(tf64 + 16 * h, a);
       }
       tc::tmem_wait_st();  // the next read of the FP64 tile sees these
       return true;
@@ -582,7 +587,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
       }
       convert(ch, ch % NST, ch & 1);
       tc::fence_async_shared();
-      tc::mbar_arrive(&full[ch & 1]);
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&full[ch & 1]);
       if (ch + NST - 1 < nch) load(ch + NST - 1, (ch + NST - 1) % NST);
       tc::cp_commit();
       if (ch >= 1 && (ch - 1) % NF == NF - 1 && !flush(ch - 1)) bad = 1;
