@@ -615,9 +615,13 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
     // accumulator out of TMEM, 8 columns at a time
     const int rl = 32 * (warp & 3) + lane, cb = 32 * (warp >> 2);
     const uint32_t tsm = tbase + tlanes + (uint32_t)(32 * (warp >> 2));
+    const double sc = (MODE == 1 || MODE == 3) && r0 + rl < p.M
+                          ? p.alpha * (p.w ? p.w[(r0 + rl) >> 1] : 1.0)
+                          : 0.0;
 #pragma unroll 1
     for (int pc = 0; pc < 4; ++pc) {
       uint32_t a[16], sm[8];
+      double accs[8];
       tc::tmem_ld16(tf64 + 16 * pc, a);
       tc::tmem_ld8u(tsm + 8 * pc, sm);
 #pragma unroll
@@ -637,14 +641,29 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
           if (r < p.M && ch < p.nch && j < p.jp)
             p.part[(size_t)blockIdx.z * p.M * p.N + (size_t)(ch * p.jp + j) * p.M + r] = acc;
         } else {
-          const int pt = r0 + rl, i = c0 + cb + e;
+          accs[e8] = acc;
+        }
+      }
+      if (MODE == 1 || MODE == 3) {
+        // out = alpha w (acc [+ diag]) + beta out: every load of the piece is
+        // issued before its first store, so their latencies overlap
+        const int pt = r0 + rl;
+        double ov[8], dg[8];
+#pragma unroll
+        for (int e8 = 0; e8 < 8; ++e8) {
+          const int i = c0 + cb + 8 * pc + e8;
+          const bool ok = pt < p.M && i < p.N;
+          ov[e8] = (ok && p.beta != 0.0) ? p.out[(size_t)i * p.ldo + pt] : 0.0;
+          dg[e8] = (MODE == 1 && ok && i < p.nin)
+                       ? p.B[(size_t)i * p.ldb + i] * p.A[(size_t)i * p.lda + pt]
+                       : 0.0;
+        }
+#pragma unroll
+        for (int e8 = 0; e8 < 8; ++e8) {
+          const int i = c0 + cb + 8 * pc + e8;
           if (pt < p.M && i < p.N) {
-            const double sc = p.alpha * (p.w ? p.w[pt >> 1] : 1.0);
-            double v = acc;
-            if (MODE == 1 && i < p.nin)
-              v = fma(p.B[(size_t)i * p.ldb + i], p.A[(size_t)i * p.lda + pt], v);
-            double* o = p.out + (size_t)i * p.ldo + pt;
-            *o = p.beta == 0.0 ? sc * v : fma(p.beta, *o, sc * v);
+            const double v = sc * (accs[e8] + dg[e8]);
+            p.out[(size_t)i * p.ldo + pt] = p.beta == 0.0 ? v : fma(p.beta, ov[e8], v);
           }
         }
       }
