@@ -7,6 +7,9 @@
 #   src_piny_physics_v1.0/abinito_physics/cp_nonlocal/cp_ees_nonlocal.C  EES non-local
 #   src_piny_physics_v1.0/interface/cp_ewald/set_cp_ewald.C  get_bspline_wght1d,
 #                                                           init_nonlocal_ees
+#   src_piny_physics_v1.0/abinito_physics/cp_xc_fnctl/cp_becke.C, cp_grad_rho_ctrl.C,
+#                         cp_pz_lda.C   becke_gcx_lda, lyp_gcc, CP_getGGAFunctional,
+#                                       CP_exc_calc
 # The shims in oracle/ref_shim stand in for the Charm++/PINY headers, and
 # oracle/ref_mathlib.c for the Fortran GENMATMUL.  Test infrastructure only.
 set -e
@@ -26,7 +29,10 @@ EESFLAGS="-O2 -fPIC -w -DCHARM_ON -DSIMP_NINT -include $HERE/ref_shim/ees_shim.h
   -include $PINY/include/class_defs/piny_constants.h -I $HERE/ref_shim -I $HERE/ref_shim/sub \
   -I $REF -I $REF/src_charm_driver/utility -I $PINY/include/class_defs -I $REF/include"
 for f in "$PINY/abinito_physics/cp_nonlocal/cp_ees_nonlocal.C" \
-         "$PINY/interface/cp_ewald/set_cp_ewald.C" "$HERE/ref_ees.cpp"; do
+         "$PINY/interface/cp_ewald/set_cp_ewald.C" "$HERE/ref_ees.cpp" \
+         "$PINY/abinito_physics/cp_xc_fnctl/cp_becke.C" \
+         "$PINY/abinito_physics/cp_xc_fnctl/cp_grad_rho_ctrl.C" \
+         "$PINY/abinito_physics/cp_xc_fnctl/cp_pz_lda.C" "$HERE/ref_xc.cpp"; do
   g++ $EESFLAGS -c "$f" -o "$OUT/$(basename "$f" | sed 's/\.[Cc]p*$//').o"
 done
 g++ -O2 -fPIC -shared -w -o "$OUT/libref.so" \
@@ -36,5 +42,6 @@ g++ -O2 -fPIC -shared -w -o "$OUT/libref.so" \
   "$REF/src_mathlib/lst_sort_clean.C" \
   "$REF/src_piny_physics_v1.0/abinito_physics/cp_orthog/cp_lowdin.C" \
   "$HERE/ref_driver.cpp" "$OUT/ref_mathlib.o" \
-  "$OUT/cp_ees_nonlocal.o" "$OUT/set_cp_ewald.o" "$OUT/ref_ees.o"
+  "$OUT/cp_ees_nonlocal.o" "$OUT/set_cp_ewald.o" "$OUT/ref_ees.o" \
+  "$OUT/cp_becke.o" "$OUT/cp_grad_rho_ctrl.o" "$OUT/cp_pz_lda.o" "$OUT/ref_xc.o"
 echo "$OUT/libref.so"
