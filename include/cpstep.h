@@ -50,7 +50,17 @@ extern "C" {
 #define CPSTEP_E_NL 7      /* ENL        (EES non-local)                      */
 #define CPSTEP_E_TOT 8     /* ELEC_ENERGY_TOT = EKE+ENL+EHART+EExt+EEXC       */
 #define CPSTEP_E_FICT 9    /* fictitious kinetic energy (get_fictKE)          */
+#define CPSTEP_E_EXC_GGA 10 /* gradient correction part of EEXC (BLYP:
+                               CP_getGGAFunctional exc_gga_ret)               */
 #define CPSTEP_NENERGY 12
+
+/* Exchange-correlation functionals (cpstep_set_xc).  PZ-LDA is the default;
+ * BLYP is Slater exchange (CP_exc_calc with cp_lyp = 1) plus the Becke 88
+ * exchange gradient correction and LYP correlation of CP_getGGAFunctional,
+ * with the density gradients and the White-Bird divergence on the density
+ * sphere (CP_Rho_GSpacePlane divRhoVksGspace / acceptWhiteByrd). */
+#define CPSTEP_XC_PZ_LDA 0
+#define CPSTEP_XC_BLYP 1
 
 #define CPSTEP_MAX_TYPES 16   /* atom types a context accepts (cpstep_set_atoms) */
 
@@ -299,6 +309,18 @@ CPSTEP_API int cpstep_ortho_tmat(cpstep_ctx* ctx, const double* d_s, double* d_t
  * cpstep_vks_from_rho: the chain CP_exc_calc -> fftRhoRtoRhoG -> CP_hart_eext_calc
  *   -> FFTVks -> acceptHartVks (CP_Rho_RealSpacePlane.C:1365-1415):
  *   d_vks_r = v_xc + V_H + V_loc on the grid, the five energies, forces.
+ *   With BLYP the gradient correction joins after fftRhoRtoRhoG: the density
+ *   gradients (divRhoVksGspace), CP_getGGAFunctional, the White-Bird
+ *   divergence (whiteByrdFFT, acceptWhiteByrd); EEXC then includes EXC_GGA.
+ * cpstep_set_xc: CPSTEP_XC_PZ_LDA (default) or CPSTEP_XC_BLYP; the BLYP
+ *   density cut-off gradient_cutoff (the reference's \gradient_cutoff,
+ *   5e-5 when <= 0).  Applies to cpstep_exc_calc, cpstep_vks_from_rho and
+ *   the step.
+ * cpstep_gga_functional: CPXCFNCTS::CP_getGGAFunctional
+ *   (cp_xc_fnctl/cp_grad_rho_ctrl.C:32-193) with Becke 88 and LYP on the dense
+ *   grid: d_vks += df/drho; d_gx, d_gy, d_gz (the density gradient on entry)
+ *   <- unit(grad rho) df/d|grad rho|; d_energies[EXC_GGA] = E_GGA.  Points
+ *   with an exactly zero gradient get zero there (the reference divides 0 by 0).
  * d_energies: device array of CPSTEP_NENERGY doubles; only the named slots are written.
  */
 CPSTEP_API int cpstep_set_atoms(cpstep_ctx* ctx, int natm, int ntyp, const int* typ,
@@ -315,6 +337,10 @@ CPSTEP_API int cpstep_hart_eext(cpstep_ctx* ctx, const double* d_rhog, double* d
 CPSTEP_API int cpstep_vks_fft_g2r(cpstep_ctx* ctx, const double* d_vksg, double* d_v_r);
 CPSTEP_API int cpstep_vks_from_rho(cpstep_ctx* ctx, const double* d_rho_r, double* d_vks_r,
                                    double* d_energies, double* d_force);
+CPSTEP_API int cpstep_set_xc(cpstep_ctx* ctx, int functional, double gradient_cutoff);
+CPSTEP_API int cpstep_gga_functional(cpstep_ctx* ctx, const double* d_rho, double* d_gx,
+                                     double* d_gy, double* d_gz, double* d_vks,
+                                     double* d_energies);
 
 /* ---------------------------------------------------------------------------
  * EES non-local pseudopotential (Kleinman-Bylander s and p channels,

@@ -70,6 +70,8 @@ SIGNATURES = {
     "cpstep_hart_eext": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "cpstep_vks_fft_g2r": (ctypes.c_int, [_vp, _vp, _vp]),
     "cpstep_vks_from_rho": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cpstep_set_xc": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),
+    "cpstep_gga_functional": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cpstep_nl_grid_size": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int]),
     "cpstep_set_nonlocal": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            _c_int_p, _c_int_p, _c_int_p, _c_dbl_p, _c_dbl_p,
@@ -111,7 +113,7 @@ SIGNATURES = {
                                            _vp, _vp, _vp]),
 }
 NENERGY = 12
-E_EXC, E_MUXC, E_HART, E_EXT, E_EWD, E_EXT_G0, E_KE, E_NL, E_TOT, E_FICT = range(10)
+E_EXC, E_MUXC, E_HART, E_EXT, E_EWD, E_EXT_G0, E_KE, E_NL, E_TOT, E_FICT, E_EXC_GGA = range(11)
 
 
 class CpstepError(RuntimeError):

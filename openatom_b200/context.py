@@ -270,6 +270,25 @@ class StepContext:
         _lib.call("cpstep_vks_from_rho", self._h, ptr(rho), ptr(v), ptr(e), ptr(f))
         return v, e, f
 
+    XC = {"pz_lda": 0, "blyp": 1}
+
+    def set_xc(self, functional="pz_lda", gradient_cutoff=5.0e-5):
+        """Exchange-correlation functional of the density side and the step:
+        "pz_lda" (default) or "blyp" (Slater exchange + Becke 88 + LYP, the
+        reference's cp_becke / cp_lyp options) with its density cut-off."""
+        _lib.call("cpstep_set_xc", self._h, self.XC[functional], float(gradient_cutoff))
+
+    def gga_functional(self, rho, gx, gy, gz, vks):
+        """CP_getGGAFunctional on given density gradients: returns (vks + df/drho,
+        ux, uy, uz, E_GGA) with u = unit(grad rho) df/d|grad rho|."""
+        self._sync_stream()
+        v = vks.clone()
+        ux, uy, uz = gx.clone(), gy.clone(), gz.clone()
+        e = self._energies()
+        _lib.call("cpstep_gga_functional", self._h, ptr(rho), ptr(ux), ptr(uy), ptr(uz), ptr(v),
+                  ptr(e))
+        return v, ux, uy, uz, e
+
     # -- electronic step -----------------------------------------------------
     def set_cp_mass(self, tau_fs=25.0, cut_ry=None):
         """set_cpmass: CP coefficient masses (cut defaults to the state cutoff)."""

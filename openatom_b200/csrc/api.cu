@@ -452,8 +452,30 @@ int cpstep_vks_from_rho(cpstep_ctx* c, const double* d_rho_r, double* d_vks_r,
   if (!c || !d_rho_r || !d_vks_r || !d_energies) return CPSTEP_ERR_ARG;
   if (int rc = rho_xc(c, d_rho_r, d_vks_r, d_energies)) return rc;
   if (int rc = rho_r2g(c, d_rho_r)) return rc;
+  if (c->xc == CPSTEP_XC_BLYP)
+    if (int rc = rho_gga(c, d_rho_r, d_vks_r, d_energies)) return rc;
   if (int rc = rho_hart(c, d_energies, d_force)) return rc;
   return rho_vks_r(c, d_vks_r);
+}
+
+int cpstep_set_xc(cpstep_ctx* c, int functional, double gradient_cutoff) {
+  if (!c || (functional != CPSTEP_XC_PZ_LDA && functional != CPSTEP_XC_BLYP))
+    return CPSTEP_ERR_ARG;
+  graph_drop(c);
+  if (functional == CPSTEP_XC_BLYP && !c->d_gga_r) {
+    const size_t nr = (size_t)c->nx * c->ny * c->nz;
+    CPSTEP_CUDA_TRY(cudaMalloc(&c->d_gga_r, sizeof(double) * 3 * nr));
+    CPSTEP_CUDA_TRY(cudaMalloc(&c->d_gga_g, sizeof(double2) * 4 * (size_t)c->rg.npts));
+  }
+  c->xc = functional;
+  c->gga_cut = gradient_cutoff > 0.0 ? gradient_cutoff : 5.0e-5;
+  return CPSTEP_OK;
+}
+
+int cpstep_gga_functional(cpstep_ctx* c, const double* d_rho, double* d_gx, double* d_gy,
+                          double* d_gz, double* d_vks, double* d_energies) {
+  if (!c || !d_rho || !d_gx || !d_gy || !d_gz || !d_vks || !d_energies) return CPSTEP_ERR_ARG;
+  return rho_gga_functional(c, d_rho, d_gx, d_gy, d_gz, d_vks, d_energies, 0);
 }
 
 int cpstep_nl_grid_size(int kmax, double scale, int n_interp) {

@@ -214,6 +214,12 @@ struct cpstep_ctx {
   AtomData atoms;
   NlData nl;
   int rho_izero = -1;
+  // exchange-correlation functional (CPSTEP_XC_*) and the BLYP scratch: the
+  // three gradient grids [3][N_r] and four packed density-sphere arrays
+  int xc = 0;
+  double gga_cut = 5.0e-5;
+  double* d_gga_r = nullptr;
+  double2* d_gga_g = nullptr;
   double* d_energies = nullptr;  // [CPSTEP_NENERGY]
   // electronic step
   int* d_cls = nullptr;      // point class (0 redundant Gx=0, 1 G=0, 2 unique Gx=0, 3 Gx>0)
@@ -349,6 +355,9 @@ int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* p
 int atoms_set_positions(cpstep_ctx* c, const double* h_pos);
 int rho_xc(cpstep_ctx* c, const double* rho_r, double* vxc, double* energies);
 int rho_r2g(cpstep_ctx* c, const double* rho_r);
+int rho_gga(cpstep_ctx* c, const double* rho_r, double* vks_r, double* energies);
+int rho_gga_functional(cpstep_ctx* c, const double* rho_r, double* gx, double* gy, double* gz,
+                       double* vks_r, double* energies, int add_to_exc);
 int rho_hart(cpstep_ctx* c, double* energies, double* force);
 int rho_vks_r(cpstep_ctx* c, double* vks_r);
 int rho_conj_scale(cpstep_ctx* c, const double* in, double* out, int n, double s);

@@ -1,8 +1,14 @@
-// Density side of the step: PZ-LDA exchange-correlation, the density FFT on
-// the density sphere, Hartree + local pseudopotential + reciprocal Ewald in G
-// space with the atom forces, and V_KS(r).
+// Density side of the step: PZ-LDA or BLYP exchange-correlation, the density
+// FFT on the density sphere, Hartree + local pseudopotential + reciprocal
+// Ewald in G space with the atom forces, and V_KS(r).
 //
 //   CPXCFNCTS::CP_exc_calc       src_piny_physics_v1.0/abinito_physics/cp_xc_fnctl/cp_pz_lda.C:23-170
+//   BLYP gradient correction     CP_getGGAFunctional (cp_xc_fnctl/cp_grad_rho_ctrl.C:32-193),
+//                                becke_gcx_lda / lyp_gcc (cp_becke.C:20-173); gradients and
+//                                White-Bird term CP_Rho_GSpacePlane::divRhoVksGspace /
+//                                acceptWhiteByrd (CP_Rho_GSpacePlane.C:278-400),
+//                                CP_Rho_RealSpacePlane::whiteByrdFFT / acceptWhiteByrd
+//                                (CP_Rho_RealSpacePlane.C:1237-1340)
 //   CPLOCAL::CP_hart_eext_calc   src_piny_physics_v1.0/abinito_physics/cp_local/cp_hart_ext.C:56-405
 //   CP_get_vpsnow (spline)       cp_hart_ext.C:433-475
 //   density FFTs                 CP_Rho_RealSpacePlane::fftRhoRtoRhoG (cp_density_ctrl/
@@ -28,8 +34,10 @@ namespace rho {
 // PZ-LDA constants (cp_pz_lda.C:47-53)
 __constant__ double kPZ[7] = {-0.14230, 1.05290, 0.33340, 0.03110, -0.0480, 0.00200, -0.01160};
 
+// corr = 0 drops the PZ correlation (cp_lyp = 1: BLYP's LDA part is Slater
+// exchange only, cp_pz_lda.C:62-63)
 __global__ void k_xc(const double* __restrict__ rho, double* __restrict__ vxc, size_t n,
-                     double* __restrict__ part) {
+                     double corr, double* __restrict__ part) {
   __shared__ double red[32];
   const double gamma = kPZ[0], beta1 = kPZ[1], beta2 = kPZ[2], au = kPZ[3], bu = kPZ[4],
                cu = kPZ[5], du = kPZ[6];
@@ -55,6 +63,8 @@ __global__ void k_xc(const double* __restrict__ rho, double* __restrict__ vxc, s
         mufact = au * lnrs + (bu - third * au) + 2.0 * third * cu * rs * lnrs +
                  third * (2.0 * du - cu) * rs;
       }
+      cfact *= corr;
+      mufact *= corr;
       ex += xfact * r;
       ec += cfact * r;
       v = xfact + mufact;
@@ -352,6 +362,167 @@ __global__ void k_conj_scale(const double2* __restrict__ in, double2* __restrict
 
 // ===========================================================================
 
+
+namespace rho {
+
+// ---- BLYP (Becke 88 exchange gradient correction + LYP correlation)
+
+// becke_gcx_lda (cp_becke.C:44-73): the spin density rho/2, |grad|^2/4
+__device__ void becke_gcx(double rho, double g2, double& f, double& dfdn, double& dfdg) {
+  const double beta = 0.0042;  // cp_grad_rho_ctrl.C:53
+  rho *= 0.5;
+  g2 *= 0.25;
+  const double r13 = cbrt(rho), r43 = rho * r13;
+  const double x = sqrt(g2) / r43;
+  const double root = sqrt(1.0 + x * x);
+  const double asinch = log(x + root);
+  const double bterm = 1.0 + 6.0 * beta * x * asinch;
+  const double bx = x * x / bterm, bxx = x / bterm;
+  const double bpx = 2.0 * bxx - 6.0 * beta * bxx * bxx * (asinch + x / root);
+  f = -2.0 * beta * r43 * bx;
+  dfdn = -beta * ((4.0 / 3.0) * r13 * (bx - x * bpx));
+  dfdg = -beta * bpx;
+}
+
+// lyp_gcc (cp_becke.C:121-170)
+__device__ void lyp_gcc(double rho, double g2, double& f, double& dfdn, double& dfdg) {
+  const double a = 0.049180, b = 0.1320, c = 0.25330, d = 0.3490;
+  const double cf = 0.30 * 9.570780000627304;  // 0.3 (3 pi^2)^{2/3}
+  const double drho = sqrt(g2);
+  const double r13 = cbrt(rho);                 // rho^{1/3}
+  const double rm13 = 1.0 / r13;                // rho^{-1/3}
+  const double rm43 = rm13 / rho;               // rho^{-4/3}
+  const double rm113 = rm13 * rm13 / (rho * rho * rho);  // rho^{-11/3}
+  const double den = 1.0 + d * rm13, den2 = den * den;
+  const double cexp = exp(-c * rm13);
+  const double omega = cexp * rm113 / den;
+  double br = (d * rm43 + den * (c * rm43 - 11.0 / rho)) / 3.0;
+  const double domega = omega * br / den;
+  const double delta = c * rm13 + d * rm13 / den;
+  br = (d * rm13 - den) * d * rm43 / den2;
+  const double ddelta = (-c * rm43 + br) / 3.0;
+  const double rho2 = rho * rho;
+  const double term1 = -a * rho / den;
+  const double br1 = ((5.0 - 7.0 / 6.0 * delta) / 3.0) * g2;
+  const double r83 = rho2 * r13 * r13;          // rho^{8/3}
+  const double br2 = 4.0 * cf * r83 + br1;
+  const double br3 = (0.250 * br2 - 11.0 * g2 / 24.0) * rho2;
+  const double term2 = -a * b * omega * br3;
+  const double arho = 0.250 * br2 - 11.0 * g2 / 24.0;
+  const double darho = 0.250 * (32.0 * cf * (rho * r13 * r13) / 3.0 - 7.0 / 18.0 * ddelta * g2);
+  const double dprho = 2.0 * arho * rho + darho * rho2;
+  const double dterm1 = -a * (1.0 + (4.0 / 3.0) * d * rm13) / den2;
+  const double dterm2 = -a * b * (domega * br3 + omega * dprho);
+  f = term1 + term2;
+  dfdn = dterm1 + dterm2;
+  dfdg = -a * b * omega * (0.50 * ((5.0 - 7.0 / 6.0 * delta) / 3.0) - 11.0 / 12.0) * rho2 * drho;
+}
+
+// CP_getGGAFunctional's point loop (cp_grad_rho_ctrl.C:81-176): vks += df/drho,
+// g <- unit(grad rho) df/d|grad rho| in place, block partials of ex + ec
+__global__ void k_gga(const double* __restrict__ rho, double* __restrict__ gx,
+                      double* __restrict__ gy, double* __restrict__ gz, double* __restrict__ vks,
+                      size_t n, double rho_cut, double heali, double* __restrict__ part) {
+  __shared__ double red[32];
+  double e = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double r = rho[i];
+    double ux = 0.0, uy = 0.0, uz = 0.0;
+    if (r > rho_cut) {
+      const double x = gx[i], y = gy[i], z = gz[i];
+      const double g2 = x * x + y * y + z * z;
+      double rsw = (r - rho_cut) * heali;
+      rsw = fmin(fmax(rsw, 0.0), 1.0);
+      const double srho = rsw * rsw * (3.0 - 2.0 * rsw);
+      const double dsrho = 6.0 * rsw * (1.0 - rsw) * heali;
+      double fx, dfx, dgx, fc, dfc, dgc;
+      becke_gcx(r, g2, fx, dfx, dgx);
+      lyp_gcc(r, g2, fc, dfc, dgc);
+      dfx = dfx * srho + fx * dsrho;
+      dfc = dfc * srho + fc * dsrho;
+      e += (fx + fc) * srho;
+      vks[i] += dfx + dfc;
+      if (g2 > 0.0) {
+        const double s = (dgx + dgc) * srho / sqrt(g2);
+        ux = x * s;
+        uy = y * s;
+        uz = z * s;
+      }
+    }
+    gx[i] = ux;
+    gy[i] = uy;
+    gz[i] = uz;
+  }
+  e = block_sum(e, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = e;
+}
+
+// E_GGA = sum * scale -> energies[EXC_GGA] (and added to EXC when asked)
+__global__ void k_gga_energy(const double* __restrict__ part, int nblk, double scale,
+                             int add_to_exc, double* __restrict__ energies) {
+  __shared__ double red[32];
+  double e = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) e += part[i];
+  e = block_sum(e, red);
+  if (threadIdx.x == 0) {
+    energies[CPSTEP_E_EXC_GGA] = e * scale;
+    if (add_to_exc) energies[CPSTEP_E_EXC] += e * scale;
+  }
+}
+
+__device__ __forceinline__ void gvec(const double* hmati, int a, int b, int c, double (&g)[3]) {
+  const double tpi = 2.0 * M_PI;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    g[d] = tpi * ((double)a * hmati[3 * d] + (double)b * hmati[3 * d + 1] +
+                  (double)c * hmati[3 * d + 2]);
+}
+
+// The transformed density held here is conj of the reference's rho(G) and the
+// G -> r transform sums c(G) e^{-iG.r}: the gradient's input is then
+// -i g_d (transformed rho) / vol, as in divRhoVksGspace (times -i g, the
+// backward FFTs scaled 1/vol).  out[d][p], d = x, y, z.
+__global__ void k_grad_g(const double2* __restrict__ rhog, const int* __restrict__ kx,
+                         const int* __restrict__ ky, const int* __restrict__ kz, int np,
+                         const double* __restrict__ hmati, double inv_vol,
+                         double2* __restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  double g[3];
+  gvec(hmati, kx[p], ky[p], kz[p], g);
+  const double2 v = rhog[p];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    out[(size_t)d * np + p] = make_double2(g[d] * v.y * inv_vol, -g[d] * v.x * inv_vol);
+}
+
+// White-Bird: w(G) = -i g . u(G) (acceptWhiteByrd), u transformed with 1/N
+__global__ void k_div_g(const double2* __restrict__ u, const int* __restrict__ kx,
+                        const int* __restrict__ ky, const int* __restrict__ kz, int np,
+                        const double* __restrict__ hmati, double2* __restrict__ w) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  double g[3];
+  gvec(hmati, kx[p], ky[p], kz[p], g);
+  double sx = 0.0, sy = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double2 v = u[(size_t)d * np + p];
+    sx += g[d] * v.x;
+    sy += g[d] * v.y;
+  }
+  w[p] = make_double2(sy, -sx);
+}
+
+__global__ void k_sub(double* __restrict__ a, const double* __restrict__ b, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    a[i] -= b[i];
+}
+
+}  // namespace rho
+
 static int upload_i(int** d, const std::vector<int>& h) {
   CPSTEP_CUDA_TRY(cudaMalloc(d, sizeof(int) * std::max<size_t>(1, h.size())));
   CPSTEP_CUDA_TRY(cudaMemcpy(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
@@ -427,6 +598,9 @@ void rho_free(cpstep_ctx* c) {
   cudaFree(r.line_zpos); cudaFree(r.line_xy); cudaFree(r.kx); cudaFree(r.ky); cudaFree(r.kz);
   cudaFree(r.g2); cudaFree(r.wpt); cudaFree(r.pen_a); cudaFree(r.pen_b); cudaFree(r.rhog);
   cudaFree(r.vg); cudaFree(r.fterm); cudaFree(r.vhl); cudaFree(r.part);
+  cudaFree(c->d_gga_r); cudaFree(c->d_gga_g);
+  c->d_gga_r = nullptr;
+  c->d_gga_g = nullptr;
   cudaFree(c->d_energies);
   AtomData& a = c->atoms;
   cudaFree(a.typ); cudaFree(a.frac); cudaFree(a.q); cudaFree(a.vps); cudaFree(a.gzvps);
@@ -546,7 +720,8 @@ int atoms_set_positions(cpstep_ctx* c, const double* h_pos) {
 int rho_xc(cpstep_ctx* c, const double* rho_r, double* vxc, double* energies) {
   size_t nr = (size_t)c->nx * c->ny * c->nz;
   RhoGeom& r = c->rg;
-  rho::k_xc<<<r.nblk_xc, 256, 0, c->stream>>>(rho_r, vxc, nr, r.part);
+  rho::k_xc<<<r.nblk_xc, 256, 0, c->stream>>>(rho_r, vxc, nr,
+                                              c->xc == CPSTEP_XC_BLYP ? 0.0 : 1.0, r.part);
   CPSTEP_LAUNCH_CHECK();
   rho::k_sum_cols<<<2, 256, 0, c->stream>>>(r.part, r.nblk_xc, 2, energies + CPSTEP_E_EXC,
                                             c->vol / (double)nr);
@@ -559,6 +734,57 @@ int rho_r2g(cpstep_ctx* c, const double* rho_r) {
   FftJob j = rho_job(c);
   double scale = c->vol / ((double)c->nx * c->ny * c->nz);
   return c->ops64.r2g(c, j, rho_r, reinterpret_cast<double*>(c->rg.rhog), 1, scale);
+}
+
+// CP_getGGAFunctional on given gradients (overwritten with the u terms)
+int rho_gga_functional(cpstep_ctx* c, const double* rho_r, double* gx, double* gy, double* gz,
+                       double* vks_r, double* energies, int add_to_exc) {
+  const size_t nr = (size_t)c->nx * c->ny * c->nz;
+  RhoGeom& r = c->rg;
+  const double rho_cut = 0.1 * c->gga_cut, heali = 1.0 / (3.9 * c->gga_cut);
+  rho::k_gga<<<r.nblk_xc, 256, 0, c->stream>>>(rho_r, gx, gy, gz, vks_r, nr, rho_cut, heali,
+                                               r.part);
+  CPSTEP_LAUNCH_CHECK();
+  rho::k_gga_energy<<<1, 256, 0, c->stream>>>(r.part, r.nblk_xc, c->vol / (double)nr,
+                                              add_to_exc, energies);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
+// BLYP gradient correction after rho_r2g (r.rhog holds the transformed
+// density): gradients, the functional, the White-Bird term subtracted from vks
+int rho_gga(cpstep_ctx* c, const double* rho_r, double* vks_r, double* energies) {
+  if (!c->d_gga_r || !c->d_gga_g) {
+    cpstep_set_error("gga: BLYP scratch not allocated (cpstep_set_xc)");
+    return CPSTEP_ERR_STATE;
+  }
+  const size_t nr = (size_t)c->nx * c->ny * c->nz;
+  RhoGeom& r = c->rg;
+  FftJob j = rho_job(c);
+  const int np = r.npts;
+  double* gr = c->d_gga_r;
+  double2* gg = c->d_gga_g;
+  rho::k_grad_g<<<cdiv(np, 256), 256, 0, c->stream>>>(r.rhog, r.kx, r.ky, r.kz, np, c->d_hmati,
+                                                      1.0 / c->vol, gg);
+  CPSTEP_LAUNCH_CHECK();
+  for (int d = 0; d < 3; ++d)
+    if (int rc = c->ops64.g2r(c, j, reinterpret_cast<const double*>(gg + (size_t)d * np),
+                              gr + d * nr, 1))
+      return rc;
+  if (int rc = rho_gga_functional(c, rho_r, gr, gr + nr, gr + 2 * nr, vks_r, energies, 1))
+    return rc;
+  for (int d = 0; d < 3; ++d)  // u scaled 1/N on the way (whiteByrdFFT)
+    if (int rc = c->ops64.r2g(c, j, gr + d * nr, reinterpret_cast<double*>(gg + (size_t)d * np),
+                              1, 1.0 / (double)nr))
+      return rc;
+  rho::k_div_g<<<cdiv(np, 256), 256, 0, c->stream>>>(gg, r.kx, r.ky, r.kz, np, c->d_hmati,
+                                                     gg + 3 * (size_t)np);
+  CPSTEP_LAUNCH_CHECK();
+  if (int rc = c->ops64.g2r(c, j, reinterpret_cast<const double*>(gg + 3 * (size_t)np), r.vhl, 1))
+    return rc;
+  rho::k_sub<<<2 * c->num_sms, 256, 0, c->stream>>>(vks_r, r.vhl, nr);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
 }
 
 // Hartree + local + Ewald from r.rhog: conj(vks) in r.vg, energies, force terms

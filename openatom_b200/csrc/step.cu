@@ -250,6 +250,7 @@ int step_run(cpstep_ctx* c, double* psi, double* vpsi, const double* occ, double
   mark(1);
   if ((rc = rho_xc(c, c->d_rho, c->d_vks, energies))) return rc;
   if ((rc = rho_r2g(c, c->d_rho))) return rc;
+  if (c->xc == CPSTEP_XC_BLYP && (rc = rho_gga(c, c->d_rho, c->d_vks, energies))) return rc;
   if ((rc = rho_hart(c, energies, atom_force))) return rc;
   if ((rc = rho_vks_r(c, c->d_vks))) return rc;
   mark(2);

@@ -79,13 +79,17 @@ def constrain(F, psi, lay):
     return F - 0.5 * w[None] * (lam.T @ psi), lam
 
 
-def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None):
+def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None, xc="pz_lda"):
     """Energies, V_KS, constrained-force input F and atom forces (local + Ewald,
     plus the EES non-local pass when nonlocal_on: addForces adds its psi force,
-    stateSlab.C:240-272)."""
+    stateSlab.C:240-272).  xc = "blyp" takes the BLYP potential of oracle/xc.py."""
     vol = sysm.box_len ** 3
     rho = OF.density(psi, lay, occ, vol, chunk=chunk)
-    vxc, exc, muxc = OD.pz_lda(rho, vol)
+    if xc == "blyp":
+        from . import xc as OX
+        vxc, exc, muxc, _ = OX.blyp_vxc(rho, dlay, vol)
+    else:
+        vxc, exc, muxc = OD.pz_lda(rho, vol)
     rg = OD.rho_to_g(rho, dlay, vol)
     vg, eh, ee, ew, floc = OD.hart_eext(rg, dlay.kx, dlay.ky, dlay.kz, sysm.box_len,
                                        0.5 * sysm.ecut_ry, sysm.atoms_dict(), sysm.tab,
@@ -106,8 +110,10 @@ def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None):
     return en, F, floc, rho, vks
 
 
-def cp_step(psi, v, occ, sysm, lay, dlay, cmass, dt, iteration, nonlocal_on=False, nkf=None):
-    en, F, floc, rho, vks = forces(psi, occ, sysm, lay, dlay, nonlocal_on=nonlocal_on, nkf=nkf)
+def cp_step(psi, v, occ, sysm, lay, dlay, cmass, dt, iteration, nonlocal_on=False, nkf=None,
+            xc="pz_lda"):
+    en, F, floc, rho, vks = forces(psi, occ, sysm, lay, dlay, nonlocal_on=nonlocal_on, nkf=nkf,
+                                   xc=xc)
     Fc, lam = constrain(F, psi, lay)
     psi2, v2, ke = integrate(Fc, psi, v, cmass, lay, dt, iteration)
     en["FICT"] = ke
