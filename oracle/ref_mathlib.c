@@ -35,3 +35,29 @@ void rs_(int* nm, int* n, double* a, double* w, int* matz, double* z, double* fv
 }
 
 void cputime(double* t) { *t = (double)clock() / CLOCKS_PER_SEC; }
+
+/* DGEMV (BLAS): y = alpha op(A) x + beta y, A column-major lda x n (m rows),
+ * op = A for 'N', A^T for 'T'; y is not read when beta is 0. */
+void DGEMV(char* trans, int* m, int* n, double* alpha, double* a, int* lda, double* x,
+           int* incx, double* beta, double* y, int* incy) {
+  const int t = (*trans == 'T' || *trans == 't' || *trans == 'C' || *trans == 'c');
+  const int leny = t ? *n : *m, lenx = t ? *m : *n;
+  for (int i = 0; i < leny; ++i) {
+    double acc = 0.0;
+    for (int l = 0; l < lenx; ++l) {
+      const double av = t ? a[l + (long)i * *lda] : a[i + (long)l * *lda];
+      acc += av * x[(long)l * *incx];
+    }
+    double* yi = &y[(long)i * *incy];
+    *yi = *alpha * acc + (*beta == 0.0 ? 0.0 : *beta * *yi);
+  }
+}
+
+/* ZGEMV: only the non-double-packed reference paths call it; the oracle
+ * uses the double-packed ones. */
+void ZGEMV(char* trans, int* m, int* n, void* alpha, void* a, int* lda, void* x, int* incx,
+           void* beta, void* y, int* incy) {
+  (void)trans; (void)m; (void)n; (void)alpha; (void)a; (void)lda; (void)x; (void)incx;
+  (void)beta; (void)y; (void)incy;
+  fprintf(stderr, "ZGEMV is not provided by the oracle's math shim\n");
+}
