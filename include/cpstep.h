@@ -372,6 +372,22 @@ CPSTEP_API int cpstep_nl_grid_size(int kmax, double scale, int n_interp);
 CPSTEP_API int cpstep_set_nonlocal(cpstep_ctx* ctx, int nkf, int n_interp, int nchan,
                                    const int* ch_type, const int* ch_l, const int* ch_m,
                                    const double* vnl, const double* gz0, const double* vnorm);
+/* Structure-factor (non-EES) non-local path, l = 0 (the reference's path with
+ * EES off: CP_calc_Struct_Fact cp_nonlocal/cp_struct_fact.C:33-221,
+ * CP_enl_matrix_calc cp_nlmat.C:20-92, CP_enl_atm_forc_calc and
+ * CP_enl_force_calc cp_nl_energy_forc.C:29-182).
+ * cpstep_set_nonlocal_sf: channels as cpstep_set_nonlocal, each l = 0, m = 0,
+ *   at most one per type; replaces an EES set-up (and cpstep_set_nonlocal
+ *   replaces this one).  The step then adds this path's energy and forces.
+ * cpstep_sf_nonlocal: for all states, d_energies[NL] = sum_s occ_s sum_a
+ *   vnorm_a/vol z_a^2, d_fpsi -= sum_a z'_a S_a, d_fatm (if not NULL) += the
+ *   atom forces; z'_a = 2 vnorm_a/vol z_a (no occupation factor in the
+ *   forces, as in the reference). */
+CPSTEP_API int cpstep_set_nonlocal_sf(cpstep_ctx* ctx, int nchan, const int* ch_type,
+                                      const int* ch_l, const int* ch_m, const double* vnl,
+                                      const double* gz0, const double* vnorm);
+CPSTEP_API int cpstep_sf_nonlocal(cpstep_ctx* ctx, const double* d_psi, const double* d_occ,
+                                  double* d_fpsi, double* d_energies, double* d_fatm);
 CPSTEP_API int cpstep_ees_nonlocal(cpstep_ctx* ctx, const double* d_psi, const double* d_occ,
                                    double* d_fpsi, double* d_energies, double* d_fatm);
 

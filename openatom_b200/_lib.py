@@ -77,6 +77,9 @@ SIGNATURES = {
                                            _c_int_p, _c_int_p, _c_int_p, _c_dbl_p, _c_dbl_p,
                                            _c_dbl_p]),
     "cpstep_ees_nonlocal": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "cpstep_set_nonlocal_sf": (ctypes.c_int, [_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p,
+                                              _c_dbl_p, _c_dbl_p, _c_dbl_p]),
+    "cpstep_sf_nonlocal": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "cpstep_set_cp_mass": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
     "cpstep_cp_integrate": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int,
                                            _vp]),

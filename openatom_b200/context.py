@@ -217,6 +217,32 @@ class StepContext:
         _lib.call("cpstep_ees_nonlocal", self._h, ptr(psi), ptr(occ), ptr(fpsi), ptr(e), ptr(f))
         return fpsi, e, f
 
+    def set_nonlocal_sf(self, system):
+        """Structure-factor (non-EES) non-local path with the l = 0 channels of
+        `system` (cpstep_set_nonlocal_sf); replaces an EES set-up."""
+        import numpy as np
+        chans = [c for c in system.channels if c["l"] == 0]
+        ct, pct = _lib.int_array([c["type"] for c in chans])
+        cl, pcl = _lib.int_array([0 for _ in chans])
+        cm, pcm = _lib.int_array([0 for _ in chans])
+        vnl = np.ascontiguousarray(np.stack([c["vnl"] for c in chans]), dtype=np.float64)
+        gz = np.ascontiguousarray([c["gzvps0"] for c in chans], dtype=np.float64)
+        vn = np.ascontiguousarray([c["vnorm"] for c in chans], dtype=np.float64)
+        dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        self._sync_stream()
+        _lib.call("cpstep_set_nonlocal_sf", self._h, len(chans), pct, pcl, pcm, dp(vnl), dp(gz),
+                  dp(vn))
+
+    def sf_nonlocal(self, psi, occ, fpsi=None, forces=True):
+        """Structure-factor non-local pass: (fpsi accumulated, energies, atom forces)."""
+        self._sync_stream()
+        if fpsi is None:
+            fpsi = torch.zeros_like(psi)
+        e = self._energies()
+        f = torch.zeros((self.natm, 3), dtype=torch.float64, device=self.device) if forces else None
+        _lib.call("cpstep_sf_nonlocal", self._h, ptr(psi), ptr(occ), ptr(fpsi), ptr(e), ptr(f))
+        return fpsi, e, f
+
     def rho_layout(self):
         import numpy as np
         n = ctypes.c_int()

@@ -289,6 +289,7 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   for (auto& e : c->prof_ev) cudaEventDestroy(e);
   nl_free(c);
+  sf_free(c);
   rho_free(c);
   step_free(c);
   statefft_free(c);
@@ -491,6 +492,25 @@ int cpstep_set_nonlocal(cpstep_ctx* c, int nkf, int n_interp, int nchan, const i
     return CPSTEP_ERR_ARG;
   }
   return nl_set(c, nkf, n_interp, nchan, ch_type, ch_l, ch_m, vnl, gz0, vnorm);
+}
+
+int cpstep_set_nonlocal_sf(cpstep_ctx* c, int nchan, const int* ch_type, const int* ch_l,
+                           const int* ch_m, const double* vnl, const double* gz0,
+                           const double* vnorm) {
+  if (!c || nchan <= 0 || !ch_type || !ch_l || !ch_m || !vnl || !gz0 || !vnorm) {
+    cpstep_set_error("set_nonlocal_sf: bad argument");
+    return CPSTEP_ERR_ARG;
+  }
+  return sf_set(c, nchan, ch_type, ch_l, ch_m, vnl, gz0, vnorm);
+}
+
+int cpstep_sf_nonlocal(cpstep_ctx* c, const double* d_psi, const double* d_occ, double* d_fpsi,
+                       double* d_energies, double* d_fatm) {
+  if (!c || !d_psi || !d_occ || !d_fpsi || !d_energies) {
+    cpstep_set_error("sf_nonlocal: bad argument");
+    return CPSTEP_ERR_ARG;
+  }
+  return sf_run(c, d_psi, d_occ, d_fpsi, d_energies, d_fatm);
 }
 
 int cpstep_ees_nonlocal(cpstep_ctx* c, const double* d_psi, const double* d_occ, double* d_fpsi,

@@ -137,6 +137,20 @@ struct AtomData {
   double* pos = nullptr;  // staging for cpstep_set_positions
 };
 
+// Structure-factor (non-EES) non-local state, l = 0 (cpstep_set_nonlocal_sf).
+struct SfData {
+  int on = 0, n = 0, ldz = 0;       // n non-local atoms (type order)
+  int* atom = nullptr;              // [n] atom index
+  int* ptab = nullptr;              // [n] projector table of the atom's type
+  double* proj = nullptr;           // [tables][npts] y00 v_0(|G|)
+  double* vn = nullptr;             // [n] vnorm / vol
+  double* rows = nullptr;           // [4 n][2 npts] S, S^x, S^y, S^z (real view)
+  double* z = nullptr;              // [nstates][4 n] projections
+  double* zs = nullptr;             // [nstates][ldz] 2 vnorm/vol z
+  double* enl_s = nullptr;          // [nstates]
+  double* fnl = nullptr;            // [nstates][natm][3]
+};
+
 // EES non-local state of a context (cpstep_set_nonlocal).
 struct NlData {
   int on = 0, nkf = 0, nchan = 0;
@@ -213,6 +227,7 @@ struct cpstep_ctx {
   RhoGeom rg;
   AtomData atoms;
   NlData nl;
+  SfData sf;
   int rho_izero = -1;
   // exchange-correlation functional (CPSTEP_XC_*) and the BLYP scratch: the
   // three gradient grids [3][N_r] and four packed density-sphere arrays
@@ -341,6 +356,11 @@ int statefft_lookup(int precision, int n, StateFftOps* o);
 int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, const int* ch_l,
            const int* ch_m, const double* vnl, const double* gz0, const double* vnorm);
 void nl_free(cpstep_ctx* c);
+int sf_set(cpstep_ctx* c, int nchan, const int* ch_type, const int* ch_l, const int* ch_m,
+           const double* vnl, const double* gz0, const double* vnorm);
+void sf_free(cpstep_ctx* c);
+int sf_run(cpstep_ctx* c, const double* psi, const double* occ, double* fpsi, double* energies,
+           double* fatm);
 int nl_run(cpstep_ctx* c, const double* psi, const double* occ, double* fpsi, double* energies,
            double* fatm);
 int nl_grid_size(int kmax, double scale, int n_interp);

@@ -487,6 +487,7 @@ int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, 
     return CPSTEP_ERR_ARG;
   }
   nl_free(c);
+  sf_free(c);  // the structure-factor path and this one exclude each other
   NlData& n = c->nl;
   n.nkf = nkf;
   n.nchan = nchan;

@@ -257,9 +257,11 @@ int step_run(cpstep_ctx* c, double* psi, double* vpsi, const double* occ, double
   // 2. V.psi force with the kinetic term (z-pencils of psi are still valid)
   if ((rc = statefft_vpsi(c, psi, c->d_vks, occ, c->d_force, c->d_eke, 1))) return rc;
   mark(3);
-  // 2b. EES non-local energy, psi force and atom forces
+  // 2b. non-local energy, psi force and atom forces (EES or structure factors)
   if (c->nl.on) {
     if ((rc = nl_run(c, psi, occ, c->d_force, energies, atom_force))) return rc;
+  } else if (c->sf.on) {
+    if ((rc = sf_run(c, psi, occ, c->d_force, energies, atom_force))) return rc;
   } else {
     CPSTEP_CUDA_TRY(cudaMemsetAsync(energies + CPSTEP_E_NL, 0, sizeof(double), c->stream));
   }

@@ -67,3 +67,33 @@ def sf_nonlocal(psi, occ, vol, s, sd, vnorm):
     f = -np.stack([np.sum(zs * zd[d], axis=1) for d in range(3)], axis=1)
     fpsi_r = -(zs.T @ real_view(s))                            # [S, 2 npts]
     return enl, f, fpsi_r.view(np.complex128)
+
+
+def system_tables(sysm):
+    """(order, proj [natm_nl, npts], vnorm [natm_nl]) for a System's l = 0
+    channels: the non-local atoms in type order (the reference's map_nl) with
+    y00 v_0(|G|) of their type on the state layout."""
+    lay = sysm.layout
+    tab = sysm.tab
+    ch0 = {c["type"]: c for c in sysm.channels if c["l"] == 0}
+    order = np.array([i for i in np.argsort(sysm.typ, kind="stable") if sysm.typ[i] in ch0])
+    tpi = 2.0 * math.pi / sysm.box_len
+    g = np.sqrt((lay.kx * tpi) ** 2 + (lay.ky * tpi) ** 2 + (lay.kz * tpi) ** 2)
+    y00 = 1.0 / math.sqrt(4.0 * math.pi)
+    proj = np.stack([y00 * spline_l0(g, ch0[sysm.typ[i]]["vnl"], ch0[sysm.typ[i]]["gzvps0"],
+                                     tab["nspl"], tab["gmin"], tab["dg"]) for i in order])
+    vn0 = np.array([ch0[sysm.typ[i]]["vnorm"] for i in order])
+    return order, proj, vn0
+
+
+def sf_pass(psi, occ, sysm):
+    """The whole pass for a System: (E_NL, atom forces [natm, 3] in atom order,
+    psi force [S, npts])."""
+    lay = sysm.layout
+    order, proj, vn0 = system_tables(sysm)
+    s, sd = struct_fact(lay.kx, lay.ky, lay.kz, sysm.box_len, sysm.pos[order] / sysm.box_len,
+                        proj)
+    enl, f, fpsi = sf_nonlocal(psi, occ, sysm.box_len ** 3, s, sd, vn0)
+    fa = np.zeros((sysm.natm, 3))
+    fa[order] = f
+    return enl, fa, fpsi

@@ -79,7 +79,8 @@ def constrain(F, psi, lay):
     return F - 0.5 * w[None] * (lam.T @ psi), lam
 
 
-def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None, xc="pz_lda"):
+def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None, xc="pz_lda",
+           nonlocal_sf=False):
     """Energies, V_KS, constrained-force input F and atom forces (local + Ewald,
     plus the EES non-local pass when nonlocal_on: addForces adds its psi force,
     stateSlab.C:240-272).  xc = "blyp" takes the BLYP potential of oracle/xc.py."""
@@ -103,6 +104,10 @@ def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None, xc=
                                          dict(pos=sysm.pos, typ=sysm.typ), sysm.channels,
                                          sysm.tab, nkf)
         floc = floc + fatm
+    if nonlocal_sf:  # the structure-factor path (oracle/sf.py)
+        from . import sf as OSF
+        enl, fatm, fnl = OSF.sf_pass(psi, occ, sysm)
+        floc = floc + fatm
     F = OF.add_forces(fv, fnl, lay)
     F, eke = OF.eke(F, psi, lay, occ, sysm.ecut_ry)
     en = dict(EXC=exc, MUXC=muxc, EHART=eh, EEXT=ee, EWD=ew, EKE=float(np.sum(eke)), ENL=enl)
@@ -111,9 +116,9 @@ def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None, xc=
 
 
 def cp_step(psi, v, occ, sysm, lay, dlay, cmass, dt, iteration, nonlocal_on=False, nkf=None,
-            xc="pz_lda"):
+            xc="pz_lda", nonlocal_sf=False):
     en, F, floc, rho, vks = forces(psi, occ, sysm, lay, dlay, nonlocal_on=nonlocal_on, nkf=nkf,
-                                   xc=xc)
+                                   xc=xc, nonlocal_sf=nonlocal_sf)
     Fc, lam = constrain(F, psi, lay)
     psi2, v2, ke = integrate(Fc, psi, v, cmass, lay, dt, iteration)
     en["FICT"] = ke

@@ -39,16 +39,8 @@ def small():
 
 
 def _l0(sysm):
-    lay = sysm.layout
-    tab = sysm.tab
+    order, proj, vn0 = OS.system_tables(sysm)
     ch0 = {c["type"]: c for c in sysm.channels if c["l"] == 0}
-    order = np.argsort(sysm.typ, kind="stable")
-    tpi = 2.0 * math.pi / sysm.box_len
-    g = np.sqrt((lay.kx * tpi) ** 2 + (lay.ky * tpi) ** 2 + (lay.kz * tpi) ** 2)
-    y00 = 1.0 / math.sqrt(4.0 * math.pi)
-    proj = np.stack([y00 * OS.spline_l0(g, ch0[sysm.typ[i]]["vnl"], ch0[sysm.typ[i]]["gzvps0"],
-                                        tab["nspl"], tab["gmin"], tab["dg"]) for i in order])
-    vn0 = np.array([ch0[sysm.typ[i]]["vnorm"] for i in order])
     return order, proj, vn0, [ch0[t] for t in sorted(ch0)]
 
 
