@@ -52,6 +52,8 @@ extern "C" {
 #define CPSTEP_E_FICT 9    /* fictitious kinetic energy (get_fictKE)          */
 #define CPSTEP_E_EXC_GGA 10 /* gradient correction part of EEXC (BLYP:
                                CP_getGGAFunctional exc_gga_ret)               */
+#define CPSTEP_E_EWD_RS 11 /* real-space Ewald + self + background (CP_getionforce:
+                               pot_ewd_rs + vself + vbgr)                    */
 #define CPSTEP_NENERGY 12
 
 /* Exchange-correlation functionals (cpstep_set_xc).  PZ-LDA is the default;
@@ -497,6 +499,22 @@ CPSTEP_API int cpstep_ctx_graph_status(cpstep_ctx* ctx, int* enabled, int* captu
  *   device between steps.  Synchronous.
  */
 CPSTEP_API int cpstep_set_positions(cpstep_ctx* ctx, const double* h_pos);
+
+/* Ions between electronic steps (CPAIMD).
+ * cpstep_ion_forces: CPRSPACEION::CP_getionforce (cp_ions/cp_rspace_ion.C:25-250,
+ *   fully periodic, no Grimme term) at the context's current positions and
+ *   charges: d_fatm [natm][3] += the real-space Ewald forces;
+ *   d_energies[EWD_RS] = pot_ewd_rs + vself + vbgr.
+ * cpstep_atoms_integrate: the NVE step of ATOMINTEGRATE::ctrl_atom_integrate
+ *   (integration_drivers.C:17-88): on device arrays [natm][3], v += dt/2 f/m
+ *   (not when itime == 0), *d_ekin = 1/2 sum m v^2 (may be NULL), v += dt/2 f/m,
+ *   x += dt v; the context's positions then follow d_pos (as
+ *   cpstep_set_positions).  d_fatm holds the total atom forces (the step's
+ *   local, reciprocal Ewald and non-local forces plus cpstep_ion_forces). */
+CPSTEP_API int cpstep_ion_forces(cpstep_ctx* ctx, double* d_fatm, double* d_energies);
+CPSTEP_API int cpstep_atoms_integrate(cpstep_ctx* ctx, int itime, double* d_pos, double* d_vel,
+                                      const double* d_fatm, const double* d_mass, double dt,
+                                      double* d_ekin);
 CPSTEP_API int cpstep_cp_step_host(cpstep_ctx* ctx, double* d_psi, double* d_vpsi,
                                    const double* d_occ, double dt, int iteration,
                                    const double* h_pos, double* h_energies,

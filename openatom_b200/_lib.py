@@ -80,6 +80,9 @@ SIGNATURES = {
     "cpstep_set_nonlocal_sf": (ctypes.c_int, [_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p,
                                               _c_dbl_p, _c_dbl_p, _c_dbl_p]),
     "cpstep_sf_nonlocal": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "cpstep_ion_forces": (ctypes.c_int, [_vp, _vp, _vp]),
+    "cpstep_atoms_integrate": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp,
+                                              ctypes.c_double, _vp]),
     "cpstep_set_cp_mass": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
     "cpstep_cp_integrate": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int,
                                            _vp]),
@@ -116,7 +119,7 @@ SIGNATURES = {
                                            _vp, _vp, _vp]),
 }
 NENERGY = 12
-E_EXC, E_MUXC, E_HART, E_EXT, E_EWD, E_EXT_G0, E_KE, E_NL, E_TOT, E_FICT, E_EXC_GGA = range(11)
+E_EXC, E_MUXC, E_HART, E_EXT, E_EWD, E_EXT_G0, E_KE, E_NL, E_TOT, E_FICT, E_EXC_GGA, E_EWD_RS = range(12)
 
 
 class CpstepError(RuntimeError):

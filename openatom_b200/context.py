@@ -243,6 +243,32 @@ class StepContext:
         _lib.call("cpstep_sf_nonlocal", self._h, ptr(psi), ptr(occ), ptr(fpsi), ptr(e), ptr(f))
         return fpsi, e, f
 
+    def set_positions(self, pos):
+        """New atom positions (natm x 3, bohr, host array): cpstep_set_positions."""
+        import numpy as np
+        p = np.ascontiguousarray(pos, dtype=np.float64)
+        self._sync_stream()
+        _lib.call("cpstep_set_positions", self._h, p.ctypes.data_as(ctypes.c_void_p))
+
+    def ion_forces(self, forces=None):
+        """CP_getionforce: (forces += real-space Ewald forces, energies with
+        EWD_RS = pot_ewd_rs + vself + vbgr) at the context's positions."""
+        self._sync_stream()
+        if forces is None:
+            forces = torch.zeros((self.natm, 3), dtype=torch.float64, device=self.device)
+        e = self._energies()
+        _lib.call("cpstep_ion_forces", self._h, ptr(forces), ptr(e))
+        return forces, e
+
+    def atoms_integrate(self, itime, pos, vel, forces, mass, dt):
+        """NVE velocity-Verlet step of the ions (in place on pos, vel [natm, 3]);
+        the context's positions follow.  Returns E_kin at the step's start."""
+        self._sync_stream()
+        ek = torch.zeros(1, dtype=torch.float64, device=self.device)
+        _lib.call("cpstep_atoms_integrate", self._h, int(itime), ptr(pos), ptr(vel), ptr(forces),
+                  ptr(mass), float(dt), ptr(ek))
+        return float(ek)
+
     def rho_layout(self):
         import numpy as np
         n = ctypes.c_int()

@@ -284,6 +284,7 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
   cudaFree(c->d_dev_err);
   cudaFree(c->d_split);
   cudaFree(c->d_lv);
+  cudaFree(c->d_ion_e);
   cudaFree(c->d_force_atoms);
   graph_drop(c);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -492,6 +493,18 @@ int cpstep_set_nonlocal(cpstep_ctx* c, int nkf, int n_interp, int nchan, const i
     return CPSTEP_ERR_ARG;
   }
   return nl_set(c, nkf, n_interp, nchan, ch_type, ch_l, ch_m, vnl, gz0, vnorm);
+}
+
+int cpstep_ion_forces(cpstep_ctx* c, double* d_fatm, double* d_energies) {
+  if (!c || !d_fatm || !d_energies) return CPSTEP_ERR_ARG;
+  return ion_forces(c, d_fatm, d_energies);
+}
+
+int cpstep_atoms_integrate(cpstep_ctx* c, int itime, double* d_pos, double* d_vel,
+                           const double* d_fatm, const double* d_mass, double dt, double* d_ekin) {
+  if (!c || itime < 0 || !d_pos || !d_vel || !d_fatm || !d_mass || !(dt > 0.0))
+    return CPSTEP_ERR_ARG;
+  return atoms_integrate(c, itime, d_pos, d_vel, d_fatm, d_mass, dt, d_ekin);
 }
 
 int cpstep_set_nonlocal_sf(cpstep_ctx* c, int nchan, const int* ch_type, const int* ch_l,

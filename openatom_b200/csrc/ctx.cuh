@@ -134,7 +134,8 @@ struct AtomData {
   int tstart[CPSTEP_MAX_TYPES + 1] = {};  // type t holds ranks [tstart[t], tstart[t+1])
   int nfblk = 0;           // blocks (rows of fpart) of the force pass
   double* fpart = nullptr;
-  double* pos = nullptr;  // staging for cpstep_set_positions
+  double* pos = nullptr;  // Cartesian positions [natm][3] (bohr)
+  std::vector<double> h_q;  // charges, host copy
 };
 
 // Structure-factor (non-EES) non-local state, l = 0 (cpstep_set_nonlocal_sf).
@@ -233,6 +234,7 @@ struct cpstep_ctx {
   // three gradient grids [3][N_r] and four packed density-sphere arrays
   int xc = 0;
   double gga_cut = 5.0e-5;
+  double* d_ion_e = nullptr;  // [natm] real-space Ewald pair energies
   double* d_gga_r = nullptr;
   double2* d_gga_g = nullptr;
   double* d_energies = nullptr;  // [CPSTEP_NENERGY]
@@ -376,6 +378,10 @@ int atoms_set_positions(cpstep_ctx* c, const double* h_pos);
 int rho_xc(cpstep_ctx* c, const double* rho_r, double* vxc, double* energies);
 int rho_r2g(cpstep_ctx* c, const double* rho_r);
 int rho_gga(cpstep_ctx* c, const double* rho_r, double* vks_r, double* energies);
+int atoms_set_positions_dev(cpstep_ctx* c, const double* d_pos);
+int ion_forces(cpstep_ctx* c, double* fatm, double* energies);
+int atoms_integrate(cpstep_ctx* c, int itime, double* pos, double* vel, const double* fatm,
+                    const double* mass, double dt, double* ekin);
 int rho_gga_functional(cpstep_ctx* c, const double* rho_r, double* gx, double* gy, double* gz,
                        double* vks_r, double* energies, int add_to_exc);
 int rho_hart(cpstep_ctx* c, double* energies, double* force);

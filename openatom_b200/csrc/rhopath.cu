@@ -661,8 +661,11 @@ int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* p
       (rc = upload_d(&a.frac, frac)) ||
       (rc = upload_d(&a.q, std::vector<double>(q, q + ntyp))) ||
       (rc = upload_d(&a.vps, std::vector<double>(vps, vps + (size_t)ntyp * 4 * nspl))) ||
-      (rc = upload_d(&a.gzvps, std::vector<double>(gzvps, gzvps + ntyp))))
+      (rc = upload_d(&a.gzvps, std::vector<double>(gzvps, gzvps + ntyp))) ||
+      (rc = upload_d(&a.pos, std::vector<double>(pos, pos + 3 * (size_t)natm))))
     return rc;
+  a.h_q.resize(natm);
+  for (int i = 0; i < natm; ++i) a.h_q[i] = q[t[i]];
   a.natm = natm;
   a.ntyp = ntyp;
   a.nspl = nspl;
@@ -708,6 +711,24 @@ int atoms_set_positions(cpstep_ctx* c, const double* h_pos) {
   if (!a.pos) CPSTEP_CUDA_TRY(cudaMalloc(&a.pos, sizeof(double) * 3 * a.natm));
   CPSTEP_CUDA_TRY(cudaMemcpyAsync(a.pos, h_pos, sizeof(double) * 3 * a.natm,
                                   cudaMemcpyHostToDevice, c->stream));
+  rho::k_frac<<<cdiv(a.natm, 128), 128, 0, c->stream>>>(a.pos, c->d_hmati, a.natm, a.frac);
+  CPSTEP_LAUNCH_CHECK();
+  rho::k_phase<<<cdiv(a.natm, 128), 128, 0, c->stream>>>(a.frac, a.natm, a.kxm, a.kym, a.kzm,
+                                                          a.rank, a.ex, a.ey, a.ez, a.ezt);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
+// new positions from device memory (the atom integrator's output)
+int atoms_set_positions_dev(cpstep_ctx* c, const double* d_pos) {
+  AtomData& a = c->atoms;
+  if (a.natm <= 0 || !a.pos) {
+    cpstep_set_error("set_positions: no atoms set");
+    return CPSTEP_ERR_STATE;
+  }
+  if (d_pos != a.pos)
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(a.pos, d_pos, sizeof(double) * 3 * a.natm,
+                                    cudaMemcpyDeviceToDevice, c->stream));
   rho::k_frac<<<cdiv(a.natm, 128), 128, 0, c->stream>>>(a.pos, c->d_hmati, a.natm, a.frac);
   CPSTEP_LAUNCH_CHECK();
   rho::k_phase<<<cdiv(a.natm, 128), 128, 0, c->stream>>>(a.frac, a.natm, a.kxm, a.kym, a.kzm,

@@ -12,6 +12,7 @@
 #                                       CP_exc_calc
 #   src_piny_physics_v1.0/abinito_physics/cp_nonlocal/cp_struct_fact.C, cp_nlmat.C,
 #                         cp_nl_energy_forc.C   the structure-factor nonlocal (l = 0)
+#   src_piny_physics_v1.0/abinito_physics/cp_ions/cp_rspace_ion.C   CP_getionforce
 # The shims in oracle/ref_shim stand in for the Charm++/PINY headers, and
 # oracle/ref_mathlib.c for the Fortran GENMATMUL.  Test infrastructure only.
 set -e
@@ -37,7 +38,8 @@ for f in "$PINY/abinito_physics/cp_nonlocal/cp_ees_nonlocal.C" \
          "$PINY/abinito_physics/cp_xc_fnctl/cp_pz_lda.C" "$HERE/ref_xc.cpp" \
          "$PINY/abinito_physics/cp_nonlocal/cp_struct_fact.C" \
          "$PINY/abinito_physics/cp_nonlocal/cp_nlmat.C" \
-         "$PINY/abinito_physics/cp_nonlocal/cp_nl_energy_forc.C" "$HERE/ref_sf.cpp"; do
+         "$PINY/abinito_physics/cp_nonlocal/cp_nl_energy_forc.C" "$HERE/ref_sf.cpp" \
+         "$PINY/abinito_physics/cp_ions/cp_rspace_ion.C" "$HERE/ref_ion.cpp"; do
   g++ $EESFLAGS -c "$f" -o "$OUT/$(basename "$f" | sed 's/\.[Cc]p*$//').o"
 done
 g++ -O2 -fPIC -shared -w -o "$OUT/libref.so" \
@@ -49,5 +51,6 @@ g++ -O2 -fPIC -shared -w -o "$OUT/libref.so" \
   "$HERE/ref_driver.cpp" "$OUT/ref_mathlib.o" \
   "$OUT/cp_ees_nonlocal.o" "$OUT/set_cp_ewald.o" "$OUT/ref_ees.o" \
   "$OUT/cp_becke.o" "$OUT/cp_grad_rho_ctrl.o" "$OUT/cp_pz_lda.o" "$OUT/ref_xc.o" \
-  "$OUT/cp_struct_fact.o" "$OUT/cp_nlmat.o" "$OUT/cp_nl_energy_forc.o" "$OUT/ref_sf.o"
+  "$OUT/cp_struct_fact.o" "$OUT/cp_nlmat.o" "$OUT/cp_nl_energy_forc.o" "$OUT/ref_sf.o" \
+  "$OUT/cp_rspace_ion.o" "$OUT/ref_ion.o"
 echo "$OUT/libref.so"
