@@ -19,13 +19,17 @@
 
 namespace stp {
 
-// v <- v + F dt/(2m) with the reference's Gx=0 / G=0 conventions; optional
-// fictitious kinetic energy at the velocities on entry (get_fictKE).
-__global__ void k_kick(double2* __restrict__ v, const double2* __restrict__ f,
-                       const double* __restrict__ cmass, const int* __restrict__ cls, int npts,
-                       int nstates, double dt2, double* __restrict__ ke_part) {
+// The whole Verlet update in one pass over psi, v and F (the two kicks, the
+// fictitious KE between them, the drift), in the per-element order of the
+// reference's half steps: second half kick of the previous step when
+// `first`, KE, first half kick, psi += v dt.
+__global__ void k_integrate(double2* __restrict__ psi, double2* __restrict__ v,
+                            const double2* __restrict__ f, const double* __restrict__ cmass,
+                            const int* __restrict__ cls, int npts, int nstates, double dt,
+                            int first, double* __restrict__ ke_part) {
   __shared__ double red[32];
   double ke = 0.0;
+  const double dt2 = 0.5 * dt;
   const size_t n = (size_t)npts * nstates;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -36,35 +40,28 @@ __global__ void k_kick(double2* __restrict__ v, const double2* __restrict__ f,
     double2 vv = v[i];
     double2 ff = f[i];
     if (c == 1) { vv.y = 0.0; ff.y = 0.0; }
-    if (ke_part) ke += (vv.x * vv.x + vv.y * vv.y) * (c == 2 ? 2.0 * m : m);
-    double fm = (c == 2) ? (2.0 * dt2) / (2.0 * m) : dt2 / m;
+    const double fm = (c == 2) ? (2.0 * dt2) / (2.0 * m) : dt2 / m;
+    if (first) {
+      vv.x += ff.x * fm;
+      vv.y += ff.y * fm;
+      if (c == 1) vv.y = 0.0;
+    }
+    ke += (vv.x * vv.x + vv.y * vv.y) * (c == 2 ? 2.0 * m : m);
     vv.x += ff.x * fm;
     vv.y += ff.y * fm;
     if (c == 1) vv.y = 0.0;
     v[i] = vv;
-  }
-  if (ke_part) {
-    double t = block_sum(ke, red);
-    if (threadIdx.x == 0) ke_part[blockIdx.x] = 0.5 * t;
-  }
-}
-
-// psi <- psi + v dt on the integrated points, then the redundant half mirrors
-// its partner: psi(0,-ky,-kz) = conj psi(0,ky,kz) (and the same for v).
-__global__ void k_drift(double2* __restrict__ psi, double2* __restrict__ v,
-                        const int* __restrict__ cls, int npts, int nstates, double dt) {
-  const size_t n = (size_t)npts * nstates;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    int p = (int)(i % npts);
-    if (cls[p] == 0) continue;
-    double2 a = psi[i], b = v[i];
-    a.x += b.x * dt;
-    a.y += b.y * dt;
+    double2 a = psi[i];
+    a.x += vv.x * dt;
+    a.y += vv.y * dt;
     psi[i] = a;
   }
+  double t = block_sum(ke, red);
+  if (threadIdx.x == 0) ke_part[blockIdx.x] = 0.5 * t;
 }
 
+// After the drift, the redundant half mirrors its partner:
+// psi(0,-ky,-kz) = conj psi(0,ky,kz) (and the same for v).
 __global__ void k_sync_red(double2* __restrict__ psi, double2* __restrict__ v,
                            const int* __restrict__ red_idx, const int* __restrict__ red_src,
                            int nred, int npts, int nstates) {
@@ -193,20 +190,14 @@ int step_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi
   double2* v = reinterpret_cast<double2*>(vpsi);
   const double2* f = reinterpret_cast<const double2*>(force);
   int nb = c->nblk_ke;
-  if (iteration > 1) {
-    stp::k_kick<<<nb, 256, 0, c->stream>>>(v, f, c->d_cmass, c->d_cls, c->npts, c->nstates,
-                                           0.5 * dt, nullptr);
-    CPSTEP_LAUNCH_CHECK();
-  }
-  stp::k_kick<<<nb, 256, 0, c->stream>>>(v, f, c->d_cmass, c->d_cls, c->npts, c->nstates,
-                                         0.5 * dt, c->d_step_part);
+  stp::k_integrate<<<nb, 256, 0, c->stream>>>(p, v, f, c->d_cmass, c->d_cls, c->npts,
+                                              c->nstates, dt, iteration > 1 ? 1 : 0,
+                                              c->d_step_part);
   CPSTEP_LAUNCH_CHECK();
   if (d_fict_ke) {
     stp::k_sum<<<1, 256, 0, c->stream>>>(c->d_step_part, nb, d_fict_ke);
     CPSTEP_LAUNCH_CHECK();
   }
-  stp::k_drift<<<nb, 256, 0, c->stream>>>(p, v, c->d_cls, c->npts, c->nstates, dt);
-  CPSTEP_LAUNCH_CHECK();
   if (c->nred) {
     stp::k_sync_red<<<nb, 256, 0, c->stream>>>(p, v, c->d_red_idx, c->d_red_src, c->nred, c->npts,
                                                c->nstates);
