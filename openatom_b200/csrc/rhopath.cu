@@ -208,6 +208,7 @@ k_hart_lines(const double2* __restrict__ rhog_t, const int* __restrict__ line_of
       const double2* zc = A.ezt + (c + A.kzm);
       for (int t = 0; t < A.ntyp; ++t) {
         double2 st = make_double2(0.0, 0.0);
+#pragma unroll 4
         for (int i = A.tstart[t]; i < A.tstart[t + 1]; ++i) {
           double2 u = su[i];
           double2 z = zc[(size_t)i * nz];
@@ -305,6 +306,7 @@ __global__ void k_local_forces_lines(const double4* __restrict__ fterm,
           double2 u = make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
           const double2* T = sT + (size_t)t * lmax;
           double px = 0.0, py = 0.0, qx = 0.0, qy = 0.0;
+#pragma unroll 4
           for (int i = 0; i < len; ++i) {
             const int c = skz[i];
             double2 e = A.ez[(size_t)(c + A.kzm) * A.natm + at];
@@ -679,7 +681,7 @@ int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* p
   CPSTEP_CUDA_TRY(cudaMalloc(&a.ey, sizeof(double2) * (2 * a.kym + 1) * natm));
   CPSTEP_CUDA_TRY(cudaMalloc(&a.ez, sizeof(double2) * (2 * a.kzm + 1) * natm));
   CPSTEP_CUDA_TRY(cudaMalloc(&a.ezt, sizeof(double2) * (2 * a.kzm + 1) * natm));
-  a.nfblk = std::max(1, std::min(c->rg.nlines, 2 * c->num_sms));
+  a.nfblk = std::max(1, std::min(c->rg.nlines, 8 * c->num_sms));  // line partials per block
   CPSTEP_CUDA_TRY(cudaMalloc(&a.fpart, sizeof(double) * 3 * (size_t)natm * a.nfblk));
   rho::k_phase<<<cdiv(natm, 128), 128, 0, c->stream>>>(a.frac, natm, a.kxm, a.kym, a.kzm, a.rank,
                                                         a.ex, a.ey, a.ez, a.ezt);
