@@ -54,7 +54,9 @@ extern "C" {
                                CP_getGGAFunctional exc_gga_ret)               */
 #define CPSTEP_E_EWD_RS 11 /* real-space Ewald + self + background (CP_getionforce:
                                pot_ewd_rs + vself + vbgr)                    */
-#define CPSTEP_NENERGY 12
+#define CPSTEP_E_NHC_KE 12 /* ekeNhc: CP thermostat kinetic energy (get_fictKE) */
+#define CPSTEP_E_NHC_POT 13 /* potNHC: CP thermostat potential (get_fictKE)     */
+#define CPSTEP_NENERGY 14
 
 /* Exchange-correlation functionals (cpstep_set_xc).  PZ-LDA is the default;
  * BLYP is Slater exchange (CP_exc_calc with cp_lyp = 1) plus the Becke 88
@@ -401,7 +403,8 @@ CPSTEP_API int cpstep_ees_nonlocal(cpstep_ctx* ctx, const double* d_psi, const d
  *   tau = tau_fs / TIME_CONV, scaled by (g^2/2)/(cut/2) above cut (Ry), G=0 halved.
  * cpstep_cp_integrate: velocity Verlet of CPINTEGRATE::CP_integrate_dyn /
  *   cp_evolve_vel / get_fictKE (cp_integrate/cp_dynamics.C:29-258) on all
- *   states, without the isokinetic Nose-Hoover chains: second half kick of the
+ *   states (with the isokinetic Nose-Hoover chains when cpstep_set_cp_thermostat
+ *   switched them on, below): second half kick of the
  *   previous step when iteration > 1, fictitious KE (d_fict_ke, may be NULL),
  *   first half kick, psi += v dt, then the redundant lower Gx=0 half is
  *   overwritten by the conjugate of its partner (sendRedPsi/unpackRedPsi,
@@ -418,6 +421,36 @@ CPSTEP_API int cpstep_ees_nonlocal(cpstep_ctx* ctx, const double* d_psi, const d
  *   (synchronises the context's stream).
  */
 CPSTEP_API int cpstep_set_cp_mass(cpstep_ctx* ctx, double tau_fs, double cut_ry);
+
+/*
+ * Isokinetic Nose-Hoover chain thermostat of the CP coefficients (ISOKIN_OPT = 1,
+ * cp_integrate/cp_dynamics.C:19).  Replaces (ctx form, one chain set per state):
+ *   CPINTEGRATE::initCPNHC         cp_integrate/cp_isokin.C:45-141
+ *   CPINTEGRATE::cp_isoNHC_update  cp_integrate/cp_isokin.C:150-311
+ *   cp_evolve_vel's thermostat calls (cp_dynamics.C:172-193) and the NHC part of
+ *   get_fictKE (:231-240)
+ * cpstep_set_cp_thermostat: te_ext (K; <= 0 switches the thermostat off and
+ *   cpstep_cp_integrate / cpstep_cp_step return to plain velocity Verlet),
+ *   tau_fs (cp_tau_nhc), num_nhc (cp_num_nhc_iso, 1..8), nck (cp_nhc_chunk,
+ *   1..8), nres (cp_respa_steps_nhc >= 1), nyosh (cp_yosh_steps_nhc in
+ *   {1,3,5,7,9}); reference defaults 2, 1, 4, 9 with tau 25 fs.  Each state's
+ *   non-redundant coefficients (G=0, the unique Gx=0 points, the rest; each in
+ *   packed order) form nck chunks as initCPNHC divides them; masses, barriers
+ *   and degrees of freedom as initCPNHC.  The chains start at x = xp = 0,
+ *   v = (sqrt(kT/mNHC[0]), 0) (on the isokinetic surface); CPSmplVel's random
+ *   sample can be loaded with cpstep_cp_thermostat_state.  Needs the CP masses.
+ *   Drops the step graph.
+ * cpstep_cp_thermostat_state: set (set = 1) or read (set = 0) the chain state,
+ *   host arrays [nstates][nck][num_nhc][2] (xNHC, xNHCP, vNHC; any may be NULL).
+ * With the thermostat on, cpstep_cp_integrate and cpstep_cp_step apply
+ * cp_isoNHC_update after the second half kick of the previous step (iteration
+ * > 1) and before the first half kick, per state and chunk, and the step's
+ * d_energies gain CPSTEP_E_NHC_KE and CPSTEP_E_NHC_POT (zero when off).
+ */
+CPSTEP_API int cpstep_set_cp_thermostat(cpstep_ctx* ctx, double te_ext, double tau_fs,
+                                        int num_nhc, int nck, int nres, int nyosh);
+CPSTEP_API int cpstep_cp_thermostat_state(cpstep_ctx* ctx, int set, double* h_x, double* h_xp,
+                                          double* h_v);
 CPSTEP_API int cpstep_cp_integrate(cpstep_ctx* ctx, const double* d_force, double* d_psi,
                                    double* d_vpsi, double dt, int iteration, double* d_fict_ke);
 CPSTEP_API int cpstep_cp_step(cpstep_ctx* ctx, double* d_psi, double* d_vpsi,

@@ -84,6 +84,10 @@ SIGNATURES = {
     "cpstep_atoms_integrate": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp,
                                               ctypes.c_double, _vp]),
     "cpstep_set_cp_mass": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
+    "cpstep_set_cp_thermostat": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int]),
+    "cpstep_cp_thermostat_state": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp]),
     "cpstep_cp_integrate": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int,
                                            _vp]),
     "cpstep_cp_step": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int, _vp,
@@ -118,8 +122,9 @@ SIGNATURES = {
     "cpstep_cp_step_host": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int,
                                            _vp, _vp, _vp]),
 }
-NENERGY = 12
-E_EXC, E_MUXC, E_HART, E_EXT, E_EWD, E_EXT_G0, E_KE, E_NL, E_TOT, E_FICT, E_EXC_GGA, E_EWD_RS = range(12)
+NENERGY = 14
+(E_EXC, E_MUXC, E_HART, E_EXT, E_EWD, E_EXT_G0, E_KE, E_NL, E_TOT, E_FICT, E_EXC_GGA, E_EWD_RS,
+ E_NHC_KE, E_NHC_POT) = range(14)
 
 
 class CpstepError(RuntimeError):

@@ -347,6 +347,32 @@ class StepContext:
         cut = self.layout.ecut_ry if cut_ry is None else cut_ry
         _lib.call("cpstep_set_cp_mass", self._h, float(tau_fs), float(cut))
 
+    def set_cp_thermostat(self, te_ext, tau_fs=25.0, num_nhc=2, nck=1, nres=4, nyosh=9):
+        """initCPNHC: the isokinetic NHC thermostat of the coefficients
+        (te_ext <= 0 switches it off); defaults as the reference's."""
+        _lib.call("cpstep_set_cp_thermostat", self._h, float(te_ext), float(tau_fs), int(num_nhc),
+                  int(nck), int(nres), int(nyosh))
+        self._nhc_shape = (self.nstates, int(nck), int(num_nhc), 2) if te_ext > 0 else None
+
+    def cp_thermostat_state(self, x=None, xp=None, v=None):
+        """Set the chain state from the given arrays [S][nck][num][2] (those not
+        None), then return (x, xp, v) as numpy arrays."""
+        import numpy as np
+        shp = getattr(self, "_nhc_shape", None)
+        if shp is None:   # the library reports the thermostat as off
+            _lib.call("cpstep_cp_thermostat_state", self._h, 0, None, None, None)
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (x, xp, v)]
+        for a in arrs:
+            if a is not None and a.shape != shp:
+                raise ValueError("chain state must have shape %s" % (shp,))
+        self._sync_stream()
+        if any(a is not None for a in arrs):
+            _lib.call("cpstep_cp_thermostat_state", self._h, 1,
+                      *[None if a is None else a.ctypes.data for a in arrs])
+        out = [np.zeros(shp) for _ in range(3)]
+        _lib.call("cpstep_cp_thermostat_state", self._h, 0, *[a.ctypes.data for a in out])
+        return tuple(out)
+
     def cp_integrate(self, force, psi, vpsi, dt, iteration):
         self._sync_stream()
         ke = torch.zeros(1, dtype=torch.float64, device=self.device)

@@ -291,6 +291,7 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
   for (auto& e : c->prof_ev) cudaEventDestroy(e);
   nl_free(c);
   sf_free(c);
+  nhc_free(c);
   rho_free(c);
   step_free(c);
   statefft_free(c);
@@ -541,10 +542,26 @@ int cpstep_set_cp_mass(cpstep_ctx* c, double tau_fs, double cut_ry) {
   return step_set_mass(c, tau_fs, cut_ry);
 }
 
+int cpstep_set_cp_thermostat(cpstep_ctx* c, double te_ext, double tau_fs, int num_nhc, int nck,
+                             int nres, int nyosh) {
+  if (!c) return CPSTEP_ERR_ARG;
+  if (te_ext > 0.0 && !c->d_cmass) {
+    cpstep_set_error("set_cp_thermostat: CP masses not set (cpstep_set_cp_mass)");
+    return CPSTEP_ERR_STATE;
+  }
+  graph_drop(c);
+  return nhc_set(c, te_ext, tau_fs, num_nhc, nck, nres, nyosh);
+}
+
+int cpstep_cp_thermostat_state(cpstep_ctx* c, int set, double* h_x, double* h_xp, double* h_v) {
+  if (!c) return CPSTEP_ERR_ARG;
+  return nhc_state(c, set, h_x, h_xp, h_v);
+}
+
 int cpstep_cp_integrate(cpstep_ctx* c, const double* d_force, double* d_psi, double* d_vpsi,
                         double dt, int iteration, double* d_fict_ke) {
   if (!c || !d_force || !d_psi || !d_vpsi || iteration < 1) return CPSTEP_ERR_ARG;
-  return step_integrate(c, d_force, d_psi, d_vpsi, dt, iteration, d_fict_ke);
+  return step_integrate(c, d_force, d_psi, d_vpsi, dt, iteration, d_fict_ke, nullptr);
 }
 
 int cpstep_cp_step(cpstep_ctx* c, double* d_psi, double* d_vpsi, const double* d_occ, double dt,

@@ -138,6 +138,21 @@ struct AtomData {
   std::vector<double> h_q;  // charges, host copy
 };
 
+// Isokinetic NHC thermostat of the CP coefficients (cpstep_set_cp_thermostat):
+// initCPNHC's constants, the per-point chunk map and per-(state, chunk) chains.
+struct CpNhc {
+  int on = 0;
+  int num = 0, nck = 0, nres = 0, nyosh = 0;
+  double kT = 0.0, m[2] = {0.0, 0.0};
+  double v0[8] = {0}, a2[8] = {0}, a4[8] = {0}, dfs[8] = {0};
+  signed char* d_ck = nullptr;  // chunk of each point, -1 on the redundant half
+  double *d_x = nullptr, *d_xp = nullptr, *d_vn = nullptr;  // [S][nck][num][2]
+  int nsplit = 0, span = 0;       // KE blocks per state and points per block
+  double* d_part = nullptr;       // [S][nsplit][nck]
+  double* d_scale = nullptr;      // [S][nck][2]
+  double* d_eout = nullptr;       // [S][nck][3]
+};
+
 // Structure-factor (non-EES) non-local state, l = 0 (cpstep_set_nonlocal_sf).
 struct SfData {
   int on = 0, n = 0, ldz = 0;       // n non-local atoms (type order)
@@ -229,6 +244,7 @@ struct cpstep_ctx {
   AtomData atoms;
   NlData nl;
   SfData sf;
+  CpNhc nhc;
   int rho_izero = -1;
   // exchange-correlation functional (CPSTEP_XC_*) and the BLYP scratch: the
   // three gradient grids [3][N_r] and four packed density-sphere arrays
@@ -428,7 +444,14 @@ int step_init_classes(cpstep_ctx* c);
 void step_free(cpstep_ctx* c);
 int step_set_mass(cpstep_ctx* c, double tau_fs, double cut_ry);
 int step_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi, double dt,
-                   int iteration, double* d_fict_ke);
+                   int iteration, double* d_fict_ke, double* d_enhc);
+
+// nhc.cu
+int nhc_set(cpstep_ctx* c, double te_ext, double tau_fs, int num, int nck, int nres, int nyosh);
+void nhc_free(cpstep_ctx* c);
+int nhc_state(cpstep_ctx* c, int set, double* h_x, double* h_xp, double* h_vn);
+int nhc_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi, double dt,
+                  int iteration, double* d_fict_ke, double* d_enhc);
 int step_run(cpstep_ctx* c, double* psi, double* vpsi, const double* occ, double dt,
              int iteration, double* energies, double* atom_force, int ortho_check);
 

@@ -177,11 +177,13 @@ int step_set_mass(cpstep_ctx* c, double tau_fs, double cut_ry) {
   return CPSTEP_OK;
 }
 
-// Velocity Verlet of CP_integrate_dyn without the thermostat: second half
-// kick of the previous step (iteration > 1), fictitious KE, first half kick,
-// drift, and the redundant-half sync.
+// Velocity Verlet of CP_integrate_dyn: second half kick of the previous step
+// (iteration > 1), fictitious KE, first half kick, drift (with the isokinetic
+// NHC of nhc.cu around the kicks when the thermostat is on), and the
+// redundant-half sync.  d_enhc (2 doubles, may be NULL): the NHC kinetic
+// energy and potential of get_fictKE, zero without the thermostat.
 int step_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi, double dt,
-                   int iteration, double* d_fict_ke) {
+                   int iteration, double* d_fict_ke, double* d_enhc) {
   if (!c->d_cmass) {
     cpstep_set_error("integrate: CP masses not set (cpstep_set_cp_mass)");
     return CPSTEP_ERR_STATE;
@@ -190,6 +192,17 @@ int step_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi
   double2* v = reinterpret_cast<double2*>(vpsi);
   const double2* f = reinterpret_cast<const double2*>(force);
   int nb = c->nblk_ke;
+  if (c->nhc.on) {
+    int rc = nhc_integrate(c, force, psi, vpsi, dt, iteration, d_fict_ke, d_enhc);
+    if (rc) return rc;
+    if (c->nred) {
+      stp::k_sync_red<<<nb, 256, 0, c->stream>>>(p, v, c->d_red_idx, c->d_red_src, c->nred,
+                                                 c->npts, c->nstates);
+      CPSTEP_LAUNCH_CHECK();
+    }
+    return CPSTEP_OK;
+  }
+  if (d_enhc) CPSTEP_CUDA_TRY(cudaMemsetAsync(d_enhc, 0, 2 * sizeof(double), c->stream));
   stp::k_integrate<<<nb, 256, 0, c->stream>>>(p, v, f, c->d_cmass, c->d_cls, c->npts,
                                               c->nstates, dt, iteration > 1 ? 1 : 0,
                                               c->d_step_part);
@@ -267,7 +280,8 @@ int step_run(cpstep_ctx* c, double* psi, double* vpsi, const double* occ, double
     return rc;
   mark(5);
   // 4. Verlet update
-  if ((rc = step_integrate(c, c->d_force, psi, vpsi, dt, iteration, energies + CPSTEP_E_FICT)))
+  if ((rc = step_integrate(c, c->d_force, psi, vpsi, dt, iteration, energies + CPSTEP_E_FICT,
+                           energies + CPSTEP_E_NHC_KE)))
     return rc;
   mark(6);
   // 5. S = overlap, T = (S/2)^(-1/2), psi <- psi.T

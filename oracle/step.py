@@ -116,11 +116,19 @@ def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None, xc=
 
 
 def cp_step(psi, v, occ, sysm, lay, dlay, cmass, dt, iteration, nonlocal_on=False, nkf=None,
-            xc="pz_lda", nonlocal_sf=False):
+            xc="pz_lda", nonlocal_sf=False, nhc=None):
+    """nhc = (params, per-state chain states, nres, nyosh) of oracle/isokin.py
+    runs the thermostatted integrator (the chain states are updated)."""
     en, F, floc, rho, vks = forces(psi, occ, sysm, lay, dlay, nonlocal_on=nonlocal_on, nkf=nkf,
                                    xc=xc, nonlocal_sf=nonlocal_sf)
     Fc, lam = constrain(F, psi, lay)
-    psi2, v2, ke = integrate(Fc, psi, v, cmass, lay, dt, iteration)
+    if nhc is None:
+        psi2, v2, ke = integrate(Fc, psi, v, cmass, lay, dt, iteration)
+    else:
+        from . import isokin as OK
+        cls, ridx, rsrc = point_classes(lay)
+        psi2, v2, ke, en["NHC_KE"], en["NHC_POT"] = OK.integrate_nhc(
+            Fc, psi, v, cmass, cls, ridx, rsrc, nhc[0], nhc[1], dt, iteration, nhc[2], nhc[3])
     en["FICT"] = ke
     S = OO.pc_overlap(psi2, psi2, lay.kx)
     T, it, _ = OO.schulz_tmat(S)
