@@ -35,7 +35,8 @@ constexpr int kMaxNck = 8;
 struct Par {
   int num, nck, nres, nyosh;
   double kT, m0, m1;
-  double v0[kMaxNum], a2[kMaxNum], a4[kMaxNum];
+  double c1[kMaxNum];   // -4 v0 / (a4 mNHC[1]): the double-well force factor
+  double a2[kMaxNum];
   double gkt[kMaxNck];  // degFreeSplt[k] * kT
   double w[9];          // Yoshida weights times dt / nres
 };
@@ -79,79 +80,91 @@ __global__ void k_nhc_ekin(const double2* __restrict__ v, const double2* __restr
   }
 }
 
-__device__ __forceinline__ void hh(double f0, double f1, double v0, double v1, const Par& P,
-                                   double w4, double& h, double& hdot) {
-  const double ffdot = (f0 * f0 * P.m0 + f1 * f1 * P.m1) / P.kT;
-  const double pfdot = (f0 * v0 * P.m0 + f1 * v1 * P.m1) / P.kT;
+// h and hdot of one chain's velocity update (cp_isokin.C:216-235 / :266-285);
+// 1/kT, 1/sqrt(ffdot) and 1/hdot as reciprocals, cosh and sinh from e^arg and
+// e^-arg above arg = 1/8 (below it sinh itself: e - 1/e would cancel).  The
+// update is a serial chain of 2 x nres x nyosh of these per chunk, so its
+// time is the latency of one thread's dependent FP64 operations.
+__device__ __forceinline__ void hh_step(double f0, double f1, double& v0, double& v1,
+                                        const Par& P, double ikT, double w4) {
+  const double ffdot = (f0 * f0 * P.m0 + f1 * f1 * P.m1) * ikT;
+  const double pfdot = (f0 * v0 * P.m0 + f1 * v1 * P.m1) * ikT;
+  double h, hdot;
   if (ffdot * w4 * w4 > 1.0e-10) {
-    const double fr = sqrt(ffdot);
+    const double ifr = rsqrt(ffdot);
+    const double fr = ffdot * ifr;
     const double arg = fr * w4;
-    const double ch = cosh(arg), sh = sinh(arg);
-    h = (pfdot / ffdot) * (ch - 1.0) + (1.0 / fr) * sh;
-    hdot = (pfdot / fr) * sh + ch;
+    const double e = exp(arg), ie = exp(-arg);  // independent: no dependent reciprocal
+    const double ch = 0.5 * (e + ie);
+    const double sh = arg < 0.125 ? sinh(arg) : 0.5 * (e - ie);
+    h = pfdot * ifr * ifr * (ch - 1.0) + ifr * sh;
+    hdot = pfdot * ifr * sh + ch;
   } else {
     h = (((ffdot * pfdot / 24.0 * w4 + ffdot / 6.0) * w4 + 0.50 * pfdot) * w4 + 1.0) * w4;
     hdot = ((ffdot * pfdot / 6.0 * w4 + ffdot / 2.0) * w4 + pfdot) * w4 + 1.0;
   }
+  const double ihd = 1.0 / hdot;
+  v0 = (v0 + f0 * h) * ihd;
+  v1 = (v1 + f1 * h) * ihd;
 }
 
-// cp_isoNHC_update for one chunk: returns the velocity scale; x, xp, vn are
-// this chunk's [num][2] chain arrays.
-__device__ double iso_update(double ekin, double gkt, const Par& P, double* x, double* xp,
-                             double* vn) {
-  double f[kMaxNum][2];
-  for (int i = 0; i < P.num; ++i) {
-    xp[2 * i] = 0.0;
-    const double q = xp[2 * i + 1];
-    f[i][0] = (ekin - gkt) / P.m0;
-    f[i][1] = -(4.0 * P.v0[i] / (P.a4[i] * P.m1)) * (q * (q * q - P.a2[i]));
+// cp_isoNHC_update (cp_isokin.C:150-311) for one chunk of NUM chains, all in
+// registers: returns the velocity scale; x, xp, vn are [NUM][2].
+template <int NUM>
+__device__ double iso_update(double ekin, double gkt, const Par& P, double (&x)[NUM][2],
+                             double (&xp)[NUM][2], double (&vn)[NUM][2]) {
+  const double ikT = 1.0 / P.kT, im0 = 1.0 / P.m0;
+  double f[NUM][2];
+#pragma unroll
+  for (int i = 0; i < NUM; ++i) {
+    xp[i][0] = 0.0;
+    const double q = xp[i][1];
+    f[i][0] = (ekin - gkt) * im0;
+    f[i][1] = P.c1[i] * (q * (q * q - P.a2[i]));
   }
   double scale = 1.0;
   for (int ir = 0; ir < P.nres; ++ir) {
     for (int iy = 0; iy < P.nyosh; ++iy) {
       const double w2 = P.w[iy] * 0.5, w4 = P.w[iy] * 0.25;
       double vsum = 0.0;
-      for (int i = 0; i < P.num; ++i) {
-        double h, hd;
-        hh(f[i][0], f[i][1], vn[2 * i], vn[2 * i + 1], P, w4, h, hd);
-        vn[2 * i] = (vn[2 * i] + f[i][0] * h) / hd;
-        vn[2 * i + 1] = (vn[2 * i + 1] + f[i][1] * h) / hd;
-        vsum += vn[2 * i];
+#pragma unroll
+      for (int i = 0; i < NUM; ++i) {
+        hh_step(f[i][0], f[i][1], vn[i][0], vn[i][1], P, ikT, w4);
+        vsum += vn[i][0];
       }
       const double aa = exp(-w4 * vsum);
       scale *= aa;
       ekin *= aa * aa;
-      for (int i = 0; i < P.num; ++i) {
-        x[2 * i] += P.kT * vn[2 * i] * w2;
-        x[2 * i + 1] += vn[2 * i] * (ekin - gkt) * w2;
-        xp[2 * i + 1] += vn[2 * i + 1] * w2;
+#pragma unroll
+      for (int i = 0; i < NUM; ++i) {
+        x[i][0] += P.kT * vn[i][0] * w2;
+        x[i][1] += vn[i][0] * (ekin - gkt) * w2;
+        xp[i][1] += vn[i][1] * w2;
       }
       scale *= aa;
       ekin *= aa * aa;
-      for (int i = 0; i < P.num; ++i) {
-        const double q = xp[2 * i + 1];
-        f[i][0] = (ekin - gkt) / P.m0;
-        f[i][1] = -(4.0 * P.v0[i] / (P.a4[i] * P.m1)) * (q * (q * q - P.a2[i]));
-      }
-      for (int i = 0; i < P.num; ++i) {
-        double h, hd;
-        hh(f[i][0], f[i][1], vn[2 * i], vn[2 * i + 1], P, w4, h, hd);
-        vn[2 * i] = (vn[2 * i] + f[i][0] * h) / hd;
-        vn[2 * i + 1] = (vn[2 * i + 1] + f[i][1] * h) / hd;
+#pragma unroll
+      for (int i = 0; i < NUM; ++i) {
+        const double q = xp[i][1];
+        f[i][0] = (ekin - gkt) * im0;
+        f[i][1] = P.c1[i] * (q * (q * q - P.a2[i]));
+        hh_step(f[i][0], f[i][1], vn[i][0], vn[i][1], P, ikT, w4);
       }
     }
   }
-  for (int i = 0; i < P.num; ++i) {
-    const double en = P.m0 * vn[2 * i] * vn[2 * i] + P.m1 * vn[2 * i + 1] * vn[2 * i + 1];
+#pragma unroll
+  for (int i = 0; i < NUM; ++i) {
+    const double en = P.m0 * vn[i][0] * vn[i][0] + P.m1 * vn[i][1] * vn[i][1];
     const double sc = sqrt(P.kT / en);
-    vn[2 * i] *= sc;
-    vn[2 * i + 1] *= sc;
+    vn[i][0] *= sc;
+    vn[i][1] *= sc;
   }
   return scale;
 }
 
 // one thread per (state, chunk); eout[t] = {ekin, ekinNHC (x2), potNHC} at
 // the time of get_fictKE; scale[t] = {s2, s1}
+template <int NUM>
 __global__ void k_nhc_update(Par P, const double* __restrict__ part, int nsplit, int nstates,
                              int first, double* __restrict__ x, double* __restrict__ xp,
                              double* __restrict__ vn, double* __restrict__ scale,
@@ -161,32 +174,39 @@ __global__ void k_nhc_update(Par P, const double* __restrict__ part, int nsplit,
   const int s = t / P.nck, k = t % P.nck;
   double ekin = 0.0;
   for (int q = 0; q < nsplit; ++q) ekin += part[((size_t)s * nsplit + q) * P.nck + k];
-  double xl[2 * kMaxNum], xpl[2 * kMaxNum], vl[2 * kMaxNum];
-  const size_t o = (size_t)t * P.num * 2;
-  for (int i = 0; i < 2 * P.num; ++i) {
-    xl[i] = x[o + i];
-    xpl[i] = xp[o + i];
-    vl[i] = vn[o + i];
-  }
+  double xl[NUM][2], xpl[NUM][2], vl[NUM][2];
+  const size_t o = (size_t)t * NUM * 2;
+#pragma unroll
+  for (int i = 0; i < NUM; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      xl[i][j] = x[o + 2 * i + j];
+      xpl[i][j] = xp[o + 2 * i + j];
+      vl[i][j] = vn[o + 2 * i + j];
+    }
   double s2 = 1.0;
   if (first) {
-    s2 = iso_update(ekin, P.gkt[k], P, xl, xpl, vl);
+    s2 = iso_update<NUM>(ekin, P.gkt[k], P, xl, xpl, vl);
     ekin *= s2 * s2;
   }
   double ekn = 0.0, pot = 0.0;
-  for (int i = 0; i < P.num; ++i) {
-    ekn += P.m0 * vl[2 * i] * vl[2 * i] + P.m1 * vl[2 * i + 1] * vl[2 * i + 1];
-    pot += xl[2 * i] + xl[2 * i + 1];
+#pragma unroll
+  for (int i = 0; i < NUM; ++i) {
+    ekn += P.m0 * vl[i][0] * vl[i][0] + P.m1 * vl[i][1] * vl[i][1];
+    pot += xl[i][0] + xl[i][1];
   }
   eout[3 * t] = ekin;
   eout[3 * t + 1] = ekn;
   eout[3 * t + 2] = pot;
-  const double s1 = iso_update(ekin, P.gkt[k], P, xl, xpl, vl);
-  for (int i = 0; i < 2 * P.num; ++i) {
-    x[o + i] = xl[i];
-    xp[o + i] = xpl[i];
-    vn[o + i] = vl[i];
-  }
+  const double s1 = iso_update<NUM>(ekin, P.gkt[k], P, xl, xpl, vl);
+#pragma unroll
+  for (int i = 0; i < NUM; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      x[o + 2 * i + j] = xl[i][j];
+      xp[o + 2 * i + j] = xpl[i][j];
+      vn[o + 2 * i + j] = vl[i][j];
+    }
   scale[2 * t] = s2;
   scale[2 * t + 1] = s1;
 }
@@ -384,7 +404,8 @@ int nhc_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi,
   P.num = t.num; P.nck = t.nck; P.nres = t.nres; P.nyosh = t.nyosh;
   P.kT = t.kT; P.m0 = t.m[0]; P.m1 = t.m[1];
   for (int i = 0; i < nhc::kMaxNum; ++i) {
-    P.v0[i] = t.v0[i]; P.a2[i] = t.a2[i]; P.a4[i] = t.a4[i];
+    P.a2[i] = t.a2[i];
+    P.c1[i] = i < t.num ? -(4.0 * t.v0[i] / (t.a4[i] * t.m[1])) : 0.0;
   }
   for (int k = 0; k < nhc::kMaxNck; ++k) P.gkt[k] = t.dfs[k] * t.kT;
   double w[9] = {0};
@@ -398,9 +419,21 @@ int nhc_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi,
       v, f, c->d_cmass, c->d_cls, t.d_ck, c->npts, t.span, dt, first, t.nck, t.d_part);
   CPSTEP_LAUNCH_CHECK();
   const int nt = c->nstates * t.nck;
-  nhc::k_nhc_update<<<(nt + 63) / 64, 64, 0, c->stream>>>(P, t.d_part, t.nsplit, c->nstates,
-                                                          first, t.d_x, t.d_xp, t.d_vn,
-                                                          t.d_scale, t.d_eout);
+  const dim3 ug((nt + 31) / 32), ub(32);
+#define NHC_UPDATE(N)                                                                        \
+  nhc::k_nhc_update<N><<<ug, ub, 0, c->stream>>>(P, t.d_part, t.nsplit, c->nstates, first,  \
+                                                 t.d_x, t.d_xp, t.d_vn, t.d_scale, t.d_eout)
+  switch (t.num) {
+    case 1: NHC_UPDATE(1); break;
+    case 2: NHC_UPDATE(2); break;
+    case 3: NHC_UPDATE(3); break;
+    case 4: NHC_UPDATE(4); break;
+    case 5: NHC_UPDATE(5); break;
+    case 6: NHC_UPDATE(6); break;
+    case 7: NHC_UPDATE(7); break;
+    default: NHC_UPDATE(8); break;
+  }
+#undef NHC_UPDATE
   CPSTEP_LAUNCH_CHECK();
   if (d_fict_ke || d_enhc) {
     nhc::k_nhc_sum<<<1, 256, 0, c->stream>>>(t.d_eout, nt, d_fict_ke, d_enhc);
