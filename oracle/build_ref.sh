@@ -15,6 +15,8 @@
 #   src_piny_physics_v1.0/abinito_physics/cp_ions/cp_rspace_ion.C   CP_getionforce
 #   src_piny_physics_v1.0/abinito_physics/cp_integrate/cp_isokin.C, cp_dynamics.C
 #                         initCPNHC, cp_isoNHC_update, CP_integrate_dyn
+#   src_piny_physics_v1.0/classical_physics/integrate/integration_drivers.C
+#                         integrate_nvt_2nd_half / _1st_half (massive atom NHC)
 # The shims in oracle/ref_shim stand in for the Charm++/PINY headers, and
 # oracle/ref_mathlib.c for the Fortran GENMATMUL.  Test infrastructure only.
 set -e
@@ -43,7 +45,8 @@ for f in "$PINY/abinito_physics/cp_nonlocal/cp_ees_nonlocal.C" \
          "$PINY/abinito_physics/cp_nonlocal/cp_nl_energy_forc.C" "$HERE/ref_sf.cpp" \
          "$PINY/abinito_physics/cp_ions/cp_rspace_ion.C" "$HERE/ref_ion.cpp" \
          "$PINY/abinito_physics/cp_integrate/cp_isokin.C" \
-         "$PINY/abinito_physics/cp_integrate/cp_dynamics.C" "$HERE/ref_isokin.cpp"; do
+         "$PINY/abinito_physics/cp_integrate/cp_dynamics.C" "$HERE/ref_isokin.cpp" \
+         "$PINY/classical_physics/integrate/integration_drivers.C" "$HERE/ref_atomnhc.cpp"; do
   g++ $EESFLAGS -c "$f" -o "$OUT/$(basename "$f" | sed 's/\.[Cc]p*$//').o"
 done
 g++ -O2 -fPIC -shared -w -o "$OUT/libref.so" \
@@ -57,5 +60,6 @@ g++ -O2 -fPIC -shared -w -o "$OUT/libref.so" \
   "$OUT/cp_becke.o" "$OUT/cp_grad_rho_ctrl.o" "$OUT/cp_pz_lda.o" "$OUT/ref_xc.o" \
   "$OUT/cp_struct_fact.o" "$OUT/cp_nlmat.o" "$OUT/cp_nl_energy_forc.o" "$OUT/ref_sf.o" \
   "$OUT/cp_rspace_ion.o" "$OUT/ref_ion.o" \
-  "$OUT/cp_isokin.o" "$OUT/cp_dynamics.o" "$OUT/ref_isokin.o"
+  "$OUT/cp_isokin.o" "$OUT/cp_dynamics.o" "$OUT/ref_isokin.o" \
+  "$OUT/integration_drivers.o" "$OUT/ref_atomnhc.o"
 echo "$OUT/libref.so"

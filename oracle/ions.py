@@ -16,6 +16,11 @@ TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).
   :337-355 (the NVE branch of ctrl_atom_integrate, control_integrate.C:22-200):
   v += dt/2 f/m (not on step 0), E_kin = 1/2 sum m v^2, then v += dt/2 f/m,
   x += dt v.
+* ATOMINTEGRATE::integrate_nvt_2nd_half / _1st_half / applyNHC / computeENHC
+  (integration_drivers.C:89-190, :358-565): the NVT branch with massive
+  Nose-Hoover chains (one chain per atom and Cartesian component), pinned to
+  the reference's integration_drivers.C compiled from source
+  (oracle/ref_atomnhc.cpp).
 """
 import math
 
@@ -96,3 +101,63 @@ def nve_step(itime, pos, vel, force, mass, dt):
     vel += 0.5 * dt * f / m
     pos += dt * vel
     return pos, vel, ekin
+
+
+def _yosh_w(nyosh, dt):
+    from .isokin import yosh
+    return yosh(nyosh, dt)
+
+
+def apply_nhc(vel, mass, kT, mnhc, vn, pos_kt, dt, nres, nyosh):
+    """ATOMINTEGRATE::applyNHC (integration_drivers.C:402-462) with massive
+    chains: every Cartesian component of every atom has its own chain of
+    length L = mnhc.shape[1]; vel [n, 3], vn [n, 3, L], pos_kt [n] updated
+    in place.  kT [n], mnhc [n, L]."""
+    n, L = mnhc.shape
+    w = _yosh_w(nyosh, dt / nres)
+    m = np.asarray(mass, dtype=np.float64)
+    for i in range(n):
+        mv2 = m[i] * vel[i] * vel[i]                       # [3]
+        f = np.zeros((3, L))
+        f[:, 0] = (mv2 - kT[i]) / mnhc[i, 0]
+        for ic in range(1, L):
+            f[:, ic] = (mnhc[i, ic - 1] * vn[i, :, ic - 1] ** 2 - kT[i]) / mnhc[i, ic]
+        for _ in range(nres):
+            for wy in w:
+                w2, w4, w8 = wy * 0.5, wy * 0.25, wy * 0.125
+                vn[i, :, L - 1] += f[:, L - 1] * w4
+                for ic in range(L - 2, -1, -1):
+                    aa = np.exp(-w8 * vn[i, :, ic + 1])
+                    vn[i, :, ic] = vn[i, :, ic] * aa * aa + w4 * f[:, ic] * aa
+                aa = np.exp(-w2 * vn[i, :, 0])
+                vel[i] *= aa
+                mv2 *= aa * aa
+                pre = kT[i] * w2
+                for ic in range(L):
+                    pos_kt[i] += pre * (vn[i, 0, ic] + vn[i, 1, ic] + vn[i, 2, ic])
+                f[:, 0] = (mv2 - kT[i]) / mnhc[i, 0]
+                for ic in range(L - 1):
+                    aa = np.exp(-w8 * vn[i, :, ic + 1])
+                    vn[i, :, ic] = vn[i, :, ic] * aa * aa + w4 * f[:, ic] * aa
+                    f[:, ic + 1] = (mnhc[i, ic] * vn[i, :, ic] ** 2 - kT[i]) / mnhc[i, ic + 1]
+                vn[i, :, L - 1] += f[:, L - 1] * w4
+
+
+def nvt_step(itime, pos, vel, force, mass, kT, mnhc, vn, pos_kt, dt, nres, nyosh):
+    """integrate_nvt_2nd_half / computeEkin / computeENHC / integrate_nvt_1st_half
+    (integration_drivers.C:89-190, :337-400): (pos, vel, E_kin, E_kin NHC,
+    pot NHC); vn and pos_kt updated in place."""
+    pos = np.array(pos, dtype=np.float64)
+    vel = np.array(vel, dtype=np.float64)
+    m = np.asarray(mass, dtype=np.float64)[:, None]
+    f = np.asarray(force, dtype=np.float64)
+    if itime > 0:
+        vel += 0.5 * dt * f / m
+        apply_nhc(vel, mass, kT, mnhc, vn, pos_kt, dt, nres, nyosh)
+    ekin = 0.5 * float(np.sum(m * vel * vel))
+    eknhc = 0.5 * float(np.sum(mnhc[:, None, :] * vn * vn))
+    pot = float(np.sum(pos_kt))
+    apply_nhc(vel, mass, kT, mnhc, vn, pos_kt, dt, nres, nyosh)
+    vel += 0.5 * dt * f / m
+    pos += dt * vel
+    return pos, vel, ekin, eknhc, pot

@@ -84,3 +84,36 @@ def test_nve_step_is_velocity_verlet():
     p2, v2, ek1 = OI.nve_step(1, p1, v1, f, m, 2.0)
     vh = v1 + f / m[:, None]
     assert abs(ek1 - 0.5 * np.sum(m[:, None] * vh * vh)) < 1e-12 * ek1
+
+
+@pytest.mark.parametrize("L,nres,nyosh", [(4, 1, 1), (3, 2, 3), (2, 4, 9)])
+def test_nvt_step_matches_reference(L, nres, nyosh):
+    from conftest import ref_lib as load
+    lib = load()
+    if lib is None or not hasattr(lib, "ref_atom_nvt_step"):
+        pytest.skip("oracle/_ref/libref.so with integration_drivers.C is not built")
+    vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    lib.ref_atom_nvt_step.argtypes = [i, i, i] + [vp] * 8 + [d, i, i, vp]
+    rng = np.random.default_rng(L)
+    n, dt = 9, 20.0
+    pos = rng.uniform(0.0, 10.0, (n, 3))
+    mass = rng.choice([29164.0, 1837.0], n)
+    kT = np.full(n, 300.0 / 315777.0)
+    vel = rng.standard_normal((n, 3)) * np.sqrt(kT[:, None] / mass[:, None])
+    mnhc = kT[:, None] * (200.0 / 0.0241888) ** 2 * (1.0 + 0.1 * np.arange(L))[None, :]
+    vn = rng.standard_normal((n, 3, L)) * np.sqrt(kT[:, None, None] / mnhc[:, None, :])
+    pkt = np.zeros(n)
+    rp, rv, rvn, rpk = pos.copy(), vel.copy(), vn.copy(), pkt.copy()
+    for it in range(3):
+        f = 1e-3 * rng.standard_normal((n, 3))
+        out = np.zeros(3)
+        lib.ref_atom_nvt_step(n, L, it, _p(rp), _p(rv), _p(f), _p(mass), _p(kT), _p(mnhc),
+                              _p(rvn), _p(rpk), dt, nres, nyosh, _p(out))
+        pos, vel, ek, ekn, pot = OI.nvt_step(it, pos, vel, f, mass, kT, mnhc, vn, pkt, dt, nres,
+                                             nyosh)
+        assert abs(ek - out[0]) <= 1e-13 * abs(out[0])
+        assert abs(ekn - out[1]) <= 1e-13 * abs(out[1])
+        assert abs(pot - out[2]) <= 1e-12 * max(1e-12, abs(out[2]))
+        np.testing.assert_allclose(vel, rv, rtol=1e-13, atol=1e-18)
+        np.testing.assert_allclose(vn, rvn, rtol=1e-13, atol=1e-18)
+        assert np.max(np.abs(pos - rp)) <= 1e-12
