@@ -545,6 +545,25 @@ CPSTEP_API int cpstep_set_positions(cpstep_ctx* ctx, const double* h_pos);
  *   cpstep_set_positions).  d_fatm holds the total atom forces (the step's
  *   local, reciprocal Ewald and non-local forces plus cpstep_ion_forces). */
 CPSTEP_API int cpstep_ion_forces(cpstep_ctx* ctx, double* d_fatm, double* d_energies);
+/*
+ * Massive Nose-Hoover chains of the atoms: the NVT branch of ctrl_atom_integrate
+ * (iextended_on = 1, isokin_opt = 0; integrate_nvt_2nd_half / _1st_half, applyNHC,
+ * computeENHC: classical_physics/integrate/integration_drivers.C:89-190, :358-565).
+ * cpstep_set_atom_thermostat: len_nhc (1..5; 0 returns to NVE), nres, nyosh
+ *   ({1,3,5,7,9}), h_kT [natm] (AtomNHC::kT) and h_mnhc [natm][len_nhc]
+ *   (AtomNHC::m, PhysicsAtomPosInit.C:229-256); needs the atoms; chain
+ *   velocities and posKT start at zero.  cpstep_atoms_integrate then runs, per
+ *   atom and Cartesian component: v += dt/2 f/m and applyNHC (itime > 0), E_kin,
+ *   the NHC energies, applyNHC, v += dt/2 f/m, x += dt v.
+ * cpstep_atom_thermostat_state: set (set = 1) or read the chain velocities
+ *   h_vnhc [natm][3][len_nhc] (AtomNHC::vx/vy/vz) and h_pos_kt [natm]
+ *   (AtomNHC::posKT); on read, h_energies2 (may be NULL) = {E_kin NHC, pot NHC}
+ *   of the last cpstep_atoms_integrate.
+ */
+CPSTEP_API int cpstep_set_atom_thermostat(cpstep_ctx* ctx, int len_nhc, int nres, int nyosh,
+                                          const double* h_kT, const double* h_mnhc);
+CPSTEP_API int cpstep_atom_thermostat_state(cpstep_ctx* ctx, int set, double* h_vnhc,
+                                            double* h_pos_kt, double* h_energies2);
 CPSTEP_API int cpstep_atoms_integrate(cpstep_ctx* ctx, int itime, double* d_pos, double* d_vel,
                                       const double* d_fatm, const double* d_mass, double dt,
                                       double* d_ekin);

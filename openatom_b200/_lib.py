@@ -88,6 +88,9 @@ SIGNATURES = {
                                                 ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int]),
     "cpstep_cp_thermostat_state": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp]),
+    "cpstep_set_atom_thermostat": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  _vp, _vp]),
+    "cpstep_atom_thermostat_state": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp]),
     "cpstep_cp_integrate": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int,
                                            _vp]),
     "cpstep_cp_step": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int, _vp,

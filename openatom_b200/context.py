@@ -373,6 +373,41 @@ class StepContext:
         _lib.call("cpstep_cp_thermostat_state", self._h, 0, *[a.ctypes.data for a in out])
         return tuple(out)
 
+    def set_atom_thermostat(self, len_nhc, kT=None, mnhc=None, nres=1, nyosh=1):
+        """Massive NHC of the atoms (len_nhc 0: NVE); kT [natm], mnhc [natm][len_nhc]."""
+        import numpy as np
+        if len_nhc <= 0:
+            _lib.call("cpstep_set_atom_thermostat", self._h, 0, 1, 1, None, None)
+            self._atom_nhc = None
+            return
+        kT = np.ascontiguousarray(kT, dtype=np.float64)
+        mnhc = np.ascontiguousarray(mnhc, dtype=np.float64)
+        if mnhc.shape != (kT.shape[0], len_nhc):
+            raise ValueError("mnhc must have shape (natm, len_nhc)")
+        _lib.call("cpstep_set_atom_thermostat", self._h, int(len_nhc), int(nres), int(nyosh),
+                  kT.ctypes.data, mnhc.ctypes.data)
+        self._atom_nhc = (kT.shape[0], int(len_nhc))
+
+    def atom_thermostat_state(self, vnhc=None, pos_kt=None):
+        """Set the atom chains (vnhc [natm][3][len], pos_kt [natm]; those not None),
+        then return (vnhc, pos_kt, (E_kin NHC, pot NHC) of the last step)."""
+        import numpy as np
+        shp = getattr(self, "_atom_nhc", None)
+        if shp is None:
+            _lib.call("cpstep_atom_thermostat_state", self._h, 0, None, None, None)
+        n, L = shp
+        self._sync_stream()
+        a = None if vnhc is None else np.ascontiguousarray(vnhc, dtype=np.float64).reshape(n, 3, L)
+        b = None if pos_kt is None else np.ascontiguousarray(pos_kt, dtype=np.float64).reshape(n)
+        if a is not None or b is not None:
+            _lib.call("cpstep_atom_thermostat_state", self._h, 1,
+                      None if a is None else a.ctypes.data, None if b is None else b.ctypes.data,
+                      None)
+        vo, po, eo = np.zeros((n, 3, L)), np.zeros(n), np.zeros(2)
+        _lib.call("cpstep_atom_thermostat_state", self._h, 0, vo.ctypes.data, po.ctypes.data,
+                  eo.ctypes.data)
+        return vo, po, eo
+
     def cp_integrate(self, force, psi, vpsi, dt, iteration):
         self._sync_stream()
         ke = torch.zeros(1, dtype=torch.float64, device=self.device)

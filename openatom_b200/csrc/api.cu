@@ -292,6 +292,7 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
   nl_free(c);
   sf_free(c);
   nhc_free(c);
+  atom_nvt_free(c);
   rho_free(c);
   step_free(c);
   statefft_free(c);
@@ -551,6 +552,18 @@ int cpstep_set_cp_thermostat(cpstep_ctx* c, double te_ext, double tau_fs, int nu
   }
   graph_drop(c);
   return nhc_set(c, te_ext, tau_fs, num_nhc, nck, nres, nyosh);
+}
+
+int cpstep_set_atom_thermostat(cpstep_ctx* c, int len_nhc, int nres, int nyosh,
+                               const double* h_kT, const double* h_mnhc) {
+  if (!c) return CPSTEP_ERR_ARG;
+  return atom_nvt_set(c, len_nhc, nres, nyosh, h_kT, h_mnhc);
+}
+
+int cpstep_atom_thermostat_state(cpstep_ctx* c, int set, double* h_vnhc, double* h_pos_kt,
+                                 double* h_energies2) {
+  if (!c) return CPSTEP_ERR_ARG;
+  return atom_nvt_state(c, set, h_vnhc, h_pos_kt, h_energies2);
 }
 
 int cpstep_cp_thermostat_state(cpstep_ctx* c, int set, double* h_x, double* h_xp, double* h_v) {

@@ -153,6 +153,15 @@ struct CpNhc {
   double* d_eout = nullptr;       // [S][nck][3]
 };
 
+// Massive Nose-Hoover chains of the atoms (cpstep_set_atom_thermostat).
+struct AtomNvt {
+  int len = 0, nres = 0, nyosh = 0;  // len 0: NVE
+  int natm = 0;                      // atoms the chains were set for
+  double *d_kT = nullptr, *d_mnhc = nullptr;  // [natm], [natm][len]
+  double *d_vn = nullptr, *d_pkt = nullptr;   // [natm][3][len], [natm]
+  double* d_e = nullptr;                      // {E_kin NHC, pot NHC} of the last step
+};
+
 // Structure-factor (non-EES) non-local state, l = 0 (cpstep_set_nonlocal_sf).
 struct SfData {
   int on = 0, n = 0, ldz = 0;       // n non-local atoms (type order)
@@ -245,6 +254,7 @@ struct cpstep_ctx {
   NlData nl;
   SfData sf;
   CpNhc nhc;
+  AtomNvt atom_nvt;
   int rho_izero = -1;
   // exchange-correlation functional (CPSTEP_XC_*) and the BLYP scratch: the
   // three gradient grids [3][N_r] and four packed density-sphere arrays
@@ -450,6 +460,11 @@ int step_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi
 int nhc_set(cpstep_ctx* c, double te_ext, double tau_fs, int num, int nck, int nres, int nyosh);
 void nhc_free(cpstep_ctx* c);
 int nhc_state(cpstep_ctx* c, int set, double* h_x, double* h_xp, double* h_vn);
+void nhc_yosh(int nyosh, double* w);  // set_yosh weights, unscaled
+int atom_nvt_set(cpstep_ctx* c, int len, int nres, int nyosh, const double* h_kT,
+                 const double* h_mnhc);
+void atom_nvt_free(cpstep_ctx* c);
+int atom_nvt_state(cpstep_ctx* c, int set, double* h_vn, double* h_pkt, double* h_e2);
 int nhc_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi, double dt,
                   int iteration, double* d_fict_ke, double* d_enhc);
 int step_run(cpstep_ctx* c, double* psi, double* vpsi, const double* occ, double dt,

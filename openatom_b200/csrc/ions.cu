@@ -118,6 +118,100 @@ __global__ void k_atoms_nve(double* __restrict__ pos, double* __restrict__ vel,
   if (threadIdx.x == 0 && ekin) *ekin = 0.5 * e;
 }
 
+// NVT with massive Nose-Hoover chains (integrate_nvt_2nd_half / _1st_half,
+// applyNHC, computeENHC: integration_drivers.C:89-190, :358-565): every
+// Cartesian component of every atom has its own chain of length L; one thread
+// per atom (the three components in lockstep, so the chain positions add up
+// in the reference's order).
+constexpr int kMaxLen = 5;
+
+struct NvtPar {
+  int len, nres, nyosh;
+  double w[9];  // Yoshida weights times dt / nres
+};
+
+__device__ void apply_nhc(double* v, double m, double kT, const double* mn, double (*vn)[kMaxLen],
+                          double& pkt, const NvtPar& P) {
+  const int L = P.len;
+  double f[3][kMaxLen], mv2[3];
+  for (int d = 0; d < 3; ++d) {
+    mv2[d] = m * v[d] * v[d];
+    f[d][0] = (mv2[d] - kT) / mn[0];
+    for (int ic = 1; ic < L; ++ic) f[d][ic] = (mn[ic - 1] * vn[d][ic - 1] * vn[d][ic - 1] - kT) / mn[ic];
+  }
+  for (int ir = 0; ir < P.nres; ++ir) {
+    for (int iy = 0; iy < P.nyosh; ++iy) {
+      const double w2 = P.w[iy] * 0.5, w4 = P.w[iy] * 0.25, w8 = P.w[iy] * 0.125;
+      for (int d = 0; d < 3; ++d) {
+        vn[d][L - 1] += f[d][L - 1] * w4;
+        for (int ic = L - 2; ic >= 0; --ic) {
+          const double aa = exp(-w8 * vn[d][ic + 1]);
+          vn[d][ic] = vn[d][ic] * aa * aa + w4 * f[d][ic] * aa;
+        }
+        const double aa = exp(-w2 * vn[d][0]);
+        v[d] *= aa;
+        mv2[d] *= aa * aa;
+      }
+      const double pre = kT * w2;
+      for (int ic = 0; ic < L; ++ic) pkt += pre * (vn[0][ic] + vn[1][ic] + vn[2][ic]);
+      for (int d = 0; d < 3; ++d) {
+        f[d][0] = (mv2[d] - kT) / mn[0];
+        for (int ic = 0; ic < L - 1; ++ic) {
+          const double aa = exp(-w8 * vn[d][ic + 1]);
+          vn[d][ic] = vn[d][ic] * aa * aa + w4 * f[d][ic] * aa;
+          f[d][ic + 1] = (mn[ic] * vn[d][ic] * vn[d][ic] - kT) / mn[ic + 1];
+        }
+        vn[d][L - 1] += f[d][L - 1] * w4;
+      }
+    }
+  }
+}
+
+// ekin[0] = E_kin; enhc = {E_kin NHC, pot NHC} at the time of computeENHC
+__global__ void k_atoms_nvt(double* __restrict__ pos, double* __restrict__ vel,
+                            const double* __restrict__ f, const double* __restrict__ mass,
+                            const double* __restrict__ kTa, const double* __restrict__ mnhc,
+                            double* __restrict__ vnhc, double* __restrict__ pkta, int natm,
+                            double dt, int itime, NvtPar P, double* __restrict__ ekin,
+                            double* __restrict__ enhc) {
+  __shared__ double red[32];
+  double e = 0.0, en = 0.0, ep = 0.0;
+  const int L = P.len;
+  for (int i = threadIdx.x; i < natm; i += blockDim.x) {
+    const double m = mass[i], h = 0.5 * dt / m, kT = kTa[i];
+    const double* mn = mnhc + (size_t)i * L;
+    double v[3], vn[3][kMaxLen], pkt = pkta[i];
+    for (int d = 0; d < 3; ++d) {
+      v[d] = vel[3 * i + d];
+      for (int ic = 0; ic < L; ++ic) vn[d][ic] = vnhc[((size_t)i * 3 + d) * L + ic];
+    }
+    if (itime > 0) {
+      for (int d = 0; d < 3; ++d) v[d] += h * f[3 * i + d];
+      apply_nhc(v, m, kT, mn, vn, pkt, P);
+    }
+    e += m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    for (int ic = 0; ic < L; ++ic)
+      en += mn[ic] * (vn[0][ic] * vn[0][ic] + vn[1][ic] * vn[1][ic] + vn[2][ic] * vn[2][ic]);
+    ep += pkt;
+    apply_nhc(v, m, kT, mn, vn, pkt, P);
+    for (int d = 0; d < 3; ++d) {
+      v[d] += h * f[3 * i + d];
+      vel[3 * i + d] = v[d];
+      pos[3 * i + d] += dt * v[d];
+      for (int ic = 0; ic < L; ++ic) vnhc[((size_t)i * 3 + d) * L + ic] = vn[d][ic];
+    }
+    pkta[i] = pkt;
+  }
+  e = block_sum(e, red);
+  en = block_sum(en, red);
+  ep = block_sum(ep, red);
+  if (threadIdx.x == 0) {
+    if (ekin) *ekin = 0.5 * e;
+    enhc[0] = 0.5 * en;
+    enhc[1] = ep;
+  }
+}
+
 }  // namespace ions
 
 namespace {
@@ -184,7 +278,80 @@ int atoms_integrate(cpstep_ctx* c, int itime, double* pos, double* vel, const do
     cpstep_set_error("atoms_integrate: no atoms set");
     return CPSTEP_ERR_STATE;
   }
-  ions::k_atoms_nve<<<1, 256, 0, c->stream>>>(pos, vel, fatm, mass, a.natm, dt, itime, ekin);
+  AtomNvt& t = c->atom_nvt;
+  if (t.len > 0 && t.natm != a.natm) {
+    cpstep_set_error("atoms_integrate: atom thermostat set for %d atoms, %d now", t.natm, a.natm);
+    return CPSTEP_ERR_STATE;
+  }
+  if (t.len > 0) {
+    ions::NvtPar P;
+    P.len = t.len; P.nres = t.nres; P.nyosh = t.nyosh;
+    double w[9] = {0};
+    nhc_yosh(t.nyosh, w);
+    for (int k = 0; k < 9; ++k) P.w[k] = w[k] * (dt / t.nres);
+    ions::k_atoms_nvt<<<1, 256, 0, c->stream>>>(pos, vel, fatm, mass, t.d_kT, t.d_mnhc, t.d_vn,
+                                                t.d_pkt, a.natm, dt, itime, P, ekin, t.d_e);
+  } else {
+    ions::k_atoms_nve<<<1, 256, 0, c->stream>>>(pos, vel, fatm, mass, a.natm, dt, itime, ekin);
+  }
   CPSTEP_LAUNCH_CHECK();
   return atoms_set_positions_dev(c, pos);
+}
+
+void atom_nvt_free(cpstep_ctx* c) {
+  AtomNvt& t = c->atom_nvt;
+  cudaFree(t.d_kT); cudaFree(t.d_mnhc); cudaFree(t.d_vn); cudaFree(t.d_pkt); cudaFree(t.d_e);
+  t = AtomNvt();
+}
+
+int atom_nvt_set(cpstep_ctx* c, int len, int nres, int nyosh, const double* h_kT,
+                 const double* h_mnhc) {
+  atom_nvt_free(c);
+  if (len <= 0) return CPSTEP_OK;  // NVE
+  const int n = c->atoms.natm;
+  if (n <= 0) {
+    cpstep_set_error("set_atom_thermostat: no atoms set");
+    return CPSTEP_ERR_STATE;
+  }
+  if (len > ions::kMaxLen || nres < 1 || !h_kT || !h_mnhc ||
+      !(nyosh == 1 || nyosh == 3 || nyosh == 5 || nyosh == 7 || nyosh == 9)) {
+    cpstep_set_error("set_atom_thermostat: len_nhc in 1..%d, nres >= 1, nyosh in {1,3,5,7,9}",
+                     ions::kMaxLen);
+    return CPSTEP_ERR_ARG;
+  }
+  AtomNvt& t = c->atom_nvt;
+  t.len = len; t.nres = nres; t.nyosh = nyosh; t.natm = n;
+  CPSTEP_CUDA_TRY(cudaMalloc(&t.d_kT, sizeof(double) * n));
+  CPSTEP_CUDA_TRY(cudaMalloc(&t.d_mnhc, sizeof(double) * n * len));
+  CPSTEP_CUDA_TRY(cudaMalloc(&t.d_vn, sizeof(double) * n * 3 * len));
+  CPSTEP_CUDA_TRY(cudaMalloc(&t.d_pkt, sizeof(double) * n));
+  CPSTEP_CUDA_TRY(cudaMalloc(&t.d_e, sizeof(double) * 2));
+  CPSTEP_CUDA_TRY(cudaMemcpy(t.d_kT, h_kT, sizeof(double) * n, cudaMemcpyHostToDevice));
+  CPSTEP_CUDA_TRY(cudaMemcpy(t.d_mnhc, h_mnhc, sizeof(double) * n * len, cudaMemcpyHostToDevice));
+  CPSTEP_CUDA_TRY(cudaMemset(t.d_vn, 0, sizeof(double) * n * 3 * len));
+  CPSTEP_CUDA_TRY(cudaMemset(t.d_pkt, 0, sizeof(double) * n));
+  CPSTEP_CUDA_TRY(cudaMemset(t.d_e, 0, sizeof(double) * 2));
+  return CPSTEP_OK;
+}
+
+int atom_nvt_state(cpstep_ctx* c, int set, double* h_vn, double* h_pkt, double* h_e2) {
+  AtomNvt& t = c->atom_nvt;
+  if (t.len <= 0) {
+    cpstep_set_error("atom_thermostat_state: the atom thermostat is off");
+    return CPSTEP_ERR_STATE;
+  }
+  const int n = t.natm;
+  const size_t bv = sizeof(double) * n * 3 * t.len, bp = sizeof(double) * n;
+  auto dir = set ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+  if (h_vn) CPSTEP_CUDA_TRY(cudaMemcpyAsync(set ? (void*)t.d_vn : (void*)h_vn,
+                                            set ? (const void*)h_vn : (const void*)t.d_vn, bv,
+                                            dir, c->stream));
+  if (h_pkt) CPSTEP_CUDA_TRY(cudaMemcpyAsync(set ? (void*)t.d_pkt : (void*)h_pkt,
+                                             set ? (const void*)h_pkt : (const void*)t.d_pkt, bp,
+                                             dir, c->stream));
+  if (h_e2 && !set)
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(h_e2, t.d_e, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream));
+  CPSTEP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CPSTEP_OK;
 }

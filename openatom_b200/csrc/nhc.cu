@@ -303,6 +303,8 @@ void yosh(int nyosh, double* w) {
 
 }  // namespace nhc
 
+void nhc_yosh(int nyosh, double* w) { nhc::yosh(nyosh, w); }
+
 void nhc_free(cpstep_ctx* c) {
   CpNhc& t = c->nhc;
   cudaFree(t.d_ck); cudaFree(t.d_x); cudaFree(t.d_xp); cudaFree(t.d_vn);

@@ -83,3 +83,48 @@ def test_atoms_integrate_matches_oracle_and_moves_the_context(isys):
     finally:
         ctx.close()
         ref.close()
+
+
+@pytest.mark.parametrize("L,nres,nyosh", [(4, 1, 1), (2, 4, 9)])
+def test_atoms_nvt_matches_oracle(isys, L, nres, nyosh):
+    """The massive-NHC NVT atom step against oracle/ions.py nvt_step (pinned to
+    integration_drivers.C) over three steps, chains loaded from a sample."""
+    import torch
+    from oracle import ions as OI
+    from openatom_b200.context import StepContext
+    s = isys
+    n = s.natm
+    rng = np.random.default_rng(L * 7 + nyosh)
+    mass = np.where(np.asarray(s.typ) == s.typ[0], 29164.0, 1837.0).astype(np.float64)
+    kT = np.full(n, 300.0 / 315777.0)
+    mnhc = kT[:, None] * (200.0 / 0.0241888) ** 2 * (1.0 + 0.1 * np.arange(L))[None, :]
+    vn = rng.standard_normal((n, 3, L)) * np.sqrt(kT[:, None, None] / mnhc[:, None, :])
+    pkt = np.zeros(n)
+    pos_h = np.array(s.pos, dtype=np.float64)
+    vel_h = rng.standard_normal((n, 3)) * np.sqrt(kT[:, None] / mass[:, None])
+    ctx = StepContext(s.layout, s.nstates, precision="fp64")
+    try:
+        ctx.set_atoms(s)
+        ctx.set_atom_thermostat(L, kT, mnhc, nres, nyosh)
+        ctx.atom_thermostat_state(vn, pkt)
+        pos = torch.from_numpy(pos_h.copy()).cuda()
+        vel = torch.from_numpy(vel_h.copy()).cuda()
+        dm = torch.from_numpy(mass).cuda()
+        for it in range(3):
+            f = 1e-3 * rng.standard_normal((n, 3))
+            ek = ctx.atoms_integrate(it, pos, vel, torch.from_numpy(f).cuda(), dm, 20.0)
+            pos_h, vel_h, ekr, eknr, potr = OI.nvt_step(it, pos_h, vel_h, f, mass, kT, mnhc, vn,
+                                                        pkt, 20.0, nres, nyosh)
+            gvn, gpk, ge = ctx.atom_thermostat_state()
+            assert abs(ek - ekr) <= 1e-12 * ekr
+            assert abs(ge[0] - eknr) <= 1e-12 * eknr
+            assert abs(ge[1] - potr) <= 1e-12 * max(1e-12, abs(potr))
+            assert np.max(np.abs(vel.cpu().numpy() - vel_h)) <= 1e-12 * np.max(np.abs(vel_h))
+            assert np.max(np.abs(gvn - vn)) <= 1e-12 * np.max(np.abs(vn))
+            assert np.max(np.abs(pos.cpu().numpy() - pos_h)) <= 1e-12
+        ctx.set_atom_thermostat(0)
+        from openatom_b200 import _lib
+        with pytest.raises(_lib.CpstepError):
+            ctx.atom_thermostat_state()
+    finally:
+        ctx.close()
