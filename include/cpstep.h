@@ -38,6 +38,8 @@ extern "C" {
 #define CPSTEP_ERR_LAYOUT 3   /* inconsistent G-vector layout (util.C:956-1052 checks) */
 #define CPSTEP_ERR_NOCONV 4   /* Ortho S->T iteration did not converge (ortho.C:129-133) */
 #define CPSTEP_ERR_STATE 5    /* call out of order */
+#define CPSTEP_ERR_NORB 6     /* S fails cp_norb_tol on the first dynamics step
+                                 (Ortho::maxCheck, orthog_ctrl/ortho.C:477-482) */
 
 /* slots of the energies array (Hartree): the reference's Iter [n] names */
 #define CPSTEP_E_EXC 0     /* EEXC       (CP_exc_calc exc_ret)                */
@@ -412,11 +414,13 @@ CPSTEP_API int cpstep_ees_nonlocal(cpstep_ctx* ctx, const double* d_psi, const d
  * cpstep_cp_step: one electronic step on orthonormal psi (S = 2 I):
  *   rho -> V_KS (XC, Hartree, local, Ewald) -> F = V.psi + kinetic force
  *   (+ the EES non-local force when cpstep_set_nonlocal was called) ->
- *   lambda = <psi|F>, F <- F - wpt/2 psi.lambda -> Verlet -> S -> T = (S/2)^-1/2
- *   -> psi <- psi.T.  d_energies (CPSTEP_NENERGY doubles, device) receives
- *   every slot; d_atom_force (may be NULL) the local + Ewald (+ non-local)
- *   atom forces.
+ *   lambda = <psi|F> -> the constraint of cpstep_set_constraint (below) ->
+ *   Verlet -> S -> T = (S/2)^-1/2 -> psi = (the integrated coefficients).T.
+ *   d_energies (CPSTEP_NENERGY doubles, device) receives every slot;
+ *   d_atom_force (may be NULL) the local + Ewald (+ non-local) atom forces.
  *   Asynchronous: the Ortho convergence of the step is read by cpstep_step_status.
+ *   With the orthoT constraint, iteration 1 returns CPSTEP_ERR_NORB (after the
+ *   step) when S of the integrated coefficients fails cp_norb_tol.
  * cpstep_step_status: iterations and convergence flag of the last Ortho launch
  *   (synchronises the context's stream).
  */
@@ -457,6 +461,50 @@ CPSTEP_API int cpstep_cp_step(cpstep_ctx* ctx, double* d_psi, double* d_vpsi,
                               const double* d_occ, double dt, int iteration,
                               double* d_energies, double* d_atom_force);
 CPSTEP_API int cpstep_step_status(cpstep_ctx* ctx, int* ortho_iters, int* converged);
+
+/*
+ * The orthonormality constraint of cpstep_cp_step.
+ * CPSTEP_CONSTRAINT_ORTHO_T (the default): the reference's CP dynamics
+ *   (cp_min_opt = 0).  The context carries the non-orthogonal coefficients
+ *   psi_no (CP_State_GSpacePlane's packedPlaneDataScr) and orthoT (the T of
+ *   the previous step, Ortho::orthoT, orthog_ctrl/ortho.C:358-365).  Per step:
+ *     gamma = orthoT lambda              Ortho::acceptSectionLambda (ortho.C:541-583)
+ *     F_c = F.orthoT - W psi.gamma       PairCalculator::bwMultiplyDynOrthoT and the
+ *                                        gamma product of bwMultiplyHelper
+ *                                        (paircalc/ckPairCalculator.C:1444-1510,
+ *                                        :1372-1420), unpackLambda / doLambda
+ *                                        (CP_State_GSpacePlane.C:2060-2268):
+ *                                        W = 1/2 on Gx=0, 1 elsewhere
+ *     Verlet on psi_no with F_c; S = overlap(psi_no); T; psi = psi_no.T
+ *     max |S - 2I| >= tol_norb (Ortho::maxCheck, ortho.C:461-483) after the
+ *     first step: the finite-difference PsiV reset (finiteDifferencePsiV,
+ *     CP_State_GSpacePlane.C:3707-3770, order 0): psi_no <- psi,
+ *     v = (psi(t+dt) - psi(t)) / dt, orthoT <- I, and the next step has no
+ *     second half kick (halfStepEvolve = 0, cp_dynamics.C:58).
+ *   Iteration 1 starts from psi_no = psi and orthoT = I unless a state was
+ *   loaded with cpstep_dyn_state since the last step.
+ * CPSTEP_CONSTRAINT_LOWDIN: F <- F - W psi.lambda (the minimisation
+ *   constraint, CP_State_GSpacePlane.C:2079-2088), Verlet on psi itself, then
+ *   psi <- psi.T; no state between steps.
+ * cpstep_set_constraint: form and tol_norb (cp_norb_tol, reference default
+ *   0.003, set_sim_dict.C:1161-1162; > 0).  Drops the step graph and the
+ *   carried state.
+ * cpstep_dyn_state: read (set = 0) or load (set = 1) the carried state:
+ *   device arrays d_psi_no [nstates][npts] complex128 and d_tmat (nstates^2,
+ *   column-major), and the host int *h_half_step (the reference's
+ *   halfStepEvolve: 0 after a reset, when the next step has no second half
+ *   kick; 1 otherwise).  On a read any pointer may be NULL; a load needs both
+ *   arrays (h_half_step NULL loads 1).  A load marks the state for the next
+ *   step (iteration 1 then keeps it).
+ * cpstep_dyn_status: max |S - 2I| of the last step's check and the PsiV
+ *   resets so far (synchronises the context's stream); either may be NULL.
+ */
+#define CPSTEP_CONSTRAINT_ORTHO_T 0
+#define CPSTEP_CONSTRAINT_LOWDIN 1
+CPSTEP_API int cpstep_set_constraint(cpstep_ctx* ctx, int form, double tol_norb);
+CPSTEP_API int cpstep_dyn_state(cpstep_ctx* ctx, int set, double* d_psi_no, double* d_tmat,
+                                int* h_half_step);
+CPSTEP_API int cpstep_dyn_status(cpstep_ctx* ctx, double* max_dev, int* resets);
 
 /*
  * CUDA graph of the step (no reference counterpart; the reference's step is a

@@ -15,6 +15,9 @@ CPSTEP_ERR_CUDA = 2
 CPSTEP_ERR_LAYOUT = 3
 CPSTEP_ERR_NOCONV = 4
 CPSTEP_ERR_STATE = 5
+CPSTEP_ERR_NORB = 6
+CONSTRAINT_ORTHO_T = 0
+CONSTRAINT_LOWDIN = 1
 PREC_FP64 = 0
 PREC_MIXED = 1
 
@@ -96,6 +99,9 @@ SIGNATURES = {
     "cpstep_cp_step": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int, _vp,
                                       _vp]),
     "cpstep_step_status": (ctypes.c_int, [_vp, _c_int_p, _c_int_p]),
+    "cpstep_set_constraint": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),
+    "cpstep_dyn_state": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _c_int_p]),
+    "cpstep_dyn_status": (ctypes.c_int, [_vp, _c_dbl_p, _c_int_p]),
     "cpstep_set_gemm_path": (ctypes.c_int, [_vp, ctypes.c_int]),
     "cpstep_state_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _vp,
                                           _vp, _vp, _vp, ctypes.c_int, ctypes.c_int,

@@ -427,6 +427,38 @@ class StepContext:
                   int(iteration), ptr(e), ptr(f))
         return e, f
 
+    def set_constraint(self, form="ortho_t", tol_norb=0.003):
+        """The step's orthonormality constraint: "ortho_t" (the reference's CP
+        dynamics: non-orthogonal coefficients and orthoT carried between
+        steps, PsiV reset when max|S-2I| >= tol_norb) or "lowdin"."""
+        f = {"ortho_t": _lib.CONSTRAINT_ORTHO_T, "lowdin": _lib.CONSTRAINT_LOWDIN}[form]
+        _lib.call("cpstep_set_constraint", self._h, f, float(tol_norb))
+
+    def dyn_state(self, psi_no=None, tmat=None, half_step=1):
+        """Load (psi_no and tmat given) or read the carried state of the orthoT
+        form: (psi_no, tmat, half_step) with half_step the reference's
+        halfStepEvolve (0 right after a PsiV reset)."""
+        self._sync_stream()
+        if psi_no is not None or tmat is not None:
+            tcm = tmat.t().contiguous()  # column-major for the C ABI
+            h = ctypes.c_int(int(half_step))
+            _lib.call("cpstep_dyn_state", self._h, 1, ptr(psi_no), ptr(tcm), ctypes.byref(h))
+            torch.cuda.synchronize(self.device)
+            return psi_no, tmat, int(half_step)
+        p = torch.empty((self.nstates, self.layout.npts), dtype=torch.complex128,
+                        device=self.device)
+        t = torch.empty((self.nstates, self.nstates), dtype=torch.float64, device=self.device)
+        h = ctypes.c_int()
+        _lib.call("cpstep_dyn_state", self._h, 0, ptr(p), ptr(t), ctypes.byref(h))
+        torch.cuda.synchronize(self.device)
+        return p, t.t().contiguous(), h.value
+
+    def dyn_status(self):
+        """(max |S - 2I| of the last step's check, PsiV resets so far)."""
+        d, r = ctypes.c_double(), ctypes.c_int()
+        _lib.call("cpstep_dyn_status", self._h, ctypes.byref(d), ctypes.byref(r))
+        return d.value, r.value
+
     def set_gemm_path(self, tensor_cores):
         """Mixed contexts: overlap / back-multiply on the tensor cores (split BF16) or in FP64."""
         _lib.call("cpstep_set_gemm_path", self._h, 1 if tensor_cores else 0)

@@ -585,6 +585,23 @@ int cpstep_cp_step(cpstep_ctx* c, double* d_psi, double* d_vpsi, const double* d
     return CPSTEP_ERR_STATE;
   }
   // the first step (no second half kick) and profiled steps run directly
+  if (iteration <= 1 && c->dyn_form == CPSTEP_CONSTRAINT_ORTHO_T) {
+    int rc = step_run(c, d_psi, d_vpsi, d_occ, dt, iteration, d_energies, d_atom_force, 0);
+    if (rc) return rc;
+    int fl[4] = {0, 0, 0, 0};
+    double dev = 0.0;
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(fl, c->d_dyn_flags, sizeof(fl), cudaMemcpyDeviceToHost,
+                                    c->stream));
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(&dev, c->d_dyn_dev, sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream));
+    CPSTEP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (fl[3]) {
+      cpstep_set_error("cp_step: S fails cp_norb_tol on the first step (max |S - 2I| = %g >= %g)",
+                       dev, c->tol_norb);
+      return CPSTEP_ERR_NORB;
+    }
+    return CPSTEP_OK;
+  }
   if (!c->use_graph || iteration <= 1 || c->profile)
     return step_run(c, d_psi, d_vpsi, d_occ, dt, iteration, d_energies, d_atom_force, 0);
   const cpstep_ctx::StepKey key{d_psi, d_vpsi, d_occ, dt, d_energies, d_atom_force};
@@ -629,6 +646,82 @@ int cpstep_cp_step(cpstep_ctx* c, double* d_psi, double* d_vpsi, const double* d
   c->gkernels = nk;
   CPSTEP_CUDA_TRY(cudaGraphLaunch(c->gexec, c->stream));
   __atomic_add_fetch(&g_cpstep_launches, c->gkernels, __ATOMIC_RELAXED);
+  return CPSTEP_OK;
+}
+
+int cpstep_set_constraint(cpstep_ctx* c, int form, double tol_norb) {
+  if (!c || (form != CPSTEP_CONSTRAINT_ORTHO_T && form != CPSTEP_CONSTRAINT_LOWDIN) ||
+      !(tol_norb > 0.0))
+    return CPSTEP_ERR_ARG;
+  graph_drop(c);
+  c->dyn_form = form;
+  c->tol_norb = tol_norb;
+  c->dyn_init = 0;
+  c->dyn_loaded = 0;
+  return CPSTEP_OK;
+}
+
+int cpstep_dyn_state(cpstep_ctx* c, int set, double* d_psi_no, double* d_tmat,
+                     int* h_half_step) {
+  if (!c || (set != 0 && set != 1)) return CPSTEP_ERR_ARG;
+  const size_t ncoef = (size_t)c->nstates * c->npts;
+  const size_t nt = (size_t)c->nstates * c->nstates;
+  if (set) {
+    if (!d_psi_no || !d_tmat) {
+      cpstep_set_error("dyn_state: a load needs both psi_no and orthoT");
+      return CPSTEP_ERR_ARG;
+    }
+    graph_drop(c);
+    if (!c->d_psi_no) CPSTEP_CUDA_TRY(cudaMalloc(&c->d_psi_no, sizeof(double2) * ncoef));
+    if (!c->d_tmat) CPSTEP_CUDA_TRY(cudaMalloc(&c->d_tmat, sizeof(double) * nt));
+    if (!c->d_dyn_flags) CPSTEP_CUDA_TRY(cudaMalloc(&c->d_dyn_flags, 4 * sizeof(int)));
+    if (!c->d_dyn_dev) CPSTEP_CUDA_TRY(cudaMalloc(&c->d_dyn_dev, sizeof(double)));
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(c->d_psi_no, d_psi_no, sizeof(double2) * ncoef,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(c->d_tmat, d_tmat, sizeof(double) * nt,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+    // flags: no reset pending, [1] = 1 - halfStepEvolve, no resets counted
+    int fl[4] = {0, (h_half_step && *h_half_step == 0) ? 1 : 0, 0, 0};
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(c->d_dyn_flags, fl, sizeof(fl), cudaMemcpyHostToDevice,
+                                    c->stream));
+    CPSTEP_CUDA_TRY(cudaStreamSynchronize(c->stream));  // fl is on this stack frame
+    c->dyn_init = 1;
+    c->dyn_loaded = 1;
+    return CPSTEP_OK;
+  }
+  if (!c->dyn_init) {
+    cpstep_set_error("dyn_state: no state yet (run iteration 1 or load one)");
+    return CPSTEP_ERR_STATE;
+  }
+  if (d_psi_no)
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(d_psi_no, c->d_psi_no, sizeof(double2) * ncoef,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+  if (d_tmat)
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(d_tmat, c->d_tmat, sizeof(double) * nt,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+  if (h_half_step) {
+    int fl[4] = {0, 0, 0, 0};
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(fl, c->d_dyn_flags, sizeof(fl), cudaMemcpyDeviceToHost,
+                                    c->stream));
+    CPSTEP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    *h_half_step = fl[1] ? 0 : 1;
+  }
+  return CPSTEP_OK;
+}
+
+int cpstep_dyn_status(cpstep_ctx* c, double* max_dev, int* resets) {
+  if (!c) return CPSTEP_ERR_ARG;
+  int fl[4] = {0, 0, 0, 0};
+  double dev = 0.0;
+  if (c->d_dyn_flags)
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(fl, c->d_dyn_flags, sizeof(fl), cudaMemcpyDeviceToHost,
+                                    c->stream));
+  if (c->d_dyn_dev)
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(&dev, c->d_dyn_dev, sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream));
+  CPSTEP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (max_dev) *max_dev = dev;
+  if (resets) *resets = fl[2];
   return CPSTEP_OK;
 }
 

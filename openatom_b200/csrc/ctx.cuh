@@ -276,6 +276,19 @@ struct cpstep_ctx {
   double *d_psi_tmp = nullptr, *d_rho = nullptr, *d_vks = nullptr, *d_eke = nullptr;
   double* d_force = nullptr;
   double* d_force_atoms = nullptr;  // staging of cpstep_cp_step_host
+  // the orthonormality constraint of the step (cpstep_set_constraint):
+  // CPSTEP_CONSTRAINT_ORTHO_T carries the non-orthogonal coefficients d_psi_no
+  // and orthoT (d_tmat, the previous step's T) between steps;
+  // CPSTEP_CONSTRAINT_LOWDIN needs neither
+  int dyn_form = 0;
+  double tol_norb = 0.003;
+  int dyn_init = 0;             // d_psi_no / d_tmat hold a state (iteration 1 or loaded)
+  int dyn_loaded = 0;           // loaded by cpstep_dyn_state since the last step
+  double* d_psi_no = nullptr;   // [nstates][npts] complex
+  double* d_gamma = nullptr;    // gamma = orthoT lambda, S x S column-major
+  int* d_dyn_flags = nullptr;   // [0] reset in this step, [1] next integrate skips the
+                                // second half kick, [2] resets so far, [3] first-step failure
+  double* d_dyn_dev = nullptr;  // max |S - 2I| of the last step
   // phase timing (cpstep_ctx_profile): events recorded on the context's stream
   // (a ring of PROF_RING steps' events, folded into prof_ms when it fills or
   // when cpstep_phase_times is called, so profiling adds no per-step sync)
@@ -454,7 +467,8 @@ int step_init_classes(cpstep_ctx* c);
 void step_free(cpstep_ctx* c);
 int step_set_mass(cpstep_ctx* c, double tau_fs, double cut_ry);
 int step_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi, double dt,
-                   int iteration, double* d_fict_ke, double* d_enhc);
+                   int iteration, double* d_fict_ke, double* d_enhc,
+                   const int* d_skip_half = nullptr);
 
 // nhc.cu
 int nhc_set(cpstep_ctx* c, double te_ext, double tau_fs, int num, int nck, int nres, int nyosh);
@@ -466,7 +480,7 @@ int atom_nvt_set(cpstep_ctx* c, int len, int nres, int nyosh, const double* h_kT
 void atom_nvt_free(cpstep_ctx* c);
 int atom_nvt_state(cpstep_ctx* c, int set, double* h_vn, double* h_pkt, double* h_e2);
 int nhc_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi, double dt,
-                  int iteration, double* d_fict_ke, double* d_enhc);
+                  int iteration, double* d_fict_ke, double* d_enhc, const int* d_skip_half);
 int step_run(cpstep_ctx* c, double* psi, double* vpsi, const double* occ, double dt,
              int iteration, double* energies, double* atom_force, int ortho_check);
 

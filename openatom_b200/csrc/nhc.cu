@@ -44,8 +44,10 @@ struct Par {
 __global__ void k_nhc_ekin(const double2* __restrict__ v, const double2* __restrict__ f,
                            const double* __restrict__ cmass, const int* __restrict__ cls,
                            const signed char* __restrict__ ck, int npts, int span, double dt,
-                           int first, int nck, double* __restrict__ part) {
+                           int first_in, const int* __restrict__ skip, int nck,
+                           double* __restrict__ part) {
   __shared__ double red[32];
+  const int first = first_in && !(skip && *skip);
   const int s = blockIdx.y;
   const int p0 = blockIdx.x * span, p1 = min(npts, p0 + span);
   const double dt2 = 0.5 * dt;
@@ -166,9 +168,11 @@ __device__ double iso_update(double ekin, double gkt, const Par& P, double (&x)[
 // the time of get_fictKE; scale[t] = {s2, s1}
 template <int NUM>
 __global__ void k_nhc_update(Par P, const double* __restrict__ part, int nsplit, int nstates,
-                             int first, double* __restrict__ x, double* __restrict__ xp,
+                             int first_in, const int* __restrict__ skip,
+                             double* __restrict__ x, double* __restrict__ xp,
                              double* __restrict__ vn, double* __restrict__ scale,
                              double* __restrict__ eout) {
+  const int first = first_in && !(skip && *skip);
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nstates * P.nck) return;
   const int s = t / P.nck, k = t % P.nck;
@@ -237,7 +241,8 @@ __global__ void k_nhc_apply(double2* __restrict__ psi, double2* __restrict__ v,
                             const double2* __restrict__ f, const double* __restrict__ cmass,
                             const int* __restrict__ cls, const signed char* __restrict__ ck,
                             const double* __restrict__ scale, int nck, int npts, int nstates,
-                            double dt, int first) {
+                            double dt, int first_in, const int* __restrict__ skip) {
+  const int first = first_in && !(skip && *skip);
   const double dt2 = 0.5 * dt;
   const size_t n = (size_t)npts * nstates;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -400,7 +405,7 @@ int nhc_state(cpstep_ctx* c, int set, double* h_x, double* h_xp, double* h_vn) {
 }
 
 int nhc_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi, double dt,
-                  int iteration, double* d_fict_ke, double* d_enhc) {
+                  int iteration, double* d_fict_ke, double* d_enhc, const int* d_skip_half) {
   CpNhc& t = c->nhc;
   nhc::Par P;
   P.num = t.num; P.nck = t.nck; P.nres = t.nres; P.nyosh = t.nyosh;
@@ -418,13 +423,14 @@ int nhc_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi,
   double2* v = reinterpret_cast<double2*>(vpsi);
   const double2* f = reinterpret_cast<const double2*>(force);
   nhc::k_nhc_ekin<<<dim3(t.nsplit, c->nstates), 256, 0, c->stream>>>(
-      v, f, c->d_cmass, c->d_cls, t.d_ck, c->npts, t.span, dt, first, t.nck, t.d_part);
+      v, f, c->d_cmass, c->d_cls, t.d_ck, c->npts, t.span, dt, first, d_skip_half, t.nck,
+      t.d_part);
   CPSTEP_LAUNCH_CHECK();
   const int nt = c->nstates * t.nck;
   const dim3 ug((nt + 31) / 32), ub(32);
 #define NHC_UPDATE(N)                                                                        \
   nhc::k_nhc_update<N><<<ug, ub, 0, c->stream>>>(P, t.d_part, t.nsplit, c->nstates, first,  \
-                                                 t.d_x, t.d_xp, t.d_vn, t.d_scale, t.d_eout)
+                                                 d_skip_half, t.d_x, t.d_xp, t.d_vn, t.d_scale, t.d_eout)
   switch (t.num) {
     case 1: NHC_UPDATE(1); break;
     case 2: NHC_UPDATE(2); break;
@@ -443,7 +449,7 @@ int nhc_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi,
   }
   nhc::k_nhc_apply<<<c->nblk_ke, 256, 0, c->stream>>>(p, v, f, c->d_cmass, c->d_cls, t.d_ck,
                                                        t.d_scale, t.nck, c->npts, c->nstates,
-                                                       dt, first);
+                                                       dt, first, d_skip_half);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }

@@ -8,6 +8,23 @@
 //                  cp_state_ctrl/CP_State_GSpacePlane.C:2862-3061
 //   lambda, constrained force, S, T, psi.T  (PairCalculator / Ortho, see paircalc.cu, ortho.cu)
 //
+// The constraint of the reference's CP dynamics (CPSTEP_CONSTRAINT_ORTHO_T,
+// the default), src_charm_driver/:
+//   lambda = <psi_o|F>   asymmetric PairCalculator, alpha = 1 (main/cpaimd.C:2527)
+//   gamma = orthoT lambda            orthog_ctrl/ortho.C:541-583 (orthoT: the previous
+//                                    step's T, :358-365; the identity after a reset)
+//   F_c = F orthoT - W psi_o gamma   paircalc/ckPairCalculator.C:1444-1510 (-F.T) and
+//                                    :1372-1420 (gamma), negated by unpackLambda and
+//                                    scaled 1/sqrt(2) on Gx=0 by doLambda
+//                                    (cp_state_ctrl/CP_State_GSpacePlane.C:2197-2202,
+//                                    :2253-2268): W = 1/2 on Gx=0, 1 elsewhere
+//   Verlet on the non-orthogonal psi_no (doLambda restores it, integrateModForce)
+//   S = overlap(psi_no); max |S - 2I| >= cp_norb_tol fails Ortho::maxCheck
+//                                    (ortho.C:255-262, :461-483): fatal on the first
+//                                    step, later the finite-difference PsiV reset
+//                                    (CP_State_GSpacePlane.C:3707-3770, order 0)
+//   psi_o = psi_no T                 (ckPairCalculator.C:1314)
+//
 // Point classes of the packed layout (the reference's nkx0_red / nkx0_zero /
 // nkx0_uni ranges of every chunk): 0 = redundant lower Gx=0 half (overwritten
 // by the conjugate of its partner, not integrated), 1 = G=0 (imaginary parts
@@ -23,11 +40,15 @@ namespace stp {
 // fictitious KE between them, the drift), in the per-element order of the
 // reference's half steps: second half kick of the previous step when
 // `first`, KE, first half kick, psi += v dt.
+// skip (device, may be NULL): nonzero after a PsiV reset, when the reference
+// evolves the next step with halfStepEvolve = 0 (no second half kick).
 __global__ void k_integrate(double2* __restrict__ psi, double2* __restrict__ v,
                             const double2* __restrict__ f, const double* __restrict__ cmass,
                             const int* __restrict__ cls, int npts, int nstates, double dt,
-                            int first, double* __restrict__ ke_part) {
+                            int first_in, const int* __restrict__ skip,
+                            double* __restrict__ ke_part) {
   __shared__ double red[32];
+  const int first = first_in && !(skip && *skip);
   double ke = 0.0;
   const double dt2 = 0.5 * dt;
   const size_t n = (size_t)npts * nstates;
@@ -98,6 +119,81 @@ __global__ void k_energy_tot(const double* __restrict__ eke, int nstates,
   }
 }
 
+// max |S - 2I| over the n x n overlap (Ortho::array_diag_max with diag = 2,
+// ortho.h:282-310) against cp_norb_tol (Ortho::maxCheck, ortho.C:461-483):
+// after the first step a failure asks for the PsiV reset (flags[0]); on the
+// first step it is fatal (flags[3]).  A NaN fails, as !(max < tol) does there.
+__global__ void k_norb_check(const double* __restrict__ S, int n, double tol, int later,
+                             int* __restrict__ flags, double* __restrict__ dev) {
+  __shared__ double red[32];
+  double m = 0.0;
+  const int nn = n * n;
+  for (int i = threadIdx.x; i < nn; i += blockDim.x) {
+    const double a = fabs(S[i] - ((i % n) == (i / n) ? 2.0 : 0.0));
+    m = (a > m || a != a) ? a : m;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double b = __shfl_xor_sync(0xffffffffu, m, o);
+    m = (b > m || b != b) ? b : m;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = (red[w] > m || red[w] != red[w]) ? red[w] : m;
+    *dev = m;
+    const int fail = !(m < tol);
+    flags[0] = later && fail;
+    if (!later && fail) flags[3] = 1;
+  }
+}
+
+// finiteDifferencePsiV (CP_State_GSpacePlane.C:3707-3770), first part: keep
+// psi_o(t) before psi_o(t+dt) overwrites it (only when this step resets).
+__global__ void k_psiv_save(const int* __restrict__ flags, const double2* __restrict__ psi,
+                            double2* __restrict__ save, size_t n) {
+  if (!flags[0]) return;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    save[i] = psi[i];
+}
+
+// second part: psi_no <- psi_o(t+dt), v = (psi_o(t+dt) - psi_o(t)) / dt
+// (norb_fin_diff_order 0), orthoT <- I (ortho.C:545-562); the next
+// integrate runs without the second half kick (flags[1]).
+__global__ void k_psiv_apply(int* __restrict__ flags, const double2* __restrict__ psi,
+                             const double2* __restrict__ save, double2* __restrict__ psi_no,
+                             double2* __restrict__ v, double* __restrict__ T, int nst, size_t n,
+                             double rdt) {
+  const int f = flags[0];
+  if (f) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+      const double2 a = psi[i], b = save[i];
+      v[i] = make_double2((a.x - b.x) * rdt, (a.y - b.y) * rdt);
+      psi_no[i] = a;
+    }
+    const size_t nt = (size_t)nst * nst;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += stride)
+      T[i] = (i % nst) == (i / nst) ? 1.0 : 0.0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    flags[1] = f;
+    flags[2] += f;
+  }
+}
+
+// identity into T (n x n) and the reset flags cleared: the state before the
+// first step of the reference form
+__global__ void k_dyn_start(double* __restrict__ T, int n, int* __restrict__ flags,
+                            double* __restrict__ dev) {
+  const size_t nt = (size_t)n * n;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nt;
+       i += (size_t)gridDim.x * blockDim.x)
+    T[i] = (i % n) == (i / n) ? 1.0 : 0.0;
+  if (blockIdx.x == 0 && threadIdx.x < 4) flags[threadIdx.x] = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *dev = 0.0;
+}
+
 }  // namespace stp
 
 // ===========================================================================
@@ -155,7 +251,8 @@ void step_free(cpstep_ctx* c) {
   cudaFree(c->d_cls); cudaFree(c->d_red_idx); cudaFree(c->d_red_src); cudaFree(c->d_cmass);
   cudaFree(c->d_step_part); cudaFree(c->d_lambda); cudaFree(c->d_smat); cudaFree(c->d_tmat);
   cudaFree(c->d_psi_tmp); cudaFree(c->d_rho); cudaFree(c->d_vks); cudaFree(c->d_eke);
-  cudaFree(c->d_force);
+  cudaFree(c->d_force); cudaFree(c->d_psi_no); cudaFree(c->d_gamma); cudaFree(c->d_dyn_flags);
+  cudaFree(c->d_dyn_dev);
 }
 
 // set_cpmass (set_cp_ewald.C:32-74): cmass0 = 4 tau^2 CP_EMAGIC (tau in a.u.),
@@ -183,7 +280,7 @@ int step_set_mass(cpstep_ctx* c, double tau_fs, double cut_ry) {
 // redundant-half sync.  d_enhc (2 doubles, may be NULL): the NHC kinetic
 // energy and potential of get_fictKE, zero without the thermostat.
 int step_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi, double dt,
-                   int iteration, double* d_fict_ke, double* d_enhc) {
+                   int iteration, double* d_fict_ke, double* d_enhc, const int* d_skip_half) {
   if (!c->d_cmass) {
     cpstep_set_error("integrate: CP masses not set (cpstep_set_cp_mass)");
     return CPSTEP_ERR_STATE;
@@ -193,7 +290,7 @@ int step_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi
   const double2* f = reinterpret_cast<const double2*>(force);
   int nb = c->nblk_ke;
   if (c->nhc.on) {
-    int rc = nhc_integrate(c, force, psi, vpsi, dt, iteration, d_fict_ke, d_enhc);
+    int rc = nhc_integrate(c, force, psi, vpsi, dt, iteration, d_fict_ke, d_enhc, d_skip_half);
     if (rc) return rc;
     if (c->nred) {
       stp::k_sync_red<<<nb, 256, 0, c->stream>>>(p, v, c->d_red_idx, c->d_red_src, c->nred,
@@ -205,7 +302,7 @@ int step_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi
   if (d_enhc) CPSTEP_CUDA_TRY(cudaMemsetAsync(d_enhc, 0, 2 * sizeof(double), c->stream));
   stp::k_integrate<<<nb, 256, 0, c->stream>>>(p, v, f, c->d_cmass, c->d_cls, c->npts,
                                               c->nstates, dt, iteration > 1 ? 1 : 0,
-                                              c->d_step_part);
+                                              d_skip_half, c->d_step_part);
   CPSTEP_LAUNCH_CHECK();
   if (d_fict_ke) {
     stp::k_sum<<<1, 256, 0, c->stream>>>(c->d_step_part, nb, d_fict_ke);
@@ -272,27 +369,92 @@ int step_run(cpstep_ctx* c, double* psi, double* vpsi, const double* occ, double
   stp::k_energy_tot<<<1, 32, 0, c->stream>>>(c->d_eke, S, energies);
   CPSTEP_LAUNCH_CHECK();
   mark(4);
-  // 3. lambda_ji = sum_p Re(conj psi_j F_i); F <- F - (wpt/2) psi.lambda
   const int K = 2 * c->npts;
-  if ((rc = pc_overlap_launch(c, psi, c->d_force, S, S, K, nullptr, 1.0, 0.0, c->d_lambda, S))) return rc;
-  if ((rc = pc_backmul_w_launch(c, c->d_lambda, S, psi, K, c->d_force, K, S, S, K, -0.5, 1.0,
-                                c->d_wpt)))
-    return rc;
-  mark(5);
-  // 4. Verlet update
-  if ((rc = step_integrate(c, c->d_force, psi, vpsi, dt, iteration, energies + CPSTEP_E_FICT,
-                           energies + CPSTEP_E_NHC_KE)))
-    return rc;
-  mark(6);
-  // 5. S = overlap, T = (S/2)^(-1/2), psi <- psi.T
-  if ((rc = pc_overlap_launch(c, psi, psi, S, S, K, c->d_wpt, 1.0, 0.0, c->d_smat, S))) return rc;
   const int mixed = c->precision == CPSTEP_PREC_MIXED;
-  if ((rc = ortho_tmat(c, c->d_smat, c->d_tmat, S, mixed, 0, mixed ? 2e-6 : 1e-15,
-                       mixed ? 20 : 10, nullptr, nullptr, ortho_check)))
-    return rc;
-  if ((rc = pc_backmul_launch(c, c->d_tmat, S, psi, K, c->d_psi_tmp, K, S, S, K, 1.0, 0.0))) return rc;
-  CPSTEP_CUDA_TRY(cudaMemcpyAsync(psi, c->d_psi_tmp, sizeof(double2) * ncoef,
-                                  cudaMemcpyDeviceToDevice, c->stream));
+  if (c->dyn_form == CPSTEP_CONSTRAINT_LOWDIN) {
+    // 3. lambda_ji = sum_p Re(conj psi_j F_i); F <- F - (wpt/2) psi.lambda
+    if ((rc = pc_overlap_launch(c, psi, c->d_force, S, S, K, nullptr, 1.0, 0.0, c->d_lambda, S))) return rc;
+    if ((rc = pc_backmul_w_launch(c, c->d_lambda, S, psi, K, c->d_force, K, S, S, K, -0.5, 1.0,
+                                  c->d_wpt)))
+      return rc;
+    mark(5);
+    // 4. Verlet update
+    if ((rc = step_integrate(c, c->d_force, psi, vpsi, dt, iteration, energies + CPSTEP_E_FICT,
+                             energies + CPSTEP_E_NHC_KE)))
+      return rc;
+    mark(6);
+    // 5. S = overlap, T = (S/2)^(-1/2), psi <- psi.T
+    if ((rc = pc_overlap_launch(c, psi, psi, S, S, K, c->d_wpt, 1.0, 0.0, c->d_smat, S))) return rc;
+    if ((rc = ortho_tmat(c, c->d_smat, c->d_tmat, S, mixed, 0, mixed ? 2e-6 : 1e-15,
+                         mixed ? 20 : 10, nullptr, nullptr, ortho_check)))
+      return rc;
+    if ((rc = pc_backmul_launch(c, c->d_tmat, S, psi, K, c->d_psi_tmp, K, S, S, K, 1.0, 0.0))) return rc;
+    CPSTEP_CUDA_TRY(cudaMemcpyAsync(psi, c->d_psi_tmp, sizeof(double2) * ncoef,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+  } else {
+    // the reference's dynamics: psi_no and orthoT (d_tmat) carry over
+    if ((rc = ensure_buf(&c->d_psi_no, sizeof(double2) * ncoef)) ||
+        (rc = ensure_buf(&c->d_gamma, sizeof(double) * S * S)) ||
+        (rc = ensure_buf(&c->d_dyn_dev, sizeof(double))))
+      return rc;
+    if (!c->d_dyn_flags) CPSTEP_CUDA_TRY(cudaMalloc(&c->d_dyn_flags, 4 * sizeof(int)));
+    if (iteration == 1 && !c->dyn_loaded) {
+      // iteration 0 of the reference orthonormalised the input: psi_no = psi, orthoT = I
+      CPSTEP_CUDA_TRY(cudaMemcpyAsync(c->d_psi_no, psi, sizeof(double2) * ncoef,
+                                      cudaMemcpyDeviceToDevice, c->stream));
+      stp::k_dyn_start<<<cdiv(S * S, 256), 256, 0, c->stream>>>(c->d_tmat, S, c->d_dyn_flags,
+                                                                 c->d_dyn_dev);
+      CPSTEP_LAUNCH_CHECK();
+      c->dyn_init = 1;
+    } else if (!c->dyn_init) {
+      cpstep_set_error("cp_step: iteration %d of the orthoT form needs iteration 1 or a state "
+                       "loaded by cpstep_dyn_state", iteration);
+      return CPSTEP_ERR_STATE;
+    }
+    c->dyn_loaded = 0;
+    // 3. lambda = <psi_o|F>, gamma = orthoT lambda, F_c = F.orthoT - W psi_o.gamma
+    if ((rc = pc_overlap_launch(c, psi, c->d_force, S, S, K, nullptr, 1.0, 0.0, c->d_lambda, S))) return rc;
+    if ((rc = dgemm_launch(c->stream, 0, 0, S, S, S, 1.0, c->d_tmat, S, c->d_lambda, S, 0.0,
+                           c->d_gamma, S)))
+      return rc;
+    if ((rc = pc_backmul_launch(c, c->d_tmat, S, c->d_force, K, c->d_psi_tmp, K, S, S, K, 1.0,
+                                0.0)))
+      return rc;
+    if ((rc = pc_backmul_w_launch(c, c->d_gamma, S, psi, K, c->d_psi_tmp, K, S, S, K, -0.5, 1.0,
+                                  c->d_wpt)))
+      return rc;
+    mark(5);
+    // 4. Verlet update of the non-orthogonal coefficients (no second half kick
+    // after a reset: flags[1])
+    if ((rc = step_integrate(c, c->d_psi_tmp, c->d_psi_no, vpsi, dt, iteration,
+                             energies + CPSTEP_E_FICT, energies + CPSTEP_E_NHC_KE,
+                             c->d_dyn_flags + 1)))
+      return rc;
+    mark(6);
+    // 5. S = overlap(psi_no), the norb check, T = (S/2)^(-1/2), psi_o = psi_no.T
+    // written straight into psi; the PsiV reset on a failed check
+    if ((rc = pc_overlap_launch(c, c->d_psi_no, c->d_psi_no, S, S, K, c->d_wpt, 1.0, 0.0,
+                                c->d_smat, S)))
+      return rc;
+    stp::k_norb_check<<<1, 1024, 0, c->stream>>>(c->d_smat, S, c->tol_norb, iteration > 1,
+                                                 c->d_dyn_flags, c->d_dyn_dev);
+    CPSTEP_LAUNCH_CHECK();
+    if ((rc = ortho_tmat(c, c->d_smat, c->d_tmat, S, mixed, 0, mixed ? 2e-6 : 1e-15,
+                         mixed ? 20 : 10, nullptr, nullptr, ortho_check)))
+      return rc;
+    const int nb = c->nblk_ke;
+    stp::k_psiv_save<<<nb, 256, 0, c->stream>>>(c->d_dyn_flags,
+                                                 reinterpret_cast<const double2*>(psi),
+                                                 reinterpret_cast<double2*>(c->d_force), ncoef);
+    CPSTEP_LAUNCH_CHECK();
+    if ((rc = pc_backmul_launch(c, c->d_tmat, S, c->d_psi_no, K, psi, K, S, S, K, 1.0, 0.0)))
+      return rc;
+    stp::k_psiv_apply<<<nb, 256, 0, c->stream>>>(
+        c->d_dyn_flags, reinterpret_cast<const double2*>(psi),
+        reinterpret_cast<const double2*>(c->d_force), reinterpret_cast<double2*>(c->d_psi_no),
+        reinterpret_cast<double2*>(vpsi), c->d_tmat, S, ncoef, 1.0 / dt);
+    CPSTEP_LAUNCH_CHECK();
+  }
   mark(7);
   if (c->profile) c->prof_pending += 1;
   return CPSTEP_OK;

@@ -6,8 +6,10 @@ TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).
   coefficients with Gx=0 rows scaled by 1/sqrt(2): ckPairCalculator.C:682-751
   (alpha = 2 for double pack), scaling CP_State_GSpacePlane.C:3120-3123.
   Equivalent: S_ij = sum_p wpt_p Re(conj psi_i(p) psi_j(p)), wpt = 1 on Gx=0.
-* lambda (asymmetric PC) = 2 * psi_r^T F_r with psi scaled by 1/sqrt(2) and F
-  by sqrt(2) on Gx=0 (CP_State_GSpacePlane.C:1933-1954): the same weights.
+* lambda (asymmetric PC) = psi_r^T F_r: that PairCalculator runs without the
+  double-pack factor (cpaimd.C:2527, alpha = 1), and the 1/sqrt(2) scaling of
+  psi and sqrt(2) scaling of F on Gx=0 (CP_State_GSpacePlane.C:1933-1954)
+  cancel: lambda_ji = sum_p Re(conj psi_j(p) F_i(p)) with no weights.
 * Schulz iteration: CPORTHOG::get_iter_Tmat (cp_lowdin.C:180-265) and its
   distributed twin Ortho::do_iteration/step_2/step_3/tolerance_check
   (ortho.C:862-985): A = I, B = S/2; C = 3I - A B; B <- B C / 2; A <- C A / 2;

@@ -1,16 +1,45 @@
-"""Oracle: one CP electronic step in FP64 (the composition the GPU step runs).
+"""Oracle: one CP electronic step in FP64.
 
 TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).
 
+Forces on the orthonormal coefficients psi_o (the same for both forms):
   rho (fftpath.density) -> V_KS = v_xc + Hartree/local (density.py)
   F = addForces(-2/N FFT^-1[V psi]) - kinetic term          (fftpath.py)
-  lambda(i,j) = sum_p Re(conj psi_i F_j);  F_i <- F_i - wpt/2 sum_j psi_j lambda(j,i)
-      (the orthonormality constraint: with S = 2 I it removes <psi_j|F_i>)
-  velocity Verlet of CP_integrate_dyn / cp_evolve_vel / get_fictKE
-      (cp_integrate/cp_dynamics.C:29-258) without the thermostat, Gx=0 and
-      G=0 conventions of :165-200, redundant-half sync of
-      CP_State_GSpacePlane.C:2862-3061
-  S = pc_overlap(psi, psi); T = Schulz (S/2)^-1/2 (ortho.py); psi <- psi T
+  lambda(j,i) = sum_p Re(conj psi_j F_i): the asymmetric PairCalculator,
+      which runs without the double-pack factor (cpaimd.C:2527
+      isDoublePackOn = 0 -> alpha = 1 in multiplyForward,
+      ckPairCalculator.C:733-736); the 1/sqrt(2) and sqrt(2) scalings of psi
+      and F on Gx=0 (CP_State_GSpacePlane.C:1933-1954) cancel in the product.
+
+form "ortho_t" -- the reference's CP dynamics (cp_min_opt = 0), the default:
+  gamma = orthoT . lambda                  Ortho::acceptSectionLambda, ortho.C:541-583
+      (orthoT = T of the previous step's Ortho, ortho.C:358-365; the identity
+      after a norb-tolerance reset, ortho.C:545-562)
+  F_c = F . orthoT - W (psi_o . gamma)     bwMultiplyDynOrthoT (-F.T), ckPairCalculator.C:1444-1510,
+                                           and the gamma GEMM of bwMultiplyHelper (:1372-1420);
+                                           the sum negated by unpackLambda (CP_State_GSpacePlane.C:2197-2202)
+                                           and scaled 1/sqrt(2) on Gx=0 by doLambda (:2253-2259),
+                                           so W = 1/2 on Gx=0 and 1 elsewhere
+  the non-orthogonal coefficients psi_no come back (doLambda :2262-2268) and
+  are integrated (integrateModForce, :2582-2854): velocity Verlet of
+  CP_integrate_dyn / cp_evolve_vel / get_fictKE (cp_dynamics.C:29-258),
+  the second half kick skipped after a reset (halfStepEvolve = 0,
+  cp_dynamics.C:58), redundant-half sync (:2862-3061)
+  psi_no is saved (sendPsi :3090-3094); S = overlap(psi_no) (alpha = 2,
+  Gx=0 scaled 1/sqrt(2)); max |S - 2I| >= cp_norb_tol (default 0.003,
+  set_sim_dict.C:1161-1162) fails the check of Ortho::start_calc/maxCheck
+  (ortho.C:255-262, :461-483, array_diag_max ortho.h:282-310): fatal on the
+  first step, otherwise the finite-difference PsiV reset after the new psi
+  (finiteDifferencePsiV, CP_State_GSpacePlane.C:3707-3770, order 0 as the
+  default norb_fin_diff_order, set_sim_dict.C:1244-1247): psi_no <- psi_o(t+dt),
+  v = (psi_o(t+dt) - psi_o(t)) / dt, orthoT <- I, next integrate without
+  the second half kick
+  T = Schulz (S/2)^-1/2 (ortho.py); psi_o = psi_no T  (bwMultiplyHelper 'N','N', :1314)
+
+form "lowdin" -- the projection form kept as an option:
+  F_i <- F_i - W sum_j psi_j lambda(j,i) (the constraint of minimisation,
+  CP_State_GSpacePlane.C:2079-2088), Verlet on psi_o itself, S, T, psi <- psi T.
+  At T = I both forms give the same first step.
 """
 import math
 
@@ -79,6 +108,28 @@ def constrain(F, psi, lay):
     return F - 0.5 * w[None] * (lam.T @ psi), lam
 
 
+def constrain_dyn(F, psi_o, T, lay):
+    """The reference's dynamics constraint: gamma = T lambda and
+    F_c = F.T - W (psi_o.gamma), states as rows: F_c[a] = sum_k T[k,a] F[k]
+    - W sum_b gamma[b,a] psi_o[b].  Returns (F_c, lambda, gamma)."""
+    lam = OO.real_view(psi_o) @ OO.real_view(F).T        # lam[j, i] = <psi_j|F_i>
+    gam = T @ lam
+    w = np.where(lay.kx == 0, 0.5, 1.0)
+    return T.T @ F - w[None] * (gam.T @ psi_o), lam, gam
+
+
+def norb_deviation(S):
+    """max |S - 2I| over all elements (array_diag_max with diag = 2, spin-unpolarised)."""
+    return float(np.max(np.abs(S - 2.0 * np.eye(S.shape[0]))))
+
+
+def dyn_start(psi):
+    """State of the reference form before its first step: the non-orthogonal
+    coefficients are the given (orthonormal) ones and orthoT is the identity."""
+    return dict(psi_no=np.array(psi, dtype=np.complex128), T=np.eye(psi.shape[0]),
+                half_reset=False, resets=0, dev=0.0)
+
+
 def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None, xc="pz_lda",
            nonlocal_sf=False):
     """Energies, V_KS, constrained-force input F and atom forces (local + Ewald,
@@ -116,21 +167,51 @@ def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None, xc=
 
 
 def cp_step(psi, v, occ, sysm, lay, dlay, cmass, dt, iteration, nonlocal_on=False, nkf=None,
-            xc="pz_lda", nonlocal_sf=False, nhc=None):
-    """nhc = (params, per-state chain states, nres, nyosh) of oracle/isokin.py
-    runs the thermostatted integrator (the chain states are updated)."""
+            xc="pz_lda", nonlocal_sf=False, nhc=None, form="ortho_t", dyn=None, tol_norb=0.003):
+    """One step on the orthonormal coefficients psi.  nhc = (params, per-state
+    chain states, nres, nyosh) of oracle/isokin.py runs the thermostatted
+    integrator (the chain states are updated).  form "ortho_t" carries the
+    reference's dynamical state in ``dyn`` (dyn_start(psi) on iteration 1 when
+    None; the updated dict is aux["dyn"]); form "lowdin" needs none.
+    Returns (psi, v, energies, atom forces, aux)."""
     en, F, floc, rho, vks = forces(psi, occ, sysm, lay, dlay, nonlocal_on=nonlocal_on, nkf=nkf,
                                    xc=xc, nonlocal_sf=nonlocal_sf)
-    Fc, lam = constrain(F, psi, lay)
+    if form == "lowdin":
+        Fc, lam = constrain(F, psi, lay)
+        x, it_eff, gam = psi, iteration, None
+    elif form == "ortho_t":
+        if dyn is None:
+            if iteration != 1:
+                raise ValueError("form ortho_t: iteration > 1 needs the state of the last step")
+            dyn = dyn_start(psi)
+        Fc, lam, gam = constrain_dyn(F, psi, dyn["T"], lay)
+        x = dyn["psi_no"]
+        it_eff = 1 if dyn["half_reset"] else iteration
+    else:
+        raise ValueError("form must be ortho_t or lowdin")
     if nhc is None:
-        psi2, v2, ke = integrate(Fc, psi, v, cmass, lay, dt, iteration)
+        psi2, v2, ke = integrate(Fc, x, v, cmass, lay, dt, it_eff)
     else:
         from . import isokin as OK
         cls, ridx, rsrc = point_classes(lay)
         psi2, v2, ke, en["NHC_KE"], en["NHC_POT"] = OK.integrate_nhc(
-            Fc, psi, v, cmass, cls, ridx, rsrc, nhc[0], nhc[1], dt, iteration, nhc[2], nhc[3])
+            Fc, x, v, cmass, cls, ridx, rsrc, nhc[0], nhc[1], dt, it_eff, nhc[2], nhc[3])
     en["FICT"] = ke
     S = OO.pc_overlap(psi2, psi2, lay.kx)
+    aux = dict(S=S, lam=lam, gamma=gam)
+    if form == "ortho_t":
+        dev = norb_deviation(S)
+        fail = dev >= tol_norb
+        if fail and iteration == 1:
+            raise RuntimeError("S fails the norb tolerance on the first step: max|S-2I| = %g" % dev)
     T, it, _ = OO.schulz_tmat(S)
     psi3 = OO.back_multiply(psi2, T)
-    return psi3, v2, en, floc, dict(S=S, T=T, lam=lam, iters=it)
+    aux.update(T=T, iters=it)
+    if form == "ortho_t":
+        nd = dict(psi_no=psi2, T=T, half_reset=False, resets=dyn["resets"], dev=dev)
+        if fail:   # finiteDifferencePsiV, order 0
+            v2 = (psi3 - psi) / dt
+            nd.update(psi_no=psi3.copy(), T=np.eye(S.shape[0]), half_reset=True,
+                      resets=dyn["resets"] + 1)
+        aux["dyn"] = nd
+    return psi3, v2, en, floc, aux

@@ -8,6 +8,10 @@ from conftest import cuda_ok
 
 pytestmark = pytest.mark.gpu
 
+# small enough that the first step passes the default cp_norb_tol (0.003) of the
+# orthoT constraint on these random states; later steps may take the PsiV reset
+DT = 1.0
+
 SYSTEMS = [  # (box, ecut, states, atoms, grid)
     (9.0, 20.0, 6, {"O": 1, "H": 2}, 28),
     (9.0, 30.0, 12, {"O": 2, "H": 4}, 32),
@@ -48,7 +52,7 @@ def test_batch_graph_matches_single_contexts(precision):
         caps = []
         n0 = _lib.lib().cpstep_launch_count()
         for it in range(1, 6):
-            batch.step([d["psi"] for d in a], [d["v"] for d in a], [d["occ"] for d in a], 5.0,
+            batch.step([d["psi"] for d in a], [d["v"] for d in a], [d["occ"] for d in a], DT,
                        it, [d["e"] for d in a], [d["f"] for d in a])
             caps.append(batch.status()[1])
         torch.cuda.synchronize()
@@ -56,7 +60,7 @@ def test_batch_graph_matches_single_contexts(precision):
         n0 = _lib.lib().cpstep_launch_count()
         for it in range(1, 6):
             for d in b:
-                d["ctx"].cp_step(d["psi"], d["v"], d["occ"], 5.0, it, d["e"], d["f"])
+                d["ctx"].cp_step(d["psi"], d["v"], d["occ"], DT, it, d["e"], d["f"])
         torch.cuda.synchronize()
         ns = _lib.lib().cpstep_launch_count() - n0
         assert caps == [False, False, True, True, True]
@@ -68,7 +72,7 @@ def test_batch_graph_matches_single_contexts(precision):
             assert ok
         # a context's setter forces a new capture
         a[1]["ctx"].set_cp_mass(25.0, 30.0)
-        batch.step([d["psi"] for d in a], [d["v"] for d in a], [d["occ"] for d in a], 5.0, 6,
+        batch.step([d["psi"] for d in a], [d["v"] for d in a], [d["occ"] for d in a], DT, 6,
                    [d["e"] for d in a], [d["f"] for d in a])
         assert not batch.status()[1]
         torch.cuda.synchronize()

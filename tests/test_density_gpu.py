@@ -155,6 +155,7 @@ def test_step_runs_at_200(big, precision):
         ctx.set_atoms(s)
         ctx.set_nonlocal(s)
         ctx.set_cp_mass(25.0, 70.0)
+        ctx.set_constraint("ortho_t", 1.0)  # cp_norb_tol above this step's deviation
         psi = s.psi()
         v = torch.zeros_like(psi)
         e, f = ctx.cp_step(psi, v, big["occ"], 5.0, 1)

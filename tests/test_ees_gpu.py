@@ -110,7 +110,7 @@ def nlstep(nlsys):
     pn = nlsys["psi"].cpu().numpy()
     occ = nlsys["occ"].cpu().numpy()
     p1, v1, en1, f1, _ = OS.cp_step(pn, np.zeros_like(pn), occ, s, lay, dlay, cmass, DT, 1,
-                                    nonlocal_on=True, nkf=nlsys["nkf"])
+                                    nonlocal_on=True, nkf=nlsys["nkf"], tol_norb=1.0)
     return (p1, v1, en1, f1)
 
 
@@ -123,6 +123,7 @@ def _step(nlsys, precision):
         ctx.set_atoms(s)
         ctx.set_nonlocal(s)
         ctx.set_cp_mass(25.0, 30.0)
+        ctx.set_constraint("ortho_t", 1.0)  # cp_norb_tol above this step's deviation
         psi = nlsys["psi"].clone()
         v = torch.zeros_like(psi)
         e, f = ctx.cp_step(psi, v, nlsys["occ"], DT, 1)

@@ -102,7 +102,13 @@ def test_thermostat_off_restores_plain_verlet(lay):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_thermostatted_steps_match_oracle(precision):
+@pytest.mark.parametrize("reset", [False, True])
+def test_thermostatted_steps_match_oracle(precision, reset):
+    """Three thermostatted steps of the orthoT form against the oracle; with
+    reset, cp_norb_tol sits just above the first step's deviation so the
+    later steps take the PsiV reset (no second half kick and no NHC update
+    of that half after it)."""
+    import copy
     if not cuda_ok():
         pytest.skip("no CUDA device")
     import torch
@@ -121,19 +127,28 @@ def test_thermostatted_steps_match_oracle(precision):
     cmass = OS.cp_mass(lay, 25.0, 30.0)
     psi = sysm.psi()
     occ = torch.ones(sysm.nstates, dtype=torch.float64, device="cuda")
+    pn = psi.cpu().numpy()
+    vn = np.zeros_like(pn)
+    tol = 1.0
+    if reset:  # probe the first step's max |S - 2I|
+        _, _, _, _, aux = OS.cp_step(pn, vn, np.ones(sysm.nstates), sysm, lay, dlay, cmass, DT,
+                                     1, nhc=(p, copy.deepcopy(states), 4, 9), tol_norb=1.0)
+        tol = 1.5 * aux["dyn"]["dev"]
     ctx = StepContext(sysm.layout, sysm.nstates, precision=precision)
     try:
         ctx.set_atoms(sysm)
         ctx.set_cp_mass(25.0, 30.0)
         ctx.set_cp_thermostat(300.0)
+        ctx.set_constraint("ortho_t", tol)
         ctx.cp_thermostat_state(_pack(states, "x"), _pack(states, "xp"), _pack(states, "vn"))
-        pn = psi.cpu().numpy()
-        vn = np.zeros_like(pn)
         dpsi, dv = psi.clone(), torch.zeros_like(psi)
+        dyn = None
         for it in (1, 2, 3):
             e, _ = ctx.cp_step(dpsi, dv, occ, DT, it)
-            pn, vn, er, _, _ = OS.cp_step(pn, vn, np.ones(sysm.nstates), sysm, lay, dlay, cmass,
-                                          DT, it, nhc=(p, states, 4, 9))
+            pn, vn, er, _, aux = OS.cp_step(pn, vn, np.ones(sysm.nstates), sysm, lay, dlay, cmass,
+                                            DT, it, nhc=(p, states, 4, 9), tol_norb=tol, dyn=dyn)
+            dyn = aux["dyn"]
+            assert ctx.dyn_status()[1] == dyn["resets"]
             e = e.cpu().numpy()
             if precision == "fp64":
                 for name, slot in (("ETOT", 8), ("FICT", 9), ("NHC_KE", 12), ("NHC_POT", 13)):

@@ -79,7 +79,7 @@ def sfstep():
     cmass = OS.cp_mass(lay, 25.0, 30.0)
     pn = psi.cpu().numpy()
     p1, v1, en1, f1, _ = OS.cp_step(pn, np.zeros_like(pn), np.ones(sysm.nstates), sysm, lay,
-                                    dlay, cmass, DT, 1, nonlocal_sf=True)
+                                    dlay, cmass, DT, 1, nonlocal_sf=True, tol_norb=1.0)
     return dict(sys=sysm, psi=psi, occ=occ, ref=(p1, v1, en1, f1))
 
 
@@ -93,6 +93,7 @@ def test_step_with_sf_nonlocal_matches_oracle(sfstep, precision):
         ctx.set_atoms(s)
         ctx.set_nonlocal_sf(s)
         ctx.set_cp_mass(25.0, 30.0)
+        ctx.set_constraint("ortho_t", 1.0)  # cp_norb_tol above this step's deviation
         psi = sfstep["psi"].clone()
         v = torch.zeros_like(psi)
         e, f = ctx.cp_step(psi, v, sfstep["occ"], DT, 1)

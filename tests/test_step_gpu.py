@@ -1,5 +1,8 @@
 """The fused CP electronic step on the GPU vs the FP64 oracle step.
 
+Two steps of each constraint form: the reference's orthoT form (with
+cp_norb_tol above the deviations these steps reach, so no PsiV reset: the
+reset path is tested in test_dyn_gpu.py) and the Loewdin projection form.
 FP64 path: energies to 1e-10 relative, coefficients to 1e-9.
 Mixed path vs the FP64 oracle: energy per atom <= 1e-6 Ha, local atom force
 <= 1e-5 Ha/bohr, |psi^T psi - 2I| <= 1e-10 (FP64 Ortho correction).
@@ -12,6 +15,8 @@ from conftest import cuda_ok
 pytestmark = pytest.mark.gpu
 
 DT = 5.0
+TOL = 1.0    # cp_norb_tol: no reset in these two steps
+FORMS = ("ortho_t", "lowdin")
 
 
 @pytest.fixture(scope="module")
@@ -31,16 +36,22 @@ def stepsys():
     cmass = OS.cp_mass(lay, 25.0, 30.0)
     pn = psi.cpu().numpy()
     v0 = np.zeros_like(pn)
-    p1, v1, en1, f1, aux1 = OS.cp_step(pn, v0, np.ones(sysm.nstates), sysm, lay, dlay, cmass, DT, 1)
-    p2, v2, en2, f2, aux2 = OS.cp_step(p1, v1, np.ones(sysm.nstates), sysm, lay, dlay, cmass, DT, 2)
-    return dict(sys=sysm, psi=psi, occ=occ, ref=[(p1, v1, en1, f1), (p2, v2, en2, f2)])
+    ref = {}
+    for form in FORMS:
+        p1, v1, en1, f1, aux1 = OS.cp_step(pn, v0, np.ones(sysm.nstates), sysm, lay, dlay, cmass,
+                                           DT, 1, form=form, tol_norb=TOL)
+        p2, v2, en2, f2, aux2 = OS.cp_step(p1, v1, np.ones(sysm.nstates), sysm, lay, dlay, cmass,
+                                           DT, 2, form=form, tol_norb=TOL, dyn=aux1.get("dyn"))
+        ref[form] = [(p1, v1, en1, f1), (p2, v2, en2, f2)]
+    return dict(sys=sysm, psi=psi, occ=occ, ref=ref)
 
 
-def run(stepsys, precision, tensor_cores=True):
+def run(stepsys, precision, tensor_cores=True, form="ortho_t"):
     import torch
     from openatom_b200.context import StepContext
     s = stepsys["sys"]
     ctx = StepContext(s.layout, s.nstates, precision=precision)
+    ctx.set_constraint(form, TOL)
     if precision == "mixed" and not tensor_cores:
         ctx.set_gemm_path(False)
     ctx.set_atoms(s)
@@ -60,9 +71,10 @@ def run(stepsys, precision, tensor_cores=True):
 NAMES = [("EXC", 0), ("EHART", 2), ("EEXT", 3), ("EKE", 6), ("ETOT", 8), ("FICT", 9)]
 
 
-def test_fp64_step_matches_oracle(stepsys):
-    out = run(stepsys, "fp64")
-    for (p, v, e, f, ok), (pr, vr, er, fr) in zip(out, stepsys["ref"]):
+@pytest.mark.parametrize("form", FORMS)
+def test_fp64_step_matches_oracle(stepsys, form):
+    out = run(stepsys, "fp64", form=form)
+    for (p, v, e, f, ok), (pr, vr, er, fr) in zip(out, stepsys["ref"][form]):
         assert ok
         for name, slot in NAMES:
             assert abs(e[slot] - er[name]) <= 1e-10 * max(1.0, abs(er[name])), name
@@ -71,12 +83,13 @@ def test_fp64_step_matches_oracle(stepsys):
         assert np.max(np.abs(f - fr)) < 1e-9 * max(1.0, np.max(np.abs(fr)))
 
 
-def test_mixed_step_within_budget(stepsys):
+@pytest.mark.parametrize("form", FORMS)
+def test_mixed_step_within_budget(stepsys, form):
     from oracle import ortho as OO
-    out = run(stepsys, "mixed")
+    out = run(stepsys, "mixed", form=form)
     natm = stepsys["sys"].natm
     lay = stepsys["sys"].layout
-    for (p, v, e, f, ok), (pr, vr, er, fr) in zip(out, stepsys["ref"]):
+    for (p, v, e, f, ok), (pr, vr, er, fr) in zip(out, stepsys["ref"][form]):
         assert ok
         assert abs(e[8] - er["ETOT"]) / natm <= 1e-6
         assert np.max(np.abs(f - fr)) <= 1e-5
@@ -92,7 +105,7 @@ def test_mixed_step_fp64_products_orthonormal_to_fp64(stepsys):
     from oracle import ortho as OO
     out = run(stepsys, "mixed", tensor_cores=False)
     lay = stepsys["sys"].layout
-    for (p, v, e, f, ok), _ in zip(out, stepsys["ref"]):
+    for (p, v, e, f, ok), _ in zip(out, stepsys["ref"]["ortho_t"]):
         assert ok
         S = OO.pc_overlap(p, p, lay.kx)
         assert np.max(np.abs(S - 2.0 * np.eye(S.shape[0]))) < 1e-10

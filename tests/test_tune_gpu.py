@@ -18,6 +18,7 @@ def _setup(precision):
     ctx.set_atoms(sysm)
     ctx.set_nonlocal(sysm)
     ctx.set_cp_mass(25.0, 30.0)
+    ctx.set_constraint("ortho_t", 1.0)  # cp_norb_tol above this step's deviation
     occ = torch.ones(sysm.nstates, dtype=torch.float64, device="cuda")
     return sysm, ctx, occ
 
