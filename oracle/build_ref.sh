@@ -17,6 +17,12 @@
 #                         initCPNHC, cp_isoNHC_update, CP_integrate_dyn
 #   src_piny_physics_v1.0/classical_physics/integrate/integration_drivers.C
 #                         integrate_nvt_2nd_half / _1st_half (massive atom NHC)
+#   src_piny_physics_v1.0/abinito_physics/cp_nonlocal/cp_eke.C   CP_eke_calc
+#   src_piny_physics_v1.0/abinito_physics/cp_local/cp_hart_ext.C CP_hart_eext_calc
+#   src_charm_driver/fft_slab_ctrl/fftCache.C   FFTcache::expandGSpace, packGSpace:
+#       the rest of that file needs Charm++, so the two member functions are
+#       cut from it (sed, by their first and last lines) into _ref/fftcache_pack.C
+#       behind the class stand-in ref_shim/fftcache_shim.h
 # The shims in oracle/ref_shim stand in for the Charm++/PINY headers, and
 # oracle/ref_mathlib.c for the Fortran GENMATMUL.  Test infrastructure only.
 set -e
@@ -46,9 +52,21 @@ for f in "$PINY/abinito_physics/cp_nonlocal/cp_ees_nonlocal.C" \
          "$PINY/abinito_physics/cp_ions/cp_rspace_ion.C" "$HERE/ref_ion.cpp" \
          "$PINY/abinito_physics/cp_integrate/cp_isokin.C" \
          "$PINY/abinito_physics/cp_integrate/cp_dynamics.C" "$HERE/ref_isokin.cpp" \
-         "$PINY/classical_physics/integrate/integration_drivers.C" "$HERE/ref_atomnhc.cpp"; do
+         "$PINY/classical_physics/integrate/integration_drivers.C" "$HERE/ref_atomnhc.cpp" \
+         "$PINY/abinito_physics/cp_nonlocal/cp_eke.C" \
+         "$PINY/abinito_physics/cp_local/cp_hart_ext.C" "$HERE/ref_local.cpp"; do
   g++ $EESFLAGS -c "$f" -o "$OUT/$(basename "$f" | sed 's/\.[Cc]p*$//').o"
 done
+{
+  echo '#include "fftcache_shim.h"'
+  sed -n '/^void FFTcache::expandGSpace/,/^}\/\/end routine/p' \
+    "$REF/src_charm_driver/fft_slab_ctrl/fftCache.C"
+  sed -n '/^void FFTcache::packGSpace/,/^}\/\/end routine/p' \
+    "$REF/src_charm_driver/fft_slab_ctrl/fftCache.C"
+} > "$OUT/fftcache_pack.C"
+g++ -O2 -fPIC -w -include "$HERE/ref_shim/ees_shim.h" -I "$HERE/ref_shim" -I "$REF/include" \
+  -c "$OUT/fftcache_pack.C" \
+  -o "$OUT/fftcache_pack.o"
 g++ -O2 -fPIC -shared -w -o "$OUT/libref.so" \
   -I "$HERE/ref_shim" -I "$HERE/ref_shim/sub" -I "$REF" \
   -I "$REF/src_charm_driver/utility" -I "$REF/src_piny_physics_v1.0/include/class_defs" \
@@ -61,5 +79,6 @@ g++ -O2 -fPIC -shared -w -o "$OUT/libref.so" \
   "$OUT/cp_struct_fact.o" "$OUT/cp_nlmat.o" "$OUT/cp_nl_energy_forc.o" "$OUT/ref_sf.o" \
   "$OUT/cp_rspace_ion.o" "$OUT/ref_ion.o" \
   "$OUT/cp_isokin.o" "$OUT/cp_dynamics.o" "$OUT/ref_isokin.o" \
-  "$OUT/integration_drivers.o" "$OUT/ref_atomnhc.o"
+  "$OUT/integration_drivers.o" "$OUT/ref_atomnhc.o" \
+  "$OUT/cp_eke.o" "$OUT/cp_hart_ext.o" "$OUT/ref_local.o" "$OUT/fftcache_pack.o"
 echo "$OUT/libref.so"

@@ -32,7 +32,10 @@ class CkCallback {};
       exit(1);                                                        \
     }                                                                 \
   } while (0)
+/* the Charm-FFT library's point record (external, not in the tree): kz, ky,
+ * kx of a density-sphere point and its offset in the caller's array */
 struct gridPoint {
   int d1, d2, d3;
+  int offset;
 };
 double getdeth(double*);

@@ -89,6 +89,27 @@ def test_slater_part_matches_reference(ref):
     assert abs(e - exc[0]) < 1e-13 * abs(exc[0]) and abs(mu - muxc[0]) < 1e-13 * abs(muxc[0])
 
 
+@pytest.mark.parametrize("shape", [(5, 6, 7), (8, 8, 8)])
+def test_pz_lda_matches_reference(ref, shape):
+    """The benchmark's functional: CP_exc_calc with cp_lyp = 0 (Perdew-Zunger
+    correlation on both sides of rs = 1, Slater exchange) against the oracle's
+    pz_lda, densities from 1e-12 (rs ~ 6e3) to 2 (rs ~ 0.5).  At exactly zero
+    density the reference's potential is NaN (rs = inf) where the oracle and
+    the GPU put 0; a density of occupied states is positive everywhere."""
+    from oracle import density as OD
+    nf3, nf2, nf1 = shape
+    rho, _ = _grid_density(shape, 7)
+    rho.flat[0] = 1e-12
+    vol = 91.0
+    v, e, mu = OD.pz_lda(rho, vol)
+    rv = np.zeros(shape)
+    exc, muxc = np.zeros(1), np.zeros(1)
+    ref.ref_exc_calc(nf1, nf2, nf3, vol, 0, _p(np.ascontiguousarray(rho)), _p(rv), _p(exc),
+                     _p(muxc))
+    assert np.allclose(np.asarray(v).reshape(shape), rv, rtol=1e-13, atol=0.0)
+    assert abs(e - exc[0]) < 1e-13 * abs(exc[0]) and abs(mu - muxc[0]) < 1e-13 * abs(muxc[0])
+
+
 @pytest.fixture(scope="module")
 def dens():
     """A positive density band-limited inside the density sphere of a small box."""
