@@ -9,11 +9,12 @@ Our arm prints one JSON line: value = mixed-precision steps/s (whole job, all
 ranks; ranks are independent replicas), the FP64 path's steps/s beside it,
 e2e through the C-ABI host-buffer call (positions in, energies and atom forces
 out every step), the roofline of the state FFT / density / V.psi kernels, the
-CPU baseline (the FP64 oracle on the host cores, bounded sample), clocks and
-the number of library kernel launches in the timed region.
-The reference arm (--impl reference) times the FP64 CPU oracle of the same
-step on the host cores (the reference itself cannot be built here: no
-Charm++, FFTW-2, BLAS or Fortran in the image).
+CPU baseline (two whole FP64 oracle steps on the host cores), clocks and the
+number of library kernel launches in the timed region.
+The reference arm (--impl reference) times whole steps of the FP64 CPU oracle
+of the same system on the host cores (the reference itself cannot be built
+here: no Charm++, FFTW-2, BLAS or Fortran in the image); it builds its inputs
+with the oracle alone and loads nothing of the product.
 """
 import argparse
 import json
@@ -245,6 +246,9 @@ def run_ours(args, cfg, name, rank, ws, dist):
         e1.record()
         torch.cuda.synchronize()
         launches = L.cpstep_launch_count() - n0
+        # the same number of steps from the same input in both precisions
+        last = (energies.cpu().numpy().copy(), forces.cpu().numpy().copy(),
+                1 + args.warmup + args.steps, ctx.dyn_status()[1])
         clocks = clk.stop() if prec == "mixed" else None
         ms = e0.elapsed_time(e1)
         ms = max_over_ranks(ms, dist)
@@ -265,7 +269,7 @@ def run_ours(args, cfg, name, rank, ws, dist):
         it2, ok2 = ctx.step_status()
         norb_dev, resets = ctx.dyn_status()
         out[prec] = dict(ms=ms, launches=launches, clocks=clocks, phase=phase, first=first,
-                         ortho_ok=ok2, ortho_iters=it2, graph=graph,
+                         ortho_ok=ok2, ortho_iters=it2, graph=graph, last=last,
                          psiv_resets=resets, norb_dev_last=norb_dev)
         if prec == "mixed":
             # e2e: the reference-facing host-buffer call (positions in, energies/forces out)
@@ -333,64 +337,57 @@ def pc_kernel_times(ctx, psi, f, reps=5):
     return res
 
 
-def cpu_baseline(cfg, sample_states=4):
-    """FP64 oracle step time on the host cores, bounded sample, extrapolated.
-
-    FFT/density/V.psi cost is linear in the states (timed on `sample_states`);
-    the density side once; the four PairCalc products and the Ortho iteration
-    at full size (numpy BLAS)."""
+def oracle_system(cfg, tol_norb):
+    """The benchmark system for the FP64 oracle, built by the oracle alone
+    (oracle/synth.py: the product package is not imported and its library is
+    not loaded), with the GPU arm's settings: EES non-local (s + p, B-spline
+    order 8), the isokinetic NHC of the coefficients (1000 K, 2 chains, nres 4,
+    nyosh 9, chains on the isokinetic surface), the orthoT constraint."""
     import numpy as np
     from oracle import density as OD
-    from oracle import ees as OE
     from oracle import fftpath as OF
-    from oracle import layout as OL
-    from oracle import ortho as OO
-    from openatom_b200.system import System
+    from oracle import isokin as OK
+    from oracle import step as OS
+    from oracle import synth as OSY
     OF.set_workers(os.cpu_count() or 1)
-    sysm = System(cfg["box"], cfg["ecut"], cfg["nstates"], cfg["atoms"], nfft=cfg["grid"])
-    lay = OL.Layout(cfg["box"], cfg["ecut"], grid=cfg["grid"])
-    dlay = OD.density_layout(cfg["box"], cfg["ecut"], cfg["grid"])
-    rng = np.random.default_rng(0)
-    S = cfg["nstates"]
-    sub = (rng.standard_normal((sample_states, lay.npts)) + 1j * rng.standard_normal((sample_states, lay.npts))) * 1e-2
-    vol = cfg["box"] ** 3
-    occ = np.ones(sample_states)
-    t0 = time.perf_counter()
-    rho = OF.density(sub, lay, occ, vol, chunk=sample_states)
-    vks = rho * 0.1
-    fv = OF.vpsi_force(sub, vks, lay, occ, chunk=sample_states)
-    OE.nonlocal_ees(sub, lay, occ, vol, sysm.hmati(), dict(pos=sysm.pos, typ=sysm.typ),
-                    sysm.channels, sysm.tab)
-    t_fft = (time.perf_counter() - t0) / sample_states
-    t0 = time.perf_counter()
-    vxc, exc, mu = OD.pz_lda(np.abs(rho) + 1e-8, vol)
-    rg = OD.rho_to_g(rho, dlay, vol)
-    natm_s = min(16, sysm.natm)
-    a = sysm.atoms_dict()
-    a_s = dict(pos=a["pos"][:natm_s], typ=a["typ"][:natm_s], q=a["q"])
-    OD.hart_eext(rg, dlay.kx, dlay.ky, dlay.kz, cfg["box"], 0.5 * cfg["ecut"], a_s, sysm.tab,
-                 sysm.alp_ewd)
-    t_dens = (time.perf_counter() - t0)
-    t_dens *= 1.0  # the atom loop part is extrapolated below
-    t_atom = t_dens * (sysm.natm / natm_s - 1.0) * 0.5
-    K = 2 * lay.npts
-    A = rng.standard_normal((S, K))
-    t0 = time.perf_counter()
-    C = A @ A.T
-    A2 = C.T @ A
-    t_gemm = (time.perf_counter() - t0) / 2.0
-    Sm = np.eye(S) * 2.0 + 1e-3 * (C / np.max(np.abs(C)))
-    Sm = 0.5 * (Sm + Sm.T)
-    t0 = time.perf_counter()
-    OO.schulz_tmat(Sm, tol=1e-15, max_iter=10)
-    t_ortho = time.perf_counter() - t0
-    t_step = t_fft * S + t_dens + t_atom + 4 * t_gemm + t_ortho
-    sample = ("%d of %d states through the FFT/density/V.psi/EES non-local path, the density side with %d of %d "
-              "atoms (atom loop extrapolated), full-size PairCalc products and Ortho; "
-              "per-step time = sum, extrapolated linearly in states/atoms"
-              % (sample_states, S, natm_s, sysm.natm))
-    del A2
-    return t_step, sample
+    sysm = OSY.System(cfg["box"], cfg["ecut"], cfg["nstates"], cfg["atoms"], nfft=cfg["grid"])
+    lay = sysm.layout
+    cls, _, _ = OS.point_classes(lay)
+    p = OK.init_nhc(int(np.sum(cls != 0)), 1, 2, 1, CP_FICT_KE, TAU_FS)
+    psi = sysm.psi()
+    return dict(sys=sysm, lay=lay, dlay=OD.density_layout(cfg["box"], cfg["ecut"], cfg["grid"]),
+                cmass=OS.cp_mass(lay, TAU_FS, cfg["ecut"]),
+                nhc=(p, [OK.default_state(p) for _ in range(sysm.nstates)], 4, 9),
+                psi=psi, v=np.zeros_like(psi), dyn=None, occ=np.ones(sysm.nstates),
+                tol=tol_norb, it=1)
+
+
+def oracle_steps(st, n):
+    """n whole FP64 oracle steps of the system st (density, V_KS, V.psi, EES,
+    lambda, the constraint, the thermostatted Verlet, S, T, psi.T); returns
+    the wall seconds of each."""
+    from oracle import step as OS
+    times = []
+    for _ in range(n):
+        t0 = time.perf_counter()
+        st["psi"], st["v"], _, _, aux = OS.cp_step(
+            st["psi"], st["v"], st["occ"], st["sys"], st["lay"], st["dlay"], st["cmass"], DT,
+            st["it"], nonlocal_on=True, nhc=st["nhc"], tol_norb=st["tol"], dyn=st["dyn"])
+        times.append(time.perf_counter() - t0)
+        st["dyn"] = aux["dyn"]
+        st["it"] += 1
+    return times
+
+
+def cpu_baseline(cfg, tol_norb):
+    """Whole FP64 oracle steps on the host cores: one untimed step, then the
+    mean of two (about 10-30 s of CPU work)."""
+    st = oracle_system(cfg, tol_norb)
+    oracle_steps(st, 1)
+    t = oracle_steps(st, 2)
+    sample = ("2 whole FP64 oracle steps (iterations 2-3, after 1 untimed) of the same system: "
+              "numpy/scipy pocketfft, state chunks on %d host threads" % (os.cpu_count() or 1))
+    return sum(t) / len(t), sample
 
 
 def pc_roofline(us, sysm, hbm, pk, gflops, gemm_ms):
@@ -501,7 +498,12 @@ def batch16_systems(seed=4):
     return out
 
 
-def run_batch16(args):
+def batch16_measure(args):
+    """Config 4: 16 independent systems (seeded states in [16, 256], grids from
+    {32, 48, 64, 96}, 30-70 Ry), mixed precision, stepped as one batch graph,
+    against looping the single-system path over them in the plain FP64 path
+    and in the mixed path, both loops with their own step graphs.  Returns the
+    aggregate system-steps/s of the three."""
     import numpy as np
     import torch
     from openatom_b200 import _lib
@@ -524,6 +526,7 @@ def run_batch16(args):
             ctx.set_nonlocal(sysm)
             ctx.set_cp_mass(TAU_FS, sp["ecut"])
             ctx.set_cp_thermostat(CP_FICT_KE)
+            ctx.set_constraint("ortho_t", args.norb_tol)
             ctx.set_graph(graph)
             psi = sysm.psi()
             out.append(dict(ctx=ctx, psi=psi, v=torch.zeros_like(psi),
@@ -542,7 +545,7 @@ def run_batch16(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    # batched graph, mixed
+    # batched graph, mixed (the contexts' own graphs off: the batch holds one)
     mix = contexts("mixed", False)
     batch = StepBatch([d["ctx"] for d in mix])
     arg = lambda key: [d[key] for d in mix]
@@ -557,37 +560,58 @@ def run_batch16(args):
     batch.close()
     for d in mix:
         d["ctx"].close()
-    # the plain path looped over the systems (direct launches)
-    pl = contexts("fp64", False)
 
-    def loop(k):
-        for d in pl:
-            d["ctx"].cp_step(d["psi"], d["v"], d["occ"], DT, 1 + args.warmup + k, d["e"], d["f"])
+    def looped(prec):
+        """the single-system step looped over the systems, each with its graph"""
+        pl = contexts(prec, True)
 
-    for w in range(args.warmup):
+        def loop(k):
+            for d in pl:
+                d["ctx"].cp_step(d["psi"], d["v"], d["occ"], DT, 1 + args.warmup + k, d["e"],
+                                 d["f"])
+        for w in range(args.warmup):
+            for d in pl:
+                d["ctx"].cp_step(d["psi"], d["v"], d["occ"], DT, 1 + w, d["e"], d["f"])
+        ms = timed(loop, args.steps)
+        graphs = all(d["ctx"].graph_status()[1] for d in pl)
         for d in pl:
-            d["ctx"].cp_step(d["psi"], d["v"], d["occ"], DT, 1 + w, d["e"], d["f"])
-    ms_loop = timed(loop, args.steps)
-    for d in pl:
-        d["ctx"].close()
+            d["ctx"].close()
+        return ms, graphs
+    ms_loop, g64 = looped("fp64")
+    ms_mloop, gmx = looped("mixed")
     nsys = len(specs)
     v_batch = nsys * args.steps / (ms_batch / 1e3)
     v_loop = nsys * args.steps / (ms_loop / 1e3)
-    line = {
+    v_mloop = nsys * args.steps / (ms_mloop / 1e3)
+    return {
         "metric": "aggregate CP steps/sec of 16 independent systems on one GPU",
-        "value": v_batch, "unit": "system-steps/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_batch / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "mixed (as the single-system line)",
-        "data": "synthetic",
-        "config": {"workload": "16 water-like systems, states %s, grids %s" % (
+        "value": v_batch, "unit": "system-steps/s", "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_batch / args.steps,
+        "workload": "16 water-like systems, states %s, grids %s" % (
             [sp["nstates"] for sp in specs], [sp["grid"] for sp in specs]),
-                   "systems": specs, "parallelism": "one batch graph, a branch per system"},
+        "systems": specs, "parallelism": "one batch graph, a branch per system",
         "plain_fp64_loop_value": v_loop, "batched_over_plain_loop": v_batch / v_loop,
+        "mixed_loop_value": v_mloop, "batched_over_mixed_loop": v_batch / v_mloop,
+        "loops_graphed": bool(g64 and gmx),
         "gpu_launches": int(launches), "batch_graph": {"enabled": status[0],
                                                       "captured": status[1],
                                                       "kernels_per_step": status[2]},
         "energies_finite": bool(all(np.isfinite(e).all() for e in e_mix)),
     }
+
+
+def run_batch16(args):
+    r = batch16_measure(args)
+    line = {"metric": r["metric"], "value": r["value"], "unit": r["unit"], "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed (as the single-system line)", "data": "synthetic",
+            "config": {"workload": r["workload"], "systems": r["systems"],
+                       "parallelism": r["parallelism"]}}
+    line.update({k: r[k] for k in ("plain_fp64_loop_value", "batched_over_plain_loop",
+                                   "mixed_loop_value", "batched_over_mixed_loop",
+                                   "loops_graphed", "gpu_launches", "batch_graph",
+                                   "energies_finite")})
     print(json.dumps(line))
 
 
@@ -599,6 +623,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="water192", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch16", action="store_true",
+                    help="leave out the 16-system batch measurement of the main line")
     ap.add_argument("--norb-tol", type=float, default=0.05,
                     help="cp_norb_tol of the orthoT constraint (reference default 0.003; the "
                          "random, unquenched start needs more on its first step)")
@@ -624,33 +650,41 @@ def main():
         args.warmup = 3
     cfg = CONFIGS[args.config]
     wname = workload_name(args.config, cfg)
-    rank, ws, dist = dist_init()
 
     if args.impl == "reference":
-        if rank != 0:
+        # rank 0 alone times the reference's CPU path (the FP64 oracle port);
+        # no process group, no GPU, nothing of the product is loaded
+        if int(os.environ.get("RANK", "0")) != 0:
             return
         ncpu = os.cpu_count() or 1
-        times = []
-        for k in range(args.warmup + args.steps):
-            t, sample = cpu_baseline(cfg)
-            if k >= args.warmup:
-                times.append(t)
+        st = oracle_system(cfg, args.norb_tol)
+        oracle_steps(st, args.warmup)
+        times = oracle_steps(st, args.steps)
         t = statistics.mean(times)
         line = {
             "impl": "reference", "metric": METRIC, "value": 1.0 / t, "unit": "steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": wname, "precision": "FP64 CPU oracle",
-                       "parallelism": "host cores"},
+            "config": {"workload": wname, "precision": "FP64 CPU oracle (the reference's "
+                       "algorithm restated; the reference needs Charm++ and FFTW-2)",
+                       "parallelism": "host cores", "dt_au": DT,
+                       "cp_thermostat": "isokinetic NHC, %g K, 2 chains, nres 4, nyosh 9"
+                       % CP_FICT_KE,
+                       "constraint": "orthoT (the reference's CP dynamics), cp_norb_tol %g"
+                       % args.norb_tol},
+            "step_seconds": times,
             "cpu_baseline": {"value": 1.0 / t, "unit": "steps/s", "cores": ncpu, "kind": "port",
-                             "sample": sample},
+                             "sample": "%d whole FP64 oracle steps after %d untimed, "
+                                       "numpy/scipy pocketfft, state chunks on %d host threads"
+                                       % (args.steps, args.warmup, ncpu)},
             "e2e": {"value": 1.0 / t, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
         }
         print(json.dumps(line))
         return
 
+    rank, ws, dist = dist_init()
     sysm, out, e_ref, f_ref = run_ours(args, cfg, args.config, rank, ws, dist)
     import numpy as np
     mixed, fp64 = out["mixed"], out["fp64"]
@@ -697,7 +731,13 @@ def main():
         "accuracy_vs_fp64": {"energy_Ha_per_atom": err_e, "local_force_Ha_per_bohr": err_f,
                              "orthonormality_mixed": mixed["first"][4],
                              "orthonormality_fp64": fp64["first"][4],
-                             "ortho_converged": bool(mixed["ortho_ok"])},
+                             "ortho_converged": bool(mixed["ortho_ok"]),
+                             "after_steps": mixed["last"][2],
+                             "energy_Ha_per_atom_after": abs(mixed["last"][0][8] -
+                                                             fp64["last"][0][8]) / sysm.natm,
+                             "local_force_Ha_per_bohr_after": float(np.max(np.abs(
+                                 mixed["last"][1] - fp64["last"][1]))),
+                             "psiv_resets_mixed_fp64": [mixed["last"][3], fp64["last"][3]]},
         "phase_ms_mixed": {"density": ph[0], "vks": ph[1], "vpsi_kinetic": ph[2],
                            "lambda": ph[3], "integrate": ph[4], "ortho_psiT": ph[5],
                            "ees_nonlocal": ph[6]},
@@ -715,8 +755,14 @@ def main():
         "e2e": {"value": ws * args.steps / (out["e2e"]["ms"] / 1e3), "unit": "steps/s",
                 "h2d_bytes_per_step": out["e2e"]["h2d"], "d2h_bytes_per_step": out["e2e"]["d2h"]},
     }
+    if ws == 1 and not args.no_batch16:
+        b = batch16_measure(args)
+        line["batch16"] = {k: b[k] for k in ("value", "unit", "workload", "plain_fp64_loop_value",
+                                             "batched_over_plain_loop", "mixed_loop_value",
+                                             "batched_over_mixed_loop", "loops_graphed",
+                                             "batch_graph", "energies_finite")}
     if ws == 1 and not args.no_cpu_baseline:
-        t, sample = cpu_baseline(cfg)
+        t, sample = cpu_baseline(cfg, args.norb_tol)
         line["cpu_baseline"] = {"value": 1.0 / t, "unit": "steps/s", "cores": os.cpu_count() or 1,
                                 "kind": "port", "sample": sample}
     print(json.dumps(line))

@@ -79,38 +79,56 @@ def hart_eext(rho_g, kx, ky, kz, box_len, ecut_ha, atoms, tab, alp_ewd):
     vps [ntyp, 4, nspl] (vps0..vps3), gmin, dg, gzvps [ntyp].
     Returns (vks [npts] complex, ehart, eext, ewd, force [natm, 3]).
     """
+    from .fftpath import state_map
     vol = box_len ** 3
     tpi = 2.0 * math.pi / box_len
-    gx, gy, gz = kx * tpi, ky * tpi, kz * tpi
-    g2 = gx * gx + gy * gy + gz * gz
+    kx, ky, kz = np.asarray(kx), np.asarray(ky), np.asarray(kz)
+    gx_all, gy_all, gz_all = kx * tpi, ky * tpi, kz * tpi
+    g2_all = gx_all * gx_all + gy_all * gy_all + gz_all * gz_all
     ecut4 = 8.0 * ecut_ha
-    sel = (g2 <= ecut4) & (g2 != 0)
-    w = np.where(kx == 0, 1.0, 2.0)
     pos = np.asarray(atoms["pos"], dtype=np.float64)
     typ = np.asarray(atoms["typ"])
     q = np.asarray(atoms["q"], dtype=np.float64)[typ]
-    g = np.sqrt(g2)
-    vt = spline_eval(tab, g) / vol                     # [ntyp, npts]
-    vtemp = vt[typ]                                    # [natm, npts]
-    arg = np.outer(pos[:, 0], gx) + np.outer(pos[:, 1], gy) + np.outer(pos[:, 2], gz)
-    h = np.exp(1j * arg)                               # e^{iG.R}  [natm, npts]
-    vext = np.sum(h * vtemp, axis=0)
-    sewd = np.sum(h * q[:, None], axis=0)
-    hart = np.where(sel, 4.0 * math.pi / np.where(sel, g2, 1.0) / vol, 0.0)
-    vks = np.where(sel, rho_g * hart + np.conj(vext), 0.0)
-    ehart = 0.5 * np.sum(np.where(sel, hart * np.abs(rho_g) ** 2 * w, 0.0))
-    ewdf = np.where(sel, 4.0 * math.pi * np.exp(-g2 / (4.0 * alp_ewd ** 2)) / np.where(sel, g2, 1.0) / vol, 0.0)
-    ewd = 0.5 * np.sum(ewdf * np.abs(sewd) ** 2 * w)
-    eext = np.sum(np.where(sel, (rho_g * vext).real * w, 0.0))
-    # atom forces (cp_hart_ext.C:270-300)
-    rr = np.where(sel, rho_g.real * w, 0.0)
-    ri = np.where(sel, rho_g.imag * w, 0.0)
-    sr = sewd.real * ewdf * w
-    si = sewd.imag * ewdf * w
-    tr = rr[None] * vtemp + sr[None] * q[:, None]
-    ti = -ri[None] * vtemp + si[None] * q[:, None]
-    t = tr * h.imag - ti * h.real                      # [natm, npts]
-    force = np.stack([t @ gx, t @ gy, t @ gz], axis=1)
+    natm = len(typ)
+    vks = np.zeros(len(kx), dtype=np.complex128)
+
+    def part(p0, p1):
+        """Points p0..p1-1: vks there and the (ehart, ewd, eext, force) partials."""
+        gx, gy, gz, g2 = gx_all[p0:p1], gy_all[p0:p1], gz_all[p0:p1], g2_all[p0:p1]
+        rg = rho_g[p0:p1]
+        sel = (g2 <= ecut4) & (g2 != 0)
+        w = np.where(kx[p0:p1] == 0, 1.0, 2.0)
+        g = np.sqrt(g2)
+        vt = spline_eval(tab, g) / vol                     # [ntyp, n]
+        vtemp = vt[typ]                                    # [natm, n]
+        arg = np.outer(pos[:, 0], gx) + np.outer(pos[:, 1], gy) + np.outer(pos[:, 2], gz)
+        h = np.exp(1j * arg)                               # e^{iG.R}  [natm, n]
+        vext = np.sum(h * vtemp, axis=0)
+        sewd = np.sum(h * q[:, None], axis=0)
+        hart = np.where(sel, 4.0 * math.pi / np.where(sel, g2, 1.0) / vol, 0.0)
+        vks[p0:p1] = np.where(sel, rg * hart + np.conj(vext), 0.0)
+        eh = 0.5 * np.sum(np.where(sel, hart * np.abs(rg) ** 2 * w, 0.0))
+        ewdf = np.where(sel, 4.0 * math.pi * np.exp(-g2 / (4.0 * alp_ewd ** 2))
+                        / np.where(sel, g2, 1.0) / vol, 0.0)
+        ew = 0.5 * np.sum(ewdf * np.abs(sewd) ** 2 * w)
+        ee = np.sum(np.where(sel, (rg * vext).real * w, 0.0))
+        # atom forces (cp_hart_ext.C:270-300)
+        rr = np.where(sel, rg.real * w, 0.0)
+        ri = np.where(sel, rg.imag * w, 0.0)
+        sr = sewd.real * ewdf * w
+        si = sewd.imag * ewdf * w
+        tr = rr[None] * vtemp + sr[None] * q[:, None]
+        ti = -ri[None] * vtemp + si[None] * q[:, None]
+        t = tr * h.imag - ti * h.real                      # [natm, n]
+        return eh, ew, ee, np.stack([t @ gx, t @ gy, t @ gz], axis=1)
+    ehart = ewd = eext = 0.0
+    force = np.zeros((natm, 3))
+    for eh, ew, ee, fo in state_map(part, len(kx), 16384):
+        ehart += eh
+        ewd += ew
+        eext += ee
+        force += fo
+    g2 = g2_all
     # G = 0 (:345-368)
     izero = np.nonzero(g2 == 0)[0]
     if len(izero):

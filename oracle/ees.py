@@ -262,32 +262,42 @@ def nonlocal_ees(psi, lay, occ, vol, hmati, atoms, channels, spl, nkf=None,
     S = psi.shape[0]
     w = np.where(lay.kx == 0, 1.0, 2.0)
     g0 = np.nonzero((lay.kx == 0) & (lay.ky == 0) & (lay.kz == 0))[0]
-    enl = 0.0
     fpsi = np.zeros_like(psi)
+    enl = 0.0
     fatm = np.zeros((natm, 3))
     for ch in channels:
         dyp = channel_dyp(ch, lay, hmati, nkf, spl, n_interp)
         members = np.nonzero(typ == ch["type"])[0]
         vn = ch["vnorm"] / vol
-        proj = np.conj(dyp[None, :] * psi)
-        pr = OF.state_g_to_r(proj, grid)              # [S, c, b, a]
-        scr = np.zeros_like(pr)
-        for s in range(S):
-            wn = occ[s]
-            for i in members:
-                (c, b, a), mn, dx, dy, dz = stens[i]
-                vals = pr[s][c, b, a]
-                zr = float(np.sum(vals * mn))
-                enl += zr * zr * vn * wn
-                zs = zr * 2.0 * vn * wn
-                fatm[i, 0] -= float(np.sum(vals * dx)) * zs
-                fatm[i, 1] -= float(np.sum(vals * dy)) * zs
-                fatm[i, 2] -= float(np.sum(vals * dz)) * zs
-                np.add.at(scr[s], (c.ravel(), b.ravel(), a.ravel()), (zs * mn).ravel())
-        pg = OF.state_r_to_g(scr, grid)
         d = dyp.copy()
         if len(g0):
-            pg[:, g0] = pg[:, g0].real
             d[g0] = d[g0].real
-        fpsi += -w[None, :] * np.conj(d[None, :] * pg)
+
+        def chunk(s0, s1):
+            """States s0..s1-1 of this channel: (E_NL, atom forces) partials; the
+            psi force goes to fpsi.  An atom's 512 stencil points are distinct
+            grid points, so its scatter needs no accumulation within itself."""
+            proj = np.conj(dyp[None, :] * psi[s0:s1])
+            pr = OF.state_g_to_r(proj, grid)              # [s, c, b, a]
+            scr = np.zeros_like(pr)
+            wn = np.asarray(occ[s0:s1], dtype=np.float64)
+            e, fa = 0.0, np.zeros((natm, 3))
+            for i in members:
+                (c, b, a), mn, dx, dy, dz = stens[i]
+                vals = pr[:, c, b, a].reshape(s1 - s0, -1)
+                zr = vals @ mn.ravel()
+                e += float(np.sum(zr * zr * vn * wn))
+                zs = zr * 2.0 * vn * wn
+                fa[i, 0] -= float(np.sum((vals @ dx.ravel()) * zs))
+                fa[i, 1] -= float(np.sum((vals @ dy.ravel()) * zs))
+                fa[i, 2] -= float(np.sum((vals @ dz.ravel()) * zs))
+                scr[:, c, b, a] += zs[:, None, None, None] * mn[None]
+            pg = OF.state_r_to_g(scr, grid)
+            if len(g0):
+                pg[:, g0] = pg[:, g0].real
+            fpsi[s0:s1] += -w[None, :] * np.conj(d[None, :] * pg)
+            return e, fa
+        for e, fa in OF.state_map(chunk, S, 8):
+            enl += e
+            fatm += fa
     return enl, fpsi, fatm

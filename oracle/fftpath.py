@@ -20,76 +20,115 @@ exp(-2 pi i jk/n), FFTW_BACKWARD exp(+2 pi i jk/n), both unnormalised;
 * addForces                stateSlab.C:240-272 (x2 off the Gx=0 plane)
 * kinetic energy           CP_eke_calc cp_eke.C:30-140
 """
+import threading
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 import scipy.fft as sfft
 
 _WORKERS = 1
+_POOL = None
+_TLS = threading.local()
+
+
+def _w():
+    """pocketfft threads for a call: 1 inside a state_map chunk (the chunks
+    already run concurrently), all of them otherwise."""
+    return 1 if getattr(_TLS, "inner", False) else _WORKERS
 
 
 def set_workers(n):
-    """Threads the oracle's FFTs may use (pocketfft via scipy.fft)."""
-    global _WORKERS
+    """Host threads the oracle may use: state chunks run concurrently on a
+    thread pool (numpy and pocketfft release the GIL in the array work)."""
+    global _WORKERS, _POOL
     _WORKERS = max(1, int(n))
+    if _POOL is not None:
+        _POOL.shutdown()
+    _POOL = ThreadPoolExecutor(_WORKERS) if _WORKERS > 1 else None
+
+
+def state_map(fn, n, chunk):
+    """[fn(s0, s1) for the chunks of range(n)] in chunk order, concurrently when
+    set_workers gave more than one thread (results do not depend on it)."""
+    spans = [(s0, min(n, s0 + chunk)) for s0 in range(0, n, chunk)]
+    if _POOL is None or len(spans) == 1 or getattr(_TLS, "inner", False):
+        return [fn(a, b) for a, b in spans]
+
+    def run(ab):
+        _TLS.inner = True
+        try:
+            return fn(*ab)
+        finally:
+            _TLS.inner = False
+    return list(_POOL.map(run, spans))
+
+
+def _line_index(lay):
+    """Flat [nlines * n] position of every packed point (the layout of the
+    line loops of expandGSpace / packGSpace), cached on the layout."""
+    idx = getattr(lay, "_line_idx", None)
+    if idx is None:
+        t = lay.line_tables()
+        n = lay.n
+        idx = np.empty(lay.npts, dtype=np.int64)
+        for l in range(lay.nlines):
+            o, nn, npo = int(t['off'][l]), int(t['nneg'][l]), int(t['npos'][l])
+            zn, zp = int(t['zneg'][l]), int(t['zpos'][l])
+            idx[o:o + nn] = l * n + zn + np.arange(nn)
+            idx[o + nn:o + nn + npo] = l * n + zp + np.arange(npo)
+        lay._line_idx = idx
+    return idx
 
 
 def expand(psi, lay):
     """[S, npts] complex -> [S, nlines, n] complex z-lines (expandGSpace)."""
-    t = lay.line_tables()
     S = psi.shape[0]
-    n = lay.n
-    out = np.zeros((S, lay.nlines, n), dtype=np.complex128)
-    for l in range(lay.nlines):
-        o, nn, npo = int(t['off'][l]), int(t['nneg'][l]), int(t['npos'][l])
-        zn, zp = int(t['zneg'][l]), int(t['zpos'][l])
-        out[:, l, zn:zn + nn] = psi[:, o:o + nn]
-        out[:, l, zp:zp + npo] = psi[:, o + nn:o + nn + npo]
-    return out
+    out = np.zeros((S, lay.nlines * lay.n), dtype=np.complex128)
+    out[:, _line_index(lay)] = psi
+    return out.reshape(S, lay.nlines, lay.n)
 
 
 def pack(lines, lay):
     """[S, nlines, n] -> [S, npts] (packGSpace)."""
-    t = lay.line_tables()
     S = lines.shape[0]
-    out = np.zeros((S, lay.npts), dtype=np.complex128)
-    for l in range(lay.nlines):
-        o, nn, npo = int(t['off'][l]), int(t['nneg'][l]), int(t['npos'][l])
-        zn, zp = int(t['zneg'][l]), int(t['zpos'][l])
-        out[:, o:o + nn] = lines[:, l, zn:zn + nn]
-        out[:, o + nn:o + nn + npo] = lines[:, l, zp:zp + npo]
-    return out
+    return lines.reshape(S, -1)[:, _line_index(lay)]
 
 
 def state_g_to_r(psi, lay):
     """Packed psi(G) [S, npts] -> real psi(r) [S, nz, ny, nx] (FP64)."""
     n = lay.n
     t = lay.line_tables()
-    z = sfft.fft(expand(psi, lay), axis=2, workers=_WORKERS)               # FFTW_FORWARD along z
+    z = sfft.fft(expand(psi, lay), axis=2, workers=_w())               # FFTW_FORWARD along z
     S = psi.shape[0]
     plane = np.zeros((S, n, n, n // 2 + 1), dtype=np.complex128)   # [s, z, y, x]
     plane[:, :, t['y'], t['x']] = np.transpose(z, (0, 2, 1))
-    plane = sfft.fft(plane, axis=2, workers=_WORKERS)      # FFTW_FORWARD along y
+    plane = sfft.fft(plane, axis=2, workers=_w())      # FFTW_FORWARD along y
     plane = np.conj(plane)                                 # imag flip
-    return sfft.irfft(plane, n=n, axis=3, workers=_WORKERS) * n  # rfftw C2R (+i, unnormalised)
+    return sfft.irfft(plane, n=n, axis=3, workers=_w()) * n  # rfftw C2R (+i, unnormalised)
 
 
 def state_r_to_g(f, lay):
     """Real f(r) [S, nz, ny, nx] -> packed F(G) [S, npts], unscaled (FP64)."""
     n = lay.n
     t = lay.line_tables()
-    X = np.conj(sfft.rfft(f, axis=3, workers=_WORKERS))    # rfftw R2C (-i), imag flip
-    X = sfft.ifft(X, axis=2, workers=_WORKERS) * n         # FFTW_BACKWARD along y
+    X = np.conj(sfft.rfft(f, axis=3, workers=_w()))    # rfftw R2C (-i), imag flip
+    X = sfft.ifft(X, axis=2, workers=_w()) * n         # FFTW_BACKWARD along y
     lines = np.transpose(X[:, :, t['y'], t['x']], (0, 2, 1))   # [s, line, z]
-    lines = sfft.ifft(lines, axis=2, workers=_WORKERS) * n  # FFTW_BACKWARD along z
+    lines = sfft.ifft(lines, axis=2, workers=_w()) * n  # FFTW_BACKWARD along z
     return pack(lines, lay)
 
 
 def density(psi, lay, occ, vol, chunk=16):
-    """rho(r) = sum_s occ_s psi_s(r)^2 / vol, [nz, ny, nx] FP64."""
+    """rho(r) = sum_s occ_s psi_s(r)^2 / vol, [nz, ny, nx] FP64 (chunk partials
+    summed in chunk order)."""
     n = lay.n
+
+    def part(s0, s1):
+        pr = state_g_to_r(psi[s0:s1], lay)
+        return np.einsum('s,szyx->zyx', occ[s0:s1], pr * pr)
     rho = np.zeros((n, n, n))
-    for s0 in range(0, psi.shape[0], chunk):
-        pr = state_g_to_r(psi[s0:s0 + chunk], lay)
-        rho += np.einsum('s,szyx->zyx', occ[s0:s0 + chunk], pr * pr)
+    for p in state_map(part, psi.shape[0], chunk):
+        rho += p
     return rho / vol
 
 
@@ -97,10 +136,12 @@ def vpsi_force(psi, vks, lay, occ, chunk=16):
     """F(G) = -2/N * FFT^-1[occ * V_KS * psi(r)]  (before addForces)."""
     n = lay.n
     out = np.zeros(psi.shape, dtype=np.complex128)
-    for s0 in range(0, psi.shape[0], chunk):
-        pr = state_g_to_r(psi[s0:s0 + chunk], lay)
-        f = pr * vks[None] * occ[s0:s0 + chunk, None, None, None]
-        out[s0:s0 + chunk] = state_r_to_g(f, lay) * (-2.0 / float(n * n * n))
+
+    def part(s0, s1):
+        pr = state_g_to_r(psi[s0:s1], lay)
+        f = pr * vks[None] * occ[s0:s1, None, None, None]
+        out[s0:s1] = state_r_to_g(f, lay) * (-2.0 / float(n * n * n))
+    state_map(part, psi.shape[0], chunk)
     return out
 
 
