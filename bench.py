@@ -426,6 +426,8 @@ def kernel_case(args):
     sysm = System(cfg["box"], cfg["ecut"], S, cfg["atoms"], nfft=cfg["grid"])
     occ = torch.ones(S, dtype=torch.float64, device="cuda")
     ctx = StepContext(sysm.layout, S, precision=args.precision)
+    if args.plane_form is not None:
+        ctx.tune_set({"plane_shfl": args.plane_form})
     psi = sysm.psi()
     rho = ctx.density(psi, occ)
     if args.kernel_case == "statefft":
@@ -633,6 +635,8 @@ def main():
     ap.add_argument("--kernel-case", choices=["statefft", "rhoside", "ees", "paircalc"], default=None,
                     help="run a small profiling case instead of the benchmark")
     ap.add_argument("--states", type=int, default=8)
+    ap.add_argument("--plane-form", type=int, choices=[0, 1, 2], default=None,
+                    help="kernel cases: the plane-pass form (0 Stockham, 1 shuffles, 2 two-stage)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--batch16", action="store_true",
                     help="16 independent systems of uneven size stepped by one batch graph "

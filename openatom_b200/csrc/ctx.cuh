@@ -343,8 +343,9 @@ struct cpstep_ctx {
   // launch choices (cpstep_autotune, cpstep_tune_get/set); the defaults are
   // the fixed heuristics
   struct Tune {
-    int shfl = 1;         // state plane passes (density, V.psi): register shuffle FFT (1) or
-                          // shared-memory Stockham (0), where both exist
+    int shfl = 1;         // state plane passes (density, V.psi): register shuffle FFT (1),
+                          // shared-memory Stockham (0), or the two-stage form of
+                          // fft_p16.cuh (2: FP32 and N = 32, 64, 128; elsewhere as 1)
     int plane_waves = 3;  // state plane passes: blocks ~ plane_waves x SMs
     int nl_blocks = 6;    // EES plane kernels: blocks ~ nl_blocks x SMs
     int pc_split = 1;     // PairCalc overlap split-K: CTAs ~ pc_split x SMs

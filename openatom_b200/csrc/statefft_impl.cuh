@@ -26,6 +26,7 @@
 #include <vector>
 #include "ctx.cuh"
 #include "fft_shfl.cuh"
+#include "fft_p16.cuh"
 
 namespace sfft {
 
@@ -769,6 +770,273 @@ k_xy_bwd_s(const cplx<T>* __restrict__ pen, const double* __restrict__ freal,
 }
 
 // ---------------------------------------------------------------------------
+// Plane passes in the two-stage form (fft_p16.cuh), FP32, N = 32, 64, 128:
+// 256 threads, every warp 32 / R line groups of R threads, one line (a
+// column or a row pair) per group at a time.  The plane is [nplane_x][LDY]
+// with LDY odd and >= N + N/16: a column is transformed in place with its own
+// storage as the exchange scratch; row pairs use a per-group scratch line.
+// Row pairs are built straight from the plane into stride layout (imag flip,
+// Hermitian extension), C2R'd by s2b into block layout where V_KS (K3) or the
+// density (K2) is applied, and (K3) R2C'd by b2s back into stride layout,
+// where the two real rows' spectra are split with one shuffle.
+// K2 runs 512 threads (for N = 128 every line group owns one row pair of the
+// plane, so its FP64 accumulators fit the registers), K3 256 threads at two
+// blocks per SM.
+template <int N, int THREADS_>
+struct P16Shape {
+  static constexpr int THREADS = THREADS_, NW = THREADS / 32;
+  static constexpr int LPW = P16Cfg<N>::LPW, SLOTS = NW * LPW;
+  static constexpr int LDY = (P16Cfg<N>::SCR | 1) == P16Cfg<N>::SCR ? P16Cfg<N>::SCR
+                                                                   : P16Cfg<N>::SCR + 1;
+  static constexpr int SL = ((P16Cfg<N>::SCR + 15) / 16) * 16 + 8;  // row scratch stride
+  // twiddles, plane, row scratch, pencil-row staging (nlines rounded to 2)
+  static constexpr size_t bytes(int nplx, int nlines) {
+    return sizeof(cplx<float>) *
+           ((size_t)N + (size_t)nplx * LDY + (size_t)SLOTS * SL + (size_t)((nlines + 1) & ~1));
+  }
+};
+constexpr int P16_K2_THREADS = 512, P16_K3_THREADS = 256;
+
+// the pencil row of one (state, z) into the shared staging buffer with
+// cp.async (8-byte copies, one group per call): issued while the previous
+// state is transformed, waited for by p16_scatter
+__device__ __forceinline__ void p16_prefetch(const cplx<float>* __restrict__ prow,
+                                             cplx<float>* stage, int nlines) {
+  for (int l = threadIdx.x; l < nlines; l += blockDim.x)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(stage + l)),
+                 "l"(prow + l)
+                 : "memory");
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// zero the plane's N rows of every column and scatter the staged pencil row
+template <int N, int LDY>
+__device__ __forceinline__ void p16_scatter(const cplx<float>* stage, cplx<float>* plane,
+                                            const StateGeom& g) {
+  for (int i = threadIdx.x; i < g.nplane_x * LDY; i += blockDim.x) plane[i] = mk<float>(0, 0);
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();
+  for (int l = threadIdx.x; l < g.nlines; l += blockDim.x) {
+    const int xy = __ldg(g.line_xy + l);
+    plane[(xy & 0xffff) * LDY + (xy >> 16)] = stage[l];
+  }
+  __syncthreads();
+}
+
+// y-FFTs of the nplane_x columns in place (natural order in and out); groups
+// past the last column work on their own scratch line and store nothing.
+template <int N, bool INV, bool LEAN>
+__device__ __forceinline__ void p16_columns(cplx<float>* plane, int ldy, int nplx,
+                                            const P16Fft<float, N, LEAN>& F, cplx<float>* scr,
+                                            int slot, int nslots) {
+  constexpr int R = P16Cfg<N>::R;
+  for (int c0 = 0; c0 < nplx; c0 += nslots) {
+    const int c = c0 + slot;
+    const bool act = c < nplx;
+    cplx<float>* col = act ? plane + (size_t)c * ldy : scr;
+    cplx<float> v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = col[F.t + R * k];
+    F.template s2b<INV>(v, col);
+    __syncwarp();
+    if (act) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) col[F.bpos(q)] = v[q];
+    }
+    __syncwarp();
+  }
+}
+
+// C2R input of rows (ya, ya+1) in stride layout: Z = conj(Xa) + i conj(Xb) from
+// the y-transformed plane, Hermitian-extended to kx > N/2 (as shfl_build_row)
+template <int N>
+__device__ __forceinline__ void p16_build_row(const cplx<float>* plane, int ldy, int nplx, int ya,
+                                              int t, cplx<float> (&v)[16]) {
+  constexpr int R = P16Cfg<N>::R;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const int x = t + R * k;
+    cplx<float> z = mk<float>(0, 0);
+    if (x == 0) {
+      z = mk<float>(plane[ya].x, plane[ya + 1].x);
+    } else if (x < nplx) {
+      const cplx<float> a = plane[x * ldy + ya], b = plane[x * ldy + ya + 1];
+      z = mk<float>(a.x + b.y, b.x - a.y);
+    } else if (N - x < nplx) {
+      const int m = N - x;
+      const cplx<float> a = plane[m * ldy + ya], b = plane[m * ldy + ya + 1];
+      z = mk<float>(a.x - b.y, a.y + b.x);
+    }
+    v[k] = z;
+  }
+}
+
+// After b2s (forward) of a row pair: Zf[t + R b] in slot b.  Split the two real
+// rows' spectra (partner N - kx: thread R - t, slot 15 - b; thread 0 keeps its
+// own slot (16 - b) % 16), imag flip, store kx < nplane_x.  All lanes of the
+// warp call it (the shuffle); only act stores.
+template <int N>
+__device__ __forceinline__ void p16_extract_row(const cplx<float> (&v)[16], cplx<float>* plane,
+                                                int ldy, int nplx, int ya, int t, bool act) {
+  constexpr int R = P16Cfg<N>::R;
+  const int src = (R - t) % R;
+#pragma unroll
+  for (int b = 0; b < 16; ++b) {
+    cplx<float> zm;
+    zm.x = __shfl_sync(0xffffffffu, v[15 - b].x, src, R);
+    zm.y = __shfl_sync(0xffffffffu, v[15 - b].y, src, R);
+    if (t == 0) zm = v[(16 - b) % 16];
+    const int kx = t + R * b;
+    if (act && kx < nplx) {
+      const cplx<float> zk = v[b];
+      plane[kx * ldy + ya] = mk<float>(0.5f * (zk.x + zm.x), 0.5f * (zm.y - zk.y));
+      plane[kx * ldy + ya + 1] = mk<float>(0.5f * (zk.y + zm.y), 0.5f * (zk.x - zm.x));
+    }
+  }
+}
+
+// K3 (two-stage form): pencils -> psi(r) -> psi V occ -> pencils_out
+template <int N>
+__global__ void __launch_bounds__(P16_K3_THREADS, 2)
+k_xy_bwd_p16(const cplx<float>* __restrict__ pen, const float* __restrict__ vks,
+             cplx<float>* __restrict__ pen_out, StateGeom g,
+             const cplx<float>* __restrict__ twx_g, const double* __restrict__ occ,
+             int nstates, int spg) {
+  using S = P16Shape<N, P16_K3_THREADS>;
+  constexpr int LDY = S::LDY, SLOTS = S::SLOTS, R = P16Cfg<N>::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<float>* tw = reinterpret_cast<cplx<float>*>(smem_raw);
+  cplx<float>* plane = tw + N;
+  const int nplx = g.nplane_x;
+  const int slot = (threadIdx.x >> 5) * S::LPW + (threadIdx.x & 31) / R;
+  cplx<float>* scr = plane + (size_t)nplx * LDY + (size_t)slot * S::SL;
+  cplx<float>* stage = plane + (size_t)nplx * LDY + (size_t)SLOTS * S::SL;
+  const int z = blockIdx.x;
+  const int s0 = blockIdx.y * spg, s1 = min(nstates, s0 + spg);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx_g[i];
+  if (s0 < s1) p16_prefetch(pen + ((size_t)s0 * N + z) * g.nlpad, stage, g.nlines);
+  __syncthreads();
+  P16Fft<float, N> F;
+  F.init(tw);
+  const float* vplane = vks + (size_t)z * N * N;
+  for (int s = s0; s < s1; ++s) {
+    p16_scatter<N, LDY>(stage, plane, g);
+    if (s + 1 < s1) p16_prefetch(pen + ((size_t)(s + 1) * N + z) * g.nlpad, stage, g.nlines);
+    p16_columns<N, false>(plane, LDY, nplx, F, scr, slot, SLOTS);  // FFTW_FORWARD y
+    __syncthreads();
+    const float w = (float)occ[s];
+    for (int p0 = 0; p0 < N / 2; p0 += SLOTS) {
+      const int pp = p0 + slot;
+      const bool act = pp < N / 2;
+      const int ya = act ? 2 * pp : 0;
+      // V_KS of the two rows at this thread's block-layout positions, loaded
+      // (from L2) before the C2R so that the transform covers the latency
+      float va[16], vb[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int x = F.bpos(q);
+        va[q] = __ldg(vplane + ya * N + x);
+        vb[q] = __ldg(vplane + (ya + 1) * N + x);
+      }
+      cplx<float> v[16];
+      p16_build_row<N>(plane, LDY, nplx, ya, F.t, v);
+      F.template s2b<true>(v, scr);  // C2R, +i sign
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        v[q].x *= va[q] * w;
+        v[q].y *= vb[q] * w;
+      }
+      F.template b2s<false>(v, scr);  // R2C, -i sign
+      p16_extract_row<N>(v, plane, LDY, nplx, ya, F.t, act);
+    }
+    __syncthreads();
+    p16_columns<N, true>(plane, LDY, nplx, F, scr, slot, SLOTS);  // FFTW_BACKWARD y
+    __syncthreads();
+    cplx<float>* po = pen_out + ((size_t)s * N + z) * g.nlpad;
+    for (int l = threadIdx.x; l < g.nlines; l += blockDim.x) {
+      const int xy = __ldg(g.line_xy + l);
+      po[l] = plane[(xy & 0xffff) * LDY + (xy >> 16)];
+    }
+    __syncthreads();
+  }
+}
+
+// K2 (two-stage form): planes -> occ psi^2 accumulated in FP64 registers over
+// the block's states; the block's partial density of plane z goes to out
+// [group][z][y][x].  Every row pair of the plane belongs to one line group
+// (PASSES = (N/2) / SLOTS of them per group), the slots of its block layout
+// to the group's threads.
+template <int N>
+__global__ void __launch_bounds__(P16_K2_THREADS, 1)
+k_xy_fwd_p16(const cplx<float>* __restrict__ pen, StateGeom g,
+             const cplx<float>* __restrict__ twx_g, const double* __restrict__ occ,
+             int nstates, int spg, double* __restrict__ out) {
+  using S = P16Shape<N, P16_K2_THREADS>;
+  constexpr int LDY = S::LDY, SLOTS = S::SLOTS, R = P16Cfg<N>::R;
+  constexpr int PASSES = (N / 2 + SLOTS - 1) / SLOTS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<float>* tw = reinterpret_cast<cplx<float>*>(smem_raw);
+  cplx<float>* plane = tw + N;
+  const int nplx = g.nplane_x;
+  const int slot = (threadIdx.x >> 5) * S::LPW + (threadIdx.x & 31) / R;
+  cplx<float>* scr = plane + (size_t)nplx * LDY + (size_t)slot * S::SL;
+  cplx<float>* stage = plane + (size_t)nplx * LDY + (size_t)SLOTS * S::SL;
+  const int z = blockIdx.x;
+  const int s0 = blockIdx.y * spg, s1 = min(nstates, s0 + spg);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx_g[i];
+  if (s0 < s1) p16_prefetch(pen + ((size_t)s0 * N + z) * g.nlpad, stage, g.nlines);
+  __syncthreads();
+  P16Fft<float, N, true> F;
+  F.init(tw);
+  double acc[PASSES][2][16];
+#pragma unroll
+  for (int q = 0; q < PASSES; ++q)
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int k = 0; k < 16; ++k) acc[q][h][k] = 0.0;
+  for (int s = s0; s < s1; ++s) {
+    p16_scatter<N, LDY>(stage, plane, g);
+    if (s + 1 < s1) p16_prefetch(pen + ((size_t)(s + 1) * N + z) * g.nlpad, stage, g.nlines);
+    p16_columns<N, false>(plane, LDY, nplx, F, scr, slot, SLOTS);  // FFTW_FORWARD y
+    __syncthreads();
+    const double w = occ[s];
+#pragma unroll
+    for (int q = 0; q < PASSES; ++q) {
+      const int pp = slot + SLOTS * q;
+      const bool act = pp < N / 2;
+      const int ya = act ? 2 * pp : 0;
+      cplx<float> v[16];
+      p16_build_row<N>(plane, LDY, nplx, ya, F.t, v);
+      F.template s2b<true>(v, scr);  // C2R, +i sign
+      if (act) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          acc[q][0][k] += w * (double)v[k].x * (double)v[k].x;
+          acc[q][1][k] += w * (double)v[k].y * (double)v[k].y;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  double* o = out + ((size_t)blockIdx.y * N + z) * N * N;
+#pragma unroll
+  for (int q = 0; q < PASSES; ++q) {
+    const int pp = slot + SLOTS * q;
+    if (pp < N / 2) {
+      const int ya = 2 * pp;
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const int x = F.bpos(k);
+        o[(size_t)ya * N + x] = acc[q][0][k];
+        o[(size_t)(ya + 1) * N + x] = acc[q][1][k];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // K4: pencils -> backward z-FFT -> pack -> scale.
 //   MODE 0: F = scale * wpt * val (then, if occ != null, the kinetic term)
 //   MODE 1: plain pack with scale (adjoint transform)
@@ -1165,6 +1433,24 @@ struct StateFft {
   static int density(cpstep_ctx* c, const double* psi, const double* occ, double* rho) {
     const FftJob j = c->state_job();
     if (int rc = zfft_fwd(c, j, psi, c->nstates)) return rc;
+    if constexpr (P16Cfg<N>::ok && sizeof(T) == 4) {
+      if (c->tune.shfl == 2) {
+        const size_t smem = P16Shape<N, P16_K2_THREADS>::bytes(j.g.nplane_x, j.g.nlines);
+        int ng = std::min(c->ngroups_rho, plane_groups(c, c->nstates, 1));
+        int spg = cdiv(c->nstates, ng);
+        ng = cdiv(c->nstates, spg);
+        if (int rc = set_smem(k_xy_fwd_p16<N>, smem)) return rc;
+        k_xy_fwd_p16<N><<<dim3(N, ng), P16_K2_THREADS, smem, c->stream>>>(
+            reinterpret_cast<const cplx<float>*>(j.pen_a), j.g, tws<float>(c).x, occ,
+            c->nstates, spg, c->d_rho_part);
+        CPSTEP_LAUNCH_CHECK();
+        size_t nr = (size_t)N * N * N;
+        k_rho_reduce<<<2 * c->num_sms, 256, 0, c->stream>>>(c->d_rho_part, ng, nr, 1.0 / c->vol,
+                                                            rho);
+        CPSTEP_LAUNCH_CHECK();
+        return CPSTEP_OK;
+      }
+    }
     if constexpr (ShflCfg<N>::ok) {
       if (c->tune.shfl) {
         const size_t smem = SShape<T, N>::bytes(j.g.nplane_x);
@@ -1299,8 +1585,19 @@ struct StateFft {
     int spg = cdiv(c->nstates, ng);
     ng = cdiv(c->nstates, spg);
     bool shfl_done = false;
+    if constexpr (P16Cfg<N>::ok && sizeof(T) == 4) {
+      if (c->tune.shfl == 2) {
+        const size_t smem = P16Shape<N, P16_K3_THREADS>::bytes(j.g.nplane_x, j.g.nlines);
+        if (int rc = set_smem(k_xy_bwd_p16<N>, smem)) return rc;
+        k_xy_bwd_p16<N><<<dim3(N, ng), P16_K3_THREADS, smem, c->stream>>>(
+            reinterpret_cast<const cplx<float>*>(j.pen_a), reinterpret_cast<const float*>(vt),
+            reinterpret_cast<cplx<float>*>(j.pen_b), j.g, tws<float>(c).x, occ, c->nstates,
+            spg);
+        shfl_done = true;
+      }
+    }
     if constexpr (ShflCfg<N>::ok) {
-      if (c->tune.shfl) {
+      if (c->tune.shfl && !shfl_done) {
         const size_t smem = SShape<T, N>::bytes(j.g.nplane_x);
         if (int rc = set_smem(k_xy_bwd_s<T, N, 0>, smem)) return rc;
         k_xy_bwd_s<T, N, 0><<<dim3(N, ng), PTHREADS, smem, c->stream>>>(

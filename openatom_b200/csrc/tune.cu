@@ -84,7 +84,7 @@ int cpstep_tune_get(const cpstep_ctx* c, int* vals, int n) {
 
 int cpstep_tune_set(cpstep_ctx* c, const int* vals, int n) {
   if (!c || !vals || n < CPSTEP_NTUNE) return CPSTEP_ERR_ARG;
-  if ((vals[0] != 0 && vals[0] != 1) || vals[1] < 1 || vals[1] > 64 || vals[2] < 1 ||
+  if ((vals[0] < 0 || vals[0] > 2) || vals[1] < 1 || vals[1] > 64 || vals[2] < 1 ||
       vals[2] > 64 || vals[3] < 1 || vals[3] > 16 || (vals[4] != 0 && vals[4] != 1) ||
       (vals[5] != 0 && vals[5] != 1))
     return CPSTEP_ERR_ARG;
@@ -123,7 +123,13 @@ int cpstep_autotune(cpstep_ctx* c, const double* d_psi, const double* d_occ, dou
     if (int r = statefft_density(c, d_psi, d_occ, rho)) return r;
     return statefft_vpsi(c, d_psi, rho, d_occ, force, eke, 1);
   };
-  if (!rc) rc = pick(c, &c->tune.shfl, {1, 0}, planes, &ms[0]);
+  // plane-pass form: 1 register shuffles, 0 shared-memory Stockham, 2 the
+  // two-stage form (FP32, N = 32, 64, 128; elsewhere it runs as 1)
+  if (!rc) {
+    std::vector<int> forms = {1, 0};
+    if (c->precision == CPSTEP_PREC_MIXED) forms.push_back(2);
+    rc = pick(c, &c->tune.shfl, forms, planes, &ms[0]);
+  }
   if (!rc) rc = pick(c, &c->tune.plane_waves, {1, 2, 3, 6}, planes, &ms[1]);
   // 4, 5: the overlap product S (split-K width; tensor cores or FP64 in a mixed context)
   auto ovl = [&]() -> int {

@@ -135,3 +135,33 @@ def test_adjointness_of_the_two_transforms(system, ctx):
     rhs = (w[None] * (psi.conj() * Fg).real).sum(dim=1)
     tol = 1e-10 if ctx.precision == "fp64" else 1e-4
     assert float((lhs - rhs).abs().max() / lhs.abs().max()) < tol
+
+
+@pytest.mark.parametrize("form", [0, 1, 2])
+def test_plane_pass_forms_match_oracle(system, form):
+    """Density and V.psi in a mixed context with each plane-pass form: 0
+    shared-memory Stockham, 1 register shuffles, 2 the two-stage form of
+    fft_p16.cuh (grids 32, 64, 128; the others run form 1 there)."""
+    import torch
+    from oracle import fftpath as OF
+    from openatom_b200.context import StepContext
+    lay, olay = system["lay"], system["olay"]
+    psi, occ = system["psi"], system["occ"]
+    ctx = StepContext(lay, system["S"], precision="mixed")
+    try:
+        ctx.tune_set({"plane_shfl": form})
+        pn, on = psi.cpu().numpy(), occ.cpu().numpy()
+        rho = ctx.density(psi, occ).cpu().numpy()
+        ref = OF.density(pn, olay, on, lay.vol)
+        assert relerr(rho, ref) < TOL["mixed"]
+        n = lay.n
+        g = torch.Generator(device="cpu").manual_seed(9)
+        vks = torch.randn((n, n, n), generator=g, dtype=torch.float64)
+        force, eke = ctx.vks_psi(psi, vks.cuda(), occ, kinetic=True)
+        fv = OF.vpsi_force(pn, vks.numpy(), olay, on)
+        f_ref = OF.add_forces(fv, None, olay)
+        f_ref, e_ref = OF.eke(f_ref, pn, olay, on, lay.ecut_ry)
+        assert relerr(force.cpu().numpy(), f_ref) < TOL["mixed"]
+        assert ctx.device_errors() == 0
+    finally:
+        ctx.close()
