@@ -119,6 +119,7 @@ struct RhoGeom {
   double* vhl = nullptr;     // Hartree + local potential on the grid
   double* part = nullptr;    // reduction partials
   int nblk_xc = 0, nblk_h = 0;
+  int kz_runs = 0;           // every line's points have consecutive kz (phase recurrence)
 };
 
 // Atoms, pseudopotential spline tables and structure-factor phase tables.
@@ -343,7 +344,7 @@ struct cpstep_ctx {
   // launch choices (cpstep_autotune, cpstep_tune_get/set); the defaults are
   // the fixed heuristics
   struct Tune {
-    int shfl = 1;         // state plane passes (density, V.psi): register shuffle FFT (1),
+    int shfl = 2;         // state plane passes (density, V.psi): register shuffle FFT (1),
                           // shared-memory Stockham (0), or the two-stage form of
                           // fft_p16.cuh (2: FP32 and N = 32, 64, 128; elsewhere as 1)
     int plane_waves = 3;  // state plane passes: blocks ~ plane_waves x SMs

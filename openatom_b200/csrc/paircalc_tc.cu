@@ -10,9 +10,10 @@
 // (the level pairs of total order <= 2; the dropped ones are O(2^-24 |ab|)) is
 // accumulated by tcgen05.mma (kind::f16, BF16 in, FP32 accumulators in TMEM),
 // smallest terms first, h_a h_b in an accumulator of its own.  That one holds
-// at most 128 reals of K: it is then read back (tcgen05.ld) and added into an
-// FP64 copy of the tile kept in the other half of TMEM (two 32-bit columns
-// per element, read and written back with tcgen05.ld / tcgen05.st).  The five
+// at most 128 reals of K (512 in the EES products): it is then read back
+// (tcgen05.ld) and added into an FP64 copy of the tile kept in the other half
+// of TMEM (two 32-bit columns per element, read and written back with
+// tcgen05.ld / tcgen05.st).  The five
 // small products (2^-7 of the total) run over the CTA's whole K range in FP32
 // and join the FP64 tile in the epilogue: their rounding stays well below the
 // hi*hi groups' own.  The sums over the groups, the split-K slabs and the
@@ -74,7 +75,12 @@ template <int MODE, int NLD, int NST, int KC>
 struct Cfg {
   static constexpr int KS = KC / 16;                     // MMA K steps per chunk
   static constexpr int U = KC / 8;                       // 8-element units per row
-  static constexpr int NF = 128 / KC;                    // chunks per TMEM group
+  // chunks per TMEM group: the hi*hi accumulator holds 128 reals of K for the
+  // PairCalc products (S must stay orthonormal to 1e-8) and 512 for the EES
+  // sums and psi force (FP32 accumulation over 512 products leaves a relative
+  // error near 1e-6 in Z, far inside the energy budget), so their fold of the
+  // accumulator into the FP64 tile runs a quarter as often
+  static constexpr int NF = (MODE >= 2 ? 512 : 128) / KC;
   static constexpr int RS = KC + 2;                      // row stride of a [128][KC] FP64 stage
   static constexpr int RSP = ROWS + 2;                   // row stride of a [KC][128] FP64 stage
   static constexpr int RSF = KC + 4;                     // [128][KC] FP32 stage

@@ -242,6 +242,141 @@ k_hart_lines(const double2* __restrict__ rhog_t, const int* __restrict__ line_of
   }
 }
 
+// The same pass with the z phase advanced along the line instead of read per
+// point (the reference's ei_inc recursion, cp_hart_ext.C:150-210): needs the
+// points of every line at consecutive kz.  A group of HG lanes owns a line;
+// lane j owns points HPL j .. HPL j + HPL - 1 of each HG HPL-point segment.
+// Per atom (type order) a lane reads the phase at its first kz and
+// e^{i2pi sz}, then multiplies along its points; the loads of four atoms are
+// issued together.  Each lane's per-type sums are in registers; the energy
+// partials of the line are summed over its group.
+constexpr int HG = 32, HPL = 4, HWARPS = 4, HBATCH = 4;
+__global__ void __launch_bounds__(32 * HWARPS)
+k_hart_lines_rec(const double2* __restrict__ rhog_t, const int* __restrict__ line_off,
+                 int nlines, const int* __restrict__ kx, const int* __restrict__ ky,
+                 const int* __restrict__ kz, int npts, const double* __restrict__ hmati,
+                 double vol, double ecut4, double alp, Atoms A, double2* __restrict__ vg_t,
+                 double4* __restrict__ fterm, double* __restrict__ part) {
+  extern __shared__ double2 su_all[];  // [groups][natm] line phases, type order
+  const double tpi = 2.0 * M_PI, rvol = 1.0 / vol, fpi = 4.0 * M_PI;
+  const double falp2 = 4.0 * alp * alp;
+  const int lane = threadIdx.x & 31, grp = threadIdx.x / HG, j = lane & (HG - 1);
+  const int ngrp = (32 / HG) * HWARPS;
+  double2* su = su_all + (size_t)grp * A.natm;
+  const int nz = 2 * A.kzm + 1;
+  // every group walks lines l = blockIdx.x * ngrp + grp, + gridDim.x * ngrp, ...;
+  // the trip count is the same for the two groups of a warp (their shuffles)
+  for (int lb = blockIdx.x * ngrp; lb < nlines; lb += gridDim.x * ngrp) {
+    const int l = lb + grp;
+    const bool live = l < nlines;
+    const int off = live ? line_off[l] : 0;
+    const int end = live ? ((l + 1 < nlines) ? line_off[l + 1] : npts) : 0;
+    const int a = live ? kx[off] : 0, b = live ? ky[off] : 0;
+    __syncwarp();
+    if (live)
+      for (int i = j; i < A.natm; i += HG) {
+        const int at = i;  // atom index; its phase goes to its type-ordered slot
+        double2 x = A.ex[(size_t)a * A.natm + at];
+        double2 y = A.ey[(size_t)(b + A.kym) * A.natm + at];
+        su[A.rank[at]] = make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
+      }
+    __syncwarp();
+    double eh = 0.0, ee = 0.0, ew = 0.0;
+    const double gx0 = tpi * (a * hmati[0] + b * hmati[1]);
+    const double gy0 = tpi * (a * hmati[3] + b * hmati[4]);
+    const double gz0 = tpi * (a * hmati[6] + b * hmati[7]);
+    for (int s0 = off; s0 < end; s0 += HG * HPL) {
+      const int p0 = s0 + HPL * j;            // this lane's first point
+      const int np = max(0, min(HPL, end - p0));
+      const int c0 = np > 0 ? kz[p0] : 0;
+      double2 vext[HPL], sewd[HPL];
+#pragma unroll
+      for (int k = 0; k < HPL; ++k) vext[k] = sewd[k] = make_double2(0.0, 0.0);
+      double g[HPL];
+#pragma unroll
+      for (int k = 0; k < HPL; ++k) {
+        const int c = c0 + k;
+        const double gx = gx0 + tpi * c * hmati[2], gy = gy0 + tpi * c * hmati[5],
+                     gz = gz0 + tpi * c * hmati[8];
+        g[k] = gx * gx + gy * gy + gz * gz;  // g^2 here, g below
+      }
+      if (np > 0) {
+        for (int t = 0; t < A.ntyp; ++t) {
+          double2 st[HPL];
+#pragma unroll
+          for (int k = 0; k < HPL; ++k) st[k] = make_double2(0.0, 0.0);
+          const int ie = A.tstart[t + 1];
+          for (int i0 = A.tstart[t]; i0 < ie; i0 += HBATCH) {
+            double2 z[HBATCH], inc[HBATCH], u[HBATCH];
+#pragma unroll
+            for (int q = 0; q < HBATCH; ++q) {
+              const bool in = i0 + q < ie;
+              const double2* zr = A.ezt + (size_t)(in ? i0 + q : i0) * nz;
+              z[q] = in ? zr[c0 + A.kzm] : make_double2(0.0, 0.0);
+              inc[q] = zr[1 + A.kzm];
+              u[q] = su[in ? i0 + q : i0];
+            }
+#pragma unroll
+            for (int q = 0; q < HBATCH; ++q) {  // atoms in order: the sums keep it
+              double2 ph = make_double2(u[q].x * z[q].x - u[q].y * z[q].y,
+                                        u[q].x * z[q].y + u[q].y * z[q].x);
+#pragma unroll
+              for (int k = 0; k < HPL; ++k) {
+                st[k].x += ph.x;
+                st[k].y += ph.y;
+                ph = make_double2(ph.x * inc[q].x - ph.y * inc[q].y,
+                                  ph.x * inc[q].y + ph.y * inc[q].x);
+              }
+            }
+          }
+          const double qt = A.q[t];
+#pragma unroll
+          for (int k = 0; k < HPL; ++k) {
+            const double vt = (k < np && g[k] != 0.0) ? vps_at(A, t, sqrt(g[k]), rvol) : 0.0;
+            vext[k].x += vt * st[k].x;
+            vext[k].y += vt * st[k].y;
+            sewd[k].x += qt * st[k].x;
+            sewd[k].y += qt * st[k].y;
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < HPL; ++k) {
+        if (k >= np) break;
+        const int p = p0 + k;
+        const double g2 = g[k];
+        double2 out = make_double2(0.0, 0.0);
+        double4 ft = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (g2 <= ecut4 && g2 != 0.0) {
+          const double w = (a == 0) ? 1.0 : 2.0;
+          double2 r = rhog_t[p];
+          r.y = -r.y;  // reference rho(G)
+          const double hart = fpi / (g2 * vol);
+          eh += 0.5 * hart * (r.x * r.x + r.y * r.y) * w;
+          const double ewdf = fpi * exp(-g2 / falp2) / (g2 * vol);
+          ew += 0.5 * ewdf * (sewd[k].x * sewd[k].x + sewd[k].y * sewd[k].y) * w;
+          ee += (r.x * vext[k].x - r.y * vext[k].y) * w;
+          out = make_double2(r.x * hart + vext[k].x, -(r.y * hart - vext[k].y));
+          ft = make_double4(r.x * w, -r.y * w, sewd[k].x * ewdf * w, sewd[k].y * ewdf * w);
+        }
+        vg_t[p] = out;
+        fterm[p] = ft;
+      }
+    }
+#pragma unroll
+    for (int o = HG / 2; o > 0; o >>= 1) {
+      eh += __shfl_xor_sync(0xffffffffu, eh, o, HG);
+      ee += __shfl_xor_sync(0xffffffffu, ee, o, HG);
+      ew += __shfl_xor_sync(0xffffffffu, ew, o, HG);
+    }
+    if (live && j == 0) {
+      part[3 * l] = eh;
+      part[3 * l + 1] = ee;
+      part[3 * l + 2] = ew;
+    }
+  }
+}
+
 // G = 0 (cp_hart_ext.C:345-368); single thread
 __global__ void k_hart_g0(const double2* __restrict__ rhog_t, int izero, double vol, Atoms A,
                           double2* __restrict__ vg_t, double* __restrict__ eext) {
@@ -261,6 +396,7 @@ __global__ void k_hart_g0(const double2* __restrict__ rhog_t, int izero, double 
 // thread per atom) walks lines blockIdx.x, +gridDim.x, ...; T_t of the line's
 // points is staged in shared memory [ntyp][lmax] with kz beside it.
 // Writes fpart[block][natm][3].
+template <bool REC>
 __global__ void k_local_forces_lines(const double4* __restrict__ fterm,
                                      const int* __restrict__ line_off, int nlines,
                                      const int* __restrict__ kx, const int* __restrict__ ky,
@@ -306,10 +442,14 @@ __global__ void k_local_forces_lines(const double4* __restrict__ fterm,
           double2 u = make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
           const double2* T = sT + (size_t)t * lmax;
           double px = 0.0, py = 0.0, qx = 0.0, qy = 0.0;
+          // REC: kz runs up by one along the line, so e^{i2pi kz sz} is
+          // advanced by e^{i2pi sz} (the reference's ei_inc recursion)
+          double2 e = REC ? A.ez[(size_t)(skz[0] + A.kzm) * A.natm + at] : make_double2(0.0, 0.0);
+          const double2 inc = REC ? A.ez[(size_t)(1 + A.kzm) * A.natm + at] : e;
 #pragma unroll 4
           for (int i = 0; i < len; ++i) {
             const int c = skz[i];
-            double2 e = A.ez[(size_t)(c + A.kzm) * A.natm + at];
+            if (!REC) e = A.ez[(size_t)(c + A.kzm) * A.natm + at];
             double2 tt = T[i];
             double rx = e.x * tt.x - e.y * tt.y;
             double ry = e.x * tt.y + e.y * tt.x;
@@ -317,6 +457,7 @@ __global__ void k_local_forces_lines(const double4* __restrict__ fterm,
             py += ry;
             qx += c * rx;
             qy += c * ry;
+            if (REC) e = make_double2(e.x * inc.x - e.y * inc.y, e.x * inc.y + e.y * inc.x);
           }
           double ip = u.x * py + u.y * px;  // Im(u P)
           double iq = u.x * qy + u.y * qx;  // Im(u Q)
@@ -556,6 +697,17 @@ int rho_init(cpstep_ctx* c, double box_len, double ecut_ry) {
     kxmax = std::max(kxmax, rp[0]);
   }
   int np = (int)kx.size();
+  // consecutive kz along every line: the Hartree / local passes then advance
+  // the z phase by one multiplication per point
+  {
+    bool ok = true;
+    for (int l = 0; l < nl && ok; ++l) {
+      const int e = l + 1 < nl ? off[l + 1] : np;
+      for (int q = off[l]; q + 1 < e; ++q)
+        if (kz[q + 1] != kz[q] + 1) ok = false;
+    }
+    c->rg.kz_runs = ok ? 1 : 0;
+  }
   std::vector<double> g2(np), wpt(np);
   const double* hi = c->hmati;
   for (int i = 0; i < np; ++i) {
@@ -820,13 +972,26 @@ int rho_hart(cpstep_ctx* c, double* energies, double* force) {
   rho::Atoms A = atoms_view(c);
   double ecut4 = 8.0 * (0.5 * c->ecut_ry);
   double* hp = r.part + 2 * r.nblk_xc;
-  const size_t hsm = sizeof(double2) * (size_t)c->atoms.natm;
-  if (hsm > 48 * 1024)
-    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(rho::k_hart_lines,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
-  rho::k_hart_lines<<<r.nlines, rho::HT, hsm, c->stream>>>(
-      r.rhog, r.line_off, r.nlines, r.kx, r.ky, r.kz, r.npts, c->d_hmati, c->vol, ecut4,
-      c->atoms.alp_ewd, A, r.vg, r.fterm, hp);
+  if (r.kz_runs) {
+    const size_t hsm = sizeof(double2) * (size_t)c->atoms.natm * (32 / rho::HG) * rho::HWARPS;
+    if (hsm > 48 * 1024)
+      CPSTEP_CUDA_TRY(cudaFuncSetAttribute(rho::k_hart_lines_rec,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)hsm));
+    const int nb = std::min(cdiv(r.nlines, (32 / rho::HG) * rho::HWARPS), 8 * c->num_sms);
+    rho::k_hart_lines_rec<<<nb, 32 * rho::HWARPS, hsm, c->stream>>>(
+        r.rhog, r.line_off, r.nlines, r.kx, r.ky, r.kz, r.npts, c->d_hmati, c->vol, ecut4,
+        c->atoms.alp_ewd, A, r.vg, r.fterm, hp);
+  } else {
+    const size_t hsm = sizeof(double2) * (size_t)c->atoms.natm;
+    if (hsm > 48 * 1024)
+      CPSTEP_CUDA_TRY(cudaFuncSetAttribute(rho::k_hart_lines,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)hsm));
+    rho::k_hart_lines<<<r.nlines, rho::HT, hsm, c->stream>>>(
+        r.rhog, r.line_off, r.nlines, r.kx, r.ky, r.kz, r.npts, c->d_hmati, c->vol, ecut4,
+        c->atoms.alp_ewd, A, r.vg, r.fterm, hp);
+  }
   CPSTEP_LAUNCH_CHECK();
   rho::k_sum_cols<<<3, 256, 0, c->stream>>>(hp, r.nlines, 3, energies + CPSTEP_E_HART, 1.0);
   CPSTEP_LAUNCH_CHECK();
@@ -841,13 +1006,13 @@ int rho_hart(cpstep_ctx* c, double* energies, double* force) {
     const int nt = std::max(32, cdiv(cdiv(natm, per), 32) * 32);
     const int lmax = c->nz + 1;
     const size_t fsm = (sizeof(double2) * c->atoms.ntyp + sizeof(int)) * (size_t)lmax;
+    auto kf = r.kz_runs ? rho::k_local_forces_lines<true> : rho::k_local_forces_lines<false>;
     if (fsm > 48 * 1024)
-      CPSTEP_CUDA_TRY(cudaFuncSetAttribute(rho::k_local_forces_lines,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+      CPSTEP_CUDA_TRY(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)fsm));
-    rho::k_local_forces_lines<<<c->atoms.nfblk, nt, fsm, c->stream>>>(
-        r.fterm, r.line_off, r.nlines, r.kx, r.ky, r.kz, r.npts, c->d_hmati, c->vol, A, lmax,
-        c->atoms.fpart);
+    kf<<<c->atoms.nfblk, nt, fsm, c->stream>>>(r.fterm, r.line_off, r.nlines, r.kx, r.ky, r.kz,
+                                               r.npts, c->d_hmati, c->vol, A, lmax,
+                                               c->atoms.fpart);
     CPSTEP_LAUNCH_CHECK();
     rho::k_sum_cols<<<3 * natm, 256, 0, c->stream>>>(c->atoms.fpart, c->atoms.nfblk, 3 * natm,
                                                      force, 1.0);
