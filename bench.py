@@ -249,6 +249,18 @@ def run_ours(args, cfg, name, rank, ws, dist):
         # the same number of steps from the same input in both precisions
         last = (energies.cpu().numpy().copy(), forces.cpu().numpy().copy(),
                 1 + args.warmup + args.steps, ctx.dyn_status()[1])
+        # the local error after those steps: one step of each precision from
+        # the FP64 state (psi, v, the carried constraint state, the chains)
+        it_n = 2 + args.warmup + args.steps
+        if prec == "fp64":
+            snap = dict(psi=psi.clone(), v=v.clone(), dyn=ctx.dyn_state(),
+                        nhc=ctx.cp_thermostat_state())
+            p1, v1 = snap["psi"].clone(), snap["v"].clone()
+            ctx.cp_step(p1, v1, occ, DT, it_n, energies, forces)
+            local = (energies.cpu().numpy().copy(), forces.cpu().numpy().copy())
+            del p1, v1
+        else:
+            local = None  # after this context's other runs, below
         clocks = clk.stop() if prec == "mixed" else None
         ms = e0.elapsed_time(e1)
         ms = max_over_ranks(ms, dist)
@@ -269,7 +281,7 @@ def run_ours(args, cfg, name, rank, ws, dist):
         it2, ok2 = ctx.step_status()
         norb_dev, resets = ctx.dyn_status()
         out[prec] = dict(ms=ms, launches=launches, clocks=clocks, phase=phase, first=first,
-                         ortho_ok=ok2, ortho_iters=it2, graph=graph, last=last,
+                         ortho_ok=ok2, ortho_iters=it2, graph=graph, last=last, local=local,
                          psiv_resets=resets, norb_dev_last=norb_dev)
         if prec == "mixed":
             # e2e: the reference-facing host-buffer call (positions in, energies/forces out)
@@ -296,6 +308,13 @@ def run_ours(args, cfg, name, rank, ws, dist):
                               d2h=he.numel() * 8 + hf.numel() * 8)
         if prec == "mixed":
             out["pc_us"] = pc_kernel_times(ctx, psi, v)
+        if prec == "mixed":  # the mixed half of the local error (it replaces the carried state)
+            ctx.dyn_state(*snap["dyn"])
+            ctx.cp_thermostat_state(*snap["nhc"])
+            p1, v1 = snap["psi"].clone(), snap["v"].clone()
+            ctx.cp_step(p1, v1, occ, DT, it_n, energies, forces)
+            out[prec]["local"] = (energies.cpu().numpy().copy(), forces.cpu().numpy().copy())
+            del p1, v1, snap
         nl, _ = ctx.info()
         out.setdefault("nlines", nl)
         out.setdefault("npts_d", ctx.rho_layout()[0].shape[0])
@@ -741,7 +760,12 @@ def main():
                                                              fp64["last"][0][8]) / sysm.natm,
                              "local_force_Ha_per_bohr_after": float(np.max(np.abs(
                                  mixed["last"][1] - fp64["last"][1]))),
-                             "psiv_resets_mixed_fp64": [mixed["last"][3], fp64["last"][3]]},
+                             "psiv_resets_mixed_fp64": [mixed["last"][3], fp64["last"][3]],
+                             "one_step_from_the_fp64_state_after": mixed["last"][2],
+                             "energy_Ha_per_atom_one_step": abs(mixed["local"][0][8] -
+                                                                fp64["local"][0][8]) / sysm.natm,
+                             "local_force_Ha_per_bohr_one_step": float(np.max(np.abs(
+                                 mixed["local"][1] - fp64["local"][1])))},
         "phase_ms_mixed": {"density": ph[0], "vks": ph[1], "vpsi_kinetic": ph[2],
                            "lambda": ph[3], "integrate": ph[4], "ortho_psiT": ph[5],
                            "ees_nonlocal": ph[6]},

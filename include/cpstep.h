@@ -637,10 +637,13 @@ CPSTEP_API int cpstep_cp_step_host(cpstep_ctx* ctx, double* d_psi, double* d_vps
  * elsewhere give the reference's S and lambda) or NULL for all 1;
  * stream: a cudaStream_t or NULL.
  * The first call on a device looks the array's device address up
- * (cudaGetSymbolAddress) with that device current: make it before any stream
- * capture.  Every call uses the same array: two calls that can run at the
- * same time on the GPU (other streams, other host threads) race and must be
- * serialised by the caller.
+ * (cudaGetSymbolAddress) with that device current, and so does the first call
+ * after the device's current context has changed (its unique ID, cuCtxGetId,
+ * is compared on every call: a cudaDeviceReset or a primary-context reset by
+ * the application makes a new context with its own copy of the array): make
+ * those calls before any stream capture.  Every call uses the same array: two
+ * calls that can run at the same time on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller.
  */
 CPSTEP_API int cpstep_pc_overlap_noalloc(const double* d_a, const double* d_b, int na, int nb,
                                          int npts, const double* d_w, double alpha,

@@ -320,7 +320,9 @@ int atom_nvt_set(cpstep_ctx* c, int len, int nres, int nyosh, const double* h_kT
     return CPSTEP_ERR_ARG;
   }
   AtomNvt& t = c->atom_nvt;
-  t.len = len; t.nres = nres; t.nyosh = nyosh; t.natm = n;
+  // t.len is published last: a failed allocation or copy leaves the NVE branch
+  // selected (the buffers made so far are released by the next atom_nvt_free)
+  t.nres = nres; t.nyosh = nyosh; t.natm = n;
   CPSTEP_CUDA_TRY(cudaMalloc(&t.d_kT, sizeof(double) * n));
   CPSTEP_CUDA_TRY(cudaMalloc(&t.d_mnhc, sizeof(double) * n * len));
   CPSTEP_CUDA_TRY(cudaMalloc(&t.d_vn, sizeof(double) * n * 3 * len));
@@ -331,6 +333,7 @@ int atom_nvt_set(cpstep_ctx* c, int len, int nres, int nyosh, const double* h_kT
   CPSTEP_CUDA_TRY(cudaMemset(t.d_vn, 0, sizeof(double) * n * 3 * len));
   CPSTEP_CUDA_TRY(cudaMemset(t.d_pkt, 0, sizeof(double) * n));
   CPSTEP_CUDA_TRY(cudaMemset(t.d_e, 0, sizeof(double) * 2));
+  t.len = len;
   return CPSTEP_OK;
 }
 

@@ -343,7 +343,8 @@ int nhc_set(cpstep_ctx* c, double te_ext, double tau_fs, int num, int nck, int n
     return CPSTEP_ERR_ARG;
   }
   CpNhc& t = c->nhc;
-  t.on = 1;
+  // t.on is published last: a failed allocation or copy leaves the thermostat
+  // off (the buffers made so far are released by the next nhc_free)
   t.num = num; t.nck = nck; t.nres = nres; t.nyosh = nyosh;
   const double kT = te_ext / 315777.0, tau = tau_fs / 0.0241888;  // BOLTZ, TIME_CONV
   const double degfree = (double)(2 * ncoef - nzero), pre = tau * tau * kT;
@@ -381,6 +382,7 @@ int nhc_set(cpstep_ctx* c, double te_ext, double tau_fs, int num, int nck, int n
   CPSTEP_CUDA_TRY(cudaMalloc(&t.d_part, sizeof(double) * (size_t)c->nstates * t.nsplit * nck));
   CPSTEP_CUDA_TRY(cudaMalloc(&t.d_scale, sizeof(double) * 2 * (size_t)c->nstates * nck));
   CPSTEP_CUDA_TRY(cudaMalloc(&t.d_eout, sizeof(double) * 3 * (size_t)c->nstates * nck));
+  t.on = 1;
   return CPSTEP_OK;
 }
 

@@ -17,6 +17,7 @@
 // reduction of the partial tiles, so results are deterministic.
 #include <algorithm>
 #include <mutex>
+#include <cuda.h>
 #include "ctx.cuh"
 
 namespace pcalc {
@@ -478,8 +479,36 @@ static __device__ __align__(256) double g_noalloc_part[CPSTEP_NOALLOC_PART_DOUBL
 
 namespace {
 std::mutex g_noalloc_mu;
-double* g_noalloc_addr[64] = {};  // device address of the array, per device
+double* g_noalloc_addr[64] = {};            // device address of the array, per device
+unsigned long long g_noalloc_ctx[64] = {};  // unique ID of the context it was looked up in
 int g_noalloc_sms[64] = {};
+
+// Unique ID of the calling thread's current context (cuCtxGetId: never reused
+// within a process), 0 when none is current.  The driver entry points come
+// through the runtime, so the library does not link the driver library.
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext*);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long*);
+unsigned long long current_ctx_id() {
+  static PfnCtxGetCurrent get_cur = nullptr;
+  static PfnCtxGetId get_id = nullptr;
+  if (!get_cur || !get_id) {
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", reinterpret_cast<void**>(&get_cur),
+                                cudaEnableDefault, &q1) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", reinterpret_cast<void**>(&get_id),
+                                cudaEnableDefault, &q2) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      get_cur = nullptr;
+      get_id = nullptr;
+      return 0;
+    }
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_cur(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 }  // namespace
 
 extern "C" int cpstep_pc_overlap_noalloc(const double* d_a, const double* d_b, int na, int nb,
@@ -506,13 +535,17 @@ extern "C" int cpstep_pc_overlap_noalloc(const double* d_a, const double* d_b, i
   int nsm = 0;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-      // once per device, with that device current
+    const unsigned long long id = current_ctx_id();
+    if (!g_noalloc_addr[dev] || id == 0 || id != g_noalloc_ctx[dev]) {
+      // once per device and context, with that device current: the address
+      // is the array's copy in the current context (a reset of the device's
+      // primary context, cudaDeviceReset, makes a new one)
       void* addr = nullptr;
       CPSTEP_CUDA_TRY(cudaGetSymbolAddress(&addr, g_noalloc_part));
       int sms = 0;
       CPSTEP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
       g_noalloc_addr[dev] = static_cast<double*>(addr);
+      g_noalloc_ctx[dev] = current_ctx_id();
       g_noalloc_sms[dev] = sms > 0 ? sms : 148;
     }
     part = g_noalloc_addr[dev];

@@ -77,7 +77,8 @@ int cpstep_tune_get(const cpstep_ctx* c, int* vals, int n) {
   vals[1] = c->tune.plane_waves;
   vals[2] = c->tune.nl_blocks;
   vals[3] = c->tune.pc_split;
-  vals[4] = c->tc_ok;
+  // tensor cores: whether the products use them (only a mixed context does)
+  vals[4] = c->precision == CPSTEP_PREC_MIXED ? c->tc_ok : 0;
   vals[5] = c->tune.ees_gspace;
   return CPSTEP_OK;
 }

@@ -61,6 +61,36 @@ def test_noalloc_overlap_matches_context_entry_twice():
         ctx.close()
 
 
+@pytest.mark.parametrize("na,nb", [(1024, 1024), (1000, 1048)])
+def test_noalloc_at_its_scratch_limit(na, nb):
+    """Products just inside the fixed scratch (na nb <= 2^20): the split-K
+    width is bounded by the array there (one slab at 1024 x 1024), and every
+    partial tile must stay inside it."""
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    import torch
+    from openatom_b200.context import StepContext
+    from openatom_b200.layout import StateLayout
+    lay = StateLayout(9.0, 20.0)
+    g = torch.Generator(device="cpu").manual_seed(11)
+
+    def rnd(n):
+        return (torch.randn((n, lay.npts), generator=g, dtype=torch.float64)
+                + 1j * torch.randn((n, lay.npts), generator=g, dtype=torch.float64)).cuda()
+    a, b = rnd(na), rnd(nb)
+    w = torch.from_numpy(np.where(lay.kx == 0, 1.0, 2.0)).cuda()
+    ctx = StepContext(lay, max(na, nb), precision="fp64")
+    try:
+        ref = ctx.pc_overlap(a, b)
+        out = _noalloc(a, b, w, torch.zeros((nb, na), dtype=torch.float64, device="cuda"))
+        torch.cuda.synchronize()
+        r = ref.cpu().numpy()
+        assert np.max(np.abs(out.cpu().numpy() - r)) <= TOL * np.max(np.abs(r))
+        assert ctx.device_errors() == 0
+    finally:
+        ctx.close()
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     if not cuda_ok():
         pytest.skip("no CUDA device")
