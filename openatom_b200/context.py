@@ -261,8 +261,11 @@ class StepContext:
         return forces, e
 
     def atoms_integrate(self, itime, pos, vel, forces, mass, dt):
-        """NVE velocity-Verlet step of the ions (in place on pos, vel [natm, 3]);
-        the context's positions follow.  Returns E_kin at the step's start."""
+        """Velocity-Verlet step of the ions (in place on pos, vel [natm, 3]):
+        NVE, or the NVT branch with massive Nose-Hoover chains once
+        set_atom_thermostat has been called (the chains are applied around the
+        kicks on the device).  The context's positions follow.  Returns E_kin
+        at the step's start."""
         self._sync_stream()
         ek = torch.zeros(1, dtype=torch.float64, device=self.device)
         _lib.call("cpstep_atoms_integrate", self._h, int(itime), ptr(pos), ptr(vel), ptr(forces),
