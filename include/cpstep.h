@@ -327,6 +327,21 @@ CPSTEP_API int cpstep_ortho_tmat(cpstep_ctx* ctx, const double* d_s, double* d_t
  *   grid: d_vks += df/drho; d_gx, d_gy, d_gz (the density gradient on entry)
  *   <- unit(grad rho) df/d|grad rho|; d_energies[EXC_GGA] = E_GGA.  Points
  *   with an exactly zero gradient get zero there (the reference divides 0 by 0).
+ * cpstep_eext_grid_size: the EES grid of init_eext_ees
+ *   (interface/cp_ewald/set_cp_ewald.C:1419-1497) for a cubic box: the first
+ *   set_fftsizes entry >= int(2 scale (2 kmax + 1)) (+1 if below 2 (2 kmax + 1)),
+ *   kmax the states' largest |k| on an axis.  Returns the size, or -1.
+ * cpstep_set_local_ees: the EES form of cpstep_hart_eext (cp_eext_ees_opt on:
+ *   CP_Rho_RHartExt::computeAtmSF, CP_Rho_GHartExt::getHartEextEes,
+ *   CPLOCAL::eesAtmBsplineRgrp / eesPackGridRchare / eesHartEextGchare /
+ *   eesEwaldGchare / eesAtmForceRchare, cp_hart_ext.C:521-1470): the atoms'
+ *   structure factors interpolated by B-splines of order n_interp (8 is
+ *   built) on an ngrid^3 grid (cpstep_eext_grid_size) with the Euler weights
+ *   b(G); energies, vks(G) and atom forces as the reference computes them in
+ *   that form.  Applies to cpstep_hart_eext, cpstep_vks_from_rho and the step
+ *   until called with on = 0 (the explicit structure factors, the default).
+ *   Needs cpstep_set_atoms first; CPSTEP_ERR_ARG for another order or
+ *   ngrid < n_interp.
  * d_energies: device array of CPSTEP_NENERGY doubles; only the named slots are written.
  */
 CPSTEP_API int cpstep_set_atoms(cpstep_ctx* ctx, int natm, int ntyp, const int* typ,
@@ -344,6 +359,8 @@ CPSTEP_API int cpstep_vks_fft_g2r(cpstep_ctx* ctx, const double* d_vksg, double*
 CPSTEP_API int cpstep_vks_from_rho(cpstep_ctx* ctx, const double* d_rho_r, double* d_vks_r,
                                    double* d_energies, double* d_force);
 CPSTEP_API int cpstep_set_xc(cpstep_ctx* ctx, int functional, double gradient_cutoff);
+CPSTEP_API int cpstep_eext_grid_size(int kmax, double scale, int n_interp);
+CPSTEP_API int cpstep_set_local_ees(cpstep_ctx* ctx, int on, int ngrid, int n_interp);
 CPSTEP_API int cpstep_gga_functional(cpstep_ctx* ctx, const double* d_rho, double* d_gx,
                                      double* d_gy, double* d_gz, double* d_vks,
                                      double* d_energies);

@@ -76,6 +76,8 @@ SIGNATURES = {
     "cpstep_set_xc": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),
     "cpstep_gga_functional": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cpstep_nl_grid_size": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+    "cpstep_eext_grid_size": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+    "cpstep_set_local_ees": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "cpstep_set_nonlocal": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            _c_int_p, _c_int_p, _c_int_p, _c_dbl_p, _c_dbl_p,
                                            _c_dbl_p]),

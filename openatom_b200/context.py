@@ -310,6 +310,17 @@ class StepContext:
         _lib.call("cpstep_hart_eext", self._h, ptr(rhog), ptr(v), ptr(e), ptr(f))
         return v, e, f
 
+    def set_local_ees(self, on=True, ngrid=None, n_interp=8, scale=1.2):
+        """The EES form of the Hartree/local/Ewald pass (cp_eext_ees_opt): the
+        atoms' structure factors interpolated by order-n_interp B-splines on
+        an ngrid^3 grid (default: init_eext_ees's size for this layout and
+        scale).  on=False returns to the explicit structure factors."""
+        if on and ngrid is None:
+            ngrid = _lib.lib().cpstep_eext_grid_size(int(self.layout.kmax), float(scale),
+                                                     int(n_interp))
+        _lib.call("cpstep_set_local_ees", self._h, 1 if on else 0, int(ngrid or 0), int(n_interp))
+        return ngrid
+
     def vks_g2r(self, vksg):
         self._sync_stream()
         out = torch.empty((self.n, self.n, self.n), dtype=torch.float64, device=self.device)

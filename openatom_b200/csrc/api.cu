@@ -462,6 +462,17 @@ int cpstep_vks_from_rho(cpstep_ctx* c, const double* d_rho_r, double* d_vks_r,
   return rho_vks_r(c, d_vks_r);
 }
 
+int cpstep_eext_grid_size(int kmax, double scale, int n_interp) {
+  if (kmax < 0 || n_interp < 2) return -1;
+  return eext_grid_size(kmax, scale, n_interp);
+}
+
+int cpstep_set_local_ees(cpstep_ctx* c, int on, int ngrid, int n_interp) {
+  if (!c) return CPSTEP_ERR_ARG;
+  graph_drop(c);
+  return eesloc_set(c, on, ngrid, n_interp);
+}
+
 int cpstep_set_xc(cpstep_ctx* c, int functional, double gradient_cutoff) {
   if (!c || (functional != CPSTEP_XC_PZ_LDA && functional != CPSTEP_XC_BLYP))
     return CPSTEP_ERR_ARG;

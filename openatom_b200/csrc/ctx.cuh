@@ -152,6 +152,7 @@ struct CpNhc {
   double* d_part = nullptr;       // [S][nsplit][nck]
   double* d_scale = nullptr;      // [S][nck][2]
   double* d_eout = nullptr;       // [S][nck][3]
+  double* d_fm = nullptr;         // [npts] (dt/2) / cmass of the current step
 };
 
 // Massive Nose-Hoover chains of the atoms (cpstep_set_atom_thermostat).
@@ -220,6 +221,21 @@ struct NlData {
   int gspace_ok = 0;                // every type has at most 4 channels
 };
 
+// EES form of the Hartree + local + Ewald pass (cpstep_set_local_ees, the
+// reference's cp_eext_ees_opt): the atoms' B-splines on the EES grid and their
+// separable transforms with the EES weights folded in, per axis d and atom a,
+//   t_d[k][a] = bden_d(k) sum_j Mn_d[a][j] e^{+2 pi i k ig_d[a][j] / ngrid}
+// and dt_d the same sum of dMn, over the density sphere's k extents.
+struct EesLocal {
+  int on = 0, ngrid = 0, natm = 0;
+  int* ig = nullptr;                // [natm][3][8]
+  double *mn = nullptr, *dmn = nullptr;
+  double2* bden = nullptr;          // [ngrid] get_bspline_wght1d
+  double2 *tx = nullptr, *ty = nullptr, *tz = nullptr;     // [k][natm]
+  double2 *dtx = nullptr, *dty = nullptr, *dtz = nullptr;
+  double2* tzt = nullptr;           // [type-order rank][2 kzm + 1]
+};
+
 template <typename T>
 struct Twiddles {
   cplx<T>* x = nullptr;
@@ -252,6 +268,7 @@ struct cpstep_ctx {
   StateFftOps ops64;  // FP64 (density path)
   RhoGeom rg;
   AtomData atoms;
+  EesLocal eloc;
   NlData nl;
   SfData sf;
   CpNhc nhc;
@@ -407,6 +424,14 @@ int sf_run(cpstep_ctx* c, const double* psi, const double* occ, double* fpsi, do
 int nl_run(cpstep_ctx* c, const double* psi, const double* occ, double* fpsi, double* energies,
            double* fatm);
 int nl_grid_size(int kmax, double scale, int n_interp);
+int eext_grid_size(int kmax, double scale, int n_interp);
+// eesAtmBsplineRgrp's indices, Mn and dMn of every atom on an nkf grid
+// (order kNlInterp) from fractional coordinates [natm][3]
+int ees_bspline_launch(cpstep_ctx* c, const double* frac, int natm, int nkf, int* ig, double* mn,
+                       double* dmn);
+// get_bspline_wght1d: the complex EES weights of one axis, m = 0 .. ngrid-1
+void ees_bspline_weights(int n_interp, int ngrid, std::vector<double>& br,
+                         std::vector<double>& bi);
 
 // rhopath.cu
 int rho_init(cpstep_ctx* c, double box_len, double ecut_ry);
@@ -426,6 +451,8 @@ int atoms_integrate(cpstep_ctx* c, int itime, double* pos, double* vel, const do
 int rho_gga_functional(cpstep_ctx* c, const double* rho_r, double* gx, double* gy, double* gz,
                        double* vks_r, double* energies, int add_to_exc);
 int rho_hart(cpstep_ctx* c, double* energies, double* force);
+int eesloc_set(cpstep_ctx* c, int on, int ngrid, int n_interp);
+void eesloc_free(cpstep_ctx* c);
 int rho_vks_r(cpstep_ctx* c, double* vks_r);
 int rho_conj_scale(cpstep_ctx* c, const double* in, double* out, int n, double s);
 

@@ -427,6 +427,18 @@ int wrap(int v, int n) { return v < 0 ? v + n : v; }
 
 }  // namespace
 
+void ees_bspline_weights(int n_interp, int ngrid, std::vector<double>& br,
+                         std::vector<double>& bi) {
+  bspline_wght1d(n_interp, ngrid, br, bi);
+}
+
+int ees_bspline_launch(cpstep_ctx* c, const double* frac, int natm, int nkf, int* ig, double* mn,
+                       double* dmn) {
+  ees::k_nl_bspline<<<cdiv(natm, 128), 128, 0, c->stream>>>(frac, natm, nkf, ig, mn, dmn);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
 void nl_free(cpstep_ctx* c) {
   NlData& n = c->nl;
   cudaFree(n.dyp); cudaFree(n.line_zneg); cudaFree(n.line_zpos); cudaFree(n.line_xy);

@@ -243,6 +243,17 @@ int nl_grid_size(int kmax, double scale, int n_interp) {
   return nl_grid_size_of(kmax, scale, n_interp);
 }
 
+// init_eext_ees (set_cp_ewald.C:1419-1497), one axis: the same rule on the
+// density sphere's 2 (2 kmax + 1)
+int eext_grid_size(int kmax, double scale, int n_interp) {
+  const int nk = 2 * kmax + 1;
+  int nkf = (int)(2.0 * scale * (double)nk);
+  if (nkf < 2 * nk) ++nkf;
+  for (int k : kFftSizes)
+    if (k >= nkf) return k >= n_interp ? k : -1;
+  return -1;
+}
+
 extern "C" int cpstep_layout_sizes(double box_len, double ecut_ry, int* kmax, int* nfft,
                                    int* nktot_half, int* npts) {
   if (!(box_len > 0) || !(ecut_ry > 0)) {

@@ -479,6 +479,182 @@ __global__ void k_local_forces_lines(const double4* __restrict__ fterm,
 }
 
 // out[c] = scale * sum_r part[r][c]; one block per column, fixed order.
+// ---------------------------------------------------------------------------
+// The EES form of the pass (cp_eext_ees_opt; CPLOCAL::eesAtmBsplineRgrp,
+// eesPackGridRchare, eesHartEextGchare, eesEwaldGchare, eesAtmForceRchare,
+// cp_hart_ext.C:641-1470).  The reference spreads each type's atoms onto the
+// EES grid with their B-splines, transforms the grid to G, forms
+// S_t(G) b(G) and the energies per point, transforms the per-type and Ewald
+// terms back and gathers the forces through the B-spline derivatives.  The
+// spread grid of one atom is a tensor product of three 1-D stencils, so its
+// transform at G is the product of three 1-D sums, and with b(G) separable
+// too, S_t(G) b(G) = sum_{a in t} t_x[a](kx) t_y[a](ky) t_z[a](kz): the same
+// form as the explicit structure factor with the exact phases replaced by
+// the tables of EesLocal.  k_hart_lines runs on those tables unchanged; the
+// gather becomes, per atom, sum_G Re(T(G) D_a(G)) with D_a the derivative
+// tables' products (k_eloc_forces_lines).  No 3-D grid or transform is formed.
+
+// t_d / dt_d of every (atom, axis, k): the 8 stencil terms of one axis
+__global__ void k_eloc_tables(const int* __restrict__ ig, const double* __restrict__ mn,
+                              const double* __restrict__ dmn, int natm, int ngrid, int kxm,
+                              int kym, int kzm, const double2* __restrict__ bden,
+                              const int* __restrict__ rank, double2* __restrict__ tx,
+                              double2* __restrict__ ty, double2* __restrict__ tz,
+                              double2* __restrict__ dtx, double2* __restrict__ dty,
+                              double2* __restrict__ dtz, double2* __restrict__ tzt) {
+  const int nx = kxm + 1, ny = 2 * kym + 1, nz = 2 * kzm + 1;
+  const int per = nx + ny + nz;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)natm * per) return;
+  const int a = (int)(i / per);
+  const int r = (int)(i % per);
+  int d, k, slot;
+  if (r < nx) {
+    d = 0; slot = r; k = r;
+  } else if (r < nx + ny) {
+    d = 1; slot = r - nx; k = slot - kym;
+  } else {
+    d = 2; slot = r - nx - ny; k = slot - kzm;
+  }
+  const int* g = ig + ((size_t)a * 3 + d) * kNlInterp;
+  const double* m = mn + ((size_t)a * 3 + d) * kNlInterp;
+  const double* dm = dmn + ((size_t)a * 3 + d) * kNlInterp;
+  double sr = 0.0, si = 0.0, dr = 0.0, di = 0.0;
+#pragma unroll
+  for (int j = 0; j < kNlInterp; ++j) {
+    long long t = ((long long)k * g[j]) % ngrid;
+    if (t < 0) t += ngrid;
+    double sn, cs;
+    sincospi(2.0 * (double)t / (double)ngrid, &sn, &cs);
+    sr += m[j] * cs;
+    si += m[j] * sn;
+    dr += dm[j] * cs;
+    di += dm[j] * sn;
+  }
+  const double2 b = bden[((k % ngrid) + ngrid) % ngrid];
+  const double2 tv = make_double2(sr * b.x - si * b.y, sr * b.y + si * b.x);
+  const double2 dv = make_double2(dr * b.x - di * b.y, dr * b.y + di * b.x);
+  const size_t o = (size_t)slot * natm + a;
+  if (d == 0) {
+    tx[o] = tv;
+    dtx[o] = dv;
+  } else if (d == 1) {
+    ty[o] = tv;
+    dty[o] = dv;
+  } else {
+    tz[o] = tv;
+    dtz[o] = dv;
+    tzt[(size_t)rank[a] * nz + slot] = tv;
+  }
+}
+
+// G = 0 (eesHartEextGchare :1175-1205): vext(0) = sum_a gzvps/vol Re(S b)(0)
+__global__ void k_eloc_g0(const double2* __restrict__ rhog_t, int izero, double vol, Atoms A,
+                          double2* __restrict__ vg_t, double* __restrict__ eext) {
+  double v = 0.0;
+  for (int a = 0; a < A.natm; ++a) {
+    const double2 x = A.ex[a];
+    const double2 y = A.ey[(size_t)A.kym * A.natm + a];
+    const double2 z = A.ez[(size_t)A.kzm * A.natm + a];
+    const double xyr = x.x * y.x - x.y * y.y, xyi = x.x * y.y + x.y * y.x;
+    v += A.gzvps[A.typ[a]] * (xyr * z.x - xyi * z.y);
+  }
+  v /= vol;
+  vg_t[izero] = make_double2(v, 0.0);
+  *eext += v * rhog_t[izero].x;
+}
+
+// Atom forces of the EES form, line by line as k_local_forces_lines: with T
+// the per-point term (local and Ewald, as there) and, for atom a on line
+// (kx, ky), u0 = t_x t_y, ux = dt_x t_y, uy = t_x dt_y,
+//   F_a = -N sum_kz Re(T(G) [(h_r0 ux + h_r1 uy) t_z(kz) + h_r2 u0 dt_z(kz)])
+// per Cartesian row r of hmati: the dMn_x/y/z of eesAtmBsplineRgrp IV
+// (dMn grid hmati) summed against the back-transformed terms.
+struct ElocD {
+  const double2 *dtx, *dty, *dtz;
+  double grid;
+};
+__global__ void k_eloc_forces_lines(const double4* __restrict__ fterm,
+                                    const int* __restrict__ line_off, int nlines,
+                                    const int* __restrict__ kx, const int* __restrict__ ky,
+                                    const int* __restrict__ kz, int npts,
+                                    const double* __restrict__ hmati, double vol, Atoms A,
+                                    ElocD D, int lmax, double* __restrict__ fpart) {
+  extern __shared__ double2 sT[];  // [ntyp][lmax] T, then int kz[lmax]
+  int* skz = reinterpret_cast<int*>(sT + (size_t)A.ntyp * lmax);
+  const double tpi = 2.0 * M_PI, rvol = 1.0 / vol;
+  double f[4][3] = {};
+  const int nper = (A.natm + blockDim.x - 1) / blockDim.x;
+  for (int l = blockIdx.x; l < nlines; l += gridDim.x) {
+    const int off = line_off[l], end = (l + 1 < nlines) ? line_off[l + 1] : npts;
+    const int a = kx[off], b = ky[off];
+    const double g0x = tpi * (a * hmati[0] + b * hmati[1]);
+    const double g0y = tpi * (a * hmati[3] + b * hmati[4]);
+    const double g0z = tpi * (a * hmati[6] + b * hmati[7]);
+    for (int c0 = off; c0 < end; c0 += lmax) {
+      const int len = min(lmax, end - c0);
+      __syncthreads();
+      for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        const int p = c0 + i;
+        const int c = kz[p];
+        skz[i] = c;
+        double4 ft = fterm[p];
+        double gx = g0x + c * tpi * hmati[2], gy = g0y + c * tpi * hmati[5];
+        double gz = g0z + c * tpi * hmati[8];
+        double g = sqrt(gx * gx + gy * gy + gz * gz);
+        for (int t = 0; t < A.ntyp; ++t) {
+          double vt = (ft.x != 0.0 || ft.y != 0.0) ? vps_at(A, t, g, rvol) : 0.0;
+          double qt = A.q[t];
+          sT[(size_t)t * lmax + i] = make_double2(ft.x * vt + ft.z * qt, -(ft.y * vt + ft.w * qt));
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int at = threadIdx.x + k * blockDim.x;
+        if (k < nper && at < A.natm) {
+          const int t = A.typ[at];
+          const double2 x = A.ex[(size_t)a * A.natm + at];
+          const double2 y = A.ey[(size_t)(b + A.kym) * A.natm + at];
+          const double2 dx = D.dtx[(size_t)a * A.natm + at];
+          const double2 dy = D.dty[(size_t)(b + A.kym) * A.natm + at];
+          const double2 u0 = make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
+          const double2 ux = make_double2(dx.x * y.x - dx.y * y.y, dx.x * y.y + dx.y * y.x);
+          const double2 uy = make_double2(x.x * dy.x - x.y * dy.y, x.x * dy.y + x.y * dy.x);
+          const double2* T = sT + (size_t)t * lmax;
+          double px = 0.0, py = 0.0, qx = 0.0, qy = 0.0;
+#pragma unroll 4
+          for (int i = 0; i < len; ++i) {
+            const int cz = skz[i] + A.kzm;
+            const double2 z = A.ez[(size_t)cz * A.natm + at];
+            const double2 dz = D.dtz[(size_t)cz * A.natm + at];
+            const double2 tt = T[i];
+            px += tt.x * z.x - tt.y * z.y;
+            py += tt.x * z.y + tt.y * z.x;
+            qx += tt.x * dz.x - tt.y * dz.y;
+            qy += tt.x * dz.y + tt.y * dz.x;
+          }
+#pragma unroll
+          for (int r = 0; r < 3; ++r) {
+            const double h0 = hmati[3 * r], h1 = hmati[3 * r + 1], h2 = hmati[3 * r + 2];
+            const double wx = h0 * ux.x + h1 * uy.x, wy = h0 * ux.y + h1 * uy.y;
+            const double re = (wx * px - wy * py) + h2 * (u0.x * qx - u0.y * qy);
+            f[k][r] -= D.grid * re;
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int at = threadIdx.x + k * blockDim.x;
+    if (k < nper && at < A.natm) {
+      double* o = fpart + ((size_t)blockIdx.x * A.natm + at) * 3;
+      o[0] = f[k][0]; o[1] = f[k][1]; o[2] = f[k][2];
+    }
+  }
+}
+
 __global__ void k_sum_cols(const double* __restrict__ part, int nrow, int ncol,
                            double* __restrict__ out, double scale) {
   __shared__ double red[32];
@@ -756,6 +932,7 @@ void rho_free(cpstep_ctx* c) {
   c->d_gga_r = nullptr;
   c->d_gga_g = nullptr;
   cudaFree(c->d_energies);
+  eesloc_free(c);
   AtomData& a = c->atoms;
   cudaFree(a.typ); cudaFree(a.frac); cudaFree(a.q); cudaFree(a.vps); cudaFree(a.gzvps);
   cudaFree(a.ex); cudaFree(a.ey); cudaFree(a.ez); cudaFree(a.ezt); cudaFree(a.rank);
@@ -774,6 +951,8 @@ FftJob rho_job(const cpstep_ctx* c) {
   j.pen_b = r.pen_b;
   return j;
 }
+
+static int eesloc_alloc(cpstep_ctx* c);
 
 int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* pos,
               const double* q, int nspl, double gmin, double dg, const double* vps,
@@ -840,6 +1019,7 @@ int atoms_set(cpstep_ctx* c, int natm, int ntyp, const int* typ, const double* p
   CPSTEP_LAUNCH_CHECK();
   if (!c->d_hmati) CPSTEP_CUDA_TRY(cudaMalloc(&c->d_hmati, sizeof(double) * 9));
   CPSTEP_CUDA_TRY(cudaMemcpy(c->d_hmati, c->hmati, sizeof(double) * 9, cudaMemcpyHostToDevice));
+  if (c->eloc.on) return eesloc_alloc(c);  // the EES form's tables follow the atoms
   return CPSTEP_OK;
 }
 
@@ -962,6 +1142,124 @@ int rho_gga(cpstep_ctx* c, const double* rho_r, double* vks_r, double* energies)
   return CPSTEP_OK;
 }
 
+void eesloc_free(cpstep_ctx* c) {
+  EesLocal& e = c->eloc;
+  cudaFree(e.ig); cudaFree(e.mn); cudaFree(e.dmn); cudaFree(e.bden);
+  cudaFree(e.tx); cudaFree(e.ty); cudaFree(e.tz); cudaFree(e.dtx); cudaFree(e.dty);
+  cudaFree(e.dtz); cudaFree(e.tzt);
+  e = EesLocal();
+}
+
+// buffers of the EES form for the context's atoms and sphere extents
+static int eesloc_alloc(cpstep_ctx* c) {
+  EesLocal& e = c->eloc;
+  const AtomData& a = c->atoms;
+  const int ng = e.ngrid, natm = a.natm;
+  cudaFree(e.ig); cudaFree(e.mn); cudaFree(e.dmn);
+  cudaFree(e.tx); cudaFree(e.ty); cudaFree(e.tz); cudaFree(e.dtx); cudaFree(e.dty);
+  cudaFree(e.dtz); cudaFree(e.tzt);
+  const size_t nb = (size_t)natm * 3 * kNlInterp;
+  const size_t nx = (size_t)(a.kxm + 1) * natm, ny = (size_t)(2 * a.kym + 1) * natm;
+  const size_t nz = (size_t)(2 * a.kzm + 1) * natm;
+  CPSTEP_CUDA_TRY(cudaMalloc(&e.ig, sizeof(int) * nb));
+  CPSTEP_CUDA_TRY(cudaMalloc(&e.mn, sizeof(double) * nb));
+  CPSTEP_CUDA_TRY(cudaMalloc(&e.dmn, sizeof(double) * nb));
+  CPSTEP_CUDA_TRY(cudaMalloc(&e.tx, sizeof(double2) * nx));
+  CPSTEP_CUDA_TRY(cudaMalloc(&e.dtx, sizeof(double2) * nx));
+  CPSTEP_CUDA_TRY(cudaMalloc(&e.ty, sizeof(double2) * ny));
+  CPSTEP_CUDA_TRY(cudaMalloc(&e.dty, sizeof(double2) * ny));
+  CPSTEP_CUDA_TRY(cudaMalloc(&e.tz, sizeof(double2) * nz));
+  CPSTEP_CUDA_TRY(cudaMalloc(&e.dtz, sizeof(double2) * nz));
+  CPSTEP_CUDA_TRY(cudaMalloc(&e.tzt, sizeof(double2) * nz));
+  e.natm = natm;
+  (void)ng;
+  return CPSTEP_OK;
+}
+
+// cpstep_set_local_ees: on = 1 computes the pass in the EES form on an
+// ngrid^3 grid with B-splines of order n_interp (kNlInterp only), on = 0
+// returns to the explicit structure factors.
+int eesloc_set(cpstep_ctx* c, int on, int ngrid, int n_interp) {
+  if (!on) {
+    eesloc_free(c);
+    return CPSTEP_OK;
+  }
+  if (c->atoms.natm <= 0) {
+    cpstep_set_error("set_local_ees: set the atoms first (cpstep_set_atoms)");
+    return CPSTEP_ERR_STATE;
+  }
+  if (n_interp != kNlInterp || ngrid < n_interp) {
+    cpstep_set_error("set_local_ees: B-spline order %d on a %d grid (order %d is built, grid >= "
+                     "order)", n_interp, ngrid, kNlInterp);
+    return CPSTEP_ERR_ARG;
+  }
+  eesloc_free(c);
+  EesLocal& e = c->eloc;
+  e.ngrid = ngrid;
+  std::vector<double> br, bi;
+  ees_bspline_weights(n_interp, ngrid, br, bi);
+  std::vector<double2> h(ngrid);
+  for (int m = 0; m < ngrid; ++m) h[m] = make_double2(br[m], bi[m]);
+  CPSTEP_CUDA_TRY(cudaMalloc(&e.bden, sizeof(double2) * ngrid));
+  CPSTEP_CUDA_TRY(cudaMemcpy(e.bden, h.data(), sizeof(double2) * ngrid, cudaMemcpyHostToDevice));
+  if (int rc = eesloc_alloc(c)) return rc;
+  e.on = 1;  // published last: the pass reads the form from here
+  return CPSTEP_OK;
+}
+
+// the EES form of rho_hart
+static int eesloc_hart(cpstep_ctx* c, double* energies, double* force) {
+  RhoGeom& r = c->rg;
+  EesLocal& e = c->eloc;
+  const AtomData& ad = c->atoms;
+  if (e.natm != ad.natm)
+    if (int rc = eesloc_alloc(c)) return rc;
+  const int natm = ad.natm;
+  if (int rc = ees_bspline_launch(c, ad.frac, natm, e.ngrid, e.ig, e.mn, e.dmn)) return rc;
+  const long long nt = (long long)natm * ((ad.kxm + 1) + (2 * ad.kym + 1) + (2 * ad.kzm + 1));
+  rho::k_eloc_tables<<<(unsigned)((nt + 127) / 128), 128, 0, c->stream>>>(
+      e.ig, e.mn, e.dmn, natm, e.ngrid, ad.kxm, ad.kym, ad.kzm, e.bden, ad.rank, e.tx, e.ty,
+      e.tz, e.dtx, e.dty, e.dtz, e.tzt);
+  CPSTEP_LAUNCH_CHECK();
+  rho::Atoms A = atoms_view(c);
+  A.ex = e.tx; A.ey = e.ty; A.ez = e.tz; A.ezt = e.tzt;
+  const double ecut4 = 8.0 * (0.5 * c->ecut_ry);
+  double* hp = r.part + 2 * r.nblk_xc;
+  const size_t hsm = sizeof(double2) * (size_t)natm;
+  if (hsm > 48 * 1024)
+    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(rho::k_hart_lines,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
+  rho::k_hart_lines<<<r.nlines, rho::HT, hsm, c->stream>>>(
+      r.rhog, r.line_off, r.nlines, r.kx, r.ky, r.kz, r.npts, c->d_hmati, c->vol, ecut4,
+      ad.alp_ewd, A, r.vg, r.fterm, hp);
+  CPSTEP_LAUNCH_CHECK();
+  rho::k_sum_cols<<<3, 256, 0, c->stream>>>(hp, r.nlines, 3, energies + CPSTEP_E_HART, 1.0);
+  CPSTEP_LAUNCH_CHECK();
+  if (c->rho_izero >= 0) {
+    rho::k_eloc_g0<<<1, 1, 0, c->stream>>>(r.rhog, c->rho_izero, c->vol, A, r.vg,
+                                           energies + CPSTEP_E_EXT);
+    CPSTEP_LAUNCH_CHECK();
+  }
+  if (force) {
+    const int per = cdiv(natm, 256);
+    const int nthr = std::max(32, cdiv(cdiv(natm, per), 32) * 32);
+    const int lmax = c->nz + 1;
+    const size_t fsm = (sizeof(double2) * ad.ntyp + sizeof(int)) * (size_t)lmax;
+    if (fsm > 48 * 1024)
+      CPSTEP_CUDA_TRY(cudaFuncSetAttribute(rho::k_eloc_forces_lines,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)fsm));
+    rho::ElocD D{e.dtx, e.dty, e.dtz, (double)e.ngrid};
+    rho::k_eloc_forces_lines<<<ad.nfblk, nthr, fsm, c->stream>>>(
+        r.fterm, r.line_off, r.nlines, r.kx, r.ky, r.kz, r.npts, c->d_hmati, c->vol, A, D, lmax,
+        ad.fpart);
+    CPSTEP_LAUNCH_CHECK();
+    rho::k_sum_cols<<<3 * natm, 256, 0, c->stream>>>(ad.fpart, ad.nfblk, 3 * natm, force, 1.0);
+    CPSTEP_LAUNCH_CHECK();
+  }
+  return CPSTEP_OK;
+}
+
 // Hartree + local + Ewald from r.rhog: conj(vks) in r.vg, energies, force terms
 int rho_hart(cpstep_ctx* c, double* energies, double* force) {
   RhoGeom& r = c->rg;
@@ -969,6 +1267,7 @@ int rho_hart(cpstep_ctx* c, double* energies, double* force) {
     cpstep_set_error("hart_eext: no atoms set (cpstep_set_atoms)");
     return CPSTEP_ERR_STATE;
   }
+  if (c->eloc.on) return eesloc_hart(c, energies, force);
   rho::Atoms A = atoms_view(c);
   double ecut4 = 8.0 * (0.5 * c->ecut_ry);
   double* hp = r.part + 2 * r.nblk_xc;

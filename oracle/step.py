@@ -131,10 +131,12 @@ def dyn_start(psi):
 
 
 def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None, xc="pz_lda",
-           nonlocal_sf=False):
+           nonlocal_sf=False, eext_ees=None):
     """Energies, V_KS, constrained-force input F and atom forces (local + Ewald,
     plus the EES non-local pass when nonlocal_on: addForces adds its psi force,
-    stateSlab.C:240-272).  xc = "blyp" takes the BLYP potential of oracle/xc.py."""
+    stateSlab.C:240-272).  xc = "blyp" takes the BLYP potential of oracle/xc.py.
+    eext_ees = the EES grid size runs the local pass in its EES form
+    (oracle/eext_ees.py, cp_eext_ees_opt)."""
     vol = sysm.box_len ** 3
     rho = OF.density(psi, lay, occ, vol, chunk=chunk)
     if xc == "blyp":
@@ -143,9 +145,15 @@ def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None, xc=
     else:
         vxc, exc, muxc = OD.pz_lda(rho, vol)
     rg = OD.rho_to_g(rho, dlay, vol)
-    vg, eh, ee, ew, floc = OD.hart_eext(rg, dlay.kx, dlay.ky, dlay.kz, sysm.box_len,
-                                       0.5 * sysm.ecut_ry, sysm.atoms_dict(), sysm.tab,
-                                       sysm.alp_ewd)
+    if eext_ees:
+        from . import eext_ees as OXE
+        vg, eh, ee, ew, floc = OXE.hart_eext_ees(rg, dlay.kx, dlay.ky, dlay.kz, sysm.box_len,
+                                                 0.5 * sysm.ecut_ry, sysm.atoms_dict(),
+                                                 sysm.tab, sysm.alp_ewd, eext_ees)
+    else:
+        vg, eh, ee, ew, floc = OD.hart_eext(rg, dlay.kx, dlay.ky, dlay.kz, sysm.box_len,
+                                           0.5 * sysm.ecut_ry, sysm.atoms_dict(), sysm.tab,
+                                           sysm.alp_ewd)
     vks = vxc + OD.vg_to_r(vg, dlay)
     fv = OF.vpsi_force(psi, vks, lay, occ, chunk=chunk)
     enl, fnl, fatm = 0.0, None, None
@@ -167,7 +175,8 @@ def forces(psi, occ, sysm, lay, dlay, chunk=16, nonlocal_on=False, nkf=None, xc=
 
 
 def cp_step(psi, v, occ, sysm, lay, dlay, cmass, dt, iteration, nonlocal_on=False, nkf=None,
-            xc="pz_lda", nonlocal_sf=False, nhc=None, form="ortho_t", dyn=None, tol_norb=0.003):
+            xc="pz_lda", nonlocal_sf=False, nhc=None, form="ortho_t", dyn=None, tol_norb=0.003,
+            eext_ees=None):
     """One step on the orthonormal coefficients psi.  nhc = (params, per-state
     chain states, nres, nyosh) of oracle/isokin.py runs the thermostatted
     integrator (the chain states are updated).  form "ortho_t" carries the
@@ -175,7 +184,7 @@ def cp_step(psi, v, occ, sysm, lay, dlay, cmass, dt, iteration, nonlocal_on=Fals
     None; the updated dict is aux["dyn"]); form "lowdin" needs none.
     Returns (psi, v, energies, atom forces, aux)."""
     en, F, floc, rho, vks = forces(psi, occ, sysm, lay, dlay, nonlocal_on=nonlocal_on, nkf=nkf,
-                                   xc=xc, nonlocal_sf=nonlocal_sf)
+                                   xc=xc, nonlocal_sf=nonlocal_sf, eext_ees=eext_ees)
     if form == "lowdin":
         Fc, lam = constrain(F, psi, lay)
         x, it_eff, gam = psi, iteration, None
