@@ -323,8 +323,10 @@ struct cpstep_ctx {
   // state-FFT scratch (bytes sized for the working precision)
   void* d_pen_a;         // [nstates][nz][nlpad] complex  (psi z-pencils)
   void* d_pen_b;         // [nstates][nz][nlpad] complex  (V.psi z-pencils)
-  double* d_rho_part;    // [ngroups_rho][nz*ny*nx]
+  double* d_rho_part;    // [ngroups_rho][nz*ny*nx], or the two-stage density's plane partials
   int ngroups_rho;
+  size_t rho_part_elems = 0;  // doubles in d_rho_part
+  int p16_blocks_k2 = 0, p16_blocks_k3 = 0;  // resident blocks of the two-stage plane passes
   void* d_vks_t;         // V_KS in working precision [nz][ny][nx]
   double* d_eke_part;    // [nstates][nblk_z]
   int nblk_z;

@@ -41,38 +41,49 @@ struct Par {
   double w[9];          // Yoshida weights times dt / nres
 };
 
-__global__ void k_nhc_ekin(const double2* __restrict__ v, const double2* __restrict__ f,
+__global__ void __launch_bounds__(256, 4) k_nhc_ekin(const double2* __restrict__ v, const double2* __restrict__ f,
                            const double* __restrict__ cmass, const int* __restrict__ cls,
                            const signed char* __restrict__ ck, int npts, int span, double dt,
                            int first_in, const int* __restrict__ skip, int nck,
                            double* __restrict__ part) {
+  constexpr int U = 2;  // points per thread and pass, loaded before any is used
   __shared__ double red[32];
   const int first = first_in && !(skip && *skip);
   const int s = blockIdx.y;
   const int p0 = blockIdx.x * span, p1 = min(npts, p0 + span);
   const double dt2 = 0.5 * dt;
+  const int B = blockDim.x;
   double acc[kMaxNck];
 #pragma unroll
   for (int k = 0; k < kMaxNck; ++k) acc[k] = 0.0;
-  for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-    const int c = cls[p];
-    if (c == 0) continue;
-    const size_t i = (size_t)s * npts + p;
-    const double m = cmass[p];
-    double2 vv = v[i];
-    if (c == 1) vv.y = 0.0;
-    if (first) {
-      double2 ff = f[i];
-      if (c == 1) ff.y = 0.0;
-      const double fm = dt2 / m;
-      vv.x += ff.x * fm;
-      vv.y += ff.y * fm;
-      if (c == 1) vv.y = 0.0;
-    }
-    const double e = (vv.x * vv.x + vv.y * vv.y) * (c == 2 ? 2.0 * m : m);
-    const int k = ck[p];
+  const double2* vs = v + (size_t)s * npts;
+  const double2* fs = f + (size_t)s * npts;
+  for (int pb = p0 + threadIdx.x; pb < p1; pb += U * B) {
+    int c[U];
+    double2 vv[U], ff[U];
 #pragma unroll
-    for (int q = 0; q < kMaxNck; ++q) acc[q] += (q == k) ? e : 0.0;
+    for (int u = 0; u < U; ++u) {
+      const int p = pb + u * B;
+      c[u] = p < p1 ? cls[p] : 0;
+      vv[u] = c[u] ? vs[p] : make_double2(0.0, 0.0);
+      ff[u] = (c[u] && first) ? fs[p] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (c[u] == 0) continue;
+      const int p = pb + u * B;
+      const double m = cmass[p];
+      if (c[u] == 1) { vv[u].y = 0.0; ff[u].y = 0.0; }
+      if (first) {
+        const double fm = dt2 / m;
+        vv[u].x += ff[u].x * fm;
+        vv[u].y += ff[u].y * fm;
+      }
+      const double e = (vv[u].x * vv[u].x + vv[u].y * vv[u].y) * (c[u] == 2 ? 2.0 * m : m);
+      const int k = ck[p];
+#pragma unroll
+      for (int q = 0; q < kMaxNck; ++q) acc[q] += (q == k) ? e : 0.0;
+    }
   }
 #pragma unroll
   for (int q = 0; q < kMaxNck; ++q) {
@@ -237,42 +248,56 @@ __global__ void k_nhc_sum(const double* __restrict__ eout, int n, double* __rest
   }
 }
 
-__global__ void k_nhc_apply(double2* __restrict__ psi, double2* __restrict__ v,
+// grid (point blocks, states): U points per thread, all loads issued first
+__global__ void __launch_bounds__(256, 3) k_nhc_apply(double2* __restrict__ psi, double2* __restrict__ v,
                             const double2* __restrict__ f, const double* __restrict__ cmass,
                             const int* __restrict__ cls, const signed char* __restrict__ ck,
                             const double* __restrict__ scale, int nck, int npts, int nstates,
                             double dt, int first_in, const int* __restrict__ skip) {
+  constexpr int U = 4;
   const int first = first_in && !(skip && *skip);
   const double dt2 = 0.5 * dt;
-  const size_t n = (size_t)npts * nstates;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const int p = (int)(i % npts);
-    const int c = cls[p];
-    if (c == 0) continue;
-    const int s = (int)(i / npts);
-    const double2 sc = reinterpret_cast<const double2*>(scale)[(size_t)s * nck + ck[p]];
-    const double fm = dt2 / cmass[p];
-    double2 vv = v[i];
-    double2 ff = f[i];
-    if (c == 1) { vv.y = 0.0; ff.y = 0.0; }
-    if (first) {
-      vv.x += ff.x * fm;
-      vv.y += ff.y * fm;
-      if (c == 1) vv.y = 0.0;
-      vv.x *= sc.x;
-      vv.y *= sc.x;
+  const int s = blockIdx.y;
+  const int B = blockDim.x;
+  const int pb = blockIdx.x * U * B + threadIdx.x;
+  const size_t row = (size_t)s * npts;
+  const double2* sc2 = reinterpret_cast<const double2*>(scale) + (size_t)s * nck;
+  int c[U];
+  double2 vv[U], ff[U], a[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int p = pb + u * B;
+    c[u] = p < npts ? cls[p] : 0;
+    if (c[u]) {
+      vv[u] = v[row + p];
+      ff[u] = f[row + p];
+      a[u] = psi[row + p];
     }
-    vv.x *= sc.y;
-    vv.y *= sc.y;
-    vv.x += ff.x * fm;
-    vv.y += ff.y * fm;
-    if (c == 1) vv.y = 0.0;
-    v[i] = vv;
-    double2 a = psi[i];
-    a.x += vv.x * dt;
-    a.y += vv.y * dt;
-    psi[i] = a;
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    if (c[u] == 0) continue;
+    const int p = pb + u * B;
+    const double2 sc = sc2[ck[p]];
+    const double fm = dt2 / cmass[p];
+    double2 w = vv[u], g = ff[u];
+    if (c[u] == 1) { w.y = 0.0; g.y = 0.0; }
+    if (first) {
+      w.x += g.x * fm;
+      w.y += g.y * fm;
+      if (c[u] == 1) w.y = 0.0;
+      w.x *= sc.x;
+      w.y *= sc.x;
+    }
+    w.x *= sc.y;
+    w.y *= sc.y;
+    w.x += g.x * fm;
+    w.y += g.y * fm;
+    if (c[u] == 1) w.y = 0.0;
+    v[row + p] = w;
+    a[u].x += w.x * dt;
+    a[u].y += w.y * dt;
+    psi[row + p] = a[u];
   }
 }
 
@@ -376,7 +401,8 @@ int nhc_set(cpstep_ctx* c, double te_ext, double tau_fs, int num, int nck, int n
   CPSTEP_CUDA_TRY(cudaMemcpy(t.d_xp, zero.data(), sizeof(double) * nch, cudaMemcpyHostToDevice));
   CPSTEP_CUDA_TRY(cudaMemcpy(t.d_vn, vn.data(), sizeof(double) * nch, cudaMemcpyHostToDevice));
   // enough (state, span) blocks for two waves; spans of whole 256-point rows
-  t.nsplit = std::max(1, std::min((np + 255) / 256, (4 * c->num_sms + c->nstates - 1) / c->nstates));
+  // one wave of (state, span) blocks at 8 blocks of 256 threads per SM
+  t.nsplit = std::max(1, std::min((np + 255) / 256, (8 * c->num_sms) / c->nstates));
   t.span = (np + t.nsplit - 1) / t.nsplit;
   t.nsplit = (np + t.span - 1) / t.span;
   CPSTEP_CUDA_TRY(cudaMalloc(&t.d_part, sizeof(double) * (size_t)c->nstates * t.nsplit * nck));
@@ -449,7 +475,8 @@ int nhc_integrate(cpstep_ctx* c, const double* force, double* psi, double* vpsi,
     nhc::k_nhc_sum<<<1, 256, 0, c->stream>>>(t.d_eout, nt, d_fict_ke, d_enhc);
     CPSTEP_LAUNCH_CHECK();
   }
-  nhc::k_nhc_apply<<<c->nblk_ke, 256, 0, c->stream>>>(p, v, f, c->d_cmass, c->d_cls, t.d_ck,
+  nhc::k_nhc_apply<<<dim3(cdiv(c->npts, 4 * 256), c->nstates), 256, 0, c->stream>>>(
+      p, v, f, c->d_cmass, c->d_cls, t.d_ck,
                                                        t.d_scale, t.nck, c->npts, c->nstates,
                                                        dt, first, d_skip_half);
   CPSTEP_LAUNCH_CHECK();

@@ -17,6 +17,45 @@ __global__ void k_rho_reduce(const double* __restrict__ part, int ngroups, size_
   }
 }
 
+// blockIdx.x = plane z, blockIdx.y = a slice of its n^2 points.  The blocks b
+// whose item range [I b / B, I (b + 1) / B) (I = n S items, plane-major) meets
+// the plane's items [z S, (z + 1) S) are b0 = block of item z S .. b1 = block
+// of item (z + 1) S - 1, where the block of item i is ((i + 1) B - 1) / I; an
+// empty block range is skipped.  Block b's partial of plane z is its segment
+// z - (first item of b) / S.  The (partial) offsets of the plane are listed
+// once per block in shared memory.
+__global__ void k_rho_reduce_items(const double* __restrict__ part, int n, int nstates,
+                                   int nblocks, int segs, double scale, double* __restrict__ rho) {
+  constexpr int MAXP = 64;
+  __shared__ long long offs[MAXP];
+  __shared__ int np_s;
+  const int z = blockIdx.x;
+  const size_t n2 = (size_t)n * n;
+  const long long items = (long long)n * nstates;
+  if (threadIdx.x == 0) {
+    const long long ia = (long long)z * nstates, ib = ia + nstates - 1;
+    const int b0 = (int)(((ia + 1) * nblocks - 1) / items);
+    const int b1 = (int)(((ib + 1) * nblocks - 1) / items);
+    int np = 0;
+    for (int b = b0; b <= b1 && np < MAXP; ++b) {
+      const long long s0 = p16_item_start(items, b, nblocks);
+      if (s0 >= p16_item_start(items, b + 1, nblocks)) continue;
+      const int seg = z - (int)(s0 / nstates);
+      offs[np++] = ((long long)b * segs + seg) * (long long)n2;
+    }
+    np_s = np;
+  }
+  __syncthreads();
+  const int np = np_s;
+  const size_t per = (n2 + gridDim.y - 1) / gridDim.y;
+  const size_t o0 = blockIdx.y * per, o1 = min(n2, o0 + per);
+  for (size_t off = o0 + threadIdx.x; off < o1; off += blockDim.x) {
+    double a = 0.0;
+    for (int q = 0; q < np; ++q) a += part[offs[q] + off];
+    rho[(size_t)z * n2 + off] = a * scale;
+  }
+}
+
 // per-state sum of block partials in a fixed order (deterministic)
 __global__ void k_rowsum(const double* __restrict__ part, int ncol, int nrow,
                          double* __restrict__ out) {
@@ -95,7 +134,14 @@ int statefft_init(cpstep_ctx* c) {
   CPSTEP_CUDA_TRY(cudaMalloc(&c->d_pen_b, pen));
   size_t nr = (size_t)c->nx * c->ny * c->nz;
   c->ngroups_rho = std::max(1, std::min(c->nstates, 8));
-  CPSTEP_CUDA_TRY(cudaMalloc(&c->d_rho_part, sizeof(double) * nr * c->ngroups_rho));
+  // the two-stage density pass writes one plane partial per (block, plane
+  // touched): at most (ceil(items / B) / S + 2) per block, B <= 2 blocks per SM
+  size_t n2 = (size_t)c->nx * c->ny;
+  long long items = (long long)c->nz * c->nstates;
+  long long nb = 2LL * c->num_sms;
+  size_t p16 = (size_t)nb * (size_t)(cdiv((int)((items + c->num_sms - 1) / c->num_sms), c->nstates) + 1) * n2;
+  c->rho_part_elems = std::max(nr * c->ngroups_rho, p16);
+  CPSTEP_CUDA_TRY(cudaMalloc(&c->d_rho_part, sizeof(double) * c->rho_part_elems));
   CPSTEP_CUDA_TRY(cudaMalloc(&c->d_vks_t, sizeof(float) * nr));
   c->nblk_z = cdiv(c->nlines, c->ops.lb);
   CPSTEP_CUDA_TRY(cudaMalloc(&c->d_eke_part, sizeof(double) * (size_t)c->nstates * c->nblk_z));

@@ -773,12 +773,21 @@ k_xy_bwd_s(const cplx<T>* __restrict__ pen, const double* __restrict__ freal,
 // Plane passes in the two-stage form (fft_p16.cuh), FP32, N = 32, 64, 128:
 // 256 threads, every warp 32 / R line groups of R threads, one line (a
 // column or a row pair) per group at a time.  The plane is [nplane_x][LDY]
-// with LDY odd and >= N + N/16: a column is transformed in place with its own
-// storage as the exchange scratch; row pairs use a per-group scratch line.
-// Row pairs are built straight from the plane into stride layout (imag flip,
-// Hermitian extension), C2R'd by s2b into block layout where V_KS (K3) or the
-// density (K2) is applied, and (K3) R2C'd by b2s back into stride layout,
-// where the two real rows' spectra are split with one shuffle.
+// with LDY = N + 3; every line group owns a scratch line of SCR = N + N/16
+// elements, the exchange buffer of its column and row transforms.  Row pairs
+// are built straight from the plane into stride layout (imag flip, Hermitian
+// extension), C2R'd by s2b into block layout where V_KS (K3) or the density
+// (K2) is applied, and (K3) R2C'd by b2s back into stride layout, where the
+// two real rows' spectra are split with one shuffle.
+// Bank layout (8-byte elements, a warp access served as two half-warp
+// phases): with LDY odd and LDY = N + 3 the column loads, the column stores in
+// block order and the row builds put the line groups of a half warp on
+// disjoint banks, and with the scratch stride SCR (= R mod 2R) so do the
+// exchanges: every one of these warp accesses takes the minimum two
+// wavefronts (the column exchange in the plane itself took three to four).
+// The blocks split the (plane, state) items evenly, plane-major: block b
+// takes items [b I / B, (b + 1) I / B) of I = N S, so all B resident blocks
+// (B = blocks per SM x SMs) carry the same work whatever S is.
 // K2 runs 512 threads (for N = 128 every line group owns one row pair of the
 // plane, so its FP64 accumulators fit the registers), K3 256 threads at two
 // blocks per SM.
@@ -786,10 +795,9 @@ template <int N, int THREADS_>
 struct P16Shape {
   static constexpr int THREADS = THREADS_, NW = THREADS / 32;
   static constexpr int LPW = P16Cfg<N>::LPW, SLOTS = NW * LPW;
-  static constexpr int LDY = (P16Cfg<N>::SCR | 1) == P16Cfg<N>::SCR ? P16Cfg<N>::SCR
-                                                                   : P16Cfg<N>::SCR + 1;
-  static constexpr int SL = ((P16Cfg<N>::SCR + 15) / 16) * 16 + 8;  // row scratch stride
-  // twiddles, plane, row scratch, pencil-row staging (nlines rounded to 2)
+  static constexpr int LDY = N + 3;
+  static constexpr int SL = P16Cfg<N>::SCR;  // scratch line stride
+  // twiddles, plane, scratch lines, pencil-row staging (nlines rounded to 2)
   static constexpr size_t bytes(int nplx, int nlines) {
     return sizeof(cplx<float>) *
            ((size_t)N + (size_t)nplx * LDY + (size_t)SLOTS * SL + (size_t)((nlines + 1) & ~1));
@@ -824,22 +832,25 @@ __device__ __forceinline__ void p16_scatter(const cplx<float>* stage, cplx<float
   __syncthreads();
 }
 
-// y-FFTs of the nplane_x columns in place (natural order in and out); groups
-// past the last column work on their own scratch line and store nothing.
+// y-FFTs of the nplane_x columns in place (natural order in and out), the
+// exchange through the line group's own scratch; a warp leaves as soon as no
+// column is left for any of its groups, and groups past the last column of a
+// round run on their scratch and store nothing.
 template <int N, bool INV, bool LEAN>
 __device__ __forceinline__ void p16_columns(cplx<float>* plane, int ldy, int nplx,
                                             const P16Fft<float, N, LEAN>& F, cplx<float>* scr,
                                             int slot, int nslots) {
-  constexpr int R = P16Cfg<N>::R;
+  constexpr int R = P16Cfg<N>::R, LPW = P16Cfg<N>::LPW;
+  const int wslot = slot - slot % LPW;  // first slot of this warp
   for (int c0 = 0; c0 < nplx; c0 += nslots) {
+    if (c0 + wslot >= nplx) break;  // warp-uniform
     const int c = c0 + slot;
     const bool act = c < nplx;
-    cplx<float>* col = act ? plane + (size_t)c * ldy : scr;
+    cplx<float>* col = plane + (size_t)(act ? c : 0) * ldy;
     cplx<float> v[16];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) v[k] = col[F.t + R * k];
-    F.template s2b<INV>(v, col);
-    __syncwarp();
+    for (int k = 0; k < 16; ++k) v[k] = act ? col[F.t + R * k] : mk<float>(0.f, 0.f);
+    F.template s2b<INV>(v, scr);
     if (act) {
 #pragma unroll
       for (int q = 0; q < 16; ++q) col[F.bpos(q)] = v[q];
@@ -896,37 +907,53 @@ __device__ __forceinline__ void p16_extract_row(const cplx<float> (&v)[16], cplx
   }
 }
 
-// K3 (two-stage form): pencils -> psi(r) -> psi V occ -> pencils_out
+// items [i0, i1) of block b out of B over I = N S (plane-major: item i is
+// plane i / S, state i % S); the density reduction uses the same split
+__host__ __device__ __forceinline__ long long p16_item_start(long long items, int b, int nblocks) {
+  return items * b / nblocks;
+}
+
+// K3 (two-stage form): pencils -> psi(r) -> psi V occ -> pencils_out, over
+// the block's (plane, state) items
 template <int N>
 __global__ void __launch_bounds__(P16_K3_THREADS, 2)
 k_xy_bwd_p16(const cplx<float>* __restrict__ pen, const float* __restrict__ vks,
              cplx<float>* __restrict__ pen_out, StateGeom g,
              const cplx<float>* __restrict__ twx_g, const double* __restrict__ occ,
-             int nstates, int spg) {
+             int nstates) {
   using S = P16Shape<N, P16_K3_THREADS>;
-  constexpr int LDY = S::LDY, SLOTS = S::SLOTS, R = P16Cfg<N>::R;
+  constexpr int LDY = S::LDY, SLOTS = S::SLOTS, R = P16Cfg<N>::R, LPW = S::LPW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<float>* tw = reinterpret_cast<cplx<float>*>(smem_raw);
   cplx<float>* plane = tw + N;
   const int nplx = g.nplane_x;
-  const int slot = (threadIdx.x >> 5) * S::LPW + (threadIdx.x & 31) / R;
+  const int slot = (threadIdx.x >> 5) * LPW + (threadIdx.x & 31) / R;
+  const int wslot = slot - slot % LPW;
   cplx<float>* scr = plane + (size_t)nplx * LDY + (size_t)slot * S::SL;
   cplx<float>* stage = plane + (size_t)nplx * LDY + (size_t)SLOTS * S::SL;
-  const int z = blockIdx.x;
-  const int s0 = blockIdx.y * spg, s1 = min(nstates, s0 + spg);
+  const long long items = (long long)N * nstates;
+  const long long i0 = p16_item_start(items, blockIdx.x, gridDim.x);
+  const long long i1 = p16_item_start(items, blockIdx.x + 1, gridDim.x);
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx_g[i];
-  if (s0 < s1) p16_prefetch(pen + ((size_t)s0 * N + z) * g.nlpad, stage, g.nlines);
+  if (i0 < i1)
+    p16_prefetch(pen + ((size_t)(i0 % nstates) * N + (size_t)(i0 / nstates)) * g.nlpad, stage,
+                 g.nlines);
   __syncthreads();
   P16Fft<float, N> F;
   F.init(tw);
-  const float* vplane = vks + (size_t)z * N * N;
-  for (int s = s0; s < s1; ++s) {
+  for (long long it = i0; it < i1; ++it) {
+    const int z = (int)(it / nstates), s = (int)(it % nstates);
     p16_scatter<N, LDY>(stage, plane, g);
-    if (s + 1 < s1) p16_prefetch(pen + ((size_t)(s + 1) * N + z) * g.nlpad, stage, g.nlines);
+    if (it + 1 < i1)
+      p16_prefetch(pen + ((size_t)((it + 1) % nstates) * N + (size_t)((it + 1) / nstates)) *
+                             g.nlpad,
+                   stage, g.nlines);
     p16_columns<N, false>(plane, LDY, nplx, F, scr, slot, SLOTS);  // FFTW_FORWARD y
     __syncthreads();
+    const float* vplane = vks + (size_t)z * N * N;
     const float w = (float)occ[s];
     for (int p0 = 0; p0 < N / 2; p0 += SLOTS) {
+      if (p0 + wslot >= N / 2) break;  // warp-uniform: no row pair left for this warp
       const int pp = p0 + slot;
       const bool act = pp < N / 2;
       const int ya = act ? 2 * pp : 0;
@@ -963,29 +990,33 @@ k_xy_bwd_p16(const cplx<float>* __restrict__ pen, const float* __restrict__ vks,
 }
 
 // K2 (two-stage form): planes -> occ psi^2 accumulated in FP64 registers over
-// the block's states; the block's partial density of plane z goes to out
-// [group][z][y][x].  Every row pair of the plane belongs to one line group
-// (PASSES = (N/2) / SLOTS of them per group), the slots of its block layout
-// to the group's threads.
+// the block's items of one plane; each plane the block touches (segment q of
+// its item range) gets its own partial density out[b segs + q][y][x].  Every
+// row pair of the plane belongs to one line group (PASSES = (N/2) / SLOTS of
+// them per group), the slots of its block layout to the group's threads.
 template <int N>
 __global__ void __launch_bounds__(P16_K2_THREADS, 1)
 k_xy_fwd_p16(const cplx<float>* __restrict__ pen, StateGeom g,
              const cplx<float>* __restrict__ twx_g, const double* __restrict__ occ,
-             int nstates, int spg, double* __restrict__ out) {
+             int nstates, int segs, double* __restrict__ out) {
   using S = P16Shape<N, P16_K2_THREADS>;
-  constexpr int LDY = S::LDY, SLOTS = S::SLOTS, R = P16Cfg<N>::R;
+  constexpr int LDY = S::LDY, SLOTS = S::SLOTS, R = P16Cfg<N>::R, LPW = S::LPW;
   constexpr int PASSES = (N / 2 + SLOTS - 1) / SLOTS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<float>* tw = reinterpret_cast<cplx<float>*>(smem_raw);
   cplx<float>* plane = tw + N;
   const int nplx = g.nplane_x;
-  const int slot = (threadIdx.x >> 5) * S::LPW + (threadIdx.x & 31) / R;
+  const int slot = (threadIdx.x >> 5) * LPW + (threadIdx.x & 31) / R;
+  const int wslot = slot - slot % LPW;
   cplx<float>* scr = plane + (size_t)nplx * LDY + (size_t)slot * S::SL;
   cplx<float>* stage = plane + (size_t)nplx * LDY + (size_t)SLOTS * S::SL;
-  const int z = blockIdx.x;
-  const int s0 = blockIdx.y * spg, s1 = min(nstates, s0 + spg);
+  const long long items = (long long)N * nstates;
+  const long long i0 = p16_item_start(items, blockIdx.x, gridDim.x);
+  const long long i1 = p16_item_start(items, blockIdx.x + 1, gridDim.x);
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx_g[i];
-  if (s0 < s1) p16_prefetch(pen + ((size_t)s0 * N + z) * g.nlpad, stage, g.nlines);
+  if (i0 < i1)
+    p16_prefetch(pen + ((size_t)(i0 % nstates) * N + (size_t)(i0 / nstates)) * g.nlpad, stage,
+                 g.nlines);
   __syncthreads();
   P16Fft<float, N, true> F;
   F.init(tw);
@@ -996,45 +1027,68 @@ k_xy_fwd_p16(const cplx<float>* __restrict__ pen, StateGeom g,
     for (int h = 0; h < 2; ++h)
 #pragma unroll
       for (int k = 0; k < 16; ++k) acc[q][h][k] = 0.0;
-  for (int s = s0; s < s1; ++s) {
+  // the partial density of the current plane into its segment, then zero
+  auto flush = [&](int seg) {
+    double* o = out + ((size_t)blockIdx.x * segs + seg) * N * N;
+#pragma unroll
+    for (int q = 0; q < PASSES; ++q) {
+      const int pp = slot + SLOTS * q;
+      if (pp < N / 2) {
+        const int ya = 2 * pp;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int x = F.bpos(k);
+          o[(size_t)ya * N + x] = acc[q][0][k];
+          o[(size_t)(ya + 1) * N + x] = acc[q][1][k];
+          acc[q][0][k] = 0.0;
+          acc[q][1][k] = 0.0;
+        }
+      }
+    }
+  };
+  int zc = (int)(i0 / nstates), seg = 0;
+  for (long long it = i0; it < i1; ++it) {
+    const int z = (int)(it / nstates), s = (int)(it % nstates);
+    if (z != zc) {  // block-uniform
+      flush(seg);
+      zc = z;
+      ++seg;
+    }
     p16_scatter<N, LDY>(stage, plane, g);
-    if (s + 1 < s1) p16_prefetch(pen + ((size_t)(s + 1) * N + z) * g.nlpad, stage, g.nlines);
+    if (it + 1 < i1)
+      p16_prefetch(pen + ((size_t)((it + 1) % nstates) * N + (size_t)((it + 1) / nstates)) *
+                             g.nlpad,
+                   stage, g.nlines);
     p16_columns<N, false>(plane, LDY, nplx, F, scr, slot, SLOTS);  // FFTW_FORWARD y
     __syncthreads();
     const double w = occ[s];
 #pragma unroll
     for (int q = 0; q < PASSES; ++q) {
-      const int pp = slot + SLOTS * q;
-      const bool act = pp < N / 2;
-      const int ya = act ? 2 * pp : 0;
-      cplx<float> v[16];
-      p16_build_row<N>(plane, LDY, nplx, ya, F.t, v);
-      F.template s2b<true>(v, scr);  // C2R, +i sign
-      if (act) {
+      if (SLOTS * q + wslot < N / 2) {  // warp-uniform
+        const int pp = slot + SLOTS * q;
+        const bool act = pp < N / 2;
+        const int ya = act ? 2 * pp : 0;
+        cplx<float> v[16];
+        p16_build_row<N>(plane, LDY, nplx, ya, F.t, v);
+        F.template s2b<true>(v, scr);  // C2R, +i sign
+        if (act) {
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          acc[q][0][k] += w * (double)v[k].x * (double)v[k].x;
-          acc[q][1][k] += w * (double)v[k].y * (double)v[k].y;
+          for (int k = 0; k < 16; ++k) {
+            acc[q][0][k] += w * (double)v[k].x * (double)v[k].x;
+            acc[q][1][k] += w * (double)v[k].y * (double)v[k].y;
+          }
         }
       }
     }
     __syncthreads();
   }
-  double* o = out + ((size_t)blockIdx.y * N + z) * N * N;
-#pragma unroll
-  for (int q = 0; q < PASSES; ++q) {
-    const int pp = slot + SLOTS * q;
-    if (pp < N / 2) {
-      const int ya = 2 * pp;
-#pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        const int x = F.bpos(k);
-        o[(size_t)ya * N + x] = acc[q][0][k];
-        o[(size_t)(ya + 1) * N + x] = acc[q][1][k];
-      }
-    }
-  }
+  if (i0 < i1) flush(seg);
 }
+
+// sum, for every plane z, the partial densities of the blocks whose item
+// range touched it (block order: deterministic), scaled
+__global__ void k_rho_reduce_items(const double* __restrict__ part, int n, int nstates,
+                                   int nblocks, int segs, double scale, double* __restrict__ rho);
 
 // ---------------------------------------------------------------------------
 // K4: pencils -> backward z-FFT -> pack -> scale.
@@ -1407,6 +1461,21 @@ int set_smem(K kernel, size_t smem) {
   return CPSTEP_OK;
 }
 
+// resident blocks of a plane-pass kernel on this device (blocks per SM x SMs),
+// looked up once per context
+template <typename K>
+int resident_blocks(const cpstep_ctx* c, K kernel, int threads, size_t smem, int* cache) {
+  if (*cache > 0) return CPSTEP_OK;
+  int per = 0;
+  CPSTEP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem));
+  if (per < 1) {
+    cpstep_set_error("state FFT: plane-pass kernel does not fit an SM (%zu bytes shared)", smem);
+    return CPSTEP_ERR_CUDA;
+  }
+  *cache = per * c->num_sms;
+  return CPSTEP_OK;
+}
+
 // state groups for the plane passes: aim at tune.plane_waves (default 3)
 // waves of CTAs
 inline int plane_groups(const cpstep_ctx* c, int nstates, int other) {
@@ -1436,17 +1505,27 @@ struct StateFft {
     if constexpr (P16Cfg<N>::ok && sizeof(T) == 4) {
       if (c->tune.shfl == 2) {
         const size_t smem = P16Shape<N, P16_K2_THREADS>::bytes(j.g.nplane_x, j.g.nlines);
-        int ng = std::min(c->ngroups_rho, plane_groups(c, c->nstates, 1));
-        int spg = cdiv(c->nstates, ng);
-        ng = cdiv(c->nstates, spg);
         if (int rc = set_smem(k_xy_fwd_p16<N>, smem)) return rc;
-        k_xy_fwd_p16<N><<<dim3(N, ng), P16_K2_THREADS, smem, c->stream>>>(
+        if (int rc = resident_blocks(c, k_xy_fwd_p16<N>, P16_K2_THREADS, smem, &c->p16_blocks_k2))
+          return rc;
+        const int nb = c->p16_blocks_k2;
+        const long long items = (long long)N * c->nstates;
+        const int segs = (int)(((items + nb - 1) / nb + c->nstates - 1) / c->nstates) + 1;
+        if ((size_t)nb * segs * N * N > c->rho_part_elems) {
+          cpstep_set_error("state FFT: density partials need %zu doubles, %zu allocated",
+                           (size_t)nb * segs * N * N, c->rho_part_elems);
+          return CPSTEP_ERR_CUDA;
+        }
+        k_xy_fwd_p16<N><<<nb, P16_K2_THREADS, smem, c->stream>>>(
             reinterpret_cast<const cplx<float>*>(j.pen_a), j.g, tws<float>(c).x, occ,
-            c->nstates, spg, c->d_rho_part);
+            c->nstates, segs, c->d_rho_part);
         CPSTEP_LAUNCH_CHECK();
-        size_t nr = (size_t)N * N * N;
-        k_rho_reduce<<<2 * c->num_sms, 256, 0, c->stream>>>(c->d_rho_part, ng, nr, 1.0 / c->vol,
-                                                            rho);
+        if ((long long)nb > 62LL * N) {  // more blocks on one plane than the reduction lists
+          cpstep_set_error("state FFT: %d density blocks over %d planes", nb, N);
+          return CPSTEP_ERR_CUDA;
+        }
+        k_rho_reduce_items<<<dim3(N, cdiv(4 * c->num_sms, N)), 256, 0, c->stream>>>(
+            c->d_rho_part, N, c->nstates, nb, segs, 1.0 / c->vol, rho);
         CPSTEP_LAUNCH_CHECK();
         return CPSTEP_OK;
       }
@@ -1589,10 +1668,11 @@ struct StateFft {
       if (c->tune.shfl == 2) {
         const size_t smem = P16Shape<N, P16_K3_THREADS>::bytes(j.g.nplane_x, j.g.nlines);
         if (int rc = set_smem(k_xy_bwd_p16<N>, smem)) return rc;
-        k_xy_bwd_p16<N><<<dim3(N, ng), P16_K3_THREADS, smem, c->stream>>>(
+        if (int rc = resident_blocks(c, k_xy_bwd_p16<N>, P16_K3_THREADS, smem, &c->p16_blocks_k3))
+          return rc;
+        k_xy_bwd_p16<N><<<c->p16_blocks_k3, P16_K3_THREADS, smem, c->stream>>>(
             reinterpret_cast<const cplx<float>*>(j.pen_a), reinterpret_cast<const float*>(vt),
-            reinterpret_cast<cplx<float>*>(j.pen_b), j.g, tws<float>(c).x, occ, c->nstates,
-            spg);
+            reinterpret_cast<cplx<float>*>(j.pen_b), j.g, tws<float>(c).x, occ, c->nstates);
         shfl_done = true;
       }
     }

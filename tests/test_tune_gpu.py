@@ -33,7 +33,9 @@ def test_autotune_choices_and_step(precision):
     try:
         default = ctx.tune_get()
         choice, ms = ctx.autotune(sysm.psi(), occ)
-        assert choice["plane_shfl"] in (0, 1)
+        assert choice["plane_shfl"] in (0, 1, 2)  # Stockham, shuffles, two-stage (FP32)
+        if precision == "fp64":
+            assert choice["plane_shfl"] in (0, 1)
         assert choice["plane_waves"] in (1, 2, 3, 6)
         assert choice["nl_blocks"] in (3, 6, 12)
         assert choice["pc_split"] in (1, 2)
