@@ -212,6 +212,22 @@ struct NlData {
   std::vector<long long> sv_off;
   std::vector<std::vector<int>> tch;  // channels of each type, in channel order
   std::vector<float2*> tdyp;        // [nch_t][ld_d32] per type, FP32 (tensor-core path)
+  std::vector<float> tdmax;         // largest |dyp| of each type's channels (FP16 scales)
+  std::vector<std::vector<float>> tdmax_c;  // the same per channel of the type
+  float* d_hmax = nullptr;          // [2][ntyp] bound of |S| (Mn rows) and largest |Z| entry
+                                    // per type (float bits, atomicMax), written every pass
+  // FP16 levels of the S rows of every type (rows v natm_t + a, the pre-split
+  // image) at blv + blv_off[t], their scales and inverses at tsc / tinv +
+  // tsoff[t]; the A operand of the sums (w psi dyp_c) at alv
+  uint8_t* blv = nullptr;
+  std::vector<size_t> blv_off;
+  float *tsc = nullptr, *tinv = nullptr;
+  std::vector<long long> tsoff;
+  uint8_t* alv = nullptr;
+  size_t alv_bytes = 0;
+  // the psi force's operand levels: Z and the transposed Mn rows (largest type)
+  uint8_t *pf_z = nullptr, *pf_st = nullptr;
+  size_t pf_zbytes = 0, pf_stbytes = 0;
   int ld_d32 = 0;                   // npts rounded up to even
   int* d_order = nullptr;           // atom of each type-order rank
   int* d_tch = nullptr;             // [ntyp][4] channel indices (-1 unused)
@@ -467,11 +483,16 @@ void graph_drop(cpstep_ctx* c);
 int pc_part_reserve(cpstep_ctx* c, size_t elems);
 int split_reserve(cpstep_ctx* c, size_t bytes);
 int lv_reserve(cpstep_ctx* c, size_t bytes);
-int ees_tc_presplit(cpstep_ctx* c, const double* psi, int nin_max);
-int ees_tc_sums(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
-                int nch, int jp, double* C, int ldc);
-int ees_tc_force(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
-                 int nch, int natm_t, const double* Z, int ldz, double alpha, double* fpsi);
+int ees_tc_force_pre(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
+                     int nch, int natm_t, const double* Z, int ldz, double alpha, double* fpsi,
+                     const float* smax, const float* zmax, uint8_t* zlv, size_t zlv_bytes,
+                     uint8_t* stlv, size_t stlv_bytes);
+size_t ees_pf_zbytes(int nstates, int natm_t);
+size_t ees_pf_stbytes(int npts, int natm_t);
+size_t ees_lv_bytes(int rows, int K);
+int ees_tc_sums_pre(cpstep_ctx* c, const double* psi, const float2* dyp, int ld_d, int nch,
+                    const float* dmax, const uint8_t* blv, int jp, const float* cinv,
+                    uint8_t* alv, size_t alv_bytes, double* C);
 int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
                             double* C, int ldc, int sym);
 // paircalc_tc.cu (tensor-core products; *used = false when the SIMT path must run)

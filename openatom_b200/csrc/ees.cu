@@ -20,6 +20,7 @@
 #include <cmath>
 #include <vector>
 #include "ctx.cuh"
+#include "tc_sm100.cuh"
 
 namespace ees {
 
@@ -243,46 +244,122 @@ __global__ void k_ees_sep(const int* __restrict__ ig, const double* __restrict__
 struct TypeDims {
   int tstart[CPSTEP_MAX_TYPES + 1];
   long long svoff[CPSTEP_MAX_TYPES];
+  long long tsoff[CPSTEP_MAX_TYPES];  // first S row of the type in tsc / tinv
+  long long bloff[CPSTEP_MAX_TYPES];  // byte offset of the type's S-row levels
 };
 
 __device__ __forceinline__ double2 cm(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// S matrices: rows v natm_t + a (v = Mn, d/dx, d/dy, d/dz) of each type, FP32
-// complex per packed point.  One block row per atom.
-__global__ void k_ees_smat(const double2* __restrict__ sep, const int* __restrict__ kx,
-                           const int* __restrict__ ky, const int* __restrict__ kz, int npts,
-                           int km, const int* __restrict__ typ, const int* __restrict__ rank,
-                           TypeDims td, NlAtoms A, long long ld_s, float* __restrict__ sv) {
-  const int a = blockIdx.y;
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= npts) return;
-  const int t = typ[a];
-  const int nt = td.tstart[t + 1] - td.tstart[t], al = rank[a] - td.tstart[t];
+// Bounds of |S| of the rows (v, a) of every atom from the per-axis maxima of
+// its separable transforms: |S| is their product, the gradient rows are
+// bounded by the triangle inequality.  tsc = pow2_scale(bound) scales the
+// row's FP16 levels, tinv = 1 / tsc; smax[t] gets the largest Mn-row bound of
+// the type (float bits of a non-negative value, atomicMax).  One warp per atom.
+__global__ void k_ees_bound(const double2* __restrict__ sep, int natm, int km,
+                            const int* __restrict__ typ, const int* __restrict__ rank,
+                            TypeDims td, NlAtoms A, float* __restrict__ tsc,
+                            float* __restrict__ tinv, unsigned int* __restrict__ smax) {
+  const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (a >= natm) return;
   const int nk = 2 * km + 1;
   const double2* T = sep + (size_t)a * 6 * nk;
-  const int ix = kx[p] + km, iy = ky[p] + km, iz = kz[p] + km;
-  const double2 sa = T[0 * nk + ix], da = T[1 * nk + ix];
-  const double2 sb = T[2 * nk + iy], db = T[3 * nk + iy];
-  const double2 sc = T[4 * nk + iz], dc = T[5 * nk + iz];
-  const double2 sbc = cm(sb, sc);
-  const double2 S = cm(sa, sbc);
-  const double2 at = cm(da, sbc), bt = cm(sa, cm(db, sc)), ct = cm(cm(sa, sb), dc);
+  double m[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    double mx = 0.0;
+    for (int k = lane; k < nk; k += 32) {
+      const double2 v = T[q * nk + k];
+      mx = fmax(mx, hypot(v.x, v.y));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    m[q] = mx;
+  }
+  if (lane == 0) {
+    const int t = typ[a];
+    const int nt = td.tstart[t + 1] - td.tstart[t], al = rank[a] - td.tstart[t];
+    double b[4];
+    b[0] = m[0] * m[2] * m[4];
+    const double* h = A.hmati;
+    for (int v = 0; v < 3; ++v) {
+      const double h0 = fabs(h[3 * v] * A.grid), h1 = fabs(h[3 * v + 1] * A.grid),
+                   h2 = fabs(h[3 * v + 2] * A.grid);
+      b[v + 1] = m[1] * m[2] * m[4] * h0 + m[0] * m[3] * m[4] * h1 + m[0] * m[2] * m[5] * h2;
+    }
+    for (int v = 0; v < 4; ++v) {
+      const float sc = tc::pow2_scale((float)b[v]);
+      tsc[td.tsoff[t] + v * nt + al] = sc;
+      tinv[td.tsoff[t] + v * nt + al] = 1.f / sc;
+    }
+    atomicMax(smax + t, __float_as_uint((float)b[0]));
+  }
+}
+
+// S matrices, 4 points per thread: the Mn rows in FP32 (row a of the type, for
+// the psi force) and every row (v natm_t + a, v = Mn, d/dx, d/dy, d/dz) as
+// scaled FP16 levels in the pre-split image (nsp K steps per 128-row tile)
+// for the sums.  Lane i of a warp is the atom of type-order rank 8 y + (i & 7)
+// (y = blockIdx.y) at point quad (i >> 3) of the warp: the 8 atoms' 16-byte
+// pieces of a K half are one 128-byte core matrix when their rows are 8-aligned.
+__global__ void __launch_bounds__(256) k_ees_smat(
+    const double2* __restrict__ sep, const int* __restrict__ kx, const int* __restrict__ ky,
+    const int* __restrict__ kz, int npts, int km, const int* __restrict__ typ,
+    const int* __restrict__ order, int natm, TypeDims td, NlAtoms A, long long ld_s,
+    float* __restrict__ sv, const float* __restrict__ tsc, uint8_t* __restrict__ blv, int nsp) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ra = blockIdx.y * 8 + (lane & 7);
+  const int p0 = 4 * ((blockIdx.x * 8 + warp) * 4 + (lane >> 3));
+  if (ra >= natm || p0 >= npts) return;
+  const int a = order[ra];
+  const int t = typ[a];
+  const int nt = td.tstart[t + 1] - td.tstart[t], al = ra - td.tstart[t];
+  const int nk = 2 * km + 1;
+  const double2* T = sep + (size_t)a * 6 * nk;
   const double* h = A.hmati;
   const double g = A.grid;
-  double2 out[4];
-  out[0] = S;
+  float lv[4][8];
+  float* base = sv + td.svoff[t] + (size_t)al * ld_s;
 #pragma unroll
-  for (int v = 0; v < 3; ++v) {
-    const double h0 = h[3 * v] * g, h1 = h[3 * v + 1] * g, h2 = h[3 * v + 2] * g;
-    out[v + 1] = make_double2(at.x * h0 + bt.x * h1 + ct.x * h2, at.y * h0 + bt.y * h1 + ct.y * h2);
+  for (int e = 0; e < 4; ++e) {
+    const int p = p0 + e;
+    if (p < npts) {
+      const int ix = kx[p] + km, iy = ky[p] + km, iz = kz[p] + km;
+      const double2 sa = T[0 * nk + ix], da = T[1 * nk + ix];
+      const double2 sb = T[2 * nk + iy], db = T[3 * nk + iy];
+      const double2 sc = T[4 * nk + iz], dc = T[5 * nk + iz];
+      const double2 sbc = cm(sb, sc);
+      const double2 S = cm(sa, sbc);
+      const double2 at = cm(da, sbc), bt = cm(sa, cm(db, sc)), ct = cm(cm(sa, sb), dc);
+      lv[0][2 * e] = (float)S.x;
+      lv[0][2 * e + 1] = (float)S.y;
+#pragma unroll
+      for (int v = 0; v < 3; ++v) {
+        const double h0 = h[3 * v] * g, h1 = h[3 * v + 1] * g, h2 = h[3 * v + 2] * g;
+        lv[v + 1][2 * e] = (float)(at.x * h0 + bt.x * h1 + ct.x * h2);
+        lv[v + 1][2 * e + 1] = (float)(at.y * h0 + bt.y * h1 + ct.y * h2);
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) lv[v][2 * e] = lv[v][2 * e + 1] = 0.f;
+    }
   }
-  float* base = sv + td.svoff[t];
+  if (p0 + 3 < npts) {
+    *reinterpret_cast<float4*>(base + 2 * p0) = make_float4(lv[0][0], lv[0][1], lv[0][2], lv[0][3]);
+    *reinterpret_cast<float4*>(base + 2 * p0 + 4) =
+        make_float4(lv[0][4], lv[0][5], lv[0][6], lv[0][7]);
+  } else {
+    for (int e = 0; p0 + e < npts; ++e)
+      reinterpret_cast<float2*>(base)[p0 + e] = make_float2(lv[0][2 * e], lv[0][2 * e + 1]);
+  }
+  // reals 2 p0 .. 2 p0 + 7: K step p0 / 8, half (p0 / 4) & 1
+  uint8_t* bt0 = blv + td.bloff[t];
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
-    float2* o = reinterpret_cast<float2*>(base + (size_t)(v * nt + al) * ld_s) + p;
-    *o = make_float2((float)out[v].x, (float)out[v].y);
+    const int j = v * nt + al;
+    tc::split_store_h(bt0 + ((size_t)(j >> 7) * nsp + (p0 >> 3)) * (2 * tc::CM_TILE) +
+                          tc::core_off(j & 127, 8 * ((p0 >> 2) & 1)),
+                      lv[v], tsc[td.tsoff[t] + j]);
   }
 }
 
@@ -292,12 +369,14 @@ __global__ void k_ees_zglue(const double* __restrict__ C, int nstates, int nt, i
                             const int* __restrict__ chan, const double* __restrict__ vnc,
                             const int* __restrict__ order, int t0, int natm,
                             const double* __restrict__ occ, double* __restrict__ zt, int ldz,
-                            double* __restrict__ enl_s, double* __restrict__ fnl) {
+                            double* __restrict__ enl_s, double* __restrict__ fnl,
+                            unsigned int* __restrict__ zmax) {
   __shared__ double red[32];
   const int s = blockIdx.x;
   const double w = occ[s];
   const int jp = 4 * nt;
   double e = 0.0;
+  float zm = 0.f;  // largest |scaled Z| (float bits into *zmax, as k_ees_smat)
   for (int al = threadIdx.x; al < nt; al += blockDim.x) {
     const int atom = order[t0 + al];
     double f0 = 0.0, f1 = 0.0, f2 = 0.0;
@@ -310,6 +389,7 @@ __global__ void k_ees_zglue(const double* __restrict__ C, int nstates, int nt, i
       e += z * z * vn * w;
       const double zsc = z * (2.0 * vn * w);
       zt[(size_t)s * ldz + ch * nt + al] = zsc;
+      zm = fmaxf(zm, (float)fabs(zsc));
       f0 -= dx * zsc;
       f1 -= dy * zsc;
       f2 -= dz * zsc;
@@ -319,6 +399,8 @@ __global__ void k_ees_zglue(const double* __restrict__ C, int nstates, int nt, i
     f[1] += f1;
     f[2] += f2;
   }
+  for (int o = 16; o > 0; o >>= 1) zm = fmaxf(zm, __shfl_xor_sync(0xffffffffu, zm, o));
+  if ((threadIdx.x & 31) == 0 && zm > 0.f) atomicMax(zmax, __float_as_uint(zm));
   e = block_sum(e, red);
   if (threadIdx.x == 0) enl_s[s] += e;
 }
@@ -450,6 +532,19 @@ void nl_free(cpstep_ctx* c) {
   cudaFree(n.csum); cudaFree(n.zt);
   for (auto d : n.tdyp) cudaFree(d);
   n.tdyp.clear();
+  cudaFree(n.d_hmax);
+  n.d_hmax = nullptr;
+  cudaFree(n.blv);
+  cudaFree(n.tsc);
+  cudaFree(n.tinv);
+  cudaFree(n.alv);
+  cudaFree(n.pf_z);
+  cudaFree(n.pf_st);
+  n.pf_z = n.pf_st = nullptr;
+  n.pf_zbytes = n.pf_stbytes = 0;
+  n.blv = n.alv = nullptr;
+  n.tsc = n.tinv = nullptr;
+  n.alv_bytes = 0;
   n.sep = nullptr; n.sv = nullptr; n.d_order = nullptr; n.d_tch = nullptr; n.d_vn = nullptr;
   n.csum = nullptr; n.zt = nullptr; n.gspace_ok = 0;
   cudaFree(n.plist); cudaFree(n.pcount);
@@ -651,7 +746,10 @@ int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, 
     CPSTEP_CUDA_TRY(cudaMalloc(&n.csum, sizeof(double) * csz));
     CPSTEP_CUDA_TRY(cudaMalloc(&n.zt, sizeof(double) * zsz));
     n.tdyp.assign(at.ntyp, nullptr);
+    n.tdmax.assign(at.ntyp, 0.f);
+    n.tdmax_c.assign(at.ntyp, std::vector<float>(4, 0.f));
     n.ld_d32 = (c->npts + 1) / 2 * 2;
+    CPSTEP_CUDA_TRY(cudaMalloc(&n.d_hmax, sizeof(float) * 2 * std::max(1, at.ntyp)));
     std::vector<int> htch((size_t)at.ntyp * 4, -1);
     for (int t = 0; t < at.ntyp; ++t) {
       const size_t nc = n.tch[t].size();
@@ -665,11 +763,44 @@ int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, 
         htch[(size_t)t * 4 + k] = n.tch[t][k];
         CPSTEP_CUDA_TRY(cudaMemcpy(hd.data(), n.dyp + (size_t)n.tch[t][k] * c->npts,
                                    sizeof(double2) * c->npts, cudaMemcpyDeviceToHost));
-        for (int q = 0; q < c->npts; ++q)
+        for (int q = 0; q < c->npts; ++q) {
           hf[k * ld + q] = make_float2((float)hd[q].x, (float)hd[q].y);
+          n.tdmax[t] = std::max(n.tdmax[t], (float)std::hypot(hd[q].x, hd[q].y));
+          n.tdmax_c[t][k] = std::max(n.tdmax_c[t][k], (float)std::hypot(hd[q].x, hd[q].y));
+        }
       }
       CPSTEP_CUDA_TRY(cudaMemcpy(n.tdyp[t], hf.data(), sizeof(float2) * nc * ld,
                                  cudaMemcpyHostToDevice));
+    }
+    // FP16 levels of the S rows (zero past each type's rows and past K, never
+    // written there), their scales, and the A operand of the sums
+    {
+      const int K = 2 * c->npts;
+      n.blv_off.assign(at.ntyp, 0);
+      n.tsoff.assign(at.ntyp, 0);
+      size_t bl = 0;
+      long long ts = 0;
+      int nchmax = 1;
+      for (int t = 0; t < at.ntyp; ++t) {
+        const int nt = at.tstart[t + 1] - at.tstart[t];
+        n.blv_off[t] = bl;
+        n.tsoff[t] = ts;
+        bl += ees_lv_bytes(std::max(1, 4 * nt), K);
+        ts += 4LL * nt;
+        nchmax = std::max(nchmax, (int)n.tch[t].size());
+      }
+      CPSTEP_CUDA_TRY(cudaMalloc(&n.blv, bl));
+      CPSTEP_CUDA_TRY(cudaMemset(n.blv, 0, bl));
+      CPSTEP_CUDA_TRY(cudaMalloc(&n.tsc, sizeof(float) * (size_t)std::max(1LL, ts)));
+      CPSTEP_CUDA_TRY(cudaMalloc(&n.tinv, sizeof(float) * (size_t)std::max(1LL, ts)));
+      n.alv_bytes = ees_lv_bytes(nchmax * c->nstates, K);
+      CPSTEP_CUDA_TRY(cudaMalloc(&n.alv, n.alv_bytes));
+      int ntmax = 1;
+      for (int t = 0; t < at.ntyp; ++t) ntmax = std::max(ntmax, at.tstart[t + 1] - at.tstart[t]);
+      n.pf_zbytes = ees_pf_zbytes(c->nstates, ntmax);
+      n.pf_stbytes = ees_pf_stbytes(c->npts, ntmax);
+      CPSTEP_CUDA_TRY(cudaMalloc(&n.pf_z, n.pf_zbytes));
+      CPSTEP_CUDA_TRY(cudaMalloc(&n.pf_st, n.pf_stbytes));
     }
     CPSTEP_CUDA_TRY(cudaMalloc(&n.d_tch, sizeof(int) * htch.size()));
     CPSTEP_CUDA_TRY(cudaMemcpy(n.d_tch, htch.data(), sizeof(int) * htch.size(),
@@ -704,32 +835,47 @@ static int ees_gspace_run(cpstep_ctx* c, const double* psi, const double* occ, d
   CPSTEP_LAUNCH_CHECK();
   ees::TypeDims td{};
   for (int t = 0; t <= ntyp; ++t) td.tstart[t] = c->atoms.tstart[t];
-  for (int t = 0; t < ntyp; ++t) td.svoff[t] = n.sv_off[t];
+  for (int t = 0; t < ntyp; ++t) {
+    td.svoff[t] = n.sv_off[t];
+    td.tsoff[t] = n.tsoff[t];
+    td.bloff[t] = (long long)n.blv_off[t];
+  }
   NlAtoms A{};
   for (int k = 0; k < 9; ++k) A.hmati[k] = c->hmati[k];
   A.grid = (double)n.nkf;
-  ees::k_ees_smat<<<dim3(cdiv(c->npts, 256), natm), 256, 0, c->stream>>>(
-      n.sep, c->d_kx, c->d_ky, c->d_kz, c->npts, n.km, c->atoms.typ, c->atoms.rank, td, A,
-      n.ld_s, n.sv);
+  // bounds of |S| (the FP16 scales of the S rows' levels) and the largest |Z|
+  // entry per type (the psi force's)
+  CPSTEP_CUDA_TRY(cudaMemsetAsync(n.d_hmax, 0, sizeof(float) * 2 * ntyp, c->stream));
+  unsigned int* smax_u = reinterpret_cast<unsigned int*>(n.d_hmax);
+  unsigned int* zmax_u = smax_u + ntyp;
+  ees::k_ees_bound<<<cdiv(32 * natm, 256), 256, 0, c->stream>>>(
+      n.sep, natm, n.km, c->atoms.typ, c->atoms.rank, td, A, n.tsc, n.tinv, smax_u);
+  CPSTEP_LAUNCH_CHECK();
+  const int nsp_s = cdiv(2 * c->npts, 32) * 2;  // K steps of a pre-split row tile
+  ees::k_ees_smat<<<dim3(cdiv(c->npts, 128), cdiv(natm, 8)), 256, 0, c->stream>>>(
+      n.sep, c->d_kx, c->d_ky, c->d_kz, c->npts, n.km, c->atoms.typ, n.d_order, natm, td, A,
+      n.ld_s, n.sv, n.tsc, n.blv, nsp_s);
   CPSTEP_LAUNCH_CHECK();
   CPSTEP_CUDA_TRY(cudaMemsetAsync(n.enl_s, 0, sizeof(double) * S, c->stream));
   CPSTEP_CUDA_TRY(cudaMemsetAsync(n.fnl, 0, sizeof(double) * S * natm * 3, c->stream));
-  int nin_max = 1;  // the largest type's inner dimension of the psi force
-  for (int t = 0; t < ntyp; ++t)
-    nin_max = std::max(nin_max, (int)n.tch[t].size() * (c->atoms.tstart[t + 1] - c->atoms.tstart[t]));
-  if (int rc = ees_tc_presplit(c, psi, nin_max)) return rc;
   for (int t = 0; t < ntyp; ++t) {
     const int nch = (int)n.tch[t].size();
     const int nt = c->atoms.tstart[t + 1] - c->atoms.tstart[t];
     if (!nch || !nt) continue;
     const float* sv = n.sv + n.sv_off[t];
-    if (int rc = ees_tc_sums(c, sv, n.ld_s, n.tdyp[t], n.ld_d32, nch, 4 * nt, n.csum, S)) return rc;
+    if (int rc = ees_tc_sums_pre(c, psi, n.tdyp[t], n.ld_d32, nch, n.tdmax_c[t].data(),
+                                 n.blv + n.blv_off[t], 4 * nt, n.tinv + n.tsoff[t], n.alv,
+                                 n.alv_bytes, n.csum))
+      return rc;
     const int ldz = (nch * nt + 1) / 2 * 2;
     ees::k_ees_zglue<<<S, 128, 0, c->stream>>>(n.csum, S, nt, nch, n.d_tch + 4 * t, n.d_vn,
                                                 n.d_order, c->atoms.tstart[t], natm, occ, n.zt,
-                                                ldz, n.enl_s, n.fnl);
+                                                ldz, n.enl_s, n.fnl, zmax_u + t);
     CPSTEP_LAUNCH_CHECK();
-    if (int rc = ees_tc_force(c, sv, n.ld_s, n.tdyp[t], n.ld_d32, nch, nt, n.zt, ldz, -1.0, fpsi)) return rc;
+    if (int rc = ees_tc_force_pre(c, sv, n.ld_s, n.tdyp[t], n.ld_d32, nch, nt, n.zt, ldz, -1.0,
+                                  fpsi, n.d_hmax + t, n.d_hmax + ntyp + t, n.pf_z, n.pf_zbytes,
+                                  n.pf_st, n.pf_stbytes))
+      return rc;
   }
   ees::k_nl_finish<<<cdiv(std::max(1, 3 * natm), 128), 128, 0, c->stream>>>(
       n.enl_s, n.fnl, S, natm, energies, fatm);

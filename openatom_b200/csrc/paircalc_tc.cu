@@ -10,7 +10,7 @@
 // (the level pairs of total order <= 2; the dropped ones are O(2^-24 |ab|)) is
 // accumulated by tcgen05.mma (kind::f16, BF16 in, FP32 accumulators in TMEM),
 // smallest terms first, h_a h_b in an accumulator of its own.  That one holds
-// at most 128 reals of K (512 in the EES products): it is then read back
+// at most 128 reals of K: it is then read back
 // (tcgen05.ld) and added into an FP64 copy of the tile kept in the other half
 // of TMEM (two 32-bit columns per element, read and written back with
 // tcgen05.ld / tcgen05.st).  The five
@@ -33,8 +33,8 @@
 //     (the five small products in columns 0-127, hi*hi in columns 128-255;
 //     the FP64 tile holds columns 256-511), commits them to an mbarrier, and
 //     keeps the stages of a pre-split operand filled.
-// An operand that many CTAs share (psi in the EES sums, Z in the EES force,
-// T in the back-multiply) is split once, by k_presplit, into its BF16 levels
+// An operand that many CTAs share (T in the back-multiply) is split once, by
+// k_presplit, into its BF16 levels
 // in global memory in the same core-matrix image; the MMA warp brings its
 // chunks in with bulk copies (cp.async.bulk, one per chunk) and only the
 // other operand is split in the CTA.
@@ -53,21 +53,34 @@
 // it in FP64 in the epilogue (psi.T with T near I is then accurate relative
 // to T - diag T); the overlap of one operand with itself (S) sums its
 // diagonal in FP64 from the FP64 stage.
+//
+// The EES products (cp_ees_nonlocal.C's Z sums and psi force, evaluated in G
+// space) follow at the end of the file: both of their operands are split once
+// in global memory into two FP16 levels of power-of-two scaled values,
+// x s = h + m (22 significant bits of the FP32 value; s brings the largest
+// magnitude to [2^13, 2^14)), and multiplied as h m + m h + h h (three MMAs
+// per K step, kind::f16 with FP16 A and B); k_pp_tc (the sums, split-K with
+// FP64 folds every 512 reals) and k_pf_tc (the psi force, persistent over
+// point tiles) stream both operands with bulk copies and leave the CTA no
+// operand work.
 #include "ctx.cuh"
 #include "tc_sm100.cuh"
 
 namespace pctc {
 
 constexpr int ROWS = 128;                 // tile rows of A (M) and of B (N)
-constexpr int NLV = 3;                    // BF16 levels per element
+constexpr int NLV = 3;                    // BF16 levels per element (PairCalc products)
+constexpr int NLV_H = 2;                  // FP16 levels per element (EES products)
 constexpr int TILE_B = ROWS * 16 * 2;     // one K step, one level, one operand: 4 KB
 constexpr int STEP_B = NLV * TILE_B;      // one K step, all levels: 12 KB
+constexpr int STEP_H = NLV_H * TILE_B;    // the same, FP16 levels: 8 KB
 constexpr int NW = 512;                   // worker threads (warps 0-15)
 constexpr int MMA_WARP = NW / 32;         // warp 16 issues the MMAs
 constexpr int NTHR = NW + 32;
 constexpr int NSTP_MAX = 5;               // shared-memory stages of a pre-split operand (at most)
 constexpr int WBAR = 1;                   // named barrier of the workers
 constexpr uint32_t IDESC = tc::idesc_bf16_f32(ROWS, ROWS);
+constexpr uint32_t IDESC_H = tc::idesc_f16_f32(ROWS, ROWS);
 constexpr uint32_t TMEM_COLS = 512;       // two FP32 accumulators + the FP64 tile
 constexpr uint32_t TMEM_F64 = 2 * ROWS;   // first column of the FP64 tile
 
@@ -75,20 +88,16 @@ template <int MODE, int NLD, int NST, int KC>
 struct Cfg {
   static constexpr int KS = KC / 16;                     // MMA K steps per chunk
   static constexpr int U = KC / 8;                       // 8-element units per row
-  // chunks per TMEM group: the hi*hi accumulator holds 128 reals of K for the
-  // PairCalc products (S must stay orthonormal to 1e-8) and 512 for the EES
-  // sums and psi force (FP32 accumulation over 512 products leaves a relative
-  // error near 1e-6 in Z, far inside the energy budget), so their fold of the
-  // accumulator into the FP64 tile runs a quarter as often
-  static constexpr int NF = (MODE >= 2 ? 512 : 128) / KC;
+  // chunks per TMEM group: the hi*hi accumulator holds 128 reals of K (S
+  // must stay orthonormal to 1e-8)
+  static constexpr int NF = 128 / KC;
   static constexpr int RS = KC + 2;                      // row stride of a [128][KC] FP64 stage
   static constexpr int RSP = ROWS + 2;                   // row stride of a [KC][128] FP64 stage
-  static constexpr int RSF = KC + 4;                     // [128][KC] FP32 stage
-  static constexpr int RSPF = ROWS + 4;                  // [KC][128] FP32 stage
-  static constexpr int OPB = KS * STEP_B;                // one operand of one chunk, split
-  // operands split in the CTA (CA, CB) or pre-split in global memory (PA, PB)
-  static constexpr bool CA = MODE != 2, CB = MODE == 0 || MODE == 2;
-  static constexpr bool PA = MODE == 2, PB = MODE == 1 || MODE == 3;
+  static constexpr int STEP = STEP_B;                    // one K step, all levels
+  static constexpr int OPB = KS * STEP;                  // one operand of one chunk, split
+  // operands split in the CTA (CA, CB) or pre-split in global memory (PB)
+  static constexpr bool CA = true, CB = MODE == 0;
+  static constexpr bool PA = false, PB = MODE == 1;
   static constexpr bool PRE = PA || PB;
   // pre-split stages: as deep as shared memory allows (the back-multiply's
   // FP64 [KC][128] stages leave room for 3)
@@ -96,22 +105,15 @@ struct Cfg {
   static constexpr int NCONV = (CA ? 1 : 0) + (CB ? 1 : 0);
   static constexpr int RAW0 = ROWS * RS * 8;             // [128][KC] FP64
   static constexpr int WOFF = RAW0 * NLD;                // MODE 0: point weights after the rows
-  // one stage: MODE 0 the FP64 rows; MODE 1 in[j][p]; MODE 2 the FP32 S rows
-  // and 4 channels' dyp of the chunk's points; MODE 3 the FP32 S rows of the
-  // chunk's inner indices and 4 channels' dyp of the tile's points (dyp FP32)
-  static constexpr int RAW = MODE == 0   ? WOFF + KC / 2 * 8
-                             : MODE == 1 ? KC * RSP * 8
-                             : MODE == 2 ? ROWS * RSF * 4 + 4 * (KC / 2) * 8
-                                         : KC * RSPF * 4 + 4 * (ROWS / 2) * 8;
+  // one stage: MODE 0 the FP64 rows; MODE 1 in[j][p]
+  static constexpr int RAW = MODE == 0 ? WOFF + KC / 2 * 8 : KC * RSP * 8;
   static constexpr int CONV = 2 * NCONV * OPB;           // split operands, two chunk buffers
   static constexpr int PREB = PRE ? NSTP * OPB : 0;      // pre-split operand stages
   static constexpr int BYTES = 1024 + CONV + PREB + NST * RAW;  // + alignment slack
   static_assert(KC % 16 == 0 && 128 % KC == 0, "chunk");
   static_assert(RAW % 16 == 0 && OPB % 1024 == 0, "stage alignment");
   static_assert(ROWS * U * (MODE == 0 ? NLD : 1) == NW, "one 8-element unit per worker");
-  static_assert(ROWS * (KC / 2) % NW == 0 && KC * (ROWS / 2) % NW == 0 &&
-                    KC * (ROWS / 4) % NW == 0,
-                "copy mapping");
+  static_assert(ROWS * (KC / 2) % NW == 0 && KC * (ROWS / 2) % NW == 0, "copy mapping");
 };
 
 struct Args {
@@ -128,33 +130,19 @@ struct Args {
   double* part;      // overlap partial tiles [nsplit][N][M] (column-major, ld = M)
   double* out;       // backmul output [nout][ldo]
   int ldo;
-  // EES (MODE 2: forward sums, MODE 3: psi force), one atom type:
-  //   sv: S rows of the type, row j at sv + j ld_s (floats, complex pairs per
-  //       point); MODE 2 pairs j = v natm_t + a (v = Mn, d/dx, d/dy, d/dz),
-  //       MODE 3 rows a < natm_t (Mn)
-  //   dyp: the type's nch channel projectors (FP32), channel c at dyp + c ld_d
-  //        (ld_d even: 16-byte rows)
-  //   MODE 2: B-tile rows c jt + jj (c < nch, jj < jt) = channel c x pair
-  //           t jt + jj, jp pairs; output column c jp + j
-  //   MODE 3: inner index j = c natm_t + a (nin = nch natm_t)
-  const float* sv;
-  long long ld_s;
-  const float2* dyp;
-  int ld_d;
-  int nch, jt, jp, natm_t;
   double alpha, beta;
-  // pre-split operand (MODE 2: A = w psi; MODE 1: B = M^T without its
-  // diagonal; MODE 3: B = Z^T): [row tile][K step][level][4 KB], pre_nsp
-  // K steps per row tile
+  // pre-split operand (MODE 1: B = M^T without its diagonal): [row tile][K
+  // step][level][4 KB], pre_nsp K steps per row tile
   const uint8_t* pre;
   int pre_nsp;
   int* err;
 };
 
-// byte offset of (row r, k) in one K-step tile (k < 16)
-__host__ __device__ __forceinline__ int core_off(int r, int k) {
-  return (r >> 3) * 256 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
-}
+// byte offset of (row r, k) in one K-step tile (k < 16), and the FP16
+// two-level split of 8 scaled values of a row (tc_sm100.cuh)
+using tc::core_off;
+using tc::split_store_h;
+static_assert(tc::CM_TILE == TILE_B, "core-matrix tile");
 
 // 8 FP32 values of one row (8 consecutive K) -> three BF16 levels, stored as
 // 16 bytes at dst + v TILE_B
@@ -253,9 +241,9 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   int r0, c0, kbeg, kend;
-  if (MODE == 0 || MODE == 2) {
+  if (MODE == 0) {
     r0 = blockIdx.x * ROWS;
-    c0 = blockIdx.y * (MODE == 2 ? p.jt : ROWS);  // MODE 2: first pair of the B tile
+    c0 = blockIdx.y * ROWS;
     kbeg = blockIdx.z * p.kslab;
     kend = min(p.K, kbeg + p.kslab);
   } else {
@@ -304,7 +292,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
       auto pre_load = [&](int c) {
         const int st = c % NSTP;
         const uint8_t* src =
-            p.pre + ((size_t)prow * p.pre_nsp + (size_t)((kbeg + c * KC) >> 4)) * STEP_B;
+            p.pre + ((size_t)prow * p.pre_nsp + (size_t)((kbeg + c * KC) >> 4)) * C::STEP;
         tc::mbar_expect_tx(&pfull[st], C::OPB);
         tc::bulk_g2s(pre_base + (size_t)st * C::OPB, src, C::OPB, &pfull[st]);
       };
@@ -317,6 +305,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
         const uint32_t pre_s = bf_s + (uint32_t)(C::CONV + (ch % NSTP) * C::OPB);
         const uint32_t a0 = C::PA ? pre_s : bf_s + (uint32_t)conv_off(buf, 0);
         const uint32_t b0 = C::PB ? pre_s : bf_s + (uint32_t)conv_off(buf, 1);
+        // level pairs, smallest first; the last (h h) goes to its own accumulator
         constexpr int LA[6] = {2, 0, 1, 1, 0, 0};
         constexpr int LB[6] = {0, 2, 1, 0, 1, 0};
         bool ok = true;
@@ -329,8 +318,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
               ok = tc::mbar_wait_or(&tfree, (g - 1) & 1, stop);
               tc::fence_after_sync();
             }
-            const uint64_t da = tc::smem_desc_kmajor(a0 + s * STEP_B + LA[t] * TILE_B, 128, 256);
-            const uint64_t db = tc::smem_desc_kmajor(b0 + s * STEP_B + LB[t] * TILE_B, 128, 256);
+            const uint64_t da = tc::smem_desc_kmajor(a0 + s * C::STEP + LA[t] * TILE_B, 128, 256);
+            const uint64_t db = tc::smem_desc_kmajor(b0 + s * C::STEP + LB[t] * TILE_B, 128, 256);
             if (ok) tc::mma_bf16(t == 5 ? tbase + ROWS : tbase, da, db, IDESC, zero ? 0u : 1u);
           }
         }
@@ -400,44 +389,6 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
             tc::cp16(dst + r * RS + 2 * pc, g, ok ? 16 : 0);
           }
         }
-      } else if (MODE == 2) {
-        // S rows of pairs c0 .. c0 + jt, KC reals (FP32), and dyp of the chunk's points
-        float* fs = reinterpret_cast<float*>(ra);
-        for (int q = tid; q < p.jt * (KC / 4); q += NW) {
-          const int jj = q / (KC / 4), pc = q % (KC / 4);
-          const int j = c0 + jj, k = k0 + 4 * pc;
-          const bool ok = j < p.jp && k < kend;  // kend even, rows padded to 4 floats
-          const float* g = ok ? p.sv + (size_t)j * p.ld_s + k : p.sv;
-          tc::cp16(fs + jj * C::RSF + 4 * pc, g, ok ? 16 : 0);
-        }
-        float2* dd = reinterpret_cast<float2*>(fs + ROWS * C::RSF);
-        for (int q = tid; q < p.nch * (KC / 4); q += NW) {  // two points per copy
-          const int c = q / (KC / 4), e = 2 * (q % (KC / 4));
-          const int pt = (k0 >> 1) + e;
-          const int nb = 2 * pt + 2 < kend ? 16 : (2 * pt < kend ? 8 : 0);
-          tc::cp16(dd + c * (KC / 2) + e, nb ? p.dyp + (size_t)c * p.ld_d + pt : p.dyp, nb);
-        }
-      } else if (MODE == 3) {
-        // S rows (Mn) of the chunk's inner indices j = c natm_t + a over the
-        // tile's 64 points, and the channels' dyp over the same points
-        float* fs = reinterpret_cast<float*>(ra);
-#pragma unroll
-        for (int it = 0; it < KC * (ROWS / 4) / NW; ++it) {
-          const int q = tid + NW * it;
-          const int jj = q / (ROWS / 4), pc = q % (ROWS / 4);
-          const int j = k0 + jj, pr = r0 + 4 * pc;  // reals
-          const bool ok = j < kend && pr < p.M;      // M reals, rows padded to 4 floats
-          const int a = ok ? j % p.natm_t : 0;
-          const float* g = ok ? p.sv + (size_t)a * p.ld_s + pr : p.sv;
-          tc::cp16(fs + jj * C::RSPF + 4 * pc, g, ok ? 16 : 0);
-        }
-        float2* dd = reinterpret_cast<float2*>(fs + KC * C::RSPF);
-        for (int q = tid; q < p.nch * (ROWS / 4); q += NW) {  // two points per copy
-          const int c = q / (ROWS / 4), e = 2 * (q % (ROWS / 4));
-          const int pt = (r0 >> 1) + e;
-          const int nb = 2 * pt + 2 < p.M ? 16 : (2 * pt < p.M ? 8 : 0);
-          tc::cp16(dd + c * (ROWS / 2) + e, nb ? p.dyp + (size_t)c * p.ld_d + pt : p.dyp, nb);
-        }
       } else {
         // in[j][p] rows j = k0 .. k0 + KC, 128 points from r0
 #pragma unroll
@@ -457,10 +408,10 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
     auto convert = [&](int ch, int st, int buf) {
       const int k0 = kbeg + ch * KC;
       const double* ra = raw + (size_t)st * (C::RAW / 8);
-      const int op = (MODE == 0 && NLD == 2) ? (tid >> 8) : (MODE == 2 ? 1 : 0);
+      const int op = (MODE == 0 && NLD == 2) ? (tid >> 8) : 0;
       const int q = (MODE == 0 && NLD == 2) ? (tid & 255) : tid;
       const int r = (q & 7) + 8 * ((q >> 3) / U), u = (q >> 3) % U;
-      const int off = (u >> 1) * STEP_B + core_off(r, (u & 1) * 8);
+      const int off = (u >> 1) * C::STEP + core_off(r, (u & 1) * 8);
       uint8_t* dA = base + conv_off(buf, 0) + off;
       uint8_t* dB = base + conv_off(buf, 1) + off;
       const float one[4] = {1.f, 1.f, 1.f, 1.f};
@@ -471,39 +422,6 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
         for (int e = 0; e < 8; ++e) x[e] = ra[(8 * u + e) * RSP + r];
         to_f32(x, one, f);
         split_store(dA, f);
-        return;
-      }
-      // EES operands in FP32 (S is FP32): conj(dyp) S, one rounding per product
-      if (MODE == 3) {  // A[p][j] = (conj(dyp_c) S_a)(point r / 2), re or im
-        const float* fs = reinterpret_cast<const float*>(ra);
-        const float2* dd = reinterpret_cast<const float2*>(fs + KC * C::RSPF);
-        const int pl = r >> 1;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int j = k0 + 8 * u + e;
-          const int c = min(j / p.natm_t, 3);
-          const float2 sa = *reinterpret_cast<const float2*>(fs + (8 * u + e) * C::RSPF + 2 * pl);
-          const float2 d = dd[c * (ROWS / 2) + pl];
-          f[e] = (r & 1) ? fmaf(d.x, sa.y, -d.y * sa.x) : fmaf(d.x, sa.x, d.y * sa.y);
-        }
-        split_store(dA, f);
-        return;
-      }
-      if (MODE == 2) {  // B row r = channel c, pair jj: conj(dyp_c) S_pair
-        const float* fs = reinterpret_cast<const float*>(ra);
-        const float2* dd = reinterpret_cast<const float2*>(fs + ROWS * C::RSF);
-        const int c = r / p.jt, jj = r - c * p.jt;
-        const bool ok = c < p.nch;
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const float2 sa =
-              ok ? *reinterpret_cast<const float2*>(fs + jj * C::RSF + 8 * u + 2 * e)
-                 : make_float2(0.f, 0.f);
-          const float2 d = ok ? dd[c * (KC / 2) + 4 * u + e] : make_float2(0.f, 0.f);
-          f[2 * e] = fmaf(d.x, sa.x, d.y * sa.y);
-          f[2 * e + 1] = fmaf(d.x, sa.y, -d.y * sa.x);
-        }
-        split_store(dB, f);
         return;
       }
       const double2* s2 =
@@ -621,7 +539,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
     // accumulator out of TMEM, 8 columns at a time
     const int rl = 32 * (warp & 3) + lane, cb = 32 * (warp >> 2);
     const uint32_t tsm = tbase + tlanes + (uint32_t)(32 * (warp >> 2));
-    const double sc = (MODE == 1 || MODE == 3) && r0 + rl < p.M
+    const double sc = MODE == 1 && r0 + rl < p.M
                           ? p.alpha * (p.w ? p.w[(r0 + rl) >> 1] : 1.0)
                           : 0.0;
 #pragma unroll 1
@@ -641,16 +559,11 @@ __global__ void __launch_bounds__(NTHR, 1) k_pc_tc(const Args p) {
           if (r < p.M && c < p.N)
             p.part[(size_t)blockIdx.z * p.M * p.N + (size_t)c * p.M + r] =
                 (same && cb + e == rl) ? diag_s[rl] : acc;
-        } else if (MODE == 2) {  // tile column cb + e = channel ch, pair c0 + jj -> ch jp + pair
-          const int r = r0 + rl;
-          const int ch = (cb + e) / p.jt, j = c0 + (cb + e) - ch * p.jt;
-          if (r < p.M && ch < p.nch && j < p.jp)
-            p.part[(size_t)blockIdx.z * p.M * p.N + (size_t)(ch * p.jp + j) * p.M + r] = acc;
         } else {
           accs[e8] = acc;
         }
       }
-      if (MODE == 1 || MODE == 3) {
+      if (MODE == 1) {
         // out = alpha w (acc [+ diag]) + beta out: every load of the piece is
         // issued before its first store, so their latencies overlap
         const int pt = r0 + rl;
@@ -728,88 +641,645 @@ int presplit(cpstep_ctx* c, const double* src, long long ldr, int rows, int K, c
   return CPSTEP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Products of two pre-split operands (FP16 levels of power-of-two scaled
+// values, the k_presplit image): the EES sums with A = w psi dyp_c (rows
+// c S + s) and B = the S rows of one atom type (rows v natm_t + a), both
+// split once in global memory.  No operand work is left in the CTA; the roles
+// are warp-specialised:
+//   warp 17 (lane 0)  streams each chunk's A and B levels with two bulk copies
+//                     into one of PP_NST stages, as soon as the stage is free;
+//   warp 16 (lane 0)  issues the 3 MMAs per K step (h m, m h, h h, all into one
+//                     FP32 accumulator) as soon as a stage has landed, never
+//                     waiting for MMAs to complete; the fold groups (512 reals)
+//                     alternate between two accumulators;
+//   warps 0-15        add each finished group's accumulator into the FP64 tile
+//                     and write the tile.
+//   part[ks][(c jp + j) S + s] = rinv[c] cinv[j] sum_{k in slab ks} A[c S + s][k] B[j][k]
+// Handshakes (mbarriers, every wait bounded): full[st] (both copies of the
+// stage landed), empty[st] (the MMAs that read it completed), gfull[b] (a
+// group's MMAs into accumulator b completed), tfree[b] (accumulator b read
+// back).  TMEM: accumulators in columns 0-127 and 128-255, the FP64 tile in
+// 256-511.
+constexpr int PP_KC = 32;                     // reals per chunk (2 K steps)
+constexpr int PP_KS = PP_KC / 16;
+constexpr int PP_OPB = PP_KS * STEP_H;        // one operand of one chunk: 16 KB
+constexpr int PP_STAGE = 2 * PP_OPB;          // A then B
+constexpr int PP_NST = 6;                     // stages
+constexpr int PP_NF = 512 / PP_KC;            // chunks per fold group
+constexpr int PP_BYTES = 1024 + PP_NST * PP_STAGE;
+constexpr int PP_MMA_WARP = NW / 32, PP_LOAD_WARP = NW / 32 + 1;
+constexpr int PP_NTHR = NW + 64;
+
+struct PPArgs {
+  const uint8_t* a;  // [row tile][K step][level][4 KB], nsp K steps per row tile
+  const uint8_t* b;
+  int nsp;
+  int M, N, K;       // rows of A (nch S), rows of B (jp), reals
+  int kslab;         // reals per split (a multiple of 512)
+  int S, jp;         // states (rows of one channel block of A), B rows per channel block
+  float rinv[4];     // 1 / scale of A's channel blocks
+  const float* cinv; // 1 / scale of each B row (device, N entries)
+  double* part;      // [nsplit][nch jp][S]
+  int* err;
+};
+
+__global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
+  extern __shared__ uint8_t dsm[];
+  __shared__ uint64_t full[PP_NST], empty[PP_NST], gfull[2], tfree[2];
+  __shared__ uint32_t tslot;
+  __shared__ int stop_s, issued_s, req_s;
+  volatile int* stop = &stop_s;
+  const uint32_t s0 = tc::smem_u32(dsm);
+  uint8_t* base = dsm + (((s0 + 1023u) & ~1023u) - s0);
+  const uint32_t base_s = tc::smem_u32(base);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r0 = blockIdx.x * ROWS, c0 = blockIdx.y * ROWS;
+  const int kbeg = blockIdx.z * p.kslab, kend = min(p.K, kbeg + p.kslab);
+  const int nch = kend > kbeg ? (kend - kbeg + PP_KC - 1) / PP_KC : 0;
+  const int ngroups = (nch + PP_NF - 1) / PP_NF;
+
+  if (warp == 0) tc::tmem_alloc(&tslot, TMEM_COLS);
+  if (tid == 0) {
+    for (int i = 0; i < PP_NST; ++i) {
+      tc::mbar_init(&full[i], 1);
+      tc::mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      tc::mbar_init(&gfull[i], 1);
+      tc::mbar_init(&tfree[i], NW / 32);
+    }
+    stop_s = 0;
+    issued_s = 0;
+    req_s = 0;
+    tc::fence_mbar_init();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = tslot;
+  const uint32_t tlanes = (uint32_t)(32 * (warp & 3)) << 16;
+  const uint32_t tf64 = tbase + tlanes + TMEM_F64 + (uint32_t)(64 * ((warp >> 2) & 3));
+
+  if (warp == PP_LOAD_WARP) {
+    if (lane == 0) {
+      int req = 0;
+      for (; req < nch; ++req) {
+        const int st = req % PP_NST;
+        if (req >= PP_NST &&  // the MMAs of chunk req - PP_NST read this stage
+            !tc::mbar_wait_fast(&empty[st], ((req - PP_NST) / PP_NST) & 1, stop)) {
+          *stop = 1;
+          break;
+        }
+        const size_t kstep = (size_t)((kbeg + req * PP_KC) >> 4);
+        const uint8_t* ga = p.a + ((size_t)blockIdx.x * p.nsp + kstep) * STEP_H;
+        const uint8_t* gb = p.b + ((size_t)blockIdx.y * p.nsp + kstep) * STEP_H;
+        uint8_t* sa = base + (size_t)st * PP_STAGE;
+        tc::mbar_expect_tx(&full[st], PP_STAGE);
+        tc::bulk_g2s(sa, ga, PP_OPB, &full[st]);
+        tc::bulk_g2s(sa + PP_OPB, gb, PP_OPB, &full[st]);
+      }
+      req_s = req;
+    }
+    __syncwarp();
+  } else if (warp == PP_MMA_WARP) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int c = 0; c < nch; ++c) {
+        const int st = c % PP_NST, g = c / PP_NF, acc = g & 1;
+        const bool first = c % PP_NF == 0;
+        if (first && g >= 2) {  // accumulator acc was folded (group g - 2)
+          if (!tc::mbar_wait_fast(&tfree[acc], ((g - 2) >> 1) & 1, stop)) break;
+          tc::fence_after_sync();
+        }
+        if (!tc::mbar_wait_fast(&full[st], (c / PP_NST) & 1, stop)) break;
+        tc::fence_after_sync();
+        const uint32_t a0 = base_s + (uint32_t)(st * PP_STAGE), b0 = a0 + PP_OPB;
+#pragma unroll
+        for (int s = 0; s < PP_KS; ++s) {
+#pragma unroll
+          for (int t = 0; t < 3; ++t) {
+            // level pairs (m, h), (h, m), (h, h)
+            const int la = t == 0 ? 1 : 0, lb = t == 1 ? 1 : 0;
+            const uint64_t da = tc::smem_desc_kmajor(a0 + s * STEP_H + la * TILE_B, 128, 256);
+            const uint64_t db = tc::smem_desc_kmajor(b0 + s * STEP_H + lb * TILE_B, 128, 256);
+            const bool zero = first && s == 0 && t == 0;
+            tc::mma_bf16(tbase + (uint32_t)(acc * ROWS), da, db, IDESC_H, zero ? 0u : 1u);
+          }
+        }
+        tc::commit(&empty[st]);
+        if (c % PP_NF == PP_NF - 1 || c == nch - 1) tc::commit(&gfull[acc]);
+        issued = c + 1;
+      }
+      if (issued < nch) *stop = 1;
+      issued_s = issued;
+    }
+    __syncwarp();
+  } else {
+    int bad = 0;
+    for (int g = 0; g < ngroups && !bad; ++g) {
+      const int acc = g & 1;
+      if (!__all_sync(0xffffffffu, tc::mbar_wait_fast(&gfull[acc], (g >> 1) & 1, stop))) {
+        bad = 1;
+        break;
+      }
+      tc::fence_after_sync();
+      float v[32];
+      tc::tmem_ld32(tbase + tlanes + (uint32_t)(acc * ROWS + 32 * (warp >> 2)), v);
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&tfree[acc]);
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {  // 8 columns (16 words) per TMEM round trip
+        uint32_t a[16];
+        if (g > 0) {
+          tc::tmem_ld16(tf64 + 16 * h, a);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) a[e] = 0u;
+        }
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const double d =
+              __hiloint2double((int)a[2 * e + 1], (int)a[2 * e]) + (double)v[8 * h + e];
+          a[2 * e] = (uint32_t)__double2loint(d);
+          a[2 * e + 1] = (uint32_t)__double2hiint(d);
+        }
+        tc::tmem_st16(tf64 + 16 * h, a);
+      }
+      tc::tmem_wait_st();
+    }
+    if (tc::bar_or(WBAR, NW, bad)) *stop = 1;
+  }
+
+  tc::fence_before_sync();
+  __syncthreads();
+  const int failed = *stop;
+  if (!failed && warp < PP_MMA_WARP && nch > 0) {
+    tc::fence_after_sync();
+    const int rl = 32 * (warp & 3) + lane, cb = 32 * (warp >> 2);
+    const int r = r0 + rl;
+    const int ch = r < p.M ? r / p.S : 0, s = r - ch * p.S;
+    const double ri =
+        (double)(ch == 0 ? p.rinv[0] : ch == 1 ? p.rinv[1] : ch == 2 ? p.rinv[2] : p.rinv[3]);
+#pragma unroll 1
+    for (int pc = 0; pc < 4; ++pc) {
+      uint32_t a[16];
+      tc::tmem_ld16(tf64 + 16 * pc, a);
+#pragma unroll
+      for (int e8 = 0; e8 < 8; ++e8) {
+        const int j = c0 + cb + 8 * pc + e8;
+        if (r < p.M && j < p.N) {
+          const double acc = __hiloint2double((int)a[2 * e8 + 1], (int)a[2 * e8]);
+          p.part[(size_t)blockIdx.z * p.M * p.N + ((size_t)ch * p.jp + j) * p.S + s] =
+              acc * ri * (double)p.cinv[j];
+        }
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    if (failed) {
+      // requested copies land and issued MMAs complete before the CTA exits
+      for (int c = issued_s; c < req_s; ++c) tc::mbar_wait(&full[c % PP_NST], (c / PP_NST) & 1);
+      if (issued_s > 0)
+        tc::mbar_wait(&empty[(issued_s - 1) % PP_NST], ((issued_s - 1) / PP_NST) & 1);
+    }
+    __syncwarp();
+    tc::tmem_free(tbase, TMEM_COLS);
+  }
+  if (failed && tid == 0) atomicOr(p.err, 1);
+}
+
+// A of the EES sums: rows c S + s (c < nch, s < S) = w psi_s dyp_c (complex,
+// real view), scaled by sig[c] (a power of two), two FP16 levels in the
+// k_presplit image; rows past nch S and reals past K are zero.  One warp =
+// 16 states x 16 reals of one K step for every channel: psi is read once.
+struct PreA {
+  const double* psi;  // [S][K] reals
+  const double* w;    // per point (1 or 2)
+  const float2* dyp;  // channel c at dyp + c ld_d
+  int ld_d;
+  int S, K, nch, nsp;
+  float sig[4];
+  uint8_t* dst;
+  int* err;
+};
+__global__ void __launch_bounds__(256) k_presplit_ees_a(const PreA a) {
+  const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int stiles = cdiv(a.S, ROWS);
+  const long long nwarps = (long long)stiles * a.nsp * 8;
+  if (wid >= nwarps) return;
+  const int gp = (int)(wid % 8);
+  const long long rest = wid / 8;
+  const int st = (int)(rest % a.nsp);
+  const int rt = (int)(rest / a.nsp);
+  const int sl = (lane & 7) + 8 * (lane >> 4) + 16 * gp;
+  const int kh = (lane >> 3) & 1;
+  const int s = rt * ROWS + sl;
+  const int k0 = 16 * st + 8 * kh;  // first real; 4 points from k0 / 2
+  double2 x[4];
+  float ws[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int pt = (k0 >> 1) + e;
+    const bool ok = s < a.S && 2 * pt < a.K;
+    x[e] = ok ? *reinterpret_cast<const double2*>(a.psi + (size_t)s * a.K + 2 * pt)
+              : make_double2(0.0, 0.0);
+    ws[e] = ok ? (float)a.w[pt] : 0.f;
+  }
+  bool big = false;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    if (c >= a.nch) break;
+    float f[8];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int pt = (k0 >> 1) + e;
+      const float2 d = 2 * pt < a.K ? a.dyp[(size_t)c * a.ld_d + pt] : make_float2(0.f, 0.f);
+      const float xr = (float)x[e].x * ws[e], xi = (float)x[e].y * ws[e];
+      f[2 * e] = fmaf(xr, d.x, -xi * d.y);
+      f[2 * e + 1] = fmaf(xr, d.y, xi * d.x);
+    }
+    const float sc = a.sig[c];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) big |= !(fabsf(f[e] * sc) < 32768.f);
+    if (s < a.S) {  // row c S + s of A; rows past nch S are never read into the output
+      const int r = c * a.S + s;
+      split_store_h(a.dst + ((size_t)(r / ROWS) * a.nsp + st) * STEP_H + core_off(r % ROWS, 8 * kh),
+                    f, sc);
+    }
+  }
+  if (big) atomicOr(a.err, 4);
+}
+
+// ---------------------------------------------------------------------------
+// psi force of one atom type from pre-split operands:
+//   F_s(p) += alpha w(p) sum_c conj(dyp_c(p)) Q_cs(p),  Q_cs(p) = sum_a Z(c natm_t + a, s) S_a(p)
+// as D = A B^T with A = Z (rows 4 s + c, K = the type's atoms) and B = the
+// real views of the S (Mn) rows transposed (rows = reals of the points, K =
+// atoms), both FP16 levels (k_presplit_z, k_presplit_st).  One output tile =
+// 32 states x 4 channel rows x 128 reals (64 points); the CTAs of one row
+// tile walk the point tiles (persistent), the K chunks of a tile streamed like
+// k_pp_tc's (warp 17 copies, warp 16 issues into one of two accumulators),
+// and warps 0-15 finish each tile: the 4 channel rows of a state are combined
+// by lane shuffles and added into F.
+constexpr int PF_KC = 64;                 // atoms per chunk (4 K steps)
+constexpr int PF_KS = PF_KC / 16;
+constexpr int PF_OPB = PF_KS * STEP_H;    // 32 KB
+constexpr int PF_STAGE = 2 * PF_OPB;      // 64 KB
+constexpr int PF_NST = 3;
+constexpr int PF_BYTES = 1024 + PF_NST * PF_STAGE;
+constexpr uint32_t PF_TMEM_COLS = 2 * ROWS;
+
+struct PFArgs {
+  const uint8_t* a;   // Z levels [row tile][K step][level][4 KB], nks K steps per row tile
+  const uint8_t* b;   // S^T levels, the same image over the point reals
+  int nks;            // K steps: cdiv(natm_t, 16)
+  int ntile;          // row tiles of B (point tiles)
+  int S, nch, npts;
+  const float* zmax;  // the FP16 scales of Z (pow2_scale(*zmax)) and of S^T
+  const float* smax;  // (pow2_scale(*smax)), as k_presplit_z / k_presplit_st
+  const float2* dyp;  // channel c at dyp + c ld_d (FP32)
+  int ld_d;
+  const double* w;    // per point
+  double alpha;
+  double* f;          // [S][2 npts] (+=)
+  int* err;
+};
+
+__global__ void __launch_bounds__(PP_NTHR, 1) k_pf_tc(const PFArgs p) {
+  extern __shared__ uint8_t dsm[];
+  __shared__ uint64_t full[PF_NST], empty[PF_NST], gfull[2], tfree[2];
+  __shared__ uint32_t tslot;
+  __shared__ int stop_s, issued_s, req_s;
+  volatile int* stop = &stop_s;
+  const uint32_t s0 = tc::smem_u32(dsm);
+  uint8_t* base = dsm + (((s0 + 1023u) & ~1023u) - s0);
+  const uint32_t base_s = tc::smem_u32(base);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m = blockIdx.y;
+  const int nkc = (p.nks + PF_KS - 1) / PF_KS;  // K chunks per tile
+  // this CTA's point tiles: blockIdx.x, + gridDim.x, ...
+  const int ntl = p.ntile > (int)blockIdx.x ? (p.ntile - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int nitem = ntl * nkc;
+
+  if (warp == 0) tc::tmem_alloc(&tslot, PF_TMEM_COLS);
+  if (tid == 0) {
+    for (int i = 0; i < PF_NST; ++i) {
+      tc::mbar_init(&full[i], 1);
+      tc::mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      tc::mbar_init(&gfull[i], 1);
+      tc::mbar_init(&tfree[i], NW / 32);
+    }
+    stop_s = 0;
+    issued_s = 0;
+    req_s = 0;
+    tc::fence_mbar_init();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = tslot;
+  const uint32_t tlanes = (uint32_t)(32 * (warp & 3)) << 16;
+
+  if (warp == PP_LOAD_WARP) {
+    if (lane == 0) {
+      int req = 0;
+      for (; req < nitem; ++req) {
+        const int st = req % PF_NST;
+        if (req >= PF_NST && !tc::mbar_wait_fast(&empty[st], ((req - PF_NST) / PF_NST) & 1, stop)) {
+          *stop = 1;
+          break;
+        }
+        const int n = blockIdx.x + (req / nkc) * gridDim.x, kc = req % nkc;
+        const int ks0 = kc * PF_KS, ksz = min(PF_KS, p.nks - ks0);
+        const uint32_t bytes = (uint32_t)ksz * STEP_H;
+        uint8_t* sa = base + (size_t)st * PF_STAGE;
+        tc::mbar_expect_tx(&full[st], 2 * bytes);
+        tc::bulk_g2s(sa, p.a + ((size_t)m * p.nks + ks0) * STEP_H, bytes, &full[st]);
+        tc::bulk_g2s(sa + PF_OPB, p.b + ((size_t)n * p.nks + ks0) * STEP_H, bytes, &full[st]);
+      }
+      req_s = req;
+    }
+    __syncwarp();
+  } else if (warp == PP_MMA_WARP) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int it = 0; it < nitem; ++it) {
+        const int st = it % PF_NST, tl = it / nkc, kc = it % nkc, acc = tl & 1;
+        if (kc == 0 && tl >= 2) {  // accumulator acc read back (tile tl - 2)
+          if (!tc::mbar_wait_fast(&tfree[acc], ((tl - 2) >> 1) & 1, stop)) break;
+          tc::fence_after_sync();
+        }
+        if (!tc::mbar_wait_fast(&full[st], (it / PF_NST) & 1, stop)) break;
+        tc::fence_after_sync();
+        const int ksz = min(PF_KS, p.nks - kc * PF_KS);
+        const uint32_t a0 = base_s + (uint32_t)(st * PF_STAGE), b0 = a0 + PF_OPB;
+        for (int s = 0; s < ksz; ++s) {
+#pragma unroll
+          for (int t = 0; t < 3; ++t) {
+            const int la = t == 0 ? 1 : 0, lb = t == 1 ? 1 : 0;  // (m, h), (h, m), (h, h)
+            const uint64_t da = tc::smem_desc_kmajor(a0 + s * STEP_H + la * TILE_B, 128, 256);
+            const uint64_t db = tc::smem_desc_kmajor(b0 + s * STEP_H + lb * TILE_B, 128, 256);
+            const bool zero = kc == 0 && s == 0 && t == 0;
+            tc::mma_bf16(tbase + (uint32_t)(acc * ROWS), da, db, IDESC_H, zero ? 0u : 1u);
+          }
+        }
+        tc::commit(&empty[st]);
+        if (kc == nkc - 1) tc::commit(&gfull[acc]);
+        issued = it + 1;
+      }
+      if (issued < nitem) *stop = 1;
+      issued_s = issued;
+    }
+    __syncwarp();
+  } else {
+    // rows 4 s + c of this warp's lanes; columns (reals) 32 (warp / 4).. of the tile
+    const int rl = 32 * (warp & 3) + lane;
+    const int rg = m * ROWS + rl, s = rg >> 2, c = rg & 3;
+    const bool live = s < p.S && c < p.nch;
+    const double rinv = 1.0 / ((double)tc::pow2_scale(*p.zmax) * (double)tc::pow2_scale(*p.smax));
+    int bad = 0;
+    for (int tl = 0; tl < ntl && !bad; ++tl) {
+      const int acc = tl & 1;
+      if (!__all_sync(0xffffffffu, tc::mbar_wait_fast(&gfull[acc], (tl >> 1) & 1, stop))) {
+        bad = 1;
+        break;
+      }
+      tc::fence_after_sync();
+      float v[32];
+      tc::tmem_ld32(tbase + tlanes + (uint32_t)(acc * ROWS + 32 * (warp >> 2)), v);
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&tfree[acc]);
+      const int n = blockIdx.x + tl * gridDim.x;
+      const int pt0 = (n * ROWS + 32 * (warp >> 2)) >> 1;  // 16 points
+      const bool wr = c == 0 && s < p.S;
+      double2* fr = reinterpret_cast<double2*>(p.f + (size_t)(wr ? s : 0) * 2 * p.npts);
+#pragma unroll
+      for (int hf = 0; hf < 2; ++hf) {  // 8 points at a time, every load issued first
+        float2 d[8];
+        double2 fo[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int pt = pt0 + 8 * hf + e;
+          d[e] = (live && pt < p.npts) ? p.dyp[(size_t)c * p.ld_d + pt] : make_float2(0.f, 0.f);
+          fo[e] = (wr && pt < p.npts) ? fr[pt] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const float qx = v[16 * hf + 2 * e], qy = v[16 * hf + 2 * e + 1];
+          float ox = fmaf(d[e].x, qx, d[e].y * qy), oy = fmaf(d[e].x, qy, -d[e].y * qx);
+          ox += __shfl_xor_sync(0xffffffffu, ox, 1);  // conj(d) q summed over the
+          oy += __shfl_xor_sync(0xffffffffu, oy, 1);  // state's 4 channel lanes
+          ox += __shfl_xor_sync(0xffffffffu, ox, 2);
+          oy += __shfl_xor_sync(0xffffffffu, oy, 2);
+          const int pt = pt0 + 8 * hf + e;
+          if (wr && pt < p.npts) {
+            const double sc = p.alpha * p.w[pt] * rinv;
+            fr[pt] = make_double2(fma(sc, (double)ox, fo[e].x), fma(sc, (double)oy, fo[e].y));
+          }
+        }
+      }
+    }
+    if (tc::bar_or(WBAR, NW, bad)) *stop = 1;
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  const int failed = *stop;
+  if (warp == 0) {
+    tc::fence_after_sync();
+    if (failed) {
+      for (int c = issued_s; c < req_s; ++c) tc::mbar_wait(&full[c % PF_NST], (c / PF_NST) & 1);
+      if (issued_s > 0)
+        tc::mbar_wait(&empty[(issued_s - 1) % PF_NST], ((issued_s - 1) / PF_NST) & 1);
+    }
+    __syncwarp();
+    tc::tmem_free(tbase, PF_TMEM_COLS);
+  }
+  if (failed && tid == 0) atomicOr(p.err, 1);
+}
+
+// Z levels for k_pf_tc: rows 4 s + c (zero for c >= nch or s >= S), K = the
+// type's atoms a (zero past natm_t): Z(c natm_t + a, s) = zt[s ldz + c natm_t
+// + a], scaled by pow2_scale(*zmax).  One thread = 8 atoms of one row.
+__global__ void k_presplit_z(const double* __restrict__ zt, int ldz, int S, int nch, int natm_t,
+                             int nks, int nrow, const float* __restrict__ zmax,
+                             uint8_t* __restrict__ dst) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nrow * nks * 2) return;
+  const int r = (int)(i % nrow);
+  const int u = (int)(i / nrow);  // 8-atom unit: K step u / 2, half u & 1
+  const int s = r >> 2, c = r & 3;
+  const float sc = tc::pow2_scale(*zmax);
+  float f[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const int a = 8 * u + e;
+    f[e] = (s < S && c < nch && a < natm_t) ? (float)zt[(size_t)s * ldz + c * natm_t + a] : 0.f;
+  }
+  split_store_h(dst + ((size_t)(r / ROWS) * nks + (u >> 1)) * STEP_H + core_off(r % ROWS, 8 * (u & 1)),
+                f, sc);
+}
+
+// The real views of a type's Mn rows transposed for k_pf_tc: rows = reals k of
+// the points (zero past 2 npts), K = atoms (zero past natm_t), from the FP32
+// rows sv[a ld_s + k], scaled by pow2_scale(*smax).  One thread = 8 atoms of
+// one real.
+__global__ void k_presplit_st(const float* __restrict__ sv, long long ld_s, int kr, int natm_t,
+                              int nks, int nrow, const float* __restrict__ smax,
+                              uint8_t* __restrict__ dst) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nrow * nks * 2) return;
+  const int k = (int)(i % nrow);
+  const int u = (int)(i / nrow);
+  const float sc = tc::pow2_scale(*smax);
+  float f[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const int a = 8 * u + e;
+    f[e] = (k < kr && a < natm_t) ? sv[(size_t)a * ld_s + k] : 0.f;
+  }
+  split_store_h(dst + ((size_t)(k / ROWS) * nks + (u >> 1)) * STEP_H + core_off(k % ROWS, 8 * (u & 1)),
+                f, sc);
+}
+
 }  // namespace pctc
 
-// BF16 levels of w psi for the EES sums (offset 0 of the level buffer), with
-// room after them for a Z of up to nin_max inner indices (ees_tc_force).
-int ees_tc_presplit(cpstep_ctx* c, const double* psi, int nin_max) {
+// Bytes of the EES operand levels (k_presplit_ees_a and the S rows' levels):
+// FP16 two-level image of `rows` rows over K reals.
+size_t ees_lv_bytes(int rows, int K) {
   using namespace pctc;
-  const int S = c->nstates, K = 2 * c->npts;
-  if (!al16(psi) || nin_max < 1) return CPSTEP_ERR_ARG;
-  if (int rc = lv_reserve(c, pre_bytes(S, K) + pre_bytes(S, nin_max))) return rc;
-  return presplit(c, psi, K, S, K, c->d_wpt, 0, c->d_lv);
+  return (size_t)cdiv(rows, ROWS) * (size_t)pre_nsp(K) * STEP_H;
 }
 
-// EES sums of one atom type (MODE 2): C(s, ch jp + j) = sum_p wpt Re(conj psi_s
-// conj(dyp_ch) S_j), j < jp pairs; C column-major [nch jp][ldc], alpha = 1.
-// Takes psi's levels from ees_tc_presplit.
-int ees_tc_sums(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
-                int nch, int jp, double* C, int ldc) {
+// EES sums of one atom type as the product of two pre-split operands:
+// A = w psi dyp_c (rows c S + s, split here into alv, scale sig[c] =
+// pow2_scale(4 dmax[c]): |w psi| < 4 for states with psi^T psi = 2 I), B = the
+// type's S rows (rows j < jp, FP16 levels at blv, 1 / scale per row at cinv);
+// C(s, c jp + j) column-major [nch jp][S].
+int ees_tc_sums_pre(cpstep_ctx* c, const double* psi, const float2* dyp, int ld_d, int nch,
+                    const float* dmax, const uint8_t* blv, int jp, const float* cinv,
+                    uint8_t* alv, size_t alv_bytes, double* C) {
   using namespace pctc;
-  const int S = c->nstates, K = 2 * c->npts;
-  if (nch < 1 || nch > 4 || (ld_s & 3) || (ld_d & 1) || !al16(sv) || !al16(dyp) ||
-      c->lv_bytes < pre_bytes(S, K))
+  const int S = c->nstates, K = 2 * c->npts, nsp = pre_nsp(K);
+  const int M = nch * S;
+  if (nch < 1 || nch > 4 || jp < 1 || (ld_d & 1) || !al16(psi) || !al16(dyp) || !al16(blv) ||
+      !al16(alv) || alv_bytes < ees_lv_bytes(M, K))
     return CPSTEP_ERR_ARG;
-  const int jt = ROWS / nch;
-  const int tm = cdiv(S, ROWS), tn = cdiv(jp, jt);
+  PreA pa{};
+  pa.psi = psi;
+  pa.w = c->d_wpt;
+  pa.dyp = dyp;
+  pa.ld_d = ld_d;
+  pa.S = S;
+  pa.K = K;
+  pa.nch = nch;
+  pa.nsp = nsp;
+  for (int q = 0; q < 4; ++q) pa.sig[q] = q < nch ? tc::pow2_scale(4.f * dmax[q]) : 1.f;
+  pa.dst = alv;
+  pa.err = c->d_dev_err;
+  const long long warps = (long long)cdiv(S, ROWS) * nsp * 8;
+  k_presplit_ees_a<<<(unsigned)((warps + 7) / 8), 256, 0, c->stream>>>(pa);  // 8 warps per block
+  CPSTEP_LAUNCH_CHECK();
+  const int tm = cdiv(M, ROWS), tn = cdiv(jp, ROWS);
   const int want = std::max(1, c->tune.pc_split * c->num_sms / (tm * tn));
-  const int kslab = cdiv(cdiv(K, want), 128) * 128;
+  const int kslab = cdiv(cdiv(K, want), 512) * 512;  // whole fold groups per slab
   const int nsplit = cdiv(K, kslab);
-  const int N = nch * jp;
-  if (int rc = pc_part_reserve(c, (size_t)nsplit * S * N)) return rc;
-  Args p{};
-  p.lda = K;
-  p.M = S;
-  p.N = N;
-  p.K = K;
-  p.kslab = kslab;
-  p.part = c->d_pc_part;
-  p.err = c->d_dev_err;
-  p.sv = sv;
-  p.ld_s = ld_s;
-  p.dyp = dyp;
-  p.ld_d = ld_d;
-  p.nch = nch;
-  p.jt = jt;
-  p.jp = jp;
-  p.pre = c->d_lv;
-  p.pre_nsp = pre_nsp(K);
-  if (int rc = launch<2, 1, NST_PRE, KC_PRE>(c->stream, dim3(tm, tn, nsplit), p)) return rc;
-  return pc_splitk_reduce_launch(c, nsplit, S, N, 1.0, 0.0, C, ldc, 0);
+  if (int rc = pc_part_reserve(c, (size_t)nsplit * M * jp)) return rc;
+  PPArgs pp{};
+  pp.a = alv;
+  pp.b = blv;
+  pp.nsp = nsp;
+  pp.M = M;
+  pp.N = jp;
+  pp.K = K;
+  pp.kslab = kslab;
+  pp.S = S;
+  pp.jp = jp;
+  for (int q = 0; q < 4; ++q) pp.rinv[q] = 1.f / pa.sig[q];
+  pp.cinv = cinv;
+  pp.part = c->d_pc_part;
+  pp.err = c->d_dev_err;
+  static unsigned long long attr_done = 0;  // per-device attribute, one bit per device
+  int dev = 0;
+  CPSTEP_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(__atomic_load_n(&attr_done, __ATOMIC_ACQUIRE) & bit)) {
+    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(k_pp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         PP_BYTES));
+    __atomic_or_fetch(&attr_done, bit, __ATOMIC_RELEASE);
+  }
+  k_pp_tc<<<dim3(tm, tn, nsplit), PP_NTHR, PP_BYTES, c->stream>>>(pp);
+  CPSTEP_LAUNCH_CHECK();
+  return pc_splitk_reduce_launch(c, nsplit, S, nch * jp, 1.0, 0.0, C, S, 0);
 }
 
-// EES psi force of one atom type (MODE 3): fpsi_s(p) += alpha wpt(p) sum_j
-// Z(j, s) (conj(dyp_c) S_a)(p), j = c natm_t + a; Z column-major [S][ldz].
-// Z's levels go after psi's (room reserved by ees_tc_presplit).
-int ees_tc_force(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
-                 int nch, int natm_t, const double* Z, int ldz, double alpha, double* fpsi) {
+// EES psi force of one atom type from pre-split operands (k_pf_tc): Z
+// column-major [S][ldz] (inner index c natm_t + a), the type's FP32 Mn rows
+// sv[a ld_s + k]; F += alpha w (conj(dyp) S Z) as the in-CTA form below.
+// zlv and stlv hold the two operands' levels.
+int ees_tc_force_pre(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
+                     int nch, int natm_t, const double* Z, int ldz, double alpha, double* fpsi,
+                     const float* smax, const float* zmax, uint8_t* zlv, size_t zlv_bytes,
+                     uint8_t* stlv, size_t stlv_bytes) {
   using namespace pctc;
-  const int S = c->nstates, K = 2 * c->npts, nin = nch * natm_t;
-  if (nch < 1 || nch > 4 || (ld_s & 3) || (ld_d & 1) || (ldz & 1) || !al16(sv) || !al16(Z) ||
-      !al16(dyp) || c->lv_bytes < pre_bytes(S, K) + pre_bytes(S, nin))
+  const int S = c->nstates, npts = c->npts, kr = 2 * npts;
+  const int nks = cdiv(natm_t, 16), tm = cdiv(4 * S, ROWS), ntile = cdiv(kr, ROWS);
+  if (nch < 1 || nch > 4 || natm_t < 1 || (ld_s & 3) || (ld_d & 1) || !al16(fpsi) ||
+      !al16(zlv) || !al16(stlv) || zlv_bytes < (size_t)tm * nks * STEP_H ||
+      stlv_bytes < (size_t)ntile * nks * STEP_H || ldz < nch * natm_t)
     return CPSTEP_ERR_ARG;
-  uint8_t* zl = c->d_lv + pre_bytes(S, K);
-  if (int rc = presplit(c, Z, ldz, S, nin, nullptr, 0, zl)) return rc;
-  Args p{};
-  p.w = c->d_wpt;
-  p.M = K;
-  p.N = S;
-  p.K = K;
-  p.nin = nin;
-  p.out = fpsi;
-  p.ldo = K;
-  p.alpha = alpha;
-  p.beta = 1.0;
-  p.err = c->d_dev_err;
-  p.sv = sv;
-  p.ld_s = ld_s;
-  p.dyp = dyp;
-  p.ld_d = ld_d;
-  p.nch = nch;
-  p.natm_t = natm_t;
-  p.pre = zl;
-  p.pre_nsp = pre_nsp(nin);
-  return launch<3, 1, NST_PRE, KC_PRE>(c->stream, dim3(cdiv(K, ROWS), cdiv(S, ROWS)), p);
+  const long long nz = (long long)tm * ROWS * nks * 2, ns = (long long)ntile * ROWS * nks * 2;
+  k_presplit_z<<<(unsigned)((nz + 255) / 256), 256, 0, c->stream>>>(Z, ldz, S, nch, natm_t, nks,
+                                                                    tm * ROWS, zmax, zlv);
+  CPSTEP_LAUNCH_CHECK();
+  k_presplit_st<<<(unsigned)((ns + 255) / 256), 256, 0, c->stream>>>(sv, ld_s, kr, natm_t, nks,
+                                                                     ntile * ROWS, smax, stlv);
+  CPSTEP_LAUNCH_CHECK();
+  PFArgs pf{};
+  pf.a = zlv;
+  pf.b = stlv;
+  pf.nks = nks;
+  pf.ntile = ntile;
+  pf.S = S;
+  pf.nch = nch;
+  pf.npts = npts;
+  pf.zmax = zmax;
+  pf.smax = smax;
+  pf.dyp = dyp;
+  pf.ld_d = ld_d;
+  pf.w = c->d_wpt;
+  pf.alpha = alpha;
+  pf.f = fpsi;
+  pf.err = c->d_dev_err;
+  static unsigned long long attr_done = 0;  // per-device attribute, one bit per device
+  int dev = 0;
+  CPSTEP_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(__atomic_load_n(&attr_done, __ATOMIC_ACQUIRE) & bit)) {
+    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(k_pf_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         PF_BYTES));
+    __atomic_or_fetch(&attr_done, bit, __ATOMIC_RELEASE);
+  }
+  const int gx = std::max(1, std::min(ntile, c->num_sms / tm));
+  k_pf_tc<<<dim3(gx, tm), PP_NTHR, PF_BYTES, c->stream>>>(pf);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
+// Level bytes of the psi force's operands: Z (rows 4 S) and S^T (2 npts reals)
+size_t ees_pf_zbytes(int nstates, int natm_t) {
+  return (size_t)cdiv(4 * nstates, pctc::ROWS) * cdiv(natm_t, 16) * pctc::STEP_H;
+}
+size_t ees_pf_stbytes(int npts, int natm_t) {
+  return (size_t)cdiv(2 * npts, pctc::ROWS) * cdiv(natm_t, 16) * pctc::STEP_H;
 }
 
 // The tensor-core path takes 16-byte aligned operands with even leading

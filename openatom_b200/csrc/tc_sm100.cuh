@@ -5,6 +5,7 @@
 // and UMMA::InstrDescriptor name).
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <stdint.h>
 
 namespace tc {
@@ -35,6 +36,11 @@ __device__ __forceinline__ uint64_t smem_desc_kmajor(uint32_t saddr, uint32_t lb
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int m, int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
          ((uint32_t)(m >> 4) << 24);
+}
+
+// The same, FP16 A and B (format 0), FP32 D.
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int m, int n) {
+  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
 // D (+)= A B^T, issued by one thread (no output lanes disabled).
@@ -128,13 +134,21 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity, uint32
 // Bounded wait that also gives up as soon as *stop is set (another role of
 // the CTA reported an error): false on either.  Sleeps between tests.
 __device__ __forceinline__ bool mbar_wait_or(uint64_t* bar, uint32_t parity, const volatile int* stop,
-                                             uint64_t limit_ns = 1000000000ull) {
+                                             uint64_t limit_ns = 1000000000ull,
+                                             uint32_t hint_ns = 20000u) {
   const uint64_t t0 = globaltimer_ns();
   for (;;) {
-    if (mbar_test(bar, parity, 20000u)) return true;
+    if (mbar_test(bar, parity, hint_ns)) return true;
     if (*stop) return false;
     if (globaltimer_ns() - t0 > limit_ns) return false;
   }
+}
+// The same with short sleeps, for hand-overs on the critical path of a
+// pipeline (a long suspend hint can leave the waiter asleep after the phase
+// completed).
+__device__ __forceinline__ bool mbar_wait_fast(uint64_t* bar, uint32_t parity,
+                                               const volatile int* stop) {
+  return mbar_wait_or(bar, parity, stop, 1000000000ull, 200u);
 }
 
 // Arrival (release, CTA scope) of this thread.
@@ -282,6 +296,59 @@ __device__ __forceinline__ void split3_pair(float a, float b, uint32_t& h, uint3
   const float ra = a - bf16_lo(h), rb = b - bf16_hi(h);
   m = cvt_bf16x2(ra, rb);
   l = cvt_bf16x2(ra - bf16_lo(m), rb - bf16_hi(m));
+}
+
+// Two FP32 values rounded to nearest even FP16, packed: a in the low half.
+__device__ __forceinline__ uint32_t cvt_f16x2(float a, float b) {
+  uint32_t r;
+  asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+  return r;
+}
+__device__ __forceinline__ float f16_lo(uint32_t w) {
+  return __half2float(__ushort_as_half((unsigned short)(w & 0xFFFFu)));
+}
+__device__ __forceinline__ float f16_hi(uint32_t w) {
+  return __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+}
+
+// Two-level FP16 split of a pair of FP32 values already scaled by a power of
+// two into |x| < 2^15: x = h + m + r with h the nearest FP16 (11 significant
+// bits), m the nearest FP16 to the exact FP32 remainder x - h; |r| is at most
+// 2^-22 |x| (or an FP16 subnormal step, 2^-25, for the smallest values).
+__device__ __forceinline__ void split2h_pair(float a, float b, uint32_t& h, uint32_t& m) {
+  h = cvt_f16x2(a, b);
+  m = cvt_f16x2(a - f16_lo(h), b - f16_hi(h));
+}
+
+// The power of two that brings a largest magnitude `mx` to [2^13, 2^14)
+// (1 for mx = 0 or not finite): the FP16 levels then keep 22 bits of every
+// value within 2^-14 of the largest.
+__host__ __device__ __forceinline__ float pow2_scale(float mx) {
+  if (!(mx > 0.f) || !(mx < 3.0e38f)) return 1.f;
+  int e = 0;
+  frexpf(mx, &e);  // mx in [2^(e-1), 2^e)
+  return ldexpf(1.f, 14 - (e < -80 ? -80 : e));
+}
+
+// Core-matrix image of one K step (16 reals) of a 128-row operand tile,
+// K-major without swizzle: 8-row x 16-byte core matrices, the two 8-element K
+// halves 128 bytes apart, 8-row groups 256 bytes apart; one level is 4 KB
+// (CM_TILE) and the levels of a K step follow each other.  Byte offset of
+// (row r, k) in one level (k < 16).
+constexpr int CM_TILE = 128 * 16 * 2;
+__host__ __device__ __forceinline__ int core_off(int r, int k) {
+  return (r >> 3) * 256 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+// 8 FP32 values of one row (8 consecutive K) times a power of two `sc` -> two
+// FP16 levels, stored as 16 bytes at dst and at dst + CM_TILE
+__device__ __forceinline__ void split_store_h(uint8_t* dst, const float (&f)[8], float sc) {
+  uint32_t lv[2][4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) split2h_pair(f[2 * e] * sc, f[2 * e + 1] * sc, lv[0][e], lv[1][e]);
+#pragma unroll
+  for (int v = 0; v < 2; ++v)
+    *reinterpret_cast<uint4*>(dst + v * CM_TILE) = make_uint4(lv[v][0], lv[v][1], lv[v][2], lv[v][3]);
 }
 
 }  // namespace tc
