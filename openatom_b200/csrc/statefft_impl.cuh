@@ -27,6 +27,7 @@
 #include "ctx.cuh"
 #include "fft_shfl.cuh"
 #include "fft_p16.cuh"
+#include "fft_t20.cuh"
 
 namespace sfft {
 
@@ -1091,6 +1092,163 @@ __global__ void k_rho_reduce_items(const double* __restrict__ part, int n, int n
                                    int nblocks, int segs, double scale, double* __restrict__ rho);
 
 // ---------------------------------------------------------------------------
+// K3 for N = 200 in the two-stage 20 x 10 form (fft_t20.cuh), FP32: the same
+// item split and plane passes as k_xy_bwd_p16, 512 threads (16 warps of three
+// 10-thread line groups; lanes 30 and 31 work on a scratch line of their own
+// and store nothing), one block per SM.  The plane is [nplane_x][N + 3];
+// every line group (and every warp's idle pair) owns a scratch line of
+// N + N / 20 elements.
+constexpr int T20_K3_THREADS = 512;
+struct T20Shape {
+  static constexpr int N = 200, R = 10, LPW = 3, NW = T20_K3_THREADS / 32;
+  static constexpr int SLOTS = NW * LPW;        // working line groups
+  static constexpr int SCRL = NW * (LPW + 1);   // scratch lines (idle pairs included)
+  static constexpr int LDY = N + 3;
+  static constexpr int SL = T20Cfg::SCR + 2;    // scratch line stride
+  static constexpr size_t bytes(int nplx, int nlines) {
+    return sizeof(cplx<float>) *
+           ((size_t)N + (size_t)nplx * LDY + (size_t)SCRL * SL + (size_t)((nlines + 1) & ~1));
+  }
+};
+
+template <int NN>
+__global__ void __launch_bounds__(T20_K3_THREADS, 1)
+k_xy_bwd_t20(const cplx<float>* __restrict__ pen, const float* __restrict__ vks,
+             cplx<float>* __restrict__ pen_out, StateGeom g,
+             const cplx<float>* __restrict__ twx_g, const double* __restrict__ occ,
+             int nstates) {
+  static_assert(NN == 200, "the 20 x 10 two-stage form");
+  using S = T20Shape;
+  constexpr int N = S::N, LDY = S::LDY, SLOTS = S::SLOTS, R = S::R, LPW = S::LPW, P = 20;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<float>* tw = reinterpret_cast<cplx<float>*>(smem_raw);
+  cplx<float>* plane = tw + N;
+  const int nplx = g.nplane_x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = lane / R;                 // 0..2 working, 3 idle
+  const bool idle = grp >= LPW;
+  const int slot = warp * LPW + (idle ? 0 : grp);
+  const int wslot = warp * LPW;
+  cplx<float>* scr = plane + (size_t)nplx * LDY + (size_t)(warp * (LPW + 1) + grp) * S::SL;
+  cplx<float>* stage = plane + (size_t)nplx * LDY + (size_t)S::SCRL * S::SL;
+  const long long items = (long long)N * nstates;
+  const long long i0 = p16_item_start(items, blockIdx.x, gridDim.x);
+  const long long i1 = p16_item_start(items, blockIdx.x + 1, gridDim.x);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx_g[i];
+  if (i0 < i1)
+    p16_prefetch(pen + ((size_t)(i0 % nstates) * N + (size_t)(i0 / nstates)) * g.nlpad, stage,
+                 g.nlines);
+  __syncthreads();
+  T20Fft<float> F;
+  F.init(tw);
+  // partner lane of the R2C split (kx -> N - kx): thread (R - t) % R of the group
+  const int src = idle ? lane : grp * R + (R - F.t) % R;
+  for (long long it = i0; it < i1; ++it) {
+    const int z = (int)(it / nstates), s = (int)(it % nstates);
+    p16_scatter<N, LDY>(stage, plane, g);
+    if (it + 1 < i1)
+      p16_prefetch(pen + ((size_t)((it + 1) % nstates) * N + (size_t)((it + 1) / nstates)) *
+                             g.nlpad,
+                   stage, g.nlines);
+    // y pass, forward (FFTW_FORWARD y)
+    for (int c0 = 0; c0 < nplx; c0 += SLOTS) {
+      if (c0 + wslot >= nplx) break;  // warp-uniform
+      const int c = c0 + slot;
+      const bool act = !idle && c < nplx;
+      cplx<float>* col = plane + (size_t)(act ? c : 0) * LDY;
+      cplx<float> v[P];
+#pragma unroll
+      for (int k = 0; k < P; ++k) v[k] = act ? col[F.t + R * k] : mk<float>(0.f, 0.f);
+      F.template s2b<false>(v, scr);
+      if (act) {
+#pragma unroll
+        for (int q = 0; q < P; ++q) col[F.bpos(q)] = v[q];
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    const float* vplane = vks + (size_t)z * N * N;
+    const float w = (float)occ[s];
+    for (int p0 = 0; p0 < N / 2; p0 += SLOTS) {
+      if (p0 + wslot >= N / 2) break;  // warp-uniform
+      const int pp = p0 + slot;
+      const bool act = !idle && pp < N / 2;
+      const int ya = act ? 2 * pp : 0;
+      // C2R input of rows (ya, ya + 1): Z = conj(Xa) + i conj(Xb), Hermitian-
+      // extended to kx > N / 2
+      cplx<float> v[P];
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        const int x = F.t + R * k;
+        cplx<float> zv = mk<float>(0, 0);
+        if (act) {
+          if (x == 0) {
+            zv = mk<float>(plane[ya].x, plane[ya + 1].x);
+          } else if (x < nplx) {
+            const cplx<float> a = plane[x * LDY + ya], b = plane[x * LDY + ya + 1];
+            zv = mk<float>(a.x + b.y, b.x - a.y);
+          } else if (N - x < nplx) {
+            const int m = N - x;
+            const cplx<float> a = plane[m * LDY + ya], b = plane[m * LDY + ya + 1];
+            zv = mk<float>(a.x - b.y, a.y + b.x);
+          }
+        }
+        v[k] = zv;
+      }
+      F.template s2b<true>(v, scr);  // C2R, +i sign
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        const int x = F.bpos(q);
+        const float va = act ? __ldg(vplane + ya * N + x) : 0.f;
+        const float vb = act ? __ldg(vplane + (ya + 1) * N + x) : 0.f;
+        v[q].x *= va * w;
+        v[q].y *= vb * w;
+      }
+      F.template b2s<false>(v, scr);  // R2C, -i sign
+      // split the two real rows' spectra: partner N - kx in thread (R - t) % R,
+      // slot P - 1 - b (thread 0 keeps its own slot (P - b) % P); store kx < nplx
+#pragma unroll
+      for (int b = 0; b < P; ++b) {
+        cplx<float> zm;
+        zm.x = __shfl_sync(0xffffffffu, v[P - 1 - b].x, src);
+        zm.y = __shfl_sync(0xffffffffu, v[P - 1 - b].y, src);
+        if (F.t == 0) zm = v[(P - b) % P];
+        const int kx = F.t + R * b;
+        if (act && kx < nplx) {
+          const cplx<float> zk = v[b];
+          plane[kx * LDY + ya] = mk<float>(0.5f * (zk.x + zm.x), 0.5f * (zm.y - zk.y));
+          plane[kx * LDY + ya + 1] = mk<float>(0.5f * (zk.y + zm.y), 0.5f * (zk.x - zm.x));
+        }
+      }
+    }
+    __syncthreads();
+    // y pass, backward (FFTW_BACKWARD y)
+    for (int c0 = 0; c0 < nplx; c0 += SLOTS) {
+      if (c0 + wslot >= nplx) break;
+      const int c = c0 + slot;
+      const bool act = !idle && c < nplx;
+      cplx<float>* col = plane + (size_t)(act ? c : 0) * LDY;
+      cplx<float> v[P];
+#pragma unroll
+      for (int k = 0; k < P; ++k) v[k] = act ? col[F.t + R * k] : mk<float>(0.f, 0.f);
+      F.template s2b<true>(v, scr);
+      if (act) {
+#pragma unroll
+        for (int q = 0; q < P; ++q) col[F.bpos(q)] = v[q];
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    cplx<float>* po = pen_out + ((size_t)s * N + z) * g.nlpad;
+    for (int l = threadIdx.x; l < g.nlines; l += blockDim.x) {
+      const int xy = __ldg(g.line_xy + l);
+      po[l] = plane[(xy & 0xffff) * LDY + (xy >> 16)];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // K4: pencils -> backward z-FFT -> pack -> scale.
 //   MODE 0: F = scale * wpt * val (then, if occ != null, the kinetic term)
 //   MODE 1: plain pack with scale (adjoint transform)
@@ -1671,6 +1829,18 @@ struct StateFft {
         if (int rc = resident_blocks(c, k_xy_bwd_p16<N>, P16_K3_THREADS, smem, &c->p16_blocks_k3))
           return rc;
         k_xy_bwd_p16<N><<<c->p16_blocks_k3, P16_K3_THREADS, smem, c->stream>>>(
+            reinterpret_cast<const cplx<float>*>(j.pen_a), reinterpret_cast<const float*>(vt),
+            reinterpret_cast<cplx<float>*>(j.pen_b), j.g, tws<float>(c).x, occ, c->nstates);
+        shfl_done = true;
+      }
+    }
+    if constexpr (N == 200 && sizeof(T) == 4) {
+      const size_t smem = T20Shape::bytes(j.g.nplane_x, j.g.nlines);
+      if (c->tune.shfl == 2 && smem <= 227 * 1024) {  // else the Stockham form below
+        if (int rc = set_smem(k_xy_bwd_t20<N>, smem)) return rc;
+        if (int rc = resident_blocks(c, k_xy_bwd_t20<N>, T20_K3_THREADS, smem, &c->p16_blocks_k3))
+          return rc;
+        k_xy_bwd_t20<N><<<c->p16_blocks_k3, T20_K3_THREADS, smem, c->stream>>>(
             reinterpret_cast<const cplx<float>*>(j.pen_a), reinterpret_cast<const float*>(vt),
             reinterpret_cast<cplx<float>*>(j.pen_b), j.g, tws<float>(c).x, occ, c->nstates);
         shfl_done = true;

@@ -165,3 +165,39 @@ def test_plane_pass_forms_match_oracle(system, form):
         assert ctx.device_errors() == 0
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("form", [0, 2])
+def test_plane_pass_forms_n200(form):
+    """The 200^3 grid (the largest benchmark system's): V.psi in a mixed context
+    with the shared-memory Stockham form (0) and the two-stage 20 x 10 form of
+    fft_t20.cuh (2; the density pass runs form 0 there), against the oracle."""
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    import torch
+    from oracle import fftpath as OF
+    from oracle import layout as OL
+    from openatom_b200.context import StepContext
+    from openatom_b200.layout import StateLayout
+    from openatom_b200.system import make_psi
+    lay = StateLayout(12.0, 30.0, nfft=200)
+    olay = OL.Layout(12.0, 30.0, grid=200)
+    S = 6
+    psi = make_psi(lay, S, seed=5, device="cuda")
+    occ = torch.tensor([1.0, 1.0, 0.5, 1.0, 0.25, 1.0], dtype=torch.float64, device="cuda")
+    ctx = StepContext(lay, S, precision="mixed")
+    try:
+        ctx.tune_set({"plane_shfl": form})
+        pn, on = psi.cpu().numpy(), occ.cpu().numpy()
+        rho = ctx.density(psi, occ).cpu().numpy()
+        assert relerr(rho, OF.density(pn, olay, on, lay.vol)) < TOL["mixed"]
+        g = torch.Generator(device="cpu").manual_seed(9)
+        vks = torch.randn((200, 200, 200), generator=g, dtype=torch.float64)
+        force, eke = ctx.vks_psi(psi, vks.cuda(), occ, kinetic=True)
+        fv = OF.vpsi_force(pn, vks.numpy(), olay, on)
+        f_ref = OF.add_forces(fv, None, olay)
+        f_ref, e_ref = OF.eke(f_ref, pn, olay, on, lay.ecut_ry)
+        assert relerr(force.cpu().numpy(), f_ref) < TOL["mixed"]
+        assert ctx.device_errors() == 0
+    finally:
+        ctx.close()
