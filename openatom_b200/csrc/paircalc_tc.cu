@@ -1060,31 +1060,42 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pf_tc(const PFArgs p) {
       if (lane == 0) tc::mbar_arrive(&tfree[acc]);
       const int n = blockIdx.x + tl * gridDim.x;
       const int pt0 = (n * ROWS + 32 * (warp >> 2)) >> 1;  // 16 points
-      const bool wr = c == 0 && s < p.S;
+      // conj(dyp_c) Q_cs summed over the state's 4 channel lanes (shuffles);
+      // then lane c of the state adds points pt0 + c, + 4, + 8, + 12 into F
+      const bool wr = s < p.S;
       double2* fr = reinterpret_cast<double2*>(p.f + (size_t)(wr ? s : 0) * 2 * p.npts);
+      float2 d[16];
 #pragma unroll
-      for (int hf = 0; hf < 2; ++hf) {  // 8 points at a time, every load issued first
-        float2 d[8];
-        double2 fo[8];
+      for (int e = 0; e < 16; ++e) {
+        const int pt = pt0 + e;
+        d[e] = (live && pt < p.npts) ? p.dyp[(size_t)c * p.ld_d + pt] : make_float2(0.f, 0.f);
+      }
+      double2 fo[4];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int pt = pt0 + 8 * hf + e;
-          d[e] = (live && pt < p.npts) ? p.dyp[(size_t)c * p.ld_d + pt] : make_float2(0.f, 0.f);
-          fo[e] = (wr && pt < p.npts) ? fr[pt] : make_double2(0.0, 0.0);
+      for (int e4 = 0; e4 < 4; ++e4) {
+        const int pt = pt0 + 4 * e4 + c;
+        fo[e4] = (wr && pt < p.npts) ? fr[pt] : make_double2(0.0, 0.0);
+      }
+      float ox4[4], oy4[4];
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const float qx = v[2 * e], qy = v[2 * e + 1];
+        float ox = fmaf(d[e].x, qx, d[e].y * qy), oy = fmaf(d[e].x, qy, -d[e].y * qx);
+        ox += __shfl_xor_sync(0xffffffffu, ox, 1);
+        oy += __shfl_xor_sync(0xffffffffu, oy, 1);
+        ox += __shfl_xor_sync(0xffffffffu, ox, 2);
+        oy += __shfl_xor_sync(0xffffffffu, oy, 2);
+        if ((e & 3) == c) {  // compile-time e, runtime c: keep this lane's four
+          ox4[e >> 2] = ox;
+          oy4[e >> 2] = oy;
         }
+      }
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const float qx = v[16 * hf + 2 * e], qy = v[16 * hf + 2 * e + 1];
-          float ox = fmaf(d[e].x, qx, d[e].y * qy), oy = fmaf(d[e].x, qy, -d[e].y * qx);
-          ox += __shfl_xor_sync(0xffffffffu, ox, 1);  // conj(d) q summed over the
-          oy += __shfl_xor_sync(0xffffffffu, oy, 1);  // state's 4 channel lanes
-          ox += __shfl_xor_sync(0xffffffffu, ox, 2);
-          oy += __shfl_xor_sync(0xffffffffu, oy, 2);
-          const int pt = pt0 + 8 * hf + e;
-          if (wr && pt < p.npts) {
-            const double sc = p.alpha * p.w[pt] * rinv;
-            fr[pt] = make_double2(fma(sc, (double)ox, fo[e].x), fma(sc, (double)oy, fo[e].y));
-          }
+      for (int e4 = 0; e4 < 4; ++e4) {
+        const int pt = pt0 + 4 * e4 + c;
+        if (wr && pt < p.npts) {
+          const double sc = p.alpha * p.w[pt] * rinv;
+          fr[pt] = make_double2(fma(sc, (double)ox4[e4], fo[e4].x), fma(sc, (double)oy4[e4], fo[e4].y));
         }
       }
     }
