@@ -959,13 +959,33 @@ k_xy_bwd_p16(const cplx<float>* __restrict__ pen, const float* __restrict__ vks,
       const bool act = pp < N / 2;
       const int ya = act ? 2 * pp : 0;
       // V_KS of the two rows at this thread's block-layout positions, loaded
-      // (from L2) before the C2R so that the transform covers the latency
+      // (from L2) before the C2R so that the transform covers the latency.
+      // Slots m, m + R, ..., m + (H - 1) R (m < R) are the H consecutive
+      // positions H t + h + 16 m: one vector load of H floats (H = 2, 4, 8;
+      // 4 H t bytes from a row start: aligned).
       float va[16], vb[16];
+      constexpr int H = P16Cfg<N>::H;
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int x = F.bpos(q);
-        va[q] = __ldg(vplane + ya * N + x);
-        vb[q] = __ldg(vplane + (ya + 1) * N + x);
+      for (int m = 0; m < R; ++m) {
+        const int x0 = F.bpos(m);  // = H t + 16 m
+        const float* ra = vplane + ya * N + x0;
+        const float* rb = ra + N;
+        if constexpr (H == 2) {
+          const float2 a = __ldg(reinterpret_cast<const float2*>(ra));
+          const float2 b = __ldg(reinterpret_cast<const float2*>(rb));
+          va[m] = a.x; va[m + R] = a.y;
+          vb[m] = b.x; vb[m + R] = b.y;
+        } else {
+#pragma unroll
+          for (int h4 = 0; h4 < H; h4 += 4) {
+            const float4 a = __ldg(reinterpret_cast<const float4*>(ra + h4));
+            const float4 b = __ldg(reinterpret_cast<const float4*>(rb + h4));
+            va[m + (h4 + 0) * R] = a.x; va[m + (h4 + 1) * R] = a.y;
+            va[m + (h4 + 2) * R] = a.z; va[m + (h4 + 3) * R] = a.w;
+            vb[m + (h4 + 0) * R] = b.x; vb[m + (h4 + 1) * R] = b.y;
+            vb[m + (h4 + 2) * R] = b.z; vb[m + (h4 + 3) * R] = b.w;
+          }
+        }
       }
       cplx<float> v[16];
       p16_build_row<N>(plane, LDY, nplx, ya, F.t, v);
