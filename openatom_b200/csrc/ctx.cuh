@@ -503,6 +503,9 @@ int pc_overlap_tc_launch(cpstep_ctx* c, const double* a, const double* b, int M,
 int pc_backmul_tc_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
                          double* out, int ldo, int nout, int nin, int K, double alpha,
                          double beta, const double* w, bool* used);
+int pc_backmul_psiv_tc_launch(cpstep_ctx* c, const double* Tcm, int ldt, double* psi_no,
+                              double* psi, int K, int n, const int* flag, double* v, double rdt,
+                              bool* used);
 int dgemm_launch(cudaStream_t s, int ta, int tb, int m, int n, int k, double alpha,
                  const double* A, int lda, const double* B, int ldb, double beta, double* C,
                  int ldc);

@@ -642,6 +642,242 @@ int presplit(cpstep_ctx* c, const double* src, long long ldr, int rows, int K, c
 }
 
 // ---------------------------------------------------------------------------
+// Back-multiply with a short inner dimension (nin <= 128, one fold group):
+//   out[i][p] = alpha w(p) (sum_{j != i} M(j,i) in[j][p] + M(i,i) in[i][p]) + beta out[i][p]
+// the same products, levels and summation order as k_pc_tc's MODE 1, sized
+// for two CTAs per SM so that one CTA's epilogue (the output tile's stores)
+// overlaps the other's operand loads: 16-real chunks, 8 worker warps that
+// bring the FP64 rows in with cp.async (3 stages), split them into the BF16
+// levels and write the tile; warp 8 issues the MMAs and streams the
+// pre-split M^T in 3 stages.  TMEM holds the two FP32 accumulators only (256
+// columns): with one fold group the hi*hi sum and the small products meet in
+// FP64 in the epilogue, as the FP64 tile of k_pc_tc holds them after its
+// first fold.
+// The PsiV reset of the orthoT dynamics (CP_State_GSpacePlane.C:3707-3770,
+// order 0) can ride on the epilogue of psi = psi_no.T: when *psiv_flag is
+// set, v = (psi_new - psi_old) rdt and psi_no = psi_new.  The host passes it
+// only with one column tile (nout <= 128), where the CTA that writes a point
+// of psi_no is the only one that reads it.
+constexpr int BM_NW = 256;                          // worker threads (warps 0-7)
+constexpr int BM_MMA_WARP = BM_NW / 32;             // warp 8
+constexpr int BM_NTHR = BM_NW + 32;
+constexpr int BM_KC = 16;                           // reals (states) per chunk: one K step
+constexpr int BM_OPB = STEP_B;                      // one operand of one chunk: 12 KB
+constexpr int BM_NSTP = 3;                          // stages of the pre-split operand
+constexpr int BM_NST = 3;                           // FP64 stages [KC][RSP]
+constexpr int BM_RSP = ROWS + 2;
+constexpr int BM_RAW = BM_KC * BM_RSP * 8;
+constexpr int BM_BYTES = 1024 + 2 * BM_OPB + BM_NSTP * BM_OPB + BM_NST * BM_RAW;
+constexpr uint32_t BM_TMEM_COLS = 2 * ROWS;
+static_assert(2 * (BM_BYTES + 1024 + 128) <= 228 * 1024, "two CTAs per SM");
+static_assert(BM_RAW % 16 == 0 && ROWS * (BM_KC / 8) == BM_NW, "one unit per worker");
+
+struct BMArgs {
+  const double* in;   // in[j][p], row j at in + j ldi
+  const double* m;    // M column-major (column i at m + i ldm): the diagonal
+  const uint8_t* pre; // B(i, j) = M(j, i) without the diagonal, k_presplit image
+  const double* w;    // per complex point (a power of two), or none
+  int ldi, ldm, ldo, pre_nsp;
+  int np, nout, nin;  // points (reals), output rows, inner dimension (<= 128)
+  double* out;
+  double alpha, beta;
+  const int* psiv_flag;  // PsiV reset: when set, v and psi_no from the new tile
+  double* psiv_v;
+  double* psiv_no;
+  double rdt;
+  int* err;
+};
+
+// Two CTAs per SM: 18 warps over the 4 SM sub-partitions put 5 on one, whose
+// 16K registers then allow 102 per thread (the bound below).
+__global__ void __launch_bounds__(BM_NTHR, 2) k_bm_tc(const BMArgs p) {
+  extern __shared__ uint8_t dsm[];
+  __shared__ uint64_t full[2], done[2], pfull[BM_NSTP];
+  __shared__ uint32_t tslot;
+  __shared__ int stop_s, issued_s;
+  __shared__ double mdiag[ROWS];  // M(i, i) of the tile's columns
+  volatile int* stop = &stop_s;
+  const uint32_t s0 = tc::smem_u32(dsm);
+  uint8_t* base = dsm + (((s0 + 1023u) & ~1023u) - s0);
+  const uint32_t bf_s = tc::smem_u32(base);  // split A [2][level][4 KB]
+  uint8_t* pre_base = base + 2 * BM_OPB;     // M^T stages [NSTP][level][4 KB]
+  double* raw = reinterpret_cast<double*>(pre_base + BM_NSTP * BM_OPB);  // [NST][KC][RSP]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r0 = blockIdx.x * ROWS, c0 = blockIdx.y * ROWS;
+  const int nch = (p.nin + BM_KC - 1) / BM_KC;  // 1 .. 8
+
+  if (warp == 0) tc::tmem_alloc(&tslot, BM_TMEM_COLS);
+  if (tid == 0) {
+    for (int i = 0; i < 2; ++i) {
+      tc::mbar_init(&full[i], BM_NW / 32);
+      tc::mbar_init(&done[i], 1);
+    }
+    for (int i = 0; i < BM_NSTP; ++i) tc::mbar_init(&pfull[i], 1);
+    stop_s = 0;
+    issued_s = 0;
+    tc::fence_mbar_init();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = tslot;
+
+  if (warp == BM_MMA_WARP) {
+    if (lane == 0) {
+      int bad = 0, issued = 0, req = 0;
+      auto pre_load = [&](int c) {
+        const int st = c % BM_NSTP;
+        const uint8_t* src = p.pre + ((size_t)blockIdx.y * p.pre_nsp + (size_t)c) * STEP_B;
+        tc::mbar_expect_tx(&pfull[st], BM_OPB);
+        tc::bulk_g2s(pre_base + (size_t)st * BM_OPB, src, BM_OPB, &pfull[st]);
+      };
+      for (; req < nch && req < BM_NSTP; ++req) pre_load(req);
+      for (int ch = 0; ch < nch; ++ch) {
+        if (!tc::mbar_wait_or(&full[ch & 1], (ch >> 1) & 1, stop) ||
+            !tc::mbar_wait_or(&pfull[ch % BM_NSTP], (ch / BM_NSTP) & 1, stop)) {
+          bad = 1;
+          break;
+        }
+        tc::fence_after_sync();
+        const uint32_t a0 = bf_s + (uint32_t)((ch & 1) * BM_OPB);
+        const uint32_t b0 = bf_s + (uint32_t)((2 + ch % BM_NSTP) * BM_OPB);
+        // level pairs, smallest first; h h into its own accumulator
+        constexpr int LA[6] = {2, 0, 1, 1, 0, 0};
+        constexpr int LB[6] = {0, 2, 1, 0, 1, 0};
+#pragma unroll
+        for (int t = 0; t < 6; ++t) {
+          const bool zero = ch == 0 && (t == 0 || t == 5);
+          const uint64_t da = tc::smem_desc_kmajor(a0 + LA[t] * TILE_B, 128, 256);
+          const uint64_t db = tc::smem_desc_kmajor(b0 + LB[t] * TILE_B, 128, 256);
+          tc::mma_bf16(t == 5 ? tbase + ROWS : tbase, da, db, IDESC, zero ? 0u : 1u);
+        }
+        tc::commit(&done[ch & 1]);
+        issued = ch + 1;
+        if (ch >= 1 && req < nch) {  // chunk ch - 1's stage takes chunk req
+          if (!tc::mbar_wait_or(&done[(ch - 1) & 1], ((ch - 1) >> 1) & 1, stop)) {
+            bad = 1;
+            break;
+          }
+          pre_load(req++);
+        }
+      }
+      if (bad) {
+        *stop = 1;
+        for (int c = issued; c < req; ++c)  // requested copies land before the CTA exits
+          tc::mbar_wait(&pfull[c % BM_NSTP], (c / BM_NSTP) & 1);
+      }
+      issued_s = issued;
+    }
+    __syncwarp();
+  } else {
+    // ---------------- workers
+    // rows j = 16 ch .. of in (zero past nin), 128 points from r0 (zero past np)
+    auto load = [&](int ch, int st) {
+      double* ra = raw + (size_t)st * (BM_RAW / 8);
+#pragma unroll
+      for (int it = 0; it < BM_KC * (ROWS / 2) / BM_NW; ++it) {
+        const int q = tid + BM_NW * it;
+        const int jj = q / (ROWS / 2), pc = q % (ROWS / 2);
+        const int j = ch * BM_KC + jj, pt = r0 + 2 * pc;
+        const bool ok = j < p.nin && pt < p.np;  // np even: the pair is inside
+        const double* g = ok ? p.in + (size_t)j * p.ldi + pt : p.in;
+        tc::cp16(ra + jj * BM_RSP + 2 * pc, g, ok ? 16 : 0);
+      }
+    };
+    if (tid < ROWS) {
+      const int i = c0 + tid;
+      mdiag[tid] = (i < p.nout && i < p.nin) ? p.m[(size_t)i * p.ldm + i] : 0.0;
+    }
+    // unit tid: row (point) r = (tid & 7) + 8 (tid >> 4), states 8 u .. (u = (tid >> 3) & 1)
+    const int r = (tid & 7) + 8 * (tid >> 4), u = (tid >> 3) & 1;
+#pragma unroll
+    for (int ch = 0; ch < BM_NST - 1; ++ch) {
+      if (ch < nch) load(ch, ch);
+      tc::cp_commit();
+    }
+    int bad = 0;
+    for (int ch = 0; ch < nch; ++ch) {
+      tc::cp_wait<BM_NST - 2>();
+      // split buffer ch & 1 is free once the MMAs of chunk ch - 2 are done
+      const bool ok = ch < 2 || tc::mbar_wait_or(&done[ch & 1], ((ch - 2) >> 1) & 1, stop);
+      if (tc::bar_or(WBAR, BM_NW, bad || !ok)) {
+        bad = 1;
+        break;
+      }
+      const double* ra = raw + (size_t)(ch % BM_NST) * (BM_RAW / 8);
+      float f[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) f[e] = (float)ra[(8 * u + e) * BM_RSP + r];
+      split_store(base + (ch & 1) * BM_OPB + core_off(r, 8 * u), f);
+      tc::fence_async_shared();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&full[ch & 1]);
+      if (ch + BM_NST - 1 < nch) load(ch + BM_NST - 1, (ch + BM_NST - 1) % BM_NST);
+      tc::cp_commit();
+    }
+    if (!bad && !__all_sync(0xffffffffu,
+                            tc::mbar_wait_or(&done[(nch - 1) & 1], ((nch - 1) >> 1) & 1, stop)))
+      bad = 1;
+    if (tc::bar_or(WBAR, BM_NW, bad)) *stop = 1;
+    tc::cp_wait<0>();
+  }
+
+  tc::fence_before_sync();
+  __syncthreads();
+  const int failed = *stop;
+  if (!failed && warp != BM_MMA_WARP) {
+    tc::fence_after_sync();
+    // warp w: TMEM lanes 32 (w % 4).. (rows = points), columns 64 (w / 4)..
+    const uint32_t tlanes = (uint32_t)(32 * (warp & 3)) << 16;
+    const int rl = 32 * (warp & 3) + lane, cb = 64 * (warp >> 2);
+    const int pt = r0 + rl;
+    const bool prow = pt < p.np;
+    const double sc = prow ? p.alpha * (p.w ? p.w[pt >> 1] : 1.0) : 0.0;
+    const bool pv = p.psiv_flag && *p.psiv_flag;
+#pragma unroll 1
+    for (int pc = 0; pc < 8; ++pc) {
+      uint32_t sm[8], hh[8];
+      tc::tmem_ld8u(tbase + tlanes + (uint32_t)(cb + 8 * pc), sm);
+      tc::tmem_ld8u(tbase + tlanes + (uint32_t)(ROWS + cb + 8 * pc), hh);
+      // every load of the piece is issued before its first store
+      double ov[8], dg[8];
+#pragma unroll
+      for (int e8 = 0; e8 < 8; ++e8) {
+        const int i = c0 + cb + 8 * pc + e8;
+        const bool ok = prow && i < p.nout;
+        ov[e8] = (ok && (p.beta != 0.0 || pv)) ? p.out[(size_t)i * p.ldo + pt] : 0.0;
+        dg[e8] = (ok && i < p.nin) ? p.in[(size_t)i * p.ldi + pt] : 0.0;
+      }
+#pragma unroll
+      for (int e8 = 0; e8 < 8; ++e8) {
+        const int i = c0 + cb + 8 * pc + e8;
+        if (prow && i < p.nout) {
+          const double acc =
+              (double)__uint_as_float(hh[e8]) + (double)__uint_as_float(sm[e8]);
+          const double v = sc * fma(mdiag[cb + 8 * pc + e8], dg[e8], acc);
+          const double o = p.beta == 0.0 ? v : fma(p.beta, ov[e8], v);
+          p.out[(size_t)i * p.ldo + pt] = o;
+          if (pv) {
+            p.psiv_v[(size_t)i * p.ldo + pt] = (o - ov[e8]) * p.rdt;
+            p.psiv_no[(size_t)i * p.ldi + pt] = o;
+          }
+        }
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    if (failed && issued_s > 0)  // nothing may still write TMEM when it is released
+      tc::mbar_wait(&done[(issued_s - 1) & 1], ((issued_s - 1) >> 1) & 1);
+    __syncwarp();
+    tc::tmem_free(tbase, BM_TMEM_COLS);
+  }
+  if (failed && tid == 0) atomicOr(p.err, 1);
+}
+
+// ---------------------------------------------------------------------------
 // Products of two pre-split operands (FP16 levels of power-of-two scaled
 // values, the k_presplit image): the EES sums with A = w psi dyp_c (rows
 // c S + s) and B = the S rows of one atom type (rows v natm_t + a), both
@@ -1340,15 +1576,55 @@ int pc_overlap_tc_launch(cpstep_ctx* c, const double* a, const double* b, int M,
 
 // The back-multiply's matrix, B(i, j) = M(j, i) without its diagonal, is
 // split once into the level buffer (offset 0) and shared by all point tiles.
-int pc_backmul_tc_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
-                         double* out, int ldo, int nout, int nin, int K, double alpha,
-                         double beta, const double* w, bool* used) {
+static int backmul_tc(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
+                      double* out, int ldo, int nout, int nin, int K, double alpha, double beta,
+                      const double* w, const int* psiv_flag, double* psiv_v, double* psiv_no,
+                      double rdt, bool* used) {
   using namespace pctc;
   *used = false;
   if (!pc_tc_usable(c) || (K & 1) || (ldm & 1) || (ldi & 1) || !al16(Mcm) || !al16(in))
     return CPSTEP_OK;
+  if (psiv_flag && (nin > 128 || nout > ROWS)) return CPSTEP_OK;
   if (int rc = lv_reserve(c, pre_bytes(nout, nin))) return rc;
   if (int rc = presplit(c, Mcm, ldm, nout, nin, nullptr, 1, c->d_lv)) return rc;
+  if (nin <= 128) {  // one fold group: the two-CTAs-per-SM kernel
+    BMArgs b{};
+    b.in = in;
+    b.m = Mcm;
+    b.pre = c->d_lv;
+    b.w = w;
+    b.ldi = ldi;
+    b.ldm = ldm;
+    b.ldo = ldo;
+    b.pre_nsp = pre_nsp(nin);
+    b.np = K;
+    b.nout = nout;
+    b.nin = nin;
+    b.out = out;
+    b.alpha = alpha;
+    b.beta = beta;
+    b.psiv_flag = psiv_flag;
+    b.psiv_v = psiv_v;
+    b.psiv_no = psiv_no;
+    b.rdt = rdt;
+    b.err = c->d_dev_err;
+    static unsigned long long attr_done = 0;  // per-device attribute, one bit per device
+    int dev = 0;
+    CPSTEP_CUDA_TRY(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(__atomic_load_n(&attr_done, __ATOMIC_ACQUIRE) & bit)) {
+      CPSTEP_CUDA_TRY(
+          cudaFuncSetAttribute(k_bm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, BM_BYTES));
+      // the whole unified L1 as shared memory, so that two CTAs fit
+      CPSTEP_CUDA_TRY(cudaFuncSetAttribute(k_bm_tc, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                           cudaSharedmemCarveoutMaxShared));
+      __atomic_or_fetch(&attr_done, bit, __ATOMIC_RELEASE);
+    }
+    k_bm_tc<<<dim3(cdiv(K, ROWS), cdiv(nout, ROWS)), BM_NTHR, BM_BYTES, c->stream>>>(b);
+    CPSTEP_LAUNCH_CHECK();
+    *used = true;
+    return CPSTEP_OK;
+  }
   Args p{};
   p.A = in;
   p.lda = ldi;
@@ -1370,4 +1646,25 @@ int pc_backmul_tc_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double
     return rc;
   *used = true;
   return CPSTEP_OK;
+}
+
+int pc_backmul_tc_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* in, int ldi,
+                         double* out, int ldo, int nout, int nin, int K, double alpha,
+                         double beta, const double* w, bool* used) {
+  return backmul_tc(c, Mcm, ldm, in, ldi, out, ldo, nout, nin, K, alpha, beta, w, nullptr,
+                    nullptr, nullptr, 0.0, used);
+}
+
+// psi = psi_no.T with the PsiV reset in the epilogue (nin <= 128, nout <= 128,
+// tensor cores): when *flag, v = (psi_new - psi_old) rdt and psi_no = psi_new.
+// *used = false (nothing launched) where the caller must run the reset itself.
+int pc_backmul_psiv_tc_launch(cpstep_ctx* c, const double* Tcm, int ldt, double* psi_no,
+                              double* psi, int K, int n, const int* flag, double* v, double rdt,
+                              bool* used) {
+  if (psi_no == psi) {
+    *used = false;
+    return CPSTEP_OK;
+  }
+  return backmul_tc(c, Tcm, ldt, psi_no, K, psi, K, n, n, K, 1.0, 0.0, nullptr, flag, v,
+                    psi_no, rdt, used);
 }

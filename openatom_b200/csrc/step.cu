@@ -443,16 +443,23 @@ int step_run(cpstep_ctx* c, double* psi, double* vpsi, const double* occ, double
                          mixed ? 20 : 10, nullptr, nullptr, ortho_check)))
       return rc;
     const int nb = c->nblk_ke;
-    stp::k_psiv_save<<<nb, 256, 0, c->stream>>>(c->d_dyn_flags,
-                                                 reinterpret_cast<const double2*>(psi),
-                                                 reinterpret_cast<double2*>(c->d_force), ncoef);
-    CPSTEP_LAUNCH_CHECK();
-    if ((rc = pc_backmul_launch(c, c->d_tmat, S, c->d_psi_no, K, psi, K, S, S, K, 1.0, 0.0)))
+    bool fused = false;
+    if ((rc = pc_backmul_psiv_tc_launch(c, c->d_tmat, S, c->d_psi_no, psi, K, S, c->d_dyn_flags,
+                                        vpsi, 1.0 / dt, &fused)))
       return rc;
-    stp::k_psiv_apply<<<nb, 256, 0, c->stream>>>(
+    if (!fused) {
+      stp::k_psiv_save<<<nb, 256, 0, c->stream>>>(c->d_dyn_flags,
+                                                   reinterpret_cast<const double2*>(psi),
+                                                   reinterpret_cast<double2*>(c->d_force), ncoef);
+      CPSTEP_LAUNCH_CHECK();
+      if ((rc = pc_backmul_launch(c, c->d_tmat, S, c->d_psi_no, K, psi, K, S, S, K, 1.0, 0.0)))
+        return rc;
+    }
+    // the reset's v and psi_no (unless the back-multiply wrote them), T = I, the flags
+    stp::k_psiv_apply<<<fused ? cdiv(S * S, 256) : nb, 256, 0, c->stream>>>(
         c->d_dyn_flags, reinterpret_cast<const double2*>(psi),
         reinterpret_cast<const double2*>(c->d_force), reinterpret_cast<double2*>(c->d_psi_no),
-        reinterpret_cast<double2*>(vpsi), c->d_tmat, S, ncoef, 1.0 / dt);
+        reinterpret_cast<double2*>(vpsi), c->d_tmat, S, fused ? 0 : ncoef, 1.0 / dt);
     CPSTEP_LAUNCH_CHECK();
   }
   mark(7);

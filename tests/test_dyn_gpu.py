@@ -112,6 +112,11 @@ def test_mixed_dynamics_within_budget(dsys, regime):
             assert abs(e[8] - er["ETOT"]) / natm <= 1e-6, it
             assert np.max(np.abs(f.cpu().numpy() - fr)) <= 1e-5, it
             assert ctx.dyn_status()[1] == dyn["resets"], it
+            pno, _, half = ctx.dyn_state()
+            assert half == (0 if dyn["half_reset"] else 1), it
+            if dyn["half_reset"]:  # the reset's psi_no is this step's psi, bit for bit
+                assert torch.equal(pno, psi), it
+                assert np.max(np.abs(v.cpu().numpy() - vr)) <= 1e-4 * max(1.0, np.max(np.abs(vr)))
     finally:
         ctx.close()
 

@@ -70,7 +70,7 @@ def test_overlap_tensor_cores_vs_fp64(small, S):
         cm.close()
 
 
-@pytest.mark.parametrize("S,nout", [(128, 128), (300, 300), (128, 96)])
+@pytest.mark.parametrize("S,nout", [(128, 128), (300, 300), (128, 96), (40, 40), (72, 56)])
 def test_backmultiply_tensor_cores_vs_fp64(small, S, nout):
     import torch
     psi, f = _psi(small, S, seed=7 + S)
