@@ -481,6 +481,7 @@ int pc_backmul_launch(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
                       double* out, int ldo, int nout, int nin, int K, double alpha, double beta);
 void graph_drop(cpstep_ctx* c);
 int pc_part_reserve(cpstep_ctx* c, size_t elems);
+size_t pc_part_need(int nsplit, size_t mn);  // partials plus the reduction's group sums
 int split_reserve(cpstep_ctx* c, size_t bytes);
 int lv_reserve(cpstep_ctx* c, size_t bytes);
 int ees_tc_force_pre(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,

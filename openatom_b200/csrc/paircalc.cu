@@ -102,6 +102,21 @@ __global__ void k_splitk_reduce(const double* __restrict__ part, int nsplit, int
   *c = alpha * s + (beta == 0.0 ? 0.0 : beta * (*c));
 }
 
+// First pass of a long split-K reduction (many partial tiles): group g of
+// the nsplit partials summed in order, part2[g][e] (G groups).  The second
+// pass is k_splitk_reduce over the G group sums; both orders are fixed.
+__global__ void k_splitk_group(const double* __restrict__ part, int nsplit, int G, size_t mn,
+                               double* __restrict__ part2) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= mn) return;
+  const int g = blockIdx.y;
+  const int k0 = (int)((long long)nsplit * g / G), k1 = (int)((long long)nsplit * (g + 1) / G);
+  double s = 0.0;
+#pragma unroll 8
+  for (int k = k0; k < k1; ++k) s += part[(size_t)k * mn + e];
+  part2[(size_t)g * mn + e] = s;
+}
+
 // column-major C = alpha op(A) op(B) + beta C (reference DGEMM semantics)
 __global__ void __launch_bounds__(NT)
 k_dgemm(int ta, int tb, int m, int n, int k, double alpha, const double* __restrict__ A, int lda,
@@ -396,10 +411,34 @@ int split_reserve(cpstep_ctx* c, size_t bytes) {
   return CPSTEP_OK;
 }
 
+// Partials beyond 32 are first summed in 16 groups (k_splitk_group) into the
+// tail of the partial buffer: one thread per element over ~150 partials is
+// bound by the latency of its loads.
+static int splitk_groups(int nsplit) { return nsplit > 32 ? 16 : 0; }
+
+size_t pc_part_need(int nsplit, size_t mn) {
+  return (size_t)(nsplit + splitk_groups(nsplit)) * mn;
+}
+
 int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
                             double* C, int ldc, int sym) {
-  pcalc::k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, c->stream>>>(c->d_pc_part, nsplit, M, N,
-                                                                   alpha, beta, C, ldc, sym);
+  const size_t mn = (size_t)M * N;
+  const int G = splitk_groups(nsplit);
+  const double* part = c->d_pc_part;
+  if (G) {
+    if (c->pc_part_elems < pc_part_need(nsplit, mn)) {
+      cpstep_set_error("split-K reduction: partial buffer reserved without its group sums");
+      return CPSTEP_ERR_STATE;
+    }
+    double* part2 = c->d_pc_part + (size_t)nsplit * mn;
+    pcalc::k_splitk_group<<<dim3((unsigned)((mn + 255) / 256), G), 256, 0, c->stream>>>(
+        c->d_pc_part, nsplit, G, mn, part2);
+    CPSTEP_LAUNCH_CHECK();
+    part = part2;
+    nsplit = G;
+  }
+  pcalc::k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, c->stream>>>(part, nsplit, M, N, alpha,
+                                                                   beta, C, ldc, sym);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }
@@ -415,7 +454,7 @@ int pc_overlap_launch(cpstep_ctx* c, const double* a, const double* b, int M, in
   int want = std::max(1, c->tune.pc_split * c->num_sms / (tm * tn));
   int kslab = cdiv(cdiv(K, want), TK) * TK;
   int nsplit = cdiv(K, kslab);
-  if (int rc = pc_part_reserve(c, (size_t)nsplit * M * N)) return rc;
+  if (int rc = pc_part_reserve(c, pc_part_need(nsplit, (size_t)M * N))) return rc;
   k_overlap_t128<<<dim3(tm, tn, nsplit), 256, T128_SMEM, c->stream>>>(a, K, b, K, w, M, N, K,
                                                                      kslab, c->d_pc_part);
   CPSTEP_LAUNCH_CHECK();

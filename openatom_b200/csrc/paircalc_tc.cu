@@ -1439,7 +1439,7 @@ int ees_tc_sums_pre(cpstep_ctx* c, const double* psi, const float2* dyp, int ld_
   const int want = std::max(1, c->tune.pc_split * c->num_sms / (tm * tn));
   const int kslab = cdiv(cdiv(K, want), 512) * 512;  // whole fold groups per slab
   const int nsplit = cdiv(K, kslab);
-  if (int rc = pc_part_reserve(c, (size_t)nsplit * M * jp)) return rc;
+  if (int rc = pc_part_reserve(c, pc_part_need(nsplit, (size_t)M * jp))) return rc;
   PPArgs pp{};
   pp.a = alv;
   pp.b = blv;
@@ -1549,7 +1549,7 @@ int pc_overlap_tc_launch(cpstep_ctx* c, const double* a, const double* b, int M,
   const int want = std::max(1, c->tune.pc_split * c->num_sms / (tm * tn));
   const int kslab = cdiv(cdiv(K, want), 128) * 128;  // whole TMEM groups per slab
   const int nsplit = cdiv(K, kslab);
-  if (int rc = pc_part_reserve(c, (size_t)nsplit * M * N)) return rc;
+  if (int rc = pc_part_reserve(c, pc_part_need(nsplit, (size_t)M * N))) return rc;
   Args p{};
   p.A = a;
   p.B = b;
