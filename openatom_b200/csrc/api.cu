@@ -284,6 +284,7 @@ int cpstep_ctx_destroy(cpstep_ctx* c) {
   cudaFree(c->d_dev_err);
   cudaFree(c->d_split);
   cudaFree(c->d_lv);
+  cudaFree(c->d_hlv[0]); cudaFree(c->d_hlv[1]); cudaFree(c->d_pdiag);
   cudaFree(c->d_ion_e);
   cudaFree(c->d_force_atoms);
   graph_drop(c);

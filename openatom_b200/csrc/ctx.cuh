@@ -355,6 +355,12 @@ struct cpstep_ctx {
   size_t split_bytes = 0;
   uint8_t* d_lv = nullptr;  // BF16 levels of pre-split tensor-core operands (k_presplit)
   size_t lv_bytes = 0;
+  // BF16 level images of the two operands of a many-state overlap (k_presplit)
+  // and the FP64 row sums of its diagonal
+  uint8_t* d_hlv[2] = {nullptr, nullptr};
+  size_t hlv_bytes[2] = {0, 0};
+  double* d_pdiag = nullptr;
+  size_t pdiag_elems = 0;
   double* d_ortho_ws = nullptr;
   size_t ortho_ws_elems = 0;
   int* d_ortho_status = nullptr;  // [iterations, converged] of the last Ortho launch
@@ -495,7 +501,7 @@ int ees_tc_sums_pre(cpstep_ctx* c, const double* psi, const float2* dyp, int ld_
                     const float* dmax, const uint8_t* blv, int jp, const float* cinv,
                     uint8_t* alv, size_t alv_bytes, double* C);
 int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
-                            double* C, int ldc, int sym);
+                            double* C, int ldc, int sym, const double* diag = nullptr);
 // paircalc_tc.cu (tensor-core products; *used = false when the SIMT path must run)
 bool pc_tc_usable(const cpstep_ctx* c);
 int pc_overlap_tc_launch(cpstep_ctx* c, const double* a, const double* b, int M, int N, int K,

@@ -82,12 +82,14 @@ k_overlap_part(const double* __restrict__ A, int lda, const double* __restrict__
 // (i,j) and (j,i) so the result is exactly symmetric.
 __global__ void k_splitk_reduce(const double* __restrict__ part, int nsplit, int M, int N,
                                 double alpha, double beta, double* __restrict__ C, int ldc,
-                                int sym) {
+                                int sym, const double* __restrict__ diag) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= M * N) return;
   int j = e / M, i = e - j * M;
   double s = 0.0;
-  if (sym) {
+  if (diag && i == j) {  // the diagonal summed in FP64 elsewhere
+    s = diag[i];
+  } else if (sym) {
     const size_t e1 = (size_t)min(i, j) * M + max(i, j), e2 = (size_t)max(i, j) * M + min(i, j);
     double s1 = 0.0, s2 = 0.0;
     for (int k = 0; k < nsplit; ++k) {
@@ -421,7 +423,7 @@ size_t pc_part_need(int nsplit, size_t mn) {
 }
 
 int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
-                            double* C, int ldc, int sym) {
+                            double* C, int ldc, int sym, const double* diag) {
   const size_t mn = (size_t)M * N;
   const int G = splitk_groups(nsplit);
   const double* part = c->d_pc_part;
@@ -438,7 +440,7 @@ int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alph
     nsplit = G;
   }
   pcalc::k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, c->stream>>>(part, nsplit, M, N, alpha,
-                                                                   beta, C, ldc, sym);
+                                                                   beta, C, ldc, sym, diag);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }
@@ -605,7 +607,8 @@ extern "C" int cpstep_pc_overlap_noalloc(const double* d_a, const double* d_b, i
   // every partial the reduction reads is written by this call: nothing to clear
   k_overlap_part<<<dim3(tm, tn, nsplit), NT, 0, s>>>(d_a, K, d_b, K, d_w, M, N, K, kslab, part);
   CPSTEP_LAUNCH_CHECK();
-  k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, s>>>(part, nsplit, M, N, alpha, beta, d_c, ldc, 0);
+  k_splitk_reduce<<<cdiv(M * N, 256), 256, 0, s>>>(part, nsplit, M, N, alpha, beta, d_c, ldc, 0,
+                                                    nullptr);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }

@@ -169,6 +169,7 @@ struct PreArgs {
   const double* w;    // weight per complex point k / 2 (a power of two), or none
   int zero_diag;      // element (i, i) taken as zero
   uint8_t* dst;       // [row tile][step][level][4 KB]
+  uint8_t* dst2;      // the unweighted levels as well (the B operand of S), or none
 };
 
 // One warp = 16 rows x 16 reals of one K step and row tile: lane -> row
@@ -217,8 +218,14 @@ __global__ void __launch_bounds__(256) k_presplit(const PreArgs a) {
     }
   }
   float f[8];
+  const size_t off = ((size_t)rt * a.nsp + s) * STEP_B + core_off(rl, 8 * kh);
+  if (a.dst2) {
+    const float one[4] = {1.f, 1.f, 1.f, 1.f};
+    to_f32(x, one, f);
+    split_store(a.dst2 + off, f);
+  }
   to_f32(x, ws, f);
-  split_store(a.dst + ((size_t)rt * a.nsp + s) * STEP_B + core_off(rl, 8 * kh), f);
+  split_store(a.dst + off, f);
 }
 
 template <int MODE, int NLD, int NST, int KC>
@@ -634,7 +641,7 @@ inline size_t pre_bytes(int rows, int K) {
 int presplit(cpstep_ctx* c, const double* src, long long ldr, int rows, int K, const double* w,
              int zero_diag, uint8_t* dst) {
   if (!al16(src) || (ldr & 1) || rows < 1 || K < 1) return CPSTEP_ERR_ARG;
-  PreArgs a{src, ldr, rows, K, pre_nsp(K), w, zero_diag, dst};
+  PreArgs a{src, ldr, rows, K, pre_nsp(K), w, zero_diag, dst, nullptr};
   const long long threads = (long long)cdiv(rows, ROWS) * a.nsp * 8 * 32;
   k_presplit<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(a);
   CPSTEP_LAUNCH_CHECK();
@@ -880,49 +887,66 @@ __global__ void __launch_bounds__(BM_NTHR, 2) k_bm_tc(const BMArgs p) {
 // ---------------------------------------------------------------------------
 // Products of two pre-split operands (FP16 levels of power-of-two scaled
 // values, the k_presplit image): the EES sums with A = w psi dyp_c (rows
-// c S + s) and B = the S rows of one atom type (rows v natm_t + a), both
-// split once in global memory.  No operand work is left in the CTA; the roles
-// are warp-specialised:
+// c S + s) and B = the S rows of one atom type (rows v natm_t + a), and the
+// PairCalc overlaps of many states (S, lambda), both operands split once in
+// global memory.  No operand work is left in the CTA; the roles are
+// warp-specialised:
 //   warp 17 (lane 0)  streams each chunk's A and B levels with two bulk copies
 //                     into one of PP_NST stages, as soon as the stage is free;
 //   warp 16 (lane 0)  issues the 3 MMAs per K step (h m, m h, h h, all into one
 //                     FP32 accumulator) as soon as a stage has landed, never
-//                     waiting for MMAs to complete; the fold groups (512 reals)
-//                     alternate between two accumulators;
-//   warps 0-15        add each finished group's accumulator into the FP64 tile
-//                     and write the tile.
+//                     waiting for MMAs to complete; the fold groups (nf chunks)
+//                     rotate over four accumulators;
+//   warps 0-15        add each finished group's accumulator into the FP64 tile,
+//                     which they hold in registers (32 values per thread), and
+//                     write it.
 //   part[ks][(c jp + j) S + s] = rinv[c] cinv[j] sum_{k in slab ks} A[c S + s][k] B[j][k]
 // Handshakes (mbarriers, every wait bounded): full[st] (both copies of the
 // stage landed), empty[st] (the MMAs that read it completed), gfull[b] (a
 // group's MMAs into accumulator b completed), tfree[b] (accumulator b read
-// back).  TMEM: accumulators in columns 0-127 and 128-255, the FP64 tile in
-// 256-511.
+// back).  TMEM: accumulator b in columns 128 b .. 128 b + 127.
 constexpr int PP_KC = 32;                     // reals per chunk (2 K steps)
 constexpr int PP_KS = PP_KC / 16;
-constexpr int PP_OPB = PP_KS * STEP_H;        // one operand of one chunk: 16 KB
-constexpr int PP_STAGE = 2 * PP_OPB;          // A then B
-constexpr int PP_NST = 6;                     // stages
-constexpr int PP_NF = 512 / PP_KC;            // chunks per fold group
-constexpr int PP_BYTES = 1024 + PP_NST * PP_STAGE;
+constexpr int PP_NACC = 4;                    // TMEM accumulators
 constexpr int PP_MMA_WARP = NW / 32, PP_LOAD_WARP = NW / 32 + 1;
 constexpr int PP_NTHR = NW + 64;
+// NL levels per element: 2 (FP16, scaled; 3 level products) or 3 (BF16; 6)
+template <int NL>
+struct PPCfg {
+  static constexpr int STEP = NL * TILE_B;               // one K step, all levels
+  static constexpr int OPB = PP_KS * STEP;               // one operand of one chunk
+  static constexpr int STAGE = 2 * OPB;                  // A then B
+  static constexpr int NST = NL == 2 ? 6 : 4;            // stages
+  static constexpr int BYTES = 1024 + NST * STAGE;
+  static constexpr int NPROD = NL == 2 ? 3 : 6;
+  // TMEM: FP16 groups one accumulator each (4 in flight); BF16 groups two,
+  // the h h product apart from the five small ones (2 in flight)
+  static constexpr int NSLOT = NL == 2 ? 1 : 2;
+  static constexpr int NGRP = PP_NACC / NSLOT;
+};
 
 struct PPArgs {
   const uint8_t* a;  // [row tile][K step][level][4 KB], nsp K steps per row tile
   const uint8_t* b;
   int nsp;
   int M, N, K;       // rows of A (nch S), rows of B (jp), reals
-  int kslab;         // reals per split (a multiple of 512)
+  int kslab;         // reals per split (a multiple of nf PP_KC)
+  int nf;            // chunks per FP64 fold group
   int S, jp;         // states (rows of one channel block of A), B rows per channel block
   float rinv[4];     // 1 / scale of A's channel blocks
-  const float* cinv; // 1 / scale of each B row (device, N entries)
+  const float* cinv; // 1 / scale of B row j at cinv[j cstride] (device), or none (1)
+  int cstride;       // 1, or 0 for one scale of every row
   double* part;      // [nsplit][nch jp][S]
   int* err;
 };
 
+template <int NL>
 __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
+  using C = PPCfg<NL>;
+  constexpr int PP_NST = C::NST, PP_OPB = C::OPB, PP_STAGE = C::STAGE, STEP = C::STEP;
   extern __shared__ uint8_t dsm[];
-  __shared__ uint64_t full[PP_NST], empty[PP_NST], gfull[2], tfree[2];
+  constexpr int NGRP = C::NGRP, NSLOT = C::NSLOT;
+  __shared__ uint64_t full[PP_NST], empty[PP_NST], gfull[NGRP], tfree[NGRP];
   __shared__ uint32_t tslot;
   __shared__ int stop_s, issued_s, req_s;
   volatile int* stop = &stop_s;
@@ -933,7 +957,8 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
   const int r0 = blockIdx.x * ROWS, c0 = blockIdx.y * ROWS;
   const int kbeg = blockIdx.z * p.kslab, kend = min(p.K, kbeg + p.kslab);
   const int nch = kend > kbeg ? (kend - kbeg + PP_KC - 1) / PP_KC : 0;
-  const int ngroups = (nch + PP_NF - 1) / PP_NF;
+  const int nf = p.nf;
+  const int ngroups = (nch + nf - 1) / nf;
 
   if (warp == 0) tc::tmem_alloc(&tslot, TMEM_COLS);
   if (tid == 0) {
@@ -941,7 +966,7 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
       tc::mbar_init(&full[i], 1);
       tc::mbar_init(&empty[i], 1);
     }
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < NGRP; ++i) {
       tc::mbar_init(&gfull[i], 1);
       tc::mbar_init(&tfree[i], NW / 32);
     }
@@ -955,7 +980,7 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
   tc::fence_after_sync();
   const uint32_t tbase = tslot;
   const uint32_t tlanes = (uint32_t)(32 * (warp & 3)) << 16;
-  const uint32_t tf64 = tbase + tlanes + TMEM_F64 + (uint32_t)(64 * ((warp >> 2) & 3));
+  double acc64[32];  // workers: row 32 (warp % 4) + lane, columns 32 (warp / 4)..
 
   if (warp == PP_LOAD_WARP) {
     if (lane == 0) {
@@ -968,8 +993,8 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
           break;
         }
         const size_t kstep = (size_t)((kbeg + req * PP_KC) >> 4);
-        const uint8_t* ga = p.a + ((size_t)blockIdx.x * p.nsp + kstep) * STEP_H;
-        const uint8_t* gb = p.b + ((size_t)blockIdx.y * p.nsp + kstep) * STEP_H;
+        const uint8_t* ga = p.a + ((size_t)blockIdx.x * p.nsp + kstep) * STEP;
+        const uint8_t* gb = p.b + ((size_t)blockIdx.y * p.nsp + kstep) * STEP;
         uint8_t* sa = base + (size_t)st * PP_STAGE;
         tc::mbar_expect_tx(&full[st], PP_STAGE);
         tc::bulk_g2s(sa, ga, PP_OPB, &full[st]);
@@ -982,29 +1007,33 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
     if (lane == 0) {
       int issued = 0;
       for (int c = 0; c < nch; ++c) {
-        const int st = c % PP_NST, g = c / PP_NF, acc = g & 1;
-        const bool first = c % PP_NF == 0;
-        if (first && g >= 2) {  // accumulator acc was folded (group g - 2)
-          if (!tc::mbar_wait_fast(&tfree[acc], ((g - 2) >> 1) & 1, stop)) break;
+        const int st = c % PP_NST, g = c / nf, acc = g % NGRP;
+        const bool first = c % nf == 0;
+        if (first && g >= NGRP) {  // accumulator set acc was folded (group g - NGRP)
+          if (!tc::mbar_wait_fast(&tfree[acc], ((g - NGRP) / NGRP) & 1, stop)) break;
           tc::fence_after_sync();
         }
         if (!tc::mbar_wait_fast(&full[st], (c / PP_NST) & 1, stop)) break;
         tc::fence_after_sync();
         const uint32_t a0 = base_s + (uint32_t)(st * PP_STAGE), b0 = a0 + PP_OPB;
+        // level pairs, smallest first: FP16 (m, h), (h, m), (h, h); BF16 as k_pc_tc's six
+        constexpr int LA2[3] = {1, 0, 0}, LB2[3] = {0, 1, 0};
+        constexpr int LA3[6] = {2, 0, 1, 1, 0, 0}, LB3[6] = {0, 2, 1, 0, 1, 0};
 #pragma unroll
         for (int s = 0; s < PP_KS; ++s) {
 #pragma unroll
-          for (int t = 0; t < 3; ++t) {
-            // level pairs (m, h), (h, m), (h, h)
-            const int la = t == 0 ? 1 : 0, lb = t == 1 ? 1 : 0;
-            const uint64_t da = tc::smem_desc_kmajor(a0 + s * STEP_H + la * TILE_B, 128, 256);
-            const uint64_t db = tc::smem_desc_kmajor(b0 + s * STEP_H + lb * TILE_B, 128, 256);
-            const bool zero = first && s == 0 && t == 0;
-            tc::mma_bf16(tbase + (uint32_t)(acc * ROWS), da, db, IDESC_H, zero ? 0u : 1u);
+          for (int t = 0; t < C::NPROD; ++t) {
+            const int la = NL == 2 ? LA2[t % 3] : LA3[t], lb = NL == 2 ? LB2[t % 3] : LB3[t];
+            const uint64_t da = tc::smem_desc_kmajor(a0 + s * STEP + la * TILE_B, 128, 256);
+            const uint64_t db = tc::smem_desc_kmajor(b0 + s * STEP + lb * TILE_B, 128, 256);
+            const bool hh = NL == 3 && t == 5;  // BF16: h h into the set's second slot
+            const bool zero = first && s == 0 && (t == 0 || hh);
+            tc::mma_bf16(tbase + (uint32_t)((NSLOT * acc + (hh ? 1 : 0)) * ROWS), da, db,
+                         NL == 2 ? IDESC_H : IDESC, zero ? 0u : 1u);
           }
         }
         tc::commit(&empty[st]);
-        if (c % PP_NF == PP_NF - 1 || c == nch - 1) tc::commit(&gfull[acc]);
+        if (c % nf == nf - 1 || c == nch - 1) tc::commit(&gfull[acc]);
         issued = c + 1;
       }
       if (issued < nch) *stop = 1;
@@ -1012,38 +1041,39 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
     }
     __syncwarp();
   } else {
+#pragma unroll
+    for (int e = 0; e < 32; ++e) acc64[e] = 0.0;
     int bad = 0;
     for (int g = 0; g < ngroups && !bad; ++g) {
-      const int acc = g & 1;
-      if (!__all_sync(0xffffffffu, tc::mbar_wait_fast(&gfull[acc], (g >> 1) & 1, stop))) {
+      const int acc = g % NGRP;
+      if (!__all_sync(0xffffffffu, tc::mbar_wait_fast(&gfull[acc], (g / NGRP) & 1, stop))) {
         bad = 1;
         break;
       }
       tc::fence_after_sync();
-      float v[32];
-      tc::tmem_ld32(tbase + tlanes + (uint32_t)(acc * ROWS + 32 * (warp >> 2)), v);
+      const uint32_t ta = tbase + tlanes + (uint32_t)(NSLOT * acc * ROWS + 32 * (warp >> 2));
+      if (NSLOT == 1) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {  // 16 columns at a time
+          uint32_t v0[16];
+          tc::tmem_ld16(ta + 16 * h, v0);
+#pragma unroll
+          for (int e = 0; e < 16; ++e) acc64[16 * h + e] += (double)__uint_as_float(v0[e]);
+        }
+      } else {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {  // 8 columns of both slots at a time
+          uint32_t v0[8], v1[8];
+          tc::tmem_ld8u(ta + 8 * h, v0);
+          tc::tmem_ld8u(ta + ROWS + 8 * h, v1);
+#pragma unroll
+          for (int e = 0; e < 8; ++e)
+            acc64[8 * h + e] += (double)__uint_as_float(v1[e]) + (double)__uint_as_float(v0[e]);
+        }
+      }
       tc::fence_before_sync();
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&tfree[acc]);
-#pragma unroll
-      for (int h = 0; h < 4; ++h) {  // 8 columns (16 words) per TMEM round trip
-        uint32_t a[16];
-        if (g > 0) {
-          tc::tmem_ld16(tf64 + 16 * h, a);
-        } else {
-#pragma unroll
-          for (int e = 0; e < 16; ++e) a[e] = 0u;
-        }
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const double d =
-              __hiloint2double((int)a[2 * e + 1], (int)a[2 * e]) + (double)v[8 * h + e];
-          a[2 * e] = (uint32_t)__double2loint(d);
-          a[2 * e + 1] = (uint32_t)__double2hiint(d);
-        }
-        tc::tmem_st16(tf64 + 16 * h, a);
-      }
-      tc::tmem_wait_st();
     }
     if (tc::bar_or(WBAR, NW, bad)) *stop = 1;
   }
@@ -1052,25 +1082,17 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
   __syncthreads();
   const int failed = *stop;
   if (!failed && warp < PP_MMA_WARP && nch > 0) {
-    tc::fence_after_sync();
     const int rl = 32 * (warp & 3) + lane, cb = 32 * (warp >> 2);
     const int r = r0 + rl;
     const int ch = r < p.M ? r / p.S : 0, s = r - ch * p.S;
     const double ri =
         (double)(ch == 0 ? p.rinv[0] : ch == 1 ? p.rinv[1] : ch == 2 ? p.rinv[2] : p.rinv[3]);
-#pragma unroll 1
-    for (int pc = 0; pc < 4; ++pc) {
-      uint32_t a[16];
-      tc::tmem_ld16(tf64 + 16 * pc, a);
+    double* out = p.part + (size_t)blockIdx.z * p.M * p.N + (size_t)ch * p.jp * p.S + s;
 #pragma unroll
-      for (int e8 = 0; e8 < 8; ++e8) {
-        const int j = c0 + cb + 8 * pc + e8;
-        if (r < p.M && j < p.N) {
-          const double acc = __hiloint2double((int)a[2 * e8 + 1], (int)a[2 * e8]);
-          p.part[(size_t)blockIdx.z * p.M * p.N + ((size_t)ch * p.jp + j) * p.S + s] =
-              acc * ri * (double)p.cinv[j];
-        }
-      }
+    for (int e = 0; e < 32; ++e) {
+      const int j = c0 + cb + e;
+      if (r < p.M && j < p.N)
+        out[(size_t)j * p.S] = acc64[e] * ri * (p.cinv ? (double)p.cinv[j * p.cstride] : 1.0);
     }
   }
   tc::fence_before_sync();
@@ -1087,6 +1109,23 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
     tc::tmem_free(tbase, TMEM_COLS);
   }
   if (failed && tid == 0) atomicOr(p.err, 1);
+}
+
+// The diagonal of S = overlap(psi, psi) for the many-state overlap: the
+// FP64 row sums of w x^2, one block per row (fixed order).
+__global__ void __launch_bounds__(256) k_rowdot(const double* __restrict__ src, long long ldr,
+                                                int K, const double* __restrict__ w,
+                                                double* __restrict__ diag) {
+  __shared__ double red[32];
+  const double* x = src + (size_t)blockIdx.x * ldr;
+  double d = 0.0;
+  for (int k2 = threadIdx.x; 2 * k2 < K; k2 += blockDim.x) {  // point k2: reals 2 k2, 2 k2 + 1
+    const double2 v = *reinterpret_cast<const double2*>(x + 2 * k2);
+    const double ww = w ? w[k2] : 1.0;
+    d = fma(ww * v.x, v.x, fma(ww * v.y, v.y, d));
+  }
+  d = block_sum(d, red);
+  if (threadIdx.x == 0) diag[blockIdx.x] = d;
 }
 
 // A of the EES sums: rows c S + s (c < nch, s < S) = w psi_s dyp_c (complex,
@@ -1399,6 +1438,99 @@ __global__ void k_presplit_st(const float* __restrict__ sv, long long ld_s, int 
 
 }  // namespace pctc
 
+template <int NL>
+static int pp_launch(cpstep_ctx* c, dim3 grid, const pctc::PPArgs& pp) {
+  using namespace pctc;
+  constexpr int BYTES = PPCfg<NL>::BYTES;
+  static_assert(BYTES <= 227 * 1024, "shared memory");
+  static unsigned long long attr_done = 0;  // per-device attribute, one bit per device
+  int dev = 0;
+  CPSTEP_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(__atomic_load_n(&attr_done, __ATOMIC_ACQUIRE) & bit)) {
+    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(k_pp_tc<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         BYTES));
+    __atomic_or_fetch(&attr_done, bit, __ATOMIC_RELEASE);
+  }
+  k_pp_tc<NL><<<grid, PP_NTHR, BYTES, c->stream>>>(pp);
+  CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
+static int hlv_reserve(cpstep_ctx* c, int i, size_t bytes) {
+  if (bytes > c->hlv_bytes[i]) {
+    graph_drop(c);  // a captured step may hold the old buffer
+    cudaFree(c->d_hlv[i]);
+    c->d_hlv[i] = nullptr;
+    c->hlv_bytes[i] = 0;
+    CPSTEP_CUDA_TRY(cudaMalloc(&c->d_hlv[i], bytes));
+    c->hlv_bytes[i] = bytes;
+  }
+  return CPSTEP_OK;
+}
+
+// C = alpha overlap(a, b) + beta C for many states (M, N >= 256): both
+// operands split once in global memory into their three BF16 levels
+// (k_presplit; S's two images, w psi and psi, from one read of psi), the
+// product streamed by k_pp_tc<3> (six level products, FP64 folds every 128
+// reals), S's diagonal summed in FP64 (k_rowdot).  The in-CTA split of
+// k_pc_tc re-reads and re-splits each operand once per tile row or column of
+// the output.
+static int overlap_stream(cpstep_ctx* c, const double* a, const double* b, int M, int N, int K,
+                          const double* w, double alpha, double beta, double* C, int ldc) {
+  using namespace pctc;
+  const bool same = a == b && M == N;
+  const int nsp = pre_nsp(K);
+  if (int rc = hlv_reserve(c, 0, pre_bytes(M, K))) return rc;
+  if (int rc = hlv_reserve(c, 1, pre_bytes(N, K))) return rc;
+  if (same && (size_t)M > c->pdiag_elems) {
+    graph_drop(c);
+    cudaFree(c->d_pdiag);
+    c->d_pdiag = nullptr;
+    c->pdiag_elems = 0;
+    CPSTEP_CUDA_TRY(cudaMalloc(&c->d_pdiag, sizeof(double) * M));
+    c->pdiag_elems = M;
+  }
+  if (same) {
+    k_rowdot<<<M, 256, 0, c->stream>>>(a, K, K, w, c->d_pdiag);
+    CPSTEP_LAUNCH_CHECK();
+  }
+  PreArgs pa{a, K, M, K, nsp, w, 0, c->d_hlv[0], same ? c->d_hlv[1] : nullptr};
+  const long long ta = (long long)cdiv(M, ROWS) * nsp * 8 * 32;
+  k_presplit<<<(unsigned)((ta + 255) / 256), 256, 0, c->stream>>>(pa);
+  CPSTEP_LAUNCH_CHECK();
+  if (!same) {
+    PreArgs pb{b, K, N, K, nsp, nullptr, 0, c->d_hlv[1], nullptr};
+    const long long tb = (long long)cdiv(N, ROWS) * nsp * 8 * 32;
+    k_presplit<<<(unsigned)((tb + 255) / 256), 256, 0, c->stream>>>(pb);
+    CPSTEP_LAUNCH_CHECK();
+  }
+  const int tm = cdiv(M, ROWS), tn = cdiv(N, ROWS);
+  const int want = std::max(1, c->tune.pc_split * c->num_sms / (tm * tn));
+  const int kslab = cdiv(cdiv(K, want), 128) * 128;  // whole fold groups per slab
+  const int nsplit = cdiv(K, kslab);
+  if (int rc = pc_part_reserve(c, pc_part_need(nsplit, (size_t)M * N))) return rc;
+  PPArgs pp{};
+  pp.a = c->d_hlv[0];
+  pp.b = c->d_hlv[1];
+  pp.nsp = nsp;
+  pp.M = M;
+  pp.N = N;
+  pp.K = K;
+  pp.kslab = kslab;
+  pp.nf = 128 / PP_KC;
+  pp.S = M;
+  pp.jp = N;
+  for (int q = 0; q < 4; ++q) pp.rinv[q] = 1.f;
+  pp.cinv = nullptr;
+  pp.cstride = 0;
+  pp.part = c->d_pc_part;
+  pp.err = c->d_dev_err;
+  if (int rc = pp_launch<3>(c, dim3(tm, tn, nsplit), pp)) return rc;
+  return pc_splitk_reduce_launch(c, nsplit, M, N, alpha, beta, C, ldc, same ? 1 : 0,
+                                 same ? c->d_pdiag : nullptr);
+}
+
 // Bytes of the EES operand levels (k_presplit_ees_a and the S rows' levels):
 // FP16 two-level image of `rows` rows over K reals.
 size_t ees_lv_bytes(int rows, int K) {
@@ -1441,6 +1573,8 @@ int ees_tc_sums_pre(cpstep_ctx* c, const double* psi, const float2* dyp, int ld_
   const int nsplit = cdiv(K, kslab);
   if (int rc = pc_part_reserve(c, pc_part_need(nsplit, (size_t)M * jp))) return rc;
   PPArgs pp{};
+  pp.nf = 512 / PP_KC;
+  pp.cstride = 1;
   pp.a = alv;
   pp.b = blv;
   pp.nsp = nsp;
@@ -1454,17 +1588,7 @@ int ees_tc_sums_pre(cpstep_ctx* c, const double* psi, const float2* dyp, int ld_
   pp.cinv = cinv;
   pp.part = c->d_pc_part;
   pp.err = c->d_dev_err;
-  static unsigned long long attr_done = 0;  // per-device attribute, one bit per device
-  int dev = 0;
-  CPSTEP_CUDA_TRY(cudaGetDevice(&dev));
-  const unsigned long long bit = 1ull << (dev & 63);
-  if (!(__atomic_load_n(&attr_done, __ATOMIC_ACQUIRE) & bit)) {
-    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(k_pp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         PP_BYTES));
-    __atomic_or_fetch(&attr_done, bit, __ATOMIC_RELEASE);
-  }
-  k_pp_tc<<<dim3(tm, tn, nsplit), PP_NTHR, PP_BYTES, c->stream>>>(pp);
-  CPSTEP_LAUNCH_CHECK();
+  if (int rc = pp_launch<2>(c, dim3(tm, tn, nsplit), pp)) return rc;
   return pc_splitk_reduce_launch(c, nsplit, S, nch * jp, 1.0, 0.0, C, S, 0);
 }
 
@@ -1544,6 +1668,11 @@ int pc_overlap_tc_launch(cpstep_ctx* c, const double* a, const double* b, int M,
   *used = false;
   if (!pc_tc_usable(c) || (K & 1) || !al16(a) || !al16(b) || (w && w != c->d_wpt))
     return CPSTEP_OK;
+  if (M >= 2 * ROWS && N >= 2 * ROWS) {
+    if (int rc = overlap_stream(c, a, b, M, N, K, w, alpha, beta, C, ldc)) return rc;
+    *used = true;
+    return CPSTEP_OK;
+  }
   const bool one = a == b && M == N && M <= ROWS;
   const int tm = cdiv(M, ROWS), tn = cdiv(N, ROWS);
   const int want = std::max(1, c->tune.pc_split * c->num_sms / (tm * tn));

@@ -5,7 +5,10 @@ The mixed context sends cpstep_pc_overlap / cpstep_pc_backmultiply to the
 tcgen05 kernels: every FP64 element rounded to FP32 and split into three BF16
 levels, six level products accumulated in FP32 over 128-real groups, the
 groups, slabs and epilogue summed in FP64; the diagonal of S = psi^T psi and
-the diagonal of the back-multiplied matrix in FP64.  Tolerances (relative to
+the diagonal of the back-multiplied matrix in FP64.  Overlaps of 256 states
+or more split both operands once in global memory into their BF16 levels
+and stream them through the tensor cores (the six level products in one
+accumulator, FP64 folds every 128 reals; the diagonal of S still in FP64).  Tolerances (relative to
 the largest entry of the FP64 result): S 1e-7, lambda 1e-6, psi.T 2e-9
 (T near I: the error scales with T - diag T), psi.M 1e-6 for a random M.
 """
