@@ -918,6 +918,7 @@ struct PPCfg {
   static constexpr int STAGE = 2 * OPB;                  // A then B
   static constexpr int NST = NL == 2 ? 6 : 4;            // stages
   static constexpr int BYTES = 1024 + NST * STAGE;
+  static_assert(NST * STAGE >= (128 * 129 + 128) * 8, "back-multiply tile in the stages");
   static constexpr int NPROD = NL == 2 ? 3 : 6;
   // TMEM: FP16 groups one accumulator each (4 in flight); BF16 groups two,
   // the h h product apart from the five small ones (2 in flight)
@@ -938,9 +939,18 @@ struct PPArgs {
   int cstride;       // 1, or 0 for one scale of every row
   double* part;      // [nsplit][nch jp][S]
   int* err;
+  // back-multiply epilogue (BM): A = in^T (rows = points' reals), B = M^T
+  // without its diagonal, K = nin; out[i][p] = alpha w(p) (D[p][i] + M(i,i)
+  // in[i][p]) + beta out[i][p]
+  const double* in;
+  const double* m;
+  const double* w;
+  double* out;
+  int ldi, ldm, ldo;
+  double alpha, beta;
 };
 
-template <int NL>
+template <int NL, bool BM>
 __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
   using C = PPCfg<NL>;
   constexpr int PP_NST = C::NST, PP_OPB = C::OPB, PP_STAGE = C::STAGE, STEP = C::STEP;
@@ -1081,7 +1091,33 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
   tc::fence_before_sync();
   __syncthreads();
   const int failed = *stop;
-  if (!failed && warp < PP_MMA_WARP && nch > 0) {
+  if (BM && !failed && warp < PP_MMA_WARP && nch > 0) {
+    // rows = points, columns = output states: the FP64 tile through the (now
+    // idle) stage buffers, then written point-contiguous
+    double* tile = reinterpret_cast<double*>(base);  // [128][129]
+    double* mdg = tile + ROWS * (ROWS + 1);          // M(i, i) of the tile's columns
+    const int rl = 32 * (warp & 3) + lane, cb = 32 * (warp >> 2);
+#pragma unroll
+    for (int e = 0; e < 32; ++e) tile[rl * (ROWS + 1) + cb + e] = acc64[e];
+    if (tid < ROWS) {
+      const int i = c0 + tid;
+      mdg[tid] = (i < p.N && i < p.K) ? p.m[(size_t)i * p.ldm + i] : 0.0;
+    }
+    tc::bar_sync(WBAR, NW);
+#pragma unroll 4
+    for (int q = tid; q < ROWS * ROWS; q += NW) {
+      const int il = q / ROWS, pl = q % ROWS;
+      const int i = c0 + il, pt = r0 + pl;
+      if (i < p.N && pt < p.M) {
+        const double dg = i < p.K ? p.in[(size_t)i * p.ldi + pt] : 0.0;
+        const double ov = p.beta != 0.0 ? p.out[(size_t)i * p.ldo + pt] : 0.0;
+        const double sc = p.alpha * (p.w ? p.w[pt >> 1] : 1.0);
+        const double v = sc * fma(mdg[il], dg, tile[pl * (ROWS + 1) + il]);
+        p.out[(size_t)i * p.ldo + pt] = p.beta == 0.0 ? v : fma(p.beta, ov, v);
+      }
+    }
+  }
+  if (!BM && !failed && warp < PP_MMA_WARP && nch > 0) {
     const int rl = 32 * (warp & 3) + lane, cb = 32 * (warp >> 2);
     const int r = r0 + rl;
     const int ch = r < p.M ? r / p.S : 0, s = r - ch * p.S;
@@ -1126,6 +1162,37 @@ __global__ void __launch_bounds__(256) k_rowdot(const double* __restrict__ src, 
   }
   d = block_sum(d, red);
   if (threadIdx.x == 0) diag[blockIdx.x] = d;
+}
+
+// A of a many-state back-multiply: in^T (rows = the points' reals p, K =
+// states j) as three BF16 levels in the k_presplit image.  Mapping as
+// k_presplit; a lane reads its 8 states of one point, the warp's lanes
+// consecutive points (64-byte runs).
+__global__ void __launch_bounds__(256) k_presplit_t(const double* __restrict__ in, long long ldi,
+                                                    int np, int nin, int nsp,
+                                                    uint8_t* __restrict__ dst) {
+  const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = (long long)cdiv(np, ROWS) * nsp * 8;
+  if (wid >= nwarps) return;
+  const int gp = (int)(wid % 8);
+  const long long rest = wid / 8;
+  const int st = (int)(rest % nsp);
+  const long long rt = rest / nsp;
+  const int rl = (lane & 7) + 8 * (lane >> 4) + 16 * gp;
+  const int kh = (lane >> 3) & 1;
+  const long long pt = rt * ROWS + rl;
+  const int j0 = 16 * st + 8 * kh;
+  double x[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const int j = j0 + e;
+    x[e] = (pt < np && j < nin) ? in[(size_t)j * ldi + pt] : 0.0;
+  }
+  const float one[4] = {1.f, 1.f, 1.f, 1.f};
+  float f[8];
+  to_f32(x, one, f);
+  split_store(dst + ((size_t)rt * nsp + st) * STEP_B + core_off(rl, 8 * kh), f);
 }
 
 // A of the EES sums: rows c S + s (c < nch, s < S) = w psi_s dyp_c (complex,
@@ -1438,7 +1505,7 @@ __global__ void k_presplit_st(const float* __restrict__ sv, long long ld_s, int 
 
 }  // namespace pctc
 
-template <int NL>
+template <int NL, bool BM = false>
 static int pp_launch(cpstep_ctx* c, dim3 grid, const pctc::PPArgs& pp) {
   using namespace pctc;
   constexpr int BYTES = PPCfg<NL>::BYTES;
@@ -1448,11 +1515,11 @@ static int pp_launch(cpstep_ctx* c, dim3 grid, const pctc::PPArgs& pp) {
   CPSTEP_CUDA_TRY(cudaGetDevice(&dev));
   const unsigned long long bit = 1ull << (dev & 63);
   if (!(__atomic_load_n(&attr_done, __ATOMIC_ACQUIRE) & bit)) {
-    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(k_pp_tc<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CPSTEP_CUDA_TRY(cudaFuncSetAttribute(k_pp_tc<NL, BM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          BYTES));
     __atomic_or_fetch(&attr_done, bit, __ATOMIC_RELEASE);
   }
-  k_pp_tc<NL><<<grid, PP_NTHR, BYTES, c->stream>>>(pp);
+  k_pp_tc<NL, BM><<<grid, PP_NTHR, BYTES, c->stream>>>(pp);
   CPSTEP_LAUNCH_CHECK();
   return CPSTEP_OK;
 }
@@ -1716,6 +1783,36 @@ static int backmul_tc(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
   if (psiv_flag && (nin > 128 || nout > ROWS)) return CPSTEP_OK;
   if (int rc = lv_reserve(c, pre_bytes(nout, nin))) return rc;
   if (int rc = presplit(c, Mcm, ldm, nout, nin, nullptr, 1, c->d_lv)) return rc;
+  if (nin >= 2 * ROWS && !psiv_flag) {  // many states: both operands split once, streamed
+    const int nsp = pre_nsp(nin);
+    if (int rc = hlv_reserve(c, 0, pre_bytes(K, nin))) return rc;
+    const long long ta = (long long)cdiv(K, ROWS) * nsp * 8 * 32;
+    k_presplit_t<<<(unsigned)((ta + 255) / 256), 256, 0, c->stream>>>(in, ldi, K, nin, nsp,
+                                                                       c->d_hlv[0]);
+    CPSTEP_LAUNCH_CHECK();
+    PPArgs pp{};
+    pp.a = c->d_hlv[0];
+    pp.b = c->d_lv;
+    pp.nsp = nsp;
+    pp.M = K;
+    pp.N = nout;
+    pp.K = nin;
+    pp.kslab = cdiv(nin, 128) * 128;
+    pp.nf = 128 / PP_KC;
+    pp.err = c->d_dev_err;
+    pp.in = in;
+    pp.m = Mcm;
+    pp.w = w;
+    pp.out = out;
+    pp.ldi = ldi;
+    pp.ldm = ldm;
+    pp.ldo = ldo;
+    pp.alpha = alpha;
+    pp.beta = beta;
+    if (int rc = pp_launch<3, true>(c, dim3(cdiv(K, ROWS), cdiv(nout, ROWS), 1), pp)) return rc;
+    *used = true;
+    return CPSTEP_OK;
+  }
   if (nin <= 128) {  // one fold group: the two-CTAs-per-SM kernel
     BMArgs b{};
     b.in = in;
