@@ -896,18 +896,17 @@ __global__ void __launch_bounds__(BM_NTHR, 2) k_bm_tc(const BMArgs p) {
 //   warp 16 (lane 0)  issues the 3 MMAs per K step (h m, m h, h h, all into one
 //                     FP32 accumulator) as soon as a stage has landed, never
 //                     waiting for MMAs to complete; the fold groups (nf chunks)
-//                     rotate over four accumulators;
-//   warps 0-15        add each finished group's accumulator into the FP64 tile,
-//                     which they hold in registers (32 values per thread), and
-//                     write it.
+//                     alternate between two accumulator sets;
+//   warps 0-15        add each finished group's accumulator into the FP64 tile
+//                     (in TMEM for the FP16 images, in their registers, 32
+//                     values per thread, for the BF16 ones) and write it.
 //   part[ks][(c jp + j) S + s] = rinv[c] cinv[j] sum_{k in slab ks} A[c S + s][k] B[j][k]
 // Handshakes (mbarriers, every wait bounded): full[st] (both copies of the
 // stage landed), empty[st] (the MMAs that read it completed), gfull[b] (a
 // group's MMAs into accumulator b completed), tfree[b] (accumulator b read
-// back).  TMEM: accumulator b in columns 128 b .. 128 b + 127.
+// back).
 constexpr int PP_KC = 32;                     // reals per chunk (2 K steps)
 constexpr int PP_KS = PP_KC / 16;
-constexpr int PP_NACC = 4;                    // TMEM accumulators
 constexpr int PP_MMA_WARP = NW / 32, PP_LOAD_WARP = NW / 32 + 1;
 constexpr int PP_NTHR = NW + 64;
 // NL levels per element: 2 (FP16, scaled; 3 level products) or 3 (BF16; 6)
@@ -920,10 +919,12 @@ struct PPCfg {
   static constexpr int BYTES = 1024 + NST * STAGE;
   static_assert(NST * STAGE >= (128 * 129 + 128) * 8, "back-multiply tile in the stages");
   static constexpr int NPROD = NL == 2 ? 3 : 6;
-  // TMEM: FP16 groups one accumulator each (4 in flight); BF16 groups two,
-  // the h h product apart from the five small ones (2 in flight)
+  // TMEM, two fold groups in flight: FP16 one accumulator per group (columns
+  // 0-255) and the FP64 tile in columns 256-511; BF16 two per group, the h h
+  // product apart from the five small ones (all 512 columns), and the FP64
+  // tile in the fold warps' registers
   static constexpr int NSLOT = NL == 2 ? 1 : 2;
-  static constexpr int NGRP = PP_NACC / NSLOT;
+  static constexpr int NGRP = 2;
 };
 
 struct PPArgs {
@@ -931,8 +932,7 @@ struct PPArgs {
   const uint8_t* b;
   int nsp;
   int M, N, K;       // rows of A (nch S), rows of B (jp), reals
-  int kslab;         // reals per split (a multiple of nf PP_KC)
-  int nf;            // chunks per FP64 fold group
+  int kslab;         // reals per split (whole fold groups: 512 reals FP16, 128 BF16)
   int S, jp;         // states (rows of one channel block of A), B rows per channel block
   float rinv[4];     // 1 / scale of A's channel blocks
   const float* cinv; // 1 / scale of B row j at cinv[j cstride] (device), or none (1)
@@ -967,7 +967,7 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
   const int r0 = blockIdx.x * ROWS, c0 = blockIdx.y * ROWS;
   const int kbeg = blockIdx.z * p.kslab, kend = min(p.K, kbeg + p.kslab);
   const int nch = kend > kbeg ? (kend - kbeg + PP_KC - 1) / PP_KC : 0;
-  const int nf = p.nf;
+  constexpr int nf = NL == 2 ? 512 / PP_KC : 128 / PP_KC;  // chunks per fold group
   const int ngroups = (nch + nf - 1) / nf;
 
   if (warp == 0) tc::tmem_alloc(&tslot, TMEM_COLS);
@@ -990,7 +990,10 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
   tc::fence_after_sync();
   const uint32_t tbase = tslot;
   const uint32_t tlanes = (uint32_t)(32 * (warp & 3)) << 16;
-  double acc64[32];  // workers: row 32 (warp % 4) + lane, columns 32 (warp / 4)..
+  // FP16 images: the FP64 tile in TMEM columns 256-511; BF16: in the workers'
+  // registers (row 32 (warp % 4) + lane, columns 32 (warp / 4)..)
+  const uint32_t tf64 = tbase + tlanes + TMEM_F64 + (uint32_t)(64 * ((warp >> 2) & 3));
+  double acc64[NL == 2 ? 1 : 32];
 
   if (warp == PP_LOAD_WARP) {
     if (lane == 0) {
@@ -1052,7 +1055,7 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
     __syncwarp();
   } else {
 #pragma unroll
-    for (int e = 0; e < 32; ++e) acc64[e] = 0.0;
+    for (int e = 0; e < (NL == 2 ? 1 : 32); ++e) acc64[e] = 0.0;
     int bad = 0;
     for (int g = 0; g < ngroups && !bad; ++g) {
       const int acc = g % NGRP;
@@ -1062,14 +1065,34 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
       }
       tc::fence_after_sync();
       const uint32_t ta = tbase + tlanes + (uint32_t)(NSLOT * acc * ROWS + 32 * (warp >> 2));
-      if (NSLOT == 1) {
+      if constexpr (NL == 2) {
+        // the accumulator read back and released, then added into the FP64
+        // tile in TMEM columns 256-511, 8 columns (16 words) per round trip
+        float v[32];
+        tc::tmem_ld32(ta, v);
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&tfree[acc]);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {  // 16 columns at a time
-          uint32_t v0[16];
-          tc::tmem_ld16(ta + 16 * h, v0);
+        for (int h = 0; h < 4; ++h) {
+          uint32_t a[16];
+          if (g > 0) {
+            tc::tmem_ld16(tf64 + 16 * h, a);
+          } else {
 #pragma unroll
-          for (int e = 0; e < 16; ++e) acc64[16 * h + e] += (double)__uint_as_float(v0[e]);
+            for (int e = 0; e < 16; ++e) a[e] = 0u;
+          }
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const double d =
+                __hiloint2double((int)a[2 * e + 1], (int)a[2 * e]) + (double)v[8 * h + e];
+            a[2 * e] = (uint32_t)__double2loint(d);
+            a[2 * e + 1] = (uint32_t)__double2hiint(d);
+          }
+          tc::tmem_st16(tf64 + 16 * h, a);
         }
+        tc::tmem_wait_st();  // the next read of the FP64 tile sees these
+        continue;
       } else {
 #pragma unroll
         for (int h = 0; h < 4; ++h) {  // 8 columns of both slots at a time
@@ -1078,7 +1101,8 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
           tc::tmem_ld8u(ta + ROWS + 8 * h, v1);
 #pragma unroll
           for (int e = 0; e < 8; ++e)
-            acc64[8 * h + e] += (double)__uint_as_float(v1[e]) + (double)__uint_as_float(v0[e]);
+            acc64[(8 * h + e) % (NL == 2 ? 1 : 32)] +=
+                (double)__uint_as_float(v1[e]) + (double)__uint_as_float(v0[e]);
         }
       }
       tc::fence_before_sync();
@@ -1098,7 +1122,7 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
     double* mdg = tile + ROWS * (ROWS + 1);          // M(i, i) of the tile's columns
     const int rl = 32 * (warp & 3) + lane, cb = 32 * (warp >> 2);
 #pragma unroll
-    for (int e = 0; e < 32; ++e) tile[rl * (ROWS + 1) + cb + e] = acc64[e];
+    for (int e = 0; e < 32; ++e) tile[rl * (ROWS + 1) + cb + e] = acc64[e % (NL == 2 ? 1 : 32)];
     if (tid < ROWS) {
       const int i = c0 + tid;
       mdg[tid] = (i < p.N && i < p.K) ? p.m[(size_t)i * p.ldm + i] : 0.0;
@@ -1124,11 +1148,28 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
     const double ri =
         (double)(ch == 0 ? p.rinv[0] : ch == 1 ? p.rinv[1] : ch == 2 ? p.rinv[2] : p.rinv[3]);
     double* out = p.part + (size_t)blockIdx.z * p.M * p.N + (size_t)ch * p.jp * p.S + s;
+    if constexpr (NL == 2) {
+      tc::fence_after_sync();
+#pragma unroll 1
+      for (int pc = 0; pc < 4; ++pc) {
+        uint32_t a[16];
+        tc::tmem_ld16(tf64 + 16 * pc, a);
 #pragma unroll
-    for (int e = 0; e < 32; ++e) {
-      const int j = c0 + cb + e;
-      if (r < p.M && j < p.N)
-        out[(size_t)j * p.S] = acc64[e] * ri * (p.cinv ? (double)p.cinv[j * p.cstride] : 1.0);
+        for (int e8 = 0; e8 < 8; ++e8) {
+          const int j = c0 + cb + 8 * pc + e8;
+          if (r < p.M && j < p.N)
+            out[(size_t)j * p.S] = __hiloint2double((int)a[2 * e8 + 1], (int)a[2 * e8]) * ri *
+                                   (p.cinv ? (double)p.cinv[j * p.cstride] : 1.0);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 32; ++e) {
+        const int j = c0 + cb + e;
+        if (r < p.M && j < p.N)
+          out[(size_t)j * p.S] =
+              acc64[e % (NL == 2 ? 1 : 32)] * ri * (p.cinv ? (double)p.cinv[j * p.cstride] : 1.0);
+      }
     }
   }
   tc::fence_before_sync();
@@ -1585,7 +1626,6 @@ static int overlap_stream(cpstep_ctx* c, const double* a, const double* b, int M
   pp.N = N;
   pp.K = K;
   pp.kslab = kslab;
-  pp.nf = 128 / PP_KC;
   pp.S = M;
   pp.jp = N;
   for (int q = 0; q < 4; ++q) pp.rinv[q] = 1.f;
@@ -1640,7 +1680,6 @@ int ees_tc_sums_pre(cpstep_ctx* c, const double* psi, const float2* dyp, int ld_
   const int nsplit = cdiv(K, kslab);
   if (int rc = pc_part_reserve(c, pc_part_need(nsplit, (size_t)M * jp))) return rc;
   PPArgs pp{};
-  pp.nf = 512 / PP_KC;
   pp.cstride = 1;
   pp.a = alv;
   pp.b = blv;
@@ -1798,7 +1837,6 @@ static int backmul_tc(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
     pp.N = nout;
     pp.K = nin;
     pp.kslab = cdiv(nin, 128) * 128;
-    pp.nf = 128 / PP_KC;
     pp.err = c->d_dev_err;
     pp.in = in;
     pp.m = Mcm;
