@@ -1374,13 +1374,15 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pf_tc(const PFArgs p) {
   if (warp == PP_LOAD_WARP) {
     if (lane == 0) {
       int req = 0;
-      for (; req < nitem; ++req) {
+      // (tile, chunk) of item req counted along (no division by nkc in the loop)
+      for (int rt = 0, kc = 0; req < nitem; ++req, kc = kc + 1 == nkc ? 0 : kc + 1,
+               rt += kc == 0 ? 1 : 0) {
         const int st = req % PF_NST;
         if (req >= PF_NST && !tc::mbar_wait_fast(&empty[st], ((req - PF_NST) / PF_NST) & 1, stop)) {
           *stop = 1;
           break;
         }
-        const int n = blockIdx.x + (req / nkc) * gridDim.x, kc = req % nkc;
+        const int n = blockIdx.x + rt * gridDim.x;
         const int ks0 = kc * PF_KS, ksz = min(PF_KS, p.nks - ks0);
         const uint32_t bytes = (uint32_t)ksz * STEP_H;
         uint8_t* sa = base + (size_t)st * PF_STAGE;
@@ -1394,8 +1396,9 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pf_tc(const PFArgs p) {
   } else if (warp == PP_MMA_WARP) {
     if (lane == 0) {
       int issued = 0;
-      for (int it = 0; it < nitem; ++it) {
-        const int st = it % PF_NST, tl = it / nkc, kc = it % nkc, acc = tl & 1;
+      for (int it = 0, tl = 0, kc = 0; it < nitem;
+           ++it, kc = kc + 1 == nkc ? 0 : kc + 1, tl += kc == 0 ? 1 : 0) {
+        const int st = it % PF_NST, acc = tl & 1;
         if (kc == 0 && tl >= 2) {  // accumulator acc read back (tile tl - 2)
           if (!tc::mbar_wait_fast(&tfree[acc], ((tl - 2) >> 1) & 1, stop)) break;
           tc::fence_after_sync();
