@@ -497,9 +497,11 @@ int ees_tc_force_pre(cpstep_ctx* c, const float* sv, long long ld_s, const float
 size_t ees_pf_zbytes(int nstates, int natm_t);
 size_t ees_pf_stbytes(int npts, int natm_t);
 size_t ees_lv_bytes(int rows, int K);
-int ees_tc_sums_pre(cpstep_ctx* c, const double* psi, const float2* dyp, int ld_d, int nch,
-                    const float* dmax, const uint8_t* blv, int jp, const float* cinv,
-                    uint8_t* alv, size_t alv_bytes, double* C);
+int ees_tc_presplit_a(cpstep_ctx* c, const double* psi, int ntyp, const float2* const* dyp,
+                      int ld_d, const int* nch, const float* const* dmax, uint8_t* const* alv,
+                      size_t alv_bytes);
+int ees_tc_sums_pre(cpstep_ctx* c, int nch, const float* dmax, const uint8_t* blv, int jp,
+                    const float* cinv, const uint8_t* alv, double* C);
 int pc_splitk_reduce_launch(cpstep_ctx* c, int nsplit, int M, int N, double alpha, double beta,
                             double* C, int ldc, int sym, const double* diag = nullptr);
 // paircalc_tc.cu (tensor-core products; *used = false when the SIMT path must run)

@@ -793,8 +793,8 @@ int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, 
       CPSTEP_CUDA_TRY(cudaMemset(n.blv, 0, bl));
       CPSTEP_CUDA_TRY(cudaMalloc(&n.tsc, sizeof(float) * (size_t)std::max(1LL, ts)));
       CPSTEP_CUDA_TRY(cudaMalloc(&n.tinv, sizeof(float) * (size_t)std::max(1LL, ts)));
-      n.alv_bytes = ees_lv_bytes(nchmax * c->nstates, K);
-      CPSTEP_CUDA_TRY(cudaMalloc(&n.alv, n.alv_bytes));
+      n.alv_bytes = ees_lv_bytes(nchmax * c->nstates, K);  // per type; two types at a time
+      CPSTEP_CUDA_TRY(cudaMalloc(&n.alv, 2 * n.alv_bytes));
       int ntmax = 1;
       for (int t = 0; t < at.ntyp; ++t) ntmax = std::max(ntmax, at.tstart[t + 1] - at.tstart[t]);
       n.pf_zbytes = ees_pf_zbytes(c->nstates, ntmax);
@@ -858,14 +858,31 @@ static int ees_gspace_run(cpstep_ctx* c, const double* psi, const double* occ, d
   CPSTEP_LAUNCH_CHECK();
   CPSTEP_CUDA_TRY(cudaMemsetAsync(n.enl_s, 0, sizeof(double) * S, c->stream));
   CPSTEP_CUDA_TRY(cudaMemsetAsync(n.fnl, 0, sizeof(double) * S * natm * 3, c->stream));
-  for (int t = 0; t < ntyp; ++t) {
+  // the types with projectors, two at a time: A of both split from one read of psi
+  std::vector<int> tl;
+  for (int t = 0; t < ntyp; ++t)
+    if (!n.tch[t].empty() && c->atoms.tstart[t + 1] > c->atoms.tstart[t]) tl.push_back(t);
+  for (size_t q = 0; q < tl.size(); ++q) {
+    const int t = tl[q];
     const int nch = (int)n.tch[t].size();
     const int nt = c->atoms.tstart[t + 1] - c->atoms.tstart[t];
-    if (!nch || !nt) continue;
+    uint8_t* alv = n.alv + (q & 1) * n.alv_bytes;
+    if (q % 2 == 0) {
+      const int np2 = q + 1 < tl.size() ? 2 : 1;
+      const float2* dy[2];
+      const float* dm[2];
+      int nc[2];
+      uint8_t* al[2] = {n.alv, n.alv + n.alv_bytes};
+      for (int k = 0; k < np2; ++k) {
+        dy[k] = n.tdyp[tl[q + k]];
+        dm[k] = n.tdmax_c[tl[q + k]].data();
+        nc[k] = (int)n.tch[tl[q + k]].size();
+      }
+      if (int rc = ees_tc_presplit_a(c, psi, np2, dy, n.ld_d32, nc, dm, al, n.alv_bytes)) return rc;
+    }
     const float* sv = n.sv + n.sv_off[t];
-    if (int rc = ees_tc_sums_pre(c, psi, n.tdyp[t], n.ld_d32, nch, n.tdmax_c[t].data(),
-                                 n.blv + n.blv_off[t], 4 * nt, n.tinv + n.tsoff[t], n.alv,
-                                 n.alv_bytes, n.csum))
+    if (int rc = ees_tc_sums_pre(c, nch, n.tdmax_c[t].data(), n.blv + n.blv_off[t], 4 * nt,
+                                 n.tinv + n.tsoff[t], alv, n.csum))
       return rc;
     const int ldz = (nch * nt + 1) / 2 * 2;
     ees::k_ees_zglue<<<S, 128, 0, c->stream>>>(n.csum, S, nt, nch, n.d_tch + 4 * t, n.d_vn,

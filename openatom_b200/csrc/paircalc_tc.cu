@@ -663,8 +663,9 @@ int presplit(cpstep_ctx* c, const double* src, long long ldr, int rows, int K, c
 // The PsiV reset of the orthoT dynamics (CP_State_GSpacePlane.C:3707-3770,
 // order 0) can ride on the epilogue of psi = psi_no.T: when *psiv_flag is
 // set, v = (psi_new - psi_old) rdt and psi_no = psi_new.  The host passes it
-// only with one column tile (nout <= 128), where the CTA that writes a point
-// of psi_no is the only one that reads it.
+// here only with one column tile (nout <= 128), where the CTA that writes a
+// point of psi_no is the only one that reads it (many states: k_pp_tc's
+// back-multiply epilogue).
 constexpr int BM_NW = 256;                          // worker threads (warps 0-7)
 constexpr int BM_MMA_WARP = BM_NW / 32;             // warp 8
 constexpr int BM_NTHR = BM_NW + 32;
@@ -948,6 +949,13 @@ struct PPArgs {
   double* out;
   int ldi, ldm, ldo;
   double alpha, beta;
+  // the PsiV reset of psi = psi_no.T (as k_bm_tc): when *psiv_flag, v = (new -
+  // old) rdt and psi_no = new.  in is read in the kernel only at the points and
+  // states a CTA writes (the diagonal term), so any number of column tiles may
+  // write psi_no = in.
+  const int* psiv_flag;
+  double* psiv_v;
+  double rdt;
 };
 
 template <int NL, bool BM>
@@ -1128,16 +1136,22 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
       mdg[tid] = (i < p.N && i < p.K) ? p.m[(size_t)i * p.ldm + i] : 0.0;
     }
     tc::bar_sync(WBAR, NW);
+    const bool pv = p.psiv_flag && *p.psiv_flag;
 #pragma unroll 4
     for (int q = tid; q < ROWS * ROWS; q += NW) {
       const int il = q / ROWS, pl = q % ROWS;
       const int i = c0 + il, pt = r0 + pl;
       if (i < p.N && pt < p.M) {
         const double dg = i < p.K ? p.in[(size_t)i * p.ldi + pt] : 0.0;
-        const double ov = p.beta != 0.0 ? p.out[(size_t)i * p.ldo + pt] : 0.0;
+        const double ov = (p.beta != 0.0 || pv) ? p.out[(size_t)i * p.ldo + pt] : 0.0;
         const double sc = p.alpha * (p.w ? p.w[pt >> 1] : 1.0);
         const double v = sc * fma(mdg[il], dg, tile[pl * (ROWS + 1) + il]);
-        p.out[(size_t)i * p.ldo + pt] = p.beta == 0.0 ? v : fma(p.beta, ov, v);
+        const double o = p.beta == 0.0 ? v : fma(p.beta, ov, v);
+        p.out[(size_t)i * p.ldo + pt] = o;
+        if (pv) {
+          p.psiv_v[(size_t)i * p.ldo + pt] = (o - ov) * p.rdt;
+          const_cast<double*>(p.in)[(size_t)i * p.ldi + pt] = o;
+        }
       }
     }
   }
@@ -1236,18 +1250,21 @@ __global__ void __launch_bounds__(256) k_presplit_t(const double* __restrict__ i
   split_store(dst + ((size_t)rt * nsp + st) * STEP_B + core_off(rl, 8 * kh), f);
 }
 
-// A of the EES sums: rows c S + s (c < nch, s < S) = w psi_s dyp_c (complex,
-// real view), scaled by sig[c] (a power of two), two FP16 levels in the
-// k_presplit image; rows past nch S and reals past K are zero.  One warp =
-// 16 states x 16 reals of one K step for every channel: psi is read once.
+// A of the EES sums of up to two atom types: rows c S + s (c < nch[t], s < S)
+// = w psi_s dyp_{t,c} (complex, real view), scaled by sig[t][c] (a power of
+// two), two FP16 levels in the k_presplit image at dst[t]; rows past nch S
+// and reals past K are zero.  One warp = 16 states x 16 reals of one K step
+// for every channel of every type: psi is read once.
 struct PreA {
   const double* psi;  // [S][K] reals
   const double* w;    // per point (1 or 2)
-  const float2* dyp;  // channel c at dyp + c ld_d
+  int ntyp;           // 1 or 2
+  const float2* dyp[2];  // type t, channel c at dyp[t] + c ld_d
   int ld_d;
-  int S, K, nch, nsp;
-  float sig[4];
-  uint8_t* dst;
+  int S, K, nsp;
+  int nch[2];
+  float sig[2][4];
+  uint8_t* dst[2];
   int* err;
 };
 __global__ void __launch_bounds__(256) k_presplit_ees_a(const PreA a) {
@@ -1264,36 +1281,43 @@ __global__ void __launch_bounds__(256) k_presplit_ees_a(const PreA a) {
   const int kh = (lane >> 3) & 1;
   const int s = rt * ROWS + sl;
   const int k0 = 16 * st + 8 * kh;  // first real; 4 points from k0 / 2
-  double2 x[4];
-  float ws[4];
+  float xr[4], xi[4];
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
     const int pt = (k0 >> 1) + e;
     const bool ok = s < a.S && 2 * pt < a.K;
-    x[e] = ok ? *reinterpret_cast<const double2*>(a.psi + (size_t)s * a.K + 2 * pt)
-              : make_double2(0.0, 0.0);
-    ws[e] = ok ? (float)a.w[pt] : 0.f;
+    const double2 x = ok ? *reinterpret_cast<const double2*>(a.psi + (size_t)s * a.K + 2 * pt)
+                         : make_double2(0.0, 0.0);
+    const float ws = ok ? (float)a.w[pt] : 0.f;
+    xr[e] = (float)x.x * ws;
+    xi[e] = (float)x.y * ws;
   }
   bool big = false;
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    if (c >= a.nch) break;
-    float f[8];
+  for (int t = 0; t < 2; ++t) {
+    if (t >= a.ntyp) break;
+    const float2* dyp = t == 0 ? a.dyp[0] : a.dyp[1];
+    const int nch = t == 0 ? a.nch[0] : a.nch[1];
+    uint8_t* dst = t == 0 ? a.dst[0] : a.dst[1];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int pt = (k0 >> 1) + e;
-      const float2 d = 2 * pt < a.K ? a.dyp[(size_t)c * a.ld_d + pt] : make_float2(0.f, 0.f);
-      const float xr = (float)x[e].x * ws[e], xi = (float)x[e].y * ws[e];
-      f[2 * e] = fmaf(xr, d.x, -xi * d.y);
-      f[2 * e + 1] = fmaf(xr, d.y, xi * d.x);
-    }
-    const float sc = a.sig[c];
+    for (int c = 0; c < 4; ++c) {
+      if (c >= nch) break;
+      float f[8];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) big |= !(fabsf(f[e] * sc) < 32768.f);
-    if (s < a.S) {  // row c S + s of A; rows past nch S are never read into the output
-      const int r = c * a.S + s;
-      split_store_h(a.dst + ((size_t)(r / ROWS) * a.nsp + st) * STEP_H + core_off(r % ROWS, 8 * kh),
-                    f, sc);
+      for (int e = 0; e < 4; ++e) {
+        const int pt = (k0 >> 1) + e;
+        const float2 d = 2 * pt < a.K ? dyp[(size_t)c * a.ld_d + pt] : make_float2(0.f, 0.f);
+        f[2 * e] = fmaf(xr[e], d.x, -xi[e] * d.y);
+        f[2 * e + 1] = fmaf(xr[e], d.y, xi[e] * d.x);
+      }
+      const float sc = t == 0 ? a.sig[0][c] : a.sig[1][c];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) big |= !(fabsf(f[e] * sc) < 32768.f);
+      if (s < a.S) {  // row c S + s of A; rows past nch S are never read into the output
+        const int r = c * a.S + s;
+        split_store_h(dst + ((size_t)(r / ROWS) * a.nsp + st) * STEP_H + core_off(r % ROWS, 8 * kh),
+                      f, sc);
+      }
     }
   }
   if (big) atomicOr(a.err, 4);
@@ -1648,35 +1672,51 @@ size_t ees_lv_bytes(int rows, int K) {
   return (size_t)cdiv(rows, ROWS) * (size_t)pre_nsp(K) * STEP_H;
 }
 
-// EES sums of one atom type as the product of two pre-split operands:
-// A = w psi dyp_c (rows c S + s, split here into alv, scale sig[c] =
-// pow2_scale(4 dmax[c]): |w psi| < 4 for states with psi^T psi = 2 I), B = the
-// type's S rows (rows j < jp, FP16 levels at blv, 1 / scale per row at cinv);
-// C(s, c jp + j) column-major [nch jp][S].
-int ees_tc_sums_pre(cpstep_ctx* c, const double* psi, const float2* dyp, int ld_d, int nch,
-                    const float* dmax, const uint8_t* blv, int jp, const float* cinv,
-                    uint8_t* alv, size_t alv_bytes, double* C) {
+// FP16 scale of EES channel c: |w psi| < 4 for states with psi^T psi = 2 I
+static float ees_sig(const float* dmax, int c) { return tc::pow2_scale(4.f * dmax[c]); }
+
+// A of the EES sums of ntyp (1 or 2) atom types, split from one read of psi
+// into alv[t] (rows c S + s = w psi_s dyp_{t,c}, scale ees_sig(dmax[t], c)).
+int ees_tc_presplit_a(cpstep_ctx* c, const double* psi, int ntyp, const float2* const* dyp,
+                      int ld_d, const int* nch, const float* const* dmax, uint8_t* const* alv,
+                      size_t alv_bytes) {
   using namespace pctc;
   const int S = c->nstates, K = 2 * c->npts, nsp = pre_nsp(K);
-  const int M = nch * S;
-  if (nch < 1 || nch > 4 || jp < 1 || (ld_d & 1) || !al16(psi) || !al16(dyp) || !al16(blv) ||
-      !al16(alv) || alv_bytes < ees_lv_bytes(M, K))
-    return CPSTEP_ERR_ARG;
+  if (ntyp < 1 || ntyp > 2 || (ld_d & 1) || !al16(psi)) return CPSTEP_ERR_ARG;
   PreA pa{};
   pa.psi = psi;
   pa.w = c->d_wpt;
-  pa.dyp = dyp;
+  pa.ntyp = ntyp;
   pa.ld_d = ld_d;
   pa.S = S;
   pa.K = K;
-  pa.nch = nch;
   pa.nsp = nsp;
-  for (int q = 0; q < 4; ++q) pa.sig[q] = q < nch ? tc::pow2_scale(4.f * dmax[q]) : 1.f;
-  pa.dst = alv;
+  for (int t = 0; t < ntyp; ++t) {
+    if (nch[t] < 1 || nch[t] > 4 || !al16(dyp[t]) || !al16(alv[t]) ||
+        alv_bytes < ees_lv_bytes(nch[t] * S, K))
+      return CPSTEP_ERR_ARG;
+    pa.dyp[t] = dyp[t];
+    pa.nch[t] = nch[t];
+    pa.dst[t] = alv[t];
+    for (int q = 0; q < 4; ++q) pa.sig[t][q] = q < nch[t] ? ees_sig(dmax[t], q) : 1.f;
+  }
   pa.err = c->d_dev_err;
   const long long warps = (long long)cdiv(S, ROWS) * nsp * 8;
   k_presplit_ees_a<<<(unsigned)((warps + 7) / 8), 256, 0, c->stream>>>(pa);  // 8 warps per block
   CPSTEP_LAUNCH_CHECK();
+  return CPSTEP_OK;
+}
+
+// EES sums of one atom type as the product of two pre-split operands:
+// A = w psi dyp_c (rows c S + s, split by ees_tc_presplit_a into alv), B = the
+// type's S rows (rows j < jp, FP16 levels at blv, 1 / scale per row at cinv);
+// C(s, c jp + j) column-major [nch jp][S].
+int ees_tc_sums_pre(cpstep_ctx* c, int nch, const float* dmax, const uint8_t* blv, int jp,
+                    const float* cinv, const uint8_t* alv, double* C) {
+  using namespace pctc;
+  const int S = c->nstates, K = 2 * c->npts, nsp = pre_nsp(K);
+  const int M = nch * S;
+  if (nch < 1 || nch > 4 || jp < 1 || !al16(blv) || !al16(alv)) return CPSTEP_ERR_ARG;
   const int tm = cdiv(M, ROWS), tn = cdiv(jp, ROWS);
   const int want = std::max(1, c->tune.pc_split * c->num_sms / (tm * tn));
   const int kslab = cdiv(cdiv(K, want), 512) * 512;  // whole fold groups per slab
@@ -1693,7 +1733,7 @@ int ees_tc_sums_pre(cpstep_ctx* c, const double* psi, const float2* dyp, int ld_
   pp.kslab = kslab;
   pp.S = S;
   pp.jp = jp;
-  for (int q = 0; q < 4; ++q) pp.rinv[q] = 1.f / pa.sig[q];
+  for (int q = 0; q < 4; ++q) pp.rinv[q] = q < nch ? 1.f / ees_sig(dmax, q) : 1.f;
   pp.cinv = cinv;
   pp.part = c->d_pc_part;
   pp.err = c->d_dev_err;
@@ -1822,10 +1862,12 @@ static int backmul_tc(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
   *used = false;
   if (!pc_tc_usable(c) || (K & 1) || (ldm & 1) || (ldi & 1) || !al16(Mcm) || !al16(in))
     return CPSTEP_OK;
-  if (psiv_flag && (nin > 128 || nout > ROWS)) return CPSTEP_OK;
+  if (psiv_flag && psiv_no != in) return CPSTEP_ERR_ARG;  // psi_no is the input
+  // the PsiV reset rides on k_bm_tc with one column tile, or on the streaming form
+  if (psiv_flag && (nin <= 128 ? nout > ROWS : nin < 2 * ROWS)) return CPSTEP_OK;
   if (int rc = lv_reserve(c, pre_bytes(nout, nin))) return rc;
   if (int rc = presplit(c, Mcm, ldm, nout, nin, nullptr, 1, c->d_lv)) return rc;
-  if (nin >= 2 * ROWS && !psiv_flag) {  // many states: both operands split once, streamed
+  if (nin >= 2 * ROWS) {  // many states: both operands split once, streamed
     const int nsp = pre_nsp(nin);
     if (int rc = hlv_reserve(c, 0, pre_bytes(K, nin))) return rc;
     const long long ta = (long long)cdiv(K, ROWS) * nsp * 8 * 32;
@@ -1850,6 +1892,9 @@ static int backmul_tc(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
     pp.ldo = ldo;
     pp.alpha = alpha;
     pp.beta = beta;
+    pp.psiv_flag = psiv_flag;
+    pp.psiv_v = psiv_v;
+    pp.rdt = rdt;
     if (int rc = pp_launch<3, true>(c, dim3(cdiv(K, ROWS), cdiv(nout, ROWS), 1), pp)) return rc;
     *used = true;
     return CPSTEP_OK;
