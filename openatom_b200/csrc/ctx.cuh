@@ -233,7 +233,8 @@ struct NlData {
   int* d_tch = nullptr;             // [ntyp][4] channel indices (-1 unused)
   double* d_vn = nullptr;           // [nchan] vnorm / vol
   double* csum = nullptr;           // sums of one type [nch 4 natm_t][nstates]
-  double* zt = nullptr;             // scaled Z of one type [nstates][ldz]
+  double* zt = nullptr;             // scaled Z of two types, [nstates][ldz] each
+  size_t zt_slot = 0;               // doubles per type
   int gspace_ok = 0;                // every type has at most 4 channels
 };
 
@@ -490,10 +491,21 @@ int pc_part_reserve(cpstep_ctx* c, size_t elems);
 size_t pc_part_need(int nsplit, size_t mn);  // partials plus the reduction's group sums
 int split_reserve(cpstep_ctx* c, size_t bytes);
 int lv_reserve(cpstep_ctx* c, size_t bytes);
-int ees_tc_force_pre(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
-                     int nch, int natm_t, const double* Z, int ldz, double alpha, double* fpsi,
-                     const float* smax, const float* zmax, uint8_t* zlv, size_t zlv_bytes,
-                     uint8_t* stlv, size_t stlv_bytes);
+// one atom type's operands of the EES psi force (paircalc_tc.cu)
+struct EesForceType {
+  const float* sv;      // FP32 Mn rows sv[a ld_s + k]
+  long long ld_s;
+  const float2* dyp;    // channel c at dyp + c ld_d
+  int nch, natm_t;
+  const double* Z;      // [S][ldz], inner index c natm_t + a
+  int ldz;
+  const float* smax;    // largest |S| and |Z| (float bits)
+  const float* zmax;
+  uint8_t* zlv;         // level buffers of Z and S^T
+  uint8_t* stlv;
+};
+int ees_tc_force_pre(cpstep_ctx* c, int ntyp, const EesForceType* ty, int ld_d, double alpha,
+                     double* fpsi, size_t zlv_bytes, size_t stlv_bytes);
 size_t ees_pf_zbytes(int nstates, int natm_t);
 size_t ees_pf_stbytes(int npts, int natm_t);
 size_t ees_lv_bytes(int rows, int K);

@@ -744,7 +744,8 @@ int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, 
     CPSTEP_CUDA_TRY(cudaMemset(n.sv, 0, sizeof(float) * (size_t)std::max(tot, 4LL)));
     CPSTEP_CUDA_TRY(cudaMalloc(&n.sep, sizeof(double2) * na * 6 * (2 * (size_t)km + 1)));
     CPSTEP_CUDA_TRY(cudaMalloc(&n.csum, sizeof(double) * csz));
-    CPSTEP_CUDA_TRY(cudaMalloc(&n.zt, sizeof(double) * zsz));
+    n.zt_slot = zsz;  // two types at a time
+    CPSTEP_CUDA_TRY(cudaMalloc(&n.zt, sizeof(double) * 2 * zsz));
     n.tdyp.assign(at.ntyp, nullptr);
     n.tdmax.assign(at.ntyp, 0.f);
     n.tdmax_c.assign(at.ntyp, std::vector<float>(4, 0.f));
@@ -799,8 +800,8 @@ int nl_set(cpstep_ctx* c, int nkf, int n_interp, int nchan, const int* ch_type, 
       for (int t = 0; t < at.ntyp; ++t) ntmax = std::max(ntmax, at.tstart[t + 1] - at.tstart[t]);
       n.pf_zbytes = ees_pf_zbytes(c->nstates, ntmax);
       n.pf_stbytes = ees_pf_stbytes(c->npts, ntmax);
-      CPSTEP_CUDA_TRY(cudaMalloc(&n.pf_z, n.pf_zbytes));
-      CPSTEP_CUDA_TRY(cudaMalloc(&n.pf_st, n.pf_stbytes));
+      CPSTEP_CUDA_TRY(cudaMalloc(&n.pf_z, 2 * n.pf_zbytes));  // two types at a time
+      CPSTEP_CUDA_TRY(cudaMalloc(&n.pf_st, 2 * n.pf_stbytes));
     }
     CPSTEP_CUDA_TRY(cudaMalloc(&n.d_tch, sizeof(int) * htch.size()));
     CPSTEP_CUDA_TRY(cudaMemcpy(n.d_tch, htch.data(), sizeof(int) * htch.size(),
@@ -860,6 +861,7 @@ static int ees_gspace_run(cpstep_ctx* c, const double* psi, const double* occ, d
   CPSTEP_CUDA_TRY(cudaMemsetAsync(n.fnl, 0, sizeof(double) * S * natm * 3, c->stream));
   // the types with projectors, two at a time: A of both split from one read of psi
   std::vector<int> tl;
+  EesForceType ft[2];
   for (int t = 0; t < ntyp; ++t)
     if (!n.tch[t].empty() && c->atoms.tstart[t + 1] > c->atoms.tstart[t]) tl.push_back(t);
   for (size_t q = 0; q < tl.size(); ++q) {
@@ -880,19 +882,23 @@ static int ees_gspace_run(cpstep_ctx* c, const double* psi, const double* occ, d
       }
       if (int rc = ees_tc_presplit_a(c, psi, np2, dy, n.ld_d32, nc, dm, al, n.alv_bytes)) return rc;
     }
-    const float* sv = n.sv + n.sv_off[t];
     if (int rc = ees_tc_sums_pre(c, nch, n.tdmax_c[t].data(), n.blv + n.blv_off[t], 4 * nt,
                                  n.tinv + n.tsoff[t], alv, n.csum))
       return rc;
     const int ldz = (nch * nt + 1) / 2 * 2;
+    double* zt = n.zt + (q & 1) * n.zt_slot;
     ees::k_ees_zglue<<<S, 128, 0, c->stream>>>(n.csum, S, nt, nch, n.d_tch + 4 * t, n.d_vn,
-                                                n.d_order, c->atoms.tstart[t], natm, occ, n.zt,
-                                                ldz, n.enl_s, n.fnl, zmax_u + t);
+                                                n.d_order, c->atoms.tstart[t], natm, occ, zt, ldz,
+                                                n.enl_s, n.fnl, zmax_u + t);
     CPSTEP_LAUNCH_CHECK();
-    if (int rc = ees_tc_force_pre(c, sv, n.ld_s, n.tdyp[t], n.ld_d32, nch, nt, n.zt, ldz, -1.0,
-                                  fpsi, n.d_hmax + t, n.d_hmax + ntyp + t, n.pf_z, n.pf_zbytes,
-                                  n.pf_st, n.pf_stbytes))
-      return rc;
+    ft[q & 1] = EesForceType{n.sv + n.sv_off[t], n.ld_s, n.tdyp[t], nch, nt, zt, ldz,
+                             n.d_hmax + t, n.d_hmax + ntyp + t, n.pf_z + (q & 1) * n.pf_zbytes,
+                             n.pf_st + (q & 1) * n.pf_stbytes};
+    // the psi force of the pair (F read and written once for both types)
+    if (q % 2 == 1 || q + 1 == tl.size())
+      if (int rc = ees_tc_force_pre(c, (int)(q % 2) + 1, ft, n.ld_d32, -1.0, fpsi, n.pf_zbytes,
+                                    n.pf_stbytes))
+        return rc;
   }
   ees::k_nl_finish<<<cdiv(std::max(1, 3 * natm), 128), 128, 0, c->stream>>>(
       n.enl_s, n.fnl, S, natm, energies, fatm);

@@ -1324,37 +1324,40 @@ __global__ void __launch_bounds__(256) k_presplit_ees_a(const PreA a) {
 }
 
 // ---------------------------------------------------------------------------
-// psi force of one atom type from pre-split operands:
-//   F_s(p) += alpha w(p) sum_c conj(dyp_c(p)) Q_cs(p),  Q_cs(p) = sum_a Z(c natm_t + a, s) S_a(p)
-// as D = A B^T with A = Z (rows 4 s + c, K = the type's atoms) and B = the
-// real views of the S (Mn) rows transposed (rows = reals of the points, K =
-// atoms), both FP16 levels (k_presplit_z, k_presplit_st).  One output tile =
-// 32 states x 4 channel rows x 128 reals (64 points); the CTAs of one row
-// tile walk the point tiles (persistent), the K chunks of a tile streamed like
-// k_pp_tc's (warp 17 copies, warp 16 issues into one of two accumulators),
-// and warps 0-15 finish each tile: the 4 channel rows of a state are combined
-// by lane shuffles and added into F.
+// psi force of up to two atom types from pre-split operands:
+//   F_s(p) += alpha w(p) sum_t sum_c conj(dyp_tc(p)) Q_tcs(p),
+//   Q_tcs(p) = sum_{a in t} Z_t(c natm_t + a, s) S_a(p)
+// as D_t = A_t B_t^T with A_t = Z_t (rows 4 s + c, K = the type's atoms) and
+// B_t = the real views of the type's S (Mn) rows transposed (rows = reals of
+// the points, K = atoms), both FP16 levels (k_presplit_z, k_presplit_st).  One
+// output tile = 32 states x 4 channel rows x 128 reals (64 points); the CTAs
+// of one row tile walk the point tiles (persistent), the K chunks of a tile
+// (the first type's, then the second's, each into its own accumulator)
+// streamed like k_pp_tc's (warp 17 copies, warp 16 issues; two tiles in
+// flight), and warps 0-15 finish each tile: the channel rows of a state are
+// combined by lane shuffles, the types added, and F read and written once.
 constexpr int PF_KC = 64;                 // atoms per chunk (4 K steps)
 constexpr int PF_KS = PF_KC / 16;
 constexpr int PF_OPB = PF_KS * STEP_H;    // 32 KB
 constexpr int PF_STAGE = 2 * PF_OPB;      // 64 KB
 constexpr int PF_NST = 3;
 constexpr int PF_BYTES = 1024 + PF_NST * PF_STAGE;
-constexpr uint32_t PF_TMEM_COLS = 2 * ROWS;
+constexpr uint32_t PF_TMEM_COLS = 4 * ROWS;  // [tile parity][type] accumulators
 
 struct PFArgs {
-  const uint8_t* a;   // Z levels [row tile][K step][level][4 KB], nks K steps per row tile
-  const uint8_t* b;   // S^T levels, the same image over the point reals
-  int nks;            // K steps: cdiv(natm_t, 16)
-  int ntile;          // row tiles of B (point tiles)
-  int S, nch, npts;
-  const float* zmax;  // the FP16 scales of Z (pow2_scale(*zmax)) and of S^T
-  const float* smax;  // (pow2_scale(*smax)), as k_presplit_z / k_presplit_st
-  const float2* dyp;  // channel c at dyp + c ld_d (FP32)
-  int ld_d;
-  const double* w;    // per point
+  int ntyp;              // 1 or 2
+  const uint8_t* a[2];   // Z levels of type t [row tile][K step][level][4 KB], nks[t] K steps
+  const uint8_t* b[2];   // S^T levels of type t, the same image over the point reals
+  int nks[2];            // K steps of type t: cdiv(natm_t, 16)
+  int nch[2];
+  const float* zmax[2];  // the FP16 scales of Z_t (pow2_scale(*zmax[t])) and of S^T_t
+  const float* smax[2];  // (pow2_scale(*smax[t])), as k_presplit_z / k_presplit_st
+  const float2* dyp[2];  // type t, channel c at dyp[t] + c ld_d (FP32)
+  int ntile;             // row tiles of B (point tiles)
+  int S, npts, ld_d;
+  const double* w;       // per point
   double alpha;
-  double* f;          // [S][2 npts] (+=)
+  double* f;             // [S][2 npts] (+=)
   int* err;
 };
 
@@ -1369,10 +1372,12 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pf_tc(const PFArgs p) {
   const uint32_t base_s = tc::smem_u32(base);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m = blockIdx.y;
-  const int nkc = (p.nks + PF_KS - 1) / PF_KS;  // K chunks per tile
+  const int ntyp = p.ntyp;
+  const int nkc0 = (p.nks[0] + PF_KS - 1) / PF_KS;                   // K chunks per tile, type 0
+  const int nkc1 = ntyp > 1 ? (p.nks[1] + PF_KS - 1) / PF_KS : 0;    // type 1
   // this CTA's point tiles: blockIdx.x, + gridDim.x, ...
   const int ntl = p.ntile > (int)blockIdx.x ? (p.ntile - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-  const int nitem = ntl * nkc;
+  const int nitem = ntl * (nkc0 + nkc1);
 
   if (warp == 0) tc::tmem_alloc(&tslot, PF_TMEM_COLS);
   if (tid == 0) {
@@ -1398,63 +1403,86 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pf_tc(const PFArgs p) {
   if (warp == PP_LOAD_WARP) {
     if (lane == 0) {
       int req = 0;
-      // (tile, chunk) of item req counted along (no division by nkc in the loop)
-      for (int rt = 0, kc = 0; req < nitem; ++req, kc = kc + 1 == nkc ? 0 : kc + 1,
-               rt += kc == 0 ? 1 : 0) {
-        const int st = req % PF_NST;
-        if (req >= PF_NST && !tc::mbar_wait_fast(&empty[st], ((req - PF_NST) / PF_NST) & 1, stop)) {
-          *stop = 1;
-          break;
+      bool bad = false;
+      for (int tl = 0; tl < ntl && !bad; ++tl) {
+        const int n = blockIdx.x + tl * gridDim.x;
+        for (int t = 0; t < ntyp && !bad; ++t) {
+          const int nkc = t == 0 ? nkc0 : nkc1, nks = t == 0 ? p.nks[0] : p.nks[1];
+          const uint8_t* ga = t == 0 ? p.a[0] : p.a[1];
+          const uint8_t* gb = t == 0 ? p.b[0] : p.b[1];
+          for (int kc = 0; kc < nkc; ++kc, ++req) {
+            const int st = req % PF_NST;
+            if (req >= PF_NST &&
+                !tc::mbar_wait_fast(&empty[st], ((req - PF_NST) / PF_NST) & 1, stop)) {
+              *stop = 1;
+              bad = true;
+              break;
+            }
+            const int ks0 = kc * PF_KS, ksz = min(PF_KS, nks - ks0);
+            const uint32_t bytes = (uint32_t)ksz * STEP_H;
+            uint8_t* sa = base + (size_t)st * PF_STAGE;
+            tc::mbar_expect_tx(&full[st], 2 * bytes);
+            tc::bulk_g2s(sa, ga + ((size_t)m * nks + ks0) * STEP_H, bytes, &full[st]);
+            tc::bulk_g2s(sa + PF_OPB, gb + ((size_t)n * nks + ks0) * STEP_H, bytes, &full[st]);
+          }
         }
-        const int n = blockIdx.x + rt * gridDim.x;
-        const int ks0 = kc * PF_KS, ksz = min(PF_KS, p.nks - ks0);
-        const uint32_t bytes = (uint32_t)ksz * STEP_H;
-        uint8_t* sa = base + (size_t)st * PF_STAGE;
-        tc::mbar_expect_tx(&full[st], 2 * bytes);
-        tc::bulk_g2s(sa, p.a + ((size_t)m * p.nks + ks0) * STEP_H, bytes, &full[st]);
-        tc::bulk_g2s(sa + PF_OPB, p.b + ((size_t)n * p.nks + ks0) * STEP_H, bytes, &full[st]);
       }
       req_s = req;
     }
     __syncwarp();
   } else if (warp == PP_MMA_WARP) {
     if (lane == 0) {
-      int issued = 0;
-      for (int it = 0, tl = 0, kc = 0; it < nitem;
-           ++it, kc = kc + 1 == nkc ? 0 : kc + 1, tl += kc == 0 ? 1 : 0) {
-        const int st = it % PF_NST, acc = tl & 1;
-        if (kc == 0 && tl >= 2) {  // accumulator acc read back (tile tl - 2)
-          if (!tc::mbar_wait_fast(&tfree[acc], ((tl - 2) >> 1) & 1, stop)) break;
-          tc::fence_after_sync();
-        }
-        if (!tc::mbar_wait_fast(&full[st], (it / PF_NST) & 1, stop)) break;
-        tc::fence_after_sync();
-        const int ksz = min(PF_KS, p.nks - kc * PF_KS);
-        const uint32_t a0 = base_s + (uint32_t)(st * PF_STAGE), b0 = a0 + PF_OPB;
-        for (int s = 0; s < ksz; ++s) {
+      int it = 0;
+      bool bad = false;
+      for (int tl = 0; tl < ntl && !bad; ++tl) {
+        const int acc = tl & 1;
+        for (int t = 0; t < ntyp && !bad; ++t) {
+          const int nkc = t == 0 ? nkc0 : nkc1, nks = t == 0 ? p.nks[0] : p.nks[1];
+          for (int kc = 0; kc < nkc; ++kc, ++it) {
+            const int st = it % PF_NST;
+            if (t == 0 && kc == 0 && tl >= 2) {  // accumulator pair acc read back (tile tl - 2)
+              if (!tc::mbar_wait_fast(&tfree[acc], ((tl - 2) >> 1) & 1, stop)) {
+                bad = true;
+                break;
+              }
+              tc::fence_after_sync();
+            }
+            if (!tc::mbar_wait_fast(&full[st], (it / PF_NST) & 1, stop)) {
+              bad = true;
+              break;
+            }
+            tc::fence_after_sync();
+            const int ksz = min(PF_KS, nks - kc * PF_KS);
+            const uint32_t a0 = base_s + (uint32_t)(st * PF_STAGE), b0 = a0 + PF_OPB;
+            const uint32_t d = tbase + (uint32_t)((2 * acc + t) * ROWS);
+            for (int s = 0; s < ksz; ++s) {
 #pragma unroll
-          for (int t = 0; t < 3; ++t) {
-            const int la = t == 0 ? 1 : 0, lb = t == 1 ? 1 : 0;  // (m, h), (h, m), (h, h)
-            const uint64_t da = tc::smem_desc_kmajor(a0 + s * STEP_H + la * TILE_B, 128, 256);
-            const uint64_t db = tc::smem_desc_kmajor(b0 + s * STEP_H + lb * TILE_B, 128, 256);
-            const bool zero = kc == 0 && s == 0 && t == 0;
-            tc::mma_bf16(tbase + (uint32_t)(acc * ROWS), da, db, IDESC_H, zero ? 0u : 1u);
+              for (int q = 0; q < 3; ++q) {
+                const int la = q == 0 ? 1 : 0, lb = q == 1 ? 1 : 0;  // (m, h), (h, m), (h, h)
+                const uint64_t da = tc::smem_desc_kmajor(a0 + s * STEP_H + la * TILE_B, 128, 256);
+                const uint64_t db = tc::smem_desc_kmajor(b0 + s * STEP_H + lb * TILE_B, 128, 256);
+                const bool zero = kc == 0 && s == 0 && q == 0;
+                tc::mma_bf16(d, da, db, IDESC_H, zero ? 0u : 1u);
+              }
+            }
+            tc::commit(&empty[st]);
+            if (t == ntyp - 1 && kc == nkc - 1) tc::commit(&gfull[acc]);
           }
         }
-        tc::commit(&empty[st]);
-        if (kc == nkc - 1) tc::commit(&gfull[acc]);
-        issued = it + 1;
       }
-      if (issued < nitem) *stop = 1;
-      issued_s = issued;
+      if (it < nitem) *stop = 1;
+      issued_s = it;
     }
     __syncwarp();
   } else {
     // rows 4 s + c of this warp's lanes; columns (reals) 32 (warp / 4).. of the tile
     const int rl = 32 * (warp & 3) + lane;
     const int rg = m * ROWS + rl, s = rg >> 2, c = rg & 3;
-    const bool live = s < p.S && c < p.nch;
-    const double rinv = 1.0 / ((double)tc::pow2_scale(*p.zmax) * (double)tc::pow2_scale(*p.smax));
+    // 1 / (Z scale x S^T scale) of each type: powers of two, folded into dyp exactly
+    float rinv[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+      rinv[t] = t < ntyp ? 1.f / (tc::pow2_scale(*p.zmax[t]) * tc::pow2_scale(*p.smax[t])) : 0.f;
     int bad = 0;
     for (int tl = 0; tl < ntl && !bad; ++tl) {
       const int acc = tl & 1;
@@ -1463,48 +1491,62 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pf_tc(const PFArgs p) {
         break;
       }
       tc::fence_after_sync();
-      float v[32];
-      tc::tmem_ld32(tbase + tlanes + (uint32_t)(acc * ROWS + 32 * (warp >> 2)), v);
+      const int n = blockIdx.x + tl * gridDim.x;
+      const int pt0 = (n * ROWS + 32 * (warp >> 2)) >> 1;  // 16 points
+      // conj(dyp_tc) Q_tcs summed over the state's 4 channel lanes (shuffles)
+      // and the types; then lane c of the state adds points pt0 + c, + 4, + 8,
+      // + 12 into F
+      const bool wr = s < p.S;
+      double2* fr = reinterpret_cast<double2*>(p.f + (size_t)(wr ? s : 0) * 2 * p.npts);
+      float ox4[4] = {0.f, 0.f, 0.f, 0.f}, oy4[4] = {0.f, 0.f, 0.f, 0.f};
+      double2 fo[4];
+      for (int t = 0; t < ntyp; ++t) {
+        if (t == ntyp - 1) {  // F's loads in flight during the last type's products
+#pragma unroll
+          for (int e4 = 0; e4 < 4; ++e4) {
+            const int pt = pt0 + 4 * e4 + c;
+            fo[e4] = (wr && pt < p.npts) ? fr[pt] : make_double2(0.0, 0.0);
+          }
+        }
+        const bool live = s < p.S && c < (t == 0 ? p.nch[0] : p.nch[1]);
+        const float2* dyp = t == 0 ? p.dyp[0] : p.dyp[1];
+        const float ri = t == 0 ? rinv[0] : rinv[1];
+#pragma unroll
+        for (int hf = 0; hf < 2; ++hf) {  // 8 points (16 columns) at a time
+          float2 d[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const int pt = pt0 + 8 * hf + e;
+            const float2 q = (live && pt < p.npts) ? dyp[(size_t)c * p.ld_d + pt]
+                                                   : make_float2(0.f, 0.f);
+            d[e] = make_float2(q.x * ri, q.y * ri);
+          }
+          uint32_t v[16];
+          tc::tmem_ld16(tbase + tlanes + (uint32_t)((2 * acc + t) * ROWS + 32 * (warp >> 2) + 16 * hf),
+                        v);
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const float qx = __uint_as_float(v[2 * e]), qy = __uint_as_float(v[2 * e + 1]);
+            float ox = fmaf(d[e].x, qx, d[e].y * qy), oy = fmaf(d[e].x, qy, -d[e].y * qx);
+            ox += __shfl_xor_sync(0xffffffffu, ox, 1);
+            oy += __shfl_xor_sync(0xffffffffu, oy, 1);
+            ox += __shfl_xor_sync(0xffffffffu, ox, 2);
+            oy += __shfl_xor_sync(0xffffffffu, oy, 2);
+            if ((e & 3) == c) {  // compile-time e, runtime c: keep this lane's four
+              ox4[2 * hf + (e >> 2)] += ox;
+              oy4[2 * hf + (e >> 2)] += oy;
+            }
+          }
+        }
+      }
       tc::fence_before_sync();
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&tfree[acc]);
-      const int n = blockIdx.x + tl * gridDim.x;
-      const int pt0 = (n * ROWS + 32 * (warp >> 2)) >> 1;  // 16 points
-      // conj(dyp_c) Q_cs summed over the state's 4 channel lanes (shuffles);
-      // then lane c of the state adds points pt0 + c, + 4, + 8, + 12 into F
-      const bool wr = s < p.S;
-      double2* fr = reinterpret_cast<double2*>(p.f + (size_t)(wr ? s : 0) * 2 * p.npts);
-      float2 d[16];
-#pragma unroll
-      for (int e = 0; e < 16; ++e) {
-        const int pt = pt0 + e;
-        d[e] = (live && pt < p.npts) ? p.dyp[(size_t)c * p.ld_d + pt] : make_float2(0.f, 0.f);
-      }
-      double2 fo[4];
-#pragma unroll
-      for (int e4 = 0; e4 < 4; ++e4) {
-        const int pt = pt0 + 4 * e4 + c;
-        fo[e4] = (wr && pt < p.npts) ? fr[pt] : make_double2(0.0, 0.0);
-      }
-      float ox4[4], oy4[4];
-#pragma unroll
-      for (int e = 0; e < 16; ++e) {
-        const float qx = v[2 * e], qy = v[2 * e + 1];
-        float ox = fmaf(d[e].x, qx, d[e].y * qy), oy = fmaf(d[e].x, qy, -d[e].y * qx);
-        ox += __shfl_xor_sync(0xffffffffu, ox, 1);
-        oy += __shfl_xor_sync(0xffffffffu, oy, 1);
-        ox += __shfl_xor_sync(0xffffffffu, ox, 2);
-        oy += __shfl_xor_sync(0xffffffffu, oy, 2);
-        if ((e & 3) == c) {  // compile-time e, runtime c: keep this lane's four
-          ox4[e >> 2] = ox;
-          oy4[e >> 2] = oy;
-        }
-      }
 #pragma unroll
       for (int e4 = 0; e4 < 4; ++e4) {
         const int pt = pt0 + 4 * e4 + c;
         if (wr && pt < p.npts) {
-          const double sc = p.alpha * p.w[pt] * rinv;
+          const double sc = p.alpha * p.w[pt];
           fr[pt] = make_double2(fma(sc, (double)ox4[e4], fo[e4].x), fma(sc, (double)oy4[e4], fo[e4].y));
         }
       }
@@ -1741,39 +1783,43 @@ int ees_tc_sums_pre(cpstep_ctx* c, int nch, const float* dmax, const uint8_t* bl
   return pc_splitk_reduce_launch(c, nsplit, S, nch * jp, 1.0, 0.0, C, S, 0);
 }
 
-// EES psi force of one atom type from pre-split operands (k_pf_tc): Z
-// column-major [S][ldz] (inner index c natm_t + a), the type's FP32 Mn rows
-// sv[a ld_s + k]; F += alpha w (conj(dyp) S Z) as the in-CTA form below.
-// zlv and stlv hold the two operands' levels.
-int ees_tc_force_pre(cpstep_ctx* c, const float* sv, long long ld_s, const float2* dyp, int ld_d,
-                     int nch, int natm_t, const double* Z, int ldz, double alpha, double* fpsi,
-                     const float* smax, const float* zmax, uint8_t* zlv, size_t zlv_bytes,
-                     uint8_t* stlv, size_t stlv_bytes) {
+// EES psi force of one or two atom types from pre-split operands (k_pf_tc):
+// per type Z column-major [S][ldz] (inner index c natm_t + a) and the FP32
+// Mn rows sv[a ld_s + k], split into zlv and stlv; F += alpha w sum_t
+// (conj(dyp_t) S_t Z_t), F read and written once.
+int ees_tc_force_pre(cpstep_ctx* c, int ntyp, const EesForceType* ty, int ld_d, double alpha,
+                     double* fpsi, size_t zlv_bytes, size_t stlv_bytes) {
   using namespace pctc;
   const int S = c->nstates, npts = c->npts, kr = 2 * npts;
-  const int nks = cdiv(natm_t, 16), tm = cdiv(4 * S, ROWS), ntile = cdiv(kr, ROWS);
-  if (nch < 1 || nch > 4 || natm_t < 1 || (ld_s & 3) || (ld_d & 1) || !al16(fpsi) ||
-      !al16(zlv) || !al16(stlv) || zlv_bytes < (size_t)tm * nks * STEP_H ||
-      stlv_bytes < (size_t)ntile * nks * STEP_H || ldz < nch * natm_t)
-    return CPSTEP_ERR_ARG;
-  const long long nz = (long long)tm * ROWS * nks * 2, ns = (long long)ntile * ROWS * nks * 2;
-  k_presplit_z<<<(unsigned)((nz + 255) / 256), 256, 0, c->stream>>>(Z, ldz, S, nch, natm_t, nks,
-                                                                    tm * ROWS, zmax, zlv);
-  CPSTEP_LAUNCH_CHECK();
-  k_presplit_st<<<(unsigned)((ns + 255) / 256), 256, 0, c->stream>>>(sv, ld_s, kr, natm_t, nks,
-                                                                     ntile * ROWS, smax, stlv);
-  CPSTEP_LAUNCH_CHECK();
+  const int tm = cdiv(4 * S, ROWS), ntile = cdiv(kr, ROWS);
+  if (ntyp < 1 || ntyp > 2 || (ld_d & 1) || !al16(fpsi)) return CPSTEP_ERR_ARG;
   PFArgs pf{};
-  pf.a = zlv;
-  pf.b = stlv;
-  pf.nks = nks;
+  pf.ntyp = ntyp;
+  for (int t = 0; t < ntyp; ++t) {
+    const EesForceType& y = ty[t];
+    const int nks = cdiv(y.natm_t, 16);
+    if (y.nch < 1 || y.nch > 4 || y.natm_t < 1 || (y.ld_s & 3) || !al16(y.zlv) ||
+        !al16(y.stlv) || zlv_bytes < (size_t)tm * nks * STEP_H ||
+        stlv_bytes < (size_t)ntile * nks * STEP_H || y.ldz < y.nch * y.natm_t)
+      return CPSTEP_ERR_ARG;
+    const long long nz = (long long)tm * ROWS * nks * 2, ns = (long long)ntile * ROWS * nks * 2;
+    k_presplit_z<<<(unsigned)((nz + 255) / 256), 256, 0, c->stream>>>(
+        y.Z, y.ldz, S, y.nch, y.natm_t, nks, tm * ROWS, y.zmax, y.zlv);
+    CPSTEP_LAUNCH_CHECK();
+    k_presplit_st<<<(unsigned)((ns + 255) / 256), 256, 0, c->stream>>>(
+        y.sv, y.ld_s, kr, y.natm_t, nks, ntile * ROWS, y.smax, y.stlv);
+    CPSTEP_LAUNCH_CHECK();
+    pf.a[t] = y.zlv;
+    pf.b[t] = y.stlv;
+    pf.nks[t] = nks;
+    pf.nch[t] = y.nch;
+    pf.zmax[t] = y.zmax;
+    pf.smax[t] = y.smax;
+    pf.dyp[t] = y.dyp;
+  }
   pf.ntile = ntile;
   pf.S = S;
-  pf.nch = nch;
   pf.npts = npts;
-  pf.zmax = zmax;
-  pf.smax = smax;
-  pf.dyp = dyp;
   pf.ld_d = ld_d;
   pf.w = c->d_wpt;
   pf.alpha = alpha;
