@@ -60,9 +60,18 @@
 // x s = h + m (22 significant bits of the FP32 value; s brings the largest
 // magnitude to [2^13, 2^14)), and multiplied as h m + m h + h h (three MMAs
 // per K step, kind::f16 with FP16 A and B); k_pp_tc (the sums, split-K with
-// FP64 folds every 512 reals) and k_pf_tc (the psi force, persistent over
-// point tiles) stream both operands with bulk copies and leave the CTA no
-// operand work.
+// FP64 folds every 512 reals) and k_pf_tc (the psi force of both atom types,
+// persistent over point tiles) stream both operands with bulk copies and
+// leave the CTA no operand work.
+//
+// Which kernel runs a PairCalc product (mixed context):
+//   overlap S, lambda     fewer than 256 states: k_pc_tc MODE 0 (in-CTA split);
+//                         256 or more: both operands split once into BF16
+//                         levels (k_presplit) and streamed by k_pp_tc<3,false>
+//   back-multiply         nin <= 128: k_bm_tc (two CTAs per SM, PsiV reset in
+//                         the epilogue); 128 < nin < 256: k_pc_tc MODE 1;
+//                         256 or more: in^T split by k_presplit_t and streamed
+//                         by k_pp_tc<3,true>
 #include "ctx.cuh"
 #include "tc_sm100.cuh"
 
