@@ -981,7 +981,10 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
   uint8_t* base = dsm + (((s0 + 1023u) & ~1023u) - s0);
   const uint32_t base_s = tc::smem_u32(base);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int r0 = blockIdx.x * ROWS, c0 = blockIdx.y * ROWS;
+  // row and column tile; the back-multiply runs the column tiles of a point
+  // tile side by side (grid x), so that they read its A levels from L2
+  const int rt = BM ? blockIdx.y : blockIdx.x, ct = BM ? blockIdx.x : blockIdx.y;
+  const int r0 = rt * ROWS, c0 = ct * ROWS;
   const int kbeg = blockIdx.z * p.kslab, kend = min(p.K, kbeg + p.kslab);
   const int nch = kend > kbeg ? (kend - kbeg + PP_KC - 1) / PP_KC : 0;
   constexpr int nf = NL == 2 ? 512 / PP_KC : 128 / PP_KC;  // chunks per fold group
@@ -1023,8 +1026,8 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
           break;
         }
         const size_t kstep = (size_t)((kbeg + req * PP_KC) >> 4);
-        const uint8_t* ga = p.a + ((size_t)blockIdx.x * p.nsp + kstep) * STEP;
-        const uint8_t* gb = p.b + ((size_t)blockIdx.y * p.nsp + kstep) * STEP;
+        const uint8_t* ga = p.a + ((size_t)rt * p.nsp + kstep) * STEP;
+        const uint8_t* gb = p.b + ((size_t)ct * p.nsp + kstep) * STEP;
         uint8_t* sa = base + (size_t)st * PP_STAGE;
         tc::mbar_expect_tx(&full[st], PP_STAGE);
         tc::bulk_g2s(sa, ga, PP_OPB, &full[st]);
@@ -1918,11 +1921,13 @@ static int backmul_tc(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
   if (!pc_tc_usable(c) || (K & 1) || (ldm & 1) || (ldi & 1) || !al16(Mcm) || !al16(in))
     return CPSTEP_OK;
   if (psiv_flag && psiv_no != in) return CPSTEP_ERR_ARG;  // psi_no is the input
+  // many states: both operands split once and streamed (point tiles on grid y)
+  const bool stream = nin >= 2 * ROWS && cdiv(K, ROWS) <= 65535;
   // the PsiV reset rides on k_bm_tc with one column tile, or on the streaming form
-  if (psiv_flag && (nin <= 128 ? nout > ROWS : nin < 2 * ROWS)) return CPSTEP_OK;
+  if (psiv_flag && (nin <= 128 ? nout > ROWS : !stream)) return CPSTEP_OK;
   if (int rc = lv_reserve(c, pre_bytes(nout, nin))) return rc;
   if (int rc = presplit(c, Mcm, ldm, nout, nin, nullptr, 1, c->d_lv)) return rc;
-  if (nin >= 2 * ROWS) {  // many states: both operands split once, streamed
+  if (stream) {
     const int nsp = pre_nsp(nin);
     if (int rc = hlv_reserve(c, 0, pre_bytes(K, nin))) return rc;
     const long long ta = (long long)cdiv(K, ROWS) * nsp * 8 * 32;
@@ -1950,7 +1955,7 @@ static int backmul_tc(cpstep_ctx* c, const double* Mcm, int ldm, const double* i
     pp.psiv_flag = psiv_flag;
     pp.psiv_v = psiv_v;
     pp.rdt = rdt;
-    if (int rc = pp_launch<3, true>(c, dim3(cdiv(K, ROWS), cdiv(nout, ROWS), 1), pp)) return rc;
+    if (int rc = pp_launch<3, true>(c, dim3(cdiv(nout, ROWS), cdiv(K, ROWS), 1), pp)) return rc;
     *used = true;
     return CPSTEP_OK;
   }
