@@ -1149,20 +1149,34 @@ __global__ void __launch_bounds__(PP_NTHR, 1) k_pp_tc(const PPArgs p) {
     }
     tc::bar_sync(WBAR, NW);
     const bool pv = p.psiv_flag && *p.psiv_flag;
-#pragma unroll 4
-    for (int q = tid; q < ROWS * ROWS; q += NW) {
-      const int il = q / ROWS, pl = q % ROWS;
-      const int i = c0 + il, pt = r0 + pl;
-      if (i < p.N && pt < p.M) {
-        const double dg = i < p.K ? p.in[(size_t)i * p.ldi + pt] : 0.0;
-        const double ov = (p.beta != 0.0 || pv) ? p.out[(size_t)i * p.ldo + pt] : 0.0;
-        const double sc = p.alpha * (p.w ? p.w[pt >> 1] : 1.0);
-        const double v = sc * fma(mdg[il], dg, tile[pl * (ROWS + 1) + il]);
-        const double o = p.beta == 0.0 ? v : fma(p.beta, ov, v);
-        p.out[(size_t)i * p.ldo + pt] = o;
-        if (pv) {
-          p.psiv_v[(size_t)i * p.ldo + pt] = (o - ov) * p.rdt;
-          const_cast<double*>(p.in)[(size_t)i * p.ldi + pt] = o;
+    const bool rd = p.beta != 0.0 || pv;
+    const int pl = tid % ROWS, il0 = tid / ROWS;  // this thread: point pl, columns il0 + 4 k
+    const int pt = r0 + pl;
+    const double sc = pt < p.M ? p.alpha * (p.w ? p.w[pt >> 1] : 1.0) : 0.0;
+    // 32 elements per thread in two batches of 16: every load of a batch is
+    // issued before its first store (a store to out or, with the PsiV reset,
+    // to in would otherwise hold each next load back)
+#pragma unroll
+    for (int bt = 0; bt < 2; ++bt) {
+      double dg[16], ov[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const int il = il0 + 4 * (16 * bt + k), i = c0 + il;
+        const bool ok = i < p.N && pt < p.M;
+        dg[k] = (ok && i < p.K) ? p.in[(size_t)i * p.ldi + pt] : 0.0;
+        ov[k] = (ok && rd) ? p.out[(size_t)i * p.ldo + pt] : 0.0;
+      }
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const int il = il0 + 4 * (16 * bt + k), i = c0 + il;
+        if (i < p.N && pt < p.M) {
+          const double v = sc * fma(mdg[il], dg[k], tile[pl * (ROWS + 1) + il]);
+          const double o = p.beta == 0.0 ? v : fma(p.beta, ov[k], v);
+          p.out[(size_t)i * p.ldo + pt] = o;
+          if (pv) {
+            p.psiv_v[(size_t)i * p.ldo + pt] = (o - ov[k]) * p.rdt;
+            const_cast<double*>(p.in)[(size_t)i * p.ldi + pt] = o;
+          }
         }
       }
     }
